@@ -1,0 +1,168 @@
+/*
+ * Plain-data descriptions of SHAPE's model-evaluation inputs, shared by the
+ * B200 engine's C ABI (shape_b200.h) and by the CPU oracle used in tests.
+ *
+ * Every struct holds plain numbers and host pointers only. Array layouts
+ * mirror the reference's NR matrices so that a shim can fill them from the
+ * reference structs without reordering:
+ *   - POS images (struct pos_t, src/shape/shape2.h:1061-1094) are
+ *     (2n+1) x (2n+1), x index i in [-n, n] major, y index j contiguous:
+ *     element [i][j] lives at (i+n)*(2n+1) + (j+n);
+ *   - delay-Doppler images (struct deldopfrm_t obs/fit/oneovervar,
+ *     src/shape/shape2.h:1114-1182) are ndel x ndop, delay row major:
+ *     element [idel][idop] (1-based in the reference) lives at
+ *     (idel-1)*ndop + (idop-1);
+ *   - 3x3 transforms are row-major double[9], the reference's double[3][3].
+ */
+#ifndef SHAPE_TYPES_H
+#define SHAPE_TYPES_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Constants of the reference (src/shape/const.h:134-193). */
+#define SHAPE_HUGENUMBER 1.0e20
+#define SHAPE_SMALLVAL 1.0e-10
+#define SHAPE_TINYCALFACT 1.0e-40
+#define SHAPE_KM2US 6.67128190396304
+#define SHAPE_KM2HZFACT 7.72139109254982e-5
+#define SHAPE_MAXBINS 100
+#define SHAPE_AU 1.4959787061e8
+#define SHAPE_PIE 3.141592653589793
+
+/* Delay-Doppler code methods (src/shape/const.h:159-161). */
+#define SHAPE_CODE_SHORT 0
+#define SHAPE_CODE_LONG_ORIG 1
+#define SHAPE_CODE_LONG_MOD 2
+
+/* Radar scattering laws evaluated by radlaw (src/shape/radlaw.c:44-148,
+ * type codes from src/shape/shape2.h:847-880). The facet-dependent laws
+ * (TABULARLAW, HARMCOSINE_DIFF, INHOCOSINE_DIFF) are not supported. */
+#define SHAPE_RADLAW_COSINE_DIFF 1
+#define SHAPE_RADLAW_GAUSSIAN 2
+#define SHAPE_RADLAW_HAGFORS 3
+#define SHAPE_RADLAW_COSINE_QS 4
+#define SHAPE_RADLAW_GAUSSIAN_COSINE 5
+#define SHAPE_RADLAW_HAGFORS_COSINE 6
+#define SHAPE_RADLAW_COSINE_COSINE 7
+
+/* Optical scattering laws evaluated by apply_photo
+ * (src/shape/apply_photo.c:85-133, 226-248; codes src/shape/shape2.h:902-960).
+ * Hapke and the facet-dependent (harm/inho) laws are not supported. */
+#define SHAPE_OPTLAW_LAMBERT 2
+#define SHAPE_OPTLAW_LOMMEL 3
+#define SHAPE_OPTLAW_KAASALAINEN 11
+
+/* One VERTEX-type model component (struct vertices_t, src/shape/shape2.h:797-805;
+ * struct vertex_t/facet_t :723-748). Realization follows realize_coordinates
+ * (src/shape/realize_mod.c:444-479, 532-563): x = scale * (u*r + a). */
+typedef struct shape_model_desc {
+    int nv;                 /* vertices */
+    int nf;                 /* facets */
+    const double *a;        /* [nv][3] base points (vertex_t.a) */
+    const double *u;        /* [nv][3] directions of variation (vertex_t.u) */
+    const double *r;        /* [nv] deviations along u (vertex_t.r.val) */
+    double scale[3];        /* component scale factors (vertices_t.scalefactor[].val) */
+    const int *fv;          /* [nf][3] facet corner vertex indices (facet_t.v) */
+    const int *af_ptr;      /* [nv+1] CSR offsets into af_idx */
+    const int *af_idx;      /* attached-facet lists (vertex_t.af), in model-file order */
+} shape_model_desc;
+
+/* Radar scattering law parameters (union radscat_t, src/shape/shape2.h:852-900). */
+typedef struct shape_radar_law {
+    int type;               /* SHAPE_RADLAW_* */
+    double diff_R, diff_C;  /* diffuse cosine law: RC_t.R, RC_t.C (or hybrid.diff) */
+    double qs_R, qs_C;      /* quasispecular part: quasispec_t.R, .C (or hybrid.qs) */
+    double qs_cos_cutoff;   /* quasispec_t.cos_cutoff */
+} shape_radar_law;
+
+/* Optical scattering law parameters (union optscat_t, src/shape/shape2.h:902-992). */
+typedef struct shape_optical_law {
+    int type;               /* SHAPE_OPTLAW_* */
+    double R;               /* R_t.R (Lambert, Lommel) or kaas_t.R */
+    double wt, A0, D, k;    /* kaas_t fields (Kaasalainen only) */
+} shape_optical_law;
+
+/* Evaluation switches taken from struct par_t (src/shape/shape2.h:415-710). */
+typedef struct shape_eval_params {
+    int pos_smooth;         /* par->pos_smooth (default 1, src/shape/read_par.c:1372) */
+    int nsinc2;             /* par->nsinc2 */
+    int sinc2width;         /* par->sinc2width */
+    double mask_tol;        /* par->mask_tol (posmask shadow tolerance, km) */
+    double mincosine_seen;  /* par->mincosine_seen */
+    int mark_seen;          /* 1 = update per-facet "seen" flags (s != par->exclude_seen) */
+} shape_eval_params;
+
+/* One delay-Doppler frame with a single view (struct deldopfrm_t +
+ * struct deldopview_t, src/shape/shape2.h:1097-1182). */
+typedef struct shape_deldop_frame {
+    int pos_n;              /* POS half-width n: (2n+1)^2 pixels */
+    double km_per_pixel;    /* pos_t.km_per_pixel */
+    double ae[9];           /* view ecliptic -> body transform */
+    double oe[9];           /* view ecliptic -> observer transform */
+    double spin[3];         /* view total spin vector, ecliptic coords (rad/day) */
+    double deloff, dopoff;  /* view delay / Doppler offsets (bins) */
+    int ndel, ndop;         /* delay rows, Doppler columns */
+    double delcom_vig;      /* COM delay bin (1-based) after vignetting */
+    double dopcom_vig;      /* COM Doppler bin (1-based) after vignetting */
+    double dopDC_vig;       /* DC Doppler bin (1-based) after vignetting */
+    double weight;          /* frame weight */
+    double dof;             /* frame degrees of freedom */
+    int cal_floating;       /* cal.state == 'f' */
+    double cal;             /* cal.val when not floating */
+} shape_deldop_frame;
+
+/* Set-level delay-Doppler parameters (struct deldop_t, src/shape/shape2.h:1184-1215). */
+typedef struct shape_deldop_set {
+    double del_per_pixel;   /* usec per row */
+    double dop_per_pixel;   /* Hz per column */
+    double Ftx;             /* transmitter frequency (MHz) */
+    double dopscale;        /* dopscale.val */
+    int codemethod;         /* SHAPE_CODE_* */
+    int spb;                /* samples per baud */
+    int stride;             /* spb between adjacent rows */
+    int dopfftlen;          /* Doppler FFT length */
+    shape_radar_law law;    /* photo->radar[deldop->iradlaw] */
+} shape_deldop_set;
+
+/* One calculated lightcurve epoch (struct crvrend_t, src/shape/shape2.h:1344-1356). */
+typedef struct shape_lghtcrv_point {
+    int pos_n;
+    double km_per_pixel;
+    double ae[9], oe[9], se[9];
+    double solar_phase;     /* lghtcrv->solar_phase[i] (radians) */
+} shape_lghtcrv_point;
+
+/* Lightcurve set (struct lghtcrv_t, src/shape/shape2.h:1358-1398) with one view per point. */
+typedef struct shape_lghtcrv_set {
+    int ncalc;              /* calculated epochs */
+    int n;                  /* observed points */
+    const double *x;        /* [ncalc] calculated epochs (ascending) */
+    const double *t;        /* [n] observation epochs */
+    const double *obs;      /* [n] observed intensities */
+    const double *oneovervar; /* [n] 1/variance */
+    double weight, dof;
+    int cal_floating;
+    double cal;
+    shape_optical_law law;  /* photo->optical[lghtcrv->ioptlaw] */
+} shape_lghtcrv_set;
+
+/* Per-frame results of one delay-Doppler evaluation. */
+typedef struct shape_deldop_result {
+    int outbnd;             /* posvis returned 1 (model beyond POS window) */
+    double posbnd_logfactor;/* pos_t.posbnd_logfactor */
+    int badradar;           /* pos2deldop returned 1 */
+    double badradar_logfactor;
+    int xlim[2], ylim[2];   /* POS region touched by the model */
+    int idellim[2], idoplim[2];
+    double dellim[2], doplim[2];
+    double o2, m2, om;      /* chi-square partial sums */
+    double cal;             /* calibration used (floating: om/m2) */
+    double chi2;            /* frame chi-square */
+} shape_deldop_result;
+
+#ifdef __cplusplus
+}
+#endif
+#endif

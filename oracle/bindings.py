@@ -1,0 +1,289 @@
+"""Python bindings for the CPU checkers. TEST INFRASTRUCTURE ONLY.
+
+- ``Oracle``: the plain-C restatement (oracle/shape_oracle.c -> liboracle.so).
+- ``Reference``: the reference's own CPU code compiled in place
+  (oracle/build_ref.sh -> oracle/_ref/libshape_ref.so), driven through the
+  direct-call harness oracle/ref_harness.c.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+arm import this module.
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(REPO, "shape-cuda-v1.2_b200", "python"))
+
+from shape_b200 import ctypes_defs as cd  # noqa: E402
+
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libshape_ref.so")
+
+
+class OrcReal(C.Structure):
+    _fields_ = [("nv", C.c_int), ("nf", C.c_int), ("x", cd.dptr), ("vn", cd.dptr),
+                ("fn", cd.dptr), ("area", cd.dptr), ("fv", cd.iptr)]
+
+
+class OrcPos(C.Structure):
+    _fields_ = [("n", C.c_int), ("kmpp", C.c_double),
+                ("ae", C.c_double * 9), ("oe", C.c_double * 9), ("se", C.c_double * 9),
+                ("bistatic", C.c_int),
+                ("b", cd.dptr), ("cose", cd.dptr), ("cosi", cd.dptr), ("z", cd.dptr),
+                ("f", cd.iptr), ("cosill", cd.dptr), ("zill", cd.dptr), ("fill", cd.iptr),
+                ("xlim", C.c_int * 2), ("ylim", C.c_int * 2),
+                ("xlim2", C.c_int * 2), ("ylim2", C.c_int * 2),
+                ("posbnd_logfactor", C.c_double)]
+
+
+def _load(path, builder):
+    if not os.path.exists(path):
+        raise RuntimeError("%s missing: run %s" % (path, builder))
+    return C.CDLL(path)
+
+
+class Oracle:
+    """CPU restatement of the reference hot path (bit-exact FP64 order)."""
+
+    def __init__(self):
+        L = self.lib = _load(ORACLE_SO, "oracle/build_oracle.sh")
+        P = C.POINTER
+        L.orc_realize_vertex.argtypes = [P(cd.ModelDesc), cd.dptr, cd.dptr, cd.dptr, cd.dptr]
+        L.orc_pos_alloc.argtypes = [P(OrcPos), C.c_int, C.c_int]
+        L.orc_pos_free.argtypes = [P(OrcPos)]
+        L.orc_deldop_frame.argtypes = [P(cd.EvalParams), P(OrcReal), P(cd.DeldopSet),
+                                       P(cd.DeldopFrame), cd.dptr, cd.dptr, P(OrcPos),
+                                       cd.dptr, C.c_char_p, P(cd.DeldopResult)]
+        L.orc_lghtcrv_point.restype = C.c_double
+        L.orc_lghtcrv_point.argtypes = [P(cd.EvalParams), P(OrcReal), P(cd.OpticalLaw),
+                                        P(cd.LghtcrvPoint), P(OrcPos), C.c_char_p,
+                                        P(C.c_int), P(C.c_double)]
+        L.orc_spline_natural.argtypes = [cd.dptr, cd.dptr, C.c_int, cd.dptr]
+        L.orc_splint.restype = C.c_double
+        L.orc_splint.argtypes = [cd.dptr, cd.dptr, cd.dptr, C.c_int, C.c_double]
+        L.orc_radlaw.restype = C.c_double
+        L.orc_radlaw.argtypes = [P(cd.RadarLaw), C.c_double]
+
+    def realize(self, model):
+        d = model.desc()
+        x = np.zeros((model.nv, 3)); vn = np.zeros((model.nv, 3))
+        fn = np.zeros((model.nf, 3)); area = np.zeros(model.nf)
+        self.lib.orc_realize_vertex(C.byref(d), cd.as_dptr(x), cd.as_dptr(vn),
+                                    cd.as_dptr(fn), cd.as_dptr(area))
+        return {"x": x, "vn": vn, "fn": fn, "area": area, "fv": model.fv}
+
+    def _real(self, real):
+        r = OrcReal()
+        r.nv, r.nf = real["x"].shape[0], real["fn"].shape[0]
+        r.x, r.vn, r.fn = cd.as_dptr(real["x"]), cd.as_dptr(real["vn"]), cd.as_dptr(real["fn"])
+        r.area, r.fv = cd.as_dptr(real["area"]), cd.as_iptr(real["fv"])
+        return r
+
+    @staticmethod
+    def pos_arrays(pos):
+        side = 2 * pos.n + 1
+        np_ = side * side
+        get = lambda p, ct: np.ctypeslib.as_array(C.cast(p, C.POINTER(ct)), shape=(np_,)).copy()
+        return {"z": get(pos.z, C.c_double), "cose": get(pos.cose, C.c_double),
+                "cosi": get(pos.cosi, C.c_double), "f": get(pos.f, C.c_int),
+                "zill": get(pos.zill, C.c_double), "fill": get(pos.fill, C.c_int),
+                "xlim": tuple(pos.xlim), "ylim": tuple(pos.ylim),
+                "xlim2": tuple(pos.xlim2), "ylim2": tuple(pos.ylim2)}
+
+    def eval_deldop(self, model, ds, params, real=None, keep_pos=False):
+        """calc_deldop + chi2_deldop over every frame of `ds`. Returns
+        per-frame fits, results, seen flags and (optionally) POS maps."""
+        real = real or self.realize(model)
+        R = self._real(real)
+        seen = C.create_string_buffer(model.nf)
+        fits, results, poss = [], [], []
+        for f, fr in enumerate(ds.frames):
+            pos = OrcPos()
+            self.lib.orc_pos_alloc(C.byref(pos), fr.pos_n, 0)
+            fit = np.zeros(fr.ndel * fr.ndop)
+            res = cd.DeldopResult()
+            obs = np.ascontiguousarray(ds.frame_obs(f))
+            oov = np.ascontiguousarray(ds.oneovervar[ds.offsets[f]:ds.offsets[f + 1]])
+            self.lib.orc_deldop_frame(C.byref(params), C.byref(R), C.byref(ds.set), C.byref(fr),
+                                      cd.as_dptr(obs), cd.as_dptr(oov), C.byref(pos),
+                                      cd.as_dptr(fit), seen, C.byref(res))
+            fits.append(fit)
+            results.append(cd.result_to_dict(res))
+            if keep_pos:
+                poss.append(self.pos_arrays(pos))
+            self.lib.orc_pos_free(C.byref(pos))
+        return {"fits": fits, "results": results, "pos": poss,
+                "seen": np.frombuffer(seen.raw, dtype=np.uint8).copy(), "real": real}
+
+    def eval_lghtcrv(self, model, ds, params, real=None, keep_pos=False):
+        """calc_lghtcrv + chi2_lghtcrv for one lightcurve dataset."""
+        real = real or self.realize(model)
+        R = self._real(real)
+        seen = C.create_string_buffer(model.nf)
+        ys, poss, flags = [], [], []
+        for p in ds.points:
+            pos = OrcPos()
+            self.lib.orc_pos_alloc(C.byref(pos), p.pos_n, 1)
+            ob, lg = C.c_int(0), C.c_double(0.0)
+            y = self.lib.orc_lghtcrv_point(C.byref(params), C.byref(R), C.byref(ds.set.law),
+                                           C.byref(p), C.byref(pos), seen, C.byref(ob), C.byref(lg))
+            ys.append(y)
+            flags.append((ob.value, lg.value))
+            if keep_pos:
+                poss.append(self.pos_arrays(pos))
+            self.lib.orc_pos_free(C.byref(pos))
+        y = np.array(ys)
+        fit = self.spline_fit(ds.x, y, ds.t)
+        o2 = float(np.sum(ds.obs * ds.obs * ds.oneovervar))
+        m2 = float(np.sum(fit * fit * ds.oneovervar))
+        om = float(np.sum(fit * ds.obs * ds.oneovervar))
+        cal = (om / m2 if om > 0 else 1e-40) if ds.set.cal_floating else ds.set.cal
+        chi2 = ds.set.weight * (o2 - 2 * cal * om + cal * cal * m2)
+        return {"y": y, "fit": fit, "cal": cal, "chi2": chi2, "pos": poss, "flags": flags,
+                "seen": np.frombuffer(seen.raw, dtype=np.uint8).copy()}
+
+    def spline_fit(self, x, y, t):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        y2 = np.zeros_like(y)
+        self.lib.orc_spline_natural(cd.as_dptr(x), cd.as_dptr(y), len(x), cd.as_dptr(y2))
+        return np.array([self.lib.orc_splint(cd.as_dptr(x), cd.as_dptr(y), cd.as_dptr(y2), len(x), float(tt))
+                         for tt in t])
+
+
+OBJFN = C.CFUNCTYPE(C.c_double, C.c_double)
+
+
+class Reference:
+    """The reference's own CPU code (oracle/_ref/libshape_ref.so)."""
+
+    def __init__(self):
+        L = self.lib = _load(REF_SO, "oracle/build_ref.sh")
+        P = C.POINTER
+        L.ref_new.restype = C.c_void_p
+        L.ref_new.argtypes = [P(cd.ModelDesc), P(cd.EvalParams), C.c_int]
+        L.ref_set_radar_law.argtypes = [C.c_void_p, P(cd.RadarLaw)]
+        L.ref_set_optical_law.argtypes = [C.c_void_p, P(cd.OpticalLaw)]
+        L.ref_add_deldop_set.argtypes = [C.c_void_p, P(cd.DeldopSet), C.c_int,
+                                         P(cd.DeldopFrame), cd.dptr, cd.dptr]
+        L.ref_add_lghtcrv_set.argtypes = [C.c_void_p, P(cd.LghtcrvSet), P(cd.LghtcrvPoint)]
+        L.ref_set_scale.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.ref_set_r.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.ref_realize.argtypes = [C.c_void_p]
+        L.ref_evaluate.restype = C.c_double
+        L.ref_evaluate.argtypes = [C.c_void_p]
+        L.ref_calc_chi2.restype = C.c_double
+        L.ref_calc_chi2.argtypes = [C.c_void_p]
+        L.ref_evaluate_mt.restype = C.c_double
+        L.ref_evaluate_mt.argtypes = [P(C.c_void_p), C.c_int]
+        L.ref_get_realized.argtypes = [C.c_void_p, cd.dptr, cd.dptr, cd.dptr, cd.dptr]
+        L.ref_get_flags.argtypes = [C.c_void_p, cd.dptr]
+        L.ref_get_seen.argtypes = [C.c_void_p, C.c_char_p]
+        L.ref_get_deldop_frame.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr, cd.dptr,
+                                           cd.dptr, cd.iptr, P(cd.DeldopResult)]
+        L.ref_get_lghtcrv.argtypes = [C.c_void_p, C.c_int, cd.dptr, cd.dptr, cd.dptr]
+        L.ref_get_lghtcrv_pos.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr, cd.dptr,
+                                          cd.dptr, cd.iptr, cd.dptr, cd.iptr, cd.iptr]
+        L.ref_free.argtypes = [C.c_void_p]
+        L.ref_mnbrak.argtypes = [cd.dptr, cd.dptr, cd.dptr, cd.dptr, cd.dptr, cd.dptr, OBJFN]
+        L.ref_brent_abs.restype = C.c_double
+        L.ref_brent_abs.argtypes = [C.c_double, C.c_double, C.c_double, OBJFN,
+                                    C.c_double, C.c_double, cd.dptr]
+
+    def session(self, model, params, deldops=(), lghtcrvs=(), radar_law=None, optical_law=None):
+        d = model.desc()
+        h = self.lib.ref_new(C.byref(d), C.byref(params), len(deldops) + len(lghtcrvs))
+        keep = [d]
+        if deldops:
+            self.lib.ref_set_radar_law(h, C.byref(radar_law or deldops[0].set.law))
+        if lghtcrvs:
+            self.lib.ref_set_optical_law(h, C.byref(optical_law or lghtcrvs[0].set.law))
+        for ds in deldops:
+            arr = ds.frame_array()
+            keep.append(arr)
+            self.lib.ref_add_deldop_set(h, C.byref(ds.set), ds.nframes, arr,
+                                        cd.as_dptr(ds.obs), cd.as_dptr(ds.oneovervar))
+        for ls in lghtcrvs:
+            arr = ls.point_array()
+            keep.append(arr)
+            self.lib.ref_add_lghtcrv_set(h, C.byref(ls.bind()), arr)
+        return RefSession(self, h, model, keep)
+
+    def mnbrak(self, fn, ax, bx):
+        cb = OBJFN(fn)
+        a, b, c = C.c_double(ax), C.c_double(bx), C.c_double(0)
+        fa, fb, fc = C.c_double(0), C.c_double(0), C.c_double(0)
+        self.lib.ref_mnbrak(C.byref(a), C.byref(b), C.byref(c), C.byref(fa), C.byref(fb),
+                            C.byref(fc), cb)
+        return a.value, b.value, c.value, fa.value, fb.value, fc.value
+
+    def brent_abs(self, fn, ax, bx, cx, tol, abstol):
+        cb = OBJFN(fn)
+        xmin = C.c_double(0)
+        fmin = self.lib.ref_brent_abs(ax, bx, cx, cb, tol, abstol, C.byref(xmin))
+        return fmin, xmin.value
+
+
+class RefSession:
+    def __init__(self, ref, h, model, keep):
+        self.ref, self.h, self.model, self.keep = ref, h, model, keep
+        self.L = ref.lib
+
+    def evaluate(self):
+        return self.L.ref_evaluate(self.h)
+
+    def realized(self):
+        m = self.model
+        x = np.zeros((m.nv, 3)); vn = np.zeros((m.nv, 3))
+        fn = np.zeros((m.nf, 3)); area = np.zeros(m.nf)
+        self.L.ref_get_realized(self.h, cd.as_dptr(x), cd.as_dptr(vn), cd.as_dptr(fn), cd.as_dptr(area))
+        return {"x": x, "vn": vn, "fn": fn, "area": area}
+
+    def flags(self):
+        out = np.zeros(4)
+        self.L.ref_get_flags(self.h, cd.as_dptr(out))
+        return {"posbnd": int(out[0]), "posbnd_logfactor": out[1],
+                "badradar": int(out[2]), "badradar_logfactor": out[3]}
+
+    def seen(self):
+        buf = C.create_string_buffer(self.model.nf)
+        self.L.ref_get_seen(self.h, buf)
+        return np.frombuffer(buf.raw, dtype=np.uint8).copy()
+
+    def deldop_frame(self, s, f, fr):
+        side = 2 * fr.pos_n + 1
+        fit = np.zeros(fr.ndel * fr.ndop)
+        z = np.zeros(side * side); cose = np.zeros(side * side)
+        fac = np.zeros(side * side, dtype=np.int32)
+        res = cd.DeldopResult()
+        self.L.ref_get_deldop_frame(self.h, s, f, cd.as_dptr(fit), cd.as_dptr(z), cd.as_dptr(cose),
+                                    cd.as_iptr(fac), C.byref(res))
+        return {"fit": fit, "z": z, "cose": cose, "f": fac, "res": cd.result_to_dict(res)}
+
+    def lghtcrv(self, s, ds):
+        y = np.zeros(ds.set.ncalc); fit = np.zeros(ds.set.n); out = np.zeros(2)
+        self.L.ref_get_lghtcrv(self.h, s, cd.as_dptr(y), cd.as_dptr(fit), cd.as_dptr(out))
+        return {"y": y, "fit": fit, "cal": out[0], "chi2": out[1]}
+
+    def lghtcrv_pos(self, s, i, pt):
+        side = 2 * pt.pos_n + 1
+        np_ = side * side
+        z, cose, cosi, zill = (np.zeros(np_) for _ in range(4))
+        fac = np.zeros(np_, dtype=np.int32); fill = np.zeros(np_, dtype=np.int32)
+        lims = np.zeros(8, dtype=np.int32)
+        self.L.ref_get_lghtcrv_pos(self.h, s, i + 1, cd.as_dptr(z), cd.as_dptr(cose), cd.as_dptr(cosi),
+                                   cd.as_iptr(fac), cd.as_dptr(zill), cd.as_iptr(fill), cd.as_iptr(lims))
+        return {"z": z, "cose": cose, "cosi": cosi, "f": fac, "zill": zill, "fill": fill,
+                "lims": lims}
+
+    def close(self):
+        if self.h:
+            self.L.ref_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

@@ -1,0 +1,486 @@
+/*
+ * Direct-call harness around the REFERENCE SHAPE CPU code (test
+ * infrastructure only; compiled by oracle/build_ref.sh into
+ * oracle/_ref/libshape_ref.so together with the reference sources, which are
+ * compiled where they lie under the reference tree).
+ *
+ * It fills the reference's own structs (struct mod_t / dat_t / par_t,
+ * src/shape/shape2.h) from the plain descriptions of include/shape_types.h
+ * and calls the reference entry points unchanged:
+ *   realize_mod (src/shape/realize_mod.c:153), calc_fits
+ *   (src/shape/calc_fits.c:340), chi2 (src/shape/chi2.c:240), and the line
+ *   searches mnbrak / brent_abs (src/nr/mnbrak.c, src/nr/brent_abs.c).
+ * POS sizes are per frame (pos_scope LOCAL with a per-frame n), as in the
+ * reference's set_up_pos (src/shape/read_dat.c:1303-1380), so frames of
+ * different sizes can share one dataset.
+ */
+#include "head.h"
+
+#include "shape_types.h"
+
+typedef struct ref_session {
+    struct par_t par;
+    struct mod_t mod;
+    struct dat_t dat;
+    int nsets_cap;
+} ref_session;
+
+static void ref_alloc_pos(struct pos_t *pos, int n, double kmpp, int bistatic)
+{
+    memset(pos, 0, sizeof *pos);
+    pos->n = n;
+    pos->km_per_pixel = kmpp;
+    pos->b = matrix(-n, n, -n, n);
+    pos->cosi = matrix(-n, n, -n, n);
+    pos->cose = matrix(-n, n, -n, n);
+    pos->z = matrix(-n, n, -n, n);
+    pos->body = imatrix(-n, n, -n, n);
+    pos->comp = imatrix(-n, n, -n, n);
+    pos->f = imatrix(-n, n, -n, n);
+    pos->cosill = matrix(-n, n, -n, n);
+    pos->zill = matrix(-n, n, -n, n);
+    pos->bodyill = imatrix(-n, n, -n, n);
+    pos->compill = imatrix(-n, n, -n, n);
+    pos->fill = imatrix(-n, n, -n, n);
+    pos->bistatic = bistatic;
+}
+
+static void ref_free_pos(struct pos_t *pos)
+{
+    int n = pos->n;
+    if (!pos->b) return;
+    free_matrix(pos->b, -n, n, -n, n); free_matrix(pos->cosi, -n, n, -n, n);
+    free_matrix(pos->cose, -n, n, -n, n); free_matrix(pos->z, -n, n, -n, n);
+    free_imatrix(pos->body, -n, n, -n, n); free_imatrix(pos->comp, -n, n, -n, n);
+    free_imatrix(pos->f, -n, n, -n, n); free_matrix(pos->cosill, -n, n, -n, n);
+    free_matrix(pos->zill, -n, n, -n, n); free_imatrix(pos->bodyill, -n, n, -n, n);
+    free_imatrix(pos->compill, -n, n, -n, n); free_imatrix(pos->fill, -n, n, -n, n);
+}
+
+void *ref_new(const shape_model_desc *m, const shape_eval_params *ep, int max_sets)
+{
+    ref_session *S = calloc(1, sizeof *S);
+    struct par_t *par = &S->par;
+    struct mod_t *mod = &S->mod;
+    par->action = FIT;
+    par->pos_smooth = (unsigned char)ep->pos_smooth;
+    par->nsinc2 = ep->nsinc2;
+    par->sinc2width = ep->sinc2width;
+    par->mask_tol = ep->mask_tol;
+    par->mincosine_seen = ep->mincosine_seen;
+    par->exclude_seen = ep->mark_seen ? -1 : -2;
+    par->dd_gamma = 1.0;
+    par->bad_objfactor = 2.0;
+    par->warn_badradar = 0;
+    par->pos_scope = LOCAL;
+
+    mod->shape.ncomp = 1;
+    mod->shape.comp = calloc(1, sizeof(struct comp_t));
+    struct comp_t *c = &mod->shape.comp[0];
+    c->type = VERTEX;
+    struct vertices_t *real = &c->real;
+    real->nv = c->desc.ver.nv = m->nv;
+    real->nf = c->desc.ver.nf = m->nf;
+    real->v = calloc((size_t)m->nv, sizeof(struct vertex_t));
+    real->f = calloc((size_t)m->nf, sizeof(struct facet_t));
+    for (int j = 0; j < 3; j++) {
+        c->desc.ver.scalefactor[j].state = 'f';
+        c->desc.ver.scalefactor[j].val = m->scale[j];
+        real->scalefactor[j] = c->desc.ver.scalefactor[j];
+        c->off[j].state = c->rot[j].state = 'c';
+        c->off[j].val = c->rot[j].val = 0.0;
+    }
+    for (int i = 0; i < m->nv; i++) {
+        struct vertex_t *v = &real->v[i];
+        for (int j = 0; j < 3; j++) { v->a[j] = m->a[3 * i + j]; v->u[j] = m->u[3 * i + j]; }
+        v->r.state = 'f';
+        v->r.val = m->r[i];
+        v->naf = m->af_ptr[i + 1] - m->af_ptr[i];
+        v->af = malloc(sizeof(int) * (size_t)(v->naf > 0 ? v->naf : 1));
+        for (int k = 0; k < v->naf; k++) v->af[k] = m->af_idx[m->af_ptr[i] + k];
+        v->act = 1;
+        v->v_mirror = i;
+    }
+    for (int f = 0; f < m->nf; f++) {
+        for (int j = 0; j < 3; j++) real->f[f].v[j] = m->fv[3 * f + j];
+        real->f[f].act = 1;
+    }
+    /* the vertex description shares the realization's arrays (VERTEX type is
+     * its own realization, src/shape/realize_mod.c:455-458) */
+    c->desc.ver.v = real->v;
+    c->desc.ver.f = real->f;
+
+    S->dat.set = calloc((size_t)max_sets, sizeof(struct set_t));
+    S->nsets_cap = max_sets;
+    return S;
+}
+
+void ref_set_radar_law(void *h, const shape_radar_law *L)
+{
+    ref_session *S = h;
+    struct photo_t *ph = &S->mod.photo;
+    ph->nradlaws = 1;
+    ph->radtype = calloc(1, 1);
+    ph->radar = calloc(1, sizeof(union radscat_t));
+    ph->radtype[0] = (unsigned char)L->type;
+    switch (L->type) {
+    case COSINELAW_DIFF:
+        ph->radar[0].RC.R.val = L->diff_R; ph->radar[0].RC.C.val = L->diff_C; break;
+    case GAUSSIANLAW: case HAGFORSLAW: case COSINELAW_QS:
+        ph->radar[0].quasispec.R.val = L->qs_R; ph->radar[0].quasispec.C.val = L->qs_C;
+        ph->radar[0].quasispec.cos_cutoff = L->qs_cos_cutoff; break;
+    default:
+        ph->radar[0].hybrid.diff.R.val = L->diff_R; ph->radar[0].hybrid.diff.C.val = L->diff_C;
+        ph->radar[0].hybrid.qs.R.val = L->qs_R; ph->radar[0].hybrid.qs.C.val = L->qs_C;
+        ph->radar[0].hybrid.qs.cos_cutoff = L->qs_cos_cutoff; break;
+    }
+}
+
+void ref_set_optical_law(void *h, const shape_optical_law *L)
+{
+    ref_session *S = h;
+    struct photo_t *ph = &S->mod.photo;
+    ph->noptlaws = 1;
+    ph->opttype = calloc(1, 1);
+    ph->optical = calloc(1, sizeof(union optscat_t));
+    ph->opttype[0] = (unsigned char)L->type;
+    if (L->type == KAASALAINEN) {
+        ph->optical[0].kaas.R.val = L->R; ph->optical[0].kaas.wt.val = L->wt;
+        ph->optical[0].kaas.A0.val = L->A0; ph->optical[0].kaas.D.val = L->D;
+        ph->optical[0].kaas.k.val = L->k;
+    } else {
+        ph->optical[0].R.R.val = L->R;
+    }
+}
+
+static void ref_copy_rm(double out[3][3], const double *in)
+{
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) out[i][j] = in[3 * i + j];
+}
+
+int ref_add_deldop_set(void *h, const shape_deldop_set *ds, int nframes,
+                       const shape_deldop_frame *frames, const double *obs_all,
+                       const double *oov_all)
+{
+    ref_session *S = h;
+    if (S->dat.nsets >= S->nsets_cap) return -1;
+    struct set_t *set = &S->dat.set[S->dat.nsets++];
+    set->type = DELAY;
+    struct deldop_t *dd = &set->desc.deldop;
+    dd->iradlaw = 0;
+    dd->del_per_pixel = ds->del_per_pixel;
+    dd->dop_per_pixel = ds->dop_per_pixel;
+    dd->Ftx = ds->Ftx;
+    dd->dopscale.val = ds->dopscale;
+    dd->codemethod = ds->codemethod;
+    dd->spb = ds->spb;
+    dd->stride = ds->stride;
+    dd->dopfftlen = ds->dopfftlen;
+    dd->nviews = 1;
+    dd->v0 = 0;
+    dd->nframes = nframes;
+    dd->frame = calloc((size_t)nframes, sizeof(struct deldopfrm_t));
+    size_t off = 0;
+    double dof = 0.0;
+    for (int f = 0; f < nframes; f++) {
+        const shape_deldop_frame *F = &frames[f];
+        struct deldopfrm_t *fr = &dd->frame[f];
+        fr->ndel = F->ndel; fr->ndop = F->ndop;
+        fr->delcom_vig = F->delcom_vig; fr->dopcom_vig = F->dopcom_vig;
+        fr->dopDC_vig = F->dopDC_vig;
+        fr->weight = F->weight; fr->dof = F->dof;
+        fr->cal.state = F->cal_floating ? 'f' : 'c';
+        fr->cal.val = F->cal;
+        fr->sdev = 1.0;
+        fr->obs = matrix(1, F->ndel, 1, F->ndop);
+        fr->fit = matrix(1, F->ndel, 1, F->ndop);
+        fr->oneovervar = matrix(1, F->ndel, 1, F->ndop);
+        for (int i = 1; i <= F->ndel; i++)
+            for (int j = 1; j <= F->ndop; j++) {
+                size_t p = off + (size_t)(i - 1) * F->ndop + (size_t)(j - 1);
+                fr->obs[i][j] = obs_all[p];
+                fr->oneovervar[i][j] = oov_all[p];
+                fr->fit[i][j] = 0.0;
+            }
+        off += (size_t)F->ndel * F->ndop;
+        fr->view = calloc(1, sizeof(struct deldopview_t));
+        ref_copy_rm(fr->view[0].ae, F->ae);
+        ref_copy_rm(fr->view[0].oe, F->oe);
+        for (int j = 0; j < 3; j++) fr->view[0].spin[j] = F->spin[j];
+        fr->view[0].deloff = F->deloff;
+        fr->view[0].dopoff = F->dopoff;
+        ref_alloc_pos(&fr->pos, F->pos_n, F->km_per_pixel, 0);
+        dof += F->dof;
+    }
+    dd->dof = dof;
+    set->dof = dof;
+    S->dat.dof_deldop += dof;
+    S->dat.dof += dof;
+    return S->dat.nsets - 1;
+}
+
+int ref_add_lghtcrv_set(void *h, const shape_lghtcrv_set *ls, const shape_lghtcrv_point *pts)
+{
+    ref_session *S = h;
+    if (S->dat.nsets >= S->nsets_cap) return -1;
+    struct set_t *set = &S->dat.set[S->dat.nsets++];
+    set->type = LGHTCRV;
+    struct lghtcrv_t *lc = &set->desc.lghtcrv;
+    int n = ls->n, ncalc = ls->ncalc;
+    lc->ioptlaw = 0;
+    lc->nviews = 1;
+    lc->v0 = 0;
+    lc->n = n;
+    lc->ncalc = ncalc;
+    lc->weight = ls->weight;
+    lc->dof = ls->dof;
+    lc->cal.state = ls->cal_floating ? 'f' : 'c';
+    lc->cal.val = ls->cal;
+    lc->t0 = vector(1, n);
+    lc->t = matrix(1, n, 0, 0);
+    lc->obs = vector(1, n);
+    lc->oneovervar = vector(1, n);
+    lc->fit = vector(1, n);
+    lc->rotphase_calc = vector(1, ncalc);
+    lc->rotphase_obs = vector(1, n);
+    lc->x0 = vector(1, ncalc);
+    lc->x = vector(1, ncalc);
+    lc->y = vector(1, ncalc);
+    lc->y2 = vector(1, ncalc);
+    lc->solar_phase = vector(1, ncalc);
+    lc->solar_azimuth = vector(1, ncalc);
+    lc->rend = calloc((size_t)ncalc + 1, sizeof(struct crvrend_t));
+    for (int i = 1; i <= n; i++) {
+        lc->t0[i] = lc->t[i][0] = ls->t[i - 1];
+        lc->obs[i] = ls->obs[i - 1];
+        lc->oneovervar[i] = ls->oneovervar[i - 1];
+        lc->fit[i] = 0.0;
+    }
+    for (int i = 1; i <= ncalc; i++) {
+        const shape_lghtcrv_point *P = &pts[i - 1];
+        lc->x0[i] = lc->x[i] = ls->x[i - 1];
+        lc->y[i] = lc->y2[i] = 0.0;
+        lc->solar_phase[i] = P->solar_phase;
+        ref_copy_rm(lc->rend[i].ae, P->ae);
+        ref_copy_rm(lc->rend[i].oe, P->oe);
+        ref_copy_rm(lc->rend[i].se, P->se);
+        ref_alloc_pos(&lc->rend[i].pos, P->pos_n, P->km_per_pixel, 1);
+    }
+    set->dof = ls->dof;
+    S->dat.dof_lghtcrv += ls->dof;
+    S->dat.dof += ls->dof;
+    return S->dat.nsets - 1;
+}
+
+/* Scale factor j of the component (a SIZEPAR free parameter, src/shape/mkparlist.c:219-226). */
+void ref_set_scale(void *h, int j, double val)
+{
+    ref_session *S = h;
+    S->mod.shape.comp[0].desc.ver.scalefactor[j].val = val;
+}
+
+/* Vertex deviation r of vertex i (a SHAPEPAR free parameter, src/shape/mkparlist.c:227-233). */
+void ref_set_r(void *h, int i, double val)
+{
+    ref_session *S = h;
+    S->mod.shape.comp[0].real.v[i].r.val = val;
+}
+
+void ref_realize(void *h)
+{
+    ref_session *S = h;
+    realize_mod(&S->par, &S->mod);
+}
+
+/* realize_mod + calc_fits + chi2(par, dat, 0): the evaluation inside
+ * objective() (src/shape/bestfit.c:748-790) without penalties. Returns
+ * dat->chi2. stdout carries chi2_lghtcrv's per-point prints (chi2.c:1147). */
+double ref_evaluate(void *h)
+{
+    ref_session *S = h;
+    realize_mod(&S->par, &S->mod);
+    calc_fits(&S->par, &S->mod, &S->dat);
+    return chi2(&S->par, &S->dat, 0);
+}
+
+/* calc_fits + chi2 without re-realizing (model already realized). */
+double ref_calc_chi2(void *h)
+{
+    ref_session *S = h;
+    calc_fits(&S->par, &S->mod, &S->dat);
+    return chi2(&S->par, &S->dat, 0);
+}
+
+void ref_get_realized(void *h, double *x, double *vn, double *fn, double *area)
+{
+    ref_session *S = h;
+    struct vertices_t *real = &S->mod.shape.comp[0].real;
+    for (int i = 0; i < real->nv; i++)
+        for (int j = 0; j < 3; j++) { x[3 * i + j] = real->v[i].x[j]; vn[3 * i + j] = real->v[i].n[j]; }
+    for (int f = 0; f < real->nf; f++) {
+        for (int j = 0; j < 3; j++) fn[3 * f + j] = real->f[f].n[j];
+        area[f] = real->f[f].area;
+    }
+}
+
+/* Flags of par after calc_fits: [posbnd, posbnd_logfactor, badradar, badradar_logfactor]. */
+void ref_get_flags(void *h, double out[4])
+{
+    ref_session *S = h;
+    out[0] = S->par.posbnd; out[1] = S->par.posbnd_logfactor;
+    out[2] = S->par.badradar; out[3] = S->par.badradar_logfactor;
+}
+
+void ref_get_seen(void *h, unsigned char *seen)
+{
+    ref_session *S = h;
+    struct vertices_t *real = &S->mod.shape.comp[0].real;
+    for (int f = 0; f < real->nf; f++) seen[f] = real->f[f].seen;
+}
+
+static void ref_copy_pos_out(const struct pos_t *pos, double *z, double *cose, double *cosi,
+                             int *f, double *zill, int *fill, int lims[8])
+{
+    int n = pos->n, side = 2 * n + 1;
+    for (int i = -n; i <= n; i++)
+        for (int j = -n; j <= n; j++) {
+            size_t p = (size_t)(i + n) * side + (size_t)(j + n);
+            if (z) z[p] = pos->z[i][j];
+            if (cose) cose[p] = pos->cose[i][j];
+            if (cosi) cosi[p] = pos->cosi[i][j];
+            if (f) f[p] = pos->f[i][j];
+            if (zill) zill[p] = pos->zill[i][j];
+            if (fill) fill[p] = pos->fill[i][j];
+        }
+    if (lims) {
+        lims[0] = pos->xlim[0]; lims[1] = pos->xlim[1];
+        lims[2] = pos->ylim[0]; lims[3] = pos->ylim[1];
+        lims[4] = pos->xlim2[0]; lims[5] = pos->xlim2[1];
+        lims[6] = pos->ylim2[0]; lims[7] = pos->ylim2[1];
+    }
+}
+
+/* Outputs of one delay-Doppler frame after ref_evaluate. Any pointer may be NULL.
+ * res receives xlim/ylim, idellim/idoplim, dellim/doplim, badradar_logfactor,
+ * posbnd_logfactor (of the pos), cal and chi2. */
+void ref_get_deldop_frame(void *h, int s, int f, double *fit, double *z, double *cose,
+                          int *fac, shape_deldop_result *res)
+{
+    ref_session *S = h;
+    struct deldopfrm_t *fr = &S->dat.set[s].desc.deldop.frame[f];
+    if (fit)
+        for (int i = 1; i <= fr->ndel; i++)
+            for (int j = 1; j <= fr->ndop; j++)
+                fit[(size_t)(i - 1) * fr->ndop + (size_t)(j - 1)] = fr->fit[i][j];
+    int lims[8];
+    ref_copy_pos_out(&fr->pos, z, cose, NULL, fac, NULL, NULL, lims);
+    if (res) {
+        memset(res, 0, sizeof *res);
+        res->xlim[0] = lims[0]; res->xlim[1] = lims[1];
+        res->ylim[0] = lims[2]; res->ylim[1] = lims[3];
+        res->idellim[0] = fr->idellim[0]; res->idellim[1] = fr->idellim[1];
+        res->idoplim[0] = fr->idoplim[0]; res->idoplim[1] = fr->idoplim[1];
+        res->dellim[0] = fr->dellim[0]; res->dellim[1] = fr->dellim[1];
+        res->doplim[0] = fr->doplim[0]; res->doplim[1] = fr->doplim[1];
+        res->badradar_logfactor = fr->badradar_logfactor;
+        res->posbnd_logfactor = fr->pos.posbnd_logfactor;
+        res->cal = fr->cal.val;
+        res->chi2 = fr->chi2;
+    }
+}
+
+/* Outputs of a lightcurve set after ref_evaluate: y[ncalc], fit[n], [cal, chi2]. */
+void ref_get_lghtcrv(void *h, int s, double *y, double *fit, double out[2])
+{
+    ref_session *S = h;
+    struct lghtcrv_t *lc = &S->dat.set[s].desc.lghtcrv;
+    for (int i = 1; i <= lc->ncalc; i++) y[i - 1] = lc->y[i];
+    for (int i = 1; i <= lc->n; i++) fit[i - 1] = lc->fit[i];
+    out[0] = lc->cal.val;
+    out[1] = S->dat.set[s].chi2;
+}
+
+/* POS maps of one calculated lightcurve point (1-based i as in the reference). */
+void ref_get_lghtcrv_pos(void *h, int s, int i, double *z, double *cose, double *cosi,
+                         int *fac, double *zill, int *fill, int lims[8])
+{
+    ref_session *S = h;
+    ref_copy_pos_out(&S->dat.set[s].desc.lghtcrv.rend[i].pos, z, cose, cosi, fac, zill, fill, lims);
+}
+
+double ref_set_chi2(void *h, int s)
+{
+    ref_session *S = h;
+    return S->dat.set[s].chi2;
+}
+
+void ref_free(void *h)
+{
+    ref_session *S = h;
+    if (!S) return;
+    for (int s = 0; s < S->dat.nsets; s++) {
+        struct set_t *set = &S->dat.set[s];
+        if (set->type == DELAY) {
+            struct deldop_t *dd = &set->desc.deldop;
+            for (int f = 0; f < dd->nframes; f++) {
+                struct deldopfrm_t *fr = &dd->frame[f];
+                free_matrix(fr->obs, 1, fr->ndel, 1, fr->ndop);
+                free_matrix(fr->fit, 1, fr->ndel, 1, fr->ndop);
+                free_matrix(fr->oneovervar, 1, fr->ndel, 1, fr->ndop);
+                ref_free_pos(&fr->pos);
+                free(fr->view);
+            }
+            free(dd->frame);
+        } else if (set->type == LGHTCRV) {
+            struct lghtcrv_t *lc = &set->desc.lghtcrv;
+            for (int i = 1; i <= lc->ncalc; i++) ref_free_pos(&lc->rend[i].pos);
+            free(lc->rend);
+        }
+    }
+    free(S->dat.set);
+    struct vertices_t *real = &S->mod.shape.comp[0].real;
+    for (int i = 0; i < real->nv; i++) free(real->v[i].af);
+    free(real->v); free(real->f);
+    free(S->mod.shape.comp);
+    free(S);
+}
+
+/* Multi-core evaluation in the reference's host-multithreading scheme: one
+ * dataset (here: one session) per thread, as calc_fits_hmt assigns datasets
+ * to threads (src/HostMultiThreading/calc_fits_hmt.c:134-160). */
+typedef struct { void *h; double chi2; } ref_mt_job;
+static void *ref_mt_worker(void *arg)
+{
+    ref_mt_job *j = arg;
+    j->chi2 = ref_evaluate(j->h);
+    return NULL;
+}
+
+double ref_evaluate_mt(void **sessions, int nsessions)
+{
+    pthread_t *th = calloc((size_t)nsessions, sizeof(pthread_t));
+    ref_mt_job *jobs = calloc((size_t)nsessions, sizeof(ref_mt_job));
+    for (int i = 0; i < nsessions; i++) {
+        jobs[i].h = sessions[i];
+        pthread_create(&th[i], NULL, ref_mt_worker, &jobs[i]);
+    }
+    double tot = 0.0;
+    for (int i = 0; i < nsessions; i++) {
+        pthread_join(th[i], NULL);
+        tot += jobs[i].chi2;
+    }
+    free(th); free(jobs);
+    return tot;
+}
+
+/* Line searches of the reference, for pinning the engine's own bracketing
+ * and Brent minimiser: the objective is a plain C callback. */
+typedef double (*ref_objfn)(double);
+void ref_mnbrak(double *ax, double *bx, double *cx, double *fa, double *fb, double *fc, ref_objfn fn)
+{
+    mnbrak(ax, bx, cx, fa, fb, fc, fn);
+}
+double ref_brent_abs(double ax, double bx, double cx, ref_objfn fn, double tol, double abstol, double *xmin)
+{
+    return brent_abs(ax, bx, cx, fn, tol, abstol, xmin);
+}

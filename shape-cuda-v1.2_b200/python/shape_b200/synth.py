@@ -1,0 +1,465 @@
+"""Seeded synthetic SHAPE inputs with the shapes and sizes of the benchmark
+configurations (the reference ships no example .mod/.obs files).
+
+Models are single-component VERTEX models (x = scale*(u*r + a)); datasets are
+delay-Doppler frames (one view each) and lightcurves, described with the plain
+structs of include/shape_types.h. Observed images are produced by a caller-
+supplied ``synthesize`` callable that evaluates the TRUE model (the engine's
+FP64 path on a GPU, or the CPU oracle in tests), then noise is added.
+
+Seeds: 42 for shape deviations, 7 for phases and sizes, 1234 for noise.
+"""
+from dataclasses import dataclass, field
+import math
+
+import numpy as np
+
+from . import ctypes_defs as cd
+
+KM2US = 6.67128190396304
+KM2HZFACT = 7.72139109254982e-5
+DEG = math.pi / 180.0
+
+
+# --------------------------------------------------------------------- models
+
+@dataclass
+class Model:
+    a: np.ndarray          # [nv,3]
+    u: np.ndarray          # [nv,3]
+    r: np.ndarray          # [nv]
+    fv: np.ndarray         # [nf,3] int32
+    af_ptr: np.ndarray     # [nv+1] int32
+    af_idx: np.ndarray     # int32
+    scale: np.ndarray = field(default_factory=lambda: np.ones(3))
+    name: str = ""
+
+    @property
+    def nv(self):
+        return self.a.shape[0]
+
+    @property
+    def nf(self):
+        return self.fv.shape[0]
+
+    def copy(self):
+        return Model(self.a.copy(), self.u.copy(), self.r.copy(), self.fv.copy(),
+                     self.af_ptr.copy(), self.af_idx.copy(), self.scale.copy(), self.name)
+
+    def desc(self):
+        """ctypes shape_model_desc pointing into this model's arrays."""
+        for k in ("a", "u", "r"):
+            setattr(self, k, np.ascontiguousarray(getattr(self, k), dtype=np.float64))
+        for k in ("fv", "af_ptr", "af_idx"):
+            setattr(self, k, np.ascontiguousarray(getattr(self, k), dtype=np.int32))
+        d = cd.ModelDesc()
+        d.nv, d.nf = self.nv, self.nf
+        d.a, d.u, d.r = cd.as_dptr(self.a), cd.as_dptr(self.u), cd.as_dptr(self.r)
+        for j in range(3):
+            d.scale[j] = float(self.scale[j])
+        d.fv, d.af_ptr, d.af_idx = cd.as_iptr(self.fv), cd.as_iptr(self.af_ptr), cd.as_iptr(self.af_idx)
+        return d
+
+
+def _orient_outward(x, fv):
+    """Make every facet right-handed with its normal pointing away from the origin."""
+    p0, p1, p2 = x[fv[:, 0]], x[fv[:, 1]], x[fv[:, 2]]
+    nrm = np.cross(p1 - p0, p2 - p1)
+    cen = (p0 + p1 + p2) / 3.0
+    flip = np.einsum("ij,ij->i", nrm, cen) < 0
+    fv = fv.copy()
+    fv[flip, 1], fv[flip, 2] = fv[flip, 2].copy(), fv[flip, 1].copy()
+    return fv
+
+
+def _attached(nv, fv):
+    """CSR lists of the facets attached to each vertex, in increasing facet order."""
+    counts = np.zeros(nv, dtype=np.int64)
+    for k in range(3):
+        np.add.at(counts, fv[:, k], 1)
+    ptr = np.zeros(nv + 1, dtype=np.int64)
+    np.cumsum(counts, out=ptr[1:])
+    pairs = np.stack([fv.reshape(-1), np.repeat(np.arange(fv.shape[0]), 3)], axis=1)
+    order = np.lexsort((pairs[:, 1], pairs[:, 0]))
+    idx = pairs[order, 1]
+    return ptr.astype(np.int32), idx.astype(np.int32)
+
+
+def ring_sphere(nrings, nper):
+    """Unit directions and facets of a latitude-ring tessellation:
+    nrings rings of nper vertices plus 2 poles, 2*nper*nrings facets."""
+    dirs = [np.array([0.0, 0.0, 1.0])]
+    for k in range(nrings):
+        th = math.pi * (k + 1) / (nrings + 1)
+        off = 0.5 * (k % 2)
+        for m in range(nper):
+            ph = 2 * math.pi * (m + off) / nper
+            dirs.append(np.array([math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)]))
+    dirs.append(np.array([0.0, 0.0, -1.0]))
+    dirs = np.array(dirs)
+    nv = dirs.shape[0]
+    ring = lambda k, m: 1 + k * nper + (m % nper)
+    faces = []
+    for m in range(nper):
+        faces.append((0, ring(0, m), ring(0, m + 1)))
+    for k in range(nrings - 1):
+        for m in range(nper):
+            if k % 2 == 0:
+                faces.append((ring(k, m), ring(k + 1, m), ring(k, m + 1)))
+                faces.append((ring(k, m + 1), ring(k + 1, m), ring(k + 1, m + 1)))
+            else:
+                faces.append((ring(k, m), ring(k + 1, m), ring(k + 1, m + 1)))
+                faces.append((ring(k, m), ring(k + 1, m + 1), ring(k, m + 1)))
+    last = nv - 1
+    for m in range(nper):
+        faces.append((last, ring(nrings - 1, m + 1), ring(nrings - 1, m)))
+    return dirs, np.array(faces, dtype=np.int32)
+
+
+def octa_sphere(levels):
+    """Unit directions and facets of an octahedron subdivided `levels` times
+    (V = 4**levels * 4 + 2, F = 8 * 4**levels)."""
+    verts = [np.array(v, dtype=np.float64) for v in
+             [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]]
+    faces = [(4, 0, 2), (4, 2, 1), (4, 1, 3), (4, 3, 0), (5, 2, 0), (5, 1, 2), (5, 3, 1), (5, 0, 3)]
+    for _ in range(levels):
+        cache = {}
+
+        def mid(i, j):
+            key = (min(i, j), max(i, j))
+            if key not in cache:
+                p = verts[i] + verts[j]
+                verts.append(p / np.linalg.norm(p))
+                cache[key] = len(verts) - 1
+            return cache[key]
+        nf = []
+        for (a, b, c) in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.array(verts), np.array(faces, dtype=np.int32)
+
+
+def _real_sph_harm_basis(dirs, lmax):
+    """Real spherical-harmonic-like basis (unnormalised Legendre x cos/sin)."""
+    ct = dirs[:, 2]
+    ph = np.arctan2(dirs[:, 1], dirs[:, 0])
+    st = np.sqrt(np.maximum(0.0, 1 - ct * ct))
+    cols = []
+    for l in range(1, lmax + 1):
+        for m in range(0, l + 1):
+            # associated Legendre P_l^m by recurrence
+            pmm = np.ones_like(ct)
+            for k in range(1, m + 1):
+                pmm = pmm * (-(2 * k - 1)) * st
+            if l == m:
+                plm = pmm
+            else:
+                pm1 = ct * (2 * m + 1) * pmm
+                if l == m + 1:
+                    plm = pm1
+                else:
+                    pa, pb = pmm, pm1
+                    for ll in range(m + 2, l + 1):
+                        pc = (ct * (2 * ll - 1) * pb - (ll + m - 1) * pa) / (ll - m)
+                        pa, pb = pb, pc
+                    plm = pb
+            cols.append(plm * np.cos(m * ph))
+            if m > 0:
+                cols.append(plm * np.sin(m * ph))
+    B = np.stack(cols, axis=1)
+    return B / np.maximum(np.sqrt((B * B).mean(axis=0)), 1e-300)
+
+
+def make_model(dirs, fv, radius, base=None, name=""):
+    nv = dirs.shape[0]
+    if base is None:
+        a = np.zeros((nv, 3))
+        u = dirs.copy()
+        r = np.asarray(radius, dtype=np.float64).copy()
+    else:
+        a = base.copy()
+        u = dirs.copy()
+        r = np.zeros(nv)
+    xr = a + u * r[:, None]
+    fv = _orient_outward(xr, fv)
+    ptr, idx = _attached(nv, fv)
+    return Model(a, u, r, fv, ptr, idx, np.ones(3), name)
+
+
+def ellipsoid_model(semi=(1.0, 0.8, 0.6), nrings=23, nper=50):
+    """Config-1 model: triaxial ellipsoid, 23 rings x 50 + 2 poles =
+    1152 vertices / 2300 facets, as a VERTEX model with a on the surface,
+    u radial and r = 0."""
+    dirs, fv = ring_sphere(nrings, nper)
+    base = dirs * np.asarray(semi)[None, :]
+    u = base / np.linalg.norm(base, axis=1)[:, None]
+    return make_model(u, fv, None, base=base, name="ellipsoid-%d" % fv.shape[0])
+
+
+def harmonic_model(nrings=40, nper=100, lmax=8, amp=0.05, seed=42):
+    """Config-2/3 model: 4002 vertices / 8000 facets, unit sphere perturbed by
+    random real spherical harmonics up to degree 8 with 5% RMS amplitude."""
+    dirs, fv = ring_sphere(nrings, nper)
+    rng = np.random.default_rng(seed)
+    B = _real_sph_harm_basis(dirs, lmax)
+    dev = B @ rng.standard_normal(B.shape[1])
+    dev *= amp / np.sqrt((dev * dev).mean())
+    return make_model(dirs, fv, 1.0 + dev, name="harmonic-%d" % fv.shape[0])
+
+
+def noisy_octa_model(levels=6, sigma=0.03, seed=42):
+    """Config-4 model: 16386 vertices / 32768 facets, unit radii with 3%
+    Gaussian noise."""
+    dirs, fv = octa_sphere(levels)
+    rng = np.random.default_rng(seed)
+    return make_model(dirs, fv, 1.0 + sigma * rng.standard_normal(dirs.shape[0]),
+                      name="octa-%d" % fv.shape[0])
+
+
+# ------------------------------------------------------------------- geometry
+
+def unit(v):
+    v = np.asarray(v, dtype=np.float64)
+    return v / np.linalg.norm(v)
+
+
+def ecl_dir(lon_deg, lat_deg):
+    lo, la = lon_deg * DEG, lat_deg * DEG
+    return np.array([math.cos(la) * math.cos(lo), math.cos(la) * math.sin(lo), math.sin(la)])
+
+
+def body_matrix(pole, phase):
+    """ecliptic -> body rotation (rows = body axes in ecliptic coords) for a
+    principal-axis rotator with spin axis `pole` at rotation phase `phase`."""
+    zb = unit(pole)
+    x0 = np.cross([0.0, 0.0, 1.0], zb)
+    if np.linalg.norm(x0) < 1e-12:
+        x0 = np.array([1.0, 0.0, 0.0])
+    x0 = unit(x0)
+    y0 = np.cross(zb, x0)
+    xb = math.cos(phase) * x0 + math.sin(phase) * y0
+    yb = -math.sin(phase) * x0 + math.cos(phase) * y0
+    return np.stack([xb, yb, zb])
+
+
+def observer_matrix(to_obs):
+    """ecliptic -> observer rotation whose z axis points to the observer."""
+    zo = unit(to_obs)
+    north = np.array([0.0, 0.0, 1.0]) - zo[2] * zo
+    if np.linalg.norm(north) < 1e-12:
+        north = np.array([0.0, 1.0, 0.0])
+    yo = unit(north)
+    xo = np.cross(yo, zo)
+    return np.stack([xo, yo, zo])
+
+
+def rotate_about(v, axis, ang):
+    k = unit(axis)
+    v = np.asarray(v, dtype=np.float64)
+    return v * math.cos(ang) + np.cross(k, v) * math.sin(ang) + k * np.dot(k, v) * (1 - math.cos(ang))
+
+
+# ------------------------------------------------------------------- datasets
+
+@dataclass
+class DeldopDataset:
+    set: "cd.DeldopSet"
+    frames: list             # list of cd.DeldopFrame
+    obs: np.ndarray          # concatenated [sum ndel*ndop]
+    oneovervar: np.ndarray
+    offsets: np.ndarray      # [nframes+1] element offsets into obs
+
+    @property
+    def nframes(self):
+        return len(self.frames)
+
+    def frame_array(self):
+        arr = (cd.DeldopFrame * len(self.frames))(*self.frames)
+        return arr
+
+    def frame_obs(self, f):
+        return self.obs[self.offsets[f]:self.offsets[f + 1]]
+
+
+@dataclass
+class LightcurveDataset:
+    set: "cd.LghtcrvSet"
+    points: list             # list of cd.LghtcrvPoint
+    x: np.ndarray
+    t: np.ndarray
+    obs: np.ndarray
+    oneovervar: np.ndarray
+
+    def bind(self):
+        self.set.x, self.set.t = cd.as_dptr(self.x), cd.as_dptr(self.t)
+        self.set.obs, self.set.oneovervar = cd.as_dptr(self.obs), cd.as_dptr(self.oneovervar)
+        return self.set
+
+    def point_array(self):
+        return (cd.LghtcrvPoint * len(self.points))(*self.points)
+
+
+def eval_params(pos_smooth=1, nsinc2=1, sinc2width=7, mask_tol=0.0, mincosine_seen=0.0, mark_seen=1):
+    p = cd.EvalParams()
+    p.pos_smooth, p.nsinc2, p.sinc2width = pos_smooth, nsinc2, sinc2width
+    p.mask_tol, p.mincosine_seen, p.mark_seen = mask_tol, mincosine_seen, mark_seen
+    return p
+
+
+def radar_cosine(R=0.1, C=1.0):
+    law = cd.RadarLaw()
+    law.type, law.diff_R, law.diff_C = 1, R, C
+    law.qs_R, law.qs_C, law.qs_cos_cutoff = 0.0, 0.0, 0.0
+    return law
+
+
+def _frame(pos_n, kmpp, ae, oe, spin, ndel, ndop, delcom, dopcom):
+    fr = cd.DeldopFrame()
+    fr.pos_n, fr.km_per_pixel = pos_n, kmpp
+    cd.fill9(fr.ae, ae)
+    cd.fill9(fr.oe, oe)
+    for j in range(3):
+        fr.spin[j] = float(spin[j])
+    fr.deloff = fr.dopoff = 0.0
+    fr.ndel, fr.ndop = ndel, ndop
+    fr.delcom_vig, fr.dopcom_vig, fr.dopDC_vig = delcom, dopcom, dopcom
+    fr.weight = 1.0
+    fr.dof = float(ndel * ndop)
+    fr.cal_floating, fr.cal = 1, 1.0
+    return fr
+
+
+def _finish_deldop(dset, frames, synthesize, amp, sdev, seed, params):
+    sizes = [f.ndel * f.ndop for f in frames]
+    offsets = np.zeros(len(frames) + 1, dtype=np.int64)
+    np.cumsum(sizes, out=offsets[1:])
+    obs = np.zeros(int(offsets[-1]))
+    oov = np.full(int(offsets[-1]), 1.0 / (sdev * sdev))
+    ds = DeldopDataset(dset, frames, obs, oov, offsets)
+    if synthesize is not None:
+        fits = synthesize(ds, params)
+        rng = np.random.default_rng(seed)
+        for f in range(len(frames)):
+            ft = np.asarray(fits[f], dtype=np.float64)
+            peak = ft.max() if ft.size and ft.max() > 0 else 1.0
+            ds.obs[offsets[f]:offsets[f + 1]] = amp * ft / peak + sdev * rng.standard_normal(ft.size)
+    return ds
+
+
+def config1_dataset(synthesize=None, params=None):
+    """Config 1: one 100x100 delay-Doppler frame, POS 151x151 at 15 m/px,
+    period 6 h, pole (30, 60) deg, cos^2 law (COSINELAW_DIFF, C=1, R=0.1),
+    LONG_ORIG spb=1 stride=1, Ftx 2380 MHz, 0.1 usec x 0.1 Hz pixels."""
+    params = params or eval_params()
+    pole = ecl_dir(30.0, 60.0)
+    omega = 2 * math.pi / 0.25
+    to_earth = ecl_dir(0.0, 10.0)
+    ae = body_matrix(pole, 0.7)
+    oe = observer_matrix(to_earth)
+    dset = cd.DeldopSet()
+    dset.del_per_pixel, dset.dop_per_pixel = 0.1, 0.1
+    dset.Ftx, dset.dopscale = 2380.0, 1.0
+    dset.codemethod, dset.spb, dset.stride, dset.dopfftlen = 1, 1, 1, 64
+    dset.law = radar_cosine()
+    fr = _frame(75, 2.25 / 150.0, ae, oe, omega * pole, 100, 100, 70.0, 50.5)
+    return _finish_deldop(dset, [fr], synthesize, 20.0, 1.0, 1234, params)
+
+
+def batched_dataset(nframes=64, pos_range=(101, 301), ndel_range=(64, 256),
+                    ndop_range=(64, 512), synthesize=None, params=None, seed=7,
+                    radius=1.05, codemethod=1, spb=1, stride=1):
+    """Config 2 (and, with other sizes, config 4): frames at rotation phases
+    uniform in [0, 2pi), odd POS sides, delay/Doppler sizes uniform in the
+    given ranges, resolutions scaled so the target spans ~80% of each frame."""
+    params = params or eval_params()
+    rng = np.random.default_rng(seed)
+    pole = ecl_dir(30.0, 60.0)
+    omega = 2 * math.pi / 0.25
+    to_earth = ecl_dir(0.0, 10.0)
+    oe = observer_matrix(to_earth)
+    w_obs = oe @ (omega * pole)
+    w_proj = math.hypot(w_obs[0], w_obs[1])
+    Ftx = 2380.0
+    dset = cd.DeldopSet()
+    dset.Ftx, dset.dopscale = Ftx, 1.0
+    dset.codemethod, dset.spb, dset.stride, dset.dopfftlen = codemethod, spb, stride, 64
+    dset.law = radar_cosine()
+    frames = []
+    # one set-level resolution: taken from the median frame size, then each
+    # frame's POS scale adapts to its own pixel count
+    ndels = rng.integers(ndel_range[0], ndel_range[1] + 1, nframes)
+    ndops = rng.integers(ndop_range[0], ndop_range[1] + 1, nframes)
+    sides = rng.integers(pos_range[0], pos_range[1] + 1, nframes) | 1
+    phases = rng.uniform(0.0, 2 * math.pi, nframes)
+    dset.del_per_pixel = KM2US * radius / (0.75 * float(ndel_range[0]))
+    dset.dop_per_pixel = 2 * KM2HZFACT * Ftx * w_proj * radius / (0.7 * float(ndop_range[0]))
+    for f in range(nframes):
+        n = int(sides[f]) // 2
+        kmpp = 2 * radius / (0.8 * sides[f])
+        ae = body_matrix(pole, float(phases[f]))
+        ndel, ndop = int(ndels[f]), int(ndops[f])
+        delcom = 0.5 * ndel + 0.5 * (KM2US * radius / dset.del_per_pixel)
+        frames.append(_frame(n, kmpp, ae, oe, omega * pole, ndel, ndop, delcom, 0.5 * ndop + 0.5))
+    return _finish_deldop(dset, frames, synthesize, 20.0, 1.0, 1234, params)
+
+
+def config2_dataset(synthesize=None, params=None):
+    return batched_dataset(64, (101, 301), (64, 256), (64, 512), synthesize, params, seed=7)
+
+
+def config4_dataset(synthesize=None, params=None):
+    """Config 4: 16 frames, POS pos_pixels=512 (effective 511x511, n=255),
+    256x256 delay-Doppler."""
+    return batched_dataset(16, (511, 511), (256, 256), (256, 256), synthesize, params, seed=7)
+
+
+def lightcurve_dataset(npoints=200, pos_range=(129, 257), synthesize=None, params=None,
+                       seed=7, set_index=0, radius=1.05):
+    """Config 3: one lightcurve of `npoints` points, solar phase uniform in
+    5-60 deg, odd POS sides uniform in pos_range, Kaasalainen law with
+    wt=0.3 (Lommel-Seeliger 0.7 + Lambert 0.3), A0=0, k=0; calc epochs equal
+    observation epochs; 1% Gaussian noise."""
+    params = params or eval_params()
+    rng = np.random.default_rng(seed + 101 * set_index)
+    pole = ecl_dir(30.0, 60.0)
+    to_earth = ecl_dir(20.0 * set_index, 5.0 + 3.0 * set_index)
+    oe = observer_matrix(to_earth)
+    alpha = float(rng.uniform(5.0, 60.0)) * DEG
+    axis = np.cross(to_earth, [0.0, 0.0, 1.0])
+    to_sun = rotate_about(to_earth, axis, alpha)
+    se = observer_matrix(to_sun)
+    t = np.sort(rng.uniform(0.0, 0.5, npoints)) + 2458000.0 + 10.0 * set_index
+    sides = rng.integers(pos_range[0], pos_range[1] + 1, npoints) | 1
+    pts = []
+    for i in range(npoints):
+        p = cd.LghtcrvPoint()
+        p.pos_n = int(sides[i]) // 2
+        p.km_per_pixel = 2 * radius / (0.8 * sides[i])
+        phase = 2 * math.pi * (t[i] - t[0]) / 0.25
+        cd.fill9(p.ae, body_matrix(pole, phase))
+        cd.fill9(p.oe, oe)
+        cd.fill9(p.se, se)
+        p.solar_phase = alpha
+        pts.append(p)
+    ls = cd.LghtcrvSet()
+    ls.ncalc = ls.n = npoints
+    ls.weight, ls.dof = 1.0, float(npoints)
+    ls.cal_floating, ls.cal = 1, 1.0
+    law = cd.OpticalLaw()
+    law.type, law.R, law.wt, law.A0, law.D, law.k = 11, 1.0, 0.3, 0.0, 0.1, 0.0
+    ls.law = law
+    x = t.copy()
+    obs = np.ones(npoints)
+    ds = LightcurveDataset(ls, pts, x, t.copy(), obs, np.ones(npoints))
+    if synthesize is not None:
+        y = np.asarray(synthesize(ds, params), dtype=np.float64)
+        nrng = np.random.default_rng(1234 + set_index)
+        ds.obs = y * (1.0 + 0.01 * nrng.standard_normal(npoints))
+        ds.oneovervar = 1.0 / (0.01 * ds.obs) ** 2
+    ds.bind()
+    return ds
+
+
+def config3_datasets(synthesize=None, params=None, npoints=200):
+    return [lightcurve_dataset(npoints, (129, 257), synthesize, params, set_index=k) for k in range(4)]
