@@ -1,0 +1,126 @@
+/*
+ * SHAPE model-evaluation engine for NVIDIA B200 (sm_100a): C ABI.
+ *
+ * The engine replaces the reference's CPU hot path
+ *   realize_mod -> posclr/posvis -> pos2deldop / posmask+apply_photo
+ *   -> calc_fits -> chi2
+ * (h6294443/shape-cuda-v1.2: src/shape/realize_mod.c:153,
+ * src/shape/posvis.c:84, src/shape/pos2deldop.c:176,
+ * src/shape/posmask.c:58, src/shape/apply_photo.c:78,
+ * src/shape/calc_fits.c:340, src/shape/chi2.c:240) with device-resident
+ * model and frame state. A shim in the reference converts
+ * struct mod_t / dat_t / par_t into the plain descriptions of shape_types.h
+ * once, then calls shape_engine_evaluate where objective() called
+ * calc_fits + chi2 (src/shape/bestfit.c:789-790).
+ *
+ * Conventions: every function returns SHAPE_OK (0) or a negative
+ * SHAPE_E_* status; shape_last_error() gives a message for the calling
+ * thread. Host pointers are plain host memory (pinned or not); nothing in
+ * the ABI exposes device pointers. An engine handle is bound to one CUDA
+ * device and one stream; it is not thread-safe (use one handle per thread),
+ * which matches the reference's single-threaded calc_fits.
+ */
+#ifndef SHAPE_B200_H
+#define SHAPE_B200_H
+
+#include <stddef.h>
+#include "shape_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHAPE_OK 0
+#define SHAPE_E_ARG -1        /* invalid argument */
+#define SHAPE_E_CUDA -2       /* CUDA runtime error (message in shape_last_error) */
+#define SHAPE_E_STATE -3      /* call out of order (e.g. evaluate before finalize) */
+#define SHAPE_E_UNSUPPORTED -4/* law / mode not supported by the device path */
+#define SHAPE_E_NOMEM -5      /* device memory exhausted */
+#define SHAPE_E_TIMEOUT -6    /* bounded wait expired */
+
+/* Evaluation forms. */
+#define SHAPE_FORM_PLAIN_FP64 0   /* per-frame launch sequence, FP64 end to end:
+                                     facet maps bit-exact with the reference */
+#define SHAPE_FORM_BATCHED_FP64 1 /* all frames per launch, CUDA graph, FP64 */
+#define SHAPE_FORM_BATCHED_FP32 2 /* all frames per launch, CUDA graph, FP32
+                                     raster/synthesis, FP64 rotations and
+                                     compensated FP64 chi-square */
+
+typedef struct shape_engine shape_engine;
+
+/* Totals of one evaluation: what calc_fits leaves in par and chi2 returns. */
+typedef struct shape_eval_summary {
+    double chi2;               /* dat->chi2 (src/shape/chi2.c:392) */
+    double dof;                /* dat->dof */
+    double chi2_deldop, chi2_lghtcrv;
+    int posbnd;                /* par->posbnd */
+    double posbnd_logfactor;   /* par->posbnd_logfactor after /= dat->dof */
+    int badradar;              /* par->badradar */
+    double badradar_logfactor; /* after /= (dof_deldop + dof_doppler) */
+    double objective;          /* chi2/dof times bad-model factors, as in
+                                  objective() (src/shape/bestfit.c:789-866)
+                                  with no penalties */
+} shape_eval_summary;
+
+const char *shape_last_error(void);
+const char *shape_version(void);
+/* sizeof() of every struct in shape_types.h, in the order
+ * model_desc, radar_law, optical_law, eval_params, deldop_frame,
+ * deldop_set, lghtcrv_point, lghtcrv_set, deldop_result, eval_summary;
+ * lets bindings verify their layouts. Returns the number written. */
+int shape_abi_sizes(size_t *out, int max);
+
+/* Create an engine on CUDA device `device`. */
+int shape_engine_create(int device, shape_engine **out);
+void shape_engine_destroy(shape_engine *e);
+
+/* Model and datasets; replaces read_mod/read_dat's in-memory result. */
+int shape_engine_set_model(shape_engine *e, const shape_model_desc *m);
+int shape_engine_set_params(shape_engine *e, const shape_eval_params *p);
+/* Appends a delay-Doppler set; obs and oneovervar hold every frame's
+ * ndel*ndop image back to back. Returns the set index (>= 0) or a status. */
+int shape_engine_add_deldop_set(shape_engine *e, const shape_deldop_set *set,
+                                int nframes, const shape_deldop_frame *frames,
+                                const double *obs, const double *oneovervar);
+int shape_engine_add_lghtcrv_set(shape_engine *e, const shape_lghtcrv_set *set,
+                                 const shape_lghtcrv_point *points);
+/* Allocates device state for everything added so far. */
+int shape_engine_finalize(shape_engine *e);
+
+/* Free parameters (src/shape/mkparlist.c:218-235): component scale factor j
+ * (SIZEPAR) and vertex deviation r of vertex i (SHAPEPAR). */
+int shape_engine_set_scale(shape_engine *e, int j, double value);
+int shape_engine_set_vertex_r(shape_engine *e, int i, double value);
+int shape_engine_get_vertex_r(shape_engine *e, int i, double *value);
+
+/* One objective evaluation: realize_mod + calc_fits + chi2 on the device.
+ * The model state set above goes host->device inside the call; the summary
+ * comes back device->host. */
+int shape_engine_evaluate(shape_engine *e, int form, shape_eval_summary *out);
+
+/* Results of the last evaluation (device->host copies). */
+int shape_engine_get_deldop_results(shape_engine *e, shape_deldop_result *out, int max);
+int shape_engine_get_fit(shape_engine *e, int global_frame, double *fit);
+/* POS maps are kept only when enabled before the evaluation (they cost HBM
+ * traffic): keep = 1 writes z, cos(e), cos(i) and facet maps of every frame. */
+int shape_engine_keep_pos(shape_engine *e, int keep);
+int shape_engine_get_pos(shape_engine *e, int global_frame, double *z, double *cose,
+                         int *facet);
+int shape_engine_get_lghtcrv_pos(shape_engine *e, int set, int point, double *z,
+                                 double *cose, double *cosi, int *facet, double *zill,
+                                 int *fill);
+/* Lightcurve outputs: y[ncalc] (calc_lghtcrv's y), fit[n], cal, chi2. */
+int shape_engine_get_lghtcrv(shape_engine *e, int set, double *y, double *fit,
+                             double *cal, double *chi2);
+int shape_engine_get_seen(shape_engine *e, unsigned char *seen);
+/* Realized model (realize_coordinates outputs). */
+int shape_engine_get_realized(shape_engine *e, double *x, double *vn, double *fn,
+                              double *area);
+
+/* Device time of the last evaluation (CUDA events on the engine stream). */
+int shape_engine_last_time_ms(shape_engine *e, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

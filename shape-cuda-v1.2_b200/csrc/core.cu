@@ -1,0 +1,680 @@
+// FP64 core kernels of the SHAPE B200 engine: model realization, view
+// transforms, facet binning, chi-square reductions, lightcurve photometry
+// and the evaluation summary.
+//
+// This translation unit is compiled with -fmad=false: the realization, the
+// view transforms and the facet bounding boxes must reproduce the reference
+// CPU arithmetic bit for bit (no a*b+c contraction), because they decide
+// which POS pixels each facet covers. Expressions keep the reference's
+// association order; sums that the reference starts from a literal 0.0
+// (cotrans, src/util/cotrans.c; mmmul) start from 0.0 here as well.
+#include <cfloat>
+#include <climits>
+
+#include "kernels.h"
+
+namespace shape {
+
+namespace {
+
+constexpr double SMALLVAL = SHAPE_SMALLVAL;
+constexpr double HUGENUMBER = SHAPE_HUGENUMBER;
+
+__device__ inline double dmin_(double a, double b) { return (a < b) ? a : b; }
+__device__ inline double dmax_(double a, double b) { return (a > b) ? a : b; }
+__device__ inline int clamp_lo(double v) { return (v < (double)INT_MIN) ? INT_MIN : (int)v; }
+__device__ inline int clamp_hi(double v) { return (v > (double)INT_MAX) ? INT_MAX : (int)v; }
+
+// ---------------------------------------------------------------- realize
+
+// x = scale * (u*r + a)  (src/shape/realize_mod.c:471-479)
+__global__ void k_realize_vertices(int nv, const double *__restrict__ a, const double *__restrict__ u,
+                                   const double *__restrict__ r, const double *__restrict__ scale,
+                                   double4 *__restrict__ vx)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    double ri = r[i];
+    double x0 = scale[0] * (u[3 * i + 0] * ri + a[3 * i + 0]);
+    double x1 = scale[1] * (u[3 * i + 1] * ri + a[3 * i + 1]);
+    double x2 = scale[2] * (u[3 * i + 2] * ri + a[3 * i + 2]);
+    vx[i] = make_double4(x0, x1, x2, 0.0);
+}
+
+// facet normal and area: facnrm (src/shape/facnrm.c:13-25), cross
+// (src/util/cross.c), normalize (src/util/normalize.c)
+__global__ void k_realize_facets(int nf, const int *__restrict__ fv, const double4 *__restrict__ vx,
+                                 double4 *__restrict__ fn, double *__restrict__ area,
+                                 int4 *__restrict__ fvi)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    int i0 = fv[3 * f + 0], i1 = fv[3 * f + 1], i2 = fv[3 * f + 2];
+    fvi[f] = make_int4(i0, i1, i2, 0);
+    double4 p0 = vx[i0], p1 = vx[i1], p2 = vx[i2];
+    double a0 = p1.x - p0.x, a1 = p1.y - p0.y, a2 = p1.z - p0.z;
+    double b0 = p2.x - p1.x, b1 = p2.y - p1.y, b2 = p2.z - p1.z;
+    double c0 = a1 * b2 - a2 * b1;
+    double c1 = a2 * b0 - a0 * b2;
+    double c2 = a0 * b1 - a1 * b0;
+    area[f] = 0.5 * sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    double norm = 0.0;
+    norm += c0 * c0;
+    norm += c1 * c1;
+    norm += c2 * c2;
+    norm = sqrt(norm);
+    if (norm != 0.0) {
+        c0 /= norm; c1 /= norm; c2 /= norm;
+    }
+    fn[f] = make_double4(c0, c1, c2, 0.0);
+}
+
+// vertex normal = normalized sum of attached facet normals, in af order
+// (src/shape/realize_mod.c:550-563)
+__global__ void k_realize_vnormals(int nv, const int *__restrict__ af_ptr, const int *__restrict__ af_idx,
+                                   const double4 *__restrict__ fn, double4 *__restrict__ vn)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    double n0 = 0.0, n1 = 0.0, n2 = 0.0;
+    for (int j = af_ptr[i]; j < af_ptr[i + 1]; j++) {
+        double4 fnj = fn[af_idx[j]];
+        n0 += fnj.x; n1 += fnj.y; n2 += fnj.z;
+    }
+    double norm = 0.0;
+    norm += n0 * n0;
+    norm += n1 * n1;
+    norm += n2 * n2;
+    norm = sqrt(norm);
+    if (norm != 0.0) {
+        n0 /= norm; n1 /= norm; n2 /= norm;
+    }
+    vn[i] = make_double4(n0, n1, n2, 0.0);
+}
+
+// ------------------------------------------------------------- transforms
+
+__device__ inline void store_vt(double4 *vt, int i, double x, double y, double z)
+{
+    vt[i] = make_double4(x, y, z, 0.0);
+}
+__device__ inline void store_vt(float4 *vt, int i, double x, double y, double z)
+{
+    vt[i] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z), 0.0f);
+}
+
+// Vertex coordinates in each view's frame: cotrans(v, oa, x, 1) then
+// += orbit_offset (= 0.0) (src/shape/posvis.c:159-166).
+template <typename T4>
+__global__ void k_xform(const FrameGeom *__restrict__ geoms, const double4 *__restrict__ vx, int nv,
+                        T4 *__restrict__ vt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const FrameGeom &g = geoms[blockIdx.y];
+    double4 x = vx[i];
+    double t[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        t[r] = 0.0;
+        t[r] += g.oa[3 * r + 0] * x.x;
+        t[r] += g.oa[3 * r + 1] * x.y;
+        t[r] += g.oa[3 * r + 2] * x.z;
+        t[r] += 0.0;
+    }
+    store_vt(vt, g.vt_base + i, t[0], t[1], t[2]);
+}
+
+// -------------------------------------------------------------- binning
+
+// Facet culling, bounding box, outbnd flag and POSrect bookkeeping of
+// posvis (src/shape/posvis.c:142-199, 322-364), then one bin entry per
+// overlapped 16x16 tile. Bin order is arbitrary; the raster kernel sorts.
+template <typename T4>
+__global__ void k_bin(const FrameGeom *__restrict__ geoms, int view0, int nf,
+                      const int4 *__restrict__ fvi, const double4 *__restrict__ fn,
+                      const T4 *__restrict__ vt, FrameState *__restrict__ states,
+                      int *__restrict__ bin_count, int *__restrict__ bin_ids, int cap)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    int v = view0 + blockIdx.y;
+    const FrameGeom &g = geoms[v];
+    double4 nb = fn[f];
+    double nz = 0.0;
+    nz += g.oa[6] * nb.x;
+    nz += g.oa[7] * nb.y;
+    nz += g.oa[8] * nb.z;
+    if (!(nz > 0.0)) return;
+    int4 c = fvi[f];
+    T4 p0 = vt[g.vt_base + c.x], p1 = vt[g.vt_base + c.y], p2 = vt[g.vt_base + c.z];
+    const double kmpp = g.kmpp;
+    const int n = g.n;
+    double xmin = dmin_((double)p0.x, dmin_((double)p1.x, (double)p2.x));
+    double xmax = dmax_((double)p0.x, dmax_((double)p1.x, (double)p2.x));
+    double ymin = dmin_((double)p0.y, dmin_((double)p1.y, (double)p2.y));
+    double ymax = dmax_((double)p0.y, dmax_((double)p1.y, (double)p2.y));
+    double imin_d = floor(xmin / kmpp - SMALLVAL + 0.5);
+    double imax_d = floor(xmax / kmpp + SMALLVAL + 0.5);
+    double jmin_d = floor(ymin / kmpp - SMALLVAL + 0.5);
+    double jmax_d = floor(ymax / kmpp + SMALLVAL + 0.5);
+    int imin = clamp_lo(imin_d), imax = clamp_hi(imax_d);
+    int jmin = clamp_lo(jmin_d), jmax = clamp_hi(jmax_d);
+    FrameState &st = states[v];
+    if (imin < -n || imax > n || jmin < -n || jmax > n)
+        st.outbnd = 1;
+    int i1 = max(imin, -n), i2 = min(imax, n), j1 = max(jmin, -n), j2 = min(jmax, n);
+    if (i1 > n || i2 < -n || j1 > n || j2 < -n) {
+        atomicMin(&st.ofr_i[0], max(imin, -n));
+        atomicMax(&st.ofr_i[1], min(imax, n));
+        atomicMin(&st.ofr_j[0], max(jmin, -n));
+        atomicMax(&st.ofr_j[1], min(jmax, n));
+        atomicMin(&st.ofr_ov[0], dkey(imin_d));
+        atomicMax(&st.ofr_ov[1], dkey(imax_d));
+        atomicMin(&st.ofr_ov[2], dkey(jmin_d));
+        atomicMax(&st.ofr_ov[3], dkey(jmax_d));
+        return;
+    }
+    int tx0 = (i1 + n) / TILE_W, tx1 = (i2 + n) / TILE_W;
+    int ty0 = (j1 + n) / TILE_W, ty1 = (j2 + n) / TILE_W;
+    for (int tx = tx0; tx <= tx1; tx++)
+        for (int ty = ty0; ty <= ty1; ty++) {
+            int tile = g.tile_base + tx * g.tiles_x + ty;
+            int slot = atomicAdd(&bin_count[tile], 1);
+            if (slot < cap)
+                bin_ids[(size_t)tile * cap + slot] = f;
+            else
+                st.bin_overflow = 1;
+        }
+}
+
+__global__ void k_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nviews) {
+        FrameState s;
+        s.outbnd = 0;
+        s.bin_overflow = 0;
+        s.cov_i[0] = s.cov_j[0] = INT_MAX;
+        s.cov_i[1] = s.cov_j[1] = INT_MIN;
+        s.ofr_i[0] = s.ofr_j[0] = INT_MAX;
+        s.ofr_i[1] = s.ofr_j[1] = INT_MIN;
+        s.ofr_ov[0] = s.ofr_ov[2] = dkey(HUGENUMBER);
+        s.ofr_ov[1] = s.ofr_ov[3] = dkey(-HUGENUMBER);
+        s.idellim[0] = s.idoplim[0] = INT_MAX;
+        s.idellim[1] = s.idoplim[1] = INT_MIN;
+        s.dellim[0] = s.doplim[0] = dkey(HUGENUMBER);
+        s.dellim[1] = s.doplim[1] = dkey(-HUGENUMBER);
+        s.any_lit = 0;
+        st[i] = s;
+    }
+    for (int t = i; t < ntiles; t += gridDim.x * blockDim.x)
+        bin_count[t] = 0;
+}
+
+// ----------------------------------------------------------------- chi2
+
+// Neumaier-compensated accumulator.
+struct KSum {
+    double s, c;
+    __device__ void add(double x)
+    {
+        double t = s + x;
+        if (fabs(s) >= fabs(x)) c += (s - t) + x; else c += (x - t) + s;
+        s = t;
+    }
+    __device__ void merge(const KSum &o)
+    {
+        add(o.s);
+        c += o.c;
+    }
+    __device__ double value() const { return s + c; }
+};
+
+__device__ inline KSum shfl_ksum(KSum a, int off)
+{
+    KSum b;
+    b.s = __shfl_down_sync(0xffffffffu, a.s, off);
+    b.c = __shfl_down_sync(0xffffffffu, a.c, off);
+    return b;
+}
+
+// Per (frame, chunk) partial sums of chi2_deldop (src/shape/chi2.c:436-441):
+// o2 = sum obs^2/var, m2 = sum fit^2/var, om = sum fit*obs/var, each
+// product in the reference's order, accumulated with compensation.
+template <typename T>
+__global__ void k_chi2_partials(Chi2Args a)
+{
+    __shared__ double red[CHI2_THREADS / 32][6];
+    for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
+        Chi2Item item = a.items[it];
+        const FrameGeom &g = a.geoms[a.frame_view[item.frame]];
+        const long long base = g.fit_base + item.start;
+        const T *fit = static_cast<const T *>(a.fit) + base;
+        const double *obs = a.obs + base, *oov = a.oov + base;
+        KSum o2 = {0, 0}, m2 = {0, 0}, om = {0, 0};
+        for (int k = threadIdx.x; k < item.count; k += blockDim.x) {
+            double ob = obs[k], w = oov[k], ft = (double)fit[k];
+            o2.add(ob * ob * w);
+            m2.add(ft * ft * w);
+            om.add(ft * ob * w);
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            o2.merge(shfl_ksum(o2, off));
+            m2.merge(shfl_ksum(m2, off));
+            om.merge(shfl_ksum(om, off));
+        }
+        int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l == 0) {
+            red[w][0] = o2.s; red[w][1] = o2.c; red[w][2] = m2.s;
+            red[w][3] = m2.c; red[w][4] = om.s; red[w][5] = om.c;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            KSum r[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++)
+                for (int q = 0; q < 3; q++) {
+                    r[q].add(red[ww][2 * q]);
+                    r[q].c += red[ww][2 * q + 1];
+                }
+            for (int q = 0; q < 3; q++) {
+                a.partials[(size_t)it * 6 + 2 * q] = r[q].s;
+                a.partials[(size_t)it * 6 + 2 * q + 1] = r[q].c;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Per-frame results: chi2_deldop's calibration and chi-square
+// (src/shape/chi2.c:447-460) plus the posvis / pos2deldop frame outputs.
+__global__ void k_finalize_frames(FinalizeArgs a)
+{
+    int fr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fr >= a.nframes) return;
+    const FrameHost &h = a.fh[fr];
+    const FrameGeom &g = a.geoms[h.view];
+    const FrameState &st = a.states[h.view];
+    KSum q[3] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int it = h.item0; it < h.item0 + h.nitems; it++)
+        for (int k = 0; k < 3; k++) {
+            q[k].add(a.partials[(size_t)it * 6 + 2 * k]);
+            q[k].c += a.partials[(size_t)it * 6 + 2 * k + 1];
+        }
+    double o2 = q[0].value(), m2 = q[1].value(), om = q[2].value();
+    double cal = h.cal_in;
+    if (h.cal_floating)
+        cal = (om > 0.0) ? om / m2 : SHAPE_TINYCALFACT;
+    shape_deldop_result r;
+    r.o2 = o2; r.m2 = m2; r.om = om; r.cal = cal;
+    r.chi2 = h.weight * (o2 - 2 * cal * om + cal * cal * m2);
+    const int n = g.n;
+    r.xlim[0] = min(n, min(st.cov_i[0], st.ofr_i[0]));
+    r.xlim[1] = max(-n, max(st.cov_i[1], st.ofr_i[1]));
+    r.ylim[0] = min(n, min(st.cov_j[0], st.ofr_j[0]));
+    r.ylim[1] = max(-n, max(st.cov_j[1], st.ofr_j[1]));
+    r.outbnd = st.outbnd;
+    r.posbnd_logfactor = 0.0;
+    if (st.outbnd) {
+        double oimin = dkey_inv(st.ofr_ov[0]), oimax = dkey_inv(st.ofr_ov[1]);
+        double ojmin = dkey_inv(st.ofr_ov[2]), ojmax = dkey_inv(st.ofr_ov[3]);
+        if (st.cov_i[0] != INT_MAX) {
+            oimin = dmin_(oimin, (double)st.cov_i[0]);
+            oimax = dmax_(oimax, (double)st.cov_i[1]);
+            ojmin = dmin_(ojmin, (double)st.cov_j[0]);
+            ojmax = dmax_(ojmax, (double)st.cov_j[1]);
+        }
+        double xfactor = (dmax_(oimax, n) - dmin_(oimin, -n) + 1) / (2 * n + 1);
+        double yfactor = (dmax_(ojmax, n) - dmin_(ojmin, -n) + 1) / (2 * n + 1);
+        r.posbnd_logfactor = log(xfactor * yfactor);
+    }
+    r.badradar = h.badradar;
+    r.badradar_logfactor = h.badradar_logfactor;
+    r.idellim[0] = min(g.ndel + 999999, st.idellim[0]);
+    r.idellim[1] = max(-999999, st.idellim[1]);
+    r.idoplim[0] = min(g.ndop + 999999, st.idoplim[0]);
+    r.idoplim[1] = max(-999999, st.idoplim[1]);
+    double dl0 = dmin_(HUGENUMBER, dkey_inv(st.dellim[0])), dl1 = dmax_(-HUGENUMBER, dkey_inv(st.dellim[1]));
+    double pl0 = dmin_(HUGENUMBER, dkey_inv(st.doplim[0])), pl1 = dmax_(-HUGENUMBER, dkey_inv(st.doplim[1]));
+    double dpp = a.set_delpp[h.set], fpp = a.set_doppp[h.set];
+    r.dellim[0] = (dl0 - g.delshift) * dpp;
+    r.dellim[1] = (dl1 - g.delshift) * dpp;
+    r.doplim[0] = (pl0 - g.dopshift) * fpp - a.dop_extra[fr];
+    r.doplim[1] = (pl1 - g.dopshift) * fpp + a.dop_extra[fr];
+    a.results[fr] = r;
+}
+
+// ------------------------------------------------------------ lightcurves
+
+__device__ inline int iround_(double x) { return (x < 0.0) ? (int)(x - 0.5) : (int)(x + 0.5); }
+
+// posmask (src/shape/posmask.c:58-174) and apply_photo
+// (src/shape/apply_photo.c:85-133, 226-248) per POS pixel of one
+// lightcurve point; brightness summed per work item (fixed order within a
+// block, items summed in order by k_lc_finalize).
+template <typename T>
+__global__ void k_lc_photo(LcArgs a)
+{
+    __shared__ double red[32];
+    for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
+        int2 item = a.items[it];
+        const LcPointDev &P = a.pts[item.x];
+        const FrameGeom &go = a.geoms[P.obs_view];
+        const FrameGeom &gs = a.geoms[P.sun_view];
+        const int n = go.n, side = go.side;
+        const long long npix = (long long)side * side;
+        const T *Z = static_cast<const T *>(a.z) + go.pos_base;
+        T *CE = static_cast<T *>(a.cose) + go.pos_base;
+        const T *CI = static_cast<const T *>(a.cosi) + go.pos_base;
+        const T *ZI = static_cast<const T *>(a.zill) + gs.pos_base;
+        const int *F = a.f + go.pos_base;
+        const int *FI = a.fill + gs.pos_base;
+        const double bignum = 0.99 * HUGENUMBER;
+        double bsum = 0.0;
+        long long pend = (long long)item.y + a.chunk;
+        if (pend > npix) pend = npix;
+        for (long long p = item.y + threadIdx.x; p < pend; p += blockDim.x) {
+            double cose = (double)CE[p];
+            if (cose == 0.0) continue;
+            int i = (int)(p / side) - n, j = (int)(p % side) - n;
+            double xin[3] = {i * go.kmpp, j * go.kmpp, (double)Z[p]};
+            double x[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                x[r] = 0.0;
+                x[r] += P.so[3 * r + 0] * xin[0];
+                x[r] += P.so[3 * r + 1] * xin[1];
+                x[r] += P.so[3 * r + 2] * xin[2];
+            }
+            double i0 = x[0] * P.pixels_per_km, j0 = x[1] * P.pixels_per_km;
+            int im = iround_(i0), jm = iround_(j0);
+#define ZILL(a_, b_) ((double)ZI[(long long)((a_) + n) * side + ((b_) + n)])
+            if (fabs(i0) < n && fabs(j0) < n && ZILL(im, jm) > -bignum &&
+                F[p] != FI[(long long)(im + n) * side + (jm + n)]) {
+                int i1 = (int)floor(i0), j1 = (int)floor(j0);
+                double zill;
+                if (ZILL(i1, j1) > -bignum && ZILL(i1 + 1, j1) > -bignum &&
+                    ZILL(i1, j1 + 1) > -bignum && ZILL(i1 + 1, j1 + 1) > -bignum) {
+                    double t = i0 - i1, u = j0 - j1;
+                    zill = (1 - t) * (1 - u) * ZILL(i1, j1) + t * (1 - u) * ZILL(i1 + 1, j1)
+                           + t * u * ZILL(i1 + 1, j1 + 1) + (1 - t) * u * ZILL(i1, j1 + 1);
+                } else {
+                    zill = ZILL(im, jm);
+                    int i_sign = (i0 >= im) ? 1 : -1;
+                    int i2 = im + i_sign;
+                    if (abs(i2) <= n && ZILL(i2, jm) > -bignum) {
+                        zill += fabs(i0 - im) * (ZILL(i2, jm) - ZILL(im, jm));
+                    } else {
+                        i2 = im - i_sign;
+                        if (abs(i2) <= n && ZILL(i2, jm) > -bignum)
+                            zill -= fabs(i0 - im) * (ZILL(i2, jm) - ZILL(im, jm));
+                    }
+                    int j_sign = (j0 >= jm) ? 1 : -1;
+                    int j2 = jm + j_sign;
+                    if (abs(j2) <= n && ZILL(im, j2) > -bignum) {
+                        zill += fabs(j0 - jm) * (ZILL(im, j2) - ZILL(im, jm));
+                    } else {
+                        j2 = jm - j_sign;
+                        if (abs(j2) <= n && ZILL(im, j2) > -bignum)
+                            zill -= fabs(j0 - jm) * (ZILL(im, j2) - ZILL(im, jm));
+                    }
+                }
+                if (zill - x[2] > P.mask_tol) {
+                    cose = 0.0;
+                    CE[p] = (T)0;
+                }
+            }
+#undef ZILL
+            double cosi = (double)CI[p];
+            int f = F[p];
+            if (a.mark_seen && cose > a.mincosine_seen && cosi > a.mincosine_seen && f >= 0)
+                a.seen[f] = 1;
+            if (cose > 0.0 && cosi > 0.0 && f >= 0) {
+                double b;
+                if (P.law_type == SHAPE_OPTLAW_LAMBERT)
+                    b = P.intensityfactor * P.scale * cosi;
+                else if (P.law_type == SHAPE_OPTLAW_LOMMEL)
+                    b = P.intensityfactor * P.scale * cosi / (cosi + cose);
+                else
+                    b = P.intensityfactor * cosi * (P.s_ls / (cosi + cose) + P.s_l);
+                bsum += b;
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1)
+            bsum += __shfl_down_sync(0xffffffffu, bsum, off);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
+            a.partials[it] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// posbnd_logfactor of one POS view (src/shape/posvis.c:301-307).
+__device__ double view_logfactor(const FrameGeom &g, const FrameState &st)
+{
+    const int n = g.n;
+    double oimin = dkey_inv(st.ofr_ov[0]), oimax = dkey_inv(st.ofr_ov[1]);
+    double ojmin = dkey_inv(st.ofr_ov[2]), ojmax = dkey_inv(st.ofr_ov[3]);
+    if (st.cov_i[0] != INT_MAX) {
+        oimin = dmin_(oimin, (double)st.cov_i[0]);
+        oimax = dmax_(oimax, (double)st.cov_i[1]);
+        ojmin = dmin_(ojmin, (double)st.cov_j[0]);
+        ojmax = dmax_(ojmax, (double)st.cov_j[1]);
+    }
+    double xfactor = (dmax_(oimax, n) - dmin_(oimin, -n) + 1) / (2 * n + 1);
+    double yfactor = (dmax_(ojmax, n) - dmin_(ojmin, -n) + 1) / (2 * n + 1);
+    return log(xfactor * yfactor);
+}
+
+// Natural cubic spline second derivatives (tridiagonal system solved by
+// forward elimination / back substitution) and evaluation; the role of
+// spline/splint in src/shape/calc_fits.c:1923-1933.
+__device__ void spline_natural_dev(const double *x, const double *y, int n, double *y2, double *cp)
+{
+    if (n < 3) {
+        for (int i = 0; i < n; i++) y2[i] = 0.0;
+        return;
+    }
+    y2[0] = 0.0;
+    cp[0] = 0.0;
+    for (int i = 1; i < n - 1; i++) {
+        double hl = x[i] - x[i - 1], hr = x[i + 1] - x[i];
+        double diag = 2.0 * (hl + hr) - hl * cp[i - 1];
+        double rhs = 6.0 * ((y[i + 1] - y[i]) / hr - (y[i] - y[i - 1]) / hl) - hl * y2[i - 1];
+        cp[i] = hr / diag;
+        y2[i] = rhs / diag;
+    }
+    y2[n - 1] = 0.0;
+    for (int i = n - 2; i >= 1; i--)
+        y2[i] -= cp[i] * y2[i + 1];
+}
+
+__device__ double splint_dev(const double *x, const double *y, const double *y2, int n, double t)
+{
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) / 2;
+        if (x[mid] > t) hi = mid; else lo = mid;
+    }
+    double h = x[hi] - x[lo];
+    double wl = (x[hi] - t) / h, wh = (t - x[lo]) / h;
+    return wl * y[lo] + wh * y[hi] +
+           ((wl * wl * wl - wl) * y2[lo] + (wh * wh * wh - wh) * y2[hi]) * (h * h) / 6.0;
+}
+
+// One block per lightcurve set: y from brightness partials, spline to the
+// observation epochs, chi2_lghtcrv (src/shape/chi2.c:1125-1170), posbnd sum
+// (src/shape/calc_fits.c:1651-1679, 1947).
+__global__ void k_lc_finalize(LcFinalizeArgs a)
+{
+    const LcSetDev &S = a.sets[blockIdx.x];
+    for (int k = threadIdx.x; k < S.npts; k += blockDim.x) {
+        int pt = S.pt0 + k;
+        int it0 = a.pt_items[2 * pt], cnt = a.pt_items[2 * pt + 1];
+        double s = 0.0;
+        for (int it = it0; it < it0 + cnt; it++) s += a.partials[it];
+        S.y[k] = (s == 0.0) ? 1.0e-40 : s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        spline_natural_dev(S.x, S.y, S.npts, S.y2, S.fit + S.n);   // fit tail is scratch
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < S.n; k += blockDim.x)
+        S.fit[k] = splint_dev(S.x, S.y, S.y2, S.npts, S.t[k]) / 1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double o2 = 0.0, m2 = 0.0, om = 0.0;
+        for (int k = 0; k < S.n; k++) {
+            o2 += S.obs[k] * S.obs[k] * S.oov[k];
+            m2 += S.fit[k] * S.fit[k] * S.oov[k];
+            om += S.fit[k] * S.obs[k] * S.oov[k];
+        }
+        double cal = S.cal_in;
+        if (S.cal_floating)
+            cal = (om > 0.0) ? om / m2 : SHAPE_TINYCALFACT;
+        double chi2 = S.weight * (o2 - 2 * cal * om + cal * cal * m2);
+        int posbnd = 0;
+        double lsum = 0.0;
+        for (int k = 0; k < S.npts; k++) {
+            const LcPointDev &P = a.pts[S.pt0 + k];
+            const FrameState &so = a.states[P.obs_view], &ss = a.states[P.sun_view];
+            if (so.outbnd) { posbnd = 1; lsum += 0.5 * view_logfactor(a.geoms[P.obs_view], so); }
+            if (ss.outbnd) { posbnd = 1; lsum += 0.5 * view_logfactor(a.geoms[P.sun_view], ss); }
+        }
+        double *o = a.set_out + 4 * blockIdx.x;
+        o[0] = cal; o[1] = chi2; o[2] = posbnd; o[3] = lsum;
+    }
+}
+
+// Totals over all sets in dataset order: chi2 (src/shape/chi2.c:270-300),
+// the posbnd / badradar flags and log-factors of calc_fits
+// (src/shape/calc_fits.c:407-409, 511-550, 1947) and the objective's
+// bad-model multipliers (src/shape/bestfit.c:806-866), no penalties.
+__global__ void k_summary(SummaryArgs a)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double chi2 = 0.0, chi2_dd = 0.0, chi2_lc = 0.0, plog = 0.0, blog = 0.0;
+    int posbnd = 0, badradar = 0;
+    for (int s = 0; s < a.nsets; s++) {
+        const SetRec &R = a.sets[s];
+        double cs = 0.0;
+        if (R.type == 0) {
+            for (int f = R.first; f < R.first + R.count; f++) {
+                const shape_deldop_result &r = a.results[f];
+                cs += r.chi2;
+                if (r.outbnd) { posbnd = 1; plog += a.fh[f].dof * r.posbnd_logfactor; }
+                if (r.badradar) { badradar = 1; blog += a.fh[f].dof * r.badradar_logfactor / 1; }
+            }
+            chi2_dd += cs;
+        } else {
+            const double *o = a.lc_out + 4 * R.first;
+            cs = o[1];
+            if (o[2] != 0.0) posbnd = 1;
+            plog += a.lc_dof[R.first] * (o[3] / a.lc_npts[R.first]);
+            chi2_lc += cs;
+        }
+        chi2 += cs;
+    }
+    shape_eval_summary out;
+    out.chi2 = chi2;
+    out.dof = a.dof;
+    out.chi2_deldop = chi2_dd;
+    out.chi2_lghtcrv = chi2_lc;
+    out.posbnd = posbnd;
+    out.posbnd_logfactor = plog / a.dof;
+    out.badradar = badradar;
+    out.badradar_logfactor = blog / (a.dof_deldop + 0.0);
+    double err = chi2 / a.dof;
+    if (a.baddiam) err *= a.bad_objfactor * exp(a.baddiam_logfactor);
+    if (posbnd) err *= a.bad_objfactor * exp(out.posbnd_logfactor);
+    if (badradar) err *= a.bad_objfactor * exp(out.badradar_logfactor);
+    out.objective = err;
+    *a.out = out;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- launchers
+
+void launch_realize(const ModelDev &m, cudaStream_t s)
+{
+    const int B = 256;
+    k_realize_vertices<<<(m.nv + B - 1) / B, B, 0, s>>>(m.nv, m.a, m.u, m.r, m.scale, m.vx);
+    k_realize_facets<<<(m.nf + B - 1) / B, B, 0, s>>>(m.nf, m.fv, m.vx, m.fn, m.area, m.fvi);
+    k_realize_vnormals<<<(m.nv + B - 1) / B, B, 0, s>>>(m.nv, m.af_ptr, m.af_idx, m.fn, m.vn);
+}
+
+void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, cudaStream_t s)
+{
+    int n = nviews > ntiles ? nviews : ntiles;
+    int blocks = (n + 255) / 256;
+    if (blocks > 4 * 148) blocks = 4 * 148;
+    if (blocks < (nviews + 255) / 256) blocks = (nviews + 255) / 256;
+    k_reset_state<<<blocks, 256, 0, s>>>(st, nviews, bin_count, ntiles);
+}
+
+void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt, cudaStream_t s)
+{
+    dim3 grid((nv + 255) / 256, nviews);
+    k_xform<double4><<<grid, 256, 0, s>>>(g, vx, nv, vt);
+}
+
+void launch_xform_f32(const FrameGeom *g, int nviews, const double4 *vx, int nv, float4 *vt, cudaStream_t s)
+{
+    dim3 grid((nv + 255) / 256, nviews);
+    k_xform<float4><<<grid, 256, 0, s>>>(g, vx, nv, vt);
+}
+
+void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const double4 *vt,
+                    FrameState *st, int *bin_count, int *bin_ids, int cap, cudaStream_t s)
+{
+    dim3 grid((m.nf + 255) / 256, nviews);
+    k_bin<double4><<<grid, 256, 0, s>>>(g, view0, m.nf, m.fvi, m.fn, vt, st, bin_count, bin_ids, cap);
+}
+
+void launch_bin_f32(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const float4 *vt,
+                    FrameState *st, int *bin_count, int *bin_ids, int cap, cudaStream_t s)
+{
+    dim3 grid((m.nf + 255) / 256, nviews);
+    k_bin<float4><<<grid, 256, 0, s>>>(g, view0, m.nf, m.fvi, m.fn, vt, st, bin_count, bin_ids, cap);
+}
+
+void launch_chi2_partials(const Chi2Args &a, int fp32, cudaStream_t s)
+{
+    int blocks = a.nitems < 8 * 148 ? a.nitems : 8 * 148;
+    if (blocks <= 0) return;
+    if (fp32) k_chi2_partials<float><<<blocks, CHI2_THREADS, 0, s>>>(a);
+    else k_chi2_partials<double><<<blocks, CHI2_THREADS, 0, s>>>(a);
+}
+
+void launch_finalize_frames(const FinalizeArgs &a, cudaStream_t s)
+{
+    if (a.nframes <= 0) return;
+    k_finalize_frames<<<(a.nframes + 127) / 128, 128, 0, s>>>(a);
+}
+
+void launch_lc_photo(const LcArgs &a, int fp32, cudaStream_t s)
+{
+    int blocks = a.nitems < 8 * 148 ? a.nitems : 8 * 148;
+    if (blocks <= 0) return;
+    if (fp32) k_lc_photo<float><<<blocks, 256, 0, s>>>(a);
+    else k_lc_photo<double><<<blocks, 256, 0, s>>>(a);
+}
+
+void launch_lc_finalize(const LcFinalizeArgs &a, cudaStream_t s)
+{
+    if (a.nsets <= 0) return;
+    k_lc_finalize<<<a.nsets, 256, 0, s>>>(a);
+}
+
+void launch_summary(const SummaryArgs &a, cudaStream_t s)
+{
+    k_summary<<<1, 32, 0, s>>>(a);
+}
+
+}  // namespace shape

@@ -1,0 +1,1059 @@
+// Host side of the SHAPE B200 engine and its C ABI (include/shape_b200.h).
+//
+// Per-frame constants of posvis / pos2deldop / posmask / apply_photo are
+// computed here in FP64 with the reference's operation order (this file is
+// compiled with -ffp-contract=off for the host compiler), uploaded once, and
+// reused by every evaluation. An evaluation copies the free model parameters
+// (vertex deviations and scale factors) host->device, runs the kernel
+// sequence on the engine stream and copies the summary device->host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "shape_b200.h"
+
+namespace shape {
+
+static thread_local std::string g_err;
+
+static int set_err(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return set_err(e_ == cudaErrorMemoryAllocation ? SHAPE_E_NOMEM : SHAPE_E_CUDA, \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));            \
+    } while (0)
+
+// y = A x with A row-major (cotrans dir=1, src/util/cotrans.c)
+static void mv(double y[3], const double *A, const double x[3])
+{
+    double t[3];
+    for (int i = 0; i < 3; i++) {
+        t[i] = 0.0;
+        for (int k = 0; k < 3; k++) t[i] += A[3 * i + k] * x[k];
+    }
+    y[0] = t[0]; y[1] = t[1]; y[2] = t[2];
+}
+// y = A^T x (cotrans dir=-1)
+static void mtv(double y[3], const double *A, const double x[3])
+{
+    double t[3];
+    for (int i = 0; i < 3; i++) {
+        t[i] = 0.0;
+        for (int k = 0; k < 3; k++) t[i] += A[3 * k + i] * x[k];
+    }
+    y[0] = t[0]; y[1] = t[1]; y[2] = t[2];
+}
+// M = B * A^T (mtrnsps + mmmul as in src/shape/posvis.c:101-122)
+static void mul_bt(double *M, const double *B, const double *A)
+{
+    double t[9];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            t[3 * i + j] = 0.0;
+            for (int k = 0; k < 3; k++) t[3 * i + j] += B[3 * i + k] * A[3 * j + k];
+        }
+    memcpy(M, t, sizeof t);
+}
+
+struct DevMem {
+    std::vector<void *> ptrs;
+    template <typename T> int alloc(T **p, size_t count)
+    {
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+        if (e != cudaSuccess)
+            return set_err(SHAPE_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        ptrs.push_back(*p);
+        return SHAPE_OK;
+    }
+    void release()
+    {
+        for (void *p : ptrs) cudaFree(p);
+        ptrs.clear();
+    }
+};
+
+struct DdSetHost {
+    shape_deldop_set set;
+    int frame0, nframes;
+};
+struct LcSetHost {
+    shape_lghtcrv_set set;
+    int pt0, npts;
+    std::vector<double> x, t, obs, oov;
+};
+
+struct EngineImpl {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+
+    // model (host)
+    int nv = 0, nf = 0;
+    std::vector<double> a, u, r;
+    double scale[3] = {1, 1, 1};
+    std::vector<int> fv, af_ptr, af_idx;
+    bool have_model = false;
+    shape_eval_params params{1, 1, 7, 0.0, 0.0, 1};
+    double bad_objfactor = 2.0;
+
+    // datasets (host)
+    std::vector<DdSetHost> dd;
+    std::vector<shape_deldop_frame> frames;
+    std::vector<long long> frame_off;   // element offsets into obs/oov/fit
+    std::vector<double> obs, oov;
+    std::vector<LcSetHost> lc;
+    std::vector<shape_lghtcrv_point> points;
+    std::vector<SetRec> setrecs;
+    std::vector<RadarLawDev> laws;
+    double dof = 0, dof_deldop = 0, dof_lghtcrv = 0;
+
+    // derived (host)
+    std::vector<FrameGeom> geoms;
+    std::vector<FrameHost> fh;
+    std::vector<int2> work;                 // raster items
+    std::vector<int> view_work0, view_nwork;
+    std::vector<Chi2Item> chi2_items;
+    std::vector<int> frame_view;
+    std::vector<double> dop_extra, set_delpp, set_doppp;
+    std::vector<LcPointDev> lcpts;
+    std::vector<int2> lc_items;
+    std::vector<int> pt_items;
+    int nviews = 0, ntiles = 0;
+    long long fit_elems = 0, pos_elems = 0;
+    int cap = 512;
+
+    // device
+    bool finalized = false;
+    DevMem mem;
+    ModelDev md{};
+    double *d_r = nullptr, *d_scale = nullptr, *d_a = nullptr, *d_u = nullptr;
+    int *d_fv = nullptr, *d_afp = nullptr, *d_afi = nullptr;
+    FrameGeom *d_geoms = nullptr;
+    FrameState *d_states = nullptr;
+    RadarLawDev *d_laws = nullptr;
+    int2 *d_work = nullptr;
+    double4 *d_vt64 = nullptr;
+    float4 *d_vt32 = nullptr;
+    int *d_bin_count = nullptr, *d_bin_ids = nullptr;
+    double *d_obs = nullptr, *d_oov = nullptr;
+    double *d_fit64 = nullptr;
+    float *d_fit32 = nullptr;
+    void *d_pos_z = nullptr, *d_pos_cose = nullptr, *d_pos_cosi = nullptr;   // sized for double
+    int *d_pos_f = nullptr;
+    unsigned char *d_seen = nullptr;
+    Chi2Item *d_chi2_items = nullptr;
+    int *d_frame_view = nullptr;
+    double *d_partials = nullptr;
+    FrameHost *d_fh = nullptr;
+    shape_deldop_result *d_results = nullptr;
+    double *d_set_delpp = nullptr, *d_set_doppp = nullptr, *d_dop_extra = nullptr;
+    LcPointDev *d_lcpts = nullptr;
+    int2 *d_lc_items = nullptr;
+    int *d_pt_items = nullptr;
+    double *d_lc_partials = nullptr;
+    LcSetDev *d_lcsets = nullptr;
+    double *d_lc_x = nullptr, *d_lc_t = nullptr, *d_lc_obs = nullptr, *d_lc_oov = nullptr;
+    double *d_lc_y = nullptr, *d_lc_y2 = nullptr, *d_lc_fit = nullptr, *d_lc_out = nullptr;
+    double *d_lc_dof = nullptr, *d_lc_npts = nullptr;
+    SetRec *d_setrecs = nullptr;
+    shape_eval_summary *d_summary = nullptr;
+    std::vector<LcSetDev> lcdev;
+
+    // pinned staging
+    double *h_params = nullptr;             // r[nv], scale[3]
+    shape_eval_summary *h_summary = nullptr;
+
+    // graphs per form
+    cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
+    int keep_pos = 0;
+    int graph_keep_pos[3] = {0, 0, 0};
+    int last_form = -1;
+
+    ~EngineImpl() { release(); }
+
+    void release()
+    {
+        for (auto &g : gexec)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        mem.release();
+        if (h_params) { cudaFreeHost(h_params); h_params = nullptr; }
+        if (h_summary) { cudaFreeHost(h_summary); h_summary = nullptr; }
+        if (ev0) { cudaEventDestroy(ev0); ev0 = nullptr; }
+        if (ev1) { cudaEventDestroy(ev1); ev1 = nullptr; }
+        if (stream) { cudaStreamDestroy(stream); stream = nullptr; }
+    }
+
+    void invalidate_graphs()
+    {
+        for (auto &g : gexec)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+
+    int finalize();
+    int enqueue(int form);
+    int evaluate(int form, shape_eval_summary *out);
+    void fill_params(double *dst) const
+    {
+        memcpy(dst, r.data(), sizeof(double) * nv);
+        double sc[3];
+        effective_scale(sc, nullptr, nullptr);
+        memcpy(dst + nv, sc, sizeof sc);
+    }
+    // scale factors after realize_coordinates' SMALLRATIO guard
+    // (src/shape/realize_mod.c:458-470; SMALLRATIO = 0.01, :138)
+    void effective_scale(double *sc, int *baddiam, double *logf) const
+    {
+        int bd = 0;
+        double lf = 0.0;
+        for (int j = 0; j < 3; j++) {
+            double v = scale[j];
+            if (v <= 0.01) {
+                bd = 1;
+                lf += log(1 + 0.01 - v);
+                v = 0.01 / (1 + 0.01 - v);
+            }
+            sc[j] = v;
+        }
+        if (baddiam) *baddiam = bd;
+        if (logf) *logf = lf;
+    }
+};
+
+static int radar_law_index(EngineImpl &E, const shape_radar_law &L)
+{
+    if (L.type < SHAPE_RADLAW_COSINE_DIFF || L.type > SHAPE_RADLAW_COSINE_COSINE) return -1;
+    RadarLawDev d{L.type, L.diff_R, L.diff_C, L.qs_R, L.qs_C, L.qs_cos_cutoff};
+    E.laws.push_back(d);
+    return (int)E.laws.size() - 1;
+}
+
+int EngineImpl::finalize()
+{
+    if (!have_model) return set_err(SHAPE_E_STATE, "finalize: no model set");
+    if (dd.empty() && lc.empty()) return set_err(SHAPE_E_STATE, "finalize: no datasets");
+    mem.release();
+    invalidate_graphs();
+    geoms.clear(); fh.clear(); work.clear(); view_work0.clear(); view_nwork.clear();
+    chi2_items.clear(); frame_view.clear(); dop_extra.clear(); set_delpp.clear(); set_doppp.clear();
+    lcpts.clear(); lc_items.clear(); pt_items.clear(); lcdev.clear();
+
+    const int nframes = (int)frames.size();
+    const int npts = (int)points.size();
+    nviews = nframes + 2 * npts;
+    int tile_base = 0;
+    long long pos_base = 0;
+    auto add_view = [&](FrameGeom &g, int n, double kmpp) {
+        g.n = n;
+        g.side = 2 * n + 1;
+        g.kmpp = kmpp;
+        g.tiles_x = (g.side + TILE_W - 1) / TILE_W;
+        g.tile_base = tile_base;
+        g.vt_base = (int)geoms.size() * nv;
+        g.pos_base = pos_base;
+        view_work0.push_back((int)work.size());
+        view_nwork.push_back(g.tiles_x * g.tiles_x);
+        for (int t = 0; t < g.tiles_x * g.tiles_x; t++) work.push_back(make_int2((int)geoms.size(), t));
+        tile_base += g.tiles_x * g.tiles_x;
+        pos_base += (long long)g.side * g.side;
+        geoms.push_back(g);
+    };
+
+    // delay-Doppler frames: constants of pos2deldop (src/shape/pos2deldop.c:201-275)
+    laws.clear();
+    for (size_t s = 0; s < dd.size(); s++) {
+        const shape_deldop_set &S = dd[s].set;
+        set_delpp.push_back(S.del_per_pixel);
+        set_doppp.push_back(S.dop_per_pixel);
+        int law = radar_law_index(*this, S.law);
+        if (law < 0) return set_err(SHAPE_E_UNSUPPORTED, "radar scattering law not supported");
+        if (S.spb < 1 || S.stride < 1 || S.spb / S.stride < 1)
+            return set_err(SHAPE_E_ARG, "deldop set: spb/stride must be >= 1");
+        for (int k = 0; k < dd[s].nframes; k++) {
+            int fi = dd[s].frame0 + k;
+            const shape_deldop_frame &F = frames[fi];
+            FrameGeom g;
+            memset(&g, 0, sizeof g);
+            mul_bt(g.oa, F.oe, F.ae);
+            g.kind = VIEW_RADAR;
+            g.smooth = params.pos_smooth;
+            g.ndel = F.ndel;
+            g.ndop = F.ndop;
+            g.fit_base = frame_off[fi];
+            g.codemethod = S.codemethod;
+            g.spb = S.spb;
+            g.stride = S.stride;
+            g.spb_over_stride = S.spb / S.stride;
+            g.one_over_spb = 1.0 / S.spb;
+            g.spb_sq = S.spb * S.spb;
+            if (S.codemethod != SHAPE_CODE_LONG_ORIG) {
+                g.const1 = (3 * S.spb - 1) / (2.0 * S.stride);
+                g.const2 = (S.spb - 1) / (2.0 * S.stride);
+            } else {
+                g.const1 = (double)g.spb_over_stride;
+                g.const2 = 0.0;
+            }
+            g.delfact = -SHAPE_KM2US / S.del_per_pixel;
+            double w[3];
+            mv(w, F.oe, F.spin);
+            double dopfact = S.dopscale * SHAPE_KM2HZFACT * F.km_per_pixel * S.Ftx / S.dop_per_pixel;
+            g.ax = -w[1] * dopfact;
+            g.ay = w[0] * dopfact;
+            double km2Hz = sqrt(g.ax * g.ax + g.ay * g.ay) * S.dop_per_pixel / F.km_per_pixel;
+            double dx = 0.0;
+            if (w[0] != 0.0 || w[1] != 0.0)
+                dx = km2Hz * 0.5 * F.km_per_pixel * sqrt(w[0] * w[0] + w[1] * w[1]) /
+                     std::max(fabs(w[0]), fabs(w[1]));
+            dop_extra.push_back(dx);
+            g.nsinc2 = params.nsinc2;
+            g.nsinc2_sq = params.nsinc2 * params.nsinc2;
+            g.sinc2width = params.sinc2width;
+            g.xincr = g.ax / params.nsinc2;
+            g.yincr = g.ay / params.nsinc2;
+            g.dopdiff_bl = -(params.nsinc2 - 1) * (g.xincr + g.yincr) / 2;
+            g.dopdiff_max = (params.nsinc2 - 1) * (fabs(g.xincr) + fabs(g.yincr)) / 2;
+            g.delshift = F.delcom_vig + F.deloff;
+            g.dopshift = F.dopcom_vig + F.dopoff + 0.0;
+            g.dopDC_vig = F.dopDC_vig;
+            g.dopfftlen = S.dopfftlen;
+            g.law = law;
+            g.frame_index = fi;
+            FrameHost h;
+            memset(&h, 0, sizeof h);
+            h.weight = F.weight;
+            h.dof = F.dof;
+            h.cal_in = F.cal;
+            h.cal_floating = F.cal_floating;
+            if (2 * g.dopdiff_max + params.sinc2width + 1 > SHAPE_MAXBINS) {
+                h.badradar = 1;
+                h.badradar_logfactor = log((2 * g.dopdiff_max + params.sinc2width + 1) / SHAPE_MAXBINS);
+            }
+            h.view = (int)geoms.size();
+            h.set = (int)s;
+            frame_view.push_back(h.view);
+            h.item0 = (int)chi2_items.size();
+            int D = F.ndel * F.ndop, chunk = CHI2_THREADS * CHI2_ITEMS;
+            for (int st = 0; st < D; st += chunk)
+                chi2_items.push_back(Chi2Item{fi, st, std::min(chunk, D - st)});
+            h.nitems = (int)chi2_items.size() - h.item0;
+            fh.push_back(h);
+            add_view(g, F.pos_n, F.km_per_pixel);
+        }
+    }
+    // lightcurve points: two views each (src/shape/calc_fits.c:1634-1716)
+    const int LC_CHUNK = 4096;
+    for (size_t s = 0; s < lc.size(); s++) {
+        const shape_lghtcrv_set &S = lc[s].set;
+        if (S.law.type != SHAPE_OPTLAW_LAMBERT && S.law.type != SHAPE_OPTLAW_LOMMEL &&
+            S.law.type != SHAPE_OPTLAW_KAASALAINEN)
+            return set_err(SHAPE_E_UNSUPPORTED, "optical scattering law not supported");
+        LcSetDev L;
+        memset(&L, 0, sizeof L);
+        L.npts = lc[s].npts;
+        L.n = S.n;
+        L.pt0 = lc[s].pt0;
+        L.item0 = (int)lc_items.size();
+        L.weight = S.weight;
+        L.dof = S.dof;
+        L.cal_in = S.cal;
+        L.cal_floating = S.cal_floating;
+        for (int k = 0; k < lc[s].npts; k++) {
+            const shape_lghtcrv_point &P = points[lc[s].pt0 + k];
+            LcPointDev pd;
+            memset(&pd, 0, sizeof pd);
+            FrameGeom go;
+            memset(&go, 0, sizeof go);
+            mul_bt(go.oa, P.oe, P.ae);
+            double us[3] = {0.0, 0.0, 1.0};
+            mtv(us, P.se, us);
+            mv(us, P.oe, us);
+            go.usrc[0] = us[0]; go.usrc[1] = us[1]; go.usrc[2] = us[2];
+            go.kind = VIEW_LC_OBS;
+            go.smooth = params.pos_smooth;
+            go.frame_index = lc[s].pt0 + k;
+            pd.obs_view = (int)geoms.size();
+            add_view(go, P.pos_n, P.km_per_pixel);
+            FrameGeom gs;
+            memset(&gs, 0, sizeof gs);
+            mul_bt(gs.oa, P.se, P.ae);
+            gs.kind = VIEW_LC_SUN;
+            gs.smooth = 0;
+            gs.frame_index = lc[s].pt0 + k;
+            pd.sun_view = (int)geoms.size();
+            add_view(gs, P.pos_n, P.km_per_pixel);
+            mul_bt(pd.so, P.se, P.oe);
+            pd.set = (int)s;
+            pd.law_type = S.law.type;
+            pd.intensityfactor = pow(P.km_per_pixel / SHAPE_AU, 2.0);
+            if (S.law.type == SHAPE_OPTLAW_LAMBERT) {
+                pd.scale = S.law.R / SHAPE_PIE;
+            } else if (S.law.type == SHAPE_OPTLAW_LOMMEL) {
+                pd.scale = S.law.R / (4 * SHAPE_PIE);
+            } else {
+                double phasefunc = S.law.A0 * exp(-P.solar_phase / S.law.D) + S.law.k * P.solar_phase + 1;
+                pd.s_ls = (1 - S.law.wt) * phasefunc * S.law.R / (4 * SHAPE_PIE);
+                pd.s_l = S.law.wt * phasefunc * S.law.R / SHAPE_PIE;
+            }
+            pd.mask_tol = params.mask_tol;
+            pd.pixels_per_km = 1 / P.km_per_pixel;
+            int side = 2 * P.pos_n + 1;
+            long long np = (long long)side * side;
+            pt_items.push_back((int)lc_items.size());
+            int cnt = 0;
+            for (long long p0 = 0; p0 < np; p0 += LC_CHUNK, cnt++)
+                lc_items.push_back(make_int2((int)lcpts.size(), (int)p0));
+            pt_items.push_back(cnt);
+            lcpts.push_back(pd);
+        }
+        L.nitems = (int)lc_items.size() - L.item0;
+        lcdev.push_back(L);
+    }
+    if (laws.empty()) laws.push_back(RadarLawDev{SHAPE_RADLAW_COSINE_DIFF, 0.0, 0.0, 0.0, 0.0, 0.0});
+    ntiles = tile_base;
+    pos_elems = pos_base;
+    fit_elems = obs.size();
+
+    // ---- device allocations
+    int rc;
+#define AL(p, n) if ((rc = mem.alloc(&(p), (n))) != SHAPE_OK) return rc
+    AL(d_a, (size_t)3 * nv); AL(d_u, (size_t)3 * nv); AL(d_r, (size_t)nv + 3);
+    d_scale = d_r + nv;
+    AL(d_fv, (size_t)3 * nf); AL(d_afp, (size_t)nv + 1); AL(d_afi, af_idx.size());
+    AL(md.vx, (size_t)nv); AL(md.vn, (size_t)nv); AL(md.fn, (size_t)nf); AL(md.area, (size_t)nf);
+    AL(md.fvi, (size_t)nf);
+    AL(d_geoms, (size_t)nviews); AL(d_states, (size_t)nviews); AL(d_laws, laws.size());
+    AL(d_work, work.size());
+    AL(d_vt64, (size_t)nviews * nv); AL(d_vt32, (size_t)nviews * nv);
+    AL(d_bin_count, (size_t)ntiles); AL(d_bin_ids, (size_t)ntiles * cap);
+    AL(d_obs, (size_t)fit_elems); AL(d_oov, (size_t)fit_elems);
+    AL(d_fit64, (size_t)fit_elems); AL(d_fit32, (size_t)fit_elems);
+    {
+        double *pz, *pc, *pi;
+        AL(pz, (size_t)pos_elems); AL(pc, (size_t)pos_elems); AL(pi, (size_t)pos_elems);
+        d_pos_z = pz; d_pos_cose = pc; d_pos_cosi = pi;
+    }
+    AL(d_pos_f, (size_t)pos_elems);
+    AL(d_seen, (size_t)nf);
+    AL(d_chi2_items, chi2_items.size()); AL(d_frame_view, frame_view.size());
+    AL(d_partials, chi2_items.size() * 6);
+    AL(d_fh, fh.size()); AL(d_results, fh.size());
+    AL(d_set_delpp, set_delpp.size()); AL(d_set_doppp, set_doppp.size()); AL(d_dop_extra, dop_extra.size());
+    AL(d_lcpts, lcpts.size()); AL(d_lc_items, lc_items.size()); AL(d_pt_items, pt_items.size());
+    AL(d_lc_partials, lc_items.size());
+    AL(d_lcsets, lcdev.size()); AL(d_lc_out, 4 * lcdev.size());
+    AL(d_lc_dof, lcdev.size()); AL(d_lc_npts, lcdev.size());
+    AL(d_setrecs, setrecs.size());
+    AL(d_summary, 1);
+    size_t lc_tot_pts = points.size(), lc_tot_n = 0;
+    for (auto &L : lc) lc_tot_n += L.set.n;
+    AL(d_lc_x, lc_tot_pts); AL(d_lc_y, lc_tot_pts); AL(d_lc_y2, lc_tot_pts);
+    AL(d_lc_t, lc_tot_n); AL(d_lc_obs, lc_tot_n); AL(d_lc_oov, lc_tot_n);
+    AL(d_lc_fit, lc_tot_n + lc_tot_pts);
+#undef AL
+    if (!h_params) CK(cudaMallocHost((void **)&h_params, sizeof(double) * ((size_t)nv + 3)));
+    else {
+        cudaFreeHost(h_params);
+        CK(cudaMallocHost((void **)&h_params, sizeof(double) * ((size_t)nv + 3)));
+    }
+    if (!h_summary) CK(cudaMallocHost((void **)&h_summary, sizeof(shape_eval_summary)));
+
+    // ---- uploads (once)
+    cudaStream_t s = stream;
+    CK(cudaMemcpyAsync(d_a, a.data(), sizeof(double) * 3 * nv, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_u, u.data(), sizeof(double) * 3 * nv, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_fv, fv.data(), sizeof(int) * 3 * nf, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_afp, af_ptr.data(), sizeof(int) * (nv + 1), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_afi, af_idx.data(), sizeof(int) * std::max<size_t>(1, af_idx.size()),
+                       cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_geoms, geoms.data(), sizeof(FrameGeom) * nviews, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_laws, laws.data(), sizeof(RadarLawDev) * std::max<size_t>(1, laws.size()),
+                       cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_work, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, s));
+    if (fit_elems) {
+        CK(cudaMemcpyAsync(d_obs, obs.data(), sizeof(double) * fit_elems, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_oov, oov.data(), sizeof(double) * fit_elems, cudaMemcpyHostToDevice, s));
+    }
+    if (!chi2_items.empty()) {
+        CK(cudaMemcpyAsync(d_chi2_items, chi2_items.data(), sizeof(Chi2Item) * chi2_items.size(),
+                           cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_frame_view, frame_view.data(), sizeof(int) * frame_view.size(),
+                           cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_fh, fh.data(), sizeof(FrameHost) * fh.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_set_delpp, set_delpp.data(), sizeof(double) * set_delpp.size(),
+                           cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_set_doppp, set_doppp.data(), sizeof(double) * set_doppp.size(),
+                           cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_dop_extra, dop_extra.data(), sizeof(double) * dop_extra.size(),
+                           cudaMemcpyHostToDevice, s));
+    }
+    if (!lcpts.empty()) {
+        CK(cudaMemcpyAsync(d_lcpts, lcpts.data(), sizeof(LcPointDev) * lcpts.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_lc_items, lc_items.data(), sizeof(int2) * lc_items.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_pt_items, pt_items.data(), sizeof(int) * pt_items.size(), cudaMemcpyHostToDevice, s));
+        size_t px = 0, pn = 0;
+        std::vector<double> lcdof, lcnp;
+        for (size_t k = 0; k < lc.size(); k++) {
+            LcSetDev &L = lcdev[k];
+            L.x = d_lc_x + px; L.y = d_lc_y + px; L.y2 = d_lc_y2 + px;
+            L.t = d_lc_t + pn; L.obs = d_lc_obs + pn; L.oov = d_lc_oov + pn;
+            L.fit = d_lc_fit + pn + px;   // n outputs followed by npts scratch
+            CK(cudaMemcpyAsync(d_lc_x + px, lc[k].x.data(), sizeof(double) * L.npts, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(d_lc_t + pn, lc[k].t.data(), sizeof(double) * L.n, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(d_lc_obs + pn, lc[k].obs.data(), sizeof(double) * L.n, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(d_lc_oov + pn, lc[k].oov.data(), sizeof(double) * L.n, cudaMemcpyHostToDevice, s));
+            px += L.npts;
+            pn += L.n;
+            lcdof.push_back(L.dof);
+            lcnp.push_back((double)L.npts);
+        }
+        CK(cudaMemcpyAsync(d_lcsets, lcdev.data(), sizeof(LcSetDev) * lcdev.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_lc_dof, lcdof.data(), sizeof(double) * lcdof.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_lc_npts, lcnp.data(), sizeof(double) * lcnp.size(), cudaMemcpyHostToDevice, s));
+    }
+    CK(cudaMemcpyAsync(d_setrecs, setrecs.data(), sizeof(SetRec) * setrecs.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(d_seen, 0, nf, s));
+    CK(cudaStreamSynchronize(s));
+
+    CK(configure_raster_f64());
+    CK(configure_raster_f32());
+    md.nv = nv; md.nf = nf;
+    md.a = d_a; md.u = d_u; md.r = d_r; md.scale = d_scale;
+    md.fv = d_fv; md.af_ptr = d_afp; md.af_idx = d_afi;
+    finalized = true;
+    return SHAPE_OK;
+}
+
+// Enqueue one evaluation (without the H2D of parameters / D2H of the summary).
+int EngineImpl::enqueue(int form)
+{
+    cudaStream_t s = stream;
+    const bool f32 = (form == SHAPE_FORM_BATCHED_FP32);
+    launch_realize(md, s);
+    launch_reset_state(d_states, nviews, d_bin_count, ntiles, s);
+    if (fit_elems) {
+        if (f32) CK(cudaMemsetAsync(d_fit32, 0, sizeof(float) * fit_elems, s));
+        else CK(cudaMemsetAsync(d_fit64, 0, sizeof(double) * fit_elems, s));
+    }
+    CK(cudaMemsetAsync(d_seen, 0, nf, s));
+
+    RasterArgs ra;
+    memset(&ra, 0, sizeof ra);
+    ra.geoms = d_geoms;
+    ra.vt = f32 ? (const void *)d_vt32 : (const void *)d_vt64;
+    ra.fvi = md.fvi;
+    ra.vn = md.vn;
+    ra.fn = md.fn;
+    ra.nf = nf;
+    ra.bin_count = d_bin_count;
+    ra.bin_ids = d_bin_ids;
+    ra.cap = cap;
+    ra.states = d_states;
+    ra.laws = d_laws;
+    ra.fit = f32 ? (void *)d_fit32 : (void *)d_fit64;
+    ra.pos_z = d_pos_z; ra.pos_cose = d_pos_cose; ra.pos_cosi = d_pos_cosi; ra.pos_f = d_pos_f;
+    ra.seen = d_seen;
+    ra.mincosine_seen = params.mincosine_seen;
+    ra.mark_seen = params.mark_seen;
+    ra.keep_pos = keep_pos;
+
+    Chi2Args ca;
+    ca.obs = d_obs; ca.oov = d_oov;
+    ca.fit = ra.fit;
+    ca.geoms = d_geoms;
+    ca.frame_view = d_frame_view;
+    ca.partials = d_partials;
+
+    LcArgs la;
+    memset(&la, 0, sizeof la);
+    la.pts = d_lcpts; la.geoms = d_geoms; la.states = d_states;
+    la.chunk = 4096;
+    la.z = d_pos_z; la.cose = d_pos_cose; la.cosi = d_pos_cosi; la.zill = d_pos_z;
+    la.f = d_pos_f; la.fill = d_pos_f;
+    la.partials = d_lc_partials;
+    la.seen = d_seen;
+    la.mincosine_seen = params.mincosine_seen;
+    la.mark_seen = params.mark_seen;
+
+    if (form == SHAPE_FORM_PLAIN_FP64) {
+        // One view at a time, in dataset order, as calc_fits walks frames.
+        for (int v = 0; v < nviews; v++) {
+            launch_xform_f64(d_geoms + v, 1, md.vx, nv, d_vt64, s);
+            launch_bin_f64(d_geoms, v, 1, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
+            RasterArgs rv = ra;
+            rv.work = d_work + view_work0[v];
+            rv.nwork = view_nwork[v];
+            launch_raster_f64(rv, s);
+            const FrameGeom &g = geoms[v];
+            if (g.kind == VIEW_RADAR) {
+                const FrameHost &h = fh[g.frame_index];
+                Chi2Args cv = ca;
+                cv.items = d_chi2_items + h.item0;
+                cv.nitems = h.nitems;
+                cv.partials = d_partials + (size_t)h.item0 * 6;
+                launch_chi2_partials(cv, 0, s);
+            } else if (g.kind == VIEW_LC_SUN) {
+                int pt = g.frame_index;
+                LcArgs lv = la;
+                lv.items = d_lc_items + pt_items[2 * pt];
+                lv.nitems = pt_items[2 * pt + 1];
+                lv.partials = d_lc_partials + pt_items[2 * pt];
+                launch_lc_photo(lv, 0, s);
+            }
+        }
+    } else {
+        if (f32) {
+            launch_xform_f32(d_geoms, nviews, md.vx, nv, d_vt32, s);
+            launch_bin_f32(d_geoms, 0, nviews, md, d_vt32, d_states, d_bin_count, d_bin_ids, cap, s);
+        } else {
+            launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
+            launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
+        }
+        ra.work = d_work;
+        ra.nwork = (int)work.size();
+        if (f32) launch_raster_f32(ra, s); else launch_raster_f64(ra, s);
+        if (!chi2_items.empty()) {
+            ca.items = d_chi2_items;
+            ca.nitems = (int)chi2_items.size();
+            launch_chi2_partials(ca, f32 ? 1 : 0, s);
+        }
+        if (!lc_items.empty()) {
+            la.items = d_lc_items;
+            la.nitems = (int)lc_items.size();
+            launch_lc_photo(la, f32 ? 1 : 0, s);
+        }
+    }
+    if (!fh.empty()) {
+        FinalizeArgs fa;
+        memset(&fa, 0, sizeof fa);
+        fa.nframes = (int)fh.size();
+        fa.fh = d_fh; fa.geoms = d_geoms; fa.states = d_states; fa.partials = d_partials;
+        fa.results = d_results; fa.set_delpp = d_set_delpp; fa.set_doppp = d_set_doppp;
+        fa.dop_extra = d_dop_extra;
+        launch_finalize_frames(fa, s);
+    }
+    if (!lcdev.empty()) {
+        LcFinalizeArgs lf;
+        lf.nsets = (int)lcdev.size();
+        lf.sets = d_lcsets; lf.pts = d_lcpts; lf.geoms = d_geoms; lf.states = d_states;
+        lf.pt_items = d_pt_items; lf.partials = d_lc_partials; lf.set_out = d_lc_out;
+        launch_lc_finalize(lf, s);
+    }
+    SummaryArgs sa;
+    memset(&sa, 0, sizeof sa);
+    sa.nsets = (int)setrecs.size();
+    sa.sets = d_setrecs; sa.fh = d_fh; sa.results = d_results;
+    sa.lc_out = d_lc_out; sa.lc_dof = d_lc_dof; sa.lc_npts = d_lc_npts;
+    sa.dof = dof; sa.dof_deldop = dof_deldop; sa.bad_objfactor = bad_objfactor;
+    // the bad-diameter factor depends only on host-side scale factors and is
+    // applied by evaluate(), so captured graphs stay valid when it changes
+    sa.baddiam = 0;
+    sa.baddiam_logfactor = 0.0;
+    sa.out = d_summary;
+    launch_summary(sa, s);
+    CK(cudaGetLastError());
+    return SHAPE_OK;
+}
+
+int EngineImpl::evaluate(int form, shape_eval_summary *out)
+{
+    if (!finalized) return set_err(SHAPE_E_STATE, "evaluate before finalize");
+    if (form < 0 || form > 2) return set_err(SHAPE_E_ARG, "unknown form");
+    cudaStream_t s = stream;
+    fill_params(h_params);
+    int baddiam;
+    double bdl, sc[3];
+    effective_scale(sc, &baddiam, &bdl);
+    if (form == SHAPE_FORM_PLAIN_FP64) {
+        CK(cudaEventRecord(ev0, s));
+        CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s));
+        int rc = enqueue(form);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(h_summary, d_summary, sizeof(shape_eval_summary), cudaMemcpyDeviceToHost, s));
+        CK(cudaEventRecord(ev1, s));
+    } else {
+        if (gexec[form] && graph_keep_pos[form] != keep_pos) {
+            cudaGraphExecDestroy(gexec[form]);
+            gexec[form] = nullptr;
+        }
+        if (!gexec[form]) {
+            // baddiam factors are baked into the summary launch: graphs are
+            // rebuilt if the flag changes (rare: a scale factor <= 0.01).
+            cudaGraph_t graph;
+            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s);
+            int rc = enqueue(form);
+            cudaMemcpyAsync(h_summary, d_summary, sizeof(shape_eval_summary), cudaMemcpyDeviceToHost, s);
+            cudaError_t ce = cudaStreamEndCapture(s, &graph);
+            if (rc) { if (ce == cudaSuccess) cudaGraphDestroy(graph); return rc; }
+            CK(ce);
+            CK(cudaGraphInstantiate(&gexec[form], graph, 0));
+            cudaGraphDestroy(graph);
+            graph_keep_pos[form] = keep_pos;
+        }
+        CK(cudaEventRecord(ev0, s));
+        CK(cudaGraphLaunch(gexec[form], s));
+        CK(cudaEventRecord(ev1, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
+    last_form = form;
+    shape_eval_summary sm = *h_summary;
+    // bad-diameter factor depends only on the host-side scale factors
+    if (baddiam) {
+        sm.objective = sm.chi2 / sm.dof * (bad_objfactor * exp(bdl));
+        if (sm.posbnd) sm.objective *= bad_objfactor * exp(sm.posbnd_logfactor);
+        if (sm.badradar) sm.objective *= bad_objfactor * exp(sm.badradar_logfactor);
+    }
+    if (out) *out = sm;
+    return SHAPE_OK;
+}
+
+}  // namespace shape
+
+// ====================================================================== C ABI
+
+using shape::EngineImpl;
+
+struct shape_engine {
+    EngineImpl impl;
+};
+
+extern "C" {
+
+const char *shape_last_error(void) { return shape::g_err.c_str(); }
+const char *shape_version(void) { return "shape-b200 0.1 (sm_100a)"; }
+
+int shape_abi_sizes(size_t *out, int max)
+{
+    size_t v[] = {sizeof(shape_model_desc), sizeof(shape_radar_law), sizeof(shape_optical_law),
+                  sizeof(shape_eval_params), sizeof(shape_deldop_frame), sizeof(shape_deldop_set),
+                  sizeof(shape_lghtcrv_point), sizeof(shape_lghtcrv_set), sizeof(shape_deldop_result),
+                  sizeof(shape_eval_summary)};
+    int n = (int)(sizeof v / sizeof v[0]);
+    for (int i = 0; i < n && i < max; i++) out[i] = v[i];
+    return n;
+}
+
+int shape_engine_create(int device, shape_engine **out)
+{
+    if (!out) return shape::set_err(SHAPE_E_ARG, "null out");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return shape::set_err(SHAPE_E_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return shape::set_err(SHAPE_E_ARG, "bad device index");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
+    shape_engine *h = new shape_engine();
+    h->impl.device = device;
+    if (cudaStreamCreateWithFlags(&h->impl.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&h->impl.ev0) != cudaSuccess || cudaEventCreate(&h->impl.ev1) != cudaSuccess) {
+        delete h;
+        return shape::set_err(SHAPE_E_CUDA, "stream/event creation failed");
+    }
+    *out = h;
+    return SHAPE_OK;
+}
+
+void shape_engine_destroy(shape_engine *e)
+{
+    if (!e) return;
+    cudaSetDevice(e->impl.device);
+    delete e;
+}
+
+int shape_engine_set_model(shape_engine *h, const shape_model_desc *m)
+{
+    if (!h || !m || m->nv <= 0 || m->nf <= 0 || !m->a || !m->u || !m->r || !m->fv || !m->af_ptr)
+        return shape::set_err(SHAPE_E_ARG, "set_model: invalid model description");
+    EngineImpl &E = h->impl;
+    E.nv = m->nv; E.nf = m->nf;
+    E.a.assign(m->a, m->a + 3 * (size_t)m->nv);
+    E.u.assign(m->u, m->u + 3 * (size_t)m->nv);
+    E.r.assign(m->r, m->r + m->nv);
+    for (int j = 0; j < 3; j++) E.scale[j] = m->scale[j];
+    E.fv.assign(m->fv, m->fv + 3 * (size_t)m->nf);
+    for (int k = 0; k < 3 * m->nf; k++)
+        if (E.fv[k] < 0 || E.fv[k] >= m->nv) return shape::set_err(SHAPE_E_ARG, "set_model: facet vertex out of range");
+    E.af_ptr.assign(m->af_ptr, m->af_ptr + m->nv + 1);
+    int naf = E.af_ptr[m->nv];
+    if (naf < 0 || E.af_ptr[0] != 0) return shape::set_err(SHAPE_E_ARG, "set_model: bad af_ptr");
+    E.af_idx.assign(m->af_idx, m->af_idx + naf);
+    for (int k = 0; k < naf; k++)
+        if (E.af_idx[k] < 0 || E.af_idx[k] >= m->nf) return shape::set_err(SHAPE_E_ARG, "set_model: attached facet out of range");
+    E.have_model = true;
+    E.finalized = false;
+    return SHAPE_OK;
+}
+
+int shape_engine_set_params(shape_engine *h, const shape_eval_params *p)
+{
+    if (!h || !p) return shape::set_err(SHAPE_E_ARG, "null argument");
+    if (p->nsinc2 < 1 || p->sinc2width < 1) return shape::set_err(SHAPE_E_ARG, "nsinc2 and sinc2width must be >= 1");
+    h->impl.params = *p;
+    h->impl.finalized = false;
+    return SHAPE_OK;
+}
+
+int shape_engine_add_deldop_set(shape_engine *h, const shape_deldop_set *set, int nframes,
+                                const shape_deldop_frame *frames, const double *obs, const double *oov)
+{
+    if (!h || !set || nframes <= 0 || !frames || !obs || !oov)
+        return shape::set_err(SHAPE_E_ARG, "add_deldop_set: invalid argument");
+    EngineImpl &E = h->impl;
+    shape::DdSetHost d;
+    d.set = *set;
+    d.frame0 = (int)E.frames.size();
+    d.nframes = nframes;
+    size_t off = 0;
+    for (int k = 0; k < nframes; k++) {
+        const shape_deldop_frame &F = frames[k];
+        if (F.pos_n < 1 || F.ndel < 1 || F.ndop < 1 || !(F.km_per_pixel > 0))
+            return shape::set_err(SHAPE_E_ARG, "add_deldop_set: bad frame size");
+        E.frame_off.push_back((long long)E.obs.size());
+        size_t D = (size_t)F.ndel * F.ndop;
+        E.obs.insert(E.obs.end(), obs + off, obs + off + D);
+        E.oov.insert(E.oov.end(), oov + off, oov + off + D);
+        off += D;
+        E.frames.push_back(F);
+        E.dof += F.dof;
+        E.dof_deldop += F.dof;
+    }
+    E.setrecs.push_back(shape::SetRec{0, d.frame0, nframes});
+    E.dd.push_back(d);
+    E.finalized = false;
+    return (int)E.setrecs.size() - 1;
+}
+
+int shape_engine_add_lghtcrv_set(shape_engine *h, const shape_lghtcrv_set *set,
+                                 const shape_lghtcrv_point *points)
+{
+    if (!h || !set || !points || set->ncalc < 1 || set->n < 1 || !set->x || !set->t || !set->obs ||
+        !set->oneovervar)
+        return shape::set_err(SHAPE_E_ARG, "add_lghtcrv_set: invalid argument");
+    EngineImpl &E = h->impl;
+    shape::LcSetHost L;
+    L.set = *set;
+    L.pt0 = (int)E.points.size();
+    L.npts = set->ncalc;
+    L.x.assign(set->x, set->x + set->ncalc);
+    L.t.assign(set->t, set->t + set->n);
+    L.obs.assign(set->obs, set->obs + set->n);
+    L.oov.assign(set->oneovervar, set->oneovervar + set->n);
+    L.set.x = L.set.t = L.set.obs = L.set.oneovervar = nullptr;
+    for (int k = 0; k < set->ncalc; k++) {
+        if (points[k].pos_n < 1 || !(points[k].km_per_pixel > 0))
+            return shape::set_err(SHAPE_E_ARG, "add_lghtcrv_set: bad point size");
+        E.points.push_back(points[k]);
+    }
+    E.dof += set->dof;
+    E.dof_lghtcrv += set->dof;
+    E.setrecs.push_back(shape::SetRec{1, (int)E.lc.size(), 1});
+    E.lc.push_back(std::move(L));
+    E.finalized = false;
+    return (int)E.setrecs.size() - 1;
+}
+
+int shape_engine_finalize(shape_engine *h)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "null engine");
+    cudaSetDevice(h->impl.device);
+    return h->impl.finalize();
+}
+
+int shape_engine_set_scale(shape_engine *h, int j, double value)
+{
+    if (!h || j < 0 || j > 2) return shape::set_err(SHAPE_E_ARG, "set_scale: bad index");
+    h->impl.scale[j] = value;
+    return SHAPE_OK;
+}
+
+int shape_engine_set_vertex_r(shape_engine *h, int i, double value)
+{
+    if (!h || i < 0 || i >= h->impl.nv) return shape::set_err(SHAPE_E_ARG, "set_vertex_r: bad index");
+    h->impl.r[i] = value;
+    return SHAPE_OK;
+}
+
+int shape_engine_get_vertex_r(shape_engine *h, int i, double *value)
+{
+    if (!h || !value || i < 0 || i >= h->impl.nv) return shape::set_err(SHAPE_E_ARG, "get_vertex_r: bad index");
+    *value = h->impl.r[i];
+    return SHAPE_OK;
+}
+
+int shape_engine_evaluate(shape_engine *h, int form, shape_eval_summary *out)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "null engine");
+    cudaSetDevice(h->impl.device);
+    return h->impl.evaluate(form, out);
+}
+
+int shape_engine_get_deldop_results(shape_engine *h, shape_deldop_result *out, int max)
+{
+    if (!h || !out) return shape::set_err(SHAPE_E_ARG, "null argument");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0) return shape::set_err(SHAPE_E_STATE, "no evaluation yet");
+    int n = std::min<int>(max, (int)E.fh.size());
+    if (n > 0) {
+        cudaError_t e = cudaMemcpy(out, E.d_results, sizeof(shape_deldop_result) * n, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
+    }
+    return n;
+}
+
+int shape_engine_get_fit(shape_engine *h, int frame, double *fit)
+{
+    if (!h || !fit) return shape::set_err(SHAPE_E_ARG, "null argument");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0) return shape::set_err(SHAPE_E_STATE, "no evaluation yet");
+    if (frame < 0 || frame >= (int)E.frames.size()) return shape::set_err(SHAPE_E_ARG, "bad frame");
+    size_t D = (size_t)E.frames[frame].ndel * E.frames[frame].ndop;
+    long long off = E.frame_off[frame];
+    cudaError_t e;
+    if (E.last_form == SHAPE_FORM_BATCHED_FP32) {
+        std::vector<float> tmp(D);
+        e = cudaMemcpy(tmp.data(), E.d_fit32 + off, sizeof(float) * D, cudaMemcpyDeviceToHost);
+        for (size_t k = 0; k < D; k++) fit[k] = tmp[k];
+    } else {
+        e = cudaMemcpy(fit, E.d_fit64 + off, sizeof(double) * D, cudaMemcpyDeviceToHost);
+    }
+    if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
+    return SHAPE_OK;
+}
+
+int shape_engine_keep_pos(shape_engine *h, int keep)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "null engine");
+    h->impl.keep_pos = keep ? 1 : 0;
+    return SHAPE_OK;
+}
+
+static int copy_pos(EngineImpl &E, int view, double *z, double *cose, double *cosi, int *facet)
+{
+    const shape::FrameGeom &g = E.geoms[view];
+    size_t np = (size_t)g.side * g.side;
+    bool f32 = (E.last_form == SHAPE_FORM_BATCHED_FP32);
+    double *bufs[3] = {z, cose, cosi};
+    void *src[3] = {E.d_pos_z, E.d_pos_cose, E.d_pos_cosi};
+    for (int k = 0; k < 3; k++) {
+        if (!bufs[k]) continue;
+        cudaError_t e;
+        if (f32) {
+            std::vector<float> tmp(np);
+            e = cudaMemcpy(tmp.data(), (float *)src[k] + g.pos_base, sizeof(float) * np, cudaMemcpyDeviceToHost);
+            for (size_t i = 0; i < np; i++) bufs[k][i] = tmp[i];
+        } else {
+            e = cudaMemcpy(bufs[k], (double *)src[k] + g.pos_base, sizeof(double) * np, cudaMemcpyDeviceToHost);
+        }
+        if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
+    }
+    if (facet) {
+        cudaError_t e = cudaMemcpy(facet, E.d_pos_f + g.pos_base, sizeof(int) * np, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
+    }
+    return SHAPE_OK;
+}
+
+int shape_engine_get_pos(shape_engine *h, int frame, double *z, double *cose, int *facet)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "null engine");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0) return shape::set_err(SHAPE_E_STATE, "no evaluation yet");
+    if (frame < 0 || frame >= (int)E.frames.size()) return shape::set_err(SHAPE_E_ARG, "bad frame");
+    if (!E.keep_pos) return shape::set_err(SHAPE_E_STATE, "POS maps not kept (shape_engine_keep_pos)");
+    return copy_pos(E, E.frame_view[frame], z, cose, nullptr, facet);
+}
+
+int shape_engine_get_lghtcrv_pos(shape_engine *h, int set, int point, double *z, double *cose,
+                                 double *cosi, int *facet, double *zill, int *fill)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "null engine");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0) return shape::set_err(SHAPE_E_STATE, "no evaluation yet");
+    if (set < 0 || set >= (int)E.setrecs.size() || E.setrecs[set].type != 1)
+        return shape::set_err(SHAPE_E_ARG, "bad lightcurve set");
+    const shape::LcSetHost &L = E.lc[E.setrecs[set].first];
+    if (point < 0 || point >= L.npts) return shape::set_err(SHAPE_E_ARG, "bad point");
+    const shape::LcPointDev &P = E.lcpts[L.pt0 + point];
+    int rc = copy_pos(E, P.obs_view, z, cose, cosi, facet);
+    if (rc) return rc;
+    return copy_pos(E, P.sun_view, zill, nullptr, nullptr, fill);
+}
+
+int shape_engine_get_lghtcrv(shape_engine *h, int set, double *y, double *fit, double *cal, double *chi2)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "null engine");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0) return shape::set_err(SHAPE_E_STATE, "no evaluation yet");
+    if (set < 0 || set >= (int)E.setrecs.size() || E.setrecs[set].type != 1)
+        return shape::set_err(SHAPE_E_ARG, "bad lightcurve set");
+    int k = E.setrecs[set].first;
+    const shape::LcSetDev &L = E.lcdev[k];
+    cudaError_t e = cudaSuccess;
+    if (y) e = cudaMemcpy(y, L.y, sizeof(double) * L.npts, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && fit) e = cudaMemcpy(fit, L.fit, sizeof(double) * L.n, cudaMemcpyDeviceToHost);
+    double o[4];
+    if (e == cudaSuccess) e = cudaMemcpy(o, E.d_lc_out + 4 * k, sizeof o, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
+    if (cal) *cal = o[0];
+    if (chi2) *chi2 = o[1];
+    return SHAPE_OK;
+}
+
+int shape_engine_get_seen(shape_engine *h, unsigned char *seen)
+{
+    if (!h || !seen) return shape::set_err(SHAPE_E_ARG, "null argument");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0) return shape::set_err(SHAPE_E_STATE, "no evaluation yet");
+    cudaError_t e = cudaMemcpy(seen, E.d_seen, E.nf, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
+    return SHAPE_OK;
+}
+
+int shape_engine_get_realized(shape_engine *h, double *x, double *vn, double *fn, double *area)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "null engine");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0) return shape::set_err(SHAPE_E_STATE, "no evaluation yet");
+    std::vector<double4> tmp(std::max(E.nv, E.nf));
+    cudaError_t e = cudaSuccess;
+    if (x) {
+        e = cudaMemcpy(tmp.data(), E.md.vx, sizeof(double4) * E.nv, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < E.nv; i++) { x[3 * i] = tmp[i].x; x[3 * i + 1] = tmp[i].y; x[3 * i + 2] = tmp[i].z; }
+    }
+    if (e == cudaSuccess && vn) {
+        e = cudaMemcpy(tmp.data(), E.md.vn, sizeof(double4) * E.nv, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < E.nv; i++) { vn[3 * i] = tmp[i].x; vn[3 * i + 1] = tmp[i].y; vn[3 * i + 2] = tmp[i].z; }
+    }
+    if (e == cudaSuccess && fn) {
+        e = cudaMemcpy(tmp.data(), E.md.fn, sizeof(double4) * E.nf, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < E.nf; i++) { fn[3 * i] = tmp[i].x; fn[3 * i + 1] = tmp[i].y; fn[3 * i + 2] = tmp[i].z; }
+    }
+    if (e == cudaSuccess && area) e = cudaMemcpy(area, E.md.area, sizeof(double) * E.nf, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
+    return SHAPE_OK;
+}
+
+int shape_engine_last_time_ms(shape_engine *h, double *ms)
+{
+    if (!h || !ms) return shape::set_err(SHAPE_E_ARG, "null argument");
+    *ms = h->impl.last_ms;
+    return SHAPE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,151 @@
+// Kernel launchers of the SHAPE B200 engine (implemented in core.cu,
+// raster_f64.cu, raster_f32.cu). All launches take the engine stream.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "engine_internal.h"
+#include "shape_b200.h"
+
+namespace shape {
+
+struct ModelDev {
+    int nv, nf;
+    const double *a, *u, *r, *scale;   // a,u: [nv*3]
+    const int *fv;                     // [nf*3]
+    const int *af_ptr, *af_idx;
+    double4 *vx, *vn, *fn;             // realized
+    double *area;
+    int4 *fvi;                         // corner indices, padded
+};
+
+struct RasterArgs {
+    const FrameGeom *geoms;
+    const int2 *work;          // (view, tile) items
+    int nwork;
+    const void *vt;            // T4 transformed vertices
+    const int4 *fvi;
+    const double4 *vn;
+    const double4 *fn;
+    int nf;
+    const int *bin_count;
+    const int *bin_ids;
+    int cap;
+    FrameState *states;
+    const RadarLawDev *laws;
+    void *fit;                 // T image arena (radar views)
+    void *pos_z, *pos_cose, *pos_cosi;  // T POS maps (keep_pos or lightcurves)
+    int *pos_f;
+    unsigned char *seen;
+    double mincosine_seen;
+    int mark_seen;
+    int keep_pos;
+};
+
+// core.cu (FP64, no FMA contraction)
+void launch_realize(const ModelDev &m, cudaStream_t s);
+void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, cudaStream_t s);
+void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt,
+                      cudaStream_t s);
+void launch_xform_f32(const FrameGeom *g, int nviews, const double4 *vx, int nv, float4 *vt,
+                      cudaStream_t s);
+void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const double4 *vt,
+                    FrameState *st, int *bin_count, int *bin_ids, int cap, cudaStream_t s);
+void launch_bin_f32(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const float4 *vt,
+                    FrameState *st, int *bin_count, int *bin_ids, int cap, cudaStream_t s);
+
+struct Chi2Item { int frame; int start; int count; };
+struct Chi2Args {
+    const Chi2Item *items;
+    int nitems;
+    const double *obs, *oov;
+    const void *fit;             // double or float
+    const FrameGeom *geoms;      // radar views (for fit_base)
+    const int *frame_view;       // global deldop frame -> view index
+    double *partials;            // [nitems * 6]: o2, m2, om + compensations
+};
+void launch_chi2_partials(const Chi2Args &a, int fp32, cudaStream_t s);
+
+struct FrameHost {             // per deldop frame constants for finalize
+    double weight, dof, cal_in;
+    int cal_floating, badradar;
+    double badradar_logfactor;
+    int view;
+    int set;
+    int item0, nitems;
+};
+struct FinalizeArgs {
+    int nframes;
+    const FrameHost *fh;
+    const FrameGeom *geoms;
+    const FrameState *states;
+    const double *partials;
+    shape_deldop_result *results;
+    const double *set_delpp, *set_doppp;     // per set del/dop per pixel
+    const double *dop_extra;                 // per frame
+};
+void launch_finalize_frames(const FinalizeArgs &a, cudaStream_t s);
+
+struct LcArgs {
+    int npoints;
+    const LcPointDev *pts;
+    const FrameGeom *geoms;
+    const FrameState *states;
+    const int2 *items;          // (point, pixel start) work items
+    int nitems;
+    int chunk;                  // pixels per item
+    const void *z, *cosi, *zill;  // T POS maps
+    void *cose;                 // masked in place, as posmask does
+    const int *f, *fill;
+    double *partials;           // brightness partial per item
+    unsigned char *seen;
+    double mincosine_seen;
+    int mark_seen;
+};
+void launch_lc_photo(const LcArgs &a, int fp32, cudaStream_t s);
+
+struct LcSetDev {
+    int npts, n;                // calc points, observed points
+    int pt0;                    // first calc point (global)
+    int item0, nitems;          // photo items of this set's points are contiguous
+    const double *x, *t, *obs, *oov;  // device arrays
+    double *y, *y2, *fit;       // device outputs
+    double weight, dof, cal_in;
+    int cal_floating;
+};
+struct LcFinalizeArgs {
+    int nsets;
+    const LcSetDev *sets;
+    const LcPointDev *pts;
+    const FrameGeom *geoms;
+    const FrameState *states;
+    const int *pt_items;        // per point: first item, count (2 ints)
+    const double *partials;
+    double *set_out;            // per set: cal, chi2, posbnd flag, logfactor sum
+};
+void launch_lc_finalize(const LcFinalizeArgs &a, cudaStream_t s);
+
+struct SetRec { int type; int first; int count; };   // type 0 deldop (frames), 1 lightcurve (set index)
+struct SummaryArgs {
+    int nsets;
+    const SetRec *sets;
+    const FrameHost *fh;
+    const shape_deldop_result *results;
+    const double *lc_out;       // per lightcurve set: cal, chi2, posbnd, logfactor sum
+    const double *lc_dof;
+    const double *lc_npts;
+    double dof, dof_deldop;
+    double bad_objfactor;
+    int baddiam;
+    double baddiam_logfactor;
+    shape_eval_summary *out;
+};
+void launch_summary(const SummaryArgs &a, cudaStream_t s);
+
+// raster_f64.cu / raster_f32.cu
+void launch_raster_f64(const RasterArgs &a, cudaStream_t s);
+void launch_raster_f32(const RasterArgs &a, cudaStream_t s);
+cudaError_t configure_raster_f64();
+cudaError_t configure_raster_f32();
+
+}  // namespace shape

@@ -1,0 +1,255 @@
+"""ctypes binding of libshape_b200.so (C ABI: include/shape_b200.h).
+
+The library is built in-tree by shape-cuda-v1.2_b200/build.py. Loading fails
+loudly when it is missing: there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import ctypes_defs as cd
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(os.path.dirname(HERE))
+LIB_PATH = os.path.join(PKG, "lib", "libshape_b200.so")
+
+FORM_PLAIN_FP64 = 0
+FORM_BATCHED_FP64 = 1
+FORM_BATCHED_FP32 = 2
+FORMS = {"plain_fp64": 0, "batched_fp64": 1, "batched_fp32": 2}
+
+
+class EvalSummary(C.Structure):
+    _fields_ = [("chi2", C.c_double), ("dof", C.c_double), ("chi2_deldop", C.c_double),
+                ("chi2_lghtcrv", C.c_double), ("posbnd", C.c_int), ("posbnd_logfactor", C.c_double),
+                ("badradar", C.c_int), ("badradar_logfactor", C.c_double), ("objective", C.c_double)]
+
+
+ABI_ORDER = ["shape_model_desc", "shape_radar_law", "shape_optical_law", "shape_eval_params",
+             "shape_deldop_frame", "shape_deldop_set", "shape_lghtcrv_point", "shape_lghtcrv_set",
+             "shape_deldop_result"]
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load the engine library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("libshape_b200.so not found at %s: run shape-cuda-v1.2_b200/build.py" % path)
+    L = C.CDLL(path)
+    P = C.POINTER
+    vp = C.c_void_p
+    L.shape_last_error.restype = C.c_char_p
+    L.shape_version.restype = C.c_char_p
+    L.shape_abi_sizes.argtypes = [P(C.c_size_t), C.c_int]
+    L.shape_engine_create.argtypes = [C.c_int, P(vp)]
+    L.shape_engine_destroy.argtypes = [vp]
+    L.shape_engine_set_model.argtypes = [vp, P(cd.ModelDesc)]
+    L.shape_engine_set_params.argtypes = [vp, P(cd.EvalParams)]
+    L.shape_engine_add_deldop_set.argtypes = [vp, P(cd.DeldopSet), C.c_int, P(cd.DeldopFrame),
+                                              cd.dptr, cd.dptr]
+    L.shape_engine_add_lghtcrv_set.argtypes = [vp, P(cd.LghtcrvSet), P(cd.LghtcrvPoint)]
+    L.shape_engine_finalize.argtypes = [vp]
+    L.shape_engine_set_scale.argtypes = [vp, C.c_int, C.c_double]
+    L.shape_engine_set_vertex_r.argtypes = [vp, C.c_int, C.c_double]
+    L.shape_engine_get_vertex_r.argtypes = [vp, C.c_int, P(C.c_double)]
+    L.shape_engine_evaluate.argtypes = [vp, C.c_int, P(EvalSummary)]
+    L.shape_engine_get_deldop_results.argtypes = [vp, P(cd.DeldopResult), C.c_int]
+    L.shape_engine_get_fit.argtypes = [vp, C.c_int, cd.dptr]
+    L.shape_engine_keep_pos.argtypes = [vp, C.c_int]
+    L.shape_engine_get_pos.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.iptr]
+    L.shape_engine_get_lghtcrv_pos.argtypes = [vp, C.c_int, C.c_int, cd.dptr, cd.dptr, cd.dptr,
+                                               cd.iptr, cd.dptr, cd.iptr]
+    L.shape_engine_get_lghtcrv.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, P(C.c_double), P(C.c_double)]
+    L.shape_engine_get_seen.argtypes = [vp, C.c_char_p]
+    L.shape_engine_get_realized.argtypes = [vp, cd.dptr, cd.dptr, cd.dptr, cd.dptr]
+    L.shape_engine_last_time_ms.argtypes = [vp, P(C.c_double)]
+    _lib = L
+    return L
+
+
+def abi_sizes():
+    L = load_library()
+    out = (C.c_size_t * 16)()
+    n = L.shape_abi_sizes(out, 16)
+    return [out[i] for i in range(n)]
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+def _chk(rc):
+    if rc < 0:
+        raise EngineError("shape engine error %d: %s" % (rc, load_library().shape_last_error().decode()))
+    return rc
+
+
+def _summary_dict(s):
+    return {k: getattr(s, k) for k, _ in EvalSummary._fields_}
+
+
+class Engine:
+    """One engine handle: device-resident model and datasets."""
+
+    def __init__(self, device=0):
+        self.L = load_library()
+        h = C.c_void_p()
+        _chk(self.L.shape_engine_create(device, C.byref(h)))
+        self.h = h
+        self.deldops, self.lghtcrvs, self.set_index = [], [], []
+        self.model = None
+        self._keep = []
+
+    def close(self):
+        if self.h:
+            self.L.shape_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_model(self, model):
+        self.model = model
+        d = model.desc()
+        self._keep.append(d)
+        _chk(self.L.shape_engine_set_model(self.h, C.byref(d)))
+
+    def set_params(self, params):
+        _chk(self.L.shape_engine_set_params(self.h, C.byref(params)))
+
+    def add_deldop(self, ds):
+        arr = ds.frame_array()
+        self._keep.append(arr)
+        idx = _chk(self.L.shape_engine_add_deldop_set(self.h, C.byref(ds.set), ds.nframes, arr,
+                                                      cd.as_dptr(ds.obs), cd.as_dptr(ds.oneovervar)))
+        self.deldops.append(ds)
+        self.set_index.append(("deldop", len(self.deldops) - 1))
+        return idx
+
+    def add_lghtcrv(self, ds):
+        arr = ds.point_array()
+        self._keep.append(arr)
+        idx = _chk(self.L.shape_engine_add_lghtcrv_set(self.h, C.byref(ds.bind()), arr))
+        self.lghtcrvs.append(ds)
+        self.set_index.append(("lghtcrv", len(self.lghtcrvs) - 1))
+        return idx
+
+    def finalize(self):
+        _chk(self.L.shape_engine_finalize(self.h))
+
+    def keep_pos(self, keep=True):
+        _chk(self.L.shape_engine_keep_pos(self.h, 1 if keep else 0))
+
+    def set_scale(self, j, v):
+        _chk(self.L.shape_engine_set_scale(self.h, j, float(v)))
+
+    def set_vertex_r(self, i, v):
+        _chk(self.L.shape_engine_set_vertex_r(self.h, i, float(v)))
+
+    def evaluate(self, form=FORM_PLAIN_FP64):
+        if isinstance(form, str):
+            form = FORMS[form]
+        s = EvalSummary()
+        _chk(self.L.shape_engine_evaluate(self.h, form, C.byref(s)))
+        return _summary_dict(s)
+
+    def last_ms(self):
+        v = C.c_double()
+        _chk(self.L.shape_engine_last_time_ms(self.h, C.byref(v)))
+        return v.value
+
+    @property
+    def frames(self):
+        out = []
+        for ds in self.deldops:
+            out.extend(ds.frames)
+        return out
+
+    def results(self):
+        nfr = len(self.frames)
+        arr = (cd.DeldopResult * max(1, nfr))()
+        n = _chk(self.L.shape_engine_get_deldop_results(self.h, arr, nfr))
+        return [cd.result_to_dict(arr[i]) for i in range(n)]
+
+    def fit(self, frame):
+        fr = self.frames[frame]
+        out = np.zeros(fr.ndel * fr.ndop)
+        _chk(self.L.shape_engine_get_fit(self.h, frame, cd.as_dptr(out)))
+        return out
+
+    def pos(self, frame):
+        fr = self.frames[frame]
+        side = 2 * fr.pos_n + 1
+        z = np.zeros(side * side); cose = np.zeros(side * side)
+        f = np.zeros(side * side, dtype=np.int32)
+        _chk(self.L.shape_engine_get_pos(self.h, frame, cd.as_dptr(z), cd.as_dptr(cose), cd.as_iptr(f)))
+        return {"z": z, "cose": cose, "f": f}
+
+    def lghtcrv_pos(self, set_idx, point, pt):
+        side = 2 * pt.pos_n + 1
+        np_ = side * side
+        z, cose, cosi, zill = (np.zeros(np_) for _ in range(4))
+        f = np.zeros(np_, dtype=np.int32); fill = np.zeros(np_, dtype=np.int32)
+        _chk(self.L.shape_engine_get_lghtcrv_pos(self.h, set_idx, point, cd.as_dptr(z), cd.as_dptr(cose),
+                                                 cd.as_dptr(cosi), cd.as_iptr(f), cd.as_dptr(zill),
+                                                 cd.as_iptr(fill)))
+        return {"z": z, "cose": cose, "cosi": cosi, "f": f, "zill": zill, "fill": fill}
+
+    def lghtcrv(self, set_idx, ds):
+        y = np.zeros(ds.set.ncalc); fit = np.zeros(ds.set.n)
+        cal, chi2 = C.c_double(), C.c_double()
+        _chk(self.L.shape_engine_get_lghtcrv(self.h, set_idx, cd.as_dptr(y), cd.as_dptr(fit),
+                                             C.byref(cal), C.byref(chi2)))
+        return {"y": y, "fit": fit, "cal": cal.value, "chi2": chi2.value}
+
+    def seen(self):
+        buf = C.create_string_buffer(self.model.nf)
+        _chk(self.L.shape_engine_get_seen(self.h, buf))
+        return np.frombuffer(buf.raw, dtype=np.uint8).copy()
+
+    def realized(self):
+        m = self.model
+        x = np.zeros((m.nv, 3)); vn = np.zeros((m.nv, 3))
+        fn = np.zeros((m.nf, 3)); area = np.zeros(m.nf)
+        _chk(self.L.shape_engine_get_realized(self.h, cd.as_dptr(x), cd.as_dptr(vn), cd.as_dptr(fn),
+                                              cd.as_dptr(area)))
+        return {"x": x, "vn": vn, "fn": fn, "area": area}
+
+
+def make_engine(model, params, deldops=(), lghtcrvs=(), device=0):
+    e = Engine(device)
+    e.set_model(model)
+    e.set_params(params)
+    for ds in deldops:
+        e.add_deldop(ds)
+    for ds in lghtcrvs:
+        e.add_lghtcrv(ds)
+    e.finalize()
+    return e
+
+
+def engine_synthesizer(model, device=0):
+    """A ``synthesize`` callable for synth.* that evaluates the true model
+    with the engine's FP64 path (used to build observed images on a GPU)."""
+    def deldop(ds, params):
+        e = make_engine(model, params, deldops=[ds], device=device)
+        e.evaluate(FORM_PLAIN_FP64)
+        fits = [e.fit(k) for k in range(ds.nframes)]
+        e.close()
+        return fits
+
+    def lghtcrv(ds, params):
+        e = make_engine(model, params, lghtcrvs=[ds], device=device)
+        e.evaluate(FORM_PLAIN_FP64)
+        y = e.lghtcrv(0, ds)["y"]
+        e.close()
+        return y
+    return deldop, lghtcrv
