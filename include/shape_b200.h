@@ -117,6 +117,14 @@ int shape_engine_get_seen(shape_engine *e, unsigned char *seen);
 int shape_engine_get_realized(shape_engine *e, double *x, double *vn, double *fn,
                               double *area);
 
+/* Runs one evaluation of a batched form without its graph, with CUDA events
+ * between stages, and writes the stage times in ms: [0] realize, [1] state
+ * reset and image clears, [2] view transforms, [3] facet binning,
+ * [4] tile raster + delay-Doppler synthesis, [5] chi-square partials,
+ * [6] lightcurve shadowing + photometry, [7] finalize + summary.
+ * Returns the number of stages written. */
+int shape_engine_stage_times(shape_engine *e, int form, double *ms, int max);
+
 /* Device time of the last evaluation (CUDA events on the engine stream). */
 int shape_engine_last_time_ms(shape_engine *e, double *ms);
 

@@ -205,7 +205,7 @@ struct EngineImpl {
     }
 
     int finalize();
-    int enqueue(int form);
+    int enqueue(int form, cudaEvent_t *marks = nullptr);
     int evaluate(int form, shape_eval_summary *out);
     void fill_params(double *dst) const
     {
@@ -538,17 +538,23 @@ int EngineImpl::finalize()
 }
 
 // Enqueue one evaluation (without the H2D of parameters / D2H of the summary).
-int EngineImpl::enqueue(int form)
+// marks (optional, batched forms only): events recorded after each stage
+// 0 realize, 1 reset, 2 transform, 3 bin, 4 raster, 5 chi2, 6 lightcurve
+// photometry, 7 finalize + summary.
+int EngineImpl::enqueue(int form, cudaEvent_t *marks)
 {
     cudaStream_t s = stream;
     const bool f32 = (form == SHAPE_FORM_BATCHED_FP32);
+    auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], s); };
     launch_realize(md, s);
+    mark(0);
     launch_reset_state(d_states, nviews, d_bin_count, ntiles, s);
     if (fit_elems) {
         if (f32) CK(cudaMemsetAsync(d_fit32, 0, sizeof(float) * fit_elems, s));
         else CK(cudaMemsetAsync(d_fit64, 0, sizeof(double) * fit_elems, s));
     }
     CK(cudaMemsetAsync(d_seen, 0, nf, s));
+    mark(1);
 
     RasterArgs ra;
     memset(&ra, 0, sizeof ra);
@@ -615,26 +621,28 @@ int EngineImpl::enqueue(int form)
             }
         }
     } else {
-        if (f32) {
-            launch_xform_f32(d_geoms, nviews, md.vx, nv, d_vt32, s);
-            launch_bin_f32(d_geoms, 0, nviews, md, d_vt32, d_states, d_bin_count, d_bin_ids, cap, s);
-        } else {
-            launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
-            launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
-        }
+        if (f32) launch_xform_f32(d_geoms, nviews, md.vx, nv, d_vt32, s);
+        else launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
+        mark(2);
+        if (f32) launch_bin_f32(d_geoms, 0, nviews, md, d_vt32, d_states, d_bin_count, d_bin_ids, cap, s);
+        else launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
+        mark(3);
         ra.work = d_work;
         ra.nwork = (int)work.size();
         if (f32) launch_raster_f32(ra, s); else launch_raster_f64(ra, s);
+        mark(4);
         if (!chi2_items.empty()) {
             ca.items = d_chi2_items;
             ca.nitems = (int)chi2_items.size();
             launch_chi2_partials(ca, f32 ? 1 : 0, s);
         }
+        mark(5);
         if (!lc_items.empty()) {
             la.items = d_lc_items;
             la.nitems = (int)lc_items.size();
             launch_lc_photo(la, f32 ? 1 : 0, s);
         }
+        mark(6);
     }
     if (!fh.empty()) {
         FinalizeArgs fa;
@@ -664,6 +672,7 @@ int EngineImpl::enqueue(int form)
     sa.baddiam_logfactor = 0.0;
     sa.out = d_summary;
     launch_summary(sa, s);
+    mark(7);
     CK(cudaGetLastError());
     return SHAPE_OK;
 }
@@ -1047,6 +1056,36 @@ int shape_engine_get_realized(shape_engine *h, double *x, double *vn, double *fn
     if (e == cudaSuccess && area) e = cudaMemcpy(area, E.md.area, sizeof(double) * E.nf, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
     return SHAPE_OK;
+}
+
+int shape_engine_stage_times(shape_engine *h, int form, double *ms, int max)
+{
+    if (!h || !ms) return shape::set_err(SHAPE_E_ARG, "null argument");
+    EngineImpl &E = h->impl;
+    if (!E.finalized) return shape::set_err(SHAPE_E_STATE, "stage_times before finalize");
+    if (form != SHAPE_FORM_BATCHED_FP64 && form != SHAPE_FORM_BATCHED_FP32)
+        return shape::set_err(SHAPE_E_ARG, "stage_times: batched forms only");
+    cudaSetDevice(E.device);
+    cudaEvent_t ev[9];
+    for (auto &x : ev) cudaEventCreate(&x);
+    E.fill_params(E.h_params);
+    cudaMemcpyAsync(E.d_r, E.h_params, sizeof(double) * (E.nv + 3), cudaMemcpyHostToDevice, E.stream);
+    cudaEventRecord(ev[0], E.stream);
+    int rc = E.enqueue(form, ev + 1);
+    cudaError_t ce = cudaStreamSynchronize(E.stream);
+    int n = 0;
+    if (rc == SHAPE_OK && ce == cudaSuccess) {
+        for (int k = 0; k < 8 && k < max; k++, n++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+            ms[k] = t;
+        }
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(ce));
+    E.last_form = form;
+    return n;
 }
 
 int shape_engine_last_time_ms(shape_engine *h, double *ms)

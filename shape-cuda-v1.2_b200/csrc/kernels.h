@@ -40,6 +40,7 @@ struct RasterArgs {
     double mincosine_seen;
     int mark_seen;
     int keep_pos;
+    size_t smem_bytes;         // dynamic shared memory of the raster CTA (set by the launcher)
 };
 
 // core.cu (FP64, no FMA contraction)

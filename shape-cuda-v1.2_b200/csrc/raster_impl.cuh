@@ -173,34 +173,55 @@ struct PixLimits {
     double dmin, dmax, pmin, pmax;
 };
 
-// pos2deldop for one lit POS pixel (src/shape/pos2deldop.c:305-496).
+// Delay / Doppler position and footprint of one lit POS pixel
+// (src/shape/pos2deldop.c:318-367).
 template <typename T>
-__device__ void synth_pixel(const RasterArgs &a, const FrameGeom &g, int x, int y, T z, T cose,
-                            PixLimits &lim)
+struct PixDD {
+    T delPOS, dopPOS, codefactor;
+    int idel_min, idel_max, idop_min, idop_max;
+    bool ok;   // in_bounds: the whole footprint lies inside the frame
+};
+
+template <typename T>
+__device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, int x, int y, T z, PixLimits &lim)
 {
-    const T delPOS = z * (T)g.delfact + (T)g.delshift;
+    PixDD<T> d;
+    d.delPOS = z * (T)g.delfact + (T)g.delshift;
     const T const1 = (T)g.const1;
-    int idel_min = (int)floor(delPOS - const1) + 1;
-    int idel_max = (int)ceil(delPOS + const1) - 1;
-    const T dopPOS = (T)g.ax * (T)x + (T)g.ay * (T)y + (T)g.dopshift;
+    d.idel_min = (int)floor(d.delPOS - const1) + 1;
+    d.idel_max = (int)ceil(d.delPOS + const1) - 1;
+    d.dopPOS = (T)g.ax * (T)x + (T)g.ay * (T)y + (T)g.dopshift;
     const T dopdiff_max = (T)g.dopdiff_max;
     const T half_w = (T)(g.sinc2width / 2.0);
-    int idop_min = (int)floor(dopPOS - dopdiff_max + 1 - half_w);
-    int idop_max = (int)floor(dopPOS + dopdiff_max + half_w);
-    T codefactor = (g.codemethod == SHAPE_CODE_SHORT)
-                       ? sinc2<T>((dopPOS - (T)g.dopDC_vig) / (T)g.dopfftlen) : (T)1;
-    lim.idmin = min(lim.idmin, idel_min);
-    lim.idmax = max(lim.idmax, idel_max);
-    lim.ipmin = min(lim.ipmin, idop_min);
-    lim.ipmax = max(lim.ipmax, idop_max);
-    lim.dmin = fmin(lim.dmin, (double)delPOS);
-    lim.dmax = fmax(lim.dmax, (double)delPOS);
-    lim.pmin = fmin(lim.pmin, (double)dopPOS);
-    lim.pmax = fmax(lim.pmax, (double)dopPOS);
-    const int ndel = g.ndel, ndop = g.ndop;
-    bool in_bounds = (idel_min >= 1) && (idel_max <= ndel) && (idop_min >= 1) && (idop_max <= ndop);
-    if (!in_bounds || idel_max - idel_min + 1 > SHAPE_MAXBINS) return;
+    d.idop_min = (int)floor(d.dopPOS - dopdiff_max + 1 - half_w);
+    d.idop_max = (int)floor(d.dopPOS + dopdiff_max + half_w);
+    d.codefactor = (g.codemethod == SHAPE_CODE_SHORT)
+                       ? sinc2<T>((d.dopPOS - (T)g.dopDC_vig) / (T)g.dopfftlen) : (T)1;
+    lim.idmin = min(lim.idmin, d.idel_min);
+    lim.idmax = max(lim.idmax, d.idel_max);
+    lim.ipmin = min(lim.ipmin, d.idop_min);
+    lim.ipmax = max(lim.ipmax, d.idop_max);
+    lim.dmin = fmin(lim.dmin, (double)d.delPOS);
+    lim.dmax = fmax(lim.dmax, (double)d.delPOS);
+    lim.pmin = fmin(lim.pmin, (double)d.dopPOS);
+    lim.pmax = fmax(lim.pmax, (double)d.dopPOS);
+    d.ok = (d.idel_min >= 1) && (d.idel_max <= g.ndel) && (d.idop_min >= 1) && (d.idop_max <= g.ndop) &&
+           (d.idel_max - d.idel_min + 1 <= SHAPE_MAXBINS);
+    return d;
+}
 
+template <typename T> __device__ inline void atomic_add_any(T *p, T v) { atomicAdd(p, v); }
+
+// Delay and Doppler response of one pixel and its scatter into `dst`, an
+// image whose element (idel, idop) lives at dst[(idel - row0) * stride +
+// (idop - col0)] (src/shape/pos2deldop.c:371-496). dst is either the frame's
+// fit image in HBM or the tile's shared-memory accumulator.
+template <typename T>
+__device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, T cose, const PixDD<T> &d,
+                                 T *dst, int row0, int col0, int stride)
+{
+    const T delPOS = d.delPOS, dopPOS = d.dopPOS, const1 = (T)g.const1;
+    const int idel_min = d.idel_min, idel_max = d.idel_max, idop_min = d.idop_min, idop_max = d.idop_max;
     T del_c[SHAPE_MAXBINS];
     T dop_c[SHAPE_MAXBINS + 1];
     const int spb = g.spb;
@@ -259,13 +280,12 @@ __device__ void synth_pixel(const RasterArgs &a, const FrameGeom &g, int x, int 
         for (int idop = idop_min; idop <= idop_max; idop++)
             sumweights += del_c[idel - idel_min] * dop_c[min(idop - idop_min, SHAPE_MAXBINS)];
     const T kmpp = (T)g.kmpp;
-    T amp = radlaw_dev<T>(a.laws[g.law], cose) * kmpp * kmpp * codefactor / sumweights;
-    T *fit = static_cast<T *>(a.fit) + g.fit_base;
+    T amp = radlaw_dev<T>(a.laws[g.law], cose) * kmpp * kmpp * d.codefactor / sumweights;
     for (int idel = idel_min; idel <= idel_max; idel++) {
         T ad = amp * del_c[idel - idel_min];
-        T *row = fit + (long long)(idel - 1) * ndop - 1;
+        T *row = dst + (long long)(idel - row0) * stride - col0;
         for (int idop = idop_min; idop <= idop_max; idop++)
-            atomic_add_fit<T>(row + idop, ad * dop_c[min(idop - idop_min, SHAPE_MAXBINS)]);
+            atomic_add_any<T>(row + idop, ad * dop_c[min(idop - idop_min, SHAPE_MAXBINS)]);
     }
 }
 
@@ -301,6 +321,7 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
     __shared__ int s_red[RASTER_THREADS / 32][4];
     __shared__ double s_redd[RASTER_THREADS / 32][4];
     __shared__ int s_redl[RASTER_THREADS / 32][4];
+    __shared__ int s_box[RASTER_THREADS / 32][4];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
     for (int w = blockIdx.x; w < a.nwork; w += gridDim.x) {
@@ -435,12 +456,52 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
         PixLimits lim = {INT_MAX, INT_MIN, INT_MAX, INT_MIN,
                          SHAPE_HUGENUMBER, -SHAPE_HUGENUMBER, SHAPE_HUGENUMBER, -SHAPE_HUGENUMBER};
         bool lit = false;
+        PixDD<T> dd;
+        dd.ok = false;
         if (g.kind == VIEW_RADAR && covered) {
             if (a.mark_seen && (double)cosa > a.mincosine_seen)
                 a.seen[fac] = 1;
             if (cosa > (T)0) {
                 lit = true;
-                synth_pixel<T>(a, g, pi, pj, zz, cosa, lim);
+                dd = pixel_dd_setup<T>(g, pi, pj, zz, lim);
+            }
+        }
+        if (g.kind == VIEW_RADAR) {
+            // The tile's delay-Doppler footprint is accumulated in shared
+            // memory (reusing the bin / stage space, free after the replay)
+            // and flushed with one global atomic per touched bin; many pixels
+            // of a tile hit the same bins, so this removes most of the
+            // contended HBM/L2 atomics.
+            int b0 = dd.ok ? dd.idel_min : INT_MAX, b1 = dd.ok ? dd.idel_max : INT_MIN;
+            int b2 = dd.ok ? dd.idop_min : INT_MAX, b3 = dd.ok ? dd.idop_max : INT_MIN;
+            b0 = warp_min(b0); b1 = warp_max(b1); b2 = warp_min(b2); b3 = warp_max(b3);
+            if (lane == 0) { s_box[wid][0] = b0; s_box[wid][1] = b1; s_box[wid][2] = b2; s_box[wid][3] = b3; }
+            __syncthreads();
+            int r0 = INT_MAX, r1 = INT_MIN, c0 = INT_MAX, c1 = INT_MIN;
+            for (int ww = 0; ww < RASTER_THREADS / 32; ww++) {
+                r0 = min(r0, s_box[ww][0]); r1 = max(r1, s_box[ww][1]);
+                c0 = min(c0, s_box[ww][2]); c1 = max(c1, s_box[ww][3]);
+            }
+            T *fit = static_cast<T *>(a.fit) + g.fit_base;
+            if (r0 != INT_MAX) {
+                const int nr = r1 - r0 + 1, nc = c1 - c0 + 1;
+                const long long cells = (long long)nr * nc;
+                T *box = reinterpret_cast<T *>(smem);
+                if (cells <= (long long)(a.smem_bytes / sizeof(T))) {
+                    for (long long k = tid; k < cells; k += RASTER_THREADS) box[k] = (T)0;
+                    __syncthreads();
+                    if (dd.ok) pixel_dd_scatter<T>(a, g, cosa, dd, box, r0, c0, nc);
+                    __syncthreads();
+                    for (long long k = tid; k < cells; k += RASTER_THREADS) {
+                        T v = box[k];
+                        if (v != (T)0) {
+                            int rr = (int)(k / nc), cc = (int)(k % nc);
+                            atomic_add_any<T>(fit + (long long)(r0 + rr - 1) * g.ndop + (c0 + cc - 1), v);
+                        }
+                    }
+                } else if (dd.ok) {
+                    pixel_dd_scatter<T>(a, g, cosa, dd, fit, 1, 1, g.ndop);
+                }
             }
         }
         if (lane == 0) {
@@ -510,8 +571,9 @@ template <typename T>
 inline void launch_raster_t(const RasterArgs &a, cudaStream_t s)
 {
     if (a.nwork <= 0) return;
-    size_t smem = raster_smem_bytes<T>(a.cap);
-    k_raster<T><<<a.nwork, RASTER_THREADS, smem, s>>>(a);
+    RasterArgs b = a;
+    b.smem_bytes = raster_smem_bytes<T>(a.cap);
+    k_raster<T><<<a.nwork, RASTER_THREADS, b.smem_bytes, s>>>(b);
 }
 
 }  // namespace shape

@@ -68,6 +68,7 @@ def load_library(path=LIB_PATH):
     L.shape_engine_get_seen.argtypes = [vp, C.c_char_p]
     L.shape_engine_get_realized.argtypes = [vp, cd.dptr, cd.dptr, cd.dptr, cd.dptr]
     L.shape_engine_last_time_ms.argtypes = [vp, P(C.c_double)]
+    L.shape_engine_stage_times.argtypes = [vp, C.c_int, cd.dptr, C.c_int]
     _lib = L
     return L
 
@@ -165,6 +166,15 @@ class Engine:
         v = C.c_double()
         _chk(self.L.shape_engine_last_time_ms(self.h, C.byref(v)))
         return v.value
+
+    STAGES = ["realize", "reset", "transform", "bin", "raster_synth", "chi2", "lc_photo", "finalize"]
+
+    def stage_times(self, form=FORM_BATCHED_FP32):
+        if isinstance(form, str):
+            form = FORMS[form]
+        ms = np.zeros(8)
+        n = _chk(self.L.shape_engine_stage_times(self.h, form, cd.as_dptr(ms), 8))
+        return dict(zip(self.STAGES[:n], ms[:n].tolist()))
 
     @property
     def frames(self):
