@@ -125,6 +125,16 @@ int shape_engine_get_realized(shape_engine *e, double *x, double *vn, double *fn
  * Returns the number of stages written. */
 int shape_engine_stage_times(shape_engine *e, int form, double *ms, int max);
 
+/* Facet-bin capacity per 16x16 POS tile. 0 (default) lets finalize size it
+ * from a dry-run binning of the model (next power of two above 1.25x the
+ * fullest tile); tiles whose bin overflows are rasterized by an ordered scan
+ * of all facets, which is exact but slow. Takes effect at the next finalize. */
+int shape_engine_set_bin_capacity(shape_engine *e, int cap);
+/* Tuning state after finalize: [0] bin capacity, [1] largest tile count of
+ * the dry run, [2] non-empty tiles, [3] tiles, [4] tile width in pixels.
+ * Returns the number of values written. */
+int shape_engine_get_tuning(shape_engine *e, int *out, int max);
+
 /* Device time of the last evaluation (CUDA events on the engine stream). */
 int shape_engine_last_time_ms(shape_engine *e, double *ms);
 

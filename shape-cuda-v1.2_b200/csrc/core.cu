@@ -134,7 +134,7 @@ template <typename T4>
 __global__ void k_bin(const FrameGeom *__restrict__ geoms, int view0, int nf,
                       const int4 *__restrict__ fvi, const double4 *__restrict__ fn,
                       const T4 *__restrict__ vt, FrameState *__restrict__ states,
-                      int *__restrict__ bin_count, int *__restrict__ bin_ids, int cap)
+                      int *__restrict__ bin_count, int2 *__restrict__ bin_ids, int cap)
 {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nf) return;
@@ -181,10 +181,15 @@ __global__ void k_bin(const FrameGeom *__restrict__ geoms, int view0, int nf,
         for (int ty = ty0; ty <= ty1; ty++) {
             int tile = g.tile_base + tx * g.tiles_x + ty;
             int slot = atomicAdd(&bin_count[tile], 1);
-            if (slot < cap)
-                bin_ids[(size_t)tile * cap + slot] = f;
-            else
+            if (slot < cap) {
+                // bbox clipped to the tile, relative to its corner, 4 bits per bound
+                int ti0 = -n + tx * TILE_W, tj0 = -n + ty * TILE_W;
+                int ri1 = max(i1, ti0) - ti0, ri2 = min(i2, ti0 + TILE_W - 1) - ti0;
+                int rj1 = max(j1, tj0) - tj0, rj2 = min(j2, tj0 + TILE_W - 1) - tj0;
+                bin_ids[(size_t)tile * cap + slot] = make_int2(f, ri1 | (ri2 << 4) | (rj1 << 8) | (rj2 << 12));
+            } else {
                 st.bin_overflow = 1;
+            }
         }
 }
 
@@ -631,14 +636,14 @@ void launch_xform_f32(const FrameGeom *g, int nviews, const double4 *vx, int nv,
 }
 
 void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const double4 *vt,
-                    FrameState *st, int *bin_count, int *bin_ids, int cap, cudaStream_t s)
+                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s)
 {
     dim3 grid((m.nf + 255) / 256, nviews);
     k_bin<double4><<<grid, 256, 0, s>>>(g, view0, m.nf, m.fvi, m.fn, vt, st, bin_count, bin_ids, cap);
 }
 
 void launch_bin_f32(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const float4 *vt,
-                    FrameState *st, int *bin_count, int *bin_ids, int cap, cudaStream_t s)
+                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s)
 {
     dim3 grid((m.nf + 255) / 256, nviews);
     k_bin<float4><<<grid, 256, 0, s>>>(g, view0, m.nf, m.fvi, m.fn, vt, st, bin_count, bin_ids, cap);

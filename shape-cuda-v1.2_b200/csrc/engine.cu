@@ -84,6 +84,15 @@ struct DevMem {
         for (void *p : ptrs) cudaFree(p);
         ptrs.clear();
     }
+    void release_one(void *p)
+    {
+        for (auto it = ptrs.begin(); it != ptrs.end(); ++it)
+            if (*it == p) {
+                cudaFree(p);
+                ptrs.erase(it);
+                return;
+            }
+    }
 };
 
 struct DdSetHost {
@@ -149,7 +158,8 @@ struct EngineImpl {
     int2 *d_work = nullptr;
     double4 *d_vt64 = nullptr;
     float4 *d_vt32 = nullptr;
-    int *d_bin_count = nullptr, *d_bin_ids = nullptr;
+    int *d_bin_count = nullptr;
+    int2 *d_bin_ids = nullptr;
     double *d_obs = nullptr, *d_oov = nullptr;
     double *d_fit64 = nullptr;
     float *d_fit32 = nullptr;
@@ -205,7 +215,12 @@ struct EngineImpl {
     }
 
     int finalize();
+    int tune_bins();
     int enqueue(int form, cudaEvent_t *marks = nullptr);
+    // bin tuning results
+    int2 *d_work_sorted = nullptr;
+    int tuned_max_count = 0, tuned_nonempty = 0;
+    int fixed_cap = 0;            // > 0: bin capacity set by the caller, no autotuning
     int evaluate(int form, shape_eval_summary *out);
     void fill_params(double *dst) const
     {
@@ -248,6 +263,8 @@ int EngineImpl::finalize()
     if (dd.empty() && lc.empty()) return set_err(SHAPE_E_STATE, "finalize: no datasets");
     mem.release();
     invalidate_graphs();
+    d_work_sorted = nullptr;
+    cap = fixed_cap > 0 ? fixed_cap : 512;
     geoms.clear(); fh.clear(); work.clear(); view_work0.clear(); view_nwork.clear();
     chi2_items.clear(); frame_view.clear(); dop_extra.clear(); set_delpp.clear(); set_doppp.clear();
     lcpts.clear(); lc_items.clear(); pt_items.clear(); lcdev.clear();
@@ -533,7 +550,58 @@ int EngineImpl::finalize()
     md.nv = nv; md.nf = nf;
     md.a = d_a; md.u = d_u; md.r = d_r; md.scale = d_scale;
     md.fv = d_fv; md.af_ptr = d_afp; md.af_idx = d_afi;
+    rc = tune_bins();
+    if (rc) return rc;
     finalized = true;
+    return SHAPE_OK;
+}
+
+// Bin autotuning from a dry-run binning of the model as loaded: the bin
+// capacity becomes the next power of two above 1.25x the fullest tile (so a
+// fit's small model changes do not overflow into the full-scan path), and
+// the batched raster visits tiles in decreasing facet count, so the heavy
+// tiles start first instead of forming a tail.
+int EngineImpl::tune_bins()
+{
+    cudaStream_t s = stream;
+    fill_params(h_params);
+    CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s));
+    launch_realize(md, s);
+    launch_reset_state(d_states, nviews, d_bin_count, ntiles, s);
+    launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
+    launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
+    std::vector<int> counts(ntiles);
+    CK(cudaMemcpyAsync(counts.data(), d_bin_count, sizeof(int) * ntiles, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    int mx = 0, nonempty = 0;
+    for (int c : counts) { mx = std::max(mx, c); nonempty += (c > 0); }
+    tuned_max_count = mx;
+    tuned_nonempty = nonempty;
+    int want = 64;
+    while (want < (int)(1.25 * mx) + 16 && want < 8192) want *= 2;
+    if (fixed_cap > 0) want = fixed_cap;
+    if (want != cap) {
+        mem.release_one(d_bin_ids);
+        cap = want;
+        int rc = mem.alloc(&d_bin_ids, (size_t)ntiles * cap);
+        if (rc) return rc;
+    }
+    // work order for the batched forms: decreasing count, stable
+    std::vector<int> order(work.size());
+    for (size_t k = 0; k < work.size(); k++) order[k] = (int)k;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        int cx = counts[geoms[work[x].x].tile_base + work[x].y];
+        int cy = counts[geoms[work[y].x].tile_base + work[y].y];
+        return cx > cy;
+    });
+    std::vector<int2> sorted(work.size());
+    for (size_t k = 0; k < work.size(); k++) sorted[k] = work[order[k]];
+    if (!d_work_sorted) {
+        int rc = mem.alloc(&d_work_sorted, work.size());
+        if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(d_work_sorted, sorted.data(), sizeof(int2) * sorted.size(), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
     return SHAPE_OK;
 }
 
@@ -627,7 +695,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         if (f32) launch_bin_f32(d_geoms, 0, nviews, md, d_vt32, d_states, d_bin_count, d_bin_ids, cap, s);
         else launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
         mark(3);
-        ra.work = d_work;
+        ra.work = d_work_sorted;
         ra.nwork = (int)work.size();
         if (f32) launch_raster_f32(ra, s); else launch_raster_f64(ra, s);
         mark(4);
@@ -1085,6 +1153,25 @@ int shape_engine_stage_times(shape_engine *h, int form, double *ms, int max)
     if (rc) return rc;
     if (ce != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(ce));
     E.last_form = form;
+    return n;
+}
+
+int shape_engine_set_bin_capacity(shape_engine *h, int cap)
+{
+    if (!h || cap < 0 || cap > 65536) return shape::set_err(SHAPE_E_ARG, "set_bin_capacity: bad capacity");
+    h->impl.fixed_cap = cap;
+    h->impl.finalized = false;
+    return SHAPE_OK;
+}
+
+int shape_engine_get_tuning(shape_engine *h, int *out, int max)
+{
+    if (!h || !out) return shape::set_err(SHAPE_E_ARG, "null argument");
+    EngineImpl &E = h->impl;
+    if (!E.finalized) return shape::set_err(SHAPE_E_STATE, "get_tuning before finalize");
+    int v[5] = {E.cap, E.tuned_max_count, E.tuned_nonempty, E.ntiles, shape::TILE_W};
+    int n = 0;
+    for (; n < 5 && n < max; n++) out[n] = v[n];
     return n;
 }
 

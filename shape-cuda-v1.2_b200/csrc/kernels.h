@@ -29,7 +29,7 @@ struct RasterArgs {
     const double4 *fn;
     int nf;
     const int *bin_count;
-    const int *bin_ids;
+    const int2 *bin_ids;        // (facet, tile-relative bbox) entries
     int cap;
     FrameState *states;
     const RadarLawDev *laws;
@@ -51,9 +51,9 @@ void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv,
 void launch_xform_f32(const FrameGeom *g, int nviews, const double4 *vx, int nv, float4 *vt,
                       cudaStream_t s);
 void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const double4 *vt,
-                    FrameState *st, int *bin_count, int *bin_ids, int cap, cudaStream_t s);
+                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s);
 void launch_bin_f32(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const float4 *vt,
-                    FrameState *st, int *bin_count, int *bin_ids, int cap, cudaStream_t s);
+                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s);
 
 struct Chi2Item { int frame; int start; int count; };
 struct Chi2Args {

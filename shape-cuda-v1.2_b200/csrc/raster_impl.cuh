@@ -22,19 +22,19 @@
 
 #include "kernels.h"
 
+// Resident CTAs per SM the register allocation must allow (FP32 / FP64).
+#ifndef RASTER_MIN_BLOCKS
+#define RASTER_MIN_BLOCKS 3
+#endif
+#ifndef RASTER_MIN_BLOCKS_F64
+#define RASTER_MIN_BLOCKS_F64 3
+#endif
+
 namespace shape {
 
 template <typename T> struct Vec4;
 template <> struct Vec4<double> { using type = double4; };
 template <> struct Vec4<float> { using type = float4; };
-
-template <typename T>
-struct Stage {
-    T v00, v01, v02, A, B, C, D, E, F, den;
-    T nx, ny, nz;
-    int i1, i2, j1, j2;
-    int f, c0, c1, c2;
-};
 
 template <typename T> __device__ inline T tsin(T x);
 template <> __device__ inline double tsin<double>(double x) { return sin(x); }
@@ -111,9 +111,71 @@ template <typename T> __device__ T radlaw_dev(const RadarLawDev &L, T c)
     return v;
 }
 
-// Stage one facet for a view: culling, bbox and the per-facet terms of the
-// s, t, z expressions (src/shape/posvis.c:146-223). Returns false when the
-// facet faces away or misses the tile [ti0, ti1] x [tj0, tj1].
+// One staged facet of a tile (shared memory). bb packs the facet's pixel
+// bbox clipped to the tile and relative to its corner (4 bits per bound:
+// i1, i2, j1, j2); wmask has bit w set when the bbox meets warp w's 4x8
+// pixel block.
+template <typename T>
+struct Stage {
+    T v00, v01, v02, A, B, C, D, E, F, den;
+    T nx, ny, nz;        // facet normal in view coordinates (views without smoothing)
+    T q[9];              // body-frame vertex normals of the three corners (smoothing)
+    int bb, wmask, f;
+};
+
+// Warp w covers tile rows 4*(w>>1) .. +3 and columns 8*(w&1) .. +7.
+__device__ inline int warp_mask_of(int ri1, int ri2, int rj1, int rj2)
+{
+    int m = 0;
+#pragma unroll
+    for (int w = 0; w < RASTER_THREADS / 32; w++) {
+        int r0 = 4 * (w >> 1), c0 = 8 * (w & 1);
+        if (ri1 <= r0 + 3 && ri2 >= r0 && rj1 <= c0 + 7 && rj2 >= c0) m |= 1 << w;
+    }
+    return m;
+}
+
+// Facet terms of the s, t, z expressions (src/shape/posvis.c:210-228) and,
+// for views without smoothing, the facet normal in view coordinates
+// (src/shape/posvis.c:146-148).
+template <typename T>
+__device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage<T> &s)
+{
+    using T4 = typename Vec4<T>::type;
+    const T4 *vt = static_cast<const T4 *>(a.vt) + g.vt_base;
+    int4 c = a.fvi[f];
+    T4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
+    s.v00 = p0.x; s.v01 = p0.y; s.v02 = p0.z;
+    s.A = p2.y - p1.y;
+    s.B = p2.x - p1.x;
+    s.C = p1.x - p0.x;
+    s.D = p1.y - p0.y;
+    s.E = p1.z - p0.z;
+    s.F = p2.z - p1.z;
+    s.den = (T)1 / (s.C * s.A - s.B * s.D);
+    s.f = f;
+    if (g.smooth) {
+        double4 q0 = a.vn[c.x], q1 = a.vn[c.y], q2 = a.vn[c.z];
+        s.q[0] = (T)q0.x; s.q[1] = (T)q0.y; s.q[2] = (T)q0.z;
+        s.q[3] = (T)q1.x; s.q[4] = (T)q1.y; s.q[5] = (T)q1.z;
+        s.q[6] = (T)q2.x; s.q[7] = (T)q2.y; s.q[8] = (T)q2.z;
+    } else {
+        double4 nb = a.fn[f];
+        double nn[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            nn[r] = 0.0;
+            nn[r] += g.oa[3 * r + 0] * nb.x;
+            nn[r] += g.oa[3 * r + 1] * nb.y;
+            nn[r] += g.oa[3 * r + 2] * nb.z;
+        }
+        s.nx = (T)nn[0]; s.ny = (T)nn[1]; s.nz = (T)nn[2];
+    }
+}
+
+// Full staging of a facet that did not come from a bin (bin overflow path):
+// culling and bounding box as in posvis (src/shape/posvis.c:146-199).
+// Returns false when the facet faces away or misses the tile.
 template <typename T>
 __device__ bool stage_facet(const RasterArgs &a, const FrameGeom &g, int f,
                             int ti0, int ti1, int tj0, int tj1, Stage<T> &s)
@@ -121,15 +183,11 @@ __device__ bool stage_facet(const RasterArgs &a, const FrameGeom &g, int f,
     using T4 = typename Vec4<T>::type;
     const T4 *vt = static_cast<const T4 *>(a.vt) + g.vt_base;
     double4 nb = a.fn[f];
-    double nn[3];
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        nn[r] = 0.0;
-        nn[r] += g.oa[3 * r + 0] * nb.x;
-        nn[r] += g.oa[3 * r + 1] * nb.y;
-        nn[r] += g.oa[3 * r + 2] * nb.z;
-    }
-    if (!(nn[2] > 0.0)) return false;
+    double nz = 0.0;
+    nz += g.oa[6] * nb.x;
+    nz += g.oa[7] * nb.y;
+    nz += g.oa[8] * nb.z;
+    if (!(nz > 0.0)) return false;
     int4 c = a.fvi[f];
     T4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
     const double kmpp = g.kmpp;
@@ -150,17 +208,11 @@ __device__ bool stage_facet(const RasterArgs &a, const FrameGeom &g, int f,
     int i1 = max(imin, -n), i2 = min(imax, n), j1 = max(jmin, -n), j2 = min(jmax, n);
     if (i1 > n || i2 < -n || j1 > n || j2 < -n) return false;
     if (i2 < ti0 || i1 > ti1 || j2 < tj0 || j1 > tj1) return false;
-    s.v00 = p0.x; s.v01 = p0.y; s.v02 = p0.z;
-    s.A = p2.y - p1.y;
-    s.B = p2.x - p1.x;
-    s.C = p1.x - p0.x;
-    s.D = p1.y - p0.y;
-    s.E = p1.z - p0.z;
-    s.F = p2.z - p1.z;
-    s.den = (T)1 / (s.C * s.A - s.B * s.D);
-    s.nx = (T)nn[0]; s.ny = (T)nn[1]; s.nz = (T)nn[2];
-    s.i1 = i1; s.i2 = i2; s.j1 = j1; s.j2 = j2;
-    s.f = f; s.c0 = c.x; s.c1 = c.y; s.c2 = c.z;
+    int ri1 = max(i1, ti0) - ti0, ri2 = min(i2, ti1) - ti0;
+    int rj1 = max(j1, tj0) - tj0, rj2 = min(j2, tj1) - tj0;
+    s.bb = ri1 | (ri2 << 4) | (rj1 << 8) | (rj2 << 12);
+    s.wmask = warp_mask_of(ri1, ri2, rj1, rj2);
+    stage_fill<T>(a, g, f, s);
     return true;
 }
 
@@ -212,75 +264,128 @@ __device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, int x, int y, T z, PixLim
 
 template <typename T> __device__ inline void atomic_add_any(T *p, T v) { atomicAdd(p, v); }
 
+// Delay response of image row idel for a pixel at delay bin delPOS
+// (src/shape/pos2deldop.c:371-425).
+template <typename T>
+__device__ inline T del_resp(const FrameGeom &g, T delPOS, int idel)
+{
+    const int spb = g.spb;
+    T dc;
+    if (g.codemethod != SHAPE_CODE_LONG_ORIG) {
+        if (spb == 1) {
+            dc = tri2<T>(delPOS - (T)idel);
+        } else if (spb == 2) {
+            T arg = (delPOS - ((T)idel - (T)g.const2)) / (T)g.spb_over_stride;
+            dc = tri<T>(arg) + tri<T>(arg - (T)0.5);
+            dc *= dc / 4;
+        } else {
+            dc = 0;
+            int m_min = max((int)floor((delPOS - (T)idel - (T)g.const2) * (T)g.stride), 0);
+            int m_max = min((int)ceil((delPOS - (T)idel + (T)g.const1) * (T)g.stride), spb) - 1;
+            T arg = (delPOS - ((T)idel - (T)g.const2)) / (T)g.spb_over_stride
+                    - (T)m_min * (T)g.one_over_spb;
+            for (int m = m_min; m <= m_max; m++) {
+                dc += tri<T>(arg);
+                arg -= (T)g.one_over_spb;
+            }
+            dc *= dc / (T)g.spb_sq;
+        }
+    } else {
+        dc = tri2<T>((delPOS - (T)idel) / (T)g.spb_over_stride);
+    }
+    return dc;
+}
+
+// Mean sinc^2 Doppler response of column idop over nsinc2^2 points
+// (src/shape/pos2deldop.c:432-460); s2u = sin^2(pi * frac(dopPOS)) serves
+// the nsinc2 == 1 case, where sin^2(pi*(dopPOS - idop)) = s2u.
+template <typename T>
+__device__ inline T dop_resp(const FrameGeom &g, T dopPOS, T s2u, int idop)
+{
+    const int nsinc2 = g.nsinc2;
+    if (nsinc2 == 1) {
+        const T t = fabs((T)3.141592653589793 * (dopPOS - (T)idop));
+        return (t > (T)1.0e-4) ? s2u / (t * t) : (T)1.0;
+    }
+    if (nsinc2 == 2) {
+        T bl = dopPOS + (T)g.dopdiff_bl - (T)idop;
+        return (sinc2<T>(bl) + sinc2<T>(bl + (T)g.xincr) + sinc2<T>(bl + (T)g.yincr) +
+                sinc2<T>(bl + (T)g.xincr + (T)g.yincr)) / 4;
+    }
+    T left = dopPOS + (T)g.dopdiff_bl - (T)idop;
+    T sm = 0;
+    for (int i = 0; i < nsinc2; i++) {
+        T arg = left;
+        for (int j = 0; j < nsinc2; j++) {
+            sm += sinc2<T>(arg);
+            arg += (T)g.xincr;
+        }
+        left += (T)g.yincr;
+    }
+    return sm / (T)g.nsinc2_sq;
+}
+
+// Footprint sizes of the register-resident fast path.
+constexpr int FAST_ROWS = 2;
+constexpr int FAST_COLS = 8;
+
 // Delay and Doppler response of one pixel and its scatter into `dst`, an
 // image whose element (idel, idop) lives at dst[(idel - row0) * stride +
 // (idop - col0)] (src/shape/pos2deldop.c:371-496). dst is either the frame's
-// fit image in HBM or the tile's shared-memory accumulator.
+// fit image in HBM or the tile's shared-memory accumulator. Footprints of at
+// most FAST_ROWS x FAST_COLS bins (the common LONG_ORIG spb=1 / nsinc2=1 /
+// sinc2width<=7 case) keep their weights in registers and scatter through
+// fully unrolled, predicated loops, so the lanes of a warp stay converged.
 template <typename T>
 __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, T cose, const PixDD<T> &d,
                                  T *dst, int row0, int col0, int stride)
 {
-    const T delPOS = d.delPOS, dopPOS = d.dopPOS, const1 = (T)g.const1;
+    const T delPOS = d.delPOS, dopPOS = d.dopPOS;
     const int idel_min = d.idel_min, idel_max = d.idel_max, idop_min = d.idop_min, idop_max = d.idop_max;
+    const int nr = idel_max - idel_min + 1, nc = idop_max - idop_min + 1;
+    T s2u = 0;
+    if (g.nsinc2 == 1) {
+        const T su = tsin<T>((T)3.141592653589793 * (dopPOS - floor(dopPOS)));
+        s2u = su * su;
+    }
+    const T kmpp = (T)g.kmpp;
+    const T rl = radlaw_dev<T>(a.laws[g.law], cose) * kmpp * kmpp * d.codefactor;
+    if (nr <= FAST_ROWS && nc <= FAST_COLS) {
+        T dc[FAST_ROWS], pc[FAST_COLS];
+        T sdel = 0, sdop = 0;
+#pragma unroll
+        for (int r = 0; r < FAST_ROWS; r++) {
+            dc[r] = (r < nr) ? del_resp<T>(g, delPOS, idel_min + r) : (T)0;
+            if (r < nr) sdel += dc[r];
+        }
+#pragma unroll
+        for (int c = 0; c < FAST_COLS; c++) {
+            pc[c] = (c < nc) ? dop_resp<T>(g, dopPOS, s2u, idop_min + c) : (T)0;
+            if (c < nc) sdop += pc[c];
+        }
+        // sum of del_c*dop_c over the footprint = (sum del_c) * (sum dop_c)
+        // (src/shape/pos2deldop.c:462-466)
+        const T amp = rl / (sdel * sdop);
+#pragma unroll
+        for (int r = 0; r < FAST_ROWS; r++) {
+            const T ad = amp * dc[r];
+            T *row = dst + (long long)(idel_min + r - row0) * stride + (idop_min - col0);
+#pragma unroll
+            for (int c = 0; c < FAST_COLS; c++)
+                if (r < nr && c < nc) atomic_add_any<T>(row + c, ad * pc[c]);
+        }
+        return;
+    }
     T del_c[SHAPE_MAXBINS];
     T dop_c[SHAPE_MAXBINS + 1];
-    const int spb = g.spb;
-    for (int idel = idel_min; idel <= idel_max; idel++) {
-        T dc;
-        if (g.codemethod != SHAPE_CODE_LONG_ORIG) {
-            if (spb == 1) {
-                dc = tri2<T>(delPOS - (T)idel);
-            } else if (spb == 2) {
-                T arg = (delPOS - ((T)idel - (T)g.const2)) / (T)g.spb_over_stride;
-                dc = tri<T>(arg) + tri<T>(arg - (T)0.5);
-                dc *= dc / 4;
-            } else {
-                dc = 0;
-                int m_min = max((int)floor((delPOS - (T)idel - (T)g.const2) * (T)g.stride), 0);
-                int m_max = min((int)ceil((delPOS - (T)idel + const1) * (T)g.stride), spb) - 1;
-                T arg = (delPOS - ((T)idel - (T)g.const2)) / (T)g.spb_over_stride
-                        - (T)m_min * (T)g.one_over_spb;
-                for (int m = m_min; m <= m_max; m++) {
-                    dc += tri<T>(arg);
-                    arg -= (T)g.one_over_spb;
-                }
-                dc *= dc / (T)g.spb_sq;
-            }
-        } else {
-            dc = tri2<T>((delPOS - (T)idel) / (T)g.spb_over_stride);
-        }
-        del_c[idel - idel_min] = dc;
-    }
-    const int nsinc2 = g.nsinc2;
-    for (int idop = idop_min; idop <= idop_max; idop++) {
-        T sm;
-        if (nsinc2 == 1) {
-            sm = sinc2<T>(dopPOS - (T)idop);
-        } else if (nsinc2 == 2) {
-            T bl = dopPOS + (T)g.dopdiff_bl - (T)idop;
-            sm = (sinc2<T>(bl) + sinc2<T>(bl + (T)g.xincr) + sinc2<T>(bl + (T)g.yincr) +
-                  sinc2<T>(bl + (T)g.xincr + (T)g.yincr)) / 4;
-        } else {
-            T left = dopPOS + (T)g.dopdiff_bl - (T)idop;
-            sm = 0;
-            for (int i = 0; i < nsinc2; i++) {
-                T arg = left;
-                for (int j = 0; j < nsinc2; j++) {
-                    sm += sinc2<T>(arg);
-                    arg += (T)g.xincr;
-                }
-                left += (T)g.yincr;
-            }
-            sm /= (T)g.nsinc2_sq;
-        }
-        dop_c[min(idop - idop_min, SHAPE_MAXBINS)] = sm;
-    }
-    T sumweights = 0;
     for (int idel = idel_min; idel <= idel_max; idel++)
-        for (int idop = idop_min; idop <= idop_max; idop++)
-            sumweights += del_c[idel - idel_min] * dop_c[min(idop - idop_min, SHAPE_MAXBINS)];
-    const T kmpp = (T)g.kmpp;
-    T amp = radlaw_dev<T>(a.laws[g.law], cose) * kmpp * kmpp * d.codefactor / sumweights;
+        del_c[idel - idel_min] = del_resp<T>(g, delPOS, idel);
+    for (int idop = idop_min; idop <= idop_max; idop++)
+        dop_c[min(idop - idop_min, SHAPE_MAXBINS)] = dop_resp<T>(g, dopPOS, s2u, idop);
+    T sdel = 0, sdop = 0;
+    for (int idel = idel_min; idel <= idel_max; idel++) sdel += del_c[idel - idel_min];
+    for (int idop = idop_min; idop <= idop_max; idop++) sdop += dop_c[min(idop - idop_min, SHAPE_MAXBINS)];
+    const T amp = rl / (sdel * sdop);
     for (int idel = idel_min; idel <= idel_max; idel++) {
         T ad = amp * del_c[idel - idel_min];
         T *row = dst + (long long)(idel - row0) * stride - col0;
@@ -311,18 +416,21 @@ __device__ inline double warp_dmax(double v)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
+__global__ void __launch_bounds__(RASTER_THREADS, sizeof(T) == 8 ? RASTER_MIN_BLOCKS_F64 : RASTER_MIN_BLOCKS)
+k_raster(RasterArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    int *raw = reinterpret_cast<int *>(smem);
-    int *ids = raw + a.cap;
-    Stage<T> *st = reinterpret_cast<Stage<T> *>(smem + (((size_t)2 * a.cap * sizeof(int) + 15) & ~(size_t)15));
-    __shared__ int s_nst;
+    int2 *raw = reinterpret_cast<int2 *>(smem);
+    int2 *ids = raw + a.cap;
+    Stage<T> *st = reinterpret_cast<Stage<T> *>(smem + (size_t)2 * a.cap * sizeof(int2));
     __shared__ int s_red[RASTER_THREADS / 32][4];
     __shared__ double s_redd[RASTER_THREADS / 32][4];
     __shared__ int s_redl[RASTER_THREADS / 32][4];
     __shared__ int s_box[RASTER_THREADS / 32][4];
+    __shared__ T s_pz[TILE_PIX], s_pc[TILE_PIX];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    // warp wid owns a 4x8 block of the 16x16 tile
+    const int li = 4 * (wid >> 1) + (lane >> 3), lj = 8 * (wid & 1) + (lane & 7);
 
     for (int w = blockIdx.x; w < a.nwork; w += gridDim.x) {
         const int2 item = a.work[w];
@@ -332,7 +440,7 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
         const int n = g.n;
         const int ti0 = -n + tx * TILE_W, tj0 = -n + ty * TILE_W;
         const int ti1 = min(ti0 + TILE_W - 1, n), tj1 = min(tj0 + TILE_W - 1, n);
-        const int pi = ti0 + tid / TILE_W, pj = tj0 + tid % TILE_W;
+        const int pi = ti0 + li, pj = tj0 + lj;
         const bool inframe = (pi <= n) && (pj <= n);
         const int count = a.bin_count[g.tile_base + tile];
         const bool writes_pos = (g.kind != VIEW_RADAR) || a.keep_pos;
@@ -341,74 +449,80 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
         const T x0 = (T)pi * (T)g.kmpp, x1 = (T)pj * (T)g.kmpp;
         T zz = (T)(-SHAPE_HUGENUMBER), cosa = 0, cosb = 0;
         int fac = -1;
+        bool good = false;
+        T gm0 = 0, gm1 = 0, gm2 = 0;
         const bool smooth = g.smooth != 0;
         const bool bistatic_obs = (g.kind == VIEW_LC_OBS);
-        T oa[9];
-#pragma unroll
-        for (int k = 0; k < 9; k++) oa[k] = (T)g.oa[k];
-        const T us0 = (T)g.usrc[0], us1 = (T)g.usrc[1], us2 = (T)g.usrc[2];
+        const T oa6 = (T)g.oa[6], oa7 = (T)g.oa[7], oa8 = (T)g.oa[8];
 
+        // Apply posvis's update rule for one staged facet at this pixel.
+        auto visit = [&](const Stage<T> &s) {
+            const int bb = s.bb;
+            if (li < (bb & 15) || li > ((bb >> 4) & 15) || lj < ((bb >> 8) & 15) || lj > ((bb >> 12) & 15))
+                return;
+            const T dx = x0 - s.v00, dy = x1 - s.v01;
+            const T sv = (dx * s.A - s.B * dy) * s.den;
+            if (!((sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL))) return;
+            const T tv = (s.C * dy - dx * s.D) * s.den;
+            if (!((tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL))) return;
+            const T z = s.v02 + sv * s.E + tv * s.F;
+            if (!((z > zz) || (fac < 0))) return;
+            zz = z;
+            fac = s.f;
+            // cos(e) changes only when the smoothed normal faces the viewer
+            // (posvis.c:265). Its sign is that of the view-z component before
+            // normalization, so a win records the body-frame interpolated
+            // normal and the last qualifying one is normalized once, below.
+            if (smooth) {
+                const T m0 = s.q[0] + sv * (s.q[3] - s.q[0]) + tv * (s.q[6] - s.q[3]);
+                const T m1 = s.q[1] + sv * (s.q[4] - s.q[1]) + tv * (s.q[7] - s.q[4]);
+                const T m2 = s.q[2] + sv * (s.q[5] - s.q[2]) + tv * (s.q[8] - s.q[5]);
+                T r2 = 0;
+                r2 += oa6 * m0; r2 += oa7 * m1; r2 += oa8 * m2;
+                if (r2 > (T)0) { good = true; gm0 = m0; gm1 = m1; gm2 = m2; }
+            } else {
+                good = true; gm0 = s.nx; gm1 = s.ny; gm2 = s.nz;
+            }
+        };
+        // Each warp walks only the staged facets whose bbox meets its block,
+        // in staging (= facet index) order.
         auto replay = [&](int nst) {
-            for (int k = 0; k < nst; k++) {
-                const Stage<T> &s = st[k];
-                if (pi < s.i1 || pi > s.i2 || pj < s.j1 || pj > s.j2) continue;
-                const T dx = x0 - s.v00, dy = x1 - s.v01;
-                const T sv = (dx * s.A - s.B * dy) * s.den;
-                if (!((sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL))) continue;
-                const T tv = (s.C * dy - dx * s.D) * s.den;
-                if (!((tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL))) continue;
-                const T z = s.v02 + sv * s.E + tv * s.F;
-                if (!((z > zz) || (fac < 0))) continue;
-                zz = z;
-                T n0 = s.nx, n1 = s.ny, n2 = s.nz;
-                if (smooth) {
-                    double4 q0 = a.vn[s.c0], q1 = a.vn[s.c1], q2 = a.vn[s.c2];
-                    T m0 = (T)q0.x + sv * ((T)q1.x - (T)q0.x) + tv * ((T)q2.x - (T)q1.x);
-                    T m1 = (T)q0.y + sv * ((T)q1.y - (T)q0.y) + tv * ((T)q2.y - (T)q1.y);
-                    T m2 = (T)q0.z + sv * ((T)q1.z - (T)q0.z) + tv * ((T)q2.z - (T)q1.z);
-                    T r0 = 0, r1 = 0, r2 = 0;
-                    r0 += oa[0] * m0; r0 += oa[1] * m1; r0 += oa[2] * m2;
-                    r1 += oa[3] * m0; r1 += oa[4] * m1; r1 += oa[5] * m2;
-                    r2 += oa[6] * m0; r2 += oa[7] * m1; r2 += oa[8] * m2;
-                    T norm = 0;
-                    norm += r0 * r0; norm += r1 * r1; norm += r2 * r2;
-                    norm = sqrt(norm);
-                    if (norm != (T)0) { r0 /= norm; r1 /= norm; r2 /= norm; }
-                    n0 = r0; n1 = r1; n2 = r2;
+            for (int base = 0; base < nst; base += 32) {
+                const int k = base + lane;
+                const bool hit = (k < nst) && ((st[k].wmask >> wid) & 1);
+                unsigned m = __ballot_sync(0xffffffffu, hit);
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1;
+                    visit(st[base + b]);
                 }
-                if (n2 > (T)0) {
-                    cosa = n2;
-                    if (bistatic_obs) {
-                        cosb = n0 * us0 + n1 * us1 + n2 * us2;
-                        if (cosb <= (T)0) cosa = 0;
-                    }
-                }
-                fac = s.f;
             }
         };
 
         if (count > 0 && count <= a.cap) {
-            const int *bin = a.bin_ids + (size_t)(g.tile_base + tile) * a.cap;
+            const int2 *bin = a.bin_ids + (size_t)(g.tile_base + tile) * a.cap;
             for (int k = tid; k < count; k += RASTER_THREADS) raw[k] = bin[k];
             __syncthreads();
             for (int k = tid; k < count; k += RASTER_THREADS) {
-                int v = raw[k], r = 0;
-                for (int m = 0; m < count; m++) r += (raw[m] < v);
+                int2 v = raw[k];
+                int r = 0;
+                for (int m = 0; m < count; m++) r += (raw[m].x < v.x);
                 ids[r] = v;
             }
             __syncthreads();
             for (int c0 = 0; c0 < count; c0 += STAGE_FACETS) {
-                if (tid == 0) s_nst = 0;
-                __syncthreads();
-                int nst_here = min(STAGE_FACETS, count - c0);
-                if (tid < nst_here) {
+                const int nst = min(STAGE_FACETS, count - c0);
+                if (tid < nst) {
+                    const int2 e = ids[c0 + tid];
                     Stage<T> sf;
-                    bool ok = stage_facet<T>(a, g, ids[c0 + tid], ti0, ti1, tj0, tj1, sf);
-                    if (!ok) { sf.i1 = INT_MAX; sf.i2 = INT_MIN; sf.j1 = INT_MAX; sf.j2 = INT_MIN; sf.f = ids[c0 + tid]; }
+                    const int bb = e.y;
+                    sf.bb = bb;
+                    sf.wmask = warp_mask_of(bb & 15, (bb >> 4) & 15, (bb >> 8) & 15, (bb >> 12) & 15);
+                    stage_fill<T>(a, g, e.x, sf);
                     st[tid] = sf;
                 }
                 __syncthreads();
-                replay(nst_here);
+                replay(nst);
                 __syncthreads();
             }
         } else if (count > a.cap) {
@@ -434,6 +548,30 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
             }
         }
 
+        // cos(e) / cos(i) of the last winner whose smoothed normal faced the
+        // viewer: cotrans + normalize (posvis.c:250-274), once per pixel
+        if (good) {
+            T n0 = gm0, n1 = gm1, n2 = gm2;
+            if (smooth) {
+                T r0 = 0, r1 = 0, r2 = 0;
+                r0 += (T)g.oa[0] * gm0; r0 += (T)g.oa[1] * gm1; r0 += (T)g.oa[2] * gm2;
+                r1 += (T)g.oa[3] * gm0; r1 += (T)g.oa[4] * gm1; r1 += (T)g.oa[5] * gm2;
+                r2 += oa6 * gm0; r2 += oa7 * gm1; r2 += oa8 * gm2;
+                T norm = 0;
+                norm += r0 * r0; norm += r1 * r1; norm += r2 * r2;
+                norm = sqrt(norm);
+                if (norm != (T)0) { r0 /= norm; r1 /= norm; r2 /= norm; }
+                n0 = r0; n1 = r1; n2 = r2;
+            }
+            if (n2 > (T)0) {
+                cosa = n2;
+                if (bistatic_obs) {
+                    cosb = n0 * (T)g.usrc[0] + n1 * (T)g.usrc[1] + n2 * (T)g.usrc[2];
+                    if (cosb <= (T)0) cosa = 0;
+                }
+            }
+        }
+
         // ---- outputs of this tile
         const bool covered = inframe && fac >= 0;
         if (inframe && writes_pos) {
@@ -441,12 +579,8 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
             T *Z = static_cast<T *>(a.pos_z), *CE = static_cast<T *>(a.pos_cose), *CI = static_cast<T *>(a.pos_cosi);
             Z[p] = zz;
             a.pos_f[p] = fac;
-            if (g.kind != VIEW_LC_SUN) {
-                CE[p] = cosa;
-                CI[p] = cosb;
-            } else {
-                CE[p] = cosa;   // cos(incidence) in the sun view (pos->cosill)
-            }
+            CE[p] = cosa;                        // cos(e), or cos(i) in the sun view (pos->cosill)
+            if (g.kind != VIEW_LC_SUN) CI[p] = cosb;
         }
         // covered-pixel bbox (POSrect with (i,i,j,j), posvis.c:278-280)
         int cimin = covered ? pi : INT_MAX, cimax = covered ? pi : INT_MIN;
@@ -458,20 +592,32 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
         bool lit = false;
         PixDD<T> dd;
         dd.ok = false;
+        T scose = 0;
         if (g.kind == VIEW_RADAR && covered) {
             if (a.mark_seen && (double)cosa > a.mincosine_seen)
                 a.seen[fac] = 1;
-            if (cosa > (T)0) {
+        }
+        if (g.kind == VIEW_RADAR) {
+            // Synthesis runs on a permuted pixel-to-thread map: the replay
+            // wants each warp on a compact 4x8 block, but neighbouring pixels
+            // hit the same delay-Doppler bins, so compact warps would
+            // serialize their shared-memory atomics; a warp of scattered
+            // pixels rarely repeats an address.
+            const int me = li * TILE_W + lj;
+            s_pz[me] = zz;
+            s_pc[me] = (covered && cosa > (T)0) ? cosa : (T)0;
+            __syncthreads();
+            const int q = (tid * 37 + 11) & (TILE_PIX - 1);
+            scose = s_pc[q];
+            if (scose > (T)0) {
                 lit = true;
-                dd = pixel_dd_setup<T>(g, pi, pj, zz, lim);
+                dd = pixel_dd_setup<T>(g, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], lim);
             }
         }
         if (g.kind == VIEW_RADAR) {
             // The tile's delay-Doppler footprint is accumulated in shared
             // memory (reusing the bin / stage space, free after the replay)
-            // and flushed with one global atomic per touched bin; many pixels
-            // of a tile hit the same bins, so this removes most of the
-            // contended HBM/L2 atomics.
+            // and flushed with one global atomic per touched bin.
             int b0 = dd.ok ? dd.idel_min : INT_MAX, b1 = dd.ok ? dd.idel_max : INT_MIN;
             int b2 = dd.ok ? dd.idop_min : INT_MAX, b3 = dd.ok ? dd.idop_max : INT_MIN;
             b0 = warp_min(b0); b1 = warp_max(b1); b2 = warp_min(b2); b3 = warp_max(b3);
@@ -490,7 +636,7 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
                 if (cells <= (long long)(a.smem_bytes / sizeof(T))) {
                     for (long long k = tid; k < cells; k += RASTER_THREADS) box[k] = (T)0;
                     __syncthreads();
-                    if (dd.ok) pixel_dd_scatter<T>(a, g, cosa, dd, box, r0, c0, nc);
+                    if (dd.ok) pixel_dd_scatter<T>(a, g, scose, dd, box, r0, c0, nc);
                     __syncthreads();
                     for (long long k = tid; k < cells; k += RASTER_THREADS) {
                         T v = box[k];
@@ -500,7 +646,7 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
                         }
                     }
                 } else if (dd.ok) {
-                    pixel_dd_scatter<T>(a, g, cosa, dd, fit, 1, 1, g.ndop);
+                    pixel_dd_scatter<T>(a, g, scose, dd, fit, 1, 1, g.ndop);
                 }
             }
         }
@@ -557,7 +703,7 @@ __global__ void __launch_bounds__(RASTER_THREADS) k_raster(RasterArgs a)
 template <typename T>
 inline size_t raster_smem_bytes(int cap)
 {
-    return (((size_t)2 * cap * sizeof(int) + 15) & ~(size_t)15) + (size_t)STAGE_FACETS * sizeof(Stage<T>);
+    return (size_t)2 * cap * sizeof(int2) + (size_t)STAGE_FACETS * sizeof(Stage<T>);
 }
 
 // Called once per device before any launch (not inside stream capture).

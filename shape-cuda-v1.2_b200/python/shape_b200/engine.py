@@ -69,6 +69,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_get_realized.argtypes = [vp, cd.dptr, cd.dptr, cd.dptr, cd.dptr]
     L.shape_engine_last_time_ms.argtypes = [vp, P(C.c_double)]
     L.shape_engine_stage_times.argtypes = [vp, C.c_int, cd.dptr, C.c_int]
+    L.shape_engine_set_bin_capacity.argtypes = [vp, C.c_int]
+    L.shape_engine_get_tuning.argtypes = [vp, P(C.c_int), C.c_int]
     _lib = L
     return L
 
@@ -145,6 +147,15 @@ class Engine:
 
     def finalize(self):
         _chk(self.L.shape_engine_finalize(self.h))
+
+    def set_bin_capacity(self, cap):
+        _chk(self.L.shape_engine_set_bin_capacity(self.h, int(cap)))
+
+    def tuning(self):
+        out = (C.c_int * 8)()
+        n = _chk(self.L.shape_engine_get_tuning(self.h, out, 8))
+        keys = ["bin_capacity", "max_bin", "nonempty_tiles", "tiles", "tile_w"]
+        return dict(zip(keys[:n], [out[i] for i in range(n)]))
 
     def keep_pos(self, keep=True):
         _chk(self.L.shape_engine_keep_pos(self.h, 1 if keep else 0))
