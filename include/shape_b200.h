@@ -138,6 +138,29 @@ int shape_engine_get_tuning(shape_engine *e, int *out, int max);
 /* Device time of the last evaluation (CUDA events on the engine stream). */
 int shape_engine_last_time_ms(shape_engine *e, double *ms);
 
+/* Per-frame chi-square sums over images the CALLER already holds in device
+ * memory, computed without allocating any device memory. It has no
+ * counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc, such as a process whose device memory belongs to another
+ * allocator (a PyTorch or pool-managed program under a hard memory cap) or a
+ * latency-critical loop where cudaMalloc/cudaFree could synchronize the
+ * device. Frame f occupies elements [frame_offsets[f], frame_offsets[f+1])
+ * of d_obs, d_oneovervar and d_fit (device pointers, FP64); weight,
+ * cal_floating and cal (host arrays of nframes) follow chi2_deldop. On return
+ * out (host, 5*nframes doubles) holds o2, m2, om, cal and chi2 per frame.
+ * Limits: at most 4096 frames and 65536*2048 elements in total; larger
+ * requests fail with SHAPE_E_ARG. The scratch space is one fixed device
+ * array (about 3.5 MB per device, kept until the process exits); the first
+ * call on a device looks up its address, so make that first call outside
+ * any stream capture. Kernels run on the legacy default stream and the call
+ * returns after the results reach host memory. Calls share the scratch
+ * array: calls that overlap on the GPU (from several threads or streams)
+ * race on it. */
+int shape_chi2_frames_noalloc(int device, int nframes, const long long *frame_offsets,
+                              const double *d_obs, const double *d_oneovervar,
+                              const double *d_fit, const double *weight,
+                              const int *cal_floating, const double *cal, double *out);
+
 #ifdef __cplusplus
 }
 #endif

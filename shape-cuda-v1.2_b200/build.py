@@ -30,6 +30,7 @@ UNITS = [
     ("raster_f64.cu", ["-fmad=false"]),
     ("raster_f32.cu", []),
     ("engine.cu", ["-fmad=false"]),
+    ("noalloc.cu", ["-fmad=false"]),
 ]
 
 HEADERS = ["engine_internal.h", "kernels.h", "raster_impl.cuh"]

@@ -28,6 +28,9 @@ static int set_err(int code, const std::string &msg)
     return code;
 }
 
+// Shared with other translation units of the library (noalloc.cu).
+int report_error(int code, const std::string &msg) { return set_err(code, msg); }
+
 #define CK(call)                                                                           \
     do {                                                                                   \
         cudaError_t e_ = (call);                                                           \

@@ -71,6 +71,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_stage_times.argtypes = [vp, C.c_int, cd.dptr, C.c_int]
     L.shape_engine_set_bin_capacity.argtypes = [vp, C.c_int]
     L.shape_engine_get_tuning.argtypes = [vp, P(C.c_int), C.c_int]
+    L.shape_chi2_frames_noalloc.argtypes = [C.c_int, C.c_int, P(C.c_longlong), C.c_void_p, C.c_void_p,
+                                            C.c_void_p, cd.dptr, cd.iptr, cd.dptr, cd.dptr]
     _lib = L
     return L
 
