@@ -347,7 +347,7 @@ def _finish_deldop(dset, frames, synthesize, amp, sdev, seed, params):
     return ds
 
 
-def config1_dataset(synthesize=None, params=None):
+def config1_dataset(synthesize=None, params=None, pos_n=75):
     """Config 1: one 100x100 delay-Doppler frame, POS 151x151 at 15 m/px,
     period 6 h, pole (30, 60) deg, cos^2 law (COSINELAW_DIFF, C=1, R=0.1),
     LONG_ORIG spb=1 stride=1, Ftx 2380 MHz, 0.1 usec x 0.1 Hz pixels."""
@@ -362,13 +362,13 @@ def config1_dataset(synthesize=None, params=None):
     dset.Ftx, dset.dopscale = 2380.0, 1.0
     dset.codemethod, dset.spb, dset.stride, dset.dopfftlen = 1, 1, 1, 64
     dset.law = radar_cosine()
-    fr = _frame(75, 2.25 / 150.0, ae, oe, omega * pole, 100, 100, 70.0, 50.5)
+    fr = _frame(pos_n, 2.25 / 150.0, ae, oe, omega * pole, 100, 100, 70.0, 50.5)
     return _finish_deldop(dset, [fr], synthesize, 20.0, 1.0, 1234, params)
 
 
 def batched_dataset(nframes=64, pos_range=(101, 301), ndel_range=(64, 256),
                     ndop_range=(64, 512), synthesize=None, params=None, seed=7,
-                    radius=1.05, codemethod=1, spb=1, stride=1):
+                    radius=1.05, codemethod=1, spb=1, stride=1, law=None, dopfftlen=64):
     """Config 2 (and, with other sizes, config 4): frames at rotation phases
     uniform in [0, 2pi), odd POS sides, delay/Doppler sizes uniform in the
     given ranges, resolutions scaled so the target spans ~80% of each frame."""
@@ -383,8 +383,8 @@ def batched_dataset(nframes=64, pos_range=(101, 301), ndel_range=(64, 256),
     Ftx = 2380.0
     dset = cd.DeldopSet()
     dset.Ftx, dset.dopscale = Ftx, 1.0
-    dset.codemethod, dset.spb, dset.stride, dset.dopfftlen = codemethod, spb, stride, 64
-    dset.law = radar_cosine()
+    dset.codemethod, dset.spb, dset.stride, dset.dopfftlen = codemethod, spb, stride, dopfftlen
+    dset.law = law if law is not None else radar_cosine()
     frames = []
     # one set-level resolution: taken from the median frame size, then each
     # frame's POS scale adapts to its own pixel count
@@ -415,7 +415,7 @@ def config4_dataset(synthesize=None, params=None):
 
 
 def lightcurve_dataset(npoints=200, pos_range=(129, 257), synthesize=None, params=None,
-                       seed=7, set_index=0, radius=1.05):
+                       seed=7, set_index=0, radius=1.05, law_type=11):
     """Config 3: one lightcurve of `npoints` points, solar phase uniform in
     5-60 deg, odd POS sides uniform in pos_range, Kaasalainen law with
     wt=0.3 (Lommel-Seeliger 0.7 + Lambert 0.3), A0=0, k=0; calc epochs equal
@@ -447,7 +447,7 @@ def lightcurve_dataset(npoints=200, pos_range=(129, 257), synthesize=None, param
     ls.weight, ls.dof = 1.0, float(npoints)
     ls.cal_floating, ls.cal = 1, 1.0
     law = cd.OpticalLaw()
-    law.type, law.R, law.wt, law.A0, law.D, law.k = 11, 1.0, 0.3, 0.0, 0.1, 0.0
+    law.type, law.R, law.wt, law.A0, law.D, law.k = law_type, 1.0, 0.3, 0.0, 0.1, 0.0
     ls.law = law
     x = t.copy()
     obs = np.ones(npoints)

@@ -1,0 +1,53 @@
+"""The C ABI library on CPU (no GPU calls): it loads, exports every function
+that include/*.h declares, and the ctypes struct layouts of the bindings
+match the compiler's sizeof()."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+from shape_b200 import ctypes_defs as cd
+from shape_b200 import engine as eng
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in ("shape_b200.h", "shape_types.h"):
+        text = open(os.path.join(REPO, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names.update(re.findall(r"\b(shape_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+def test_library_loads_and_exports_all_declared_symbols():
+    L = eng.load_library()
+    assert L.shape_version().startswith(b"shape-b200")
+    names = declared_functions()
+    assert "shape_engine_evaluate" in names and "shape_chi2_frames_noalloc" in names
+    out = subprocess.run(["nm", "-D", "--defined-only", eng.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    missing = sorted(n for n in names if n not in exported)
+    assert not missing, missing
+    for n in names:
+        assert hasattr(L, n)
+
+
+def test_struct_layouts_match_compiler():
+    sizes = eng.abi_sizes()
+    for name, size in zip(eng.ABI_ORDER, sizes):
+        assert C.sizeof(cd.STRUCTS[name]) == size, name
+    assert C.sizeof(eng.EvalSummary) == sizes[len(eng.ABI_ORDER)]
+
+
+def test_errors_without_device_are_reported():
+    """Without a usable device, create fails with a status and a message
+    (the library never falls back to a CPU path)."""
+    import torch
+    if torch.cuda.is_available():
+        return
+    L = eng.load_library()
+    h = C.c_void_p()
+    rc = L.shape_engine_create(0, C.byref(h))
+    assert rc < 0 and len(L.shape_last_error()) > 0

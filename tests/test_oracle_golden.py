@@ -1,0 +1,129 @@
+"""The CPU oracle restatement (oracle/shape_oracle.c) against golden vectors
+produced by the reference's own CPU code (tests/golden/make_golden.py).
+
+The oracle keeps the reference's floating-point operation order, so every
+comparison here is exact: realized model, facet / z / cos(e) / shadow maps,
+fit images, chi-square, limits and flags.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import golden_cases as gc
+from oracle.bindings import Oracle
+from shape_b200 import synth
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = json.load(open(os.path.join(HERE, "golden", "reference_golden.json")))
+ARR = np.load(os.path.join(HERE, "golden", "reference_arrays.npz"))
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return Oracle()
+
+
+@pytest.mark.parametrize("name,mk", [("c1", synth.ellipsoid_model), ("c2", synth.harmonic_model),
+                                     ("octa3", gc.octa3_model)])
+def test_realize_bit_exact(orc, name, mk):
+    r = orc.realize(mk())
+    for k in ("x", "vn", "fn", "area"):
+        assert digest(r[k]) == GOLD["realize"][name][k], k
+
+
+def _calc_fits_flags(results, frames, dof_total):
+    """par flags after calc_fits (src/shape/calc_fits.c:407-409, 511-550)."""
+    posbnd = badradar = 0
+    plog = blog = 0.0
+    for r, fr in zip(results, frames):
+        if r["outbnd"]:
+            posbnd = 1
+            plog += fr.dof * r["posbnd_logfactor"]
+        if r["badradar"]:
+            badradar = 1
+            blog += fr.dof * r["badradar_logfactor"]
+    return posbnd, plog / dof_total, badradar, blog / dof_total
+
+
+@pytest.mark.parametrize("name", sorted(gc.DELDOP_CASES))
+def test_deldop_bit_exact(orc, name):
+    model_fn, ds_fn, params = gc.DELDOP_CASES[name]
+    g = GOLD["deldop"][name]
+    m = model_fn()
+    ds = ds_fn(lambda d, p: orc.eval_deldop(m, d, p)["fits"], params)
+    assert digest(ds.obs) == g["obs"], "synthesized observations differ"
+    o = orc.eval_deldop(m, ds, params, keep_pos=True)
+    for f, gf in enumerate(g["frames"]):
+        po, r = o["pos"][f], o["results"][f]
+        assert digest(po["f"].astype(np.int32)) == gf["f"], (f, "facet map")
+        assert digest(po["z"]) == gf["z"], (f, "z map")
+        assert digest(po["cose"]) == gf["cose"], (f, "cos(e) map")
+        assert digest(o["fits"][f]) == gf["fit"], (f, "fit image")
+        for k, v in gf["res"].items():
+            got = r[k]
+            if isinstance(v, list):
+                assert list(got) == v, (f, k, got, v)
+            else:
+                assert got == v, (f, k, got, v)
+    assert sum(r["chi2"] for r in o["results"]) == g["chi2"]
+    assert digest(o["seen"]) == g["seen"]
+    dof = sum(fr.dof for fr in ds.frames)
+    posbnd, plog, badradar, blog = _calc_fits_flags(o["results"], ds.frames, dof)
+    assert posbnd == g["flags"]["posbnd"] and badradar == g["flags"]["badradar"]
+    assert plog == g["flags"]["posbnd_logfactor"]
+    assert blog == g["flags"]["badradar_logfactor"]
+
+
+def test_config1_maps_match_arrays(orc):
+    m, ds_fn, params = synth.ellipsoid_model(), *gc.DELDOP_CASES["c1"][1:]
+    ds = ds_fn(lambda d, p: orc.eval_deldop(m, d, p)["fits"], params)
+    o = orc.eval_deldop(m, ds, params, keep_pos=True)
+    po = o["pos"][0]
+    cov = po["f"] >= 0
+    assert np.array_equal(po["f"].astype(np.int16), ARR["c1_f"])
+    assert np.array_equal(po["z"][cov], ARR["c1_z"])
+    assert np.array_equal(po["cose"][cov], ARR["c1_cose"])
+    assert np.array_equal(o["fits"][0], ARR["c1_fit"])
+
+
+@pytest.mark.parametrize("name", sorted(gc.LGHTCRV_CASES))
+def test_lightcurve_bit_exact(orc, name):
+    model_fn, ds_fn, params = gc.LGHTCRV_CASES[name]
+    g = GOLD["lghtcrv"][name]
+    m = model_fn()
+    ds = ds_fn(lambda d, p: orc.eval_lghtcrv(m, d, p)["y"], params)
+    assert digest(ds.obs) == g["obs"]
+    o = orc.eval_lghtcrv(m, ds, params, keep_pos=True)
+    assert o["y"].tolist() == g["y"]
+    assert o["fit"].tolist() == g["fit"]
+    assert o["cal"] == g["cal"] and o["chi2"] == g["chi2"]
+    for i, gp in enumerate(g["pos"]):
+        for k in ("z", "cose", "cosi", "f", "zill", "fill"):
+            assert digest(o["pos"][i][k]) == gp[k], (i, k)
+    assert digest(o["seen"]) == g["seen"]
+    assert all(ob == 0 for ob, _ in o["flags"]) == (g["flags"]["posbnd"] == 0)
+
+
+def test_spline_matches_reference_off_knots(orc):
+    """Natural spline between knots against the closed form for a cubic
+    with zero end curvature is hard to pin; instead check the defining
+    properties: interpolation at knots and C2 continuity."""
+    x = np.linspace(0.0, 1.0, 9) ** 1.3
+    y = np.sin(3 * x) + x
+    t = np.concatenate([x, (x[:-1] + x[1:]) / 2])
+    fit = orc.spline_fit(x, y, t)
+    assert np.array_equal(fit[:len(x)], y)
+    h = 1e-6
+    for xi in x[1:-1]:
+        d2l = (orc.spline_fit(x, y, [xi - 2 * h])[0] - 2 * orc.spline_fit(x, y, [xi - h])[0]
+               + orc.spline_fit(x, y, [xi])[0]) / h ** 2
+        d2r = (orc.spline_fit(x, y, [xi])[0] - 2 * orc.spline_fit(x, y, [xi + h])[0]
+               + orc.spline_fit(x, y, [xi + 2 * h])[0]) / h ** 2
+        assert abs(d2l - d2r) < 1e-2 * (1 + abs(d2l))
