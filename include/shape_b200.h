@@ -138,6 +138,64 @@ int shape_engine_get_tuning(shape_engine *e, int *out, int max);
 /* Device time of the last evaluation (CUDA events on the engine stream). */
 int shape_engine_last_time_ms(shape_engine *e, double *ms);
 
+/* ------------------------------------------------------------- bestfit */
+
+/* Free parameter kinds (src/shape/mkparlist.c:218-235). */
+#define SHAPE_PAR_SCALE 1      /* component scale factor index (SIZEPAR) */
+#define SHAPE_PAR_VERTEX_R 2   /* vertex deviation r of vertex index (SHAPEPAR) */
+
+/* One free parameter with its step and tolerances (par->fparstep,
+ * fpartol, fparabstol; e.g. length_step/length_tol/length_abstol). */
+typedef struct shape_fit_param {
+    int kind;
+    int index;
+    double step, tol, abstol;
+} shape_fit_param;
+
+typedef struct shape_fit_options {
+    int form;           /* SHAPE_FORM_* used for every trial evaluation */
+    double term_prec;   /* stop when the fractional decrease of an iteration < term_prec */
+    int term_maxiter;   /* 0 = no limit */
+} shape_fit_options;
+
+typedef struct shape_fit_result {
+    double initial_objective, final_objective;
+    int iterations, evaluations, trace_len;
+} shape_fit_result;
+
+/* The reference's bestfit (src/shape/bestfit.c:250-704) over the given free
+ * parameters, without penalties: per parameter, bracket a minimum of the
+ * objective starting from (value, value + step), then Brent-minimise it to
+ * tol*|x| + abstol, adopt the minimum, and iterate over all parameters
+ * until the objective's fractional decrease in an iteration is below
+ * term_prec. Each trial is one device evaluation (a graph replay in the
+ * batched forms). trace (optional, 2*trace_max doubles) receives the
+ * (parameter number, trial value) of every trial in order. */
+int shape_engine_bestfit(shape_engine *e, const shape_fit_param *params, int nparams,
+                         const shape_fit_options *opt, shape_fit_result *res, double *trace,
+                         int trace_max);
+int shape_engine_get_scale(shape_engine *e, int j, double *value);
+
+/* The two line searches of bestfit on a caller objective (host only, no
+ * device use): bracketing (src/nr/mnbrak.c) and Brent's minimiser with an
+ * absolute tolerance (src/nr/brent_abs.c). shape_brent_minimize returns the
+ * iteration count (>= 1) or a negative status. */
+typedef double (*shape_objective_fn)(double x, void *user);
+int shape_bracket_minimum(shape_objective_fn f, void *user, double *ax, double *bx, double *cx,
+                          double *fa, double *fb, double *fc);
+
+/* The same bestfit iteration on a caller objective (host only): values[k]
+ * is free parameter k; f returns the objective for the current values and
+ * sets *posbnd / *badradar for the flags of that evaluation. Lets a host
+ * program drive any objective (the reference's own calc_fits + chi2, or a
+ * multi-GPU reduction) with this fit loop. */
+typedef double (*shape_param_objective_fn)(const double *values, void *user, int *posbnd, int *badradar);
+int shape_bestfit_host(shape_param_objective_fn f, void *user, double *values,
+                       const shape_fit_param *params, int nparams, const shape_fit_options *opt,
+                       shape_fit_result *res, double *trace, int trace_max);
+int shape_brent_minimize(shape_objective_fn f, void *user, double ax, double bx, double cx,
+                         double tol, double abstol, double *xmin, double *fmin);
+
 /* Per-frame chi-square sums over images the CALLER already holds in device
  * memory, computed without allocating any device memory. It has no
  * counterpart in the reference: it exists for callers that cannot call

@@ -31,6 +31,7 @@ UNITS = [
     ("raster_f32.cu", []),
     ("engine.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
+    ("fit.cu", ["-fmad=false"]),
 ]
 
 HEADERS = ["engine_internal.h", "kernels.h", "raster_impl.cuh"]

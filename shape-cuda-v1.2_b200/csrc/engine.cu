@@ -962,6 +962,13 @@ int shape_engine_set_scale(shape_engine *h, int j, double value)
     return SHAPE_OK;
 }
 
+int shape_engine_get_scale(shape_engine *h, int j, double *value)
+{
+    if (!h || !value || j < 0 || j > 2) return shape::set_err(SHAPE_E_ARG, "get_scale: bad index");
+    *value = h->impl.scale[j];
+    return SHAPE_OK;
+}
+
 int shape_engine_set_vertex_r(shape_engine *h, int i, double value)
 {
     if (!h || i < 0 || i >= h->impl.nv) return shape::set_err(SHAPE_E_ARG, "set_vertex_r: bad index");

@@ -20,6 +20,24 @@ FORM_BATCHED_FP32 = 2
 FORMS = {"plain_fp64": 0, "batched_fp64": 1, "batched_fp32": 2}
 
 
+PAR_SCALE = 1
+PAR_VERTEX_R = 2
+
+
+class FitParam(C.Structure):
+    _fields_ = [("kind", C.c_int), ("index", C.c_int), ("step", C.c_double), ("tol", C.c_double),
+                ("abstol", C.c_double)]
+
+
+class FitOptions(C.Structure):
+    _fields_ = [("form", C.c_int), ("term_prec", C.c_double), ("term_maxiter", C.c_int)]
+
+
+class FitResult(C.Structure):
+    _fields_ = [("initial_objective", C.c_double), ("final_objective", C.c_double),
+                ("iterations", C.c_int), ("evaluations", C.c_int), ("trace_len", C.c_int)]
+
+
 class EvalSummary(C.Structure):
     _fields_ = [("chi2", C.c_double), ("dof", C.c_double), ("chi2_deldop", C.c_double),
                 ("chi2_lghtcrv", C.c_double), ("posbnd", C.c_int), ("posbnd_logfactor", C.c_double),
@@ -71,6 +89,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_stage_times.argtypes = [vp, C.c_int, cd.dptr, C.c_int]
     L.shape_engine_set_bin_capacity.argtypes = [vp, C.c_int]
     L.shape_engine_get_tuning.argtypes = [vp, P(C.c_int), C.c_int]
+    L.shape_engine_bestfit.argtypes = [vp, P(FitParam), C.c_int, P(FitOptions), P(FitResult), cd.dptr, C.c_int]
+    L.shape_engine_get_scale.argtypes = [vp, C.c_int, P(C.c_double)]
     L.shape_chi2_frames_noalloc.argtypes = [C.c_int, C.c_int, P(C.c_longlong), C.c_void_p, C.c_void_p,
                                             C.c_void_p, cd.dptr, cd.iptr, cd.dptr, cd.dptr]
     _lib = L
@@ -167,6 +187,31 @@ class Engine:
 
     def set_vertex_r(self, i, v):
         _chk(self.L.shape_engine_set_vertex_r(self.h, i, float(v)))
+
+    def get_scale(self, j):
+        v = C.c_double()
+        _chk(self.L.shape_engine_get_scale(self.h, j, C.byref(v)))
+        return v.value
+
+    def get_vertex_r(self, i):
+        v = C.c_double()
+        _chk(self.L.shape_engine_get_vertex_r(self.h, i, C.byref(v)))
+        return v.value
+
+    def bestfit(self, params, form=FORM_BATCHED_FP64, term_prec=1e-4, term_maxiter=0, trace_max=0):
+        """params: list of (kind, index, step, tol, abstol). Returns the
+        result dict and the trial trace [(param number, value), ...]."""
+        if isinstance(form, str):
+            form = FORMS[form]
+        arr = (FitParam * len(params))(*[FitParam(*t) for t in params])
+        opt = FitOptions(form, term_prec, term_maxiter)
+        res = FitResult()
+        tr = np.zeros(2 * max(1, trace_max))
+        _chk(self.L.shape_engine_bestfit(self.h, arr, len(params), C.byref(opt), C.byref(res),
+                                         cd.as_dptr(tr) if trace_max else None, trace_max))
+        out = {k: getattr(res, k) for k, _ in FitResult._fields_}
+        trace = [(int(tr[2 * i]), tr[2 * i + 1]) for i in range(res.trace_len)]
+        return out, trace
 
     def evaluate(self, form=FORM_PLAIN_FP64):
         if isinstance(form, str):

@@ -145,6 +145,47 @@ def main():
         out["linesearch"][name] = {"bracket": [a, b, c, fa, fb, fc], "n_mnbrak": n_mn,
                                    "trials": list(trials), "xmin": xmin, "fmin": fmin}
 
+    # config-1 fit with the reference's line searches and objective; the
+    # outer parameter loop follows src/shape/bestfit.c:367-651
+    m = synth.ellipsoid_model()
+    params = synth.eval_params()
+    ds = synth.config1_dataset(ref_deldop_synth(ref, m), params)
+    S = ref.session(m, params, deldops=[ds])
+    dof = sum(fr.dof for fr in ds.frames)
+    values = list(gc.FIT_START)
+    trace, state = [], {"flag": 0}
+
+    def objective():
+        for j in range(3):
+            ref.lib.ref_set_scale(S.h, j, values[j])
+        chi2 = S.evaluate()
+        fl = S.flags()
+        state["flag"] |= fl["posbnd"] | fl["badradar"]
+        return gc.objective_from(chi2, dof, fl)
+    enderr = objective()
+    start = enderr
+    it = 0
+    while True:
+        it += 1
+        beginerr = enderr
+        for k, (_, j, step, tol, abstol) in enumerate(gc.FIT_PARAMS):
+            def f(x, k=k, j=j):
+                values[j] = x
+                trace.append([k, x])
+                return objective()
+            state["flag"] = 0
+            cur = values[j]
+            a, b, c, fa, fb, fc = ref.mnbrak(f, cur, cur + step)
+            enderr, xmin = ref.brent_abs(f, a, b, c, tol, abstol)
+            values[j] = xmin
+            if state["flag"]:
+                objective()
+        if (beginerr - enderr) / enderr < gc.FIT_TERM_PREC or it >= gc.FIT_MAXITER:
+            break
+    out["bestfit_c1"] = {"trace": trace, "values": values, "initial": start, "final": enderr,
+                         "iterations": it, "obs": digest(ds.obs)}
+    S.close()
+
     with open(os.path.join(HERE, "reference_golden.json"), "w") as fh:
         json.dump(out, fh, indent=1, sort_keys=True)
     np.savez_compressed(os.path.join(HERE, "reference_arrays.npz"), **arrays)

@@ -58,6 +58,23 @@ LGHTCRV_CASES = {
 }
 
 
+# config-1 fit: the three scale factors from a 10% perturbation
+FIT_START = (1.10, 0.90, 1.10)
+FIT_PARAMS = [(1, j, 0.02, 1e-4, 1e-6) for j in range(3)]   # kind SCALE, index, step, tol, abstol
+FIT_TERM_PREC = 1e-4
+FIT_MAXITER = 3
+
+
+def objective_from(chi2, dof, flags, bad_objfactor=2.0):
+    """objective() of src/shape/bestfit.c:789-866 with no penalties."""
+    err = chi2 / dof
+    if flags["posbnd"]:
+        err *= bad_objfactor * math.exp(flags["posbnd_logfactor"])
+    if flags["badradar"]:
+        err *= bad_objfactor * math.exp(flags["badradar_logfactor"])
+    return err
+
+
 def _quad(x):
     return 3.0 * (x - 1.37) ** 2 + 0.5
 
