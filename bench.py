@@ -1,19 +1,29 @@
 """Benchmark of SHAPE's model-evaluation hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c1|c4] [--form batched_fp32|batched_fp64|plain_fp64]
+                    [--workload c2|c1|c3|c4] [--form batched_fp32|batched_fp64|plain_fp64]
+                    [--mode eval|sweep] [--no-serve] [--no-cpu-baseline]
 
 One step = one objective evaluation (realize_mod + calc_fits + chi2) of the
 workload after a bestfit-style trial change of a model parameter. Default
 workload: 64 delay-Doppler frames of uneven size (POS 101-301 px,
 64-256 x 64-512 delay-Doppler) of an 8000-facet vertex model, batched FP32
-form. Metric: frame-evals/s (one frame-eval = one delay-Doppler frame through
-raster -> synthesis -> chi-square), whole job over all ranks.
+form. Metric: frame-evals/s (one frame-eval = one delay-Doppler frame, or one
+lightcurve point, through raster -> synthesis/photometry -> chi-square),
+whole job over all ranks. The default run also replays the serving mix
+(config 5) through the continuous-batching server (`serving` key).
+
+Workloads: c1 one 100x100 frame of a 2300-facet ellipsoid; c2 the default;
+c3 four lightcurves of 200 points (two raster passes per point, shadowing);
+c4 16 frames of 511x511 POS / 256x256 delay-Doppler, 32768-facet model.
+--mode sweep (c4): one bestfit sweep over vertex-deviation parameters, each
+trial a graph replay; reports trials/s.
 
 Multi-GPU (torchrun, one rank per GPU): frames are independent given the
-model, so each rank evaluates its own 64-frame shard (weak scaling) and the
-per-rank chi-square totals are summed with one all-reduce of a few doubles
-per step (the exchange a sharded fit needs).
+model, so for c2 each rank evaluates its balanced block of a global dataset
+of 64 frames per rank (weak scaling), and the per-rank chi-square totals are
+summed with one all-reduce of a few doubles per step (the exchange a sharded
+fit needs). Other workloads run as replicas.
 
 --impl reference times the reference's own CPU code (oracle/_ref, built from
 the reference sources) on the same workload with all host cores, one dataset
@@ -39,34 +49,55 @@ from shape_b200 import synth  # noqa: E402
 
 L2_BYTES = 126 * 1024 * 1024
 
+# vertex-deviation step and tolerances of the config-4 sweep (length_step,
+# length_tol, length_abstol of the .par file; km and relative)
+SWEEP_STEP, SWEEP_TOL, SWEEP_ABSTOL = 0.01, 1e-3, 1e-5
 
-def workload(name, synthesize, params):
+
+def workload(name, dd_syn, lc_syn, params):
+    """(model, delay-Doppler datasets, lightcurve datasets, description)."""
     if name == "c1":
         m = synth.ellipsoid_model()
-        ds = synth.config1_dataset(synthesize(m), params)
-        desc = "config 1: one 100x100 delay-Doppler frame, POS 151x151, 2300-facet ellipsoid vertex model"
-    elif name == "c4":
-        m = synth.noisy_octa_model()
-        ds = synth.config4_dataset(synthesize(m), params)
-        desc = "config 4: 16 frames, POS 511x511, 256x256 delay-Doppler, 32768-facet vertex model"
-    else:
+        return m, [synth.config1_dataset(dd_syn(m), params)], [], \
+            "config 1: one 100x100 delay-Doppler frame, POS 151x151, 2300-facet ellipsoid vertex model"
+    if name == "c3":
         m = synth.harmonic_model()
-        ds = synth.config2_dataset(synthesize(m), params)
-        desc = ("config 2: 64 delay-Doppler frames, POS 101-301 px, 64-256 x 64-512 delay-Doppler, "
-                "8000-facet vertex model (sphere + degree-8 harmonics, 5% RMS)")
-    return m, ds, desc
+        return m, [], synth.config3_datasets(lc_syn(m), params), \
+            ("config 3: 4 lightcurves x 200 points, POS 129-257 px, solar phase 5-60 deg, "
+             "Kaasalainen (Lommel-Seeliger 0.7 + Lambert 0.3) law, shadowing; 8000-facet model")
+    if name == "c4":
+        m = synth.noisy_octa_model()
+        return m, [synth.config4_dataset(dd_syn(m), params)], [], \
+            "config 4: 16 frames, POS 511x511, 256x256 delay-Doppler, 32768-facet vertex model"
+    m = synth.harmonic_model()
+    return m, [synth.config2_dataset(dd_syn(m), params)], [], \
+        ("config 2: 64 delay-Doppler frames, POS 101-301 px, 64-256 x 64-512 delay-Doppler, "
+         "8000-facet vertex model (sphere + degree-8 harmonics, 5% RMS)")
 
 
-def algorithmic_bytes(model, ds, s):
+def units(dds, lcs):
+    return sum(d.nframes for d in dds) + sum(len(l.points) for l in lcs)
+
+
+def algorithmic_bytes(model, dds, lcs, s):
     """Bytes per evaluation by the hot-path byte model: element size s (8 FP64,
     4 FP32); obs and 1/var at 8 B each in both forms.
       model:  nv*6s + nf*(12 + 3s)
       frame:  POS  P*(8+s)*2   (depth/facet word + cos(e), written and read once)
-              dd   D*(2s+16)   (fit written and read, obs and 1/var read)"""
+              dd   D*(2s+16)   (fit written and read, obs and 1/var read)
+      point:  P*(32+4s)        (observer and sun views, mask, photometry)
+    Returns (model, POS part, delay-Doppler part, the raster kernel's share)."""
     b_model = model.nv * 6 * s + model.nf * (12 + 3 * s)
-    b_pos = sum((2 * f.pos_n + 1) ** 2 * (8 + s) * 2 for f in ds.frames)
-    b_dd = sum(f.ndel * f.ndop * (2 * s + 16) for f in ds.frames)
-    return b_model, b_pos, b_dd
+    frames = [f for d in dds for f in d.frames]
+    pts = [p for l in lcs for p in l.points]
+    b_pos = sum((2 * f.pos_n + 1) ** 2 * (8 + s) * 2 for f in frames)
+    b_pt = sum((2 * p.pos_n + 1) ** 2 * (32 + 4 * s) for p in pts)
+    b_dd = sum(f.ndel * f.ndop * (2 * s + 16) for f in frames)
+    # the fused raster reads the model, produces the POS words and cos(e) and
+    # writes the fit images; for lightcurves it writes both views' maps (half
+    # of the per-point figure; the photometry kernel reads them)
+    raster = b_model + b_pos + sum(f.ndel * f.ndop * s for f in frames) + b_pt // 2
+    return b_model, b_pos + b_pt, b_dd, raster
 
 
 class ClockSampler:
@@ -127,24 +158,45 @@ def dist_setup():
     from datetime import timedelta
     os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
     rank, lrank = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
-    backend = "nccl"
     import torch
     torch.cuda.set_device(lrank)
-    dist.init_process_group(backend, timeout=timedelta(seconds=120),
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                             device_id=torch.device("cuda", lrank))
     return rank, ws, lrank, dist
 
 
+def peak_hbm():
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
 # ------------------------------------------------------------ reference arm
 
-def run_reference(args, rank, ws):
-    if rank != 0:
-        return 0
-    from oracle.bindings import Reference
-    ref = Reference()
-    params = synth.eval_params()
+def ref_sessions(ref, model, params, dds, lcs, nthreads):
+    """The workload split the way the reference's host multithreading splits
+    it (one dataset per thread): frames of a delay-Doppler set in contiguous
+    shards, lightcurve sets one per session."""
+    sessions = []
+    for ds in dds:
+        shards = np.array_split(np.arange(ds.nframes), max(1, min(nthreads, ds.nframes)))
+        for sh in shards:
+            sub = synth.DeldopDataset(ds.set, [ds.frames[i] for i in sh],
+                                      np.concatenate([ds.frame_obs(i) for i in sh]),
+                                      np.concatenate([ds.oneovervar[ds.offsets[i]:ds.offsets[i + 1]]
+                                                      for i in sh]), None)
+            sub.offsets = np.concatenate([[0], np.cumsum([ds.frames[i].ndel * ds.frames[i].ndop
+                                                          for i in sh])])
+            sessions.append(ref.session(model, params, deldops=[sub]))
+    for ls in lcs:
+        sessions.append(ref.session(model, params, lghtcrvs=[ls]))
+    return sessions
 
-    def ref_synth(model):
+
+def ref_synthesizers(ref):
+    def dd(model):
         def f(ds, p):
             S = ref.session(model, p, deldops=[ds])
             S.evaluate()
@@ -152,20 +204,30 @@ def run_reference(args, rank, ws):
             S.close()
             return out
         return f
-    model, ds, desc = workload(args.workload, ref_synth, params)
-    cores = os.cpu_count() or 1
-    nthreads = min(cores, ds.nframes)
-    # one dataset shard per thread (host multithreading: one set per thread)
-    shards = np.array_split(np.arange(ds.nframes), nthreads)
-    sessions = []
-    for sh in shards:
-        sub = synth.DeldopDataset(ds.set, [ds.frames[i] for i in sh],
-                                  np.concatenate([ds.frame_obs(i) for i in sh]),
-                                  np.concatenate([ds.oneovervar[ds.offsets[i]:ds.offsets[i + 1]] for i in sh]),
-                                  None)
-        sub.offsets = np.concatenate([[0], np.cumsum([ds.frames[i].ndel * ds.frames[i].ndop for i in sh])])
-        sessions.append(ref.session(model, params, deldops=[sub]))
+
+    def lc(model):
+        def f(ds, p):
+            S = ref.session(model, p, lghtcrvs=[ds])
+            S.evaluate()
+            y = S.lghtcrv(0, ds)["y"]
+            S.close()
+            return y
+        return f
+    return dd, lc
+
+
+def run_reference(args, rank, ws):
+    if rank != 0:
+        return 0
     import ctypes as C
+    from oracle.bindings import Reference
+    ref = Reference()
+    params = synth.eval_params()
+    dd_syn, lc_syn = ref_synthesizers(ref)
+    model, dds, lcs, desc = workload(args.workload, dd_syn, lc_syn, params)
+    nu = units(dds, lcs)
+    cores = os.cpu_count() or 1
+    sessions = ref_sessions(ref, model, params, dds, lcs, cores)
     arr = (C.c_void_p * len(sessions))(*[s.h for s in sessions])
     for _ in range(args.warmup):
         ref.lib.ref_evaluate_mt(arr, len(sessions))
@@ -175,16 +237,17 @@ def run_reference(args, rank, ws):
         ref.lib.ref_evaluate_mt(arr, len(sessions))
         times.append(time.perf_counter() - t0)
     ms = 1e3 * statistics.mean(times)
-    value = ds.nframes / (ms / 1e3)
+    value = nu / (ms / 1e3)
+    threads = min(cores, len(sessions))
     line = {
         "impl": "reference", "metric": "frame-evals/sec", "value": value, "unit": "frame-evals/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": desc, "form": "reference CPU (calc_fits + chi2 per step)",
-                   "threads": nthreads, "frames": ds.nframes},
-        "cpu_baseline": {"value": value, "unit": "frame-evals/s", "cores": nthreads, "kind": "reference",
-                         "sample": "%d full evaluations of the %d-frame workload" % (args.steps, ds.nframes)},
+                   "threads": threads, "sessions": len(sessions), "frame_evals_per_step": nu},
+        "cpu_baseline": {"value": value, "unit": "frame-evals/s", "cores": threads, "kind": "reference",
+                         "sample": "%d full evaluations of the %d-unit workload" % (args.steps, nu)},
         "e2e": {"value": value, "unit": "frame-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "p50_ms": 1e3 * statistics.median(times), "p99_ms": 1e3 * float(np.percentile(times, 99)),
     }
@@ -194,9 +257,9 @@ def run_reference(args, rank, ws):
     return 0
 
 
-def cpu_baseline(model, ds, params, budget_s=15.0):
+def cpu_baseline(model, dds, lcs, params, budget_s=15.0):
     """Reference CPU code (oracle/_ref) on the host cores, bounded sample:
-    single-thread frames, then all cores with one frame shard per thread."""
+    all cores with one dataset shard per thread, then a single thread."""
     try:
         from oracle.bindings import Reference
         ref = Reference()
@@ -204,17 +267,9 @@ def cpu_baseline(model, ds, params, budget_s=15.0):
         return {"value": None, "unit": "frame-evals/s", "cores": 0, "kind": "reference",
                 "sample": "unavailable: %s" % exc}
     import ctypes as C
+    nu = units(dds, lcs)
     cores = os.cpu_count() or 1
-    nthreads = min(cores, ds.nframes)
-    shards = np.array_split(np.arange(ds.nframes), nthreads)
-    sessions = []
-    for sh in shards:
-        sub = synth.DeldopDataset(ds.set, [ds.frames[i] for i in sh],
-                                  np.concatenate([ds.frame_obs(i) for i in sh]),
-                                  np.concatenate([ds.oneovervar[ds.offsets[i]:ds.offsets[i + 1]] for i in sh]),
-                                  None)
-        sub.offsets = np.concatenate([[0], np.cumsum([ds.frames[i].ndel * ds.frames[i].ndop for i in sh])])
-        sessions.append(ref.session(model, params, deldops=[sub]))
+    sessions = ref_sessions(ref, model, params, dds, lcs, cores)
     arr = (C.c_void_p * len(sessions))(*[s.h for s in sessions])
     ref.lib.ref_evaluate_mt(arr, len(sessions))
     reps, t_all = 0, 0.0
@@ -223,8 +278,7 @@ def cpu_baseline(model, ds, params, budget_s=15.0):
         ref.lib.ref_evaluate_mt(arr, len(sessions))
         t_all += time.perf_counter() - t0
         reps += 1
-    # single thread: one full-workload session, a few evaluations
-    S1 = ref.session(model, params, deldops=[ds])
+    S1 = ref.session(model, params, deldops=dds, lghtcrvs=lcs)
     S1.evaluate()
     r1, t1 = 0, 0.0
     while t1 < budget_s / 3 and r1 < 20:
@@ -235,14 +289,137 @@ def cpu_baseline(model, ds, params, budget_s=15.0):
     S1.close()
     for s in sessions:
         s.close()
-    return {"value": ds.nframes * reps / t_all, "unit": "frame-evals/s", "cores": nthreads,
-            "kind": "reference",
-            "sample": "%d evaluations of the %d-frame workload on %d threads (one frame shard per thread)"
-                      % (reps, ds.nframes, nthreads),
-            "single_thread_value": ds.nframes * r1 / t1}
+    threads = min(cores, len(sessions))
+    return {"value": nu * reps / t_all, "unit": "frame-evals/s", "cores": threads, "kind": "reference",
+            "sample": "%d evaluations of the %d-unit workload on %d threads (one dataset shard per thread)"
+                      % (reps, nu, threads),
+            "single_thread_value": nu * r1 / t1}
 
 
 # ----------------------------------------------------------------- our arm
+
+def serving_bench(lrank, nreq=4000, rate=2000.0, budget=64 << 30, slots=16):
+    """The serving mix: a seeded Poisson stream of `rate` requests/s over the
+    config-1..4 workloads (one workload per frame count), replayed through
+    the continuous-batching server in the batched FP32 and FP64 forms. A first
+    pass of the trace warms the instances; the second is reported. The
+    offered rate saturates the GPU, so a second trace at 60% of the FP32
+    form's served rate gives the latencies of an unsaturated server."""
+    from shape_b200 import engine as eng
+    params = synth.eval_params()
+    cats, work = synth.serving_mix(lambda m: eng.engine_synthesizer(m, lrank)[0],
+                                   lambda m: eng.engine_synthesizer(m, lrank)[1], params)
+    trace = synth.serving_trace(cats, nreq, rate, seed=2026)
+    cat_of = {}
+    for c, ws_ in zip(("c1", "c2", "c3", "c4"), cats):
+        for w in ws_:
+            cat_of[w] = c
+    out, chi = {}, {}
+    sus_rate = None
+
+    def stats(st):
+        return {"frame_evals_per_s": st["frame_evals_per_s"], "requests_per_s": st["requests_per_s"],
+                "p50_latency_ms": 1e3 * st["p50_latency_s"], "p99_latency_ms": 1e3 * st["p99_latency_s"],
+                "mean_concurrency": st["mean_concurrency"], "peak_concurrency": st["peak_concurrency"],
+                "instances_created_in_run": st["instances_created"],
+                "instances_evicted_in_run": st["instances_evicted"],
+                "peak_hbm_gb": st["peak_hbm_bytes"] / 1e9}
+
+    for name, form in (("fp32", eng.FORM_BATCHED_FP32), ("fp64", eng.FORM_BATCHED_FP64)):
+        srv = eng.Server(lrank, budget, slots)
+        t0 = time.perf_counter()
+        eng.register_workloads(srv, work, params, form, lrank)
+        t_reg = time.perf_counter() - t0
+        srv.run(trace)
+        res, st = srv.run(trace)
+        chi[name] = np.array([r["chi2"] for r in res])
+        out[name] = {"offered": stats(st), "registration_s": t_reg}
+        if sus_rate is None:
+            sus_rate = 0.6 * st["requests_per_s"]
+        tr2 = synth.serving_trace(cats, int(sus_rate * 3.0), sus_rate, seed=2027)
+        srv.run(tr2[: min(len(tr2), 200)])
+        _, st2 = srv.run(tr2)
+        out[name]["sustainable"] = stats(st2)
+        srv.close()
+    out["workloads"] = len(work)
+    out["requests"] = nreq
+    out["offered_rate_req_per_s"] = rate
+    out["sustainable_rate_req_per_s"] = sus_rate
+    out["max_slots"], out["hbm_budget_gb"] = slots, budget / 1e9
+    rel = np.abs(chi["fp32"] - chi["fp64"]) / np.abs(chi["fp64"])
+    out["max_dchi2_rel_fp32_vs_fp64"] = {c: float(max([rel[i] for i, (w, _, _) in enumerate(trace)
+                                                       if cat_of[w] == c] or [0.0]))
+                                         for c in ("c1", "c2", "c3", "c4")}
+    return out
+
+
+def sweep_bench(args, lrank):
+    """Config 4: one bestfit sweep over the first args.params vertex-deviation
+    parameters (each trial a graph replay), and the reference CPU code on the
+    first few parameters of the same sweep."""
+    from shape_b200 import engine as eng
+    params = synth.eval_params()
+    dd_syn = lambda m: eng.engine_synthesizer(m, lrank)[0]
+    model, dds, lcs, desc = workload("c4", dd_syn, None, params)
+    form = eng.FORMS[args.form]
+    E = eng.make_engine(model, params, deldops=dds, device=lrank)
+    E.evaluate(form)
+    fit_params = [(eng.PAR_VERTEX_R, i, SWEEP_STEP, SWEEP_TOL, SWEEP_ABSTOL) for i in range(args.params)]
+    clocks = ClockSampler(lrank)
+    clocks.start()
+    t0 = time.perf_counter()
+    res, _ = E.bestfit(fit_params, form=form, term_prec=1e-4, term_maxiter=1)
+    dt = time.perf_counter() - t0
+    clk = clocks.stop()
+    E.close()
+    nfr = dds[0].nframes
+    line = {
+        "metric": "vertex-sweep trials/sec", "value": res["evaluations"] / dt, "unit": "trials/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32" if form == eng.FORM_BATCHED_FP32 else "f64",
+        "data": "synthetic",
+        "config": {"workload": desc + "; one bestfit sweep over %d vertex deviations" % args.params,
+                   "form": args.form, "step_tol_abstol": [SWEEP_STEP, SWEEP_TOL, SWEEP_ABSTOL]},
+        "trials": res["evaluations"], "seconds": dt, "ms_per_trial": 1e3 * dt / res["evaluations"],
+        "frame_evals_per_s": res["evaluations"] * nfr / dt,
+        "objective": [res["initial_objective"], res["final_objective"]],
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = sweep_cpu(model, dds, params, k=5)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def sweep_cpu(model, dds, params, k=5):
+    """The same sweep on the reference CPU code for the first k parameters
+    (host bestfit loop over the reference's realize_mod + calc_fits + chi2,
+    all cores, one frame shard per thread)."""
+    import ctypes as C
+    from oracle.bindings import Reference
+    from shape_b200 import engine as eng
+    ref = Reference()
+    sessions = ref_sessions(ref, model, params, dds, [], os.cpu_count() or 1)
+    arr = (C.c_void_p * len(sessions))(*[s.h for s in sessions])
+    dof = sum(f.dof for f in dds[0].frames)
+    vals = np.array([model.r[i] for i in range(k)], dtype=np.float64)
+    count = [0]
+
+    def objective(v):
+        for i in range(k):
+            for s in sessions:
+                ref.lib.ref_set_r(s.h, i, float(v[i]))
+        chi2 = ref.lib.ref_evaluate_mt(arr, len(sessions))
+        count[0] += 1
+        return chi2 / dof, 0, 0
+    fit_params = [(eng.PAR_VERTEX_R, i, SWEEP_STEP, SWEEP_TOL, SWEEP_ABSTOL) for i in range(k)]
+    t0 = time.perf_counter()
+    eng.bestfit_host(objective, vals, fit_params, term_prec=1e-4, term_maxiter=1)
+    dt = time.perf_counter() - t0
+    for s in sessions:
+        s.close()
+    return {"value": count[0] / dt, "unit": "trials/s", "cores": min(os.cpu_count() or 1, len(sessions)),
+            "kind": "reference", "sample": "first %d parameters of the sweep: %d trials" % (k, count[0])}
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -250,9 +427,12 @@ def main():
     ap.add_argument("--steps", type=int, default=600)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c4"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--form", default="batched_fp32", choices=["batched_fp32", "batched_fp64", "plain_fp64"])
+    ap.add_argument("--mode", default="eval", choices=["eval", "sweep"])
+    ap.add_argument("--params", type=int, default=2000, help="vertex parameters of the sweep mode")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-mix measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, ws, lrank, dist = dist_setup()
@@ -265,12 +445,23 @@ def main():
     import torch
     from shape_b200 import engine as eng
     torch.cuda.set_device(lrank)
+    if args.mode == "sweep":
+        return sweep_bench(args, lrank)
     params = synth.eval_params()
-    dd_synth = lambda m: eng.engine_synthesizer(m, lrank)[0]
-    model, ds, desc = workload(args.workload, dd_synth, params)
-    E = eng.make_engine(model, params, deldops=[ds], device=lrank)
+    dd_syn = lambda m: eng.engine_synthesizer(m, lrank)[0]
+    lc_syn = lambda m: eng.engine_synthesizer(m, lrank)[1]
+    model, dds, lcs, desc = workload(args.workload, dd_syn, lc_syn, params)
+    if ws > 1 and args.workload == "c2":
+        # weak scaling: a global dataset of 64 frames per rank with the
+        # config-2 distributions, each rank evaluating its balanced block
+        from shape_b200 import shard
+        glob = synth.batched_dataset(64 * ws, (101, 301), (64, 256), (64, 512), dd_syn(model), params,
+                                     seed=7)
+        dds = [shard.shard_dataset(glob, rank, ws)[0]]
+        desc += "; %d frames in all, frame blocks balanced by POS + delay-Doppler pixels" % (64 * ws)
+    E = eng.make_engine(model, params, deldops=dds, lghtcrvs=lcs, device=lrank)
     form = eng.FORMS[args.form]
-    nfr = ds.nframes
+    nu = units(dds, lcs)
     flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device="cuda")
     trial = lambda k: 1.0 + 1e-3 * math.sin(0.7 * k)
 
@@ -279,6 +470,9 @@ def main():
     chi64 = E.evaluate(eng.FORM_BATCHED_FP64)["chi2"]
     chi32 = E.evaluate(eng.FORM_BATCHED_FP32)["chi2"]
     dchi = abs(chi32 - chi64) / abs(chi64)
+
+    ev_a = torch.cuda.Event(enable_timing=True)
+    ev_b = torch.cuda.Event(enable_timing=True)
 
     def run(form_id, steps, warm, record):
         dev_ms, host_ms = [], []
@@ -293,12 +487,18 @@ def main():
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             E.set_scale(0, trial(k + warm))
-            E.evaluate(form_id)
-            host_ms.append(1e3 * (time.perf_counter() - t0))
-            dev_ms.append(E.last_ms())
+            summ = E.evaluate(form_id)
+            step_ms = E.last_ms()
             if dist and record:
-                t = torch.tensor([dev_ms[-1]], dtype=torch.float64, device="cuda")
-                dist.all_reduce(t)   # per-step exchange of the shard totals
+                # the step's one exchange: the sum of the ranks' chi-square totals
+                from shape_b200 import shard
+                ev_a.record()
+                shard.allreduce_summary(summ, dist, device="cuda")
+                ev_b.record()
+                ev_b.synchronize()
+                step_ms += ev_a.elapsed_time(ev_b)
+            host_ms.append(1e3 * (time.perf_counter() - t0))
+            dev_ms.append(step_ms)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -311,34 +511,32 @@ def main():
     time.sleep(0.3)
     dev_ms, host_ms = run(form, args.steps, args.warmup, True)
     clk = clocks.stop()
+    kpe = E.kernels_per_eval(form)
     stages = E.stage_times(form if form != eng.FORM_PLAIN_FP64 else eng.FORM_BATCHED_FP64)
 
     total_dev = sum(dev_ms)
     total_host = sum(host_ms)
+    units_all = ws * nu
     if dist:
         t = torch.tensor([total_dev, total_host], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_dev, total_host = t.tolist()
+        t = torch.tensor([float(nu)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        units_all = int(t.item())
     ms_step = total_dev / args.steps
-    value = ws * nfr / (ms_step / 1e3)
-    e2e = ws * nfr / (total_host / args.steps / 1e3)
-    plain_rate = nfr / (statistics.mean(plain_dev) / 1e3)
+    value = units_all / (ms_step / 1e3)
+    e2e = units_all / (total_host / args.steps / 1e3)
+    plain_rate = nu / (statistics.mean(plain_dev) / 1e3)
 
     s_elem = 4 if form == eng.FORM_BATCHED_FP32 else 8
-    b_model, b_pos, b_dd = algorithmic_bytes(model, ds, s_elem)
-    peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
-    try:
-        peaks = json.load(open(peaks_path))
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
-    except Exception:
-        peak, peak_src = 6650.0, "fallback"
-    # dominant kernel: the fused tile raster + delay-Doppler synthesis
+    b_model, b_pos, b_dd, rs_bytes = algorithmic_bytes(model, dds, lcs, s_elem)
+    peak, peak_src = peak_hbm()
+    # dominant kernel: the fused tile raster (+ delay-Doppler synthesis)
     rs_ms = stages.get("raster_synth", float("nan"))
-    d_elems = sum(f.ndel * f.ndop for f in ds.frames)
-    rs_bytes = b_model + b_pos + d_elems * s_elem     # model read, POS word+cos(e), fit write
     achieved = rs_bytes / (rs_ms / 1e3) / 1e9
-    traffic_path = os.path.join(REPO, "profiles", "raster_traffic.json")
     traffic = None
+    traffic_path = os.path.join(REPO, "profiles", "raster_traffic.json")
     if os.path.exists(traffic_path):
         try:
             traffic = json.load(open(traffic_path)).get(args.workload + "_" + args.form)
@@ -350,7 +548,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if form == eng.FORM_BATCHED_FP32 else "f64", "data": "synthetic",
-        "config": {"workload": desc, "form": args.form, "frames_per_gpu": nfr,
+        "config": {"workload": desc, "form": args.form, "frame_evals_per_gpu": nu,
+                   "frame_evals_total": units_all,
                    "model_facets": model.nf, "l2": "flushed (2x L2 buffer written) before every step",
                    "parallelism": "frame shards, one per GPU" if ws > 1 else "single GPU",
                    "dchi2_rel_fp32_vs_fp64": dchi,
@@ -368,12 +567,14 @@ def main():
                 "d2h_bytes_per_step": 72,
                 "what": "shape_engine_evaluate through the C ABI per bestfit trial: model parameters "
                         "host->device, chi-square summary device->host, host wall clock"},
-        "gpu_launches": 10 * args.steps if form != eng.FORM_PLAIN_FP64 else None,
+        "gpu_launches": kpe * args.steps,
         "clocks": clk,
     }
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(model, ds, params)
     E.close()
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(model, dds, lcs, params)
+    if ws == 1 and not args.no_serve and args.workload == "c2":
+        line["serving"] = serving_bench(lrank)
     if dist:
         dist.destroy_process_group()
     if rank == 0:

@@ -135,6 +135,9 @@ int shape_engine_set_bin_capacity(shape_engine *e, int cap);
  * Returns the number of values written. */
 int shape_engine_get_tuning(shape_engine *e, int *out, int max);
 
+/* Number of kernel launches one evaluation in `form` makes (after finalize). */
+int shape_engine_kernels_per_eval(shape_engine *e, int form, int *count);
+
 /* Device time of the last evaluation (CUDA events on the engine stream). */
 int shape_engine_last_time_ms(shape_engine *e, double *ms);
 
@@ -218,6 +221,54 @@ int shape_chi2_frames_noalloc(int device, int nframes, const long long *frame_of
                               const double *d_obs, const double *d_oneovervar,
                               const double *d_fit, const double *weight,
                               const int *cal_floating, const double *cal, double *out);
+
+/* Continuous-batching evaluation server (one device). It has no counterpart
+ * in the reference, whose fits evaluate one model at a time in one process;
+ * it serves many fits (workloads) from one GPU. A workload is the host
+ * description of a configured engine (model, switches, datasets), copied at
+ * registration. The server keeps device-resident instances of workloads, at
+ * most hbm_budget_bytes of device memory in total, and runs up to max_slots
+ * requests at once, each on its instance's stream. shape_server_run replays
+ * a request trace: each request is admitted, in arrival order, once its
+ * arrival time (seconds after the call starts) has passed, a slot is free
+ * and an idle instance of its workload exists or fits in the budget (idle
+ * instances of other workloads are evicted, least recently used first, to
+ * make room). A request evaluates its workload at its own scale factors;
+ * its result is the same as a lone shape_engine_evaluate of that workload at
+ * those scale factors. */
+typedef struct shape_server shape_server;
+typedef struct shape_request {
+    int workload;              /* index returned by shape_server_add_workload */
+    double arrival_s;          /* seconds after shape_server_run starts */
+    double scale[3];           /* ellipsoid scale factors of this request */
+} shape_request;
+typedef struct shape_request_result {
+    double chi2, objective;
+    double t_start, t_done;    /* seconds after shape_server_run starts */
+    double latency_s;          /* t_done - arrival_s */
+    double device_ms;          /* event time of the request's evaluation */
+    int instance;              /* instance slot that served it */
+} shape_request_result;
+typedef struct shape_server_stats {
+    double span_s;             /* first arrival window start to last completion */
+    double requests_per_s;
+    double frame_evals_per_s;  /* radar frames + lightcurve points evaluated per second */
+    double p50_latency_s, p99_latency_s;
+    double mean_concurrency;   /* time-averaged requests in flight */
+    int peak_concurrency;
+    int instances_created, instances_evicted;
+    double peak_hbm_bytes;     /* peak device bytes held by instances during the run */
+} shape_server_stats;
+int shape_server_create(int device, size_t hbm_budget_bytes, int max_slots, shape_server **out);
+void shape_server_destroy(shape_server *s);
+/* engine: a configured engine (model and datasets added; it need not be
+ * finalized). form: SHAPE_FORM_*. Returns the workload index (>= 0) or a
+ * negative status. */
+int shape_server_add_workload(shape_server *s, shape_engine *engine, int form);
+/* Device bytes one instance of workload w holds (0 before its first instance). */
+int shape_server_workload_bytes(shape_server *s, int w, size_t *bytes);
+int shape_server_run(shape_server *s, const shape_request *req, int n, shape_request_result *res,
+                     shape_server_stats *stats);
 
 #ifdef __cplusplus
 }

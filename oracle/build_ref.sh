@@ -25,7 +25,7 @@ if [ ! -d "$SRC/shape" ]; then
     exit 2
 fi
 mkdir -p "$OBJ"
-INC="-I$SRC/shape -I$SRC/util -I$SRC/nr -I$SRC/astro -I$SRC/pgm -I$SRC/HostMultiThreading -I/usr/local/cuda/include -I$REPO/include"
+INC="-I$SRC/shape -I$SRC/util -I$SRC/nr -I$SRC/astro -I$SRC/pgm -I$SRC/HostMultiThreading -I/usr/local/cuda/include -I$REPO/include -I$HERE"
 objs=()
 for d in shape util nr astro pgm HostMultiThreading; do
     for f in "$SRC/$d"/*.c; do
@@ -41,5 +41,5 @@ done
 $CC $CFLAGS -c "$HERE/refstubs.c" -o "$OBJ/refstubs.o"
 $CC $CFLAGS -c -I- -I"$HERE/refshim/shape" $INC "$HERE/ref_harness.c" -o "$OBJ/ref_harness.o" 2>&1 | grep -v "obsolete option" || true
 $CC -shared -o "$OUT/libshape_ref.so" "${objs[@]}" "$OBJ/refstubs.o" "$OBJ/ref_harness.o" \
-    -lm -lpthread -Wl,--no-undefined
+    -lm -lpthread -Wl,-soname,libshape_ref.so -Wl,--no-undefined
 echo "built $OUT/libshape_ref.so"

@@ -17,13 +17,7 @@
 #include "head.h"
 
 #include "shape_types.h"
-
-typedef struct ref_session {
-    struct par_t par;
-    struct mod_t mod;
-    struct dat_t dat;
-    int nsets_cap;
-} ref_session;
+#include "ref_session.h"
 
 static void ref_alloc_pos(struct pos_t *pos, int n, double kmpp, int bistatic)
 {

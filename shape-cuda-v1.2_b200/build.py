@@ -32,9 +32,10 @@ UNITS = [
     ("engine.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
     ("fit.cu", ["-fmad=false"]),
+    ("server.cu", ["-fmad=false"]),
 ]
 
-HEADERS = ["engine_internal.h", "kernels.h", "raster_impl.cuh"]
+HEADERS = ["engine_internal.h", "engine_impl.h", "kernels.h", "raster_impl.cuh"]
 
 
 def _newer(src_list, target):
@@ -61,7 +62,8 @@ def build(force=False, verbose=False):
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
     if force or _newer(objs, LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread",
+                                                                   "-Xlinker", "-soname=libshape_b200.so"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

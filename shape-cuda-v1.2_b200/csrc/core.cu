@@ -293,10 +293,8 @@ __global__ void k_chi2_partials(Chi2Args a)
 
 // Per-frame results: chi2_deldop's calibration and chi-square
 // (src/shape/chi2.c:447-460) plus the posvis / pos2deldop frame outputs.
-__global__ void k_finalize_frames(FinalizeArgs a)
+__device__ void finalize_frame(const FinalizeArgs &a, int fr)
 {
-    int fr = blockIdx.x * blockDim.x + threadIdx.x;
-    if (fr >= a.nframes) return;
     const FrameHost &h = a.fh[fr];
     const FrameGeom &g = a.geoms[h.view];
     const FrameState &st = a.states[h.view];
@@ -347,6 +345,12 @@ __global__ void k_finalize_frames(FinalizeArgs a)
     r.doplim[0] = (pl0 - g.dopshift) * fpp - a.dop_extra[fr];
     r.doplim[1] = (pl1 - g.dopshift) * fpp + a.dop_extra[fr];
     a.results[fr] = r;
+}
+
+__global__ void k_finalize_frames(FinalizeArgs a)
+{
+    int fr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (fr < a.nframes) finalize_frame(a, fr);
 }
 
 // ------------------------------------------------------------ lightcurves
@@ -514,30 +518,70 @@ __device__ double splint_dev(const double *x, const double *y, const double *y2,
 // One block per lightcurve set: y from brightness partials, spline to the
 // observation epochs, chi2_lghtcrv (src/shape/chi2.c:1125-1170), posbnd sum
 // (src/shape/calc_fits.c:1651-1679, 1947).
+//
+// The recurrences (spline elimination, the chi-square sums, the log-factor
+// sum) stay serial in the reference's order, so results are bit-identical to
+// it; when a.smem_per_set > 0 their operands are first gathered into shared
+// memory by the whole block, so the serial loops run at shared-memory latency
+// instead of one global round trip per step.
 __global__ void k_lc_finalize(LcFinalizeArgs a)
 {
+    extern __shared__ double lsm[];
     const LcSetDev &S = a.sets[blockIdx.x];
-    for (int k = threadIdx.x; k < S.npts; k += blockDim.x) {
+    const int np = S.npts, n = S.n;
+    const bool use_sm = a.smem_per_set > 0;
+    // shared layout: x y y2 cp [np] | t obs oov fit [n] | lo ls [np] (doubles), flags [np] (int)
+    double *x = use_sm ? lsm : const_cast<double *>(S.x);
+    double *y = use_sm ? lsm + np : S.y;
+    double *y2 = use_sm ? lsm + 2 * np : S.y2;
+    double *cp = use_sm ? lsm + 3 * np : S.fit + n;       // global path: fit tail is scratch
+    double *tt = use_sm ? lsm + 4 * np : const_cast<double *>(S.t);
+    double *obs = use_sm ? tt + n : const_cast<double *>(S.obs);
+    double *oov = use_sm ? tt + 2 * n : const_cast<double *>(S.oov);
+    double *fit = use_sm ? tt + 3 * n : S.fit;
+    double *lo = tt + 4 * n, *ls = lo + np;
+    int *pflag = reinterpret_cast<int *>(ls + np);
+    for (int k = threadIdx.x; k < np; k += blockDim.x) {
         int pt = S.pt0 + k;
         int it0 = a.pt_items[2 * pt], cnt = a.pt_items[2 * pt + 1];
-        double s = 0.0;
-        for (int it = it0; it < it0 + cnt; it++) s += a.partials[it];
-        S.y[k] = (s == 0.0) ? 1.0e-40 : s;
+        double sum = 0.0;
+        for (int it = it0; it < it0 + cnt; it++) sum += a.partials[it];
+        sum = (sum == 0.0) ? 1.0e-40 : sum;
+        y[k] = sum;
+        if (use_sm) {
+            S.y[k] = sum;
+            x[k] = S.x[k];
+            // per-point posbnd log-factor terms, summed serially below
+            const LcPointDev &P = a.pts[pt];
+            const FrameState &so = a.states[P.obs_view], &ss = a.states[P.sun_view];
+            lo[k] = so.outbnd ? 0.5 * view_logfactor(a.geoms[P.obs_view], so) : 0.0;
+            ls[k] = ss.outbnd ? 0.5 * view_logfactor(a.geoms[P.sun_view], ss) : 0.0;
+            pflag[k] = (so.outbnd ? 1 : 0) | (ss.outbnd ? 2 : 0);
+        }
     }
+    if (use_sm)
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            tt[k] = S.t[k];
+            obs[k] = S.obs[k];
+            oov[k] = S.oov[k];
+        }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        spline_natural_dev(S.x, S.y, S.npts, S.y2, S.fit + S.n);   // fit tail is scratch
+    if (threadIdx.x == 0) spline_natural_dev(x, y, np, y2, cp);
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double v = splint_dev(x, y, y2, np, tt[k]) / 1;
+        fit[k] = v;
+        if (use_sm) S.fit[k] = v;
     }
-    __syncthreads();
-    for (int k = threadIdx.x; k < S.n; k += blockDim.x)
-        S.fit[k] = splint_dev(S.x, S.y, S.y2, S.npts, S.t[k]) / 1;
+    if (use_sm)
+        for (int k = threadIdx.x; k < np; k += blockDim.x) S.y2[k] = y2[k];
     __syncthreads();
     if (threadIdx.x == 0) {
         double o2 = 0.0, m2 = 0.0, om = 0.0;
-        for (int k = 0; k < S.n; k++) {
-            o2 += S.obs[k] * S.obs[k] * S.oov[k];
-            m2 += S.fit[k] * S.fit[k] * S.oov[k];
-            om += S.fit[k] * S.obs[k] * S.oov[k];
+        for (int k = 0; k < n; k++) {
+            o2 += obs[k] * obs[k] * oov[k];
+            m2 += fit[k] * fit[k] * oov[k];
+            om += fit[k] * obs[k] * oov[k];
         }
         double cal = S.cal_in;
         if (S.cal_floating)
@@ -545,11 +589,16 @@ __global__ void k_lc_finalize(LcFinalizeArgs a)
         double chi2 = S.weight * (o2 - 2 * cal * om + cal * cal * m2);
         int posbnd = 0;
         double lsum = 0.0;
-        for (int k = 0; k < S.npts; k++) {
-            const LcPointDev &P = a.pts[S.pt0 + k];
-            const FrameState &so = a.states[P.obs_view], &ss = a.states[P.sun_view];
-            if (so.outbnd) { posbnd = 1; lsum += 0.5 * view_logfactor(a.geoms[P.obs_view], so); }
-            if (ss.outbnd) { posbnd = 1; lsum += 0.5 * view_logfactor(a.geoms[P.sun_view], ss); }
+        for (int k = 0; k < np; k++) {
+            if (use_sm) {
+                if (pflag[k] & 1) { posbnd = 1; lsum += lo[k]; }
+                if (pflag[k] & 2) { posbnd = 1; lsum += ls[k]; }
+            } else {
+                const LcPointDev &P = a.pts[S.pt0 + k];
+                const FrameState &so = a.states[P.obs_view], &ss = a.states[P.sun_view];
+                if (so.outbnd) { posbnd = 1; lsum += 0.5 * view_logfactor(a.geoms[P.obs_view], so); }
+                if (ss.outbnd) { posbnd = 1; lsum += 0.5 * view_logfactor(a.geoms[P.sun_view], ss); }
+            }
         }
         double *o = a.set_out + 4 * blockIdx.x;
         o[0] = cal; o[1] = chi2; o[2] = posbnd; o[3] = lsum;
@@ -560,8 +609,11 @@ __global__ void k_lc_finalize(LcFinalizeArgs a)
 // the posbnd / badradar flags and log-factors of calc_fits
 // (src/shape/calc_fits.c:407-409, 511-550, 1947) and the objective's
 // bad-model multipliers (src/shape/bestfit.c:806-866), no penalties.
-__global__ void k_summary(SummaryArgs a)
+__global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
 {
+    // per-frame results first (one thread per frame), then the totals
+    for (int fr = threadIdx.x; fr < fa.nframes; fr += blockDim.x) finalize_frame(fa, fr);
+    __syncthreads();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double chi2 = 0.0, chi2_dd = 0.0, chi2_lc = 0.0, plog = 0.0, blog = 0.0;
     int posbnd = 0, badradar = 0;
@@ -671,15 +723,30 @@ void launch_lc_photo(const LcArgs &a, int fp32, cudaStream_t s)
     else k_lc_photo<double><<<blocks, 256, 0, s>>>(a);
 }
 
+// Shared memory one set needs (0 when it exceeds the block's budget: the
+// kernel then works on the global arrays).
+size_t lc_finalize_smem(int npts, int n)
+{
+    size_t b = sizeof(double) * (6 * (size_t)npts + 4 * (size_t)n) + sizeof(int) * (size_t)npts;
+    return b <= LC_FINALIZE_SMEM_MAX ? b : 0;
+}
+
+cudaError_t configure_lc_finalize()
+{
+    return cudaFuncSetAttribute(k_lc_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)LC_FINALIZE_SMEM_MAX);
+}
+
 void launch_lc_finalize(const LcFinalizeArgs &a, cudaStream_t s)
 {
     if (a.nsets <= 0) return;
-    k_lc_finalize<<<a.nsets, 256, 0, s>>>(a);
+    k_lc_finalize<<<a.nsets, 256, a.smem_per_set, s>>>(a);
 }
 
-void launch_summary(const SummaryArgs &a, cudaStream_t s)
+void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s)
 {
-    k_summary<<<1, 32, 0, s>>>(a);
+    k_summary<<<1, 256, 0, s>>>(fa, a);
 }
+
 
 }  // namespace shape

@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "engine_impl.h"
 #include "kernels.h"
 #include "shape_b200.h"
 
@@ -71,191 +72,11 @@ static void mul_bt(double *M, const double *B, const double *A)
     memcpy(M, t, sizeof t);
 }
 
-struct DevMem {
-    std::vector<void *> ptrs;
-    template <typename T> int alloc(T **p, size_t count)
-    {
-        if (count == 0) count = 1;
-        cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
-        if (e != cudaSuccess)
-            return set_err(SHAPE_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        ptrs.push_back(*p);
-        return SHAPE_OK;
-    }
-    void release()
-    {
-        for (void *p : ptrs) cudaFree(p);
-        ptrs.clear();
-    }
-    void release_one(void *p)
-    {
-        for (auto it = ptrs.begin(); it != ptrs.end(); ++it)
-            if (*it == p) {
-                cudaFree(p);
-                ptrs.erase(it);
-                return;
-            }
-    }
-};
-
-struct DdSetHost {
-    shape_deldop_set set;
-    int frame0, nframes;
-};
-struct LcSetHost {
-    shape_lghtcrv_set set;
-    int pt0, npts;
-    std::vector<double> x, t, obs, oov;
-};
-
-struct EngineImpl {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    float last_ms = 0.f;
-
-    // model (host)
-    int nv = 0, nf = 0;
-    std::vector<double> a, u, r;
-    double scale[3] = {1, 1, 1};
-    std::vector<int> fv, af_ptr, af_idx;
-    bool have_model = false;
-    shape_eval_params params{1, 1, 7, 0.0, 0.0, 1};
-    double bad_objfactor = 2.0;
-
-    // datasets (host)
-    std::vector<DdSetHost> dd;
-    std::vector<shape_deldop_frame> frames;
-    std::vector<long long> frame_off;   // element offsets into obs/oov/fit
-    std::vector<double> obs, oov;
-    std::vector<LcSetHost> lc;
-    std::vector<shape_lghtcrv_point> points;
-    std::vector<SetRec> setrecs;
-    std::vector<RadarLawDev> laws;
-    double dof = 0, dof_deldop = 0, dof_lghtcrv = 0;
-
-    // derived (host)
-    std::vector<FrameGeom> geoms;
-    std::vector<FrameHost> fh;
-    std::vector<int2> work;                 // raster items
-    std::vector<int> view_work0, view_nwork;
-    std::vector<Chi2Item> chi2_items;
-    std::vector<int> frame_view;
-    std::vector<double> dop_extra, set_delpp, set_doppp;
-    std::vector<LcPointDev> lcpts;
-    std::vector<int2> lc_items;
-    std::vector<int> pt_items;
-    int nviews = 0, ntiles = 0;
-    long long fit_elems = 0, pos_elems = 0;
-    int cap = 512;
-
-    // device
-    bool finalized = false;
-    DevMem mem;
-    ModelDev md{};
-    double *d_r = nullptr, *d_scale = nullptr, *d_a = nullptr, *d_u = nullptr;
-    int *d_fv = nullptr, *d_afp = nullptr, *d_afi = nullptr;
-    FrameGeom *d_geoms = nullptr;
-    FrameState *d_states = nullptr;
-    RadarLawDev *d_laws = nullptr;
-    int2 *d_work = nullptr;
-    double4 *d_vt64 = nullptr;
-    float4 *d_vt32 = nullptr;
-    int *d_bin_count = nullptr;
-    int2 *d_bin_ids = nullptr;
-    double *d_obs = nullptr, *d_oov = nullptr;
-    double *d_fit64 = nullptr;
-    float *d_fit32 = nullptr;
-    void *d_pos_z = nullptr, *d_pos_cose = nullptr, *d_pos_cosi = nullptr;   // sized for double
-    int *d_pos_f = nullptr;
-    unsigned char *d_seen = nullptr;
-    Chi2Item *d_chi2_items = nullptr;
-    int *d_frame_view = nullptr;
-    double *d_partials = nullptr;
-    FrameHost *d_fh = nullptr;
-    shape_deldop_result *d_results = nullptr;
-    double *d_set_delpp = nullptr, *d_set_doppp = nullptr, *d_dop_extra = nullptr;
-    LcPointDev *d_lcpts = nullptr;
-    int2 *d_lc_items = nullptr;
-    int *d_pt_items = nullptr;
-    double *d_lc_partials = nullptr;
-    LcSetDev *d_lcsets = nullptr;
-    double *d_lc_x = nullptr, *d_lc_t = nullptr, *d_lc_obs = nullptr, *d_lc_oov = nullptr;
-    double *d_lc_y = nullptr, *d_lc_y2 = nullptr, *d_lc_fit = nullptr, *d_lc_out = nullptr;
-    double *d_lc_dof = nullptr, *d_lc_npts = nullptr;
-    SetRec *d_setrecs = nullptr;
-    shape_eval_summary *d_summary = nullptr;
-    std::vector<LcSetDev> lcdev;
-
-    // pinned staging
-    double *h_params = nullptr;             // r[nv], scale[3]
-    shape_eval_summary *h_summary = nullptr;
-
-    // graphs per form
-    cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
-    int keep_pos = 0;
-    int graph_keep_pos[3] = {0, 0, 0};
-    int last_form = -1;
-
-    ~EngineImpl() { release(); }
-
-    void release()
-    {
-        for (auto &g : gexec)
-            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-        mem.release();
-        if (h_params) { cudaFreeHost(h_params); h_params = nullptr; }
-        if (h_summary) { cudaFreeHost(h_summary); h_summary = nullptr; }
-        if (ev0) { cudaEventDestroy(ev0); ev0 = nullptr; }
-        if (ev1) { cudaEventDestroy(ev1); ev1 = nullptr; }
-        if (stream) { cudaStreamDestroy(stream); stream = nullptr; }
-    }
-
-    void invalidate_graphs()
-    {
-        for (auto &g : gexec)
-            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-    }
-
-    int finalize();
-    int tune_bins();
-    int enqueue(int form, cudaEvent_t *marks = nullptr);
-    // bin tuning results
-    int2 *d_work_sorted = nullptr;
-    int tuned_max_count = 0, tuned_nonempty = 0;
-    int fixed_cap = 0;            // > 0: bin capacity set by the caller, no autotuning
-    int evaluate(int form, shape_eval_summary *out);
-    void fill_params(double *dst) const
-    {
-        memcpy(dst, r.data(), sizeof(double) * nv);
-        double sc[3];
-        effective_scale(sc, nullptr, nullptr);
-        memcpy(dst + nv, sc, sizeof sc);
-    }
-    // scale factors after realize_coordinates' SMALLRATIO guard
-    // (src/shape/realize_mod.c:458-470; SMALLRATIO = 0.01, :138)
-    void effective_scale(double *sc, int *baddiam, double *logf) const
-    {
-        int bd = 0;
-        double lf = 0.0;
-        for (int j = 0; j < 3; j++) {
-            double v = scale[j];
-            if (v <= 0.01) {
-                bd = 1;
-                lf += log(1 + 0.01 - v);
-                v = 0.01 / (1 + 0.01 - v);
-            }
-            sc[j] = v;
-        }
-        if (baddiam) *baddiam = bd;
-        if (logf) *logf = lf;
-    }
-};
-
 static int radar_law_index(EngineImpl &E, const shape_radar_law &L)
 {
     if (L.type < SHAPE_RADLAW_COSINE_DIFF || L.type > SHAPE_RADLAW_COSINE_COSINE) return -1;
-    RadarLawDev d{L.type, L.diff_R, L.diff_C, L.qs_R, L.qs_C, L.qs_cos_cutoff};
+    RadarLawDev d{L.type, L.diff_R, L.diff_C, L.qs_R, L.qs_C, L.qs_cos_cutoff,
+                  2 * L.diff_C - 1 == 1.0, 2 * L.qs_C - 1 == 1.0};
     E.laws.push_back(d);
     return (int)E.laws.size() - 1;
 }
@@ -290,6 +111,14 @@ int EngineImpl::finalize()
         for (int t = 0; t < g.tiles_x * g.tiles_x; t++) work.push_back(make_int2((int)geoms.size(), t));
         tile_base += g.tiles_x * g.tiles_x;
         pos_base += (long long)g.side * g.side;
+        const double fv[FDD_N] = {g.delfact, g.delshift, g.ax, g.ay, g.dopshift, g.const1, g.const2,
+                                  g.one_over_spb, g.xincr, g.yincr, g.dopdiff_bl, g.dopdiff_max,
+                                  g.dopDC_vig, g.dopfftlen, g.kmpp, g.sinc2width / 2.0,
+                                  (double)g.spb_over_stride, (double)g.stride, (double)g.spb_sq,
+                                  (double)g.nsinc2_sq};
+        for (int k = 0; k < FDD_N; k++) g.fdd[k] = (float)fv[k];
+        for (int k = 0; k < 9; k++) g.foa[k] = (float)g.oa[k];
+        for (int k = 0; k < 3; k++) g.foa[9 + k] = (float)g.usrc[k];
         geoms.push_back(g);
     };
 
@@ -442,7 +271,7 @@ int EngineImpl::finalize()
         L.nitems = (int)lc_items.size() - L.item0;
         lcdev.push_back(L);
     }
-    if (laws.empty()) laws.push_back(RadarLawDev{SHAPE_RADLAW_COSINE_DIFF, 0.0, 0.0, 0.0, 0.0, 0.0});
+    if (laws.empty()) laws.push_back(RadarLawDev{SHAPE_RADLAW_COSINE_DIFF, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0});
     ntiles = tile_base;
     pos_elems = pos_base;
     fit_elems = obs.size();
@@ -550,6 +379,7 @@ int EngineImpl::finalize()
 
     CK(configure_raster_f64());
     CK(configure_raster_f32());
+    CK(configure_lc_finalize());
     md.nv = nv; md.nf = nf;
     md.a = d_a; md.u = d_u; md.r = d_r; md.scale = d_scale;
     md.fv = d_fv; md.af_ptr = d_afp; md.af_idx = d_afi;
@@ -698,6 +528,8 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         if (f32) launch_bin_f32(d_geoms, 0, nviews, md, d_vt32, d_states, d_bin_count, d_bin_ids, cap, s);
         else launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
         mark(3);
+        // one CTA per tile, heaviest tiles first (empty tiles sort last and
+        // exit at once); the block scheduler balances the rest
         ra.work = d_work_sorted;
         ra.nwork = (int)work.size();
         if (f32) launch_raster_f32(ra, s); else launch_raster_f64(ra, s);
@@ -715,20 +547,23 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         }
         mark(6);
     }
-    if (!fh.empty()) {
-        FinalizeArgs fa;
-        memset(&fa, 0, sizeof fa);
-        fa.nframes = (int)fh.size();
-        fa.fh = d_fh; fa.geoms = d_geoms; fa.states = d_states; fa.partials = d_partials;
-        fa.results = d_results; fa.set_delpp = d_set_delpp; fa.set_doppp = d_set_doppp;
-        fa.dop_extra = d_dop_extra;
-        launch_finalize_frames(fa, s);
-    }
+    FinalizeArgs fa;
+    memset(&fa, 0, sizeof fa);
+    fa.nframes = (int)fh.size();
+    fa.fh = d_fh; fa.geoms = d_geoms; fa.states = d_states; fa.partials = d_partials;
+    fa.results = d_results; fa.set_delpp = d_set_delpp; fa.set_doppp = d_set_doppp;
+    fa.dop_extra = d_dop_extra;
     if (!lcdev.empty()) {
         LcFinalizeArgs lf;
         lf.nsets = (int)lcdev.size();
         lf.sets = d_lcsets; lf.pts = d_lcpts; lf.geoms = d_geoms; lf.states = d_states;
         lf.pt_items = d_pt_items; lf.partials = d_lc_partials; lf.set_out = d_lc_out;
+        size_t sm = 1;
+        for (const LcSetDev &L : lcdev) {
+            size_t b = lc_finalize_smem(L.npts, L.n);
+            sm = (b == 0 || sm == 0) ? 0 : std::max(sm, b);
+        }
+        lf.smem_per_set = sm;
         launch_lc_finalize(lf, s);
     }
     SummaryArgs sa;
@@ -742,21 +577,47 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     sa.baddiam = 0;
     sa.baddiam_logfactor = 0.0;
     sa.out = d_summary;
-    launch_summary(sa, s);
+    launch_summary(fa, sa, s);
     mark(7);
     CK(cudaGetLastError());
     return SHAPE_OK;
 }
 
+// Kernel launches enqueue() makes for one evaluation in this form (memsets
+// and copies excluded).
+int EngineImpl::kernels_per_eval(int form) const
+{
+    int n = 3 + 1;                       // realize (vertices, facets, normals), state reset
+    if (form == SHAPE_FORM_PLAIN_FP64) {
+        for (int v = 0; v < nviews; v++)
+            n += 3 + (geoms[v].kind == VIEW_RADAR || geoms[v].kind == VIEW_LC_SUN ? 1 : 0);
+    } else {
+        n += 3;                          // transform, bin, raster
+        n += chi2_items.empty() ? 0 : 1;
+        n += lc_items.empty() ? 0 : 1;
+    }
+    n += lcdev.empty() ? 0 : 1;          // lightcurve finalize
+    return n + 1;                        // finalize + summary
+}
+
 int EngineImpl::evaluate(int form, shape_eval_summary *out)
+{
+    int rc = launch(form);
+    if (rc) return rc;
+    return finish(out);
+}
+
+// Enqueues one evaluation on the engine stream and returns without waiting:
+// parameters host->device, the kernel sequence (a graph replay for the
+// batched forms), the summary device->host, then event ev1.
+int EngineImpl::launch(int form)
 {
     if (!finalized) return set_err(SHAPE_E_STATE, "evaluate before finalize");
     if (form < 0 || form > 2) return set_err(SHAPE_E_ARG, "unknown form");
     cudaStream_t s = stream;
     fill_params(h_params);
-    int baddiam;
-    double bdl, sc[3];
-    effective_scale(sc, &baddiam, &bdl);
+    double sc[3];
+    effective_scale(sc, &pending_baddiam, &pending_bdl);
     if (form == SHAPE_FORM_PLAIN_FP64) {
         CK(cudaEventRecord(ev0, s));
         CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s));
@@ -788,12 +649,28 @@ int EngineImpl::evaluate(int form, shape_eval_summary *out)
         CK(cudaGraphLaunch(gexec[form], s));
         CK(cudaEventRecord(ev1, s));
     }
-    CK(cudaStreamSynchronize(s));
-    CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
     last_form = form;
+    return SHAPE_OK;
+}
+
+// 1 when the last launch has completed on the device, 0 otherwise.
+int EngineImpl::poll()
+{
+    cudaError_t e = cudaEventQuery(ev1);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) return 0;
+    return set_err(SHAPE_E_CUDA, std::string("cudaEventQuery: ") + cudaGetErrorString(e));
+}
+
+// Waits for the last launch and returns its summary.
+int EngineImpl::finish(shape_eval_summary *out)
+{
+    CK(cudaEventSynchronize(ev1));
+    CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
     shape_eval_summary sm = *h_summary;
     // bad-diameter factor depends only on the host-side scale factors
-    if (baddiam) {
+    if (pending_baddiam) {
+        const double bdl = pending_bdl;
         sm.objective = sm.chi2 / sm.dof * (bad_objfactor * exp(bdl));
         if (sm.posbnd) sm.objective *= bad_objfactor * exp(sm.posbnd_logfactor);
         if (sm.badradar) sm.objective *= bad_objfactor * exp(sm.badradar_logfactor);
@@ -807,10 +684,6 @@ int EngineImpl::evaluate(int form, shape_eval_summary *out)
 // ====================================================================== C ABI
 
 using shape::EngineImpl;
-
-struct shape_engine {
-    EngineImpl impl;
-};
 
 extern "C" {
 
@@ -1183,6 +1056,14 @@ int shape_engine_get_tuning(shape_engine *h, int *out, int max)
     int n = 0;
     for (; n < 5 && n < max; n++) out[n] = v[n];
     return n;
+}
+
+int shape_engine_kernels_per_eval(shape_engine *h, int form, int *count)
+{
+    if (!h || !count || form < 0 || form > 2) return shape::set_err(SHAPE_E_ARG, "bad argument");
+    if (!h->impl.finalized) return shape::set_err(SHAPE_E_STATE, "kernels_per_eval before finalize");
+    *count = h->impl.kernels_per_eval(form);
+    return SHAPE_OK;
 }
 
 int shape_engine_last_time_ms(shape_engine *h, double *ms)

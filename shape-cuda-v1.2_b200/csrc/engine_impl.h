@@ -1,0 +1,235 @@
+// EngineImpl: host-side state of one engine (model, datasets, device
+// arenas, graphs). Shared by engine.cu (evaluation, C ABI) and server.cu
+// (continuous-batching request loop).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "shape_b200.h"
+
+namespace shape {
+
+int report_error(int code, const std::string &msg);   // engine.cu
+
+struct DevMem {
+    std::vector<void *> ptrs;
+    std::vector<size_t> sizes;
+    size_t bytes = 0;             // device bytes held (the engine's HBM footprint)
+    template <typename T> int alloc(T **p, size_t count)
+    {
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+        if (e != cudaSuccess)
+            return report_error(SHAPE_E_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        ptrs.push_back(*p);
+        sizes.push_back(count * sizeof(T));
+        bytes += count * sizeof(T);
+        return SHAPE_OK;
+    }
+    void release()
+    {
+        for (void *p : ptrs) cudaFree(p);
+        ptrs.clear();
+        sizes.clear();
+        bytes = 0;
+    }
+    void release_one(void *p)
+    {
+        for (size_t k = 0; k < ptrs.size(); k++)
+            if (ptrs[k] == p) {
+                cudaFree(p);
+                bytes -= sizes[k];
+                ptrs.erase(ptrs.begin() + k);
+                sizes.erase(sizes.begin() + k);
+                return;
+            }
+    }
+};
+
+struct DdSetHost {
+    shape_deldop_set set;
+    int frame0, nframes;
+};
+struct LcSetHost {
+    shape_lghtcrv_set set;
+    int pt0, npts;
+    std::vector<double> x, t, obs, oov;
+};
+
+struct EngineImpl {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+
+    // model (host)
+    int nv = 0, nf = 0;
+    std::vector<double> a, u, r;
+    double scale[3] = {1, 1, 1};
+    std::vector<int> fv, af_ptr, af_idx;
+    bool have_model = false;
+    shape_eval_params params{1, 1, 7, 0.0, 0.0, 1};
+    double bad_objfactor = 2.0;
+
+    // datasets (host)
+    std::vector<DdSetHost> dd;
+    std::vector<shape_deldop_frame> frames;
+    std::vector<long long> frame_off;   // element offsets into obs/oov/fit
+    std::vector<double> obs, oov;
+    std::vector<LcSetHost> lc;
+    std::vector<shape_lghtcrv_point> points;
+    std::vector<SetRec> setrecs;
+    std::vector<RadarLawDev> laws;
+    double dof = 0, dof_deldop = 0, dof_lghtcrv = 0;
+
+    // derived (host)
+    std::vector<FrameGeom> geoms;
+    std::vector<FrameHost> fh;
+    std::vector<int2> work;                 // raster items
+    std::vector<int> view_work0, view_nwork;
+    std::vector<Chi2Item> chi2_items;
+    std::vector<int> frame_view;
+    std::vector<double> dop_extra, set_delpp, set_doppp;
+    std::vector<LcPointDev> lcpts;
+    std::vector<int2> lc_items;
+    std::vector<int> pt_items;
+    int nviews = 0, ntiles = 0;
+    long long fit_elems = 0, pos_elems = 0;
+    int cap = 512;
+
+    // device
+    bool finalized = false;
+    DevMem mem;
+    ModelDev md{};
+    double *d_r = nullptr, *d_scale = nullptr, *d_a = nullptr, *d_u = nullptr;
+    int *d_fv = nullptr, *d_afp = nullptr, *d_afi = nullptr;
+    FrameGeom *d_geoms = nullptr;
+    FrameState *d_states = nullptr;
+    RadarLawDev *d_laws = nullptr;
+    int2 *d_work = nullptr;
+    double4 *d_vt64 = nullptr;
+    float4 *d_vt32 = nullptr;
+    int *d_bin_count = nullptr;
+    int2 *d_bin_ids = nullptr;
+    double *d_obs = nullptr, *d_oov = nullptr;
+    double *d_fit64 = nullptr;
+    float *d_fit32 = nullptr;
+    void *d_pos_z = nullptr, *d_pos_cose = nullptr, *d_pos_cosi = nullptr;   // sized for double
+    int *d_pos_f = nullptr;
+    unsigned char *d_seen = nullptr;
+    Chi2Item *d_chi2_items = nullptr;
+    int *d_frame_view = nullptr;
+    double *d_partials = nullptr;
+    FrameHost *d_fh = nullptr;
+    shape_deldop_result *d_results = nullptr;
+    double *d_set_delpp = nullptr, *d_set_doppp = nullptr, *d_dop_extra = nullptr;
+    LcPointDev *d_lcpts = nullptr;
+    int2 *d_lc_items = nullptr;
+    int *d_pt_items = nullptr;
+    double *d_lc_partials = nullptr;
+    LcSetDev *d_lcsets = nullptr;
+    double *d_lc_x = nullptr, *d_lc_t = nullptr, *d_lc_obs = nullptr, *d_lc_oov = nullptr;
+    double *d_lc_y = nullptr, *d_lc_y2 = nullptr, *d_lc_fit = nullptr, *d_lc_out = nullptr;
+    double *d_lc_dof = nullptr, *d_lc_npts = nullptr;
+    SetRec *d_setrecs = nullptr;
+    shape_eval_summary *d_summary = nullptr;
+    std::vector<LcSetDev> lcdev;
+
+    // pinned staging
+    double *h_params = nullptr;             // r[nv], scale[3]
+    shape_eval_summary *h_summary = nullptr;
+
+    // graphs per form
+    cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
+    int keep_pos = 0;
+    int graph_keep_pos[3] = {0, 0, 0};
+    int last_form = -1;
+
+    ~EngineImpl() { release(); }
+
+    void release()
+    {
+        for (auto &g : gexec)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+        mem.release();
+        if (h_params) { cudaFreeHost(h_params); h_params = nullptr; }
+        if (h_summary) { cudaFreeHost(h_summary); h_summary = nullptr; }
+        if (ev0) { cudaEventDestroy(ev0); ev0 = nullptr; }
+        if (ev1) { cudaEventDestroy(ev1); ev1 = nullptr; }
+        if (stream) { cudaStreamDestroy(stream); stream = nullptr; }
+    }
+
+    void invalidate_graphs()
+    {
+        for (auto &g : gexec)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+
+    int finalize();
+    int tune_bins();
+    int enqueue(int form, cudaEvent_t *marks = nullptr);
+    int launch(int form);
+    int poll();
+    int finish(shape_eval_summary *out);
+    int pending_baddiam = 0;
+    double pending_bdl = 0.0;
+    size_t footprint() const { return mem.bytes + sizeof(double) * ((size_t)nv + 3) + sizeof(shape_eval_summary); }
+    // copies the host description (model, switches, datasets) of another
+    // engine; finalize() then builds this engine's own device state
+    void clone_host_state(const EngineImpl &o)
+    {
+        nv = o.nv; nf = o.nf; a = o.a; u = o.u; r = o.r;
+        for (int j = 0; j < 3; j++) scale[j] = o.scale[j];
+        fv = o.fv; af_ptr = o.af_ptr; af_idx = o.af_idx; have_model = o.have_model;
+        params = o.params; bad_objfactor = o.bad_objfactor;
+        dd = o.dd; frames = o.frames; frame_off = o.frame_off; obs = o.obs; oov = o.oov;
+        lc = o.lc; points = o.points; setrecs = o.setrecs;
+        dof = o.dof; dof_deldop = o.dof_deldop; dof_lghtcrv = o.dof_lghtcrv;
+        fixed_cap = o.fixed_cap;
+        finalized = false;
+    }
+    // bin tuning results
+    int2 *d_work_sorted = nullptr;
+    int tuned_max_count = 0, tuned_nonempty = 0;
+    int fixed_cap = 0;            // > 0: bin capacity set by the caller, no autotuning
+    int evaluate(int form, shape_eval_summary *out);
+    int kernels_per_eval(int form) const;
+    void fill_params(double *dst) const
+    {
+        memcpy(dst, r.data(), sizeof(double) * nv);
+        double sc[3];
+        effective_scale(sc, nullptr, nullptr);
+        memcpy(dst + nv, sc, sizeof sc);
+    }
+    // scale factors after realize_coordinates' SMALLRATIO guard
+    // (src/shape/realize_mod.c:458-470; SMALLRATIO = 0.01, :138)
+    void effective_scale(double *sc, int *baddiam, double *logf) const
+    {
+        int bd = 0;
+        double lf = 0.0;
+        for (int j = 0; j < 3; j++) {
+            double v = scale[j];
+            if (v <= 0.01) {
+                bd = 1;
+                lf += log(1 + 0.01 - v);
+                v = 0.01 / (1 + 0.01 - v);
+            }
+            sc[j] = v;
+        }
+        if (baddiam) *baddiam = bd;
+        if (logf) *logf = lf;
+    }
+};
+
+}  // namespace shape
+
+// the C ABI handle of an engine
+struct shape_engine {
+    shape::EngineImpl impl;
+};

@@ -50,6 +50,18 @@ struct FrameGeom {
     int codemethod, spb, stride, spb_over_stride, spb_sq, nsinc2, nsinc2_sq, sinc2width;
     int law;             // index into the radar law table
     int frame_index;     // global delay-Doppler frame index or lightcurve point index
+    // the synthesis constants rounded to float on the host for the FP32
+    // raster, in FDD_* order (five float4 loads per tile instead of one
+    // double->float conversion per constant per pixel)
+    alignas(16) float fdd[20];
+    alignas(16) float foa[12];   // oa[9] and usrc[3] rounded to float
+};
+
+// Order of FrameGeom::fdd.
+enum {
+    FDD_DELFACT, FDD_DELSHIFT, FDD_AX, FDD_AY, FDD_DOPSHIFT, FDD_CONST1, FDD_CONST2, FDD_ONE_OVER_SPB,
+    FDD_XINCR, FDD_YINCR, FDD_DOPDIFF_BL, FDD_DOPDIFF_MAX, FDD_DOPDC_VIG, FDD_DOPFFTLEN, FDD_KMPP,
+    FDD_HALF_W, FDD_SPB_OVER_STRIDE, FDD_STRIDE, FDD_SPB_SQ, FDD_NSINC2_SQ, FDD_N
 };
 
 // Per-view accumulators, reset by k_reset_state each evaluation.
@@ -68,6 +80,7 @@ struct FrameState {
 struct RadarLawDev {
     int type;
     double diff_R, diff_C, qs_R, qs_C, qs_cos_cutoff;
+    int diff_linear, qs_linear;   // 2C - 1 == 1: cos^(2C-1) is cos itself
 };
 
 // Lightcurve point descriptor (one calc epoch).

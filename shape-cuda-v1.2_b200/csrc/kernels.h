@@ -22,7 +22,7 @@ struct ModelDev {
 struct RasterArgs {
     const FrameGeom *geoms;
     const int2 *work;          // (view, tile) items
-    int nwork;
+    int nwork;                 // items
     const void *vt;            // T4 transformed vertices
     const int4 *fvi;
     const double4 *vn;
@@ -123,7 +123,11 @@ struct LcFinalizeArgs {
     const int *pt_items;        // per point: first item, count (2 ints)
     const double *partials;
     double *set_out;            // per set: cal, chi2, posbnd flag, logfactor sum
+    size_t smem_per_set;        // dynamic shared memory (lc_finalize_smem of the largest set), 0: global
 };
+constexpr size_t LC_FINALIZE_SMEM_MAX = 160 * 1024;
+size_t lc_finalize_smem(int npts, int n);
+cudaError_t configure_lc_finalize();
 void launch_lc_finalize(const LcFinalizeArgs &a, cudaStream_t s);
 
 struct SetRec { int type; int first; int count; };   // type 0 deldop (frames), 1 lightcurve (set index)
@@ -141,7 +145,8 @@ struct SummaryArgs {
     double baddiam_logfactor;
     shape_eval_summary *out;
 };
-void launch_summary(const SummaryArgs &a, cudaStream_t s);
+// per-frame finalize (as launch_finalize_frames) fused with the totals
+void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s);
 
 // raster_f64.cu / raster_f32.cu
 void launch_raster_f64(const RasterArgs &a, cudaStream_t s);

@@ -18,6 +18,7 @@
 // fit image, so POS maps never travel through HBM unless requested.
 #pragma once
 
+#include <algorithm>
 #include <climits>
 
 #include "kernels.h"
@@ -65,7 +66,7 @@ template <typename T> __device__ T radlaw_dev(const RadarLawDev &L, T c)
     T v = (T)-9.99, tan2inc, sin2inc, arg;
     switch (L.type) {
     case SHAPE_RADLAW_COSINE_DIFF:
-        v = (T)L.diff_R * ((T)L.diff_C + 1) * tpow<T>(c, 2 * (T)L.diff_C - 1);
+        v = (T)L.diff_R * ((T)L.diff_C + 1) * (L.diff_linear ? c : tpow<T>(c, 2 * (T)L.diff_C - 1));
         break;
     case SHAPE_RADLAW_GAUSSIAN:
         if (c >= (T)L.qs_cos_cutoff) {
@@ -82,18 +83,18 @@ template <typename T> __device__ T radlaw_dev(const RadarLawDev &L, T c)
         break;
     case SHAPE_RADLAW_COSINE_QS:
         if (c >= (T)L.qs_cos_cutoff)
-            v = (T)L.qs_R * ((T)L.qs_C + 1) * tpow<T>(c, 2 * (T)L.qs_C - 1);
+            v = (T)L.qs_R * ((T)L.qs_C + 1) * (L.qs_linear ? c : tpow<T>(c, 2 * (T)L.qs_C - 1));
         else v = 0;
         break;
     case SHAPE_RADLAW_GAUSSIAN_COSINE:
-        v = (T)L.diff_R * ((T)L.diff_C + 1) * tpow<T>(c, 2 * (T)L.diff_C - 1);
+        v = (T)L.diff_R * ((T)L.diff_C + 1) * (L.diff_linear ? c : tpow<T>(c, 2 * (T)L.diff_C - 1));
         if (c >= (T)L.qs_cos_cutoff) {
             tan2inc = 1 / (c * c) - 1;
             v += (T)L.qs_R * (T)L.qs_C * texp<T>(-(T)L.qs_C * tan2inc) / (c * c * c * c * c);
         }
         break;
     case SHAPE_RADLAW_HAGFORS_COSINE:
-        v = (T)L.diff_R * ((T)L.diff_C + 1) * tpow<T>(c, 2 * (T)L.diff_C - 1);
+        v = (T)L.diff_R * ((T)L.diff_C + 1) * (L.diff_linear ? c : tpow<T>(c, 2 * (T)L.diff_C - 1));
         if (c >= (T)L.qs_cos_cutoff) {
             sin2inc = 1 - c * c;
             arg = c * c * c * c + (T)L.qs_C * sin2inc;
@@ -101,9 +102,9 @@ template <typename T> __device__ T radlaw_dev(const RadarLawDev &L, T c)
         }
         break;
     case SHAPE_RADLAW_COSINE_COSINE:
-        v = (T)L.diff_R * ((T)L.diff_C + 1) * tpow<T>(c, 2 * (T)L.diff_C - 1);
+        v = (T)L.diff_R * ((T)L.diff_C + 1) * (L.diff_linear ? c : tpow<T>(c, 2 * (T)L.diff_C - 1));
         if (c >= (T)L.qs_cos_cutoff)
-            v += (T)L.qs_R * ((T)L.qs_C + 1) * tpow<T>(c, 2 * (T)L.qs_C - 1);
+            v += (T)L.qs_R * ((T)L.qs_C + 1) * (L.qs_linear ? c : tpow<T>(c, 2 * (T)L.qs_C - 1));
         break;
     default:
         break;
@@ -115,13 +116,26 @@ template <typename T> __device__ T radlaw_dev(const RadarLawDev &L, T c)
 // bbox clipped to the tile and relative to its corner (4 bits per bound:
 // i1, i2, j1, j2); wmask has bit w set when the bbox meets warp w's 4x8
 // pixel block.
+//
+// The terms the per-pixel test reads are packed in three 4-vectors, so a
+// visit loads them with three vector loads (every lane of a warp reads the
+// same staged facet: broadcasts, no bank conflicts):
+//   p0 = (v00, v01, A, B), p1 = (den, C, D, v02), p2 = (E, F, nx, ny).
 template <typename T>
 struct Stage {
-    T v00, v01, v02, A, B, C, D, E, F, den;
-    T nx, ny, nz;        // facet normal in view coordinates (views without smoothing)
+    typename Vec4<T>::type p0, p1, p2;
+    T nz;                // facet normal in view coordinates: (p2.z, p2.w, nz), views without smoothing
     T q[9];              // body-frame vertex normals of the three corners (smoothing)
     int bb, wmask, f;
 };
+
+template <typename T>
+__device__ inline typename Vec4<T>::type vec4(T x, T y, T z, T w)
+{
+    typename Vec4<T>::type v;
+    v.x = x; v.y = y; v.z = z; v.w = w;
+    return v;
+}
 
 // Warp w covers tile rows 4*(w>>1) .. +3 and columns 8*(w&1) .. +7.
 __device__ inline int warp_mask_of(int ri1, int ri2, int rj1, int rj2)
@@ -145,14 +159,15 @@ __device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage
     const T4 *vt = static_cast<const T4 *>(a.vt) + g.vt_base;
     int4 c = a.fvi[f];
     T4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
-    s.v00 = p0.x; s.v01 = p0.y; s.v02 = p0.z;
-    s.A = p2.y - p1.y;
-    s.B = p2.x - p1.x;
-    s.C = p1.x - p0.x;
-    s.D = p1.y - p0.y;
-    s.E = p1.z - p0.z;
-    s.F = p2.z - p1.z;
-    s.den = (T)1 / (s.C * s.A - s.B * s.D);
+    const T A = p2.y - p1.y;
+    const T B = p2.x - p1.x;
+    const T C = p1.x - p0.x;
+    const T D = p1.y - p0.y;
+    const T E = p1.z - p0.z;
+    const T F = p2.z - p1.z;
+    const T den = (T)1 / (C * A - B * D);
+    s.p0 = vec4<T>(p0.x, p0.y, A, B);
+    s.p1 = vec4<T>(den, C, D, p0.z);
     s.f = f;
     if (g.smooth) {
         double4 q0 = a.vn[c.x], q1 = a.vn[c.y], q2 = a.vn[c.z];
@@ -169,8 +184,11 @@ __device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage
             nn[r] += g.oa[3 * r + 1] * nb.y;
             nn[r] += g.oa[3 * r + 2] * nb.z;
         }
-        s.nx = (T)nn[0]; s.ny = (T)nn[1]; s.nz = (T)nn[2];
+        s.p2 = vec4<T>(E, F, (T)nn[0], (T)nn[1]);
+        s.nz = (T)nn[2];
+        return;
     }
+    s.p2 = vec4<T>(E, F, (T)0, (T)0);
 }
 
 // Full staging of a facet that did not come from a bin (bin overflow path):
@@ -216,6 +234,58 @@ __device__ bool stage_facet(const RasterArgs &a, const FrameGeom &g, int f,
     return true;
 }
 
+// pos2deldop constants of one frame in the raster's arithmetic type: the
+// FP64 raster reads them from FrameGeom, the FP32 raster from the
+// host-rounded float copies (FrameGeom::fdd), once per tile.
+template <typename T>
+struct DDC {
+    T delfact, delshift, ax, ay, dopshift, const1, const2, one_over_spb;
+    T xincr, yincr, dopdiff_bl, dopdiff_max, dopDC_vig, dopfftlen, kmpp, half_w;
+    T spb_over_stride, stride, spb_sq, nsinc2_sq;
+};
+
+template <typename T> __device__ inline DDC<T> load_ddc(const FrameGeom &g);
+template <> __device__ inline DDC<double> load_ddc<double>(const FrameGeom &g)
+{
+    DDC<double> c;
+    c.delfact = g.delfact; c.delshift = g.delshift; c.ax = g.ax; c.ay = g.ay; c.dopshift = g.dopshift;
+    c.const1 = g.const1; c.const2 = g.const2; c.one_over_spb = g.one_over_spb;
+    c.xincr = g.xincr; c.yincr = g.yincr; c.dopdiff_bl = g.dopdiff_bl; c.dopdiff_max = g.dopdiff_max;
+    c.dopDC_vig = g.dopDC_vig; c.dopfftlen = g.dopfftlen; c.kmpp = g.kmpp; c.half_w = g.sinc2width / 2.0;
+    c.spb_over_stride = (double)g.spb_over_stride; c.stride = (double)g.stride;
+    c.spb_sq = (double)g.spb_sq; c.nsinc2_sq = (double)g.nsinc2_sq;
+    return c;
+}
+template <> __device__ inline DDC<float> load_ddc<float>(const FrameGeom &g)
+{
+    const float4 *p = reinterpret_cast<const float4 *>(g.fdd);
+    const float4 a = p[0], b = p[1], d = p[2], e = p[3], f = p[4];
+    DDC<float> c;
+    c.delfact = a.x; c.delshift = a.y; c.ax = a.z; c.ay = a.w;
+    c.dopshift = b.x; c.const1 = b.y; c.const2 = b.z; c.one_over_spb = b.w;
+    c.xincr = d.x; c.yincr = d.y; c.dopdiff_bl = d.z; c.dopdiff_max = d.w;
+    c.dopDC_vig = e.x; c.dopfftlen = e.y; c.kmpp = e.z; c.half_w = e.w;
+    c.spb_over_stride = f.x; c.stride = f.y; c.spb_sq = f.z; c.nsinc2_sq = f.w;
+    return c;
+}
+
+// The view rotation (observer <- body) and the sun direction in the raster's
+// arithmetic type: out[0..8] = oa, out[9..11] = usrc.
+template <typename T> __device__ inline void load_oa(const FrameGeom &g, T *out);
+template <> __device__ inline void load_oa<double>(const FrameGeom &g, double *out)
+{
+    for (int k = 0; k < 9; k++) out[k] = g.oa[k];
+    for (int k = 0; k < 3; k++) out[9 + k] = g.usrc[k];
+}
+template <> __device__ inline void load_oa<float>(const FrameGeom &g, float *out)
+{
+    const float4 *p = reinterpret_cast<const float4 *>(g.foa);
+    const float4 a = p[0], b = p[1], c = p[2];
+    out[0] = a.x; out[1] = a.y; out[2] = a.z; out[3] = a.w;
+    out[4] = b.x; out[5] = b.y; out[6] = b.z; out[7] = b.w;
+    out[8] = c.x; out[9] = c.y; out[10] = c.z; out[11] = c.w;
+}
+
 template <typename T> __device__ inline void atomic_add_fit(T *p, T v);
 template <> __device__ inline void atomic_add_fit<double>(double *p, double v) { atomicAdd(p, v); }
 template <> __device__ inline void atomic_add_fit<float>(float *p, float v) { atomicAdd(p, v); }
@@ -235,20 +305,20 @@ struct PixDD {
 };
 
 template <typename T>
-__device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, int x, int y, T z, PixLimits &lim)
+__device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, const DDC<T> &k, int x, int y, T z, PixLimits &lim)
 {
     PixDD<T> d;
-    d.delPOS = z * (T)g.delfact + (T)g.delshift;
-    const T const1 = (T)g.const1;
+    d.delPOS = z * k.delfact + k.delshift;
+    const T const1 = k.const1;
     d.idel_min = (int)floor(d.delPOS - const1) + 1;
     d.idel_max = (int)ceil(d.delPOS + const1) - 1;
-    d.dopPOS = (T)g.ax * (T)x + (T)g.ay * (T)y + (T)g.dopshift;
-    const T dopdiff_max = (T)g.dopdiff_max;
-    const T half_w = (T)(g.sinc2width / 2.0);
+    d.dopPOS = k.ax * (T)x + k.ay * (T)y + k.dopshift;
+    const T dopdiff_max = k.dopdiff_max;
+    const T half_w = k.half_w;
     d.idop_min = (int)floor(d.dopPOS - dopdiff_max + 1 - half_w);
     d.idop_max = (int)floor(d.dopPOS + dopdiff_max + half_w);
     d.codefactor = (g.codemethod == SHAPE_CODE_SHORT)
-                       ? sinc2<T>((d.dopPOS - (T)g.dopDC_vig) / (T)g.dopfftlen) : (T)1;
+                       ? sinc2<T>((d.dopPOS - k.dopDC_vig) / k.dopfftlen) : (T)1;
     lim.idmin = min(lim.idmin, d.idel_min);
     lim.idmax = max(lim.idmax, d.idel_max);
     lim.ipmin = min(lim.ipmin, d.idop_min);
@@ -266,32 +336,35 @@ template <typename T> __device__ inline void atomic_add_any(T *p, T v) { atomicA
 
 // Delay response of image row idel for a pixel at delay bin delPOS
 // (src/shape/pos2deldop.c:371-425).
+//
+// ddel = delPOS - idel. The fast path forms it as (delPOS - idel_min) - r
+// with a literal r: both subtractions of integers are exact at these
+// magnitudes, so the value is the same as delPOS - (idel_min + r).
 template <typename T>
-__device__ inline T del_resp(const FrameGeom &g, T delPOS, int idel)
+__device__ inline T del_resp(const FrameGeom &g, const DDC<T> &k, T delPOS, T ddel, int idel)
 {
     const int spb = g.spb;
     T dc;
     if (g.codemethod != SHAPE_CODE_LONG_ORIG) {
         if (spb == 1) {
-            dc = tri2<T>(delPOS - (T)idel);
+            dc = tri2<T>(ddel);
         } else if (spb == 2) {
-            T arg = (delPOS - ((T)idel - (T)g.const2)) / (T)g.spb_over_stride;
+            T arg = (delPOS - ((T)idel - k.const2)) / k.spb_over_stride;
             dc = tri<T>(arg) + tri<T>(arg - (T)0.5);
             dc *= dc / 4;
         } else {
             dc = 0;
-            int m_min = max((int)floor((delPOS - (T)idel - (T)g.const2) * (T)g.stride), 0);
-            int m_max = min((int)ceil((delPOS - (T)idel + (T)g.const1) * (T)g.stride), spb) - 1;
-            T arg = (delPOS - ((T)idel - (T)g.const2)) / (T)g.spb_over_stride
-                    - (T)m_min * (T)g.one_over_spb;
+            int m_min = max((int)floor((ddel - k.const2) * k.stride), 0);
+            int m_max = min((int)ceil((ddel + k.const1) * k.stride), spb) - 1;
+            T arg = (delPOS - ((T)idel - k.const2)) / k.spb_over_stride - (T)m_min * k.one_over_spb;
             for (int m = m_min; m <= m_max; m++) {
                 dc += tri<T>(arg);
-                arg -= (T)g.one_over_spb;
+                arg -= k.one_over_spb;
             }
-            dc *= dc / (T)g.spb_sq;
+            dc *= dc / k.spb_sq;
         }
     } else {
-        dc = tri2<T>((delPOS - (T)idel) / (T)g.spb_over_stride);
+        dc = tri2<T>(ddel / k.spb_over_stride);
     }
     return dc;
 }
@@ -299,30 +372,31 @@ __device__ inline T del_resp(const FrameGeom &g, T delPOS, int idel)
 // Mean sinc^2 Doppler response of column idop over nsinc2^2 points
 // (src/shape/pos2deldop.c:432-460); s2u = sin^2(pi * frac(dopPOS)) serves
 // the nsinc2 == 1 case, where sin^2(pi*(dopPOS - idop)) = s2u.
+// ddop = dopPOS - idop, formed like ddel above.
 template <typename T>
-__device__ inline T dop_resp(const FrameGeom &g, T dopPOS, T s2u, int idop)
+__device__ inline T dop_resp(const FrameGeom &g, const DDC<T> &k, T dopPOS, T ddop, T s2u, int idop)
 {
     const int nsinc2 = g.nsinc2;
     if (nsinc2 == 1) {
-        const T t = fabs((T)3.141592653589793 * (dopPOS - (T)idop));
+        const T t = fabs((T)3.141592653589793 * ddop);
         return (t > (T)1.0e-4) ? s2u / (t * t) : (T)1.0;
     }
     if (nsinc2 == 2) {
-        T bl = dopPOS + (T)g.dopdiff_bl - (T)idop;
-        return (sinc2<T>(bl) + sinc2<T>(bl + (T)g.xincr) + sinc2<T>(bl + (T)g.yincr) +
-                sinc2<T>(bl + (T)g.xincr + (T)g.yincr)) / 4;
+        T bl = dopPOS + k.dopdiff_bl - (T)idop;
+        return (sinc2<T>(bl) + sinc2<T>(bl + k.xincr) + sinc2<T>(bl + k.yincr) +
+                sinc2<T>(bl + k.xincr + k.yincr)) / 4;
     }
-    T left = dopPOS + (T)g.dopdiff_bl - (T)idop;
+    T left = dopPOS + k.dopdiff_bl - (T)idop;
     T sm = 0;
     for (int i = 0; i < nsinc2; i++) {
         T arg = left;
         for (int j = 0; j < nsinc2; j++) {
             sm += sinc2<T>(arg);
-            arg += (T)g.xincr;
+            arg += k.xincr;
         }
-        left += (T)g.yincr;
+        left += k.yincr;
     }
-    return sm / (T)g.nsinc2_sq;
+    return sm / k.nsinc2_sq;
 }
 
 // Footprint sizes of the register-resident fast path.
@@ -337,8 +411,8 @@ constexpr int FAST_COLS = 8;
 // sinc2width<=7 case) keep their weights in registers and scatter through
 // fully unrolled, predicated loops, so the lanes of a warp stay converged.
 template <typename T>
-__device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, T cose, const PixDD<T> &d,
-                                 T *dst, int row0, int col0, int stride)
+__device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const DDC<T> &k, T cose,
+                                 const PixDD<T> &d, T *dst, int row0, int col0, int stride)
 {
     const T delPOS = d.delPOS, dopPOS = d.dopPOS;
     const int idel_min = d.idel_min, idel_max = d.idel_max, idop_min = d.idop_min, idop_max = d.idop_max;
@@ -348,19 +422,20 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, T cose
         const T su = tsin<T>((T)3.141592653589793 * (dopPOS - floor(dopPOS)));
         s2u = su * su;
     }
-    const T kmpp = (T)g.kmpp;
+    const T kmpp = k.kmpp;
     const T rl = radlaw_dev<T>(a.laws[g.law], cose) * kmpp * kmpp * d.codefactor;
     if (nr <= FAST_ROWS && nc <= FAST_COLS) {
         T dc[FAST_ROWS], pc[FAST_COLS];
         T sdel = 0, sdop = 0;
+        const T ddel0 = delPOS - (T)idel_min, ddop0 = dopPOS - (T)idop_min;
 #pragma unroll
         for (int r = 0; r < FAST_ROWS; r++) {
-            dc[r] = (r < nr) ? del_resp<T>(g, delPOS, idel_min + r) : (T)0;
+            dc[r] = (r < nr) ? del_resp<T>(g, k, delPOS, ddel0 - (T)r, idel_min + r) : (T)0;
             if (r < nr) sdel += dc[r];
         }
 #pragma unroll
         for (int c = 0; c < FAST_COLS; c++) {
-            pc[c] = (c < nc) ? dop_resp<T>(g, dopPOS, s2u, idop_min + c) : (T)0;
+            pc[c] = (c < nc) ? dop_resp<T>(g, k, dopPOS, ddop0 - (T)c, s2u, idop_min + c) : (T)0;
             if (c < nc) sdop += pc[c];
         }
         // sum of del_c*dop_c over the footprint = (sum del_c) * (sum dop_c)
@@ -379,9 +454,9 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, T cose
     T del_c[SHAPE_MAXBINS];
     T dop_c[SHAPE_MAXBINS + 1];
     for (int idel = idel_min; idel <= idel_max; idel++)
-        del_c[idel - idel_min] = del_resp<T>(g, delPOS, idel);
+        del_c[idel - idel_min] = del_resp<T>(g, k, delPOS, delPOS - (T)idel, idel);
     for (int idop = idop_min; idop <= idop_max; idop++)
-        dop_c[min(idop - idop_min, SHAPE_MAXBINS)] = dop_resp<T>(g, dopPOS, s2u, idop);
+        dop_c[min(idop - idop_min, SHAPE_MAXBINS)] = dop_resp<T>(g, k, dopPOS, dopPOS - (T)idop, s2u, idop);
     T sdel = 0, sdop = 0;
     for (int idel = idel_min; idel <= idel_max; idel++) sdel += del_c[idel - idel_min];
     for (int idop = idop_min; idop <= idop_max; idop++) sdop += dop_c[min(idop - idop_min, SHAPE_MAXBINS)];
@@ -460,12 +535,14 @@ k_raster(RasterArgs a)
             const int bb = s.bb;
             if (li < (bb & 15) || li > ((bb >> 4) & 15) || lj < ((bb >> 8) & 15) || lj > ((bb >> 12) & 15))
                 return;
-            const T dx = x0 - s.v00, dy = x1 - s.v01;
-            const T sv = (dx * s.A - s.B * dy) * s.den;
+            const auto p0 = s.p0, p1 = s.p1;
+            const T dx = x0 - p0.x, dy = x1 - p0.y;
+            const T sv = (dx * p0.z - p0.w * dy) * p1.x;
             if (!((sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL))) return;
-            const T tv = (s.C * dy - dx * s.D) * s.den;
+            const T tv = (p1.y * dy - dx * p1.z) * p1.x;
             if (!((tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL))) return;
-            const T z = s.v02 + sv * s.E + tv * s.F;
+            const auto p2 = s.p2;
+            const T z = p1.w + sv * p2.x + tv * p2.y;
             if (!((z > zz) || (fac < 0))) return;
             zz = z;
             fac = s.f;
@@ -481,7 +558,7 @@ k_raster(RasterArgs a)
                 r2 += oa6 * m0; r2 += oa7 * m1; r2 += oa8 * m2;
                 if (r2 > (T)0) { good = true; gm0 = m0; gm1 = m1; gm2 = m2; }
             } else {
-                good = true; gm0 = s.nx; gm1 = s.ny; gm2 = s.nz;
+                good = true; gm0 = p2.z; gm1 = p2.w; gm2 = s.nz;
             }
         };
         // Each warp walks only the staged facets whose bbox meets its block,
@@ -552,10 +629,12 @@ k_raster(RasterArgs a)
         // viewer: cotrans + normalize (posvis.c:250-274), once per pixel
         if (good) {
             T n0 = gm0, n1 = gm1, n2 = gm2;
+            T oa[12];
+            load_oa<T>(g, oa);
             if (smooth) {
                 T r0 = 0, r1 = 0, r2 = 0;
-                r0 += (T)g.oa[0] * gm0; r0 += (T)g.oa[1] * gm1; r0 += (T)g.oa[2] * gm2;
-                r1 += (T)g.oa[3] * gm0; r1 += (T)g.oa[4] * gm1; r1 += (T)g.oa[5] * gm2;
+                r0 += oa[0] * gm0; r0 += oa[1] * gm1; r0 += oa[2] * gm2;
+                r1 += oa[3] * gm0; r1 += oa[4] * gm1; r1 += oa[5] * gm2;
                 r2 += oa6 * gm0; r2 += oa7 * gm1; r2 += oa8 * gm2;
                 T norm = 0;
                 norm += r0 * r0; norm += r1 * r1; norm += r2 * r2;
@@ -566,7 +645,7 @@ k_raster(RasterArgs a)
             if (n2 > (T)0) {
                 cosa = n2;
                 if (bistatic_obs) {
-                    cosb = n0 * (T)g.usrc[0] + n1 * (T)g.usrc[1] + n2 * (T)g.usrc[2];
+                    cosb = n0 * oa[9] + n1 * oa[10] + n2 * oa[11];
                     if (cosb <= (T)0) cosa = 0;
                 }
             }
@@ -597,6 +676,7 @@ k_raster(RasterArgs a)
             if (a.mark_seen && (double)cosa > a.mincosine_seen)
                 a.seen[fac] = 1;
         }
+        const DDC<T> kc = load_ddc<T>(g);
         if (g.kind == VIEW_RADAR) {
             // Synthesis runs on a permuted pixel-to-thread map: the replay
             // wants each warp on a compact 4x8 block, but neighbouring pixels
@@ -611,7 +691,7 @@ k_raster(RasterArgs a)
             scose = s_pc[q];
             if (scose > (T)0) {
                 lit = true;
-                dd = pixel_dd_setup<T>(g, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], lim);
+                dd = pixel_dd_setup<T>(g, kc, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], lim);
             }
         }
         if (g.kind == VIEW_RADAR) {
@@ -636,7 +716,7 @@ k_raster(RasterArgs a)
                 if (cells <= (long long)(a.smem_bytes / sizeof(T))) {
                     for (long long k = tid; k < cells; k += RASTER_THREADS) box[k] = (T)0;
                     __syncthreads();
-                    if (dd.ok) pixel_dd_scatter<T>(a, g, scose, dd, box, r0, c0, nc);
+                    if (dd.ok) pixel_dd_scatter<T>(a, g, kc, scose, dd, box, r0, c0, nc);
                     __syncthreads();
                     for (long long k = tid; k < cells; k += RASTER_THREADS) {
                         T v = box[k];
@@ -646,7 +726,7 @@ k_raster(RasterArgs a)
                         }
                     }
                 } else if (dd.ok) {
-                    pixel_dd_scatter<T>(a, g, scose, dd, fit, 1, 1, g.ndop);
+                    pixel_dd_scatter<T>(a, g, kc, scose, dd, fit, 1, 1, g.ndop);
                 }
             }
         }

@@ -1,0 +1,472 @@
+/*
+ * Drop-in replacement of the reference's calc_fits for the B200 engine.
+ *
+ * This file is compiled INSIDE the reference tree, next to
+ * src/shape/calc_fits.c, with the reference's own head.h, and linked against
+ * libshape_b200.so:
+ *
+ *   void calc_fits(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
+ *       keeps the signature of src/shape/calc_fits.c:340 (declared at
+ *       src/shape/shape2.h:1451). It evaluates every dataset on the GPU and
+ *       writes back what the reference's calc_fits leaves in par, mod and dat:
+ *       par->posbnd / posbnd_logfactor / badradar / badradar_logfactor
+ *       (src/shape/calc_fits.c:349-354, 407-409), facet "seen" flags
+ *       (:358-360, 522-530), every delay-Doppler frame's fit image, region
+ *       limits and badradar_logfactor (src/shape/pos2deldop.c:279-288,
+ *       337-354, 543-548), every lightcurve's y and fit arrays
+ *       (src/shape/calc_fits.c:1712-1716, 1923-1933), and, for the write
+ *       action, the POS z / cos(e) / facet images. The reference's chi2()
+ *       (src/shape/chi2.c:240) then runs unchanged on those images.
+ *
+ *   double calc_fits_chi2_b200(struct par_t *par, struct mod_t *mod,
+ *                              struct dat_t *dat)
+ *       replaces the two lines `calc_fits(spar, smod, sdat); err =
+ *       chi2(spar, sdat, 0);` of objective() (src/shape/bestfit.c:789-790).
+ *       It evaluates on the GPU and copies back only the totals: the par
+ *       flags above, cal and chi2 of every frame and lightcurve, set chi2 and
+ *       dat->chi2, which it returns. No fit image crosses PCIe.
+ *
+ * The engine is built on the first call and rebuilt whenever the data or
+ * the view geometry change (a fingerprint of everything except the free
+ * shape parameters is compared on every call); the vertex deviations r and
+ * the component scale factors, the parameters bestfit varies in a shape fit
+ * (src/shape/mkparlist.c:218-235), are pushed on every call.
+ *
+ * Supported inputs (anything else stops with bailout(), the reference's
+ * error convention): one VERTEX component; delay-Doppler and lightcurve
+ * sets with one view per frame/point; radar laws COSINELAW_DIFF,
+ * GAUSSIANLAW, HAGFORSLAW, COSINELAW_QS and the three hybrids; optical laws
+ * LAMBERTLAW, LOMMEL and KAASALAINEN; dd_gamma = 1; exclude_seen not naming
+ * a set of the dataset.
+ *
+ * Environment: SHAPE_B200_FORM = plain_fp64 | batched_fp64 (default) |
+ * batched_fp32; SHAPE_B200_DEVICE = CUDA device index (default 0).
+ * Set SHAPE_B200_CALC_FITS to another name at compile time to build the
+ * replacement beside the reference's own calc_fits (as the tests do).
+ */
+#include "head.h"
+
+#include <stdint.h>
+
+#include "shape_b200.h"
+
+#ifndef SHAPE_B200_CALC_FITS
+#define SHAPE_B200_CALC_FITS calc_fits
+#endif
+#ifndef SHAPE_B200_CALC_FITS_CHI2
+#define SHAPE_B200_CALC_FITS_CHI2 calc_fits_chi2_b200
+#endif
+
+static shape_engine *g_eng = NULL;
+static uint64_t g_fingerprint = 0;
+static int g_form = SHAPE_FORM_BATCHED_FP64;
+static int g_keep_pos = 0;
+
+static void b200_fail(const char *what)
+{
+    static char msg[600];
+    snprintf(msg, sizeof msg, "shape_b200: %s: %s\n", what, shape_last_error());
+    bailout(msg);
+}
+
+static void b200_check(int rc, const char *what)
+{
+    if (rc < 0) b200_fail(what);
+}
+
+static void b200_unsupported(const char *what)
+{
+    static char msg[600];
+    snprintf(msg, sizeof msg, "shape_b200: unsupported input: %s\n", what);
+    bailout(msg);
+}
+
+/* ------------------------------------------------------------ fingerprint */
+
+static uint64_t fnv(uint64_t h, const void *p, size_t n)
+{
+    const unsigned char *b = (const unsigned char *)p;
+    for (size_t k = 0; k < n; k++) {
+        h ^= b[k];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+#define FNV(h, x) ((h) = fnv((h), &(x), sizeof(x)))
+
+/* Everything the engine was built from except the free shape parameters. */
+static uint64_t b200_fingerprint(const struct par_t *par, const struct mod_t *mod,
+                                 const struct dat_t *dat)
+{
+    uint64_t h = 1469598103934665603ULL;
+    const void *pm = mod, *pd = dat;
+    FNV(h, pm); FNV(h, pd);
+    FNV(h, par->pos_smooth); FNV(h, par->nsinc2); FNV(h, par->sinc2width);
+    FNV(h, par->mask_tol); FNV(h, par->mincosine_seen); FNV(h, par->exclude_seen);
+    FNV(h, par->bad_objfactor); FNV(h, par->action);
+    FNV(h, mod->shape.ncomp);
+    const struct photo_t *ph = &mod->photo;
+    for (int k = 0; k < ph->nradlaws; k++) {
+        FNV(h, ph->radtype[k]);
+        h = fnv(h, &ph->radar[k], sizeof(union radscat_t));
+    }
+    for (int k = 0; k < ph->noptlaws; k++) {
+        FNV(h, ph->opttype[k]);
+        h = fnv(h, &ph->optical[k], sizeof(union optscat_t));
+    }
+    FNV(h, dat->nsets);
+    for (int s = 0; s < dat->nsets; s++) {
+        const struct set_t *set = &dat->set[s];
+        FNV(h, set->type);
+        if (set->type == DELAY) {
+            const struct deldop_t *dd = &set->desc.deldop;
+            FNV(h, dd->nframes); FNV(h, dd->nviews); FNV(h, dd->iradlaw);
+            FNV(h, dd->del_per_pixel); FNV(h, dd->dop_per_pixel); FNV(h, dd->Ftx);
+            FNV(h, dd->dopscale.val); FNV(h, dd->codemethod); FNV(h, dd->spb);
+            FNV(h, dd->stride); FNV(h, dd->dopfftlen);
+            for (int f = 0; f < dd->nframes; f++) {
+                const struct deldopfrm_t *fr = &dd->frame[f];
+                FNV(h, fr->ndel); FNV(h, fr->ndop); FNV(h, fr->pos.n);
+                FNV(h, fr->pos.km_per_pixel); FNV(h, fr->weight); FNV(h, fr->dof);
+                FNV(h, fr->cal.state);
+                if (fr->cal.state != 'f') FNV(h, fr->cal.val);
+                FNV(h, fr->delcom_vig); FNV(h, fr->dopcom_vig); FNV(h, fr->dopDC_vig);
+                const void *po = fr->obs, *pv = fr->oneovervar;
+                FNV(h, po); FNV(h, pv);
+                const struct deldopview_t *v = &fr->view[dd->v0];
+                FNV(h, v->ae); FNV(h, v->oe); FNV(h, v->spin); FNV(h, v->deloff); FNV(h, v->dopoff);
+            }
+        } else if (set->type == LGHTCRV) {
+            const struct lghtcrv_t *lc = &set->desc.lghtcrv;
+            FNV(h, lc->n); FNV(h, lc->ncalc); FNV(h, lc->nviews); FNV(h, lc->ioptlaw);
+            FNV(h, lc->weight); FNV(h, lc->dof); FNV(h, lc->cal.state);
+            if (lc->cal.state != 'f') FNV(h, lc->cal.val);
+            const void *po = lc->obs, *pv = lc->oneovervar;
+            FNV(h, po); FNV(h, pv);
+            for (int i = 1; i <= lc->n; i++) FNV(h, lc->t[i][lc->v0]);
+            for (int i = 1; i <= lc->ncalc; i++) {
+                const struct crvrend_t *r = &lc->rend[i];
+                FNV(h, lc->x[i]); FNV(h, lc->solar_phase[i]);
+                FNV(h, r->pos.n); FNV(h, r->pos.km_per_pixel);
+                FNV(h, r->ae); FNV(h, r->oe); FNV(h, r->se);
+            }
+        }
+    }
+    return h;
+}
+
+/* ------------------------------------------------------------ conversion */
+
+static void rm9(double out[9], double in[3][3])
+{
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) out[3 * i + j] = in[i][j];
+}
+
+static shape_radar_law radar_law_of(const struct photo_t *ph, int ilaw)
+{
+    shape_radar_law L;
+    memset(&L, 0, sizeof L);
+    if (ilaw < 0 || ilaw >= ph->nradlaws) b200_unsupported("radar law index out of range");
+    L.type = ph->radtype[ilaw];
+    const union radscat_t *r = &ph->radar[ilaw];
+    switch (L.type) {
+    case COSINELAW_DIFF:
+        L.diff_R = r->RC.R.val; L.diff_C = r->RC.C.val; break;
+    case GAUSSIANLAW: case HAGFORSLAW: case COSINELAW_QS:
+        L.qs_R = r->quasispec.R.val; L.qs_C = r->quasispec.C.val;
+        L.qs_cos_cutoff = r->quasispec.cos_cutoff; break;
+    case GAUSSIAN_COSINE: case HAGFORS_COSINE: case COSINE_COSINE:
+        L.qs_R = r->hybrid.qs.R.val; L.qs_C = r->hybrid.qs.C.val;
+        L.qs_cos_cutoff = r->hybrid.qs.cos_cutoff;
+        L.diff_R = r->hybrid.diff.R.val; L.diff_C = r->hybrid.diff.C.val; break;
+    default:
+        b200_unsupported("radar scattering law (facet-dependent or tabular)");
+    }
+    return L;
+}
+
+static shape_optical_law optical_law_of(const struct photo_t *ph, int ilaw)
+{
+    shape_optical_law L;
+    memset(&L, 0, sizeof L);
+    if (ilaw < 0 || ilaw >= ph->noptlaws) b200_unsupported("optical law index out of range");
+    L.type = ph->opttype[ilaw];
+    const union optscat_t *o = &ph->optical[ilaw];
+    switch (L.type) {
+    case LAMBERTLAW: case LOMMEL:
+        L.R = o->R.R.val; break;
+    case KAASALAINEN:
+        L.R = o->kaas.R.val; L.wt = o->kaas.wt.val; L.A0 = o->kaas.A0.val;
+        L.D = o->kaas.D.val; L.k = o->kaas.k.val; break;
+    default:
+        b200_unsupported("optical scattering law (Hapke or facet-dependent)");
+    }
+    return L;
+}
+
+static void b200_build(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
+{
+    if (mod->shape.ncomp != 1 || mod->shape.comp[0].type != VERTEX)
+        b200_unsupported("model must be a single VERTEX component");
+    if (par->dd_gamma != 1.0) b200_unsupported("dd_gamma != 1");
+    if (par->exclude_seen >= 0 && par->exclude_seen < dat->nsets)
+        b200_unsupported("exclude_seen names a dataset");
+    const char *fs = getenv("SHAPE_B200_FORM");
+    g_form = SHAPE_FORM_BATCHED_FP64;
+    if (fs && !strcmp(fs, "plain_fp64")) g_form = SHAPE_FORM_PLAIN_FP64;
+    if (fs && !strcmp(fs, "batched_fp32")) g_form = SHAPE_FORM_BATCHED_FP32;
+    const char *ds = getenv("SHAPE_B200_DEVICE");
+    int device = ds ? atoi(ds) : 0;
+
+    if (g_eng) shape_engine_destroy(g_eng);
+    g_eng = NULL;
+    b200_check(shape_engine_create(device, &g_eng), "engine_create");
+
+    struct comp_t *c = &mod->shape.comp[0];
+    struct vertices_t *real = &c->real;
+    int nv = real->nv, nf = real->nf;
+    double *a = malloc(sizeof(double) * 3 * nv), *u = malloc(sizeof(double) * 3 * nv);
+    double *r = malloc(sizeof(double) * nv);
+    int *fv = malloc(sizeof(int) * 3 * nf), *afp = malloc(sizeof(int) * (nv + 1));
+    int naf = 0;
+    for (int i = 0; i < nv; i++) naf += real->v[i].naf;
+    int *afi = malloc(sizeof(int) * (naf > 0 ? naf : 1));
+    afp[0] = 0;
+    for (int i = 0; i < nv; i++) {
+        for (int j = 0; j < 3; j++) { a[3 * i + j] = real->v[i].a[j]; u[3 * i + j] = real->v[i].u[j]; }
+        r[i] = real->v[i].r.val;
+        for (int k = 0; k < real->v[i].naf; k++) afi[afp[i] + k] = real->v[i].af[k];
+        afp[i + 1] = afp[i] + real->v[i].naf;
+    }
+    for (int f = 0; f < nf; f++)
+        for (int j = 0; j < 3; j++) fv[3 * f + j] = real->f[f].v[j];
+    shape_model_desc m;
+    m.nv = nv; m.nf = nf; m.a = a; m.u = u; m.r = r; m.fv = fv; m.af_ptr = afp; m.af_idx = afi;
+    for (int j = 0; j < 3; j++) m.scale[j] = c->desc.ver.scalefactor[j].val;
+    b200_check(shape_engine_set_model(g_eng, &m), "set_model");
+    free(a); free(u); free(r); free(fv); free(afp); free(afi);
+
+    shape_eval_params ep;
+    ep.pos_smooth = par->pos_smooth;
+    ep.nsinc2 = par->nsinc2;
+    ep.sinc2width = par->sinc2width;
+    ep.mask_tol = par->mask_tol;
+    ep.mincosine_seen = par->mincosine_seen;
+    ep.mark_seen = 1;
+    b200_check(shape_engine_set_params(g_eng, &ep), "set_params");
+
+    for (int s = 0; s < dat->nsets; s++) {
+        struct set_t *set = &dat->set[s];
+        if (set->type == DELAY) {
+            struct deldop_t *dd = &set->desc.deldop;
+            if (dd->nviews != 1) b200_unsupported("delay-Doppler smearing (nviews > 1)");
+            shape_deldop_set S;
+            S.del_per_pixel = dd->del_per_pixel; S.dop_per_pixel = dd->dop_per_pixel;
+            S.Ftx = dd->Ftx; S.dopscale = dd->dopscale.val; S.codemethod = dd->codemethod;
+            S.spb = dd->spb; S.stride = dd->stride; S.dopfftlen = dd->dopfftlen;
+            S.law = radar_law_of(&mod->photo, dd->iradlaw);
+            shape_deldop_frame *F = calloc((size_t)dd->nframes, sizeof *F);
+            size_t total = 0;
+            for (int f = 0; f < dd->nframes; f++) total += (size_t)dd->frame[f].ndel * dd->frame[f].ndop;
+            double *obs = malloc(sizeof(double) * (total ? total : 1));
+            double *oov = malloc(sizeof(double) * (total ? total : 1));
+            size_t off = 0;
+            for (int f = 0; f < dd->nframes; f++) {
+                struct deldopfrm_t *fr = &dd->frame[f];
+                struct deldopview_t *v = &fr->view[dd->v0];
+                shape_deldop_frame *G = &F[f];
+                G->pos_n = fr->pos.n; G->km_per_pixel = fr->pos.km_per_pixel;
+                rm9(G->ae, v->ae); rm9(G->oe, v->oe);
+                for (int j = 0; j < 3; j++) G->spin[j] = v->spin[j];
+                G->deloff = v->deloff; G->dopoff = v->dopoff;
+                G->ndel = fr->ndel; G->ndop = fr->ndop;
+                G->delcom_vig = fr->delcom_vig; G->dopcom_vig = fr->dopcom_vig;
+                G->dopDC_vig = fr->dopDC_vig;
+                G->weight = fr->weight; G->dof = fr->dof;
+                G->cal_floating = (fr->cal.state == 'f');
+                G->cal = fr->cal.val;
+                for (int i = 1; i <= fr->ndel; i++)
+                    for (int j = 1; j <= fr->ndop; j++, off++) {
+                        obs[off] = fr->obs[i][j];
+                        oov[off] = fr->oneovervar[i][j];
+                    }
+            }
+            int rc = shape_engine_add_deldop_set(g_eng, &S, dd->nframes, F, obs, oov);
+            free(F); free(obs); free(oov);
+            b200_check(rc, "add_deldop_set");
+        } else if (set->type == LGHTCRV) {
+            struct lghtcrv_t *lc = &set->desc.lghtcrv;
+            if (lc->nviews != 1) b200_unsupported("lightcurve smearing (nviews > 1)");
+            shape_lghtcrv_set L;
+            double *x = malloc(sizeof(double) * lc->ncalc), *t = malloc(sizeof(double) * lc->n);
+            double *obs = malloc(sizeof(double) * lc->n), *oov = malloc(sizeof(double) * lc->n);
+            for (int i = 1; i <= lc->ncalc; i++) x[i - 1] = lc->x[i];
+            for (int i = 1; i <= lc->n; i++) {
+                t[i - 1] = lc->t[i][lc->v0];
+                obs[i - 1] = lc->obs[i];
+                oov[i - 1] = lc->oneovervar[i];
+            }
+            L.ncalc = lc->ncalc; L.n = lc->n; L.x = x; L.t = t; L.obs = obs; L.oneovervar = oov;
+            L.weight = lc->weight; L.dof = lc->dof;
+            L.cal_floating = (lc->cal.state == 'f'); L.cal = lc->cal.val;
+            L.law = optical_law_of(&mod->photo, lc->ioptlaw);
+            shape_lghtcrv_point *P = calloc((size_t)lc->ncalc, sizeof *P);
+            for (int i = 1; i <= lc->ncalc; i++) {
+                struct crvrend_t *rd = &lc->rend[i];
+                P[i - 1].pos_n = rd->pos.n;
+                P[i - 1].km_per_pixel = rd->pos.km_per_pixel;
+                rm9(P[i - 1].ae, rd->ae); rm9(P[i - 1].oe, rd->oe); rm9(P[i - 1].se, rd->se);
+                P[i - 1].solar_phase = lc->solar_phase[i];
+            }
+            int rc = shape_engine_add_lghtcrv_set(g_eng, &L, P);
+            free(x); free(t); free(obs); free(oov); free(P);
+            b200_check(rc, "add_lghtcrv_set");
+        } else {
+            b200_unsupported("Doppler and plane-of-sky datasets");
+        }
+    }
+    g_keep_pos = (par->action == WRITE);
+    b200_check(shape_engine_keep_pos(g_eng, g_keep_pos), "keep_pos");
+    b200_check(shape_engine_finalize(g_eng), "finalize");
+}
+
+/* Builds or reuses the engine, pushes the free shape parameters, evaluates. */
+static void b200_evaluate(struct par_t *par, struct mod_t *mod, struct dat_t *dat,
+                          shape_eval_summary *sm)
+{
+    uint64_t fp = b200_fingerprint(par, mod, dat);
+    if (!g_eng || fp != g_fingerprint) {
+        b200_build(par, mod, dat);
+        g_fingerprint = fp;
+    }
+    struct comp_t *c = &mod->shape.comp[0];
+    for (int j = 0; j < 3; j++)
+        b200_check(shape_engine_set_scale(g_eng, j, c->desc.ver.scalefactor[j].val), "set_scale");
+    for (int i = 0; i < c->real.nv; i++)
+        b200_check(shape_engine_set_vertex_r(g_eng, i, c->real.v[i].r.val), "set_vertex_r");
+    b200_check(shape_engine_evaluate(g_eng, g_form, sm), "evaluate");
+
+    /* flags of calc_fits (src/shape/calc_fits.c:349-354, 407-409) */
+    par->posbnd = sm->posbnd;
+    par->posbnd_logfactor = sm->posbnd_logfactor;
+    par->badradar = sm->badradar;
+    par->badradar_logfactor = sm->badradar_logfactor;
+    par->badposet = 0;
+    par->badposet_logfactor = 0.0;
+
+    /* facet "seen" flags */
+    int nf = c->real.nf;
+    unsigned char *seen = malloc((size_t)nf);
+    b200_check(shape_engine_get_seen(g_eng, seen), "get_seen");
+    for (int f = 0; f < nf; f++) c->real.f[f].seen = seen[f];
+    free(seen);
+}
+
+static int total_frames(const struct dat_t *dat)
+{
+    int n = 0;
+    for (int s = 0; s < dat->nsets; s++)
+        if (dat->set[s].type == DELAY) n += dat->set[s].desc.deldop.nframes;
+    return n;
+}
+
+/* Per-frame limits, log-factor, cal and chi2 from the engine's results. */
+static void copy_frame_results(struct dat_t *dat, int with_chi2)
+{
+    int nfr = total_frames(dat);
+    if (nfr == 0) return;
+    shape_deldop_result *R = malloc(sizeof *R * (size_t)nfr);
+    b200_check(shape_engine_get_deldop_results(g_eng, R, nfr), "get_deldop_results");
+    int g = 0;
+    for (int s = 0; s < dat->nsets; s++) {
+        if (dat->set[s].type != DELAY) continue;
+        struct deldop_t *dd = &dat->set[s].desc.deldop;
+        double set_chi2 = 0.0;
+        for (int f = 0; f < dd->nframes; f++, g++) {
+            struct deldopfrm_t *fr = &dd->frame[f];
+            const shape_deldop_result *q = &R[g];
+            for (int k = 0; k < 2; k++) {
+                fr->pos.xlim[k] = q->xlim[k]; fr->pos.ylim[k] = q->ylim[k];
+                fr->idellim[k] = q->idellim[k]; fr->idoplim[k] = q->idoplim[k];
+                fr->dellim[k] = q->dellim[k]; fr->doplim[k] = q->doplim[k];
+            }
+            fr->badradar_logfactor = q->badradar_logfactor;
+            fr->pos.posbnd_logfactor = q->posbnd_logfactor;
+            if (with_chi2) {
+                if (fr->cal.state == 'f') fr->cal.val = q->cal;
+                fr->chi2 = q->chi2;
+                set_chi2 += q->chi2;
+            }
+        }
+        if (with_chi2) dat->set[s].chi2 = set_chi2;
+    }
+    free(R);
+}
+
+void SHAPE_B200_CALC_FITS(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
+{
+    shape_eval_summary sm;
+    b200_evaluate(par, mod, dat, &sm);
+    copy_frame_results(dat, 0);
+    size_t maxd = 1;
+    for (int s = 0; s < dat->nsets; s++)
+        if (dat->set[s].type == DELAY)
+            for (int f = 0; f < dat->set[s].desc.deldop.nframes; f++) {
+                size_t D = (size_t)dat->set[s].desc.deldop.frame[f].ndel * dat->set[s].desc.deldop.frame[f].ndop;
+                if (D > maxd) maxd = D;
+            }
+    double *buf = malloc(sizeof(double) * maxd);
+    int g = 0;
+    for (int s = 0; s < dat->nsets; s++) {
+        struct set_t *set = &dat->set[s];
+        if (set->type == DELAY) {
+            struct deldop_t *dd = &set->desc.deldop;
+            for (int f = 0; f < dd->nframes; f++, g++) {
+                struct deldopfrm_t *fr = &dd->frame[f];
+                b200_check(shape_engine_get_fit(g_eng, g, buf), "get_fit");
+                size_t k = 0;
+                for (int i = 1; i <= fr->ndel; i++)
+                    for (int j = 1; j <= fr->ndop; j++) fr->fit[i][j] = buf[k++];
+                if (g_keep_pos) {
+                    int n = fr->pos.n, side = 2 * n + 1;
+                    size_t np = (size_t)side * side;
+                    double *z = malloc(sizeof(double) * np), *ce = malloc(sizeof(double) * np);
+                    int *fa = malloc(sizeof(int) * np);
+                    b200_check(shape_engine_get_pos(g_eng, g, z, ce, fa), "get_pos");
+                    for (int i = -n; i <= n; i++)
+                        for (int j = -n; j <= n; j++) {
+                            size_t p = (size_t)(i + n) * side + (size_t)(j + n);
+                            fr->pos.z[i][j] = z[p]; fr->pos.cose[i][j] = ce[p]; fr->pos.f[i][j] = fa[p];
+                        }
+                    free(z); free(ce); free(fa);
+                }
+            }
+        } else if (set->type == LGHTCRV) {
+            struct lghtcrv_t *lc = &set->desc.lghtcrv;
+            double *y = malloc(sizeof(double) * lc->ncalc), *fit = malloc(sizeof(double) * lc->n);
+            b200_check(shape_engine_get_lghtcrv(g_eng, s, y, fit, NULL, NULL), "get_lghtcrv");
+            for (int i = 1; i <= lc->ncalc; i++) lc->y[i] = y[i - 1];
+            for (int i = 1; i <= lc->n; i++) lc->fit[i] = fit[i - 1];
+            free(y); free(fit);
+        }
+    }
+    free(buf);
+}
+
+double SHAPE_B200_CALC_FITS_CHI2(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
+{
+    shape_eval_summary sm;
+    b200_evaluate(par, mod, dat, &sm);
+    copy_frame_results(dat, 1);
+    for (int s = 0; s < dat->nsets; s++) {
+        struct set_t *set = &dat->set[s];
+        if (set->type != LGHTCRV) continue;
+        double cal, chi2v;
+        b200_check(shape_engine_get_lghtcrv(g_eng, s, NULL, NULL, &cal, &chi2v), "get_lghtcrv");
+        if (set->desc.lghtcrv.cal.state == 'f') set->desc.lghtcrv.cal.val = cal;
+        set->chi2 = chi2v;
+    }
+    dat->chi2 = sm.chi2;
+    return sm.chi2;
+}

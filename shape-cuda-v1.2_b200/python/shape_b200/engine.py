@@ -38,6 +38,24 @@ class FitResult(C.Structure):
                 ("iterations", C.c_int), ("evaluations", C.c_int), ("trace_len", C.c_int)]
 
 
+class Request(C.Structure):
+    _fields_ = [("workload", C.c_int), ("arrival_s", C.c_double), ("scale", C.c_double * 3)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("chi2", C.c_double), ("objective", C.c_double), ("t_start", C.c_double),
+                ("t_done", C.c_double), ("latency_s", C.c_double), ("device_ms", C.c_double),
+                ("instance", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("span_s", C.c_double), ("requests_per_s", C.c_double), ("frame_evals_per_s", C.c_double),
+                ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double),
+                ("mean_concurrency", C.c_double), ("peak_concurrency", C.c_int),
+                ("instances_created", C.c_int), ("instances_evicted", C.c_int),
+                ("peak_hbm_bytes", C.c_double)]
+
+
 class EvalSummary(C.Structure):
     _fields_ = [("chi2", C.c_double), ("dof", C.c_double), ("chi2_deldop", C.c_double),
                 ("chi2_lghtcrv", C.c_double), ("posbnd", C.c_int), ("posbnd_logfactor", C.c_double),
@@ -93,6 +111,12 @@ def load_library(path=LIB_PATH):
     L.shape_engine_get_scale.argtypes = [vp, C.c_int, P(C.c_double)]
     L.shape_chi2_frames_noalloc.argtypes = [C.c_int, C.c_int, P(C.c_longlong), C.c_void_p, C.c_void_p,
                                             C.c_void_p, cd.dptr, cd.iptr, cd.dptr, cd.dptr]
+    L.shape_engine_kernels_per_eval.argtypes = [vp, C.c_int, P(C.c_int)]
+    L.shape_server_create.argtypes = [C.c_int, C.c_size_t, C.c_int, P(vp)]
+    L.shape_server_destroy.argtypes = [vp]
+    L.shape_server_add_workload.argtypes = [vp, vp, C.c_int]
+    L.shape_server_workload_bytes.argtypes = [vp, C.c_int, P(C.c_size_t)]
+    L.shape_server_run.argtypes = [vp, P(Request), C.c_int, P(RequestResult), P(ServerStats)]
     _lib = L
     return L
 
@@ -220,6 +244,11 @@ class Engine:
         _chk(self.L.shape_engine_evaluate(self.h, form, C.byref(s)))
         return _summary_dict(s)
 
+    def kernels_per_eval(self, form):
+        n = C.c_int()
+        _chk(self.L.shape_engine_kernels_per_eval(self.h, form, C.byref(n)))
+        return n.value
+
     def last_ms(self):
         v = C.c_double()
         _chk(self.L.shape_engine_last_time_ms(self.h, C.byref(v)))
@@ -321,3 +350,110 @@ def engine_synthesizer(model, device=0):
         e.close()
         return y
     return deldop, lghtcrv
+
+
+class Server:
+    """Continuous-batching evaluation server on one device (shape_server_*).
+
+    Workloads are registered from configured engines; run() replays a trace of
+    (workload, arrival time, scale factors) requests and returns per-request
+    results and the trace's statistics."""
+
+    def __init__(self, device=0, hbm_budget_bytes=8 << 30, max_slots=8):
+        self.L = load_library()
+        h = C.c_void_p()
+        _chk(self.L.shape_server_create(device, hbm_budget_bytes, max_slots, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.L.shape_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_workload(self, engine, form=FORM_BATCHED_FP32):
+        return _chk(self.L.shape_server_add_workload(self.h, engine.h, form))
+
+    def workload_bytes(self, w):
+        b = C.c_size_t()
+        _chk(self.L.shape_server_workload_bytes(self.h, w, C.byref(b)))
+        return b.value
+
+    def run(self, requests):
+        """requests: sequence of (workload, arrival_s, (s0, s1, s2)).
+        Returns (list of result dicts, stats dict)."""
+        n = len(requests)
+        req = (Request * n)()
+        for i, (w, t, sc) in enumerate(requests):
+            req[i].workload = w
+            req[i].arrival_s = t
+            for j in range(3):
+                req[i].scale[j] = sc[j]
+        res = (RequestResult * n)()
+        st = ServerStats()
+        _chk(self.L.shape_server_run(self.h, req, n, res, C.byref(st)))
+        out = [{k: getattr(r, k) for k, _ in RequestResult._fields_} for r in res]
+        return out, {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+
+PARAM_OBJECTIVE = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int),
+                              C.POINTER(C.c_int))
+
+
+def bestfit_host(objective, values, params, term_prec=1e-4, term_maxiter=0, trace_max=0):
+    """shape_bestfit_host: the bestfit iteration on a host objective.
+    objective(values) -> (objective value, posbnd, badradar); values: start
+    values of the free parameters (updated in place)."""
+    L = load_library()
+    L.shape_bestfit_host.argtypes = [PARAM_OBJECTIVE, C.c_void_p, cd.dptr, C.POINTER(FitParam), C.c_int,
+                                     C.POINTER(FitOptions), C.POINTER(FitResult), cd.dptr, C.c_int]
+    n = len(params)
+
+    def cb(vals, user, posbnd, badradar):
+        v, pb, br = objective(np.ctypeslib.as_array(vals, shape=(n,)))
+        posbnd[0], badradar[0] = int(pb), int(br)
+        return v
+    fn = PARAM_OBJECTIVE(cb)
+    arr = (FitParam * n)(*[FitParam(*t) for t in params])
+    opt = FitOptions(0, term_prec, term_maxiter)
+    res = FitResult()
+    vals = np.ascontiguousarray(values, dtype=np.float64)
+    tr = np.zeros(2 * max(1, trace_max))
+    _chk(L.shape_bestfit_host(fn, None, cd.as_dptr(vals), arr, n, C.byref(opt), C.byref(res),
+                              cd.as_dptr(tr) if trace_max else None, trace_max))
+    values[:] = vals
+    return {k: getattr(res, k) for k, _ in FitResult._fields_}
+
+
+def register_workloads(server, work, params, form, device=0):
+    """Registers every (category, model, deldop datasets, lightcurve
+    datasets) entry of `work` with the server in one form; returns the
+    workload indices."""
+    ids = []
+    for _, model, dds, lcs in work:
+        e = Engine(device)
+        e.set_model(model)
+        e.set_params(params)
+        for ds in dds:
+            e.add_deldop(ds)
+        for ds in lcs:
+            e.add_lghtcrv(ds)
+        ids.append(server.add_workload(e, form))
+        e.close()
+    return ids
+
+
+def poisson_trace(nreq, rate_per_s, nworkloads, seed=0, scale_jitter=0.05):
+    """Seeded Poisson arrivals: exponential gaps of mean 1/rate, workloads
+    drawn uniformly, scale factors 1 +- scale_jitter."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_per_s, nreq))
+    t -= t[0]
+    w = rng.integers(0, nworkloads, nreq)
+    sc = 1.0 + scale_jitter * rng.uniform(-1, 1, (nreq, 3))
+    return [(int(w[i]), float(t[i]), tuple(float(x) for x in sc[i])) for i in range(nreq)]

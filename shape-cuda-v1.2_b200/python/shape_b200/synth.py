@@ -463,3 +463,70 @@ def lightcurve_dataset(npoints=200, pos_range=(129, 257), synthesize=None, param
 
 def config3_datasets(synthesize=None, params=None, npoints=200):
     return [lightcurve_dataset(npoints, (129, 257), synthesize, params, set_index=k) for k in range(4)]
+
+
+# ------------------------------------------------------------- serving mix
+
+def frame_prefix(ds, k):
+    """The first k frames of a delay-Doppler dataset (observations shared)."""
+    off = ds.offsets[:k + 1].copy()
+    return DeldopDataset(ds.set, ds.frames[:k], ds.obs[:off[-1]], ds.oneovervar[:off[-1]], off)
+
+
+def config1_frames(nframes=4, synthesize=None, params=None, pos_n=75):
+    """Config-1 geometry (ellipsoid, 151x151 POS, 100x100 delay-Doppler) at
+    nframes rotation phases 0.7 + 2*pi*j/nframes."""
+    params = params or eval_params()
+    one = config1_dataset(None, params, pos_n)
+    pole = ecl_dir(30.0, 60.0)
+    frames = []
+    for j in range(nframes):
+        fr = cd.DeldopFrame.from_buffer_copy(one.frames[0])
+        cd.fill9(fr.ae, body_matrix(pole, 0.7 + 2 * math.pi * j / nframes))
+        frames.append(fr)
+    return _finish_deldop(one.set, frames, synthesize, 20.0, 1.0, 1234, params)
+
+
+def serving_mix(synthesize_dd, synthesize_lc, params=None):
+    """Workloads of the serving mix: the config-1 model with 1-4 frames,
+    the config-2 model with 8-64 frames, the config-3 lightcurve sets (4 x
+    200 points) and the config-4 model with 1-16 frames; one workload per
+    frame count. Returns (categories, workloads) where workloads[i] =
+    (category, model, deldop datasets, lightcurve datasets) and
+    categories[c] lists the workload indices of category c (a request picks a
+    category uniformly, then a workload of it uniformly)."""
+    params = params or eval_params()
+    m1, m2, m4 = ellipsoid_model(), harmonic_model(), noisy_octa_model()
+    d1 = config1_frames(4, synthesize_dd(m1), params)
+    d2 = config2_dataset(synthesize_dd(m2), params)
+    d4 = config4_dataset(synthesize_dd(m4), params)
+    lc = config3_datasets(synthesize_lc(m2), params)
+    work, cats = [], [[], [], [], []]
+    for k in range(1, 5):
+        cats[0].append(len(work))
+        work.append(("c1", m1, [frame_prefix(d1, k)], []))
+    for k in range(8, 65):
+        cats[1].append(len(work))
+        work.append(("c2", m2, [frame_prefix(d2, k)], []))
+    cats[2].append(len(work))
+    work.append(("c3", m2, [], lc))
+    for k in range(1, 17):
+        cats[3].append(len(work))
+        work.append(("c4", m4, [frame_prefix(d4, k)], []))
+    return cats, work
+
+
+def serving_trace(cats, nreq, rate_per_s, seed=0, scale_jitter=0.02):
+    """Seeded Poisson request stream over the serving mix: exponential gaps
+    of mean 1/rate, a category uniformly, then a workload of it uniformly,
+    scale factors 1 +- scale_jitter."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_per_s, nreq))
+    t -= t[0]
+    out = []
+    for i in range(nreq):
+        c = cats[int(rng.integers(0, len(cats)))]
+        w = c[int(rng.integers(0, len(c)))]
+        sc = 1.0 + scale_jitter * rng.uniform(-1, 1, 3)
+        out.append((w, float(t[i]), tuple(float(x) for x in sc)))
+    return out

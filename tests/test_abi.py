@@ -51,3 +51,26 @@ def test_errors_without_device_are_reported():
     h = C.c_void_p()
     rc = L.shape_engine_create(0, C.byref(h))
     assert rc < 0 and len(L.shape_last_error()) > 0
+
+
+def test_dropin_compiles_against_reference_headers(tmp_path):
+    """The calc_fits drop-in compiles against the reference's struct
+    definitions and exports calc_fits (signature of src/shape/shape2.h:1451)
+    and calc_fits_chi2_b200 under their default names."""
+    import pytest
+    ref_src = os.environ.get("REF_ROOT", "/root/reference") + "/src"
+    if not os.path.isdir(os.path.join(ref_src, "shape")):
+        pytest.skip("reference headers not present")
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    inc = ["-I" + os.path.join(ref_src, d) for d in ("shape", "util", "nr", "astro", "pgm",
+                                                     "HostMultiThreading")]
+    obj = str(tmp_path / "dropin.o")
+    subprocess.run(["gcc", "-O2", "-std=gnu99", "-w", "-c", "-iquote",
+                    os.path.join(repo, "oracle", "refshim", "shape"), "-I-",
+                    "-I" + os.path.join(repo, "oracle", "refshim", "shape")] + inc +
+                   ["-I/usr/local/cuda/include", "-I" + os.path.join(repo, "include"),
+                    os.path.join(repo, "shape-cuda-v1.2_b200", "dropin", "shape_b200_dropin.c"), "-o", obj],
+                   check=True)
+    syms = subprocess.run(["nm", "-g", "--defined-only", obj], capture_output=True, text=True,
+                          check=True).stdout.split()
+    assert "calc_fits" in syms and "calc_fits_chi2_b200" in syms

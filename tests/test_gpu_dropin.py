@@ -1,0 +1,126 @@
+"""The calc_fits drop-in (shape-cuda-v1.2_b200/dropin/shape_b200_dropin.c)
+against the reference's own calc_fits, both called on the reference's structs
+in one process (oracle/_ref/libshape_dropin.so, built by
+oracle/build_dropin.sh with the drop-in's symbols renamed).
+
+Drop-in calc_fits followed by the reference's chi2 must reproduce the
+reference: chi-square to relative 1e-10, fit images to 1e-12 of their peak
+(FP64 forms), region limits and flags exactly, seen flags exactly; the
+totals-only objective path (calc_fits_chi2_b200) must give the same chi2,
+frame chi2 and calibration factors."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import golden_cases as gc
+from shape_b200 import ctypes_defs as cd
+
+pytestmark = pytest.mark.gpu
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DROPIN_SO = os.path.join(REPO, "oracle", "_ref", "libshape_dropin.so")
+
+
+@pytest.fixture(scope="module")
+def dropin():
+    from oracle.bindings import Reference
+    ref = Reference()
+    if not os.path.exists(DROPIN_SO):
+        pytest.fail("oracle/_ref/libshape_dropin.so missing: run oracle/build_dropin.sh")
+    L = C.CDLL(DROPIN_SO)
+    L.ref_dropin_evaluate.restype = C.c_double
+    L.ref_dropin_evaluate.argtypes = [C.c_void_p]
+    L.ref_dropin_objective.restype = C.c_double
+    L.ref_dropin_objective.argtypes = [C.c_void_p]
+    L.ref_get_chi2s.argtypes = [C.c_void_p, C.c_int, cd.dptr, cd.dptr, cd.dptr, cd.dptr]
+    return ref, L
+
+
+def _inputs(name):
+    if name == "mixed":
+        m = gc.octa3_model()
+        p = gc.P_DEFAULT
+        dd = gc.DELDOP_CASES["small_long_orig"][1](cases.dd_synth(m), p)
+        lc = gc.LGHTCRV_CASES["kaasalainen"][1](cases.lc_synth(m), p)
+        return m, p, [dd], [lc]
+    if name in gc.DELDOP_CASES:
+        mk, build, p = gc.DELDOP_CASES[name]
+        m = mk()
+        return m, p, [build(cases.dd_synth(m), p)], []
+    mk, build, p = gc.LGHTCRV_CASES[name]
+    m = mk()
+    return m, p, [], [build(cases.lc_synth(m), p)]
+
+
+def _chi2s(L, sess, s, nfr):
+    d, st = C.c_double(), C.c_double()
+    fc, fk = np.zeros(max(nfr, 1)), np.zeros(max(nfr, 1))
+    L.ref_get_chi2s(sess.h, s, C.byref(d), C.byref(st), cd.as_dptr(fc), cd.as_dptr(fk))
+    return d.value, st.value, fc, fk
+
+
+def _compare_outputs(a, b, dds, lcs):
+    fa, fb = a.flags(), b.flags()
+    assert fa["posbnd"] == fb["posbnd"] and fa["badradar"] == fb["badradar"]
+    for k in ("posbnd_logfactor", "badradar_logfactor"):
+        # a lightcurve-only dataset divides badradar_logfactor by zero radar
+        # dof (src/shape/calc_fits.c:409): NaN on both sides
+        if np.isnan(fa[k]):
+            assert np.isnan(fb[k]), k
+        else:
+            assert abs(fa[k] - fb[k]) <= 1e-12 * max(1.0, abs(fa[k])), k
+    assert np.array_equal(a.seen(), b.seen())
+    for s, ds in enumerate(dds):
+        for f, fr in enumerate(ds.frames):
+            ra, rb = a.deldop_frame(s, f, fr), b.deldop_frame(s, f, fr)
+            peak = max(np.abs(ra["fit"]).max(), 1e-300)
+            assert np.abs(ra["fit"] - rb["fit"]).max() <= 1e-12 * peak, (s, f)
+            for k in ("xlim", "ylim", "idellim", "idoplim"):
+                assert list(ra["res"][k]) == list(rb["res"][k]), (s, f, k)
+            for k in ("dellim", "doplim"):
+                assert np.allclose(ra["res"][k], rb["res"][k], rtol=1e-12, atol=0), (s, f, k)
+    for k, ds in enumerate(lcs):
+        s = len(dds) + k
+        ya, yb = a.lghtcrv(s, ds), b.lghtcrv(s, ds)
+        assert np.allclose(ya["y"], yb["y"], rtol=1e-12, atol=0)
+        assert np.allclose(ya["fit"], yb["fit"], rtol=1e-12, atol=0)
+
+
+CASES = ["c1", "c1_outbnd", "small_short", "small_long_mod_spb3_nsinc3", "law_hagfors_cosine",
+         "kaasalainen", "lommel", "c3_short", "mixed"]
+
+
+@pytest.mark.parametrize("form", ["plain_fp64", "batched_fp64"])
+@pytest.mark.parametrize("name", CASES)
+def test_dropin_calc_fits_matches_reference(dropin, name, form, monkeypatch, cuda_device):
+    ref, L = dropin
+    monkeypatch.setenv("SHAPE_B200_FORM", form)
+    m, p, dds, lcs = _inputs(name)
+    sa = ref.session(m, p, deldops=dds, lghtcrvs=lcs)
+    sb = ref.session(m, p, deldops=dds, lghtcrvs=lcs)
+    sc = ref.session(m, p, deldops=dds, lghtcrvs=lcs)
+    for trial, scale0 in enumerate((None, 1.03)):
+        if scale0 is not None:       # a bestfit trial: engine reused, parameters pushed
+            for s in (sa, sb, sc):
+                ref.lib.ref_set_scale(s.h, 0, scale0)
+        ca = sa.evaluate()
+        cb = L.ref_dropin_evaluate(sb.h)
+        cc = L.ref_dropin_objective(sc.h)
+        assert abs(cb - ca) <= 1e-10 * abs(ca), (trial, ca, cb)
+        assert abs(cc - ca) <= 1e-10 * abs(ca), (trial, ca, cc)
+        _compare_outputs(sa, sb, dds, lcs)
+        fa, fc = sa.flags(), sc.flags()
+        assert (fa["posbnd"], fa["badradar"]) == (fc["posbnd"], fc["badradar"])
+        for s in range(len(dds) + len(lcs)):
+            nfr = dds[s].nframes if s < len(dds) else 1
+            da, sta, fca, fka = _chi2s(L, sa, s, nfr)
+            dc, stc, fcc, fkc = _chi2s(L, sc, s, nfr)
+            assert abs(dc - da) <= 1e-10 * abs(da)
+            assert abs(stc - sta) <= 1e-10 * abs(sta)
+            assert np.allclose(fcc[:nfr], fca[:nfr], rtol=1e-10, atol=0)
+            assert np.allclose(fkc[:nfr], fka[:nfr], rtol=1e-10, atol=0)
+    for s in (sa, sb, sc):
+        s.close()
