@@ -28,30 +28,21 @@ __device__ inline int clamp_hi(double v) { return (v > (double)INT_MAX) ? INT_MA
 // ---------------------------------------------------------------- realize
 
 // x = scale * (u*r + a)  (src/shape/realize_mod.c:471-479)
-__global__ void k_realize_vertices(int nv, const double *__restrict__ a, const double *__restrict__ u,
-                                   const double *__restrict__ r, const double *__restrict__ scale,
-                                   double4 *__restrict__ vx)
+__device__ inline double4 realize_vertex(int i, const double *__restrict__ a, const double *__restrict__ u,
+                                         const double *__restrict__ r, const double *__restrict__ scale)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nv) return;
     double ri = r[i];
     double x0 = scale[0] * (u[3 * i + 0] * ri + a[3 * i + 0]);
     double x1 = scale[1] * (u[3 * i + 1] * ri + a[3 * i + 1]);
     double x2 = scale[2] * (u[3 * i + 2] * ri + a[3 * i + 2]);
-    vx[i] = make_double4(x0, x1, x2, 0.0);
+    return make_double4(x0, x1, x2, 0.0);
 }
 
 // facet normal and area: facnrm (src/shape/facnrm.c:13-25), cross
 // (src/util/cross.c), normalize (src/util/normalize.c)
-__global__ void k_realize_facets(int nf, const int *__restrict__ fv, const double4 *__restrict__ vx,
-                                 double4 *__restrict__ fn, double *__restrict__ area,
-                                 int4 *__restrict__ fvi)
+__device__ inline void realize_facet(int f, const int *__restrict__ fv, double4 p0, double4 p1, double4 p2,
+                                     double4 *__restrict__ fn, double *__restrict__ area)
 {
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= nf) return;
-    int i0 = fv[3 * f + 0], i1 = fv[3 * f + 1], i2 = fv[3 * f + 2];
-    fvi[f] = make_int4(i0, i1, i2, 0);
-    double4 p0 = vx[i0], p1 = vx[i1], p2 = vx[i2];
     double a0 = p1.x - p0.x, a1 = p1.y - p0.y, a2 = p1.z - p0.z;
     double b0 = p2.x - p1.x, b1 = p2.y - p1.y, b2 = p2.z - p1.z;
     double c0 = a1 * b2 - a2 * b1;
@@ -67,6 +58,26 @@ __global__ void k_realize_facets(int nf, const int *__restrict__ fv, const doubl
         c0 /= norm; c1 /= norm; c2 /= norm;
     }
     fn[f] = make_double4(c0, c1, c2, 0.0);
+}
+
+// Vertices and facets in one launch: threads [0, nf) realize a facet from
+// its three corners, which they compute themselves with the vertex formula
+// (same operations, so the same bits as the vertex threads), and threads
+// [nf, nf + nv) realize the vertices for the later stages.
+__global__ void k_realize_vf(int nv, int nf, const double *__restrict__ a, const double *__restrict__ u,
+                             const double *__restrict__ r, const double *__restrict__ scale,
+                             const int *__restrict__ fv, double4 *__restrict__ vx, double4 *__restrict__ fn,
+                             double *__restrict__ area, int4 *__restrict__ fvi)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nf) {
+        int i0 = fv[3 * k + 0], i1 = fv[3 * k + 1], i2 = fv[3 * k + 2];
+        fvi[k] = make_int4(i0, i1, i2, 0);
+        realize_facet(k, fv, realize_vertex(i0, a, u, r, scale), realize_vertex(i1, a, u, r, scale),
+                      realize_vertex(i2, a, u, r, scale), fn, area);
+    } else if (k < nf + nv) {
+        vx[k - nf] = realize_vertex(k - nf, a, u, r, scale);
+    }
 }
 
 // vertex normal = normalized sum of attached facet normals, in af order
@@ -258,11 +269,23 @@ __global__ void k_chi2_partials(Chi2Args a)
         const T *fit = static_cast<const T *>(a.fit) + base;
         const double *obs = a.obs + base, *oov = a.oov + base;
         KSum o2 = {0, 0}, m2 = {0, 0}, om = {0, 0};
-        for (int k = threadIdx.x; k < item.count; k += blockDim.x) {
-            double ob = obs[k], w = oov[k], ft = (double)fit[k];
-            o2.add(ob * ob * w);
-            m2.add(ft * ft * w);
-            om.add(ft * ob * w);
+        // all of a thread's loads are issued before its (serial, in-order)
+        // compensated adds, so their latencies overlap
+        double ob[CHI2_ITEMS], wv[CHI2_ITEMS], ft[CHI2_ITEMS];
+#pragma unroll
+        for (int j = 0; j < CHI2_ITEMS; j++) {
+            const int k = threadIdx.x + j * CHI2_THREADS;
+            const bool in = k < item.count;
+            ob[j] = in ? obs[k] : 0.0;
+            wv[j] = in ? oov[k] : 0.0;
+            ft[j] = in ? (double)fit[k] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < CHI2_ITEMS; j++) {
+            if (threadIdx.x + j * CHI2_THREADS >= item.count) break;
+            o2.add(ob[j] * ob[j] * wv[j]);
+            m2.add(ft[j] * ft[j] * wv[j]);
+            om.add(ft[j] * ob[j] * wv[j]);
         }
         for (int off = 16; off > 0; off >>= 1) {
             o2.merge(shfl_ksum(o2, off));
@@ -293,7 +316,7 @@ __global__ void k_chi2_partials(Chi2Args a)
 
 // Per-frame results: chi2_deldop's calibration and chi-square
 // (src/shape/chi2.c:447-460) plus the posvis / pos2deldop frame outputs.
-__device__ void finalize_frame(const FinalizeArgs &a, int fr)
+__device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr)
 {
     const FrameHost &h = a.fh[fr];
     const FrameGeom &g = a.geoms[h.view];
@@ -345,6 +368,7 @@ __device__ void finalize_frame(const FinalizeArgs &a, int fr)
     r.doplim[0] = (pl0 - g.dopshift) * fpp - a.dop_extra[fr];
     r.doplim[1] = (pl1 - g.dopshift) * fpp + a.dop_extra[fr];
     a.results[fr] = r;
+    return r;
 }
 
 __global__ void k_finalize_frames(FinalizeArgs a)
@@ -609,10 +633,27 @@ __global__ void k_lc_finalize(LcFinalizeArgs a)
 // the posbnd / badradar flags and log-factors of calc_fits
 // (src/shape/calc_fits.c:407-409, 511-550, 1947) and the objective's
 // bad-model multipliers (src/shape/bestfit.c:806-866), no penalties.
+//
+// The totals are serial sums in dataset order (the reference's order). With
+// a.smem_frames set, each frame's thread leaves its chi2 and dof-weighted
+// log-factor terms in shared memory, so the serial pass reads shared memory
+// instead of waiting on one global load per frame.
 __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
 {
+    extern __shared__ double ssm[];
+    const bool use_sm = a.smem_frames;
+    double *s_chi2 = ssm, *s_plog = ssm + fa.nframes, *s_blog = ssm + 2 * (size_t)fa.nframes;
+    unsigned char *s_flag = reinterpret_cast<unsigned char *>(ssm + 3 * (size_t)fa.nframes);
     // per-frame results first (one thread per frame), then the totals
-    for (int fr = threadIdx.x; fr < fa.nframes; fr += blockDim.x) finalize_frame(fa, fr);
+    for (int fr = threadIdx.x; fr < fa.nframes; fr += blockDim.x) {
+        const shape_deldop_result r = finalize_frame(fa, fr);
+        if (use_sm) {
+            s_chi2[fr] = r.chi2;
+            s_plog[fr] = a.fh[fr].dof * r.posbnd_logfactor;
+            s_blog[fr] = a.fh[fr].dof * r.badradar_logfactor / 1;
+            s_flag[fr] = (r.outbnd ? 1 : 0) | (r.badradar ? 2 : 0);
+        }
+    }
     __syncthreads();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double chi2 = 0.0, chi2_dd = 0.0, chi2_lc = 0.0, plog = 0.0, blog = 0.0;
@@ -622,6 +663,12 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
         double cs = 0.0;
         if (R.type == 0) {
             for (int f = R.first; f < R.first + R.count; f++) {
+                if (use_sm) {
+                    cs += s_chi2[f];
+                    if (s_flag[f] & 1) { posbnd = 1; plog += s_plog[f]; }
+                    if (s_flag[f] & 2) { badradar = 1; blog += s_blog[f]; }
+                    continue;
+                }
                 const shape_deldop_result &r = a.results[f];
                 cs += r.chi2;
                 if (r.outbnd) { posbnd = 1; plog += a.fh[f].dof * r.posbnd_logfactor; }
@@ -658,12 +705,23 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
 
 // ------------------------------------------------------------- launchers
 
-void launch_realize(const ModelDev &m, cudaStream_t s)
+void launch_realize_vf(const ModelDev &m, cudaStream_t s)
 {
     const int B = 256;
-    k_realize_vertices<<<(m.nv + B - 1) / B, B, 0, s>>>(m.nv, m.a, m.u, m.r, m.scale, m.vx);
-    k_realize_facets<<<(m.nf + B - 1) / B, B, 0, s>>>(m.nf, m.fv, m.vx, m.fn, m.area, m.fvi);
+    k_realize_vf<<<(m.nf + m.nv + B - 1) / B, B, 0, s>>>(m.nv, m.nf, m.a, m.u, m.r, m.scale, m.fv, m.vx,
+                                                          m.fn, m.area, m.fvi);
+}
+
+void launch_realize_vn(const ModelDev &m, cudaStream_t s)
+{
+    const int B = 256;
     k_realize_vnormals<<<(m.nv + B - 1) / B, B, 0, s>>>(m.nv, m.af_ptr, m.af_idx, m.fn, m.vn);
+}
+
+void launch_realize(const ModelDev &m, cudaStream_t s)
+{
+    launch_realize_vf(m, s);
+    launch_realize_vn(m, s);
 }
 
 void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, cudaStream_t s)
@@ -743,9 +801,23 @@ void launch_lc_finalize(const LcFinalizeArgs &a, cudaStream_t s)
     k_lc_finalize<<<a.nsets, 256, a.smem_per_set, s>>>(a);
 }
 
+size_t summary_smem(int nframes)
+{
+    size_t b = (3 * sizeof(double) + 1) * (size_t)nframes + 8;
+    return b <= SUMMARY_SMEM_MAX ? b : 0;
+}
+
+cudaError_t configure_summary()
+{
+    return cudaFuncSetAttribute(k_summary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SUMMARY_SMEM_MAX);
+}
+
 void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s)
 {
-    k_summary<<<1, 256, 0, s>>>(fa, a);
+    SummaryArgs b = a;
+    const size_t sm = summary_smem(fa.nframes);
+    b.smem_frames = (sm > 0 && fa.nframes > 0) ? 1 : 0;
+    k_summary<<<1, 256, b.smem_frames ? sm : 0, s>>>(fa, b);
 }
 
 

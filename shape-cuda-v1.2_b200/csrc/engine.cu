@@ -377,9 +377,14 @@ int EngineImpl::finalize()
     CK(cudaMemsetAsync(d_seen, 0, nf, s));
     CK(cudaStreamSynchronize(s));
 
+    if (!stream2) {
+        CK(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
+        for (auto &e : evf) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     CK(configure_raster_f64());
     CK(configure_raster_f32());
     CK(configure_lc_finalize());
+    CK(configure_summary());
     md.nv = nv; md.nf = nf;
     md.a = d_a; md.u = d_u; md.r = d_r; md.scale = d_scale;
     md.fv = d_fv; md.af_ptr = d_afp; md.af_idx = d_afi;
@@ -447,14 +452,34 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     cudaStream_t s = stream;
     const bool f32 = (form == SHAPE_FORM_BATCHED_FP32);
     auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], s); };
-    launch_realize(md, s);
-    mark(0);
-    launch_reset_state(d_states, nviews, d_bin_count, ntiles, s);
-    if (fit_elems) {
-        if (f32) CK(cudaMemsetAsync(d_fit32, 0, sizeof(float) * fit_elems, s));
-        else CK(cudaMemsetAsync(d_fit64, 0, sizeof(double) * fit_elems, s));
+    // The batched forms run the state reset, the image clears and the vertex
+    // normals on a side branch (stream2) that rejoins before binning and
+    // before the raster; the plain form and stage timing run them in line.
+    const bool fork = (form != SHAPE_FORM_PLAIN_FP64) && !marks;
+    cudaStream_t sr = fork ? stream2 : s;
+    if (fork) {
+        CK(cudaEventRecord(evf[0], s));
+        CK(cudaStreamWaitEvent(stream2, evf[0], 0));
     }
-    CK(cudaMemsetAsync(d_seen, 0, nf, s));
+    if (fork) {
+        launch_realize_vf(md, s);
+        CK(cudaEventRecord(evf[1], s));
+    } else {
+        launch_realize(md, s);
+    }
+    mark(0);
+    launch_reset_state(d_states, nviews, d_bin_count, ntiles, sr);
+    if (fit_elems) {
+        if (f32) CK(cudaMemsetAsync(d_fit32, 0, sizeof(float) * fit_elems, sr));
+        else CK(cudaMemsetAsync(d_fit64, 0, sizeof(double) * fit_elems, sr));
+    }
+    CK(cudaMemsetAsync(d_seen, 0, nf, sr));
+    if (fork) {
+        CK(cudaEventRecord(evf[2], stream2));        // reset and clears done
+        CK(cudaStreamWaitEvent(stream2, evf[1], 0));  // facet normals exist
+        launch_realize_vn(md, stream2);
+        CK(cudaEventRecord(evf[3], stream2));        // vertex normals done
+    }
     mark(1);
 
     RasterArgs ra;
@@ -525,8 +550,10 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         if (f32) launch_xform_f32(d_geoms, nviews, md.vx, nv, d_vt32, s);
         else launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
         mark(2);
+        if (fork) CK(cudaStreamWaitEvent(s, evf[2], 0));
         if (f32) launch_bin_f32(d_geoms, 0, nviews, md, d_vt32, d_states, d_bin_count, d_bin_ids, cap, s);
         else launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
+        if (fork) CK(cudaStreamWaitEvent(s, evf[3], 0));
         mark(3);
         // one CTA per tile, heaviest tiles first (empty tiles sort last and
         // exit at once); the block scheduler balances the rest
@@ -587,7 +614,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
 // and copies excluded).
 int EngineImpl::kernels_per_eval(int form) const
 {
-    int n = 3 + 1;                       // realize (vertices, facets, normals), state reset
+    int n = 2 + 1;                       // realize (vertices + facets, vertex normals), state reset
     if (form == SHAPE_FORM_PLAIN_FP64) {
         for (int v = 0; v < nviews; v++)
             n += 3 + (geoms[v].kind == VIEW_RADAR || geoms[v].kind == VIEW_LC_SUN ? 1 : 0);

@@ -66,6 +66,10 @@ struct EngineImpl {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // side branch of the batched graph (state reset, image clears, vertex
+    // normals) and its fork / join events
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t evf[4] = {nullptr, nullptr, nullptr, nullptr};
     float last_ms = 0.f;
 
     // model (host)
@@ -162,6 +166,9 @@ struct EngineImpl {
         if (h_summary) { cudaFreeHost(h_summary); h_summary = nullptr; }
         if (ev0) { cudaEventDestroy(ev0); ev0 = nullptr; }
         if (ev1) { cudaEventDestroy(ev1); ev1 = nullptr; }
+        for (auto &e : evf)
+            if (e) { cudaEventDestroy(e); e = nullptr; }
+        if (stream2) { cudaStreamDestroy(stream2); stream2 = nullptr; }
         if (stream) { cudaStreamDestroy(stream); stream = nullptr; }
     }
 

@@ -44,7 +44,9 @@ struct RasterArgs {
 };
 
 // core.cu (FP64, no FMA contraction)
-void launch_realize(const ModelDev &m, cudaStream_t s);
+void launch_realize(const ModelDev &m, cudaStream_t s);      // launch_realize_vf + launch_realize_vn
+void launch_realize_vf(const ModelDev &m, cudaStream_t s);   // vertices, facet normals and areas
+void launch_realize_vn(const ModelDev &m, cudaStream_t s);   // vertex normals (after _vf)
 void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, cudaStream_t s);
 void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt,
                       cudaStream_t s);
@@ -144,7 +146,11 @@ struct SummaryArgs {
     int baddiam;
     double baddiam_logfactor;
     shape_eval_summary *out;
+    int smem_frames;            // set by launch_summary: per-frame terms staged in shared memory
 };
+constexpr size_t SUMMARY_SMEM_MAX = 160 * 1024;
+size_t summary_smem(int nframes);
+cudaError_t configure_summary();
 // per-frame finalize (as launch_finalize_frames) fused with the totals
 void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s);
 

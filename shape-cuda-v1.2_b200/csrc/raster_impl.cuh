@@ -25,7 +25,7 @@
 
 // Resident CTAs per SM the register allocation must allow (FP32 / FP64).
 #ifndef RASTER_MIN_BLOCKS
-#define RASTER_MIN_BLOCKS 3
+#define RASTER_MIN_BLOCKS 4
 #endif
 #ifndef RASTER_MIN_BLOCKS_F64
 #define RASTER_MIN_BLOCKS_F64 3
@@ -786,10 +786,17 @@ inline size_t raster_smem_bytes(int cap)
     return (size_t)2 * cap * sizeof(int2) + (size_t)STAGE_FACETS * sizeof(Stage<T>);
 }
 
-// Called once per device before any launch (not inside stream capture).
+// Called once per device before any launch (not inside stream capture). The
+// FP32 kernel runs 4 CTAs per SM, which needs the largest shared-memory
+// carveout; the FP64 kernel (3 CTAs per SM) keeps the default.
 template <typename T>
 inline cudaError_t configure_raster_t()
 {
+    if (sizeof(T) == 4) {
+        cudaError_t e = cudaFuncSetAttribute(k_raster<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                             cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+    }
     return cudaFuncSetAttribute(k_raster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
