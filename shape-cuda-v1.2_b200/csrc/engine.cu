@@ -289,7 +289,10 @@ int EngineImpl::finalize()
     AL(d_vt64, (size_t)nviews * nv); AL(d_vt32, (size_t)nviews * nv);
     AL(d_bin_count, (size_t)ntiles); AL(d_bin_ids, (size_t)ntiles * cap);
     AL(d_obs, (size_t)fit_elems); AL(d_oov, (size_t)fit_elems);
-    AL(d_fit64, (size_t)fit_elems); AL(d_fit32, (size_t)fit_elems);
+    // the FP32 raster adds rows of its footprints with aligned 16-byte
+    // vector reductions that may reach up to 8 elements past a row's last
+    // bin (adding zero); the padding keeps the last frame's in the array
+    AL(d_fit64, (size_t)fit_elems); AL(d_fit32, (size_t)fit_elems + FIT32_PAD);
     {
         double *pz, *pc, *pi;
         AL(pz, (size_t)pos_elems); AL(pc, (size_t)pos_elems); AL(pi, (size_t)pos_elems);

@@ -25,6 +25,7 @@ constexpr int RASTER_THREADS = TILE_PIX;
 constexpr int STAGE_FACETS = 128;   // facets staged in shared memory per pass
 constexpr int CHI2_THREADS = 256;
 constexpr int CHI2_ITEMS = 8;       // elements per thread per chi2 block
+constexpr int FIT32_PAD = 16;       // FP32 fit arena padding (vector reductions, k_raster)
 
 // View kinds of a FrameGeom.
 constexpr int VIEW_RADAR = 0;       // delay-Doppler frame, observer view

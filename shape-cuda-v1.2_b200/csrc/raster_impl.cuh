@@ -469,6 +469,74 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
     }
 }
 
+// One footprint row of the FP32 raster straight into the frame's fit image:
+// the row's FAST_COLS-wide weights land in the 16-byte aligned groups that
+// cover them (M = misalignment of the first bin, in floats), as vector
+// reductions; group lanes outside the footprint add zero, which leaves
+// those cells unchanged.
+template <int M>
+__device__ inline void red_row_f32(float4 *base, const float (&w)[FAST_COLS], float ad, int nc)
+{
+    float v[12];
+#pragma unroll
+    for (int j = 0; j < 12; j++) {
+        const int c = j - M;
+        v[j] = (c >= 0 && c < FAST_COLS && c < nc) ? ad * w[c >= 0 && c < FAST_COLS ? c : 0] : 0.0f;
+    }
+    atomicAdd(base, make_float4(v[0], v[1], v[2], v[3]));
+    if (M + nc > 4) atomicAdd(base + 1, make_float4(v[4], v[5], v[6], v[7]));
+    if (M + nc > 8) atomicAdd(base + 2, make_float4(v[8], v[9], v[10], v[11]));
+}
+
+// FP32 delay-Doppler scatter without a shared-memory accumulator: the same
+// weights as pixel_dd_scatter's fast path, added to the fit image in HBM by
+// 16-byte vector reductions (at most 2 rows x 3 per pixel instead of 16
+// scalar atomics); footprints beyond FAST_ROWS x FAST_COLS take the generic
+// path with scalar atomics.
+__device__ inline void pixel_dd_scatter_f32_direct(const RasterArgs &a, const FrameGeom &g, const DDC<float> &k,
+                                            float cose, const PixDD<float> &d, float *fit)
+{
+    const int nr = d.idel_max - d.idel_min + 1, nc = d.idop_max - d.idop_min + 1;
+    if (nr > FAST_ROWS || nc > FAST_COLS) {
+        pixel_dd_scatter<float>(a, g, k, cose, d, fit, 1, 1, g.ndop);
+        return;
+    }
+    float s2u = 0.0f;
+    if (g.nsinc2 == 1) {
+        const float su = sinf(3.141592653589793f * (d.dopPOS - floorf(d.dopPOS)));
+        s2u = su * su;
+    }
+    const float rl = radlaw_dev<float>(a.laws[g.law], cose) * k.kmpp * k.kmpp * d.codefactor;
+    float dc[FAST_ROWS], pc[FAST_COLS];
+    float sdel = 0.0f, sdop = 0.0f;
+    const float ddel0 = d.delPOS - (float)d.idel_min, ddop0 = d.dopPOS - (float)d.idop_min;
+#pragma unroll
+    for (int r = 0; r < FAST_ROWS; r++) {
+        dc[r] = (r < nr) ? del_resp<float>(g, k, d.delPOS, ddel0 - (float)r, d.idel_min + r) : 0.0f;
+        if (r < nr) sdel += dc[r];
+    }
+#pragma unroll
+    for (int c = 0; c < FAST_COLS; c++) {
+        pc[c] = (c < nc) ? dop_resp<float>(g, k, d.dopPOS, ddop0 - (float)c, s2u, d.idop_min + c) : 0.0f;
+        if (c < nc) sdop += pc[c];
+    }
+    const float amp = rl / (sdel * sdop);
+#pragma unroll
+    for (int r = 0; r < FAST_ROWS; r++) {
+        if (r >= nr) break;
+        const float ad = amp * dc[r];
+        float *cell = fit + (long long)(d.idel_min + r - 1) * g.ndop + (d.idop_min - 1);
+        const int mis = (int)((reinterpret_cast<uintptr_t>(cell) >> 2) & 3);
+        float4 *base = reinterpret_cast<float4 *>(cell - mis);
+        switch (mis) {
+        case 0: red_row_f32<0>(base, pc, ad, nc); break;
+        case 1: red_row_f32<1>(base, pc, ad, nc); break;
+        case 2: red_row_f32<2>(base, pc, ad, nc); break;
+        default: red_row_f32<3>(base, pc, ad, nc); break;
+        }
+    }
+}
+
 __device__ inline int warp_min(int v)
 {
     for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -694,7 +762,10 @@ k_raster(RasterArgs a)
                 dd = pixel_dd_setup<T>(g, kc, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], lim);
             }
         }
-        if (g.kind == VIEW_RADAR) {
+        if constexpr (sizeof(T) == 4) {
+            if (g.kind == VIEW_RADAR && dd.ok)
+                pixel_dd_scatter_f32_direct(a, g, kc, scose, dd, static_cast<float *>(a.fit) + g.fit_base);
+        } else if (g.kind == VIEW_RADAR) {
             // The tile's delay-Doppler footprint is accumulated in shared
             // memory (reusing the bin / stage space, free after the replay)
             // and flushed with one global atomic per touched bin.
