@@ -109,10 +109,6 @@ __device__ inline void store_vt(double4 *vt, int i, double x, double y, double z
 {
     vt[i] = make_double4(x, y, z, 0.0);
 }
-__device__ inline void store_vt(float4 *vt, int i, double x, double y, double z)
-{
-    vt[i] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z), 0.0f);
-}
 
 // Vertex coordinates in each view's frame: cotrans(v, oa, x, 1) then
 // += orbit_offset (= 0.0) (src/shape/posvis.c:159-166).
@@ -396,10 +392,10 @@ __global__ void k_lc_photo(LcArgs a)
         const FrameGeom &gs = a.geoms[P.sun_view];
         const int n = go.n, side = go.side;
         const long long npix = (long long)side * side;
-        const T *Z = static_cast<const T *>(a.z) + go.pos_base;
+        const double *Z = a.z + go.pos_base;
         T *CE = static_cast<T *>(a.cose) + go.pos_base;
         const T *CI = static_cast<const T *>(a.cosi) + go.pos_base;
-        const T *ZI = static_cast<const T *>(a.zill) + gs.pos_base;
+        const double *ZI = a.zill + gs.pos_base;
         const int *F = a.f + go.pos_base;
         const int *FI = a.fill + gs.pos_base;
         const double bignum = 0.99 * HUGENUMBER;
@@ -739,11 +735,6 @@ void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv,
     k_xform<double4><<<grid, 256, 0, s>>>(g, vx, nv, vt);
 }
 
-void launch_xform_f32(const FrameGeom *g, int nviews, const double4 *vx, int nv, float4 *vt, cudaStream_t s)
-{
-    dim3 grid((nv + 255) / 256, nviews);
-    k_xform<float4><<<grid, 256, 0, s>>>(g, vx, nv, vt);
-}
 
 void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const double4 *vt,
                     FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s)
@@ -752,12 +743,6 @@ void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m
     k_bin<double4><<<grid, 256, 0, s>>>(g, view0, m.nf, m.fvi, m.fn, vt, st, bin_count, bin_ids, cap);
 }
 
-void launch_bin_f32(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const float4 *vt,
-                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s)
-{
-    dim3 grid((m.nf + 255) / 256, nviews);
-    k_bin<float4><<<grid, 256, 0, s>>>(g, view0, m.nf, m.fvi, m.fn, vt, st, bin_count, bin_ids, cap);
-}
 
 void launch_chi2_partials(const Chi2Args &a, int fp32, cudaStream_t s)
 {

@@ -286,7 +286,7 @@ int EngineImpl::finalize()
     AL(md.fvi, (size_t)nf);
     AL(d_geoms, (size_t)nviews); AL(d_states, (size_t)nviews); AL(d_laws, laws.size());
     AL(d_work, work.size());
-    AL(d_vt64, (size_t)nviews * nv); AL(d_vt32, (size_t)nviews * nv);
+    AL(d_vt64, (size_t)nviews * nv);
     AL(d_bin_count, (size_t)ntiles); AL(d_bin_ids, (size_t)ntiles * cap);
     AL(d_obs, (size_t)fit_elems); AL(d_oov, (size_t)fit_elems);
     // the FP32 raster adds rows of its footprints with aligned 16-byte
@@ -488,7 +488,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     RasterArgs ra;
     memset(&ra, 0, sizeof ra);
     ra.geoms = d_geoms;
-    ra.vt = f32 ? (const void *)d_vt32 : (const void *)d_vt64;
+    ra.vt = d_vt64;         // both forms stage from the FP64 view-frame vertices
     ra.fvi = md.fvi;
     ra.vn = md.vn;
     ra.fn = md.fn;
@@ -516,7 +516,8 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     memset(&la, 0, sizeof la);
     la.pts = d_lcpts; la.geoms = d_geoms; la.states = d_states;
     la.chunk = 4096;
-    la.z = d_pos_z; la.cose = d_pos_cose; la.cosi = d_pos_cosi; la.zill = d_pos_z;
+    la.z = static_cast<const double *>(d_pos_z); la.cose = d_pos_cose; la.cosi = d_pos_cosi;
+    la.zill = static_cast<const double *>(d_pos_z);
     la.f = d_pos_f; la.fill = d_pos_f;
     la.partials = d_lc_partials;
     la.seen = d_seen;
@@ -550,12 +551,10 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
             }
         }
     } else {
-        if (f32) launch_xform_f32(d_geoms, nviews, md.vx, nv, d_vt32, s);
-        else launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
+        launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
         mark(2);
         if (fork) CK(cudaStreamWaitEvent(s, evf[2], 0));
-        if (f32) launch_bin_f32(d_geoms, 0, nviews, md, d_vt32, d_states, d_bin_count, d_bin_ids, cap, s);
-        else launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
+        launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
         if (fork) CK(cudaStreamWaitEvent(s, evf[3], 0));
         mark(3);
         // one CTA per tile, heaviest tiles first (empty tiles sort last and
@@ -943,7 +942,7 @@ static int copy_pos(EngineImpl &E, int view, double *z, double *cose, double *co
     for (int k = 0; k < 3; k++) {
         if (!bufs[k]) continue;
         cudaError_t e;
-        if (f32) {
+        if (f32 && k > 0) {        // depth maps are FP64 in both forms
             std::vector<float> tmp(np);
             e = cudaMemcpy(tmp.data(), (float *)src[k] + g.pos_base, sizeof(float) * np, cudaMemcpyDeviceToHost);
             for (size_t i = 0; i < np; i++) bufs[k][i] = tmp[i];

@@ -118,7 +118,6 @@ struct EngineImpl {
     RadarLawDev *d_laws = nullptr;
     int2 *d_work = nullptr;
     double4 *d_vt64 = nullptr;
-    float4 *d_vt32 = nullptr;
     int *d_bin_count = nullptr;
     int2 *d_bin_ids = nullptr;
     double *d_obs = nullptr, *d_oov = nullptr;

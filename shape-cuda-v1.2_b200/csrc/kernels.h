@@ -23,7 +23,7 @@ struct RasterArgs {
     const FrameGeom *geoms;
     const int2 *work;          // (view, tile) items
     int nwork;                 // items
-    const void *vt;            // T4 transformed vertices
+    const void *vt;            // double4 view-frame vertices (both forms)
     const int4 *fvi;
     const double4 *vn;
     const double4 *fn;
@@ -34,7 +34,7 @@ struct RasterArgs {
     FrameState *states;
     const RadarLawDev *laws;
     void *fit;                 // T image arena (radar views)
-    void *pos_z, *pos_cose, *pos_cosi;  // T POS maps (keep_pos or lightcurves)
+    void *pos_z, *pos_cose, *pos_cosi;  // POS maps: z double, cos(e) / cos(i) T (keep_pos or lightcurves)
     int *pos_f;
     unsigned char *seen;
     double mincosine_seen;
@@ -50,11 +50,7 @@ void launch_realize_vn(const ModelDev &m, cudaStream_t s);   // vertex normals (
 void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, cudaStream_t s);
 void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt,
                       cudaStream_t s);
-void launch_xform_f32(const FrameGeom *g, int nviews, const double4 *vx, int nv, float4 *vt,
-                      cudaStream_t s);
 void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const double4 *vt,
-                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s);
-void launch_bin_f32(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const float4 *vt,
                     FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s);
 
 struct Chi2Item { int frame; int start; int count; };
@@ -97,7 +93,8 @@ struct LcArgs {
     const int2 *items;          // (point, pixel start) work items
     int nitems;
     int chunk;                  // pixels per item
-    const void *z, *cosi, *zill;  // T POS maps
+    const double *z, *zill;     // POS depth maps (FP64 in both forms)
+    const void *cosi;           // T POS map
     void *cose;                 // masked in place, as posmask does
     const int *f, *fill;
     double *partials;           // brightness partial per item

@@ -151,23 +151,35 @@ __device__ inline int warp_mask_of(int ri1, int ri2, int rj1, int rj2)
 
 // Facet terms of the s, t, z expressions (src/shape/posvis.c:210-228) and,
 // for views without smoothing, the facet normal in view coordinates
-// (src/shape/posvis.c:146-148).
+// (src/shape/posvis.c:146-148). Both forms stage from the FP64 view-frame
+// vertices. The FP32 form stores the corner position relative to the tile
+// origin (ox, oy), the edge differences and 1/den rounded from FP64 values,
+// so its per-pixel arithmetic works on small, accurately rounded numbers.
 template <typename T>
-__device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage<T> &s)
+__device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage<T> &s, double ox, double oy)
 {
-    using T4 = typename Vec4<T>::type;
-    const T4 *vt = static_cast<const T4 *>(a.vt) + g.vt_base;
+    const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
     int4 c = a.fvi[f];
-    T4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
-    const T A = p2.y - p1.y;
-    const T B = p2.x - p1.x;
-    const T C = p1.x - p0.x;
-    const T D = p1.y - p0.y;
-    const T E = p1.z - p0.z;
-    const T F = p2.z - p1.z;
-    const T den = (T)1 / (C * A - B * D);
-    s.p0 = vec4<T>(p0.x, p0.y, A, B);
-    s.p1 = vec4<T>(den, C, D, p0.z);
+    double4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
+    T E, F;
+    if constexpr (sizeof(T) == 8) {
+        const T A = p2.y - p1.y;
+        const T B = p2.x - p1.x;
+        const T C = p1.x - p0.x;
+        const T D = p1.y - p0.y;
+        E = p1.z - p0.z;
+        F = p2.z - p1.z;
+        const T den = (T)1 / (C * A - B * D);
+        s.p0 = vec4<T>(p0.x, p0.y, A, B);
+        s.p1 = vec4<T>(den, C, D, p0.z);
+        (void)ox; (void)oy;
+    } else {
+        const double A = p2.y - p1.y, B = p2.x - p1.x, C = p1.x - p0.x, D = p1.y - p0.y;
+        E = (T)(p1.z - p0.z);
+        F = (T)(p2.z - p1.z);
+        s.p0 = vec4<T>((T)(p0.x - ox), (T)(p0.y - oy), (T)A, (T)B);
+        s.p1 = vec4<T>((T)(1.0 / (C * A - B * D)), (T)C, (T)D, (T)p0.z);
+    }
     s.f = f;
     if (g.smooth) {
         double4 q0 = a.vn[c.x], q1 = a.vn[c.y], q2 = a.vn[c.z];
@@ -196,10 +208,9 @@ __device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage
 // Returns false when the facet faces away or misses the tile.
 template <typename T>
 __device__ bool stage_facet(const RasterArgs &a, const FrameGeom &g, int f,
-                            int ti0, int ti1, int tj0, int tj1, Stage<T> &s)
+                            int ti0, int ti1, int tj0, int tj1, Stage<T> &s, double ox, double oy)
 {
-    using T4 = typename Vec4<T>::type;
-    const T4 *vt = static_cast<const T4 *>(a.vt) + g.vt_base;
+    const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
     double4 nb = a.fn[f];
     double nz = 0.0;
     nz += g.oa[6] * nb.x;
@@ -207,7 +218,7 @@ __device__ bool stage_facet(const RasterArgs &a, const FrameGeom &g, int f,
     nz += g.oa[8] * nb.z;
     if (!(nz > 0.0)) return false;
     int4 c = a.fvi[f];
-    T4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
+    double4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
     const double kmpp = g.kmpp;
     const int n = g.n;
     double x0d = p0.x, x1d = p1.x, x2d = p2.x, y0d = p0.y, y1d = p1.y, y2d = p2.y;
@@ -230,7 +241,7 @@ __device__ bool stage_facet(const RasterArgs &a, const FrameGeom &g, int f,
     int rj1 = max(j1, tj0) - tj0, rj2 = min(j2, tj1) - tj0;
     s.bb = ri1 | (ri2 << 4) | (rj1 << 8) | (rj2 << 12);
     s.wmask = warp_mask_of(ri1, ri2, rj1, rj2);
-    stage_fill<T>(a, g, f, s);
+    stage_fill<T>(a, g, f, s, ox, oy);
     return true;
 }
 
@@ -300,6 +311,7 @@ struct PixLimits {
 template <typename T>
 struct PixDD {
     T delPOS, dopPOS, codefactor;
+    T ddel0, ddop0, dfrac;     // FP32 form: delPOS - idel_min, dopPOS - idop_min, frac(dopPOS) from FP64
     int idel_min, idel_max, idop_min, idop_max;
     bool ok;   // in_bounds: the whole footprint lies inside the frame
 };
@@ -327,6 +339,40 @@ __device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, const DDC<T> &k, int x, i
     lim.dmax = fmax(lim.dmax, (double)d.delPOS);
     lim.pmin = fmin(lim.pmin, (double)d.dopPOS);
     lim.pmax = fmax(lim.pmax, (double)d.dopPOS);
+    d.ok = (d.idel_min >= 1) && (d.idel_max <= g.ndel) && (d.idop_min >= 1) && (d.idop_max <= g.ndop) &&
+           (d.idel_max - d.idel_min + 1 <= SHAPE_MAXBINS);
+    return d;
+}
+
+// FP32 form: the pixel's delay and Doppler positions in FP64 from its FP64
+// depth (src/shape/pos2deldop.c:318-367), so the bin range and the in-frame
+// test are the FP64 form's, and the fractional offsets the FP32 response
+// weights take are rounded from FP64 values.
+__device__ inline PixDD<float> pixel_dd_setup_x(const FrameGeom &g, int x, int y, double z, PixLimits &lim)
+{
+    PixDD<float> d;
+    const double del = z * g.delfact + g.delshift;
+    d.idel_min = (int)floor(del - g.const1) + 1;
+    d.idel_max = (int)ceil(del + g.const1) - 1;
+    const double dop = g.ax * (double)x + g.ay * (double)y + g.dopshift;
+    const double half_w = g.sinc2width / 2.0;
+    d.idop_min = (int)floor(dop - g.dopdiff_max + 1 - half_w);
+    d.idop_max = (int)floor(dop + g.dopdiff_max + half_w);
+    d.delPOS = (float)del;
+    d.dopPOS = (float)dop;
+    d.ddel0 = (float)(del - (double)d.idel_min);
+    d.ddop0 = (float)(dop - (double)d.idop_min);
+    d.dfrac = (float)(dop - floor(dop));
+    d.codefactor = (g.codemethod == SHAPE_CODE_SHORT) ? sinc2<float>((float)((dop - g.dopDC_vig) / g.dopfftlen))
+                                                       : 1.0f;
+    lim.idmin = min(lim.idmin, d.idel_min);
+    lim.idmax = max(lim.idmax, d.idel_max);
+    lim.ipmin = min(lim.ipmin, d.idop_min);
+    lim.ipmax = max(lim.ipmax, d.idop_max);
+    lim.dmin = fmin(lim.dmin, del);
+    lim.dmax = fmax(lim.dmax, del);
+    lim.pmin = fmin(lim.pmin, dop);
+    lim.pmax = fmax(lim.pmax, dop);
     d.ok = (d.idel_min >= 1) && (d.idel_max <= g.ndel) && (d.idop_min >= 1) && (d.idop_max <= g.ndop) &&
            (d.idel_max - d.idel_min + 1 <= SHAPE_MAXBINS);
     return d;
@@ -405,8 +451,8 @@ constexpr int FAST_COLS = 8;
 
 // Delay and Doppler response of one pixel and its scatter into `dst`, an
 // image whose element (idel, idop) lives at dst[(idel - row0) * stride +
-// (idop - col0)] (src/shape/pos2deldop.c:371-496). dst is either the frame's
-// fit image in HBM or the tile's shared-memory accumulator. Footprints of at
+// (idop - col0)] (src/shape/pos2deldop.c:371-496); the raster passes the
+// frame's fit image in HBM (row0 = col0 = 1, stride = ndop). Footprints of at
 // most FAST_ROWS x FAST_COLS bins (the common LONG_ORIG spb=1 / nsinc2=1 /
 // sinc2width<=7 case) keep their weights in registers and scatter through
 // fully unrolled, predicated loops, so the lanes of a warp stay converged.
@@ -503,13 +549,13 @@ __device__ inline void pixel_dd_scatter_f32_direct(const RasterArgs &a, const Fr
     }
     float s2u = 0.0f;
     if (g.nsinc2 == 1) {
-        const float su = sinf(3.141592653589793f * (d.dopPOS - floorf(d.dopPOS)));
+        const float su = sinf(3.141592653589793f * d.dfrac);
         s2u = su * su;
     }
     const float rl = radlaw_dev<float>(a.laws[g.law], cose) * k.kmpp * k.kmpp * d.codefactor;
     float dc[FAST_ROWS], pc[FAST_COLS];
     float sdel = 0.0f, sdop = 0.0f;
-    const float ddel0 = d.delPOS - (float)d.idel_min, ddop0 = d.dopPOS - (float)d.idop_min;
+    const float ddel0 = d.ddel0, ddop0 = d.ddop0;
 #pragma unroll
     for (int r = 0; r < FAST_ROWS; r++) {
         dc[r] = (r < nr) ? del_resp<float>(g, k, d.delPOS, ddel0 - (float)r, d.idel_min + r) : 0.0f;
@@ -569,8 +615,8 @@ k_raster(RasterArgs a)
     __shared__ int s_red[RASTER_THREADS / 32][4];
     __shared__ double s_redd[RASTER_THREADS / 32][4];
     __shared__ int s_redl[RASTER_THREADS / 32][4];
-    __shared__ int s_box[RASTER_THREADS / 32][4];
-    __shared__ T s_pz[TILE_PIX], s_pc[TILE_PIX];
+    __shared__ double s_pz[TILE_PIX];
+    __shared__ T s_pc[TILE_PIX];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     // warp wid owns a 4x8 block of the 16x16 tile
     const int li = 4 * (wid >> 1) + (lane >> 3), lj = 8 * (wid & 1) + (lane & 7);
@@ -589,8 +635,13 @@ k_raster(RasterArgs a)
         const bool writes_pos = (g.kind != VIEW_RADAR) || a.keep_pos;
         if (count == 0 && !writes_pos) continue;
 
-        const T x0 = (T)pi * (T)g.kmpp, x1 = (T)pj * (T)g.kmpp;
+        // pixel centre: absolute (FP64 form) or relative to the tile origin
+        // (FP32 form, matching the tile-relative staged corners)
+        const double ox = (double)ti0 * g.kmpp, oy = (double)tj0 * g.kmpp;
+        const T x0 = (sizeof(T) == 8) ? (T)pi * (T)g.kmpp : (T)((double)li * g.kmpp);
+        const T x1 = (sizeof(T) == 8) ? (T)pj * (T)g.kmpp : (T)((double)lj * g.kmpp);
         T zz = (T)(-SHAPE_HUGENUMBER), cosa = 0, cosb = 0;
+        T zrel = 0;      // FP32 form: the winner's depth above its first corner
         int fac = -1;
         bool good = false;
         T gm0 = 0, gm1 = 0, gm2 = 0;
@@ -610,9 +661,16 @@ k_raster(RasterArgs a)
             const T tv = (p1.y * dy - dx * p1.z) * p1.x;
             if (!((tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL))) return;
             const auto p2 = s.p2;
-            const T z = p1.w + sv * p2.x + tv * p2.y;
+            T z, zr = 0;
+            if constexpr (sizeof(T) == 8) {
+                z = p1.w + sv * p2.x + tv * p2.y;
+            } else {
+                zr = sv * p2.x + tv * p2.y;
+                z = p1.w + zr;
+            }
             if (!((z > zz) || (fac < 0))) return;
             zz = z;
+            zrel = zr;
             fac = s.f;
             // cos(e) changes only when the smoothed normal faces the viewer
             // (posvis.c:265). Its sign is that of the view-z component before
@@ -663,7 +721,7 @@ k_raster(RasterArgs a)
                     const int bb = e.y;
                     sf.bb = bb;
                     sf.wmask = warp_mask_of(bb & 15, (bb >> 4) & 15, (bb >> 8) & 15, (bb >> 12) & 15);
-                    stage_fill<T>(a, g, e.x, sf);
+                    stage_fill<T>(a, g, e.x, sf, ox, oy);
                     st[tid] = sf;
                 }
                 __syncthreads();
@@ -677,7 +735,7 @@ k_raster(RasterArgs a)
                 Stage<T> sf;
                 bool ok = false;
                 if (tid < STAGE_FACETS && c0 + tid < a.nf)
-                    ok = stage_facet<T>(a, g, c0 + tid, ti0, ti1, tj0, tj1, sf);
+                    ok = stage_facet<T>(a, g, c0 + tid, ti0, ti1, tj0, tj1, sf, ox, oy);
                 unsigned bal = __ballot_sync(0xffffffffu, ok);
                 if (lane == 0) s_red[wid][0] = __popc(bal);
                 __syncthreads();
@@ -721,10 +779,22 @@ k_raster(RasterArgs a)
 
         // ---- outputs of this tile
         const bool covered = inframe && fac >= 0;
+        // FP64 depth: the FP32 form adds the winner's FP32 depth offset to its
+        // first corner's FP64 depth
+        double z64 = (double)zz;
+        if constexpr (sizeof(T) == 4) {
+            if (fac >= 0) {
+                const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
+                z64 = vt[a.fvi[fac].x].z + (double)zrel;
+            } else {
+                z64 = -SHAPE_HUGENUMBER;
+            }
+        }
         if (inframe && writes_pos) {
             long long p = g.pos_base + (long long)(pi + n) * g.side + (pj + n);
-            T *Z = static_cast<T *>(a.pos_z), *CE = static_cast<T *>(a.pos_cose), *CI = static_cast<T *>(a.pos_cosi);
-            Z[p] = zz;
+            double *Z = static_cast<double *>(a.pos_z);
+            T *CE = static_cast<T *>(a.pos_cose), *CI = static_cast<T *>(a.pos_cosi);
+            Z[p] = z64;
             a.pos_f[p] = fac;
             CE[p] = cosa;                        // cos(e), or cos(i) in the sun view (pos->cosill)
             if (g.kind != VIEW_LC_SUN) CI[p] = cosb;
@@ -748,58 +818,31 @@ k_raster(RasterArgs a)
         if (g.kind == VIEW_RADAR) {
             // Synthesis runs on a permuted pixel-to-thread map: the replay
             // wants each warp on a compact 4x8 block, but neighbouring pixels
-            // hit the same delay-Doppler bins, so compact warps would
-            // serialize their shared-memory atomics; a warp of scattered
-            // pixels rarely repeats an address.
+            // hit the same delay-Doppler bins, so a compact warp's atomics
+            // would repeat addresses within one instruction; a warp of
+            // scattered pixels rarely does.
             const int me = li * TILE_W + lj;
-            s_pz[me] = zz;
+            s_pz[me] = z64;
             s_pc[me] = (covered && cosa > (T)0) ? cosa : (T)0;
             __syncthreads();
             const int q = (tid * 37 + 11) & (TILE_PIX - 1);
             scose = s_pc[q];
             if (scose > (T)0) {
                 lit = true;
-                dd = pixel_dd_setup<T>(g, kc, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], lim);
+                if constexpr (sizeof(T) == 4)
+                    dd = pixel_dd_setup_x(g, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], lim);
+                else
+                    dd = pixel_dd_setup<T>(g, kc, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], lim);
             }
         }
-        if constexpr (sizeof(T) == 4) {
-            if (g.kind == VIEW_RADAR && dd.ok)
+        // The footprint goes straight to the frame's fit image in HBM: FP32 as
+        // 16-byte vector reductions, FP64 as scalar atomics (both measured
+        // faster than a shared-memory accumulator flushed per tile).
+        if (g.kind == VIEW_RADAR && dd.ok) {
+            if constexpr (sizeof(T) == 4)
                 pixel_dd_scatter_f32_direct(a, g, kc, scose, dd, static_cast<float *>(a.fit) + g.fit_base);
-        } else if (g.kind == VIEW_RADAR) {
-            // The tile's delay-Doppler footprint is accumulated in shared
-            // memory (reusing the bin / stage space, free after the replay)
-            // and flushed with one global atomic per touched bin.
-            int b0 = dd.ok ? dd.idel_min : INT_MAX, b1 = dd.ok ? dd.idel_max : INT_MIN;
-            int b2 = dd.ok ? dd.idop_min : INT_MAX, b3 = dd.ok ? dd.idop_max : INT_MIN;
-            b0 = warp_min(b0); b1 = warp_max(b1); b2 = warp_min(b2); b3 = warp_max(b3);
-            if (lane == 0) { s_box[wid][0] = b0; s_box[wid][1] = b1; s_box[wid][2] = b2; s_box[wid][3] = b3; }
-            __syncthreads();
-            int r0 = INT_MAX, r1 = INT_MIN, c0 = INT_MAX, c1 = INT_MIN;
-            for (int ww = 0; ww < RASTER_THREADS / 32; ww++) {
-                r0 = min(r0, s_box[ww][0]); r1 = max(r1, s_box[ww][1]);
-                c0 = min(c0, s_box[ww][2]); c1 = max(c1, s_box[ww][3]);
-            }
-            T *fit = static_cast<T *>(a.fit) + g.fit_base;
-            if (r0 != INT_MAX) {
-                const int nr = r1 - r0 + 1, nc = c1 - c0 + 1;
-                const long long cells = (long long)nr * nc;
-                T *box = reinterpret_cast<T *>(smem);
-                if (cells <= (long long)(a.smem_bytes / sizeof(T))) {
-                    for (long long k = tid; k < cells; k += RASTER_THREADS) box[k] = (T)0;
-                    __syncthreads();
-                    if (dd.ok) pixel_dd_scatter<T>(a, g, kc, scose, dd, box, r0, c0, nc);
-                    __syncthreads();
-                    for (long long k = tid; k < cells; k += RASTER_THREADS) {
-                        T v = box[k];
-                        if (v != (T)0) {
-                            int rr = (int)(k / nc), cc = (int)(k % nc);
-                            atomic_add_any<T>(fit + (long long)(r0 + rr - 1) * g.ndop + (c0 + cc - 1), v);
-                        }
-                    }
-                } else if (dd.ok) {
-                    pixel_dd_scatter<T>(a, g, kc, scose, dd, fit, 1, 1, g.ndop);
-                }
-            }
+            else
+                pixel_dd_scatter<T>(a, g, kc, scose, dd, static_cast<T *>(a.fit) + g.fit_base, 1, 1, g.ndop);
         }
         if (lane == 0) {
             s_red[wid][0] = cimin; s_red[wid][1] = cimax; s_red[wid][2] = cjmin; s_red[wid][3] = cjmax;
