@@ -66,7 +66,8 @@ const char *shape_last_error(void);
 const char *shape_version(void);
 /* sizeof() of every struct in shape_types.h, in the order
  * model_desc, radar_law, optical_law, eval_params, deldop_frame,
- * deldop_set, lghtcrv_point, lghtcrv_set, deldop_result, eval_summary;
+ * deldop_set, lghtcrv_point, lghtcrv_set, deldop_result, eval_summary,
+ * doppler_frame, doppler_set;
  * lets bindings verify their layouts. Returns the number written. */
 int shape_abi_sizes(size_t *out, int max);
 

@@ -126,6 +126,33 @@ typedef struct shape_deldop_set {
     shape_radar_law law;    /* photo->radar[deldop->iradlaw] */
 } shape_deldop_set;
 
+/* One Doppler frame (spectrum) with a single view (struct dopfrm_t +
+ * struct dopview_t, src/shape/shape2.h:1217-1263). */
+typedef struct shape_doppler_frame {
+    int pos_n;              /* POS half-width n: (2n+1)^2 pixels */
+    double km_per_pixel;    /* pos_t.km_per_pixel */
+    double ae[9];           /* view ecliptic -> body transform */
+    double oe[9];           /* view ecliptic -> observer transform */
+    double spin[3];         /* view total spin vector, ecliptic coords (rad/day) */
+    double dopoff;          /* view Doppler offset (bins) */
+    int ndop;               /* Doppler bins after vignetting */
+    double dopcom_vig;      /* COM Doppler bin (1-based) after vignetting */
+    double weight;          /* frame weight */
+    double dof;             /* frame degrees of freedom */
+    int cal_floating;       /* cal.state == 'f' */
+    double cal;             /* cal.val when not floating */
+    double sdev;            /* receiver noise sdev: variance of the overflow
+                               spectrum bins (src/shape/pos2doppler.c:459-476) */
+} shape_doppler_frame;
+
+/* Set-level Doppler parameters (struct doppler_t, src/shape/shape2.h:1266-1287). */
+typedef struct shape_doppler_set {
+    double dop_per_bin;     /* Hz per bin */
+    double Ftx;             /* transmitter frequency (MHz) */
+    double dopscale;        /* dopscale.val */
+    shape_radar_law law;    /* photo->radar[doppler->iradlaw] */
+} shape_doppler_set;
+
 /* One calculated lightcurve epoch (struct crvrend_t, src/shape/shape2.h:1344-1356). */
 typedef struct shape_lghtcrv_point {
     int pos_n;
@@ -148,7 +175,9 @@ typedef struct shape_lghtcrv_set {
     shape_optical_law law;  /* photo->optical[lghtcrv->ioptlaw] */
 } shape_lghtcrv_set;
 
-/* Per-frame results of one delay-Doppler evaluation. */
+/* Per-frame results of one radar frame evaluation (delay-Doppler image or
+ * Doppler spectrum; a Doppler frame leaves the delay fields at their blank
+ * values, and its o2 / m2 include the overflow spectrum's terms). */
 typedef struct shape_deldop_result {
     int outbnd;             /* posvis returned 1 (model beyond POS window) */
     double posbnd_logfactor;/* pos_t.posbnd_logfactor */

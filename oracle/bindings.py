@@ -58,6 +58,9 @@ class Oracle:
         L.orc_deldop_frame.argtypes = [P(cd.EvalParams), P(OrcReal), P(cd.DeldopSet),
                                        P(cd.DeldopFrame), cd.dptr, cd.dptr, P(OrcPos),
                                        cd.dptr, C.c_char_p, P(cd.DeldopResult)]
+        L.orc_doppler_frame.argtypes = [P(cd.EvalParams), P(OrcReal), P(cd.DopplerSet),
+                                        P(cd.DopplerFrame), cd.dptr, cd.dptr, P(OrcPos),
+                                        cd.dptr, C.c_char_p, P(cd.DeldopResult)]
         L.orc_lghtcrv_point.restype = C.c_double
         L.orc_lghtcrv_point.argtypes = [P(cd.EvalParams), P(OrcReal), P(cd.OpticalLaw),
                                         P(cd.LghtcrvPoint), P(OrcPos), C.c_char_p,
@@ -119,6 +122,30 @@ class Oracle:
         return {"fits": fits, "results": results, "pos": poss,
                 "seen": np.frombuffer(seen.raw, dtype=np.uint8).copy(), "real": real}
 
+    def eval_doppler(self, model, ds, params, real=None, keep_pos=False):
+        """calc_doppler + chi2_doppler over every frame of the Doppler set `ds`."""
+        real = real or self.realize(model)
+        R = self._real(real)
+        seen = C.create_string_buffer(model.nf)
+        fits, results, poss = [], [], []
+        for f, fr in enumerate(ds.frames):
+            pos = OrcPos()
+            self.lib.orc_pos_alloc(C.byref(pos), fr.pos_n, 0)
+            fit = np.zeros(fr.ndop)
+            res = cd.DeldopResult()
+            obs = np.ascontiguousarray(ds.frame_obs(f))
+            oov = np.ascontiguousarray(ds.oneovervar[ds.offsets[f]:ds.offsets[f + 1]])
+            self.lib.orc_doppler_frame(C.byref(params), C.byref(R), C.byref(ds.set), C.byref(fr),
+                                       cd.as_dptr(obs), cd.as_dptr(oov), C.byref(pos),
+                                       cd.as_dptr(fit), seen, C.byref(res))
+            fits.append(fit)
+            results.append(cd.result_to_dict(res))
+            if keep_pos:
+                poss.append(self.pos_arrays(pos))
+            self.lib.orc_pos_free(C.byref(pos))
+        return {"fits": fits, "results": results, "pos": poss,
+                "seen": np.frombuffer(seen.raw, dtype=np.uint8).copy(), "real": real}
+
     def eval_lghtcrv(self, model, ds, params, real=None, keep_pos=False):
         """calc_lghtcrv + chi2_lghtcrv for one lightcurve dataset."""
         real = real or self.realize(model)
@@ -171,6 +198,10 @@ class Reference:
         L.ref_add_deldop_set.argtypes = [C.c_void_p, P(cd.DeldopSet), C.c_int,
                                          P(cd.DeldopFrame), cd.dptr, cd.dptr]
         L.ref_add_lghtcrv_set.argtypes = [C.c_void_p, P(cd.LghtcrvSet), P(cd.LghtcrvPoint)]
+        L.ref_add_doppler_set.argtypes = [C.c_void_p, P(cd.DopplerSet), C.c_int,
+                                          P(cd.DopplerFrame), cd.dptr, cd.dptr]
+        L.ref_get_doppler_frame.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr, cd.dptr,
+                                            cd.dptr, cd.iptr, P(cd.DeldopResult)]
         L.ref_set_scale.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.ref_set_r.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.ref_realize.argtypes = [C.c_void_p]
@@ -194,12 +225,16 @@ class Reference:
         L.ref_brent_abs.argtypes = [C.c_double, C.c_double, C.c_double, OBJFN,
                                     C.c_double, C.c_double, cd.dptr]
 
-    def session(self, model, params, deldops=(), lghtcrvs=(), radar_law=None, optical_law=None):
+    def session(self, model, params, deldops=(), lghtcrvs=(), radar_law=None, optical_law=None,
+                dopplers=()):
+        """A reference session with the sets in the order deldops, dopplers,
+        lightcurves (all radar sets share one radar law)."""
         d = model.desc()
-        h = self.lib.ref_new(C.byref(d), C.byref(params), len(deldops) + len(lghtcrvs))
+        h = self.lib.ref_new(C.byref(d), C.byref(params), len(deldops) + len(dopplers) + len(lghtcrvs))
         keep = [d]
-        if deldops:
-            self.lib.ref_set_radar_law(h, C.byref(radar_law or deldops[0].set.law))
+        if deldops or dopplers:
+            first = deldops[0] if deldops else dopplers[0]
+            self.lib.ref_set_radar_law(h, C.byref(radar_law or first.set.law))
         if lghtcrvs:
             self.lib.ref_set_optical_law(h, C.byref(optical_law or lghtcrvs[0].set.law))
         for ds in deldops:
@@ -207,6 +242,11 @@ class Reference:
             keep.append(arr)
             self.lib.ref_add_deldop_set(h, C.byref(ds.set), ds.nframes, arr,
                                         cd.as_dptr(ds.obs), cd.as_dptr(ds.oneovervar))
+        for ds in dopplers:
+            arr = ds.frame_array()
+            keep.append(arr)
+            self.lib.ref_add_doppler_set(h, C.byref(ds.set), ds.nframes, arr,
+                                         cd.as_dptr(ds.obs), cd.as_dptr(ds.oneovervar))
         for ls in lghtcrvs:
             arr = ls.point_array()
             keep.append(arr)
@@ -262,6 +302,16 @@ class RefSession:
         res = cd.DeldopResult()
         self.L.ref_get_deldop_frame(self.h, s, f, cd.as_dptr(fit), cd.as_dptr(z), cd.as_dptr(cose),
                                     cd.as_iptr(fac), C.byref(res))
+        return {"fit": fit, "z": z, "cose": cose, "f": fac, "res": cd.result_to_dict(res)}
+
+    def doppler_frame(self, s, f, fr):
+        side = 2 * fr.pos_n + 1
+        fit = np.zeros(fr.ndop)
+        z = np.zeros(side * side); cose = np.zeros(side * side)
+        fac = np.zeros(side * side, dtype=np.int32)
+        res = cd.DeldopResult()
+        self.L.ref_get_doppler_frame(self.h, s, f, cd.as_dptr(fit), cd.as_dptr(z), cd.as_dptr(cose),
+                                     cd.as_iptr(fac), C.byref(res))
         return {"fit": fit, "z": z, "cose": cose, "f": fac, "res": cd.result_to_dict(res)}
 
     def lghtcrv(self, s, ds):

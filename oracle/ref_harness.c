@@ -213,6 +213,61 @@ int ref_add_deldop_set(void *h, const shape_deldop_set *ds, int nframes,
     return S->dat.nsets - 1;
 }
 
+/* A Doppler set (struct doppler_t, src/shape/shape2.h:1266-1287) with one
+ * view per frame; obs_all / oov_all hold every frame's ndop bins back to back. */
+int ref_add_doppler_set(void *h, const shape_doppler_set *ds, int nframes,
+                        const shape_doppler_frame *frames, const double *obs_all,
+                        const double *oov_all)
+{
+    ref_session *S = h;
+    if (S->dat.nsets >= S->nsets_cap) return -1;
+    struct set_t *set = &S->dat.set[S->dat.nsets++];
+    set->type = DOPPLER;
+    struct doppler_t *dp = &set->desc.doppler;
+    dp->iradlaw = 0;
+    dp->dop_per_bin = ds->dop_per_bin;
+    dp->Ftx = ds->Ftx;
+    dp->dopscale.val = ds->dopscale;
+    dp->nviews = 1;
+    dp->v0 = 0;
+    dp->nframes = nframes;
+    dp->frame = calloc((size_t)nframes, sizeof(struct dopfrm_t));
+    size_t off = 0;
+    double dof = 0.0;
+    for (int f = 0; f < nframes; f++) {
+        const shape_doppler_frame *F = &frames[f];
+        struct dopfrm_t *fr = &dp->frame[f];
+        fr->ndop = F->ndop;
+        fr->dopcom_vig = F->dopcom_vig;
+        fr->weight = F->weight;
+        fr->dof = F->dof;
+        fr->sdev = F->sdev;
+        fr->cal.state = F->cal_floating ? 'f' : 'c';
+        fr->cal.val = F->cal;
+        fr->obs = vector(1, F->ndop);
+        fr->fit = vector(1, F->ndop);
+        fr->oneovervar = vector(1, F->ndop);
+        for (int j = 1; j <= F->ndop; j++) {
+            fr->obs[j] = obs_all[off + (size_t)(j - 1)];
+            fr->oneovervar[j] = oov_all[off + (size_t)(j - 1)];
+            fr->fit[j] = 0.0;
+        }
+        off += (size_t)F->ndop;
+        fr->view = calloc(1, sizeof(struct dopview_t));
+        ref_copy_rm(fr->view[0].ae, F->ae);
+        ref_copy_rm(fr->view[0].oe, F->oe);
+        for (int j = 0; j < 3; j++) fr->view[0].spin[j] = F->spin[j];
+        fr->view[0].dopoff = F->dopoff;
+        ref_alloc_pos(&fr->pos, F->pos_n, F->km_per_pixel, 0);
+        dof += F->dof;
+    }
+    dp->dof = dof;
+    set->dof = dof;
+    S->dat.dof_doppler += dof;
+    S->dat.dof += dof;
+    return S->dat.nsets - 1;
+}
+
 int ref_add_lghtcrv_set(void *h, const shape_lghtcrv_set *ls, const shape_lghtcrv_point *pts)
 {
     ref_session *S = h;
@@ -383,6 +438,31 @@ void ref_get_deldop_frame(void *h, int s, int f, double *fit, double *z, double 
     }
 }
 
+/* Outputs of one Doppler frame after ref_evaluate (delay fields blank). */
+void ref_get_doppler_frame(void *h, int s, int f, double *fit, double *z, double *cose,
+                           int *fac, shape_deldop_result *res)
+{
+    ref_session *S = h;
+    struct dopfrm_t *fr = &S->dat.set[s].desc.doppler.frame[f];
+    if (fit)
+        for (int j = 1; j <= fr->ndop; j++) fit[j - 1] = fr->fit[j];
+    int lims[8];
+    ref_copy_pos_out(&fr->pos, z, cose, NULL, fac, NULL, NULL, lims);
+    if (res) {
+        memset(res, 0, sizeof *res);
+        res->xlim[0] = lims[0]; res->xlim[1] = lims[1];
+        res->ylim[0] = lims[2]; res->ylim[1] = lims[3];
+        res->idoplim[0] = fr->idoplim[0]; res->idoplim[1] = fr->idoplim[1];
+        res->doplim[0] = fr->doplim[0]; res->doplim[1] = fr->doplim[1];
+        res->badradar_logfactor = fr->badradar_logfactor;
+        res->posbnd_logfactor = fr->pos.posbnd_logfactor;
+        res->o2 = fr->overflow_o2;     /* the overflow terms (chi2 sums are local to chi2_doppler) */
+        res->m2 = fr->overflow_m2;
+        res->cal = fr->cal.val;
+        res->chi2 = fr->chi2;
+    }
+}
+
 /* Outputs of a lightcurve set after ref_evaluate: y[ncalc], fit[n], [cal, chi2]. */
 void ref_get_lghtcrv(void *h, int s, double *y, double *fit, double out[2])
 {
@@ -425,6 +505,17 @@ void ref_free(void *h)
                 free(fr->view);
             }
             free(dd->frame);
+        } else if (set->type == DOPPLER) {
+            struct doppler_t *dp = &set->desc.doppler;
+            for (int f = 0; f < dp->nframes; f++) {
+                struct dopfrm_t *fr = &dp->frame[f];
+                free_vector(fr->obs, 1, fr->ndop);
+                free_vector(fr->fit, 1, fr->ndop);
+                free_vector(fr->oneovervar, 1, fr->ndop);
+                ref_free_pos(&fr->pos);
+                free(fr->view);
+            }
+            free(dp->frame);
         } else if (set->type == LGHTCRV) {
             struct lghtcrv_t *lc = &set->desc.lghtcrv;
             for (int i = 1; i <= lc->ncalc; i++) ref_free_pos(&lc->rend[i].pos);

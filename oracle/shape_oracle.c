@@ -565,6 +565,136 @@ int orc_pos2deldop(const shape_eval_params *par, const shape_deldop_set *set,
     return badradar;
 }
 
+/* --------------------------------------------------------------- pos2doppler */
+
+/* pos2doppler (src/shape/pos2doppler.c:149-501) for body 0, one view, no
+ * orbital offsets, speckle off. fit (ndop) must be cleared by the caller
+ * (src/shape/calc_fits.c:914). Pixels whose sinc^2 footprint leaves the
+ * spectrum go to an overflow spectrum of ORC_MAXOVERFLOW bins centred on the
+ * COM; ovf receives its chi-square terms {o2, m2, xsec, dopmean}
+ * (pos2doppler.c:451-499). Returns badradar. */
+#define ORC_MAXOVERFLOW 2000
+int orc_pos2doppler(const shape_eval_params *par, const shape_doppler_set *set,
+                    const shape_doppler_frame *frm, const orc_pos *pos, double *fit,
+                    shape_deldop_result *res, double ovf[4])
+{
+    const int n = pos->n, side = 2 * n + 1, ndop = frm->ndop;
+    double w[3], dop_c[SHAPE_MAXBINS + 1];
+    int badradar = 0, any_overflow = 0, idop0 = 0;
+    double *overflow = calloc(ORC_MAXOVERFLOW, sizeof(double));
+
+    res->idellim[0] = res->idellim[1] = 0;
+    res->dellim[0] = res->dellim[1] = 0.0;
+    res->idoplim[0] = ndop + 999999; res->idoplim[1] = -999999;
+    res->doplim[0] = SHAPE_HUGENUMBER; res->doplim[1] = -SHAPE_HUGENUMBER;
+    res->badradar_logfactor = 0.0;
+
+    orc_mv(w, frm->oe, frm->spin);
+    const double dopfact = set->dopscale * SHAPE_KM2HZFACT * pos->kmpp * set->Ftx / set->dop_per_bin;
+    const double ax = -w[1] * dopfact;
+    const double ay = w[0] * dopfact;
+    const double km2Hz = sqrt(ax * ax + ay * ay) * set->dop_per_bin / pos->kmpp;
+    double dop_extra;
+    if (w[0] != 0.0 || w[1] != 0.0)
+        dop_extra = km2Hz * 0.5 * pos->kmpp * sqrt(w[0] * w[0] + w[1] * w[1]) / ORC_MAX(fabs(w[0]), fabs(w[1]));
+    else
+        dop_extra = 0.0;
+    const int nsinc2 = par->nsinc2;
+    const int nsinc2_sq = nsinc2 * nsinc2;
+    const double xincr = ax / nsinc2, yincr = ay / nsinc2;
+    const double dopdiff_bl = -(nsinc2 - 1) * (xincr + yincr) / 2;
+    const double dopdiff_max = (nsinc2 - 1) * (fabs(xincr) + fabs(yincr)) / 2;
+    if (2 * dopdiff_max + par->sinc2width + 1 > SHAPE_MAXBINS) {
+        badradar = 1;
+        res->badradar_logfactor += log((2 * dopdiff_max + par->sinc2width + 1) / SHAPE_MAXBINS);
+    }
+    const double dopshift = frm->dopcom_vig + frm->dopoff + 0.0;
+
+    for (int x = pos->xlim[0]; x <= pos->xlim[1]; x++)
+        for (int y = pos->ylim[0]; y <= pos->ylim[1]; y++) {
+            size_t p = (size_t)(x + n) * side + (size_t)(y + n);
+            if (!(pos->cose[p] > 0.0 && pos->f[p] >= 0))
+                continue;
+            double dopPOS = ax * (x - 0.0) + ay * (y - 0.0) + dopshift;
+            int idop_min = (int)floor(dopPOS - dopdiff_max + 1 - par->sinc2width / 2.0);
+            int idop_max = (int)floor(dopPOS + dopdiff_max + par->sinc2width / 2.0);
+            if (idop_min < res->idoplim[0]) res->idoplim[0] = idop_min;
+            if (idop_max > res->idoplim[1]) res->idoplim[1] = idop_max;
+            res->doplim[0] = ORC_MIN(res->doplim[0], dopPOS);
+            res->doplim[1] = ORC_MAX(res->doplim[1], dopPOS);
+            int in_bounds = (idop_min >= 1) && (idop_max <= ndop);
+            if (!in_bounds && !any_overflow) {
+                any_overflow = 1;
+                memset(overflow, 0, sizeof(double) * ORC_MAXOVERFLOW);
+                idop0 = ORC_MAXOVERFLOW / 2 - (int)floor(dopshift + 0.5);
+            }
+            for (int idop = idop_min; idop <= idop_max; idop++) {
+                double sm;
+                if (nsinc2 == 1) {
+                    sm = orc_sinc2(dopPOS - idop);
+                } else if (nsinc2 == 2) {
+                    double bl = dopPOS + dopdiff_bl - idop;
+                    sm = (orc_sinc2(bl) + orc_sinc2(bl + xincr) + orc_sinc2(bl + yincr) +
+                          orc_sinc2(bl + xincr + yincr)) / 4;
+                } else {
+                    double left = dopPOS + dopdiff_bl - idop;
+                    sm = 0.0;
+                    for (int i = 0; i < nsinc2; i++) {
+                        double arg = left;
+                        for (int j = 0; j < nsinc2; j++) {
+                            sm += orc_sinc2(arg);
+                            arg += xincr;
+                        }
+                        left += yincr;
+                    }
+                    sm /= nsinc2_sq;
+                }
+                dop_c[ORC_MIN(idop - idop_min, SHAPE_MAXBINS)] = sm;
+            }
+            double sumweights = 0.0;
+            for (int idop = idop_min; idop <= idop_max; idop++)
+                sumweights += dop_c[ORC_MIN(idop - idop_min, SHAPE_MAXBINS)];
+            double amp = orc_radlaw(&set->law, pos->cose[p]) * pos->kmpp * pos->kmpp / sumweights;
+            if (in_bounds) {
+                for (int idop = idop_min; idop <= idop_max; idop++)
+                    fit[idop - 1] += amp * dop_c[ORC_MIN(idop - idop_min, SHAPE_MAXBINS)];
+            } else {
+                int idop1 = ORC_MAX(idop_min, -idop0);
+                int idop2 = ORC_MIN(idop_max, -idop0 + ORC_MAXOVERFLOW - 1);
+                for (int idop = idop1; idop <= idop2; idop++)
+                    overflow[idop + idop0] += amp * dop_c[ORC_MIN(idop - idop_min, SHAPE_MAXBINS)];
+            }
+        }
+
+    res->doplim[0] = (res->doplim[0] - dopshift) * set->dop_per_bin - dop_extra;
+    res->doplim[1] = (res->doplim[1] - dopshift) * set->dop_per_bin + dop_extra;
+
+    const double variance = frm->sdev * frm->sdev;
+    ovf[0] = ovf[1] = ovf[2] = ovf[3] = 0.0;
+    if (any_overflow) {
+        int j1 = ORC_MAX(res->idoplim[0] + idop0, 0);
+        int j2 = ORC_MIN(res->idoplim[1] + idop0, ORC_MAXOVERFLOW - 1);
+        for (int j = j1; j <= j2; j++)
+            if (overflow[j] != 0.0) {
+                ovf[0] += 1.0;
+                ovf[1] += overflow[j] * overflow[j] / variance;
+                ovf[2] += overflow[j];
+                ovf[3] += (j - idop0) * overflow[j];
+            }
+        if (ovf[2] != 0.0)
+            ovf[3] /= ovf[2];
+        if ((res->idoplim[0] + idop0) < 0 || (res->idoplim[1] + idop0) >= ORC_MAXOVERFLOW) {
+            badradar = 1;
+            double dopfactor = (ORC_MAX(res->idoplim[1] + idop0, ORC_MAXOVERFLOW) -
+                                ORC_MIN(res->idoplim[0] + idop0, 0)) / (1.0 * ORC_MAXOVERFLOW);
+            res->badradar_logfactor += log(dopfactor);
+        }
+    }
+    free(overflow);
+    res->badradar = badradar;
+    return badradar;
+}
+
 /* -------------------------------------------------------------- apply_photo */
 
 /* apply_photo (src/shape/apply_photo.c:78-309) for the Lambert, Lommel and
@@ -624,6 +754,26 @@ void orc_chi2_frame(const double *obs, const double *oneovervar, const double *f
     *chi2 = weight * (so2 - 2 * c * som + c * c * sm2);
 }
 
+/* One frame of chi2_doppler (src/shape/chi2.c:722-780): the sums start from
+ * the overflow spectrum's o2 and m2 (pos2doppler.c:451-499). */
+void orc_chi2_doppler_frame(const double *obs, const double *oneovervar, const double *fit,
+                            int ndop, double ovf_o2, double ovf_m2, double weight,
+                            int cal_floating, double cal_in, double *o2, double *m2,
+                            double *om, double *cal, double *chi2)
+{
+    double so2 = ovf_o2, sm2 = ovf_m2, som = 0.0;
+    for (int j = 0; j < ndop; j++) {
+        so2 += obs[j] * obs[j] * oneovervar[j];
+        sm2 += fit[j] * fit[j] * oneovervar[j];
+        som += fit[j] * obs[j] * oneovervar[j];
+    }
+    double c = cal_in;
+    if (cal_floating)
+        c = (som > 0.0) ? som / sm2 : SHAPE_TINYCALFACT;
+    *o2 = so2; *m2 = sm2; *om = som; *cal = c;
+    *chi2 = weight * (so2 - 2 * c * som + c * c * sm2);
+}
+
 /* --------------------------------------------------------------- composites */
 
 void orc_deldop_frame(const shape_eval_params *par, const orc_real *real,
@@ -655,6 +805,39 @@ void orc_deldop_frame(const shape_eval_params *par, const orc_real *real,
     orc_chi2_frame(obs, oneovervar, fit, frm->ndel * frm->ndop, frm->weight,
                    frm->cal_floating, frm->cal, &res->o2, &res->m2, &res->om,
                    &res->cal, &res->chi2);
+}
+
+/* calc_doppler for one frame (src/shape/calc_fits.c:860-935) then its chi2. */
+void orc_doppler_frame(const shape_eval_params *par, const orc_real *real,
+                       const shape_doppler_set *set, const shape_doppler_frame *frm,
+                       const double *obs, const double *oneovervar,
+                       orc_pos *pos, double *fit, unsigned char *seen,
+                       shape_deldop_result *res)
+{
+    const double zero3[3] = {0.0, 0.0, 0.0};
+    memcpy(pos->ae, frm->ae, sizeof pos->ae);
+    memcpy(pos->oe, frm->oe, sizeof pos->oe);
+    pos->kmpp = frm->km_per_pixel;
+    pos->bistatic = 0;
+    orc_posclr(pos);
+    res->outbnd = orc_posvis(real, zero3, pos, par->pos_smooth, 0);
+    res->posbnd_logfactor = pos->posbnd_logfactor;
+    const int n = pos->n, side = 2 * n + 1;
+    if (seen && par->mark_seen)
+        for (int k = pos->xlim[0]; k <= pos->xlim[1]; k++)
+            for (int l = pos->ylim[0]; l <= pos->ylim[1]; l++) {
+                size_t p = (size_t)(k + n) * side + (size_t)(l + n);
+                if (pos->cose[p] > par->mincosine_seen && pos->f[p] >= 0)
+                    seen[pos->f[p]] = 1;
+            }
+    memset(fit, 0, sizeof(double) * (size_t)frm->ndop);
+    double ovf[4];
+    orc_pos2doppler(par, set, frm, pos, fit, res, ovf);
+    res->xlim[0] = pos->xlim[0]; res->xlim[1] = pos->xlim[1];
+    res->ylim[0] = pos->ylim[0]; res->ylim[1] = pos->ylim[1];
+    orc_chi2_doppler_frame(obs, oneovervar, fit, frm->ndop, ovf[0], ovf[1], frm->weight,
+                           frm->cal_floating, frm->cal, &res->o2, &res->m2, &res->om,
+                           &res->cal, &res->chi2);
 }
 
 double orc_lghtcrv_point(const shape_eval_params *par, const orc_real *real,

@@ -57,6 +57,18 @@ double orc_radlaw(const shape_radar_law *law, double cosinc);
 int orc_pos2deldop(const shape_eval_params *par, const shape_deldop_set *set,
                    const shape_deldop_frame *frm, const orc_pos *pos,
                    double *fit, shape_deldop_result *res);
+int orc_pos2doppler(const shape_eval_params *par, const shape_doppler_set *set,
+                    const shape_doppler_frame *frm, const orc_pos *pos, double *fit,
+                    shape_deldop_result *res, double ovf[4]);
+void orc_chi2_doppler_frame(const double *obs, const double *oneovervar, const double *fit,
+                            int ndop, double ovf_o2, double ovf_m2, double weight,
+                            int cal_floating, double cal_in, double *o2, double *m2,
+                            double *om, double *cal, double *chi2);
+void orc_doppler_frame(const shape_eval_params *par, const orc_real *real,
+                       const shape_doppler_set *set, const shape_doppler_frame *frm,
+                       const double *obs, const double *oneovervar,
+                       orc_pos *pos, double *fit, unsigned char *seen,
+                       shape_deldop_result *res);
 double orc_apply_photo(const shape_optical_law *law, double phase,
                        double intensityfactor, orc_pos *pos);
 void orc_chi2_frame(const double *obs, const double *oneovervar, const double *fit,

@@ -64,6 +64,23 @@ class DeldopSet(C.Structure):
     ]
 
 
+class DopplerFrame(C.Structure):
+    _fields_ = [
+        ("pos_n", C.c_int), ("km_per_pixel", C.c_double),
+        ("ae", C.c_double * 9), ("oe", C.c_double * 9), ("spin", C.c_double * 3),
+        ("dopoff", C.c_double), ("ndop", C.c_int), ("dopcom_vig", C.c_double),
+        ("weight", C.c_double), ("dof", C.c_double),
+        ("cal_floating", C.c_int), ("cal", C.c_double), ("sdev", C.c_double),
+    ]
+
+
+class DopplerSet(C.Structure):
+    _fields_ = [
+        ("dop_per_bin", C.c_double), ("Ftx", C.c_double), ("dopscale", C.c_double),
+        ("law", RadarLaw),
+    ]
+
+
 class LghtcrvPoint(C.Structure):
     _fields_ = [
         ("pos_n", C.c_int), ("km_per_pixel", C.c_double),
@@ -100,6 +117,7 @@ STRUCTS = {
     "shape_deldop_frame": DeldopFrame, "shape_deldop_set": DeldopSet,
     "shape_lghtcrv_point": LghtcrvPoint, "shape_lghtcrv_set": LghtcrvSet,
     "shape_deldop_result": DeldopResult,
+    "shape_doppler_frame": DopplerFrame, "shape_doppler_set": DopplerSet,
 }
 
 

@@ -283,6 +283,25 @@ class DeldopDataset:
 
 
 @dataclass
+class DopplerDataset:
+    set: "cd.DopplerSet"
+    frames: list             # list of cd.DopplerFrame
+    obs: np.ndarray          # concatenated [sum ndop]
+    oneovervar: np.ndarray
+    offsets: np.ndarray      # [nframes+1] element offsets into obs
+
+    @property
+    def nframes(self):
+        return len(self.frames)
+
+    def frame_array(self):
+        return (cd.DopplerFrame * len(self.frames))(*self.frames)
+
+    def frame_obs(self, f):
+        return self.obs[self.offsets[f]:self.offsets[f + 1]]
+
+
+@dataclass
 class LightcurveDataset:
     set: "cd.LghtcrvSet"
     points: list             # list of cd.LghtcrvPoint
@@ -412,6 +431,62 @@ def config4_dataset(synthesize=None, params=None):
     """Config 4: 16 frames, POS pos_pixels=512 (effective 511x511, n=255),
     256x256 delay-Doppler."""
     return batched_dataset(16, (511, 511), (256, 256), (256, 256), synthesize, params, seed=7)
+
+
+def doppler_dataset(nframes=8, pos_range=(101, 301), ndop_range=(64, 256), synthesize=None,
+                    params=None, seed=13, radius=1.05, law=None, span=0.7, sdev=1.0):
+    """Doppler-only frames (spectra) at rotation phases uniform in [0, 2pi):
+    odd POS sides and spectrum lengths uniform in the given ranges, one
+    set-level resolution chosen so the limb-to-limb bandwidth spans `span` of
+    the shortest spectrum (span > 1 pushes the model past the spectrum edges
+    and into the overflow spectrum)."""
+    params = params or eval_params()
+    rng = np.random.default_rng(seed)
+    pole = ecl_dir(30.0, 60.0)
+    omega = 2 * math.pi / 0.25
+    to_earth = ecl_dir(0.0, 10.0)
+    oe = observer_matrix(to_earth)
+    w_obs = oe @ (omega * pole)
+    w_proj = math.hypot(w_obs[0], w_obs[1])
+    Ftx = 2380.0
+    dset = cd.DopplerSet()
+    dset.Ftx, dset.dopscale = Ftx, 1.0
+    dset.law = law if law is not None else radar_cosine()
+    ndops = rng.integers(ndop_range[0], ndop_range[1] + 1, nframes)
+    sides = rng.integers(pos_range[0], pos_range[1] + 1, nframes) | 1
+    phases = rng.uniform(0.0, 2 * math.pi, nframes)
+    dset.dop_per_bin = 2 * KM2HZFACT * Ftx * w_proj * radius / (span * float(ndop_range[0]))
+    frames = []
+    for f in range(nframes):
+        fr = cd.DopplerFrame()
+        fr.pos_n = int(sides[f]) // 2
+        fr.km_per_pixel = 2 * radius / (0.8 * sides[f])
+        cd.fill9(fr.ae, body_matrix(pole, float(phases[f])))
+        cd.fill9(fr.oe, oe)
+        for j in range(3):
+            fr.spin[j] = float(omega * pole[j])
+        fr.dopoff = 0.0
+        fr.ndop = int(ndops[f])
+        fr.dopcom_vig = 0.5 * fr.ndop + 0.5
+        fr.weight = 1.0
+        fr.dof = float(fr.ndop)
+        fr.cal_floating, fr.cal = 1, 1.0
+        fr.sdev = sdev
+        frames.append(fr)
+    sizes = [fr.ndop for fr in frames]
+    offsets = np.zeros(nframes + 1, dtype=np.int64)
+    np.cumsum(sizes, out=offsets[1:])
+    obs = np.zeros(int(offsets[-1]))
+    oov = np.full(int(offsets[-1]), 1.0 / (sdev * sdev))
+    ds = DopplerDataset(dset, frames, obs, oov, offsets)
+    if synthesize is not None:
+        fits = synthesize(ds, params)
+        nrng = np.random.default_rng(seed + 1000)
+        for f in range(nframes):
+            ft = np.asarray(fits[f], dtype=np.float64)
+            peak = ft.max() if ft.size and ft.max() > 0 else 1.0
+            ds.obs[offsets[f]:offsets[f + 1]] = 20.0 * ft / peak + sdev * nrng.standard_normal(ft.size)
+    return ds
 
 
 def lightcurve_dataset(npoints=200, pos_range=(129, 257), synthesize=None, params=None,

@@ -58,6 +58,16 @@ def ref_deldop_synth(ref, model):
     return f
 
 
+def ref_doppler_synth(ref, model):
+    def f(ds, p):
+        S = ref.session(model, p, dopplers=[ds])
+        S.evaluate()
+        out = [S.doppler_frame(0, k, fr)["fit"] for k, fr in enumerate(ds.frames)]
+        S.close()
+        return out
+    return f
+
+
 def ref_lc_synth(ref, model):
     def f(ds, p):
         S = ref.session(model, p, lghtcrvs=[ds])
@@ -83,9 +93,24 @@ def deldop_record(S, s, ds):
     return frames
 
 
+def doppler_record(S, s, ds):
+    frames = []
+    for k, fr in enumerate(ds.frames):
+        r = S.doppler_frame(s, k, fr)
+        frames.append({
+            "f": digest(r["f"].astype(np.int32)), "fit": digest(r["fit"]), "fit_sum": float(r["fit"].sum()),
+            "covered": int((r["f"] >= 0).sum()),
+            "overflow_o2": r["res"]["o2"], "overflow_m2": r["res"]["m2"],
+            "res": {k2: (list(v) if isinstance(v, tuple) else v) for k2, v in r["res"].items()
+                    if k2 in ("xlim", "ylim", "idoplim", "doplim", "posbnd_logfactor",
+                              "badradar_logfactor", "cal", "chi2")},
+        })
+    return frames
+
+
 def main():
     ref = Reference()
-    out = {"deldop": {}, "lghtcrv": {}, "realize": {}}
+    out = {"deldop": {}, "lghtcrv": {}, "realize": {}, "doppler": {}}
     arrays = {}
 
     # realization digests (bit-exact targets)
@@ -113,6 +138,16 @@ def main():
             arrays["c1_z"] = r["z"][cov]
             arrays["c1_cose"] = r["cose"][cov]
             arrays["c1_fit"] = r["fit"]
+        S.close()
+
+    # Doppler cases
+    for name, (model_fn, ds_fn, params) in gc.DOPPLER_CASES.items():
+        m = model_fn()
+        ds = ds_fn(ref_doppler_synth(ref, m), params)
+        S = ref.session(m, params, dopplers=[ds])
+        chi2 = S.evaluate()
+        out["doppler"][name] = {"chi2": chi2, "frames": doppler_record(S, 0, ds), "flags": S.flags(),
+                                "seen": digest(S.seen()), "obs": digest(ds.obs)}
         S.close()
 
     # lightcurve cases

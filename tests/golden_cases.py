@@ -46,6 +46,21 @@ DELDOP_CASES = {
     "law_cosine_cosine": (octa3_model, _small(law_=law(7)), P_DEFAULT),
 }
 
+def _dop(span=0.7, law_=None, seed=21, pos=(41, 61), ndop=(32, 64), nframes=3):
+    return lambda s, p: synth.doppler_dataset(nframes, pos, ndop, s, p, seed=seed, span=span, law=law_)
+
+
+# Doppler-only sets: in-frame spectra, spectra whose model spills into the
+# overflow spectrum, a model wider than the overflow spectrum (badradar),
+# nsinc2 = 2 and a hybrid radar law.
+DOPPLER_CASES = {
+    "dop_small": (octa3_model, _dop(), P_DEFAULT),
+    "dop_overflow": (octa3_model, _dop(span=1.6), P_DEFAULT),
+    "dop_overflow_far": (octa3_model, _dop(span=130.0, ndop=(24, 32), nframes=2), P_DEFAULT),
+    "dop_nsinc2": (octa3_model, _dop(seed=23), synth.eval_params(nsinc2=2)),
+    "dop_law_hagfors_cosine": (octa3_model, _dop(law_=law(6), seed=25), P_DEFAULT),
+}
+
 LGHTCRV_CASES = {
     "kaasalainen": (octa3_model, lambda s, p: synth.lightcurve_dataset(6, (41, 61), s, p, seed=5),
                     synth.eval_params(mask_tol=0.0)),

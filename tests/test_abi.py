@@ -39,6 +39,8 @@ def test_struct_layouts_match_compiler():
     for name, size in zip(eng.ABI_ORDER, sizes):
         assert C.sizeof(cd.STRUCTS[name]) == size, name
     assert C.sizeof(eng.EvalSummary) == sizes[len(eng.ABI_ORDER)]
+    for k, name in enumerate(("shape_doppler_frame", "shape_doppler_set")):
+        assert C.sizeof(cd.STRUCTS[name]) == sizes[len(eng.ABI_ORDER) + 1 + k], name
 
 
 def test_errors_without_device_are_reported():

@@ -81,6 +81,35 @@ def test_deldop_bit_exact(orc, name):
     assert blog == g["flags"]["badradar_logfactor"]
 
 
+@pytest.mark.parametrize("name", sorted(gc.DOPPLER_CASES))
+def test_doppler_bit_exact(orc, name):
+    """pos2doppler + chi2_doppler, including the overflow spectrum's chi-square
+    terms and the badradar factor of a model wider than it."""
+    model_fn, ds_fn, params = gc.DOPPLER_CASES[name]
+    g = GOLD["doppler"][name]
+    m = model_fn()
+    ds = ds_fn(lambda d, p: orc.eval_doppler(m, d, p)["fits"], params)
+    assert digest(ds.obs) == g["obs"], "synthesized observations differ"
+    o = orc.eval_doppler(m, ds, params, keep_pos=True)
+    for f, gf in enumerate(g["frames"]):
+        po, r = o["pos"][f], o["results"][f]
+        assert digest(po["f"].astype(np.int32)) == gf["f"], (f, "facet map")
+        assert digest(o["fits"][f]) == gf["fit"], (f, "fit spectrum")
+        for k, v in gf["res"].items():
+            got = r[k]
+            if isinstance(v, list):
+                assert list(got) == v, (f, k, got, v)
+            else:
+                assert got == v, (f, k, got, v)
+    assert sum(r["chi2"] for r in o["results"]) == g["chi2"]
+    assert digest(o["seen"]) == g["seen"]
+    dof = sum(fr.dof for fr in ds.frames)
+    posbnd, plog, badradar, blog = _calc_fits_flags(o["results"], ds.frames, dof)
+    assert posbnd == g["flags"]["posbnd"] and badradar == g["flags"]["badradar"]
+    assert plog == g["flags"]["posbnd_logfactor"]
+    assert blog == g["flags"]["badradar_logfactor"]
+
+
 def test_config1_maps_match_arrays(orc):
     m, ds_fn, params = synth.ellipsoid_model(), *gc.DELDOP_CASES["c1"][1:]
     ds = ds_fn(lambda d, p: orc.eval_deldop(m, d, p)["fits"], params)
