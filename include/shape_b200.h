@@ -85,6 +85,16 @@ int shape_engine_add_deldop_set(shape_engine *e, const shape_deldop_set *set,
                                 const double *obs, const double *oneovervar);
 int shape_engine_add_lghtcrv_set(shape_engine *e, const shape_lghtcrv_set *set,
                                  const shape_lghtcrv_point *points);
+/* Appends a Doppler set (calc_doppler / pos2doppler / chi2_doppler,
+ * src/shape/calc_fits.c:830, src/shape/pos2doppler.c:149,
+ * src/shape/chi2.c:722); obs and oneovervar hold every frame's ndop bins back
+ * to back. Its frames join the radar frames (fit, results, POS maps) as
+ * 1 x ndop images; footprints that leave a spectrum go to its overflow
+ * spectrum, whose chi-square terms enter the frame's o2 and m2. Returns the
+ * set index (>= 0) or a status. */
+int shape_engine_add_doppler_set(shape_engine *e, const shape_doppler_set *set,
+                                 int nframes, const shape_doppler_frame *frames,
+                                 const double *obs, const double *oneovervar);
 /* Allocates device state for everything added so far. */
 int shape_engine_finalize(shape_engine *e);
 
@@ -99,8 +109,15 @@ int shape_engine_get_vertex_r(shape_engine *e, int i, double *value);
  * comes back device->host. */
 int shape_engine_evaluate(shape_engine *e, int form, shape_eval_summary *out);
 
-/* Results of the last evaluation (device->host copies). */
+/* Results of the last evaluation (device->host copies). Radar frames
+ * (delay-Doppler and Doppler) in dataset order. */
 int shape_engine_get_deldop_results(shape_engine *e, shape_deldop_result *out, int max);
+/* Overflow-spectrum terms of the radar frames of the last evaluation, 4 per
+ * frame: overflow_o2, overflow_m2, overflow_xsec, overflow_dopmean
+ * (struct dopfrm_t, src/shape/shape2.h:1253-1256); zeros for delay-Doppler
+ * frames, whose overflow terms the reference leaves at zero. Returns the
+ * number of frames written. */
+int shape_engine_get_radar_overflow(shape_engine *e, double *out, int max);
 int shape_engine_get_fit(shape_engine *e, int global_frame, double *fit);
 /* POS maps are kept only when enabled before the evaluation (they cost HBM
  * traffic): keep = 1 writes z, cos(e), cos(i) and facet maps of every frame. */

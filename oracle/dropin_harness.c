@@ -42,6 +42,12 @@ void ref_get_chi2s(void *h, int s, double *dat_chi2, double *set_chi2, double *f
             frame_chi2[f] = dd->frame[f].chi2;
             frame_cal[f] = dd->frame[f].cal.val;
         }
+    } else if (S->dat.set[s].type == DOPPLER) {
+        struct doppler_t *dp = &S->dat.set[s].desc.doppler;
+        for (int f = 0; f < dp->nframes; f++) {
+            frame_chi2[f] = dp->frame[f].chi2;
+            frame_cal[f] = dp->frame[f].cal.val;
+        }
     } else if (S->dat.set[s].type == LGHTCRV) {
         frame_chi2[0] = S->dat.set[s].chi2;
         frame_cal[0] = S->dat.set[s].desc.lghtcrv.cal.val;

@@ -218,6 +218,7 @@ __global__ void k_reset_state(FrameState *st, int nviews, int *bin_count, int nt
         s.dellim[0] = s.doplim[0] = dkey(HUGENUMBER);
         s.dellim[1] = s.doplim[1] = dkey(-HUGENUMBER);
         s.any_lit = 0;
+        s.any_overflow = 0;
         st[i] = s;
     }
     for (int t = i; t < ntiles; t += gridDim.x * blockDim.x)
@@ -317,7 +318,10 @@ __device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr)
     const FrameHost &h = a.fh[fr];
     const FrameGeom &g = a.geoms[h.view];
     const FrameState &st = a.states[h.view];
-    KSum q[3] = {{0, 0}, {0, 0}, {0, 0}};
+    // a Doppler frame's sums start from its overflow spectrum's o2 and m2
+    // (src/shape/chi2.c:745-747)
+    const double *ovf = (h.dop_index >= 0) ? a.ovf_out + (size_t)h.dop_index * DOP_OVF_TERMS : nullptr;
+    KSum q[3] = {{ovf ? ovf[0] : 0.0, 0}, {ovf ? ovf[1] : 0.0, 0}, {0, 0}};
     for (int it = h.item0; it < h.item0 + h.nitems; it++)
         for (int k = 0; k < 3; k++) {
             q[k].add(a.partials[(size_t)it * 6 + 2 * k]);
@@ -352,6 +356,10 @@ __device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr)
     }
     r.badradar = h.badradar;
     r.badradar_logfactor = h.badradar_logfactor;
+    if (ovf && ovf[4] != 0.0) {       // model wider than the overflow spectrum
+        r.badradar = 1;
+        r.badradar_logfactor += ovf[5];
+    }
     r.idellim[0] = min(g.ndel + 999999, st.idellim[0]);
     r.idellim[1] = max(-999999, st.idellim[1]);
     r.idoplim[0] = min(g.ndop + 999999, st.idoplim[0]);
@@ -363,6 +371,10 @@ __device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr)
     r.dellim[1] = (dl1 - g.delshift) * dpp;
     r.doplim[0] = (pl0 - g.dopshift) * fpp - a.dop_extra[fr];
     r.doplim[1] = (pl1 - g.dopshift) * fpp + a.dop_extra[fr];
+    if (g.dop1d) {                    // a spectrum has no delay axis
+        r.idellim[0] = r.idellim[1] = 0;
+        r.dellim[0] = r.dellim[1] = 0.0;
+    }
     a.results[fr] = r;
     return r;
 }
@@ -371,6 +383,65 @@ __global__ void k_finalize_frames(FinalizeArgs a)
 {
     int fr = blockIdx.x * blockDim.x + threadIdx.x;
     if (fr < a.nframes) finalize_frame(a, fr);
+}
+
+// Overflow spectra of the Doppler frames (src/shape/pos2doppler.c:451-499):
+// one block per frame sums the bins inside the frame's Doppler limits
+// (count of nonzero bins, squares over the noise variance, cross section and
+// its mean bin) and flags a model wider than the overflow spectrum.
+__global__ void k_doppler_overflow(DopOvfArgs a)
+{
+    __shared__ double red[4][32];
+    const int k = blockIdx.x;
+    const int fr = a.frames[k];
+    const FrameHost &h = a.fh[fr];
+    const FrameGeom &g = a.geoms[h.view];
+    const FrameState &st = a.states[h.view];
+    double *out = a.out + (size_t)k * DOP_OVF_TERMS;
+    if (!st.any_overflow) {
+        if (threadIdx.x < DOP_OVF_TERMS) out[threadIdx.x] = 0.0;
+        return;
+    }
+    const double *ov = a.ovf + g.ovf_base;
+    const double variance = h.sdev * h.sdev;
+    const int idop0 = g.idop0;
+    const int j1 = max(st.idoplim[0] + idop0, 0), j2 = min(st.idoplim[1] + idop0, DOP_MAXOVERFLOW - 1);
+    double o2 = 0.0, m2 = 0.0, xs = 0.0, dm = 0.0;
+    for (int j = j1 + (int)threadIdx.x; j <= j2; j += blockDim.x) {
+        const double v = ov[j];
+        if (v != 0.0) {
+            o2 += 1.0;
+            m2 += v * v / variance;
+            xs += v;
+            dm += (j - idop0) * v;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        o2 += __shfl_down_sync(0xffffffffu, o2, o);
+        m2 += __shfl_down_sync(0xffffffffu, m2, o);
+        xs += __shfl_down_sync(0xffffffffu, xs, o);
+        dm += __shfl_down_sync(0xffffffffu, dm, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = o2; red[1][w] = m2; red[2][w] = xs; red[3][w] = dm; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        o2 = m2 = xs = dm = 0.0;
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) {
+            o2 += red[0][ww]; m2 += red[1][ww]; xs += red[2][ww]; dm += red[3][ww];
+        }
+        if (xs != 0.0) dm /= xs;
+        out[0] = o2; out[1] = m2; out[2] = xs; out[3] = dm;
+        const int lo = st.idoplim[0] + idop0, hi = st.idoplim[1] + idop0;
+        if (lo < 0 || hi >= DOP_MAXOVERFLOW) {
+            const double dopfactor = (max(hi, DOP_MAXOVERFLOW) - min(lo, 0)) / (1.0 * DOP_MAXOVERFLOW);
+            out[4] = 1.0;
+            out[5] = log(dopfactor);
+        } else {
+            out[4] = 0.0;
+            out[5] = 0.0;
+        }
+    }
 }
 
 // ------------------------------------------------------------ lightcurves
@@ -688,7 +759,7 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
     out.posbnd = posbnd;
     out.posbnd_logfactor = plog / a.dof;
     out.badradar = badradar;
-    out.badradar_logfactor = blog / (a.dof_deldop + 0.0);
+    out.badradar_logfactor = blog / a.dof_radar;
     double err = chi2 / a.dof;
     if (a.baddiam) err *= a.bad_objfactor * exp(a.baddiam_logfactor);
     if (posbnd) err *= a.bad_objfactor * exp(out.posbnd_logfactor);
@@ -750,6 +821,12 @@ void launch_chi2_partials(const Chi2Args &a, int fp32, cudaStream_t s)
     if (blocks <= 0) return;
     if (fp32) k_chi2_partials<float><<<blocks, CHI2_THREADS, 0, s>>>(a);
     else k_chi2_partials<double><<<blocks, CHI2_THREADS, 0, s>>>(a);
+}
+
+void launch_doppler_overflow(const DopOvfArgs &a, cudaStream_t s)
+{
+    if (a.n <= 0) return;
+    k_doppler_overflow<<<a.n, 256, 0, s>>>(a);
 }
 
 void launch_finalize_frames(const FinalizeArgs &a, cudaStream_t s)

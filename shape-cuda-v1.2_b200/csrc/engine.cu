@@ -91,7 +91,7 @@ int EngineImpl::finalize()
     cap = fixed_cap > 0 ? fixed_cap : 512;
     geoms.clear(); fh.clear(); work.clear(); view_work0.clear(); view_nwork.clear();
     chi2_items.clear(); frame_view.clear(); dop_extra.clear(); set_delpp.clear(); set_doppp.clear();
-    lcpts.clear(); lc_items.clear(); pt_items.clear(); lcdev.clear();
+    lcpts.clear(); lc_items.clear(); pt_items.clear(); lcdev.clear(); dop_frames.clear();
 
     const int nframes = (int)frames.size();
     const int npts = (int)points.size();
@@ -156,7 +156,9 @@ int EngineImpl::finalize()
                 g.const1 = (double)g.spb_over_stride;
                 g.const2 = 0.0;
             }
-            g.delfact = -SHAPE_KM2US / S.del_per_pixel;
+            // a Doppler frame's single row: delPOS = z*0 + 1 = 1 exactly, so its
+            // delay response tri2(0) is 1 and its weights are pos2doppler's
+            g.delfact = dd[s].doppler ? 0.0 : -SHAPE_KM2US / S.del_per_pixel;
             double w[3];
             mv(w, F.oe, F.spin);
             double dopfact = S.dopscale * SHAPE_KM2HZFACT * F.km_per_pixel * S.Ftx / S.dop_per_pixel;
@@ -181,6 +183,11 @@ int EngineImpl::finalize()
             g.dopfftlen = S.dopfftlen;
             g.law = law;
             g.frame_index = fi;
+            g.dop1d = dd[s].doppler;
+            if (g.dop1d) {
+                g.idop0 = DOP_MAXOVERFLOW / 2 - (int)floor(g.dopshift + 0.5);
+                g.ovf_base = (long long)dop_frames.size() * DOP_MAXOVERFLOW;
+            }
             FrameHost h;
             memset(&h, 0, sizeof h);
             h.weight = F.weight;
@@ -193,6 +200,9 @@ int EngineImpl::finalize()
             }
             h.view = (int)geoms.size();
             h.set = (int)s;
+            h.dop_index = g.dop1d ? (int)dop_frames.size() : -1;
+            h.sdev = frame_sdev[fi];
+            if (g.dop1d) dop_frames.push_back(fi);
             frame_view.push_back(h.view);
             h.item0 = (int)chi2_items.size();
             int D = F.ndel * F.ndop, chunk = CHI2_THREADS * CHI2_ITEMS;
@@ -309,6 +319,11 @@ int EngineImpl::finalize()
     AL(d_lcsets, lcdev.size()); AL(d_lc_out, 4 * lcdev.size());
     AL(d_lc_dof, lcdev.size()); AL(d_lc_npts, lcdev.size());
     AL(d_setrecs, setrecs.size());
+    if (!dop_frames.empty()) {
+        AL(d_ovf, dop_frames.size() * DOP_MAXOVERFLOW);
+        AL(d_ovf_out, dop_frames.size() * DOP_OVF_TERMS);
+        AL(d_dop_frames, dop_frames.size());
+    }
     AL(d_summary, 1);
     size_t lc_tot_pts = points.size(), lc_tot_n = 0;
     for (auto &L : lc) lc_tot_n += L.set.n;
@@ -377,6 +392,9 @@ int EngineImpl::finalize()
         CK(cudaMemcpyAsync(d_lc_npts, lcnp.data(), sizeof(double) * lcnp.size(), cudaMemcpyHostToDevice, s));
     }
     CK(cudaMemcpyAsync(d_setrecs, setrecs.data(), sizeof(SetRec) * setrecs.size(), cudaMemcpyHostToDevice, s));
+    if (!dop_frames.empty())
+        CK(cudaMemcpyAsync(d_dop_frames, dop_frames.data(), sizeof(int) * dop_frames.size(),
+                           cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(d_seen, 0, nf, s));
     CK(cudaStreamSynchronize(s));
 
@@ -477,6 +495,8 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         else CK(cudaMemsetAsync(d_fit64, 0, sizeof(double) * fit_elems, sr));
     }
     CK(cudaMemsetAsync(d_seen, 0, nf, sr));
+    if (!dop_frames.empty())
+        CK(cudaMemsetAsync(d_ovf, 0, sizeof(double) * dop_frames.size() * DOP_MAXOVERFLOW, sr));
     if (fork) {
         CK(cudaEventRecord(evf[2], stream2));        // reset and clears done
         CK(cudaStreamWaitEvent(stream2, evf[1], 0));  // facet normals exist
@@ -504,6 +524,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     ra.mincosine_seen = params.mincosine_seen;
     ra.mark_seen = params.mark_seen;
     ra.keep_pos = keep_pos;
+    ra.ovf = d_ovf;
 
     Chi2Args ca;
     ca.obs = d_obs; ca.oov = d_oov;
@@ -582,6 +603,14 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     fa.fh = d_fh; fa.geoms = d_geoms; fa.states = d_states; fa.partials = d_partials;
     fa.results = d_results; fa.set_delpp = d_set_delpp; fa.set_doppp = d_set_doppp;
     fa.dop_extra = d_dop_extra;
+    fa.ovf_out = d_ovf_out;
+    if (!dop_frames.empty()) {
+        DopOvfArgs oa;
+        oa.n = (int)dop_frames.size();
+        oa.frames = d_dop_frames; oa.fh = d_fh; oa.geoms = d_geoms; oa.states = d_states;
+        oa.ovf = d_ovf; oa.out = d_ovf_out;
+        launch_doppler_overflow(oa, s);
+    }
     if (!lcdev.empty()) {
         LcFinalizeArgs lf;
         lf.nsets = (int)lcdev.size();
@@ -600,7 +629,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     sa.nsets = (int)setrecs.size();
     sa.sets = d_setrecs; sa.fh = d_fh; sa.results = d_results;
     sa.lc_out = d_lc_out; sa.lc_dof = d_lc_dof; sa.lc_npts = d_lc_npts;
-    sa.dof = dof; sa.dof_deldop = dof_deldop; sa.bad_objfactor = bad_objfactor;
+    sa.dof = dof; sa.dof_radar = dof_deldop + dof_doppler; sa.bad_objfactor = bad_objfactor;
     // the bad-diameter factor depends only on host-side scale factors and is
     // applied by evaluate(), so captured graphs stay valid when it changes
     sa.baddiam = 0;
@@ -626,6 +655,7 @@ int EngineImpl::kernels_per_eval(int form) const
         n += lc_items.empty() ? 0 : 1;
     }
     n += lcdev.empty() ? 0 : 1;          // lightcurve finalize
+    n += dop_frames.empty() ? 0 : 1;     // Doppler overflow spectra
     return n + 1;                        // finalize + summary
 }
 
@@ -724,7 +754,7 @@ int shape_abi_sizes(size_t *out, int max)
     size_t v[] = {sizeof(shape_model_desc), sizeof(shape_radar_law), sizeof(shape_optical_law),
                   sizeof(shape_eval_params), sizeof(shape_deldop_frame), sizeof(shape_deldop_set),
                   sizeof(shape_lghtcrv_point), sizeof(shape_lghtcrv_set), sizeof(shape_deldop_result),
-                  sizeof(shape_eval_summary)};
+                  sizeof(shape_eval_summary), sizeof(shape_doppler_frame), sizeof(shape_doppler_set)};
     int n = (int)(sizeof v / sizeof v[0]);
     for (int i = 0; i < n && i < max; i++) out[i] = v[i];
     return n;
@@ -812,6 +842,7 @@ int shape_engine_add_deldop_set(shape_engine *h, const shape_deldop_set *set, in
         E.oov.insert(E.oov.end(), oov + off, oov + off + D);
         off += D;
         E.frames.push_back(F);
+        E.frame_sdev.push_back(0.0);
         E.dof += F.dof;
         E.dof_deldop += F.dof;
     }
@@ -819,6 +850,75 @@ int shape_engine_add_deldop_set(shape_engine *h, const shape_deldop_set *set, in
     E.dd.push_back(d);
     E.finalized = false;
     return (int)E.setrecs.size() - 1;
+}
+
+// A Doppler set runs as a delay-Doppler set of one-row frames (LONG_ORIG,
+// spb = stride = 1, zero delay scale, delay bin 1), which reproduces
+// pos2doppler's weights; the overflow spectrum is the Doppler frames' own.
+int shape_engine_add_doppler_set(shape_engine *h, const shape_doppler_set *set, int nframes,
+                                 const shape_doppler_frame *frames, const double *obs, const double *oov)
+{
+    if (!h || !set || nframes <= 0 || !frames || !obs || !oov)
+        return shape::set_err(SHAPE_E_ARG, "add_doppler_set: invalid argument");
+    if (!(set->dop_per_bin > 0)) return shape::set_err(SHAPE_E_ARG, "add_doppler_set: dop_per_bin must be > 0");
+    EngineImpl &E = h->impl;
+    shape::DdSetHost d;
+    memset(&d.set, 0, sizeof d.set);
+    d.set.del_per_pixel = 1.0;
+    d.set.dop_per_pixel = set->dop_per_bin;
+    d.set.Ftx = set->Ftx;
+    d.set.dopscale = set->dopscale;
+    d.set.codemethod = SHAPE_CODE_LONG_ORIG;
+    d.set.spb = d.set.stride = 1;
+    d.set.dopfftlen = 1;
+    d.set.law = set->law;
+    d.doppler = 1;
+    d.frame0 = (int)E.frames.size();
+    d.nframes = nframes;
+    size_t off = 0;
+    for (int k = 0; k < nframes; k++) {
+        const shape_doppler_frame &P = frames[k];
+        if (P.pos_n < 1 || P.ndop < 1 || !(P.km_per_pixel > 0))
+            return shape::set_err(SHAPE_E_ARG, "add_doppler_set: bad frame size");
+        shape_deldop_frame F;
+        memset(&F, 0, sizeof F);
+        F.pos_n = P.pos_n; F.km_per_pixel = P.km_per_pixel;
+        memcpy(F.ae, P.ae, sizeof F.ae); memcpy(F.oe, P.oe, sizeof F.oe); memcpy(F.spin, P.spin, sizeof F.spin);
+        F.deloff = 0.0; F.dopoff = P.dopoff;
+        F.ndel = 1; F.ndop = P.ndop;
+        F.delcom_vig = 1.0; F.dopcom_vig = P.dopcom_vig; F.dopDC_vig = 0.0;
+        F.weight = P.weight; F.dof = P.dof; F.cal_floating = P.cal_floating; F.cal = P.cal;
+        E.frame_off.push_back((long long)E.obs.size());
+        E.obs.insert(E.obs.end(), obs + off, obs + off + P.ndop);
+        E.oov.insert(E.oov.end(), oov + off, oov + off + P.ndop);
+        off += (size_t)P.ndop;
+        E.frames.push_back(F);
+        E.frame_sdev.push_back(P.sdev);
+        E.dof += P.dof;
+        E.dof_doppler += P.dof;
+    }
+    E.setrecs.push_back(shape::SetRec{0, d.frame0, nframes});
+    E.dd.push_back(d);
+    E.finalized = false;
+    return (int)E.setrecs.size() - 1;
+}
+
+int shape_engine_get_radar_overflow(shape_engine *h, double *out, int max)
+{
+    if (!h || !out) return shape::set_err(SHAPE_E_ARG, "null argument");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0) return shape::set_err(SHAPE_E_STATE, "no evaluation yet");
+    const int n = std::min<int>(max, (int)E.fh.size());
+    std::vector<double> dop(E.dop_frames.size() * shape::DOP_OVF_TERMS);
+    if (!dop.empty()) {
+        cudaError_t e = cudaMemcpy(dop.data(), E.d_ovf_out, sizeof(double) * dop.size(), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(e));
+    }
+    for (int f = 0; f < n; f++) {
+        const int k = E.fh[f].dop_index;
+        for (int j = 0; j < 4; j++) out[4 * f + j] = (k >= 0) ? dop[(size_t)k * shape::DOP_OVF_TERMS + j] : 0.0;
+    }
+    return n;
 }
 
 int shape_engine_add_lghtcrv_set(shape_engine *h, const shape_lghtcrv_set *set,

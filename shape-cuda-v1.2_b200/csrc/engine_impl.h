@@ -53,8 +53,9 @@ struct DevMem {
 };
 
 struct DdSetHost {
-    shape_deldop_set set;
+    shape_deldop_set set;       // a Doppler set is held as a one-row delay-Doppler set
     int frame0, nframes;
+    int doppler = 0;            // 1: Doppler spectra (shape_engine_add_doppler_set)
 };
 struct LcSetHost {
     shape_lghtcrv_set set;
@@ -90,7 +91,8 @@ struct EngineImpl {
     std::vector<shape_lghtcrv_point> points;
     std::vector<SetRec> setrecs;
     std::vector<RadarLawDev> laws;
-    double dof = 0, dof_deldop = 0, dof_lghtcrv = 0;
+    double dof = 0, dof_deldop = 0, dof_doppler = 0, dof_lghtcrv = 0;
+    std::vector<double> frame_sdev;     // per radar frame: Doppler noise sdev (0 for delay-Doppler)
 
     // derived (host)
     std::vector<FrameGeom> geoms;
@@ -143,6 +145,9 @@ struct EngineImpl {
     SetRec *d_setrecs = nullptr;
     shape_eval_summary *d_summary = nullptr;
     std::vector<LcSetDev> lcdev;
+    std::vector<int> dop_frames;        // global indices of the Doppler frames
+    double *d_ovf = nullptr, *d_ovf_out = nullptr;
+    int *d_dop_frames = nullptr;
 
     // pinned staging
     double *h_params = nullptr;             // r[nv], scale[3]
@@ -196,7 +201,8 @@ struct EngineImpl {
         params = o.params; bad_objfactor = o.bad_objfactor;
         dd = o.dd; frames = o.frames; frame_off = o.frame_off; obs = o.obs; oov = o.oov;
         lc = o.lc; points = o.points; setrecs = o.setrecs;
-        dof = o.dof; dof_deldop = o.dof_deldop; dof_lghtcrv = o.dof_lghtcrv;
+        dof = o.dof; dof_deldop = o.dof_deldop; dof_doppler = o.dof_doppler; dof_lghtcrv = o.dof_lghtcrv;
+        frame_sdev = o.frame_sdev;
         fixed_cap = o.fixed_cap;
         finalized = false;
     }

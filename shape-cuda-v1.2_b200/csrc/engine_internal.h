@@ -26,6 +26,7 @@ constexpr int STAGE_FACETS = 128;   // facets staged in shared memory per pass
 constexpr int CHI2_THREADS = 256;
 constexpr int CHI2_ITEMS = 8;       // elements per thread per chi2 block
 constexpr int FIT32_PAD = 16;       // FP32 fit arena padding (vector reductions, k_raster)
+constexpr int DOP_MAXOVERFLOW = 2000;   // Doppler overflow spectrum bins (MAXOVERFLOW, src/shape/const.h:181)
 
 // View kinds of a FrameGeom.
 constexpr int VIEW_RADAR = 0;       // delay-Doppler frame, observer view
@@ -50,7 +51,13 @@ struct FrameGeom {
     double xincr, yincr, dopdiff_bl, dopdiff_max, dopDC_vig, dopfftlen;
     int codemethod, spb, stride, spb_over_stride, spb_sq, nsinc2, nsinc2_sq, sinc2width;
     int law;             // index into the radar law table
-    int frame_index;     // global delay-Doppler frame index or lightcurve point index
+    int frame_index;     // global radar frame index or lightcurve point index
+    // Doppler-only frames run as one-row delay-Doppler frames whose delay
+    // response is exactly 1; pixels whose footprint leaves the spectrum go to
+    // an overflow spectrum of DOP_MAXOVERFLOW bins (src/shape/pos2doppler.c)
+    int dop1d;           // 1: Doppler spectrum
+    int idop0;           // overflow bin of spectrum bin 0: MAXOVERFLOW/2 - floor(dopshift + 0.5)
+    long long ovf_base;  // first element of this frame's overflow spectrum
     // the synthesis constants rounded to float on the host for the FP32
     // raster, in FDD_* order (five float4 loads per tile instead of one
     // double->float conversion per constant per pixel)
@@ -75,6 +82,7 @@ struct FrameState {
     int idellim[2], idoplim[2];
     unsigned long long dellim[2], doplim[2];  // ordered keys of min / max
     int any_lit;
+    int any_overflow;                // Doppler frame: a footprint left the spectrum
 };
 
 // Radar scattering law table entry (mirror of shape_radar_law).

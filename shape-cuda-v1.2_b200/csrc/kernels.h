@@ -40,6 +40,7 @@ struct RasterArgs {
     double mincosine_seen;
     int mark_seen;
     int keep_pos;
+    double *ovf;               // Doppler overflow spectra (DOP_MAXOVERFLOW per Doppler frame)
     size_t smem_bytes;         // dynamic shared memory of the raster CTA (set by the launcher)
 };
 
@@ -65,13 +66,15 @@ struct Chi2Args {
 };
 void launch_chi2_partials(const Chi2Args &a, int fp32, cudaStream_t s);
 
-struct FrameHost {             // per deldop frame constants for finalize
+struct FrameHost {             // per radar frame constants for finalize
     double weight, dof, cal_in;
     int cal_floating, badradar;
     double badradar_logfactor;
     int view;
     int set;
     int item0, nitems;
+    int dop_index;             // Doppler frame: index of its overflow terms, else -1
+    double sdev;               // Doppler frame: receiver noise sdev (overflow variance)
 };
 struct FinalizeArgs {
     int nframes;
@@ -82,8 +85,24 @@ struct FinalizeArgs {
     shape_deldop_result *results;
     const double *set_delpp, *set_doppp;     // per set del/dop per pixel
     const double *dop_extra;                 // per frame
+    const double *ovf_out;                   // per Doppler frame: DOP_OVF_TERMS values
 };
 void launch_finalize_frames(const FinalizeArgs &a, cudaStream_t s);
+
+// Doppler overflow spectra (src/shape/pos2doppler.c:451-499): per Doppler
+// frame o2, m2, xsec, mean bin, and the badradar flag and log-factor of a
+// model wider than the overflow spectrum.
+constexpr int DOP_OVF_TERMS = 6;
+struct DopOvfArgs {
+    int n;                      // Doppler frames
+    const int *frames;          // their global radar frame indices
+    const FrameHost *fh;
+    const FrameGeom *geoms;
+    const FrameState *states;
+    const double *ovf;          // overflow spectra
+    double *out;                // [n * DOP_OVF_TERMS]
+};
+void launch_doppler_overflow(const DopOvfArgs &a, cudaStream_t s);
 
 struct LcArgs {
     int npoints;
@@ -138,7 +157,7 @@ struct SummaryArgs {
     const double *lc_out;       // per lightcurve set: cal, chi2, posbnd, logfactor sum
     const double *lc_dof;
     const double *lc_npts;
-    double dof, dof_deldop;
+    double dof, dof_radar;      // all data / delay-Doppler + Doppler (calc_fits.c:409)
     double bad_objfactor;
     int baddiam;
     double baddiam_logfactor;

@@ -583,6 +583,38 @@ __device__ inline void pixel_dd_scatter_f32_direct(const RasterArgs &a, const Fr
     }
 }
 
+// A Doppler pixel whose footprint leaves the spectrum adds its contributions
+// to the frame's overflow spectrum instead (src/shape/pos2doppler.c:399-414):
+// the same weights as pixel_dd_scatter's generic path (one row, delay
+// response 1), bins clipped to the overflow spectrum.
+template <typename T>
+__device__ void pixel_dop_overflow(const RasterArgs &a, const FrameGeom &g, const DDC<T> &k, T cose,
+                                   const PixDD<T> &d)
+{
+    const int idop_min = d.idop_min, idop_max = d.idop_max;
+    T s2u = 0;
+    if (g.nsinc2 == 1) {
+        T fr;
+        if constexpr (sizeof(T) == 4) fr = d.dfrac; else fr = d.dopPOS - floor(d.dopPOS);
+        const T su = tsin<T>((T)3.141592653589793 * fr);
+        s2u = su * su;
+    }
+    const T rl = radlaw_dev<T>(a.laws[g.law], cose) * k.kmpp * k.kmpp * d.codefactor;
+    T dop_c[SHAPE_MAXBINS + 1];
+    for (int idop = idop_min; idop <= idop_max; idop++) {
+        T ddop;
+        if constexpr (sizeof(T) == 4) ddop = d.ddop0 - (T)(idop - idop_min); else ddop = d.dopPOS - (T)idop;
+        dop_c[min(idop - idop_min, SHAPE_MAXBINS)] = dop_resp<T>(g, k, d.dopPOS, ddop, s2u, idop);
+    }
+    T sdop = 0;
+    for (int idop = idop_min; idop <= idop_max; idop++) sdop += dop_c[min(idop - idop_min, SHAPE_MAXBINS)];
+    const T amp = rl / ((T)1 * sdop);
+    double *ov = a.ovf + g.ovf_base;
+    const int idop1 = max(idop_min, -g.idop0), idop2 = min(idop_max, -g.idop0 + DOP_MAXOVERFLOW - 1);
+    for (int idop = idop1; idop <= idop2; idop++)
+        atomicAdd(ov + idop + g.idop0, (double)(amp * (T)1 * dop_c[min(idop - idop_min, SHAPE_MAXBINS)]));
+}
+
 __device__ inline int warp_min(int v)
 {
     for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -843,6 +875,9 @@ k_raster(RasterArgs a)
                 pixel_dd_scatter_f32_direct(a, g, kc, scose, dd, static_cast<float *>(a.fit) + g.fit_base);
             else
                 pixel_dd_scatter<T>(a, g, kc, scose, dd, static_cast<T *>(a.fit) + g.fit_base, 1, 1, g.ndop);
+        } else if (g.kind == VIEW_RADAR && g.dop1d && lit) {
+            a.states[item.x].any_overflow = 1;
+            pixel_dop_overflow<T>(a, g, kc, scose, dd);
         }
         if (lane == 0) {
             s_red[wid][0] = cimin; s_red[wid][1] = cimax; s_red[wid][2] = cjmin; s_red[wid][3] = cjmax;

@@ -14,7 +14,9 @@
  *       (:358-360, 522-530), every delay-Doppler frame's fit image, region
  *       limits and badradar_logfactor (src/shape/pos2deldop.c:279-288,
  *       337-354, 543-548), every lightcurve's y and fit arrays
- *       (src/shape/calc_fits.c:1712-1716, 1923-1933), and, for the write
+ *       (src/shape/calc_fits.c:1712-1716, 1923-1933), every Doppler frame's
+ *       fit spectrum, limits and overflow-spectrum terms
+ *       (src/shape/pos2doppler.c:170-176, 451-499), and, for the write
  *       action, the POS z / cos(e) / facet images. The reference's chi2()
  *       (src/shape/chi2.c:240) then runs unchanged on those images.
  *
@@ -33,8 +35,8 @@
  * (src/shape/mkparlist.c:218-235), are pushed on every call.
  *
  * Supported inputs (anything else stops with bailout(), the reference's
- * error convention): one VERTEX component; delay-Doppler and lightcurve
- * sets with one view per frame/point; radar laws COSINELAW_DIFF,
+ * error convention): one VERTEX component; delay-Doppler, Doppler and
+ * lightcurve sets with one view per frame/point (speckle off); radar laws COSINELAW_DIFF,
  * GAUSSIANLAW, HAGFORSLAW, COSINELAW_QS and the three hybrids; optical laws
  * LAMBERTLAW, LOMMEL and KAASALAINEN; dd_gamma = 1; exclude_seen not naming
  * a set of the dataset.
@@ -103,7 +105,7 @@ static uint64_t b200_fingerprint(const struct par_t *par, const struct mod_t *mo
     FNV(h, pm); FNV(h, pd);
     FNV(h, par->pos_smooth); FNV(h, par->nsinc2); FNV(h, par->sinc2width);
     FNV(h, par->mask_tol); FNV(h, par->mincosine_seen); FNV(h, par->exclude_seen);
-    FNV(h, par->bad_objfactor); FNV(h, par->action);
+    FNV(h, par->bad_objfactor); FNV(h, par->action); FNV(h, par->speckle);
     FNV(h, mod->shape.ncomp);
     const struct photo_t *ph = &mod->photo;
     for (int k = 0; k < ph->nradlaws; k++) {
@@ -135,6 +137,21 @@ static uint64_t b200_fingerprint(const struct par_t *par, const struct mod_t *mo
                 FNV(h, po); FNV(h, pv);
                 const struct deldopview_t *v = &fr->view[dd->v0];
                 FNV(h, v->ae); FNV(h, v->oe); FNV(h, v->spin); FNV(h, v->deloff); FNV(h, v->dopoff);
+            }
+        } else if (set->type == DOPPLER) {
+            const struct doppler_t *dp = &set->desc.doppler;
+            FNV(h, dp->nframes); FNV(h, dp->nviews); FNV(h, dp->iradlaw);
+            FNV(h, dp->dop_per_bin); FNV(h, dp->Ftx); FNV(h, dp->dopscale.val);
+            for (int f = 0; f < dp->nframes; f++) {
+                const struct dopfrm_t *fr = &dp->frame[f];
+                FNV(h, fr->ndop); FNV(h, fr->pos.n); FNV(h, fr->pos.km_per_pixel);
+                FNV(h, fr->weight); FNV(h, fr->dof); FNV(h, fr->sdev); FNV(h, fr->cal.state);
+                if (fr->cal.state != 'f') FNV(h, fr->cal.val);
+                FNV(h, fr->dopcom_vig);
+                const void *po = fr->obs, *pv = fr->oneovervar;
+                FNV(h, po); FNV(h, pv);
+                const struct dopview_t *v = &fr->view[dp->v0];
+                FNV(h, v->ae); FNV(h, v->oe); FNV(h, v->spin); FNV(h, v->dopoff);
             }
         } else if (set->type == LGHTCRV) {
             const struct lghtcrv_t *lc = &set->desc.lghtcrv;
@@ -212,6 +229,7 @@ static void b200_build(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
     if (par->dd_gamma != 1.0) b200_unsupported("dd_gamma != 1");
     if (par->exclude_seen >= 0 && par->exclude_seen < dat->nsets)
         b200_unsupported("exclude_seen names a dataset");
+    if (par->speckle) b200_unsupported("speckle noise in the Doppler overflow variance");
     const char *fs = getenv("SHAPE_B200_FORM");
     g_form = SHAPE_FORM_BATCHED_FP64;
     if (fs && !strcmp(fs, "plain_fp64")) g_form = SHAPE_FORM_PLAIN_FP64;
@@ -295,6 +313,38 @@ static void b200_build(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
             int rc = shape_engine_add_deldop_set(g_eng, &S, dd->nframes, F, obs, oov);
             free(F); free(obs); free(oov);
             b200_check(rc, "add_deldop_set");
+        } else if (set->type == DOPPLER) {
+            struct doppler_t *dp = &set->desc.doppler;
+            if (dp->nviews != 1) b200_unsupported("Doppler smearing (nviews > 1)");
+            shape_doppler_set S;
+            S.dop_per_bin = dp->dop_per_bin; S.Ftx = dp->Ftx; S.dopscale = dp->dopscale.val;
+            S.law = radar_law_of(&mod->photo, dp->iradlaw);
+            shape_doppler_frame *F = calloc((size_t)dp->nframes, sizeof *F);
+            size_t total = 0;
+            for (int f = 0; f < dp->nframes; f++) total += (size_t)dp->frame[f].ndop;
+            double *obs = malloc(sizeof(double) * (total ? total : 1));
+            double *oov = malloc(sizeof(double) * (total ? total : 1));
+            size_t off = 0;
+            for (int f = 0; f < dp->nframes; f++) {
+                struct dopfrm_t *fr = &dp->frame[f];
+                struct dopview_t *v = &fr->view[dp->v0];
+                shape_doppler_frame *G = &F[f];
+                G->pos_n = fr->pos.n; G->km_per_pixel = fr->pos.km_per_pixel;
+                rm9(G->ae, v->ae); rm9(G->oe, v->oe);
+                for (int j = 0; j < 3; j++) G->spin[j] = v->spin[j];
+                G->dopoff = v->dopoff;
+                G->ndop = fr->ndop; G->dopcom_vig = fr->dopcom_vig;
+                G->weight = fr->weight; G->dof = fr->dof;
+                G->cal_floating = (fr->cal.state == 'f'); G->cal = fr->cal.val;
+                G->sdev = fr->sdev;
+                for (int j = 1; j <= fr->ndop; j++, off++) {
+                    obs[off] = fr->obs[j];
+                    oov[off] = fr->oneovervar[j];
+                }
+            }
+            int rc = shape_engine_add_doppler_set(g_eng, &S, dp->nframes, F, obs, oov);
+            free(F); free(obs); free(oov);
+            b200_check(rc, "add_doppler_set");
         } else if (set->type == LGHTCRV) {
             struct lghtcrv_t *lc = &set->desc.lghtcrv;
             if (lc->nviews != 1) b200_unsupported("lightcurve smearing (nviews > 1)");
@@ -323,7 +373,7 @@ static void b200_build(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
             free(x); free(t); free(obs); free(oov); free(P);
             b200_check(rc, "add_lghtcrv_set");
         } else {
-            b200_unsupported("Doppler and plane-of-sky datasets");
+            b200_unsupported("plane-of-sky datasets");
         }
     }
     g_keep_pos = (par->action == WRITE);
@@ -363,11 +413,15 @@ static void b200_evaluate(struct par_t *par, struct mod_t *mod, struct dat_t *da
     free(seen);
 }
 
+/* Radar frames in the engine's order: delay-Doppler and Doppler sets in
+ * dataset order. */
 static int total_frames(const struct dat_t *dat)
 {
     int n = 0;
-    for (int s = 0; s < dat->nsets; s++)
+    for (int s = 0; s < dat->nsets; s++) {
         if (dat->set[s].type == DELAY) n += dat->set[s].desc.deldop.nframes;
+        if (dat->set[s].type == DOPPLER) n += dat->set[s].desc.doppler.nframes;
+    }
     return n;
 }
 
@@ -377,9 +431,36 @@ static void copy_frame_results(struct dat_t *dat, int with_chi2)
     int nfr = total_frames(dat);
     if (nfr == 0) return;
     shape_deldop_result *R = malloc(sizeof *R * (size_t)nfr);
+    double *O = malloc(sizeof(double) * 4 * (size_t)nfr);
     b200_check(shape_engine_get_deldop_results(g_eng, R, nfr), "get_deldop_results");
+    b200_check(shape_engine_get_radar_overflow(g_eng, O, nfr), "get_radar_overflow");
     int g = 0;
     for (int s = 0; s < dat->nsets; s++) {
+        if (dat->set[s].type == DOPPLER) {
+            struct doppler_t *dp = &dat->set[s].desc.doppler;
+            double set_chi2 = 0.0;
+            for (int f = 0; f < dp->nframes; f++, g++) {
+                struct dopfrm_t *fr = &dp->frame[f];
+                const shape_deldop_result *q = &R[g];
+                for (int k = 0; k < 2; k++) {
+                    fr->pos.xlim[k] = q->xlim[k]; fr->pos.ylim[k] = q->ylim[k];
+                    fr->idoplim[k] = q->idoplim[k]; fr->doplim[k] = q->doplim[k];
+                }
+                fr->badradar_logfactor = q->badradar_logfactor;
+                fr->pos.posbnd_logfactor = q->posbnd_logfactor;
+                fr->overflow_o2 = O[4 * g + 0];
+                fr->overflow_m2 = O[4 * g + 1];
+                fr->overflow_xsec = O[4 * g + 2];
+                fr->overflow_dopmean = O[4 * g + 3];
+                if (with_chi2) {
+                    if (fr->cal.state == 'f') fr->cal.val = q->cal;
+                    fr->chi2 = q->chi2;
+                    set_chi2 += q->chi2;
+                }
+            }
+            if (with_chi2) dat->set[s].chi2 = set_chi2;
+            continue;
+        }
         if (dat->set[s].type != DELAY) continue;
         struct deldop_t *dd = &dat->set[s].desc.deldop;
         double set_chi2 = 0.0;
@@ -402,6 +483,7 @@ static void copy_frame_results(struct dat_t *dat, int with_chi2)
         if (with_chi2) dat->set[s].chi2 = set_chi2;
     }
     free(R);
+    free(O);
 }
 
 void SHAPE_B200_CALC_FITS(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
@@ -410,12 +492,17 @@ void SHAPE_B200_CALC_FITS(struct par_t *par, struct mod_t *mod, struct dat_t *da
     b200_evaluate(par, mod, dat, &sm);
     copy_frame_results(dat, 0);
     size_t maxd = 1;
-    for (int s = 0; s < dat->nsets; s++)
+    for (int s = 0; s < dat->nsets; s++) {
         if (dat->set[s].type == DELAY)
             for (int f = 0; f < dat->set[s].desc.deldop.nframes; f++) {
                 size_t D = (size_t)dat->set[s].desc.deldop.frame[f].ndel * dat->set[s].desc.deldop.frame[f].ndop;
                 if (D > maxd) maxd = D;
             }
+        if (dat->set[s].type == DOPPLER)
+            for (int f = 0; f < dat->set[s].desc.doppler.nframes; f++)
+                if ((size_t)dat->set[s].desc.doppler.frame[f].ndop > maxd)
+                    maxd = (size_t)dat->set[s].desc.doppler.frame[f].ndop;
+    }
     double *buf = malloc(sizeof(double) * maxd);
     int g = 0;
     for (int s = 0; s < dat->nsets; s++) {
@@ -428,6 +515,26 @@ void SHAPE_B200_CALC_FITS(struct par_t *par, struct mod_t *mod, struct dat_t *da
                 size_t k = 0;
                 for (int i = 1; i <= fr->ndel; i++)
                     for (int j = 1; j <= fr->ndop; j++) fr->fit[i][j] = buf[k++];
+                if (g_keep_pos) {
+                    int n = fr->pos.n, side = 2 * n + 1;
+                    size_t np = (size_t)side * side;
+                    double *z = malloc(sizeof(double) * np), *ce = malloc(sizeof(double) * np);
+                    int *fa = malloc(sizeof(int) * np);
+                    b200_check(shape_engine_get_pos(g_eng, g, z, ce, fa), "get_pos");
+                    for (int i = -n; i <= n; i++)
+                        for (int j = -n; j <= n; j++) {
+                            size_t p = (size_t)(i + n) * side + (size_t)(j + n);
+                            fr->pos.z[i][j] = z[p]; fr->pos.cose[i][j] = ce[p]; fr->pos.f[i][j] = fa[p];
+                        }
+                    free(z); free(ce); free(fa);
+                }
+            }
+        } else if (set->type == DOPPLER) {
+            struct doppler_t *dp = &set->desc.doppler;
+            for (int f = 0; f < dp->nframes; f++, g++) {
+                struct dopfrm_t *fr = &dp->frame[f];
+                b200_check(shape_engine_get_fit(g_eng, g, buf), "get_fit");
+                for (int j = 1; j <= fr->ndop; j++) fr->fit[j] = buf[j - 1];
                 if (g_keep_pos) {
                     int n = fr->pos.n, side = 2 * n + 1;
                     size_t np = (size_t)side * side;

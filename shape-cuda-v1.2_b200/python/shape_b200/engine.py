@@ -89,6 +89,9 @@ def load_library(path=LIB_PATH):
     L.shape_engine_add_deldop_set.argtypes = [vp, P(cd.DeldopSet), C.c_int, P(cd.DeldopFrame),
                                               cd.dptr, cd.dptr]
     L.shape_engine_add_lghtcrv_set.argtypes = [vp, P(cd.LghtcrvSet), P(cd.LghtcrvPoint)]
+    L.shape_engine_add_doppler_set.argtypes = [vp, P(cd.DopplerSet), C.c_int, P(cd.DopplerFrame),
+                                               cd.dptr, cd.dptr]
+    L.shape_engine_get_radar_overflow.argtypes = [vp, cd.dptr, C.c_int]
     L.shape_engine_finalize.argtypes = [vp]
     L.shape_engine_set_scale.argtypes = [vp, C.c_int, C.c_double]
     L.shape_engine_set_vertex_r.argtypes = [vp, C.c_int, C.c_double]
@@ -182,6 +185,23 @@ class Engine:
         self.deldops.append(ds)
         self.set_index.append(("deldop", len(self.deldops) - 1))
         return idx
+
+    def add_doppler(self, ds):
+        """A Doppler set; its frames join the radar frames in call order."""
+        arr = ds.frame_array()
+        self._keep.append(arr)
+        idx = _chk(self.L.shape_engine_add_doppler_set(self.h, C.byref(ds.set), ds.nframes, arr,
+                                                       cd.as_dptr(ds.obs), cd.as_dptr(ds.oneovervar)))
+        self.deldops.append(ds)
+        self.set_index.append(("doppler", len(self.deldops) - 1))
+        return idx
+
+    def radar_overflow(self):
+        """[overflow_o2, overflow_m2, overflow_xsec, overflow_dopmean] per radar frame."""
+        nfr = len(self.frames)
+        out = np.zeros(4 * max(1, nfr))
+        n = _chk(self.L.shape_engine_get_radar_overflow(self.h, cd.as_dptr(out), nfr))
+        return out[:4 * n].reshape(n, 4)
 
     def add_lghtcrv(self, ds):
         arr = ds.point_array()
@@ -278,7 +298,7 @@ class Engine:
 
     def fit(self, frame):
         fr = self.frames[frame]
-        out = np.zeros(fr.ndel * fr.ndop)
+        out = np.zeros(getattr(fr, "ndel", 1) * fr.ndop)
         _chk(self.L.shape_engine_get_fit(self.h, frame, cd.as_dptr(out)))
         return out
 
@@ -321,12 +341,15 @@ class Engine:
         return {"x": x, "vn": vn, "fn": fn, "area": area}
 
 
-def make_engine(model, params, deldops=(), lghtcrvs=(), device=0):
+def make_engine(model, params, deldops=(), lghtcrvs=(), device=0, dopplers=()):
+    """An engine with the sets added in the order deldops, dopplers, lightcurves."""
     e = Engine(device)
     e.set_model(model)
     e.set_params(params)
     for ds in deldops:
         e.add_deldop(ds)
+    for ds in dopplers:
+        e.add_doppler(ds)
     for ds in lghtcrvs:
         e.add_lghtcrv(ds)
     e.finalize()
@@ -350,6 +373,17 @@ def engine_synthesizer(model, device=0):
         e.close()
         return y
     return deldop, lghtcrv
+
+
+def engine_doppler_synthesizer(model, device=0):
+    """A ``synthesize`` callable for synth.doppler_dataset (FP64 engine path)."""
+    def doppler(ds, params):
+        e = make_engine(model, params, dopplers=[ds], device=device)
+        e.evaluate(FORM_PLAIN_FP64)
+        fits = [e.fit(k) for k in range(ds.nframes)]
+        e.close()
+        return fits
+    return doppler
 
 
 class Server:

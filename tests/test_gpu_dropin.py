@@ -39,20 +39,30 @@ def dropin():
     return ref, L
 
 
+def _dop_synth(m):
+    return lambda d, p: cases.orc().eval_doppler(m, d, p)["fits"]
+
+
 def _inputs(name):
+    """(model, params, deldops, lightcurves, dopplers)."""
     if name == "mixed":
         m = gc.octa3_model()
         p = gc.P_DEFAULT
         dd = gc.DELDOP_CASES["small_long_orig"][1](cases.dd_synth(m), p)
+        dp = gc.DOPPLER_CASES["dop_overflow"][1](_dop_synth(m), p)
         lc = gc.LGHTCRV_CASES["kaasalainen"][1](cases.lc_synth(m), p)
-        return m, p, [dd], [lc]
+        return m, p, [dd], [lc], [dp]
     if name in gc.DELDOP_CASES:
         mk, build, p = gc.DELDOP_CASES[name]
         m = mk()
-        return m, p, [build(cases.dd_synth(m), p)], []
+        return m, p, [build(cases.dd_synth(m), p)], [], []
+    if name in gc.DOPPLER_CASES:
+        mk, build, p = gc.DOPPLER_CASES[name]
+        m = mk()
+        return m, p, [], [], [build(_dop_synth(m), p)]
     mk, build, p = gc.LGHTCRV_CASES[name]
     m = mk()
-    return m, p, [], [build(cases.lc_synth(m), p)]
+    return m, p, [], [build(cases.lc_synth(m), p)], []
 
 
 def _chi2s(L, sess, s, nfr):
@@ -62,7 +72,7 @@ def _chi2s(L, sess, s, nfr):
     return d.value, st.value, fc, fk
 
 
-def _compare_outputs(a, b, dds, lcs):
+def _compare_outputs(a, b, dds, lcs, dps):
     fa, fb = a.flags(), b.flags()
     assert fa["posbnd"] == fb["posbnd"] and fa["badradar"] == fb["badradar"]
     for k in ("posbnd_logfactor", "badradar_logfactor"):
@@ -82,15 +92,26 @@ def _compare_outputs(a, b, dds, lcs):
                 assert list(ra["res"][k]) == list(rb["res"][k]), (s, f, k)
             for k in ("dellim", "doplim"):
                 assert np.allclose(ra["res"][k], rb["res"][k], rtol=1e-12, atol=0), (s, f, k)
-    for k, ds in enumerate(lcs):
+    for k, ds in enumerate(dps):
         s = len(dds) + k
+        for f, fr in enumerate(ds.frames):
+            ra, rb = a.doppler_frame(s, f, fr), b.doppler_frame(s, f, fr)
+            peak = max(np.abs(ra["fit"]).max(), 1e-300)
+            assert np.abs(ra["fit"] - rb["fit"]).max() <= 1e-12 * peak, (s, f)
+            assert list(ra["res"]["idoplim"]) == list(rb["res"]["idoplim"]), (s, f)
+            assert np.allclose(ra["res"]["doplim"], rb["res"]["doplim"], rtol=1e-12, atol=0), (s, f)
+            # overflow spectrum terms written back for chi2_doppler (o2: bin count, m2)
+            assert ra["res"]["o2"] == rb["res"]["o2"], (s, f)
+            assert abs(ra["res"]["m2"] - rb["res"]["m2"]) <= 1e-12 * max(1e-300, abs(ra["res"]["m2"]))
+    for k, ds in enumerate(lcs):
+        s = len(dds) + len(dps) + k
         ya, yb = a.lghtcrv(s, ds), b.lghtcrv(s, ds)
         assert np.allclose(ya["y"], yb["y"], rtol=1e-12, atol=0)
         assert np.allclose(ya["fit"], yb["fit"], rtol=1e-12, atol=0)
 
 
 CASES = ["c1", "c1_outbnd", "small_short", "small_long_mod_spb3_nsinc3", "law_hagfors_cosine",
-         "kaasalainen", "lommel", "c3_short", "mixed"]
+         "kaasalainen", "lommel", "c3_short", "dop_small", "dop_overflow", "dop_overflow_far", "mixed"]
 
 
 @pytest.mark.parametrize("form", ["plain_fp64", "batched_fp64"])
@@ -98,10 +119,10 @@ CASES = ["c1", "c1_outbnd", "small_short", "small_long_mod_spb3_nsinc3", "law_ha
 def test_dropin_calc_fits_matches_reference(dropin, name, form, monkeypatch, cuda_device):
     ref, L = dropin
     monkeypatch.setenv("SHAPE_B200_FORM", form)
-    m, p, dds, lcs = _inputs(name)
-    sa = ref.session(m, p, deldops=dds, lghtcrvs=lcs)
-    sb = ref.session(m, p, deldops=dds, lghtcrvs=lcs)
-    sc = ref.session(m, p, deldops=dds, lghtcrvs=lcs)
+    m, p, dds, lcs, dps = _inputs(name)
+    sa = ref.session(m, p, deldops=dds, lghtcrvs=lcs, dopplers=dps)
+    sb = ref.session(m, p, deldops=dds, lghtcrvs=lcs, dopplers=dps)
+    sc = ref.session(m, p, deldops=dds, lghtcrvs=lcs, dopplers=dps)
     for trial, scale0 in enumerate((None, 1.03)):
         if scale0 is not None:       # a bestfit trial: engine reused, parameters pushed
             for s in (sa, sb, sc):
@@ -111,11 +132,12 @@ def test_dropin_calc_fits_matches_reference(dropin, name, form, monkeypatch, cud
         cc = L.ref_dropin_objective(sc.h)
         assert abs(cb - ca) <= 1e-10 * abs(ca), (trial, ca, cb)
         assert abs(cc - ca) <= 1e-10 * abs(ca), (trial, ca, cc)
-        _compare_outputs(sa, sb, dds, lcs)
+        _compare_outputs(sa, sb, dds, lcs, dps)
         fa, fc = sa.flags(), sc.flags()
         assert (fa["posbnd"], fa["badradar"]) == (fc["posbnd"], fc["badradar"])
-        for s in range(len(dds) + len(lcs)):
-            nfr = dds[s].nframes if s < len(dds) else 1
+        radar = list(dds) + list(dps)
+        for s in range(len(radar) + len(lcs)):
+            nfr = radar[s].nframes if s < len(radar) else 1
             da, sta, fca, fka = _chi2s(L, sa, s, nfr)
             dc, stc, fcc, fkc = _chi2s(L, sc, s, nfr)
             assert abs(dc - da) <= 1e-10 * abs(da)
