@@ -313,7 +313,8 @@ __global__ void k_chi2_partials(Chi2Args a)
 
 // Per-frame results: chi2_deldop's calibration and chi-square
 // (src/shape/chi2.c:447-460) plus the posvis / pos2deldop frame outputs.
-__device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr)
+// part: the chi-square partials (6 per item), in global or shared memory.
+__device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr, const double *part)
 {
     const FrameHost &h = a.fh[fr];
     const FrameGeom &g = a.geoms[h.view];
@@ -324,8 +325,8 @@ __device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr)
     KSum q[3] = {{ovf ? ovf[0] : 0.0, 0}, {ovf ? ovf[1] : 0.0, 0}, {0, 0}};
     for (int it = h.item0; it < h.item0 + h.nitems; it++)
         for (int k = 0; k < 3; k++) {
-            q[k].add(a.partials[(size_t)it * 6 + 2 * k]);
-            q[k].c += a.partials[(size_t)it * 6 + 2 * k + 1];
+            q[k].add(part[(size_t)it * 6 + 2 * k]);
+            q[k].c += part[(size_t)it * 6 + 2 * k + 1];
         }
     double o2 = q[0].value(), m2 = q[1].value(), om = q[2].value();
     double cal = h.cal_in;
@@ -379,11 +380,6 @@ __device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr)
     return r;
 }
 
-__global__ void k_finalize_frames(FinalizeArgs a)
-{
-    int fr = blockIdx.x * blockDim.x + threadIdx.x;
-    if (fr < a.nframes) finalize_frame(a, fr);
-}
 
 // Overflow spectra of the Doppler frames (src/shape/pos2doppler.c:451-499):
 // one block per frame sums the bins inside the frame's Doppler limits
@@ -711,9 +707,18 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
     const bool use_sm = a.smem_frames;
     double *s_chi2 = ssm, *s_plog = ssm + fa.nframes, *s_blog = ssm + 2 * (size_t)fa.nframes;
     unsigned char *s_flag = reinterpret_cast<unsigned char *>(ssm + 3 * (size_t)fa.nframes);
-    // per-frame results first (one thread per frame), then the totals
+    // the chi-square partials are copied to shared memory by the whole block
+    // first, so each frame's serial merge reads shared memory
+    const double *part = fa.partials;
+    if (use_sm && a.smem_partials) {
+        double *sp = reinterpret_cast<double *>(s_flag + ((fa.nframes + 7) & ~7));
+        for (size_t k = threadIdx.x; k < 6 * (size_t)a.nitems; k += blockDim.x) sp[k] = fa.partials[k];
+        __syncthreads();
+        part = sp;
+    }
+    // per-frame results (one thread per frame), then the totals
     for (int fr = threadIdx.x; fr < fa.nframes; fr += blockDim.x) {
-        const shape_deldop_result r = finalize_frame(fa, fr);
+        const shape_deldop_result r = finalize_frame(fa, fr, part);
         if (use_sm) {
             s_chi2[fr] = r.chi2;
             s_plog[fr] = a.fh[fr].dof * r.posbnd_logfactor;
@@ -829,11 +834,6 @@ void launch_doppler_overflow(const DopOvfArgs &a, cudaStream_t s)
     k_doppler_overflow<<<a.n, 256, 0, s>>>(a);
 }
 
-void launch_finalize_frames(const FinalizeArgs &a, cudaStream_t s)
-{
-    if (a.nframes <= 0) return;
-    k_finalize_frames<<<(a.nframes + 127) / 128, 128, 0, s>>>(a);
-}
 
 void launch_lc_photo(const LcArgs &a, int fp32, cudaStream_t s)
 {
@@ -863,9 +863,14 @@ void launch_lc_finalize(const LcFinalizeArgs &a, cudaStream_t s)
     k_lc_finalize<<<a.nsets, 256, a.smem_per_set, s>>>(a);
 }
 
-size_t summary_smem(int nframes)
+// Shared memory of the summary: per-frame terms, then (when they fit) the
+// chi-square partials; *with_partials tells which.
+size_t summary_smem(int nframes, int nitems, int *with_partials)
 {
-    size_t b = (3 * sizeof(double) + 1) * (size_t)nframes + 8;
+    size_t b = 3 * sizeof(double) * (size_t)nframes + (((size_t)nframes + 7) & ~(size_t)7);
+    size_t bp = b + 6 * sizeof(double) * (size_t)nitems;
+    *with_partials = bp <= SUMMARY_SMEM_MAX;
+    if (*with_partials) return bp;
     return b <= SUMMARY_SMEM_MAX ? b : 0;
 }
 
@@ -877,8 +882,10 @@ cudaError_t configure_summary()
 void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s)
 {
     SummaryArgs b = a;
-    const size_t sm = summary_smem(fa.nframes);
+    int wp = 0;
+    const size_t sm = summary_smem(fa.nframes, a.nitems, &wp);
     b.smem_frames = (sm > 0 && fa.nframes > 0) ? 1 : 0;
+    b.smem_partials = b.smem_frames && wp;
     k_summary<<<1, 256, b.smem_frames ? sm : 0, s>>>(fa, b);
 }
 

@@ -630,6 +630,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     sa.sets = d_setrecs; sa.fh = d_fh; sa.results = d_results;
     sa.lc_out = d_lc_out; sa.lc_dof = d_lc_dof; sa.lc_npts = d_lc_npts;
     sa.dof = dof; sa.dof_radar = dof_deldop + dof_doppler; sa.bad_objfactor = bad_objfactor;
+    sa.nitems = (int)chi2_items.size();
     // the bad-diameter factor depends only on host-side scale factors and is
     // applied by evaluate(), so captured graphs stay valid when it changes
     sa.baddiam = 0;

@@ -87,7 +87,6 @@ struct FinalizeArgs {
     const double *dop_extra;                 // per frame
     const double *ovf_out;                   // per Doppler frame: DOP_OVF_TERMS values
 };
-void launch_finalize_frames(const FinalizeArgs &a, cudaStream_t s);
 
 // Doppler overflow spectra (src/shape/pos2doppler.c:451-499): per Doppler
 // frame o2, m2, xsec, mean bin, and the badradar flag and log-factor of a
@@ -162,10 +161,12 @@ struct SummaryArgs {
     int baddiam;
     double baddiam_logfactor;
     shape_eval_summary *out;
+    int nitems;                 // chi-square partial items (6 doubles each)
     int smem_frames;            // set by launch_summary: per-frame terms staged in shared memory
+    int smem_partials;          // set by launch_summary: partials staged in shared memory too
 };
 constexpr size_t SUMMARY_SMEM_MAX = 160 * 1024;
-size_t summary_smem(int nframes);
+size_t summary_smem(int nframes, int nitems, int *with_partials);
 cudaError_t configure_summary();
 // per-frame finalize (as launch_finalize_frames) fused with the totals
 void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s);
