@@ -711,8 +711,15 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
     // first, so each frame's serial merge reads shared memory
     const double *part = fa.partials;
     if (use_sm && a.smem_partials) {
-        double *sp = reinterpret_cast<double *>(s_flag + ((fa.nframes + 7) & ~7));
-        for (size_t k = threadIdx.x; k < 6 * (size_t)a.nitems; k += blockDim.x) sp[k] = fa.partials[k];
+        // partials start at the first 16-byte boundary after the flags
+        const size_t poff = (25 * (size_t)fa.nframes + 15) & ~(size_t)15;
+        double *sp = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(ssm) + poff);
+        // 16-byte loads, eight in flight per thread before their stores
+        const double2 *src = reinterpret_cast<const double2 *>(fa.partials);
+        double2 *dst = reinterpret_cast<double2 *>(sp);
+        const int n2 = 3 * a.nitems;
+#pragma unroll 8
+        for (int k = threadIdx.x; k < n2; k += blockDim.x) dst[k] = src[k];
         __syncthreads();
         part = sp;
     }
@@ -867,8 +874,8 @@ void launch_lc_finalize(const LcFinalizeArgs &a, cudaStream_t s)
 // chi-square partials; *with_partials tells which.
 size_t summary_smem(int nframes, int nitems, int *with_partials)
 {
-    size_t b = 3 * sizeof(double) * (size_t)nframes + (((size_t)nframes + 7) & ~(size_t)7);
-    size_t bp = b + 6 * sizeof(double) * (size_t)nitems;
+    size_t b = 3 * sizeof(double) * (size_t)nframes + (size_t)nframes;   // terms and flags
+    size_t bp = ((b + 15) & ~(size_t)15) + 6 * sizeof(double) * (size_t)nitems;
     *with_partials = bp <= SUMMARY_SMEM_MAX;
     if (*with_partials) return bp;
     return b <= SUMMARY_SMEM_MAX ? b : 0;
