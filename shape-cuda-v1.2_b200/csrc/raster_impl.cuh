@@ -126,8 +126,21 @@ struct Stage {
     typename Vec4<T>::type p0, p1, p2;
     T nz;                // facet normal in view coordinates: (p2.z, p2.w, nz), views without smoothing
     T q[9];              // body-frame vertex normals of the three corners (smoothing)
-    int bb, wmask, f;
+    unsigned bb;         // pixel bbox in the tile as byte bounds (pack_bb)
+    int wmask, f;
 };
+
+// A facet's bbox in its tile (rows ri1..ri2, columns rj1..rj2) packed so one
+// byte-wise comparison tests a pixel: pixel (li, lj) packed by pack_px lies
+// inside iff every byte of its word is >= the same byte of the bbox word.
+__host__ __device__ inline unsigned pack_bb(int ri1, int ri2, int rj1, int rj2)
+{
+    return (unsigned)ri1 | ((unsigned)rj1 << 8) | ((unsigned)(15 - ri2) << 16) | ((unsigned)(15 - rj2) << 24);
+}
+__device__ inline unsigned pack_px(int li, int lj)
+{
+    return (unsigned)li | ((unsigned)lj << 8) | ((unsigned)(15 - li) << 16) | ((unsigned)(15 - lj) << 24);
+}
 
 template <typename T>
 __device__ inline typename Vec4<T>::type vec4(T x, T y, T z, T w)
@@ -239,7 +252,7 @@ __device__ bool stage_facet(const RasterArgs &a, const FrameGeom &g, int f,
     if (i2 < ti0 || i1 > ti1 || j2 < tj0 || j1 > tj1) return false;
     int ri1 = max(i1, ti0) - ti0, ri2 = min(i2, ti1) - ti0;
     int rj1 = max(j1, tj0) - tj0, rj2 = min(j2, tj1) - tj0;
-    s.bb = ri1 | (ri2 << 4) | (rj1 << 8) | (rj2 << 12);
+    s.bb = pack_bb(ri1, ri2, rj1, rj2);
     s.wmask = warp_mask_of(ri1, ri2, rj1, rj2);
     stage_fill<T>(a, g, f, s, ox, oy);
     return true;
@@ -682,10 +695,9 @@ k_raster(RasterArgs a)
         const T oa6 = (T)g.oa[6], oa7 = (T)g.oa[7], oa8 = (T)g.oa[8];
 
         // Apply posvis's update rule for one staged facet at this pixel.
+        const unsigned pxw = pack_px(li, lj);
         auto visit = [&](const Stage<T> &s) {
-            const int bb = s.bb;
-            if (li < (bb & 15) || li > ((bb >> 4) & 15) || lj < ((bb >> 8) & 15) || lj > ((bb >> 12) & 15))
-                return;
+            if (__vcmpgeu4(pxw, s.bb) != 0xffffffffu) return;   // pixel outside the facet's bbox
             const auto p0 = s.p0, p1 = s.p1;
             const T dx = x0 - p0.x, dy = x1 - p0.y;
             const T sv = (dx * p0.z - p0.w * dy) * p1.x;
@@ -751,7 +763,7 @@ k_raster(RasterArgs a)
                     const int2 e = ids[c0 + tid];
                     Stage<T> sf;
                     const int bb = e.y;
-                    sf.bb = bb;
+                    sf.bb = pack_bb(bb & 15, (bb >> 4) & 15, (bb >> 8) & 15, (bb >> 12) & 15);
                     sf.wmask = warp_mask_of(bb & 15, (bb >> 4) & 15, (bb >> 8) & 15, (bb >> 12) & 15);
                     stage_fill<T>(a, g, e.x, sf, ox, oy);
                     st[tid] = sf;
