@@ -438,7 +438,10 @@ __device__ inline T dop_resp(const FrameGeom &g, const DDC<T> &k, T dopPOS, T dd
     const int nsinc2 = g.nsinc2;
     if (nsinc2 == 1) {
         const T t = fabs((T)3.141592653589793 * ddop);
-        return (t > (T)1.0e-4) ? s2u / (t * t) : (T)1.0;
+        // FP32 form: the fast quotient (2 ulp; t*t is far from its
+        // underflow range) in place of the IEEE division
+        if constexpr (sizeof(T) == 4) return (t > 1.0e-4f) ? __fdividef(s2u, t * t) : 1.0f;
+        else return (t > 1.0e-4) ? s2u / (t * t) : 1.0;
     }
     if (nsinc2 == 2) {
         T bl = dopPOS + k.dopdiff_bl - (T)idop;
@@ -529,22 +532,25 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
 }
 
 // One footprint row of the FP32 raster straight into the frame's fit image:
-// the row's FAST_COLS-wide weights land in the 16-byte aligned groups that
-// cover them (M = misalignment of the first bin, in floats), as vector
-// reductions; group lanes outside the footprint add zero, which leaves
-// those cells unchanged.
-template <int M>
-__device__ inline void red_row_f32(float4 *base, const float (&w)[FAST_COLS], float ad, int nc)
+// the row's FAST_COLS-wide weights (zero beyond the footprint) are shifted
+// by the misalignment m of the first bin (0..3 floats) into the 16-byte
+// aligned groups that cover them and land as vector reductions; group lanes
+// outside the footprint add zero, which leaves those cells unchanged. The
+// shift is two rounds of conditional moves, so the lanes of a warp stay
+// converged whatever their misalignments.
+__device__ inline void red_row_f32(float4 *base, const float (&w)[FAST_COLS], float ad, int m, int nc)
 {
     float v[12];
 #pragma unroll
-    for (int j = 0; j < 12; j++) {
-        const int c = j - M;
-        v[j] = (c >= 0 && c < FAST_COLS && c < nc) ? ad * w[c >= 0 && c < FAST_COLS ? c : 0] : 0.0f;
-    }
-    atomicAdd(base, make_float4(v[0], v[1], v[2], v[3]));
-    if (M + nc > 4) atomicAdd(base + 1, make_float4(v[4], v[5], v[6], v[7]));
-    if (M + nc > 8) atomicAdd(base + 2, make_float4(v[8], v[9], v[10], v[11]));
+    for (int j = 0; j < 12; j++) v[j] = (j < FAST_COLS) ? w[j] : 0.0f;
+    const bool s1 = (m & 1) != 0, s2 = (m & 2) != 0;
+#pragma unroll
+    for (int j = 11; j >= 0; j--) v[j] = s1 ? (j >= 1 ? v[j - 1] : 0.0f) : v[j];
+#pragma unroll
+    for (int j = 11; j >= 0; j--) v[j] = s2 ? (j >= 2 ? v[j - 2] : 0.0f) : v[j];
+    atomicAdd(base, make_float4(ad * v[0], ad * v[1], ad * v[2], ad * v[3]));
+    if (m + nc > 4) atomicAdd(base + 1, make_float4(ad * v[4], ad * v[5], ad * v[6], ad * v[7]));
+    if (m + nc > 8) atomicAdd(base + 2, make_float4(ad * v[8], ad * v[9], ad * v[10], ad * v[11]));
 }
 
 // FP32 delay-Doppler scatter without a shared-memory accumulator: the same
@@ -579,20 +585,14 @@ __device__ inline void pixel_dd_scatter_f32_direct(const RasterArgs &a, const Fr
         pc[c] = (c < nc) ? dop_resp<float>(g, k, d.dopPOS, ddop0 - (float)c, s2u, d.idop_min + c) : 0.0f;
         if (c < nc) sdop += pc[c];
     }
-    const float amp = rl / (sdel * sdop);
+    const float amp = __fdividef(rl, sdel * sdop);
 #pragma unroll
     for (int r = 0; r < FAST_ROWS; r++) {
         if (r >= nr) break;
         const float ad = amp * dc[r];
         float *cell = fit + (long long)(d.idel_min + r - 1) * g.ndop + (d.idop_min - 1);
         const int mis = (int)((reinterpret_cast<uintptr_t>(cell) >> 2) & 3);
-        float4 *base = reinterpret_cast<float4 *>(cell - mis);
-        switch (mis) {
-        case 0: red_row_f32<0>(base, pc, ad, nc); break;
-        case 1: red_row_f32<1>(base, pc, ad, nc); break;
-        case 2: red_row_f32<2>(base, pc, ad, nc); break;
-        default: red_row_f32<3>(base, pc, ad, nc); break;
-        }
+        red_row_f32(reinterpret_cast<float4 *>(cell - mis), pc, ad, mis, nc);
     }
 }
 
