@@ -314,9 +314,10 @@ template <typename T> __device__ inline void atomic_add_fit(T *p, T v);
 template <> __device__ inline void atomic_add_fit<double>(double *p, double v) { atomicAdd(p, v); }
 template <> __device__ inline void atomic_add_fit<float>(float *p, float v) { atomicAdd(p, v); }
 
-struct PixLimits {
-    int idmin, idmax, ipmin, ipmax;
-    double dmin, dmax, pmin, pmax;
+// FP64 delay and Doppler position of a lit pixel; a tile reduces them to the
+// frame's limits (dd_bin_limits turns the extremes into bin limits).
+struct PixPos {
+    double del, dop;
 };
 
 // Delay / Doppler position and footprint of one lit POS pixel
@@ -330,7 +331,7 @@ struct PixDD {
 };
 
 template <typename T>
-__device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, const DDC<T> &k, int x, int y, T z, PixLimits &lim)
+__device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, const DDC<T> &k, int x, int y, T z, PixPos &pp)
 {
     PixDD<T> d;
     d.delPOS = z * k.delfact + k.delshift;
@@ -344,14 +345,8 @@ __device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, const DDC<T> &k, int x, i
     d.idop_max = (int)floor(d.dopPOS + dopdiff_max + half_w);
     d.codefactor = (g.codemethod == SHAPE_CODE_SHORT)
                        ? sinc2<T>((d.dopPOS - k.dopDC_vig) / k.dopfftlen) : (T)1;
-    lim.idmin = min(lim.idmin, d.idel_min);
-    lim.idmax = max(lim.idmax, d.idel_max);
-    lim.ipmin = min(lim.ipmin, d.idop_min);
-    lim.ipmax = max(lim.ipmax, d.idop_max);
-    lim.dmin = fmin(lim.dmin, (double)d.delPOS);
-    lim.dmax = fmax(lim.dmax, (double)d.delPOS);
-    lim.pmin = fmin(lim.pmin, (double)d.dopPOS);
-    lim.pmax = fmax(lim.pmax, (double)d.dopPOS);
+    pp.del = (double)d.delPOS;
+    pp.dop = (double)d.dopPOS;
     d.ok = (d.idel_min >= 1) && (d.idel_max <= g.ndel) && (d.idop_min >= 1) && (d.idop_max <= g.ndop) &&
            (d.idel_max - d.idel_min + 1 <= SHAPE_MAXBINS);
     return d;
@@ -361,7 +356,7 @@ __device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, const DDC<T> &k, int x, i
 // depth (src/shape/pos2deldop.c:318-367), so the bin range and the in-frame
 // test are the FP64 form's, and the fractional offsets the FP32 response
 // weights take are rounded from FP64 values.
-__device__ inline PixDD<float> pixel_dd_setup_x(const FrameGeom &g, int x, int y, double z, PixLimits &lim)
+__device__ inline PixDD<float> pixel_dd_setup_x(const FrameGeom &g, int x, int y, double z, PixPos &pp)
 {
     PixDD<float> d;
     const double del = z * g.delfact + g.delshift;
@@ -378,17 +373,26 @@ __device__ inline PixDD<float> pixel_dd_setup_x(const FrameGeom &g, int x, int y
     d.dfrac = (float)(dop - floor(dop));
     d.codefactor = (g.codemethod == SHAPE_CODE_SHORT) ? sinc2<float>((float)((dop - g.dopDC_vig) / g.dopfftlen))
                                                        : 1.0f;
-    lim.idmin = min(lim.idmin, d.idel_min);
-    lim.idmax = max(lim.idmax, d.idel_max);
-    lim.ipmin = min(lim.ipmin, d.idop_min);
-    lim.ipmax = max(lim.ipmax, d.idop_max);
-    lim.dmin = fmin(lim.dmin, del);
-    lim.dmax = fmax(lim.dmax, del);
-    lim.pmin = fmin(lim.pmin, dop);
-    lim.pmax = fmax(lim.pmax, dop);
+    pp.del = del;
+    pp.dop = dop;
     d.ok = (d.idel_min >= 1) && (d.idel_max <= g.ndel) && (d.idop_min >= 1) && (d.idop_max <= g.ndop) &&
            (d.idel_max - d.idel_min + 1 <= SHAPE_MAXBINS);
     return d;
+}
+
+// Bin limits (idel_min, idel_max, idop_min, idop_max) of a set of lit
+// pixels from the extremes of their FP64 delay and Doppler positions. Each
+// bound is computed per pixel above by the same expression, a non-decreasing
+// function of the position (floor/ceil of correctly rounded sums), so its
+// extreme over the set is its value at the extreme position: the same
+// integers as a min/max over the pixels' own bounds.
+__device__ inline void dd_bin_limits(const FrameGeom &g, double dmin, double dmax, double pmin, double pmax, int *l)
+{
+    const double half_w = g.sinc2width / 2.0;
+    l[0] = (int)floor(dmin - g.const1) + 1;
+    l[1] = (int)ceil(dmax + g.const1) - 1;
+    l[2] = (int)floor(pmin - g.dopdiff_max + 1 - half_w);
+    l[3] = (int)floor(pmax + g.dopdiff_max + half_w);
 }
 
 template <typename T> __device__ inline void atomic_add_any(T *p, T v) { atomicAdd(p, v); }
@@ -628,25 +632,22 @@ __device__ void pixel_dop_overflow(const RasterArgs &a, const FrameGeom &g, cons
         atomicAdd(ov + idop + g.idop0, (double)(amp * (T)1 * dop_c[min(idop - idop_min, SHAPE_MAXBINS)]));
 }
 
-__device__ inline int warp_min(int v)
+// Warp-wide extremes with the hardware warp reduction (one instruction per
+// 32-bit word); 64-bit order-preserving keys (dkey) reduce their high words
+// first, then the low words of the lanes holding the extreme high word.
+__device__ inline int warp_min(int v) { return __reduce_min_sync(0xffffffffu, v); }
+__device__ inline int warp_max(int v) { return __reduce_max_sync(0xffffffffu, v); }
+__device__ inline unsigned long long warp_kmin(unsigned long long k)
 {
-    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
+    const unsigned hi = __reduce_min_sync(0xffffffffu, (unsigned)(k >> 32));
+    const unsigned lo = __reduce_min_sync(0xffffffffu, ((unsigned)(k >> 32) == hi) ? (unsigned)k : 0xffffffffu);
+    return ((unsigned long long)hi << 32) | lo;
 }
-__device__ inline int warp_max(int v)
+__device__ inline unsigned long long warp_kmax(unsigned long long k)
 {
-    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ inline double warp_dmin(double v)
-{
-    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-__device__ inline double warp_dmax(double v)
-{
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
+    const unsigned hi = __reduce_max_sync(0xffffffffu, (unsigned)(k >> 32));
+    const unsigned lo = __reduce_max_sync(0xffffffffu, ((unsigned)(k >> 32) == hi) ? (unsigned)k : 0u);
+    return ((unsigned long long)hi << 32) | lo;
 }
 
 template <typename T>
@@ -658,8 +659,7 @@ k_raster(RasterArgs a)
     int2 *ids = raw + a.cap;
     Stage<T> *st = reinterpret_cast<Stage<T> *>(smem + (size_t)2 * a.cap * sizeof(int2));
     __shared__ int s_red[RASTER_THREADS / 32][4];
-    __shared__ double s_redd[RASTER_THREADS / 32][4];
-    __shared__ int s_redl[RASTER_THREADS / 32][4];
+    __shared__ unsigned long long s_redk[RASTER_THREADS / 32][4];
     __shared__ double s_pz[TILE_PIX];
     __shared__ T s_pc[TILE_PIX];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -848,8 +848,7 @@ k_raster(RasterArgs a)
         int cjmin = covered ? pj : INT_MAX, cjmax = covered ? pj : INT_MIN;
         cimin = warp_min(cimin); cimax = warp_max(cimax);
         cjmin = warp_min(cjmin); cjmax = warp_max(cjmax);
-        PixLimits lim = {INT_MAX, INT_MIN, INT_MAX, INT_MIN,
-                         SHAPE_HUGENUMBER, -SHAPE_HUGENUMBER, SHAPE_HUGENUMBER, -SHAPE_HUGENUMBER};
+        PixPos pp = {0.0, 0.0};
         bool lit = false;
         PixDD<T> dd;
         dd.ok = false;
@@ -874,9 +873,9 @@ k_raster(RasterArgs a)
             if (scose > (T)0) {
                 lit = true;
                 if constexpr (sizeof(T) == 4)
-                    dd = pixel_dd_setup_x(g, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], lim);
+                    dd = pixel_dd_setup_x(g, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], pp);
                 else
-                    dd = pixel_dd_setup<T>(g, kc, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], lim);
+                    dd = pixel_dd_setup<T>(g, kc, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], pp);
             }
         }
         // The footprint goes straight to the frame's fit image in HBM: FP32 as
@@ -894,17 +893,14 @@ k_raster(RasterArgs a)
         if (lane == 0) {
             s_red[wid][0] = cimin; s_red[wid][1] = cimax; s_red[wid][2] = cjmin; s_red[wid][3] = cjmax;
         }
-        unsigned anylit = __ballot_sync(0xffffffffu, lit);
         if (g.kind == VIEW_RADAR) {
-            lim.idmin = warp_min(lim.idmin); lim.idmax = warp_max(lim.idmax);
-            lim.ipmin = warp_min(lim.ipmin); lim.ipmax = warp_max(lim.ipmax);
-            lim.dmin = warp_dmin(lim.dmin); lim.dmax = warp_dmax(lim.dmax);
-            lim.pmin = warp_dmin(lim.pmin); lim.pmax = warp_dmax(lim.pmax);
+            // delay / Doppler extremes of the lit pixels as dkey keys (unlit
+            // lanes hold the neutral key)
+            const unsigned long long kd = dkey(pp.del), kp = dkey(pp.dop);
+            const unsigned long long k0 = warp_kmin(lit ? kd : ~0ull), k1 = warp_kmax(lit ? kd : 0ull);
+            const unsigned long long k2 = warp_kmin(lit ? kp : ~0ull), k3 = warp_kmax(lit ? kp : 0ull);
             if (lane == 0) {
-                s_redl[wid][0] = anylit ? lim.idmin : INT_MAX; s_redl[wid][1] = anylit ? lim.idmax : INT_MIN;
-                s_redl[wid][2] = anylit ? lim.ipmin : INT_MAX; s_redl[wid][3] = anylit ? lim.ipmax : INT_MIN;
-                s_redd[wid][0] = lim.dmin; s_redd[wid][1] = lim.dmax;
-                s_redd[wid][2] = lim.pmin; s_redd[wid][3] = lim.pmax;
+                s_redk[wid][0] = k0; s_redk[wid][1] = k1; s_redk[wid][2] = k2; s_redk[wid][3] = k3;
             }
         }
         __syncthreads();
@@ -920,19 +916,18 @@ k_raster(RasterArgs a)
                 atomicMin(&S.cov_j[0], v2); atomicMax(&S.cov_j[1], v3);
             }
             if (g.kind == VIEW_RADAR) {
-                int l0 = INT_MAX, l1 = INT_MIN, l2 = INT_MAX, l3 = INT_MIN;
-                double d0 = SHAPE_HUGENUMBER, d1 = -SHAPE_HUGENUMBER, d2 = SHAPE_HUGENUMBER, d3 = -SHAPE_HUGENUMBER;
+                unsigned long long k0 = ~0ull, k1 = 0ull, k2 = ~0ull, k3 = 0ull;
                 for (int ww = 0; ww < RASTER_THREADS / 32; ww++) {
-                    l0 = min(l0, s_redl[ww][0]); l1 = max(l1, s_redl[ww][1]);
-                    l2 = min(l2, s_redl[ww][2]); l3 = max(l3, s_redl[ww][3]);
-                    d0 = fmin(d0, s_redd[ww][0]); d1 = fmax(d1, s_redd[ww][1]);
-                    d2 = fmin(d2, s_redd[ww][2]); d3 = fmax(d3, s_redd[ww][3]);
+                    k0 = min(k0, s_redk[ww][0]); k1 = max(k1, s_redk[ww][1]);
+                    k2 = min(k2, s_redk[ww][2]); k3 = max(k3, s_redk[ww][3]);
                 }
-                if (l0 != INT_MAX) {
-                    atomicMin(&S.idellim[0], l0); atomicMax(&S.idellim[1], l1);
-                    atomicMin(&S.idoplim[0], l2); atomicMax(&S.idoplim[1], l3);
-                    atomicMin(&S.dellim[0], dkey(d0)); atomicMax(&S.dellim[1], dkey(d1));
-                    atomicMin(&S.doplim[0], dkey(d2)); atomicMax(&S.doplim[1], dkey(d3));
+                if (k0 != ~0ull) {        // a lit pixel in the tile
+                    int l[4];
+                    dd_bin_limits(g, dkey_inv(k0), dkey_inv(k1), dkey_inv(k2), dkey_inv(k3), l);
+                    atomicMin(&S.idellim[0], l[0]); atomicMax(&S.idellim[1], l[1]);
+                    atomicMin(&S.idoplim[0], l[2]); atomicMax(&S.idoplim[1], l[3]);
+                    atomicMin(&S.dellim[0], k0); atomicMax(&S.dellim[1], k1);
+                    atomicMin(&S.doplim[0], k2); atomicMax(&S.doplim[1], k3);
                     S.any_lit = 1;
                 }
             }
