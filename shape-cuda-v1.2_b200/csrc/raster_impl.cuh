@@ -119,8 +119,12 @@ template <typename T> __device__ T radlaw_dev(const RadarLawDev &L, T c)
 //
 // The terms the per-pixel test reads are packed in three 4-vectors, so a
 // visit loads them with three vector loads (every lane of a warp reads the
-// same staged facet: broadcasts, no bank conflicts):
-//   p0 = (v00, v01, A, B), p1 = (den, C, D, v02), p2 = (E, F, nx, ny).
+// same staged facet: broadcasts, no bank conflicts). FP64 form, posvis's
+// own terms: p0 = (v00, v01, A, B), p1 = (den, C, D, v02),
+// p2 = (E, F, nx, ny). FP32 form, s, t and the depth above the first corner
+// as affine functions of the tile-relative pixel centre (x, y):
+// s = a0 + a1 x + a2 y, t = b0 + b1 x + b2 y, zr = c0 + c1 x + c2 y, with
+// p0 = (a0, a1, a2, b0), p1 = (b1, b2, c0, c1), p2 = (c2, v02, nx, ny).
 template <typename T>
 struct Stage {
     typename Vec4<T>::type p0, p1, p2;
@@ -187,11 +191,18 @@ __device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage
         s.p1 = vec4<T>(den, C, D, p0.z);
         (void)ox; (void)oy;
     } else {
+        // the affine coefficients in FP64 from posvis's terms, rounded once
         const double A = p2.y - p1.y, B = p2.x - p1.x, C = p1.x - p0.x, D = p1.y - p0.y;
-        E = (T)(p1.z - p0.z);
-        F = (T)(p2.z - p1.z);
-        s.p0 = vec4<T>((T)(p0.x - ox), (T)(p0.y - oy), (T)A, (T)B);
-        s.p1 = vec4<T>((T)(1.0 / (C * A - B * D)), (T)C, (T)D, (T)p0.z);
+        const double Ez = p1.z - p0.z, Fz = p2.z - p1.z;
+        const double den = 1.0 / (C * A - B * D);
+        const double V0 = p0.x - ox, V1 = p0.y - oy;
+        const double a1 = den * A, a2 = -den * B, a0 = den * (B * V1 - A * V0);
+        const double b1 = -den * D, b2 = den * C, b0 = den * (D * V0 - C * V1);
+        const double c0 = Ez * a0 + Fz * b0, c1 = Ez * a1 + Fz * b1, c2 = Ez * a2 + Fz * b2;
+        s.p0 = vec4<T>((T)a0, (T)a1, (T)a2, (T)b0);
+        s.p1 = vec4<T>((T)b1, (T)b2, (T)c0, (T)c1);
+        E = (T)c2;       // p2 = (c2, v02, nx, ny)
+        F = (T)p0.z;
     }
     s.f = f;
     if (g.smooth) {
@@ -660,6 +671,9 @@ k_raster(RasterArgs a)
     Stage<T> *st = reinterpret_cast<Stage<T> *>(smem + (size_t)2 * a.cap * sizeof(int2));
     __shared__ int s_red[RASTER_THREADS / 32][4];
     __shared__ unsigned long long s_redk[RASTER_THREADS / 32][4];
+    __shared__ int s_scan[RASTER_THREADS / 32];
+    // facet bitmap words (and as many prefix counts) the staging buffer holds
+    constexpr int BITMAP_WORDS = (int)(STAGE_FACETS * sizeof(Stage<T>) / (2 * sizeof(unsigned)));
     __shared__ double s_pz[TILE_PIX];
     __shared__ T s_pc[TILE_PIX];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -697,22 +711,32 @@ k_raster(RasterArgs a)
         // Apply posvis's update rule for one staged facet at this pixel.
         const unsigned pxw = pack_px(li, lj);
         auto visit = [&](const Stage<T> &s) {
-            if (__vcmpgeu4(pxw, s.bb) != 0xffffffffu) return;   // pixel outside the facet's bbox
-            const auto p0 = s.p0, p1 = s.p1;
-            const T dx = x0 - p0.x, dy = x1 - p0.y;
-            const T sv = (dx * p0.z - p0.w * dy) * p1.x;
-            if (!((sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL))) return;
-            const T tv = (p1.y * dy - dx * p1.z) * p1.x;
-            if (!((tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL))) return;
-            const auto p2 = s.p2;
-            T z, zr = 0;
+            T sv, tv, z, zr = 0;
             if constexpr (sizeof(T) == 8) {
+                if (__vcmpgeu4(pxw, s.bb) != 0xffffffffu) return;   // pixel outside the facet's bbox
+                const auto p0 = s.p0, p1 = s.p1;
+                const T dx = x0 - p0.x, dy = x1 - p0.y;
+                sv = (dx * p0.z - p0.w * dy) * p1.x;
+                if (!((sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL))) return;
+                tv = (p1.y * dy - dx * p1.z) * p1.x;
+                if (!((tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL))) return;
+                const auto p2 = s.p2;
                 z = p1.w + sv * p2.x + tv * p2.y;
+                if (!((z > zz) || (fac < 0))) return;
             } else {
-                zr = sv * p2.x + tv * p2.y;
-                z = p1.w + zr;
+                // the whole test without early exits (a warp runs every step
+                // for some lane anyway), then one branch for a win
+                const auto p0 = s.p0, p1 = s.p1, p2 = s.p2;
+                const bool inb = __vcmpgeu4(pxw, s.bb) == 0xffffffffu;   // pixel in the facet's bbox
+                sv = fmaf(p0.y, x0, fmaf(p0.z, x1, p0.x));
+                tv = fmaf(p1.x, x0, fmaf(p1.y, x1, p0.w));
+                zr = fmaf(p1.w, x0, fmaf(p2.x, x1, p1.z));
+                z = p2.y + zr;
+                const bool in = inb && (sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL) &&
+                                (tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL);
+                if (!(in && ((z > zz) || (fac < 0)))) return;
             }
-            if (!((z > zz) || (fac < 0))) return;
+            const auto p2 = s.p2;
             zz = z;
             zrel = zr;
             fac = s.f;
@@ -748,13 +772,59 @@ k_raster(RasterArgs a)
 
         if (count > 0 && count <= a.cap) {
             const int2 *bin = a.bin_ids + (size_t)(g.tile_base + tile) * a.cap;
-            for (int k = tid; k < count; k += RASTER_THREADS) raw[k] = bin[k];
-            __syncthreads();
-            for (int k = tid; k < count; k += RASTER_THREADS) {
-                int2 v = raw[k];
-                int r = 0;
-                for (int m = 0; m < count; m++) r += (raw[m].x < v.x);
-                ids[r] = v;
+            // The bin in facet-index order (posvis walks facets in index
+            // order). A bin's facets are distinct, so a facet's rank is the
+            // number of set bits below it in a bitmap of the bin's facets:
+            // O(nf/32 + count) per tile. The bitmap and its per-word prefix
+            // counts live in the staging buffer, idle until staging starts;
+            // models too large for it rank by comparisons.
+            const int nw = (a.nf + 31) >> 5;
+            if (nw <= BITMAP_WORDS) {
+                unsigned *W = reinterpret_cast<unsigned *>(st);
+                int *P = reinterpret_cast<int *>(W + BITMAP_WORDS);
+                for (int w = tid; w < nw; w += RASTER_THREADS) W[w] = 0u;
+                __syncthreads();
+                for (int k = tid; k < count; k += RASTER_THREADS) {
+                    const int2 v = bin[k];
+                    raw[k] = v;
+                    atomicOr(&W[v.x >> 5], 1u << (v.x & 31));
+                }
+                __syncthreads();
+                // exclusive prefix of the words' popcounts: a contiguous run
+                // of words per thread, then a block scan of the run totals
+                const int wpt = (nw + RASTER_THREADS - 1) / RASTER_THREADS;
+                const int w0 = min(tid * wpt, nw), w1 = min(w0 + wpt, nw);
+                int run = 0;
+                for (int w = w0; w < w1; w++) run += __popc(W[w]);
+                int inc = run;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += t;
+                }
+                if (lane == 31) s_scan[wid] = inc;
+                __syncthreads();
+                int before = inc - run;
+                for (int ww = 0; ww < wid; ww++) before += s_scan[ww];
+                for (int w = w0; w < w1; w++) {
+                    P[w] = before;
+                    before += __popc(W[w]);
+                }
+                __syncthreads();
+                for (int k = tid; k < count; k += RASTER_THREADS) {
+                    const int2 v = raw[k];
+                    const int w = v.x >> 5;
+                    ids[P[w] + __popc(W[w] & ((1u << (v.x & 31)) - 1u))] = v;
+                }
+            } else {
+                for (int k = tid; k < count; k += RASTER_THREADS) raw[k] = bin[k];
+                __syncthreads();
+                for (int k = tid; k < count; k += RASTER_THREADS) {
+                    int2 v = raw[k];
+                    int r = 0;
+                    for (int m = 0; m < count; m++) r += (raw[m].x < v.x);
+                    ids[r] = v;
+                }
             }
             __syncthreads();
             for (int c0 = 0; c0 < count; c0 += STAGE_FACETS) {
