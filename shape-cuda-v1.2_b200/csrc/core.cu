@@ -256,65 +256,23 @@ __device__ inline KSum shfl_ksum(KSum a, int off)
 // o2 = sum obs^2/var, m2 = sum fit^2/var, om = sum fit*obs/var, each
 // product in the reference's order, accumulated with compensation.
 template <typename T>
+__device__ void chi2_item_partials(const Chi2Args &a, const Chi2Item &item, double (*red)[6], double *part);
+
+template <typename T>
 __global__ void k_chi2_partials(Chi2Args a)
 {
     __shared__ double red[CHI2_THREADS / 32][6];
     for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
-        Chi2Item item = a.items[it];
-        const FrameGeom &g = a.geoms[a.frame_view[item.frame]];
-        const long long base = g.fit_base + item.start;
-        const T *fit = static_cast<const T *>(a.fit) + base;
-        const double *obs = a.obs + base, *oov = a.oov + base;
-        KSum o2 = {0, 0}, m2 = {0, 0}, om = {0, 0};
-        // all of a thread's loads are issued before its (serial, in-order)
-        // compensated adds, so their latencies overlap
-        double ob[CHI2_ITEMS], wv[CHI2_ITEMS], ft[CHI2_ITEMS];
-#pragma unroll
-        for (int j = 0; j < CHI2_ITEMS; j++) {
-            const int k = threadIdx.x + j * CHI2_THREADS;
-            const bool in = k < item.count;
-            ob[j] = in ? obs[k] : 0.0;
-            wv[j] = in ? oov[k] : 0.0;
-            ft[j] = in ? (double)fit[k] : 0.0;
-        }
-#pragma unroll
-        for (int j = 0; j < CHI2_ITEMS; j++) {
-            if (threadIdx.x + j * CHI2_THREADS >= item.count) break;
-            o2.add(ob[j] * ob[j] * wv[j]);
-            m2.add(ft[j] * ft[j] * wv[j]);
-            om.add(ft[j] * ob[j] * wv[j]);
-        }
-        for (int off = 16; off > 0; off >>= 1) {
-            o2.merge(shfl_ksum(o2, off));
-            m2.merge(shfl_ksum(m2, off));
-            om.merge(shfl_ksum(om, off));
-        }
-        int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        if (l == 0) {
-            red[w][0] = o2.s; red[w][1] = o2.c; red[w][2] = m2.s;
-            red[w][3] = m2.c; red[w][4] = om.s; red[w][5] = om.c;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            KSum r[3] = {{0, 0}, {0, 0}, {0, 0}};
-            for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++)
-                for (int q = 0; q < 3; q++) {
-                    r[q].add(red[ww][2 * q]);
-                    r[q].c += red[ww][2 * q + 1];
-                }
-            for (int q = 0; q < 3; q++) {
-                a.partials[(size_t)it * 6 + 2 * q] = r[q].s;
-                a.partials[(size_t)it * 6 + 2 * q + 1] = r[q].c;
-            }
-        }
+        chi2_item_partials<T>(a, a.items[it], red, a.partials + (size_t)it * 6);
         __syncthreads();
     }
 }
 
 // Per-frame results: chi2_deldop's calibration and chi-square
 // (src/shape/chi2.c:447-460) plus the posvis / pos2deldop frame outputs.
-// part: the chi-square partials (6 per item), in global or shared memory.
-__device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr, const double *part)
+// part: the chi-square partials (6 per item), in global or shared memory;
+// part0: the index of the frame's first item in part.
+__device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr, const double *part, int part0)
 {
     const FrameHost &h = a.fh[fr];
     const FrameGeom &g = a.geoms[h.view];
@@ -323,10 +281,10 @@ __device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr, con
     // (src/shape/chi2.c:745-747)
     const double *ovf = (h.dop_index >= 0) ? a.ovf_out + (size_t)h.dop_index * DOP_OVF_TERMS : nullptr;
     KSum q[3] = {{ovf ? ovf[0] : 0.0, 0}, {ovf ? ovf[1] : 0.0, 0}, {0, 0}};
-    for (int it = h.item0; it < h.item0 + h.nitems; it++)
+    for (int it = 0; it < h.nitems; it++)
         for (int k = 0; k < 3; k++) {
-            q[k].add(part[(size_t)it * 6 + 2 * k]);
-            q[k].c += part[(size_t)it * 6 + 2 * k + 1];
+            q[k].add(part[(size_t)(part0 + it) * 6 + 2 * k]);
+            q[k].c += part[(size_t)(part0 + it) * 6 + 2 * k + 1];
         }
     double o2 = q[0].value(), m2 = q[1].value(), om = q[2].value();
     double cal = h.cal_in;
@@ -701,6 +659,9 @@ __global__ void k_lc_finalize(LcFinalizeArgs a)
 // a.smem_frames set, each frame's thread leaves its chi2 and dof-weighted
 // log-factor terms in shared memory, so the serial pass reads shared memory
 // instead of waiting on one global load per frame.
+template <typename Term>
+__device__ void summary_totals(const SummaryArgs &a, Term term);
+
 __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
 {
     extern __shared__ double ssm[];
@@ -725,7 +686,7 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
     }
     // per-frame results (one thread per frame), then the totals
     for (int fr = threadIdx.x; fr < fa.nframes; fr += blockDim.x) {
-        const shape_deldop_result r = finalize_frame(fa, fr, part);
+        const shape_deldop_result r = finalize_frame(fa, fr, part, fa.fh[fr].item0);
         if (use_sm) {
             s_chi2[fr] = r.chi2;
             s_plog[fr] = a.fh[fr].dof * r.posbnd_logfactor;
@@ -735,6 +696,27 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
     }
     __syncthreads();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (use_sm)
+        summary_totals(a, [&](int f, double &c, double &pl, double &bl, int &fl) {
+            c = s_chi2[f]; pl = s_plog[f]; bl = s_blog[f]; fl = s_flag[f];
+        });
+    else
+        summary_totals(a, [&](int f, double &c, double &pl, double &bl, int &fl) {
+            const shape_deldop_result &r = a.results[f];
+            c = r.chi2;
+            pl = a.fh[f].dof * r.posbnd_logfactor;
+            bl = a.fh[f].dof * r.badradar_logfactor / 1;
+            fl = (r.outbnd ? 1 : 0) | (r.badradar ? 2 : 0);
+        });
+}
+
+// The totals: serial sums over the sets in dataset order (the reference's
+// order, src/shape/chi2.c:270-300 and calc_fits.c:407-409), the flags and
+// the objective. term(f, chi2, dof*posbnd_logfactor, dof*badradar_logfactor,
+// flags) gives radar frame f's terms (flags: 1 outbnd, 2 badradar).
+template <typename Term>
+__device__ void summary_totals(const SummaryArgs &a, Term term)
+{
     double chi2 = 0.0, chi2_dd = 0.0, chi2_lc = 0.0, plog = 0.0, blog = 0.0;
     int posbnd = 0, badradar = 0;
     for (int s = 0; s < a.nsets; s++) {
@@ -742,16 +724,12 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
         double cs = 0.0;
         if (R.type == 0) {
             for (int f = R.first; f < R.first + R.count; f++) {
-                if (use_sm) {
-                    cs += s_chi2[f];
-                    if (s_flag[f] & 1) { posbnd = 1; plog += s_plog[f]; }
-                    if (s_flag[f] & 2) { badradar = 1; blog += s_blog[f]; }
-                    continue;
-                }
-                const shape_deldop_result &r = a.results[f];
-                cs += r.chi2;
-                if (r.outbnd) { posbnd = 1; plog += a.fh[f].dof * r.posbnd_logfactor; }
-                if (r.badradar) { badradar = 1; blog += a.fh[f].dof * r.badradar_logfactor / 1; }
+                double c, pl, bl;
+                int fl;
+                term(f, c, pl, bl, fl);
+                cs += c;
+                if (fl & 1) { posbnd = 1; plog += pl; }
+                if (fl & 2) { badradar = 1; blog += bl; }
             }
             chi2_dd += cs;
         } else {
@@ -778,6 +756,119 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
     if (badradar) err *= a.bad_objfactor * exp(out.badradar_logfactor);
     out.objective = err;
     *a.out = out;
+}
+
+// One item's chi-square partial sums (the body of k_chi2_partials), left by
+// thread 0 in part[0..5].
+template <typename T>
+__device__ void chi2_item_partials(const Chi2Args &a, const Chi2Item &item, double (*red)[6], double *part)
+{
+    const FrameGeom &g = a.geoms[a.frame_view[item.frame]];
+    const long long base = g.fit_base + item.start;
+    const T *fit = static_cast<const T *>(a.fit) + base;
+    const double *obs = a.obs + base, *oov = a.oov + base;
+    KSum o2 = {0, 0}, m2 = {0, 0}, om = {0, 0};
+    double ob[CHI2_ITEMS], wv[CHI2_ITEMS], ft[CHI2_ITEMS];
+#pragma unroll
+    for (int j = 0; j < CHI2_ITEMS; j++) {
+        const int k = threadIdx.x + j * CHI2_THREADS;
+        const bool in = k < item.count;
+        ob[j] = in ? obs[k] : 0.0;
+        wv[j] = in ? oov[k] : 0.0;
+        ft[j] = in ? (double)fit[k] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < CHI2_ITEMS; j++) {
+        if (threadIdx.x + j * CHI2_THREADS >= item.count) break;
+        o2.add(ob[j] * ob[j] * wv[j]);
+        m2.add(ft[j] * ft[j] * wv[j]);
+        om.add(ft[j] * ob[j] * wv[j]);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        o2.merge(shfl_ksum(o2, off));
+        m2.merge(shfl_ksum(m2, off));
+        om.merge(shfl_ksum(om, off));
+    }
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        red[w][0] = o2.s; red[w][1] = o2.c; red[w][2] = m2.s;
+        red[w][3] = m2.c; red[w][4] = om.s; red[w][5] = om.c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        KSum r[3] = {{0, 0}, {0, 0}, {0, 0}};
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++)
+            for (int q = 0; q < 3; q++) {
+                r[q].add(red[ww][2 * q]);
+                r[q].c += red[ww][2 * q + 1];
+            }
+        for (int q = 0; q < 3; q++) {
+            part[2 * q] = r[q].s;
+            part[2 * q + 1] = r[q].c;
+        }
+    }
+}
+
+// Chi-square partials, per-frame results and totals in one launch. Each
+// block computes chunks (items) as k_chi2_partials does; the block that
+// completes a frame's last item (a per-frame counter) finalizes that frame
+// from its items' partials in item order, and the block that finalizes the
+// last frame computes the totals in dataset order. The sums and their order
+// are those of k_chi2_partials + k_summary, so the results are the same.
+// Values another block wrote in this launch are read through L2 (__ldcg)
+// after a fence. counters: [nframes] per-frame finished items, then the
+// finished frames; zero before the launch.
+template <typename T>
+__global__ void __launch_bounds__(CHI2_THREADS) k_chi2_summary(Chi2Args ca, FinalizeArgs fa, SummaryArgs sa,
+                                                               int *counters)
+{
+    __shared__ double red[CHI2_THREADS / 32][6];
+    __shared__ __align__(16) unsigned char stage[FUSED_STAGE_BYTES];
+    __shared__ int s_last;
+    double *s_part = reinterpret_cast<double *>(stage);
+    for (int it = blockIdx.x; it < ca.nitems; it += gridDim.x) {
+        const Chi2Item item = ca.items[it];
+        chi2_item_partials<T>(ca, item, red, ca.partials + (size_t)it * 6);
+        const int fr = item.frame;
+        const FrameHost &h = fa.fh[fr];
+        if (threadIdx.x == 0) {
+            __threadfence();                                  // partials before the count
+            s_last = (atomicAdd(&counters[fr], 1) == h.nitems - 1);
+        }
+        __syncthreads();
+        if (s_last) {                                         // block-uniform
+            __threadfence();
+            // the frame's partials to shared memory, then its results
+            for (int k = threadIdx.x; k < 6 * h.nitems; k += blockDim.x)
+                s_part[k] = __ldcg(ca.partials + (size_t)h.item0 * 6 + k);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                finalize_frame(fa, fr, s_part, 0);
+                __threadfence();                              // results before the count
+                s_last = (atomicAdd(&counters[fa.nframes], 1) == fa.nframes - 1);
+            }
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                double *s_chi2 = reinterpret_cast<double *>(stage);
+                double *s_plog = s_chi2 + fa.nframes, *s_blog = s_plog + fa.nframes;
+                unsigned char *s_flag = reinterpret_cast<unsigned char *>(s_blog + fa.nframes);
+                for (int f = threadIdx.x; f < fa.nframes; f += blockDim.x) {
+                    const shape_deldop_result *r = fa.results + f;
+                    s_chi2[f] = __ldcg(&r->chi2);
+                    s_plog[f] = fa.fh[f].dof * __ldcg(&r->posbnd_logfactor);
+                    s_blog[f] = fa.fh[f].dof * __ldcg(&r->badradar_logfactor) / 1;
+                    s_flag[f] = (__ldcg(&r->outbnd) ? 1 : 0) | (__ldcg(&r->badradar) ? 2 : 0);
+                }
+                __syncthreads();
+                if (threadIdx.x == 0)
+                    summary_totals(sa, [&](int f, double &c, double &pl, double &bl, int &fl) {
+                        c = s_chi2[f]; pl = s_plog[f]; bl = s_blog[f]; fl = s_flag[f];
+                    });
+            }
+        }
+        __syncthreads();
+    }
 }
 
 }  // namespace
@@ -884,6 +975,21 @@ size_t summary_smem(int nframes, int nitems, int *with_partials)
 cudaError_t configure_summary()
 {
     return cudaFuncSetAttribute(k_summary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SUMMARY_SMEM_MAX);
+}
+
+bool chi2_summary_fits(int nframes, int max_frame_items)
+{
+    return nframes > 0 && (size_t)nframes * 25 <= FUSED_STAGE_BYTES &&
+           (size_t)max_frame_items * 6 * sizeof(double) <= FUSED_STAGE_BYTES;
+}
+
+void launch_chi2_summary(const Chi2Args &ca, const FinalizeArgs &fa, const SummaryArgs &sa, int *counters,
+                         int fp32, cudaStream_t s)
+{
+    int blocks = ca.nitems < 8 * 148 ? ca.nitems : 8 * 148;
+    if (blocks <= 0) return;
+    if (fp32) k_chi2_summary<float><<<blocks, CHI2_THREADS, 0, s>>>(ca, fa, sa, counters);
+    else k_chi2_summary<double><<<blocks, CHI2_THREADS, 0, s>>>(ca, fa, sa, counters);
 }
 
 void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s)

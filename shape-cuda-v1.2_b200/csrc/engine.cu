@@ -213,6 +213,15 @@ int EngineImpl::finalize()
             add_view(g, F.pos_n, F.km_per_pixel);
         }
     }
+    {
+        // the fused chi-square / summary kernel needs every frame to own an
+        // item and its staging buffer to hold a frame's partials and the
+        // per-frame terms
+        int max_items = 0;
+        bool every = true;
+        for (const FrameHost &h : fh) { max_items = std::max(max_items, h.nitems); every = every && h.nitems > 0; }
+        fused_chi2 = every && !chi2_items.empty() && chi2_summary_fits((int)fh.size(), max_items);
+    }
     // lightcurve points: two views each (src/shape/calc_fits.c:1634-1716)
     const int LC_CHUNK = 4096;
     for (size_t s = 0; s < lc.size(); s++) {
@@ -312,6 +321,7 @@ int EngineImpl::finalize()
     AL(d_seen, (size_t)nf);
     AL(d_chi2_items, chi2_items.size()); AL(d_frame_view, frame_view.size());
     AL(d_partials, chi2_items.size() * 6);
+    AL(d_chi2_counters, fh.size() + 1);
     AL(d_fh, fh.size()); AL(d_results, fh.size());
     AL(d_set_delpp, set_delpp.size()); AL(d_set_doppp, set_doppp.size()); AL(d_dop_extra, dop_extra.size());
     AL(d_lcpts, lcpts.size()); AL(d_lc_items, lc_items.size()); AL(d_pt_items, pt_items.size());
@@ -497,6 +507,8 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     CK(cudaMemsetAsync(d_seen, 0, nf, sr));
     if (!dop_frames.empty())
         CK(cudaMemsetAsync(d_ovf, 0, sizeof(double) * dop_frames.size() * DOP_MAXOVERFLOW, sr));
+    const bool fused = fused_chi2 && form != SHAPE_FORM_PLAIN_FP64;
+    if (fused) CK(cudaMemsetAsync(d_chi2_counters, 0, sizeof(int) * (fh.size() + 1), sr));
     if (fork) {
         CK(cudaEventRecord(evf[2], stream2));        // reset and clears done
         CK(cudaStreamWaitEvent(stream2, evf[1], 0));  // facet normals exist
@@ -584,11 +596,10 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         ra.nwork = (int)work.size();
         if (f32) launch_raster_f32(ra, s); else launch_raster_f64(ra, s);
         mark(4);
-        if (!chi2_items.empty()) {
-            ca.items = d_chi2_items;
-            ca.nitems = (int)chi2_items.size();
-            launch_chi2_partials(ca, f32 ? 1 : 0, s);
-        }
+        ca.items = d_chi2_items;
+        ca.nitems = (int)chi2_items.size();
+        // fused: the chi-square partials run with the summary, last
+        if (!chi2_items.empty() && !fused) launch_chi2_partials(ca, f32 ? 1 : 0, s);
         mark(5);
         if (!lc_items.empty()) {
             la.items = d_lc_items;
@@ -636,7 +647,8 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     sa.baddiam = 0;
     sa.baddiam_logfactor = 0.0;
     sa.out = d_summary;
-    launch_summary(fa, sa, s);
+    if (fused) launch_chi2_summary(ca, fa, sa, d_chi2_counters, f32 ? 1 : 0, s);
+    else launch_summary(fa, sa, s);
     mark(7);
     CK(cudaGetLastError());
     return SHAPE_OK;
@@ -652,12 +664,12 @@ int EngineImpl::kernels_per_eval(int form) const
             n += 3 + (geoms[v].kind == VIEW_RADAR || geoms[v].kind == VIEW_LC_SUN ? 1 : 0);
     } else {
         n += 3;                          // transform, bin, raster
-        n += chi2_items.empty() ? 0 : 1;
+        n += (chi2_items.empty() || fused_chi2) ? 0 : 1;   // fused: counted with the summary
         n += lc_items.empty() ? 0 : 1;
     }
     n += lcdev.empty() ? 0 : 1;          // lightcurve finalize
     n += dop_frames.empty() ? 0 : 1;     // Doppler overflow spectra
-    return n + 1;                        // finalize + summary
+    return n + 1;                        // finalize + summary (with the chi-square partials when fused)
 }
 
 int EngineImpl::evaluate(int form, shape_eval_summary *out)

@@ -131,6 +131,8 @@ struct EngineImpl {
     Chi2Item *d_chi2_items = nullptr;
     int *d_frame_view = nullptr;
     double *d_partials = nullptr;
+    int *d_chi2_counters = nullptr;   // fused chi-square / summary: per-frame items done, frames done
+    bool fused_chi2 = false;          // batched forms run k_chi2_summary
     FrameHost *d_fh = nullptr;
     shape_deldop_result *d_results = nullptr;
     double *d_set_delpp = nullptr, *d_set_doppp = nullptr, *d_dop_extra = nullptr;

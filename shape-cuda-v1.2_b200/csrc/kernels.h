@@ -171,6 +171,15 @@ cudaError_t configure_summary();
 // per-frame finalize (as launch_finalize_frames) fused with the totals
 void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s);
 
+// Chi-square partials + per-frame finalize + totals in one launch (the
+// batched forms). Its shared staging holds one frame's partials and then
+// every frame's terms; chi2_summary_fits says whether a dataset fits.
+constexpr size_t FUSED_STAGE_BYTES = 24 * 1024;
+bool chi2_summary_fits(int nframes, int max_frame_items);
+// counters: nframes + 1 ints, zero before the launch
+void launch_chi2_summary(const Chi2Args &ca, const FinalizeArgs &fa, const SummaryArgs &sa, int *counters,
+                         int fp32, cudaStream_t s);
+
 // raster_f64.cu / raster_f32.cu
 void launch_raster_f64(const RasterArgs &a, cudaStream_t s);
 void launch_raster_f32(const RasterArgs &a, cudaStream_t s);
