@@ -24,16 +24,28 @@
 #include "kernels.h"
 
 // Resident CTAs per SM the register allocation must allow (FP32 / FP64).
-// The FP32 raster is latency-bound: 6 CTAs (40 registers, some spilled to
-// L1) measured faster than 5 (48) and 4 (64).
+// Both rasters are latency-bound: FP32 at 8 CTAs (32 registers, spills to
+// L1) measured faster than 6 (40), 5 (48) and 4 (64); FP64 at 4 CTAs (64
+// registers) faster than 3 (80).
 #ifndef RASTER_MIN_BLOCKS
-#define RASTER_MIN_BLOCKS 6
+#define RASTER_MIN_BLOCKS 8
 #endif
 #ifndef RASTER_MIN_BLOCKS_F64
-#define RASTER_MIN_BLOCKS_F64 3
+#define RASTER_MIN_BLOCKS_F64 4
 #endif
 
 namespace shape {
+
+// Largest facet bitmap (32-bit words) the bin rank uses: models up to 262144
+// facets; larger ones rank by comparisons.
+constexpr int BITMAP_MAX_WORDS = 8192;
+
+// Bytes of the ranked bin at the start of a raster CTA's shared memory,
+// rounded up so the staging area after it starts on a 32-byte boundary.
+__host__ __device__ inline size_t raster_ids_bytes(int cap)
+{
+    return ((size_t)cap * 8 + 31) & ~(size_t)31;
+}
 
 template <typename T> struct Vec4;
 template <> struct Vec4<double> { using type = double4; };
@@ -667,15 +679,15 @@ template <typename T>
 __global__ void __launch_bounds__(RASTER_THREADS, sizeof(T) == 8 ? RASTER_MIN_BLOCKS_F64 : RASTER_MIN_BLOCKS)
 k_raster(RasterArgs a)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
-    int2 *raw = reinterpret_cast<int2 *>(smem);
-    int2 *ids = raw + a.cap;
-    Stage<T> *st = reinterpret_cast<Stage<T> *>(smem + (size_t)2 * a.cap * sizeof(int2));
+    extern __shared__ __align__(32) unsigned char smem[];
+    // dynamic shared memory: the ranked bin, then the staging area, which
+    // holds the facet bitmap, its prefix counts and the raw bin while the bin
+    // is ranked (raster_smem_bytes sizes it for both uses)
+    int2 *ids = reinterpret_cast<int2 *>(smem);
+    Stage<T> *st = reinterpret_cast<Stage<T> *>(smem + raster_ids_bytes(a.cap));
     __shared__ int s_red[RASTER_THREADS / 32][4];
     __shared__ unsigned long long s_redk[RASTER_THREADS / 32][4];
     __shared__ int s_scan[RASTER_THREADS / 32];
-    // facet bitmap words (and as many prefix counts) the staging buffer holds
-    constexpr int BITMAP_WORDS = (int)(STAGE_FACETS * sizeof(Stage<T>) / (2 * sizeof(unsigned)));
     __shared__ double s_pz[TILE_PIX];
     __shared__ T s_pc[TILE_PIX];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -777,13 +789,15 @@ k_raster(RasterArgs a)
             // The bin in facet-index order (posvis walks facets in index
             // order). A bin's facets are distinct, so a facet's rank is the
             // number of set bits below it in a bitmap of the bin's facets:
-            // O(nf/32 + count) per tile. The bitmap and its per-word prefix
-            // counts live in the staging buffer, idle until staging starts;
-            // models too large for it rank by comparisons.
+            // O(nf/32 + count) per tile. The bitmap, its per-word prefix
+            // counts and the raw bin live in the staging area, idle until
+            // staging starts; models too large for a bitmap rank by
+            // comparisons.
             const int nw = (a.nf + 31) >> 5;
-            if (nw <= BITMAP_WORDS) {
+            if (nw <= BITMAP_MAX_WORDS) {
                 unsigned *W = reinterpret_cast<unsigned *>(st);
-                int *P = reinterpret_cast<int *>(W + BITMAP_WORDS);
+                int *P = reinterpret_cast<int *>(W + nw);
+                int2 *raw = reinterpret_cast<int2 *>(P + nw);
                 for (int w = tid; w < nw; w += RASTER_THREADS) W[w] = 0u;
                 __syncthreads();
                 for (int k = tid; k < count; k += RASTER_THREADS) {
@@ -819,6 +833,7 @@ k_raster(RasterArgs a)
                     ids[P[w] + __popc(W[w] & ((1u << (v.x & 31)) - 1u))] = v;
                 }
             } else {
+                int2 *raw = reinterpret_cast<int2 *>(st);
                 for (int k = tid; k < count; k += RASTER_THREADS) raw[k] = bin[k];
                 __syncthreads();
                 for (int k = tid; k < count; k += RASTER_THREADS) {
@@ -950,6 +965,20 @@ k_raster(RasterArgs a)
                     dd = pixel_dd_setup<T>(g, kc, ti0 + q / TILE_W, tj0 + q % TILE_W, s_pz[q], pp);
             }
         }
+        if (lane == 0) {
+            s_red[wid][0] = cimin; s_red[wid][1] = cimax; s_red[wid][2] = cjmin; s_red[wid][3] = cjmax;
+        }
+        // (reduced before the scatter, so the positions are not live across it)
+        if (g.kind == VIEW_RADAR) {
+            // delay / Doppler extremes of the lit pixels as dkey keys (unlit
+            // lanes hold the neutral key)
+            const unsigned long long kd = dkey(pp.del), kp = dkey(pp.dop);
+            const unsigned long long k0 = warp_kmin(lit ? kd : ~0ull), k1 = warp_kmax(lit ? kd : 0ull);
+            const unsigned long long k2 = warp_kmin(lit ? kp : ~0ull), k3 = warp_kmax(lit ? kp : 0ull);
+            if (lane == 0) {
+                s_redk[wid][0] = k0; s_redk[wid][1] = k1; s_redk[wid][2] = k2; s_redk[wid][3] = k3;
+            }
+        }
         // The footprint goes straight to the frame's fit image in HBM: FP32 as
         // 16-byte vector reductions, FP64 as scalar atomics (both measured
         // faster than a shared-memory accumulator flushed per tile).
@@ -961,19 +990,6 @@ k_raster(RasterArgs a)
         } else if (g.kind == VIEW_RADAR && g.dop1d && lit) {
             a.states[item.x].any_overflow = 1;
             pixel_dop_overflow<T>(a, g, kc, scose, dd);
-        }
-        if (lane == 0) {
-            s_red[wid][0] = cimin; s_red[wid][1] = cimax; s_red[wid][2] = cjmin; s_red[wid][3] = cjmax;
-        }
-        if (g.kind == VIEW_RADAR) {
-            // delay / Doppler extremes of the lit pixels as dkey keys (unlit
-            // lanes hold the neutral key)
-            const unsigned long long kd = dkey(pp.del), kp = dkey(pp.dop);
-            const unsigned long long k0 = warp_kmin(lit ? kd : ~0ull), k1 = warp_kmax(lit ? kd : 0ull);
-            const unsigned long long k2 = warp_kmin(lit ? kp : ~0ull), k3 = warp_kmax(lit ? kp : 0ull);
-            if (lane == 0) {
-                s_redk[wid][0] = k0; s_redk[wid][1] = k1; s_redk[wid][2] = k2; s_redk[wid][3] = k3;
-            }
         }
         __syncthreads();
         if (tid == 0) {
@@ -1008,23 +1024,26 @@ k_raster(RasterArgs a)
     }
 }
 
+// Dynamic shared memory of a raster CTA: the ranked bin, then the staging
+// area, large enough for the staged facets and for the rank's scratch (the
+// bitmap and prefix counts, 8 bytes per 32 facets, plus the raw bin).
 template <typename T>
-inline size_t raster_smem_bytes(int cap)
+inline size_t raster_smem_bytes(int cap, int nf)
 {
-    return (size_t)2 * cap * sizeof(int2) + (size_t)STAGE_FACETS * sizeof(Stage<T>);
+    const size_t nw = ((size_t)nf + 31) / 32;
+    const size_t scratch = (nw <= (size_t)BITMAP_MAX_WORDS ? 8 * nw : 0) + (size_t)cap * sizeof(int2);
+    return raster_ids_bytes(cap) + std::max((size_t)STAGE_FACETS * sizeof(Stage<T>), scratch);
 }
 
-// Called once per device before any launch (not inside stream capture). The
-// FP32 kernel runs 6 CTAs per SM, which needs the largest shared-memory
-// carveout; the FP64 kernel (3 CTAs per SM) keeps the default.
+// Called once per device before any launch (not inside stream capture).
+// Both kernels run several CTAs per SM (8 FP32, 4 FP64), which needs the
+// largest shared-memory carveout.
 template <typename T>
 inline cudaError_t configure_raster_t()
 {
-    if (sizeof(T) == 4) {
-        cudaError_t e = cudaFuncSetAttribute(k_raster<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                             cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) return e;
-    }
+    cudaError_t e = cudaFuncSetAttribute(k_raster<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_raster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
@@ -1033,7 +1052,7 @@ inline void launch_raster_t(const RasterArgs &a, cudaStream_t s)
 {
     if (a.nwork <= 0) return;
     RasterArgs b = a;
-    b.smem_bytes = raster_smem_bytes<T>(a.cap);
+    b.smem_bytes = raster_smem_bytes<T>(a.cap, a.nf);
     k_raster<T><<<a.nwork, RASTER_THREADS, b.smem_bytes, s>>>(b);
 }
 
