@@ -256,14 +256,14 @@ __device__ inline KSum shfl_ksum(KSum a, int off)
 // o2 = sum obs^2/var, m2 = sum fit^2/var, om = sum fit*obs/var, each
 // product in the reference's order, accumulated with compensation.
 template <typename T>
-__device__ void chi2_item_partials(const Chi2Args &a, const Chi2Item &item, double (*red)[6], double *part);
+__device__ void chi2_item_partials(const Chi2Args &a, int it, const Chi2Item &item, double (*red)[6], double *part);
 
 template <typename T>
 __global__ void k_chi2_partials(Chi2Args a)
 {
     __shared__ double red[CHI2_THREADS / 32][6];
     for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
-        chi2_item_partials<T>(a, a.items[it], red, a.partials + (size_t)it * 6);
+        chi2_item_partials<T>(a, it, a.items[it], red, a.partials + (size_t)it * 6);
         __syncthreads();
     }
 }
@@ -759,28 +759,35 @@ __device__ void summary_totals(const SummaryArgs &a, Term term)
 }
 
 // One item's chi-square partial sums (the body of k_chi2_partials), left by
-// thread 0 in part[0..5].
+// thread 0 in part[0..5]. With a.o2pre set, o2 is the item's precomputed
+// partial and obs / 1/var are read only where the fit is nonzero: a zero
+// fit bin adds exact zeros to m2 and om, so the sums keep their values.
 template <typename T>
-__device__ void chi2_item_partials(const Chi2Args &a, const Chi2Item &item, double (*red)[6], double *part)
+__device__ void chi2_item_partials(const Chi2Args &a, int it, const Chi2Item &item, double (*red)[6], double *part)
 {
     const FrameGeom &g = a.geoms[a.frame_view[item.frame]];
     const long long base = g.fit_base + item.start;
     const T *fit = static_cast<const T *>(a.fit) + base;
     const double *obs = a.obs + base, *oov = a.oov + base;
+    const bool pre = a.o2pre != nullptr;
     KSum o2 = {0, 0}, m2 = {0, 0}, om = {0, 0};
     double ob[CHI2_ITEMS], wv[CHI2_ITEMS], ft[CHI2_ITEMS];
 #pragma unroll
     for (int j = 0; j < CHI2_ITEMS; j++) {
         const int k = threadIdx.x + j * CHI2_THREADS;
-        const bool in = k < item.count;
+        ft[j] = (k < item.count) ? (double)fit[k] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < CHI2_ITEMS; j++) {
+        const int k = threadIdx.x + j * CHI2_THREADS;
+        const bool in = (k < item.count) && (!pre || ft[j] != 0.0);
         ob[j] = in ? obs[k] : 0.0;
         wv[j] = in ? oov[k] : 0.0;
-        ft[j] = in ? (double)fit[k] : 0.0;
     }
 #pragma unroll
     for (int j = 0; j < CHI2_ITEMS; j++) {
         if (threadIdx.x + j * CHI2_THREADS >= item.count) break;
-        o2.add(ob[j] * ob[j] * wv[j]);
+        if (!pre) o2.add(ob[j] * ob[j] * wv[j]);
         m2.add(ft[j] * ft[j] * wv[j]);
         om.add(ft[j] * ob[j] * wv[j]);
     }
@@ -802,6 +809,10 @@ __device__ void chi2_item_partials(const Chi2Args &a, const Chi2Item &item, doub
                 r[q].add(red[ww][2 * q]);
                 r[q].c += red[ww][2 * q + 1];
             }
+        if (pre) {
+            r[0].s = a.o2pre[2 * (size_t)it];
+            r[0].c = a.o2pre[2 * (size_t)it + 1];
+        }
         for (int q = 0; q < 3; q++) {
             part[2 * q] = r[q].s;
             part[2 * q + 1] = r[q].c;
@@ -828,7 +839,7 @@ __global__ void __launch_bounds__(CHI2_THREADS) k_chi2_summary(Chi2Args ca, Fina
     double *s_part = reinterpret_cast<double *>(stage);
     for (int it = blockIdx.x; it < ca.nitems; it += gridDim.x) {
         const Chi2Item item = ca.items[it];
-        chi2_item_partials<T>(ca, item, red, ca.partials + (size_t)it * 6);
+        chi2_item_partials<T>(ca, it, item, red, ca.partials + (size_t)it * 6);
         const int fr = item.frame;
         const FrameHost &h = fa.fh[fr];
         if (threadIdx.x == 0) {

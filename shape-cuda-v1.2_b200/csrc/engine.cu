@@ -321,6 +321,7 @@ int EngineImpl::finalize()
     AL(d_seen, (size_t)nf);
     AL(d_chi2_items, chi2_items.size()); AL(d_frame_view, frame_view.size());
     AL(d_partials, chi2_items.size() * 6);
+    AL(d_o2pre, chi2_items.size() * 2);
     AL(d_chi2_counters, fh.size() + 1);
     AL(d_fh, fh.size()); AL(d_results, fh.size());
     AL(d_set_delpp, set_delpp.size()); AL(d_set_doppp, set_doppp.size()); AL(d_dop_extra, dop_extra.size());
@@ -376,6 +377,20 @@ int EngineImpl::finalize()
                            cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(d_dop_extra, dop_extra.data(), sizeof(double) * dop_extra.size(),
                            cudaMemcpyHostToDevice, s));
+    }
+    if (!chi2_items.empty()) {
+        // o2 = sum obs^2/var of each item depends on the data only: summed
+        // once here by the evaluation's own kernel and order, then kept
+        CK(cudaMemsetAsync(d_fit64, 0, sizeof(double) * fit_elems, s));
+        Chi2Args c0;
+        memset(&c0, 0, sizeof c0);
+        c0.items = d_chi2_items; c0.nitems = (int)chi2_items.size();
+        c0.obs = d_obs; c0.oov = d_oov; c0.fit = d_fit64;
+        c0.geoms = d_geoms; c0.frame_view = d_frame_view; c0.partials = d_partials;
+        c0.o2pre = nullptr;
+        launch_chi2_partials(c0, 0, s);
+        CK(cudaMemcpy2DAsync(d_o2pre, 2 * sizeof(double), d_partials, 6 * sizeof(double), 2 * sizeof(double),
+                             chi2_items.size(), cudaMemcpyDeviceToDevice, s));
     }
     if (!lcpts.empty()) {
         CK(cudaMemcpyAsync(d_lcpts, lcpts.data(), sizeof(LcPointDev) * lcpts.size(), cudaMemcpyHostToDevice, s));
@@ -544,6 +559,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     ca.geoms = d_geoms;
     ca.frame_view = d_frame_view;
     ca.partials = d_partials;
+    ca.o2pre = d_o2pre;
 
     LcArgs la;
     memset(&la, 0, sizeof la);
@@ -573,6 +589,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
                 cv.items = d_chi2_items + h.item0;
                 cv.nitems = h.nitems;
                 cv.partials = d_partials + (size_t)h.item0 * 6;
+                cv.o2pre = d_o2pre + (size_t)h.item0 * 2;
                 launch_chi2_partials(cv, 0, s);
             } else if (g.kind == VIEW_LC_SUN) {
                 int pt = g.frame_index;

@@ -131,6 +131,7 @@ struct EngineImpl {
     Chi2Item *d_chi2_items = nullptr;
     int *d_frame_view = nullptr;
     double *d_partials = nullptr;
+    double *d_o2pre = nullptr;        // per chi-square item: o2 partial (model independent)
     int *d_chi2_counters = nullptr;   // fused chi-square / summary: per-frame items done, frames done
     bool fused_chi2 = false;          // batched forms run k_chi2_summary
     FrameHost *d_fh = nullptr;

@@ -63,6 +63,9 @@ struct Chi2Args {
     const FrameGeom *geoms;      // radar views (for fit_base)
     const int *frame_view;       // global deldop frame -> view index
     double *partials;            // [nitems * 6]: o2, m2, om + compensations
+    // [nitems * 2]: each item's o2 partial (sum and compensation), computed
+    // once per dataset by the same code; null: o2 is summed per launch
+    const double *o2pre;
 };
 void launch_chi2_partials(const Chi2Args &a, int fp32, cudaStream_t s);
 
