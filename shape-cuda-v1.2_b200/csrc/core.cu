@@ -184,6 +184,32 @@ __global__ void k_bin(const FrameGeom *__restrict__ geoms, int view0, int nf,
     }
     int tx0 = (i1 + n) / TILE_W, tx1 = (i2 + n) / TILE_W;
     int ty0 = (j1 + n) / TILE_W, ty1 = (j2 + n) / TILE_W;
+    {
+        // facets inside one tile (most of them): lanes of a warp with the
+        // same tile reserve their slots with one atomic
+        const unsigned act = __activemask();
+        const bool single = (tx0 == tx1) && (ty0 == ty1);
+        const unsigned sm = __ballot_sync(act, single);
+        if (single) {
+            const int tile = g.tile_base + tx0 * g.tiles_x + ty0;
+            const int lane = threadIdx.x & 31;
+            const unsigned peers = __match_any_sync(sm, tile);
+            const int leader = __ffs(peers) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&bin_count[tile], __popc(peers));
+            base = __shfl_sync(peers, base, leader);
+            const int slot = base + __popc(peers & ((1u << lane) - 1u));
+            if (slot < cap) {
+                int ti0 = -n + tx0 * TILE_W, tj0 = -n + ty0 * TILE_W;
+                int ri1 = max(i1, ti0) - ti0, ri2 = min(i2, ti0 + TILE_W - 1) - ti0;
+                int rj1 = max(j1, tj0) - tj0, rj2 = min(j2, tj0 + TILE_W - 1) - tj0;
+                bin_ids[(size_t)tile * cap + slot] = make_int2(f, ri1 | (ri2 << 4) | (rj1 << 8) | (rj2 << 12));
+            } else {
+                st.bin_overflow = 1;
+            }
+            return;
+        }
+    }
     for (int tx = tx0; tx <= tx1; tx++)
         for (int ty = ty0; ty <= ty1; ty++) {
             int tile = g.tile_base + tx * g.tiles_x + ty;
@@ -268,15 +294,14 @@ __global__ void k_chi2_partials(Chi2Args a)
     }
 }
 
-// Per-frame results: chi2_deldop's calibration and chi-square
-// (src/shape/chi2.c:447-460) plus the posvis / pos2deldop frame outputs.
+// A frame's chi-square terms: chi2_deldop's sums, calibration and
+// chi-square (src/shape/chi2.c:436-460) from the frame's item partials.
 // part: the chi-square partials (6 per item), in global or shared memory;
 // part0: the index of the frame's first item in part.
-__device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr, const double *part, int part0)
+__device__ void finalize_frame_chi2(const FinalizeArgs &a, int fr, const double *part, int part0,
+                                    shape_deldop_result &r)
 {
     const FrameHost &h = a.fh[fr];
-    const FrameGeom &g = a.geoms[h.view];
-    const FrameState &st = a.states[h.view];
     // a Doppler frame's sums start from its overflow spectrum's o2 and m2
     // (src/shape/chi2.c:745-747)
     const double *ovf = (h.dop_index >= 0) ? a.ovf_out + (size_t)h.dop_index * DOP_OVF_TERMS : nullptr;
@@ -290,9 +315,18 @@ __device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr, con
     double cal = h.cal_in;
     if (h.cal_floating)
         cal = (om > 0.0) ? om / m2 : SHAPE_TINYCALFACT;
-    shape_deldop_result r;
     r.o2 = o2; r.m2 = m2; r.om = om; r.cal = cal;
     r.chi2 = h.weight * (o2 - 2 * cal * om + cal * cal * m2);
+}
+
+// A frame's posvis / pos2deldop outputs (limits, flags, log-factors), which
+// do not depend on the chi-square sums.
+__device__ void finalize_frame_geom(const FinalizeArgs &a, int fr, shape_deldop_result &r)
+{
+    const FrameHost &h = a.fh[fr];
+    const FrameGeom &g = a.geoms[h.view];
+    const FrameState &st = a.states[h.view];
+    const double *ovf = (h.dop_index >= 0) ? a.ovf_out + (size_t)h.dop_index * DOP_OVF_TERMS : nullptr;
     const int n = g.n;
     r.xlim[0] = min(n, min(st.cov_i[0], st.ofr_i[0]));
     r.xlim[1] = max(-n, max(st.cov_i[1], st.ofr_i[1]));
@@ -334,6 +368,14 @@ __device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr, con
         r.idellim[0] = r.idellim[1] = 0;
         r.dellim[0] = r.dellim[1] = 0.0;
     }
+}
+
+// Per-frame results: both parts, stored in a.results[fr].
+__device__ shape_deldop_result finalize_frame(const FinalizeArgs &a, int fr, const double *part, int part0)
+{
+    shape_deldop_result r;
+    finalize_frame_chi2(a, fr, part, part0, r);
+    finalize_frame_geom(a, fr, r);
     a.results[fr] = r;
     return r;
 }
@@ -820,15 +862,17 @@ __device__ void chi2_item_partials(const Chi2Args &a, int it, const Chi2Item &it
     }
 }
 
-// Chi-square partials, per-frame results and totals in one launch. Each
-// block computes chunks (items) as k_chi2_partials does; the block that
-// completes a frame's last item (a per-frame counter) finalizes that frame
-// from its items' partials in item order, and the block that finalizes the
-// last frame computes the totals in dataset order. The sums and their order
-// are those of k_chi2_partials + k_summary, so the results are the same.
-// Values another block wrote in this launch are read through L2 (__ldcg)
-// after a fence. counters: [nframes] per-frame finished items, then the
-// finished frames; zero before the launch.
+// Chi-square partials, per-frame results and totals in one launch. Blocks
+// first fill each frame's chi-square-independent outputs (limits, flags,
+// log-factors: finalize_frame_geom), one frame per block, then compute
+// chunks (items) as k_chi2_partials does. A frame's counter takes one count
+// for its outputs and one per item; the block that makes the last count
+// adds the frame's chi-square terms from its items' partials in item order,
+// and the block that completes the last frame computes the totals in
+// dataset order. The sums and their order are those of k_chi2_partials +
+// k_summary, so the results are the same. Values another block wrote in
+// this launch are read through L2 (__ldcg) after a fence. counters:
+// [nframes] per frame, then the finished frames; zero before the launch.
 template <typename T>
 __global__ void __launch_bounds__(CHI2_THREADS) k_chi2_summary(Chi2Args ca, FinalizeArgs fa, SummaryArgs sa,
                                                                int *counters)
@@ -837,24 +881,47 @@ __global__ void __launch_bounds__(CHI2_THREADS) k_chi2_summary(Chi2Args ca, Fina
     __shared__ __align__(16) unsigned char stage[FUSED_STAGE_BYTES];
     __shared__ int s_last;
     double *s_part = reinterpret_cast<double *>(stage);
-    for (int it = blockIdx.x; it < ca.nitems; it += gridDim.x) {
-        const Chi2Item item = ca.items[it];
-        chi2_item_partials<T>(ca, it, item, red, ca.partials + (size_t)it * 6);
-        const int fr = item.frame;
+    const int nwork = fa.nframes + ca.nitems;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        int fr;
+        if (w < fa.nframes) {                                 // a frame's outputs
+            fr = w;
+            if (threadIdx.x == 0) {
+                shape_deldop_result r;
+                finalize_frame_geom(fa, fr, r);
+                shape_deldop_result *out = fa.results + fr;
+                out->xlim[0] = r.xlim[0]; out->xlim[1] = r.xlim[1];
+                out->ylim[0] = r.ylim[0]; out->ylim[1] = r.ylim[1];
+                out->outbnd = r.outbnd; out->posbnd_logfactor = r.posbnd_logfactor;
+                out->badradar = r.badradar; out->badradar_logfactor = r.badradar_logfactor;
+                out->idellim[0] = r.idellim[0]; out->idellim[1] = r.idellim[1];
+                out->idoplim[0] = r.idoplim[0]; out->idoplim[1] = r.idoplim[1];
+                out->dellim[0] = r.dellim[0]; out->dellim[1] = r.dellim[1];
+                out->doplim[0] = r.doplim[0]; out->doplim[1] = r.doplim[1];
+            }
+        } else {                                              // a chunk's partials
+            const int it = w - fa.nframes;
+            const Chi2Item item = ca.items[it];
+            chi2_item_partials<T>(ca, it, item, red, ca.partials + (size_t)it * 6);
+            fr = item.frame;
+        }
         const FrameHost &h = fa.fh[fr];
         if (threadIdx.x == 0) {
-            __threadfence();                                  // partials before the count
-            s_last = (atomicAdd(&counters[fr], 1) == h.nitems - 1);
+            __threadfence();                                  // outputs / partials before the count
+            s_last = (atomicAdd(&counters[fr], 1) == h.nitems);
         }
         __syncthreads();
         if (s_last) {                                         // block-uniform
             __threadfence();
-            // the frame's partials to shared memory, then its results
+            // the frame's partials to shared memory, then its chi-square terms
             for (int k = threadIdx.x; k < 6 * h.nitems; k += blockDim.x)
                 s_part[k] = __ldcg(ca.partials + (size_t)h.item0 * 6 + k);
             __syncthreads();
             if (threadIdx.x == 0) {
-                finalize_frame(fa, fr, s_part, 0);
+                shape_deldop_result r;
+                finalize_frame_chi2(fa, fr, s_part, 0, r);
+                shape_deldop_result *out = fa.results + fr;
+                out->o2 = r.o2; out->m2 = r.m2; out->om = r.om; out->cal = r.cal; out->chi2 = r.chi2;
                 __threadfence();                              // results before the count
                 s_last = (atomicAdd(&counters[fa.nframes], 1) == fa.nframes - 1);
             }
@@ -997,8 +1064,9 @@ bool chi2_summary_fits(int nframes, int max_frame_items)
 void launch_chi2_summary(const Chi2Args &ca, const FinalizeArgs &fa, const SummaryArgs &sa, int *counters,
                          int fp32, cudaStream_t s)
 {
-    int blocks = ca.nitems < 8 * 148 ? ca.nitems : 8 * 148;
-    if (blocks <= 0) return;
+    const int nwork = fa.nframes + ca.nitems;       // frame outputs, then chunks
+    int blocks = nwork < 8 * 148 ? nwork : 8 * 148;
+    if (blocks <= 0 || ca.nitems <= 0) return;
     if (fp32) k_chi2_summary<float><<<blocks, CHI2_THREADS, 0, s>>>(ca, fa, sa, counters);
     else k_chi2_summary<double><<<blocks, CHI2_THREADS, 0, s>>>(ca, fa, sa, counters);
 }
