@@ -611,6 +611,10 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         // exit at once); the block scheduler balances the rest
         ra.work = d_work_sorted;
         ra.nwork = (int)work.size();
+        // one CTA per tile that was non-empty when the bins were tuned (they
+        // lead the sorted list); the grid-stride loop visits the tiles after
+        // them, empty then, so those cost no CTA launches of their own
+        ra.grid = tuned_nonempty;
         if (f32) launch_raster_f32(ra, s); else launch_raster_f64(ra, s);
         mark(4);
         ca.items = d_chi2_items;

@@ -1053,7 +1053,8 @@ inline void launch_raster_t(const RasterArgs &a, cudaStream_t s)
     if (a.nwork <= 0) return;
     RasterArgs b = a;
     b.smem_bytes = raster_smem_bytes<T>(a.cap, a.nf);
-    k_raster<T><<<a.nwork, RASTER_THREADS, b.smem_bytes, s>>>(b);
+    const int grid = (a.grid > 0 && a.grid < a.nwork) ? a.grid : a.nwork;
+    k_raster<T><<<grid, RASTER_THREADS, b.smem_bytes, s>>>(b);
 }
 
 }  // namespace shape
