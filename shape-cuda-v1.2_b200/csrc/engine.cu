@@ -478,8 +478,21 @@ int EngineImpl::tune_bins()
         int cy = counts[geoms[work[y].x].tile_base + work[y].y];
         return cx > cy;
     });
+    // radar tiles first, lightcurve-view tiles after them, each part in
+    // decreasing count: the batched FP32 form rasters the two parts with
+    // different kernels
+    std::stable_partition(order.begin(), order.end(),
+                          [&](int x) { return geoms[work[x].x].kind == VIEW_RADAR; });
     std::vector<int2> sorted(work.size());
-    for (size_t k = 0; k < work.size(); k++) sorted[k] = work[order[k]];
+    work_radar = nonempty_radar = nonempty_lc = 0;
+    for (size_t k = 0; k < work.size(); k++) {
+        sorted[k] = work[order[k]];
+        const bool radar = geoms[sorted[k].x].kind == VIEW_RADAR;
+        const bool busy = counts[geoms[sorted[k].x].tile_base + sorted[k].y] > 0;
+        work_radar += radar;
+        nonempty_radar += radar && busy;
+        nonempty_lc += !radar && busy;
+    }
     if (!d_work_sorted) {
         int rc = mem.alloc(&d_work_sorted, work.size());
         if (rc) return rc;
@@ -609,13 +622,27 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         mark(3);
         // one CTA per tile, heaviest tiles first (empty tiles sort last and
         // exit at once); the block scheduler balances the rest
-        ra.work = d_work_sorted;
-        ra.nwork = (int)work.size();
         // one CTA per tile that was non-empty when the bins were tuned (they
-        // lead the sorted list); the grid-stride loop visits the tiles after
-        // them, empty then, so those cost no CTA launches of their own
-        ra.grid = tuned_nonempty;
-        if (f32) launch_raster_f32(ra, s); else launch_raster_f64(ra, s);
+        // lead each part of the sorted list); the grid-stride loop visits the
+        // tiles after them, empty then, so those cost no CTA launches of
+        // their own. The FP32 form rasters lightcurve views with its exact
+        // variant, in a second launch.
+        ra.work = d_work_sorted;
+        if (f32) {
+            RasterArgs rr = ra, rl = ra;
+            rr.nwork = work_radar;
+            rr.grid = nonempty_radar;
+            rl.work = d_work_sorted + work_radar;
+            rl.nwork = (int)work.size() - work_radar;
+            rl.grid = nonempty_lc;
+            rl.exact = 1;
+            launch_raster_f32(rr, s);
+            launch_raster_f32(rl, s);
+        } else {
+            ra.nwork = (int)work.size();
+            ra.grid = tuned_nonempty;
+            launch_raster_f64(ra, s);
+        }
         mark(4);
         ca.items = d_chi2_items;
         ca.nitems = (int)chi2_items.size();
@@ -685,6 +712,8 @@ int EngineImpl::kernels_per_eval(int form) const
             n += 3 + (geoms[v].kind == VIEW_RADAR || geoms[v].kind == VIEW_LC_SUN ? 1 : 0);
     } else {
         n += 3;                          // transform, bin, raster
+        if (form == SHAPE_FORM_BATCHED_FP32 && work_radar > 0 && work_radar < (int)work.size())
+            n += 1;                      // FP32: radar and lightcurve views in two launches
         n += (chi2_items.empty() || fused_chi2) ? 0 : 1;   // fused: counted with the summary
         n += lc_items.empty() ? 0 : 1;
     }

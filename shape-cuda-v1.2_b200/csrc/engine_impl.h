@@ -212,6 +212,10 @@ struct EngineImpl {
     // bin tuning results
     int2 *d_work_sorted = nullptr;
     int tuned_max_count = 0, tuned_nonempty = 0;
+    // the sorted work list holds radar tiles first (work_radar of them, the
+    // first nonempty_radar non-empty at tuning), then lightcurve-view tiles
+    // (nonempty_lc non-empty at tuning)
+    int work_radar = 0, nonempty_radar = 0, nonempty_lc = 0;
     int fixed_cap = 0;            // > 0: bin capacity set by the caller, no autotuning
     int evaluate(int form, shape_eval_summary *out);
     int kernels_per_eval(int form) const;

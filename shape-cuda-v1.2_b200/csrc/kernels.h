@@ -24,6 +24,7 @@ struct RasterArgs {
     const int2 *work;          // (view, tile) items
     int nwork;                 // items
     int grid;                  // CTAs (0: one per item); fewer CTAs stride over the rest
+    int exact;                 // FP32 form: the exact variant (lightcurve views)
     const void *vt;            // double4 view-frame vertices (both forms)
     const int4 *fvi;
     const double4 *vn;

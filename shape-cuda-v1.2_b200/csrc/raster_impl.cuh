@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstddef>
 
 #include "kernels.h"
 
@@ -142,11 +143,15 @@ template <typename T> __device__ T radlaw_dev(const RadarLawDev &L, T c)
 template <typename T>
 struct Stage {
     typename Vec4<T>::type p0, p1, p2;
+    // one 16-byte group, read with one vector load per visit
+    unsigned bb;         // pixel bbox in the tile as byte bounds (pack_bb)
+    float es, et, ez;    // FP32 form: error bounds of the FP32 s, t and depth over the tile
     T nz;                // facet normal in view coordinates: (p2.z, p2.w, nz), views without smoothing
     T q[9];              // body-frame vertex normals of the three corners (smoothing)
-    unsigned bb;         // pixel bbox in the tile as byte bounds (pack_bb)
     int wmask, f;
 };
+static_assert(offsetof(Stage<float>, bb) % 16 == 0 && offsetof(Stage<double>, bb) % 16 == 0,
+              "the bbox / error-bound group is read as one 16-byte vector");
 
 // A facet's bbox in its tile (rows ri1..ri2, columns rj1..rj2) packed so one
 // byte-wise comparison tests a pixel: pixel (li, lj) packed by pack_px lies
@@ -217,6 +222,15 @@ __device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage
         s.p1 = vec4<T>((T)b1, (T)b2, (T)c0, (T)c1);
         E = (T)c2;       // p2 = (c2, v02, nx, ny)
         F = (T)p0.z;
+        // Bounds on the FP32 values' error at any pixel centre of the tile
+        // (x, y in [0, 16 kmpp)): 8 units of 2^-24 of the summed magnitudes
+        // of the terms (rounded coefficients, two fused multiply-adds, the
+        // depth's add); at least 1e-9, so a value past twice its bound
+        // also clears posvis's 1e-10 tolerance.
+        const double xs = 16.0 * g.kmpp, u = 8.0 / 16777216.0;
+        s.es = (float)fmax(1e-9, u * (fabs(a0) + (fabs(a1) + fabs(a2)) * xs));
+        s.et = (float)fmax(1e-9, u * (fabs(b0) + (fabs(b1) + fabs(b2)) * xs));
+        s.ez = (float)(u * (fabs(p0.z) + fabs(c0) + (fabs(c1) + fabs(c2)) * xs));
     }
     s.f = f;
     if (g.smooth) {
@@ -657,6 +671,85 @@ __device__ void pixel_dop_overflow(const RasterArgs &a, const FrameGeom &g, cons
         atomicAdd(ov + idop + g.idop0, (double)(amp * (T)1 * dop_c[min(idop - idop_min, SHAPE_MAXBINS)]));
 }
 
+// FP32 form: the FP64 depth of facet c at the pixel centre (x0, y0), with
+// the FP64 form's terms and operation order (stage_fill and the visit's s,
+// t, z), rounded op by op so no multiply-add is fused: the same value the
+// FP64 raster stores for this facet. posmask compares such depths with the
+// sun view's, where a few 1e-8 km decide a pixel's shadow.
+__device__ inline double facet_depth64(const double4 *vt, int4 c, double x0, double y0)
+{
+    const double4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
+    const double A = __dsub_rn(p2.y, p1.y), B = __dsub_rn(p2.x, p1.x);
+    const double C = __dsub_rn(p1.x, p0.x), D = __dsub_rn(p1.y, p0.y);
+    const double E = __dsub_rn(p1.z, p0.z), F = __dsub_rn(p2.z, p1.z);
+    const double den = 1.0 / __dsub_rn(__dmul_rn(C, A), __dmul_rn(B, D));
+    const double dx = __dsub_rn(x0, p0.x), dy = __dsub_rn(y0, p0.y);
+    const double sv = __dmul_rn(__dsub_rn(__dmul_rn(dx, A), __dmul_rn(B, dy)), den);
+    const double tv = __dmul_rn(__dsub_rn(__dmul_rn(C, dy), __dmul_rn(dx, D)), den);
+    return __dadd_rn(__dadd_rn(p0.z, __dmul_rn(sv, E)), __dmul_rn(tv, F));
+}
+
+// FP32 form, rare path: posvis at one pixel by the FP64 form's rules (the
+// FP64 visit's s, t, depth and tolerance, rounded op by op; its update rule
+// and order-dependent smoothed normal), over the tile's bin in facet order.
+// ids: the bin's (facet, packed tile bbox) entries, sorted; (li, lj): the
+// pixel in the tile; (x0, y0): its centre. Returns the winner's facet
+// (-1: none) and writes its FP32 depth and the cos(e) state.
+static __device__ __forceinline__ int pixel_posvis64(const RasterArgs &a, const FrameGeom &g, const int2 *ids,
+                                                  int count, int li, int lj, double x0, double y0, float *zz,
+                                                  bool *good, float *gm)
+{
+    const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
+    double zw = -SHAPE_HUGENUMBER;
+    int fac = -1;
+    for (int k = 0; k < count; k++) {
+        const int2 e = ids[k];
+        const int b = e.y;
+        if (li < (b & 15) || li > ((b >> 4) & 15) || lj < ((b >> 8) & 15) || lj > ((b >> 12) & 15)) continue;
+        const int4 c = a.fvi[e.x];
+        const double4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
+        const double A = __dsub_rn(p2.y, p1.y), B = __dsub_rn(p2.x, p1.x);
+        const double C = __dsub_rn(p1.x, p0.x), D = __dsub_rn(p1.y, p0.y);
+        const double E = __dsub_rn(p1.z, p0.z), F = __dsub_rn(p2.z, p1.z);
+        const double den = 1.0 / __dsub_rn(__dmul_rn(C, A), __dmul_rn(B, D));
+        const double dx = __dsub_rn(x0, p0.x), dy = __dsub_rn(y0, p0.y);
+        const double sv = __dmul_rn(__dsub_rn(__dmul_rn(dx, A), __dmul_rn(B, dy)), den);
+        if (!((sv >= -SHAPE_SMALLVAL) && (sv <= __dadd_rn(1.0, SHAPE_SMALLVAL)))) continue;
+        const double tv = __dmul_rn(__dsub_rn(__dmul_rn(C, dy), __dmul_rn(dx, D)), den);
+        if (!((tv >= -SHAPE_SMALLVAL) && (tv <= __dadd_rn(sv, SHAPE_SMALLVAL)))) continue;
+        const double z = __dadd_rn(__dadd_rn(p0.z, __dmul_rn(sv, E)), __dmul_rn(tv, F));
+        if (!((z > zw) || (fac < 0))) continue;
+        zw = z;
+        fac = e.x;
+        if (g.smooth) {
+            const double4 q0 = a.vn[c.x], q1 = a.vn[c.y], q2 = a.vn[c.z];
+            const double m0 = __dadd_rn(__dadd_rn(q0.x, __dmul_rn(sv, __dsub_rn(q1.x, q0.x))),
+                                        __dmul_rn(tv, __dsub_rn(q2.x, q1.x)));
+            const double m1 = __dadd_rn(__dadd_rn(q0.y, __dmul_rn(sv, __dsub_rn(q1.y, q0.y))),
+                                        __dmul_rn(tv, __dsub_rn(q2.y, q1.y)));
+            const double m2 = __dadd_rn(__dadd_rn(q0.z, __dmul_rn(sv, __dsub_rn(q1.z, q0.z))),
+                                        __dmul_rn(tv, __dsub_rn(q2.z, q1.z)));
+            double r2 = 0.0;
+            r2 = __dadd_rn(r2, __dmul_rn(g.oa[6], m0));
+            r2 = __dadd_rn(r2, __dmul_rn(g.oa[7], m1));
+            r2 = __dadd_rn(r2, __dmul_rn(g.oa[8], m2));
+            if (r2 > 0.0) { *good = true; gm[0] = (float)m0; gm[1] = (float)m1; gm[2] = (float)m2; }
+        } else {
+            const double4 nb = a.fn[e.x];
+            double nn[3];
+            for (int r = 0; r < 3; r++) {
+                nn[r] = 0.0;
+                nn[r] = __dadd_rn(nn[r], __dmul_rn(g.oa[3 * r + 0], nb.x));
+                nn[r] = __dadd_rn(nn[r], __dmul_rn(g.oa[3 * r + 1], nb.y));
+                nn[r] = __dadd_rn(nn[r], __dmul_rn(g.oa[3 * r + 2], nb.z));
+            }
+            *good = true; gm[0] = (float)nn[0]; gm[1] = (float)nn[1]; gm[2] = (float)nn[2];
+        }
+    }
+    *zz = (float)zw;
+    return fac;
+}
+
 // Warp-wide extremes with the hardware warp reduction (one instruction per
 // 32-bit word); 64-bit order-preserving keys (dkey) reduce their high words
 // first, then the low words of the lanes holding the extreme high word.
@@ -675,7 +768,12 @@ __device__ inline unsigned long long warp_kmax(unsigned long long k)
     return ((unsigned long long)hi << 32) | lo;
 }
 
-template <typename T>
+// The tile raster. EXACT (FP32 form, lightcurve views): a pixel with a
+// decision within FP32 error is redone by the FP64 form's rules, so facet
+// assignment, depth and the shadow test's inputs are the FP64 form's;
+// without it (radar views) the FP32 test's tolerance is the staged error
+// bound, which keeps pixels on shared edges covered.
+template <typename T, bool EXACT>
 __global__ void __launch_bounds__(RASTER_THREADS, sizeof(T) == 8 ? RASTER_MIN_BLOCKS_F64 : RASTER_MIN_BLOCKS)
 k_raster(RasterArgs a)
 {
@@ -714,8 +812,9 @@ k_raster(RasterArgs a)
         const T x0 = (sizeof(T) == 8) ? (T)pi * (T)g.kmpp : (T)((double)li * g.kmpp);
         const T x1 = (sizeof(T) == 8) ? (T)pj * (T)g.kmpp : (T)((double)lj * g.kmpp);
         T zz = (T)(-SHAPE_HUGENUMBER), cosa = 0, cosb = 0;
-        T zrel = 0;      // FP32 form: the winner's depth above its first corner
         int fac = -1;
+        T zze = 0;       // FP32 form: the winner's depth error bound
+        bool amb = false;   // FP32 form: a decision within FP32 error (pixel_posvis64 redoes it)
         bool good = false;
         T gm0 = 0, gm1 = 0, gm2 = 0;
         const bool smooth = g.smooth != 0;
@@ -738,21 +837,36 @@ k_raster(RasterArgs a)
                 z = p1.w + sv * p2.x + tv * p2.y;
                 if (!((z > zz) || (fac < 0))) return;
             } else {
-                // the whole test without early exits (a warp runs every step
-                // for some lane anyway), then one branch for a win
+                // FP32 test without early exits (a warp runs every step for
+                // some lane anyway). A value within its error bound of a
+                // boundary of the test, or a depth within the bounds of the
+                // winner's, marks the pixel ambiguous: after the replay it is
+                // redone by the FP64 form's own rules (pixel_posvis64), so the
+                // FP32 form assigns facets as the FP64 form does.
                 const auto p0 = s.p0, p1 = s.p1, p2 = s.p2;
-                const bool inb = __vcmpgeu4(pxw, s.bb) == 0xffffffffu;   // pixel in the facet's bbox
+                const float4 be = *reinterpret_cast<const float4 *>(&s.bb);   // bb, es, et, ez
+                const bool inb = __vcmpgeu4(pxw, __float_as_uint(be.x)) == 0xffffffffu;   // pixel in the facet's bbox
                 sv = fmaf(p0.y, x0, fmaf(p0.z, x1, p0.x));
                 tv = fmaf(p1.x, x0, fmaf(p1.y, x1, p0.w));
                 zr = fmaf(p1.w, x0, fmaf(p2.x, x1, p1.z));
                 z = p2.y + zr;
-                const bool in = inb && (sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL) &&
-                                (tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL);
-                if (!(in && ((z > zz) || (fac < 0)))) return;
+                const T es = be.y, et = be.z, est = es + et;
+                if constexpr (EXACT) {
+                    const bool out = !inb || (sv < -2 * es) || (sv > 1 + 2 * es) || (tv < -2 * et) ||
+                                     (tv > sv + 2 * est);
+                    if (out) return;
+                    const bool sure = (sv >= es) && (sv <= 1 - es) && (tv >= et) && (tv <= sv - est);
+                    const bool near = (fac >= 0) && (fabsf(z - zz) <= be.w + zze);
+                    amb = amb || !sure || near;
+                    if (!((z > zz) || (fac < 0))) return;
+                    zze = be.w;
+                } else {
+                    const bool in = inb && (sv >= -es) && (sv <= 1 + es) && (tv >= -et) && (tv <= sv + est);
+                    if (!(in && ((z > zz) || (fac < 0)))) return;
+                }
             }
             const auto p2 = s.p2;
             zz = z;
-            zrel = zr;
             fac = s.f;
             // cos(e) changes only when the smoothed normal faces the viewer
             // (posvis.c:265). Its sign is that of the view-z component before
@@ -764,6 +878,8 @@ k_raster(RasterArgs a)
                 const T m2 = s.q[2] + sv * (s.q[5] - s.q[2]) + tv * (s.q[8] - s.q[5]);
                 T r2 = 0;
                 r2 += oa6 * m0; r2 += oa7 * m1; r2 += oa8 * m2;
+                if constexpr (sizeof(T) == 4 && EXACT)     // the sign of r2 within FP32 error
+                    amb = amb || (fabsf(r2) <= 4 * (s.es + s.et) + 1e-6f * (fabsf(m0) + fabsf(m1) + fabsf(m2)));
                 if (r2 > (T)0) { good = true; gm0 = m0; gm1 = m1; gm2 = m2; }
             } else {
                 good = true; gm0 = p2.z; gm1 = p2.w; gm2 = s.nz;
@@ -882,6 +998,19 @@ k_raster(RasterArgs a)
             }
         }
 
+        // FP32 form: a pixel with a decision within FP32 error is redone by
+        // the FP64 form's rules over the sorted bin (a bin-overflow tile,
+        // which has no sorted bin, keeps its FP32 decisions)
+        if constexpr (sizeof(T) == 4 && EXACT) {
+            if (amb && count > 0 && count <= a.cap) {
+                float gmv[3] = {0.0f, 0.0f, 0.0f};
+                good = false;
+                fac = pixel_posvis64(a, g, ids, count, li, lj, (double)pi * g.kmpp, (double)pj * g.kmpp, &zz,
+                                     &good, gmv);
+                gm0 = gmv[0]; gm1 = gmv[1]; gm2 = gmv[2];
+            }
+        }
+
         // cos(e) / cos(i) of the last winner whose smoothed normal faced the
         // viewer: cotrans + normalize (posvis.c:250-274), once per pixel
         if (good) {
@@ -910,15 +1039,17 @@ k_raster(RasterArgs a)
 
         // ---- outputs of this tile
         const bool covered = inframe && fac >= 0;
-        // FP64 depth: the FP32 form adds the winner's FP32 depth offset to its
-        // first corner's FP64 depth
+        // FP64 depth. FP32 form: a radar pixel keeps its FP32 depth (about
+        // 1e-7 km, 1e-5 of a delay bin); a lightcurve view recomputes the
+        // winning facet's depth in FP64 (facet_depth64), because posmask's
+        // shadow test compares it with the sun view's to a few 1e-8 km.
         double z64 = (double)zz;
         if constexpr (sizeof(T) == 4) {
-            if (fac >= 0) {
-                const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
-                z64 = vt[a.fvi[fac].x].z + (double)zrel;
-            } else {
+            if (fac < 0) {
                 z64 = -SHAPE_HUGENUMBER;
+            } else if (g.kind != VIEW_RADAR) {
+                const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
+                z64 = facet_depth64(vt, a.fvi[fac], (double)pi * g.kmpp, (double)pj * g.kmpp);
             }
         }
         if (inframe && writes_pos) {
@@ -1038,13 +1169,20 @@ inline size_t raster_smem_bytes(int cap, int nf)
 // Called once per device before any launch (not inside stream capture).
 // Both kernels run several CTAs per SM (8 FP32, 4 FP64), which needs the
 // largest shared-memory carveout.
+template <typename T, bool EXACT>
+inline cudaError_t configure_raster_one()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_raster<T, EXACT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_raster<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
 template <typename T>
 inline cudaError_t configure_raster_t()
 {
-    cudaError_t e = cudaFuncSetAttribute(k_raster<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                         cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_raster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaError_t e = configure_raster_one<T, false>();
+    if (e != cudaSuccess || sizeof(T) == 8) return e;
+    return configure_raster_one<T, true>();
 }
 
 template <typename T>
@@ -1054,7 +1192,10 @@ inline void launch_raster_t(const RasterArgs &a, cudaStream_t s)
     RasterArgs b = a;
     b.smem_bytes = raster_smem_bytes<T>(a.cap, a.nf);
     const int grid = (a.grid > 0 && a.grid < a.nwork) ? a.grid : a.nwork;
-    k_raster<T><<<grid, RASTER_THREADS, b.smem_bytes, s>>>(b);
+    // the FP64 form is exact by construction; the FP32 form runs its exact
+    // variant on lightcurve views
+    if (sizeof(T) == 4 && a.exact) k_raster<T, true><<<grid, RASTER_THREADS, b.smem_bytes, s>>>(b);
+    else k_raster<T, false><<<grid, RASTER_THREADS, b.smem_bytes, s>>>(b);
 }
 
 }  // namespace shape

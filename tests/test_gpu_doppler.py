@@ -91,5 +91,5 @@ def test_mixed_deldop_doppler_lightcurve(cuda_device):
         for k, r in enumerate(od["results"] + op["results"]):
             assert abs(res[k]["chi2"] - r["chi2"]) <= 1e-10 * abs(r["chi2"]), (form, k)
     s32 = e.evaluate(eng.FORM_BATCHED_FP32)
-    assert abs(s32["chi2"] - chi2_o) <= 5e-2 * chi2_o     # lightcurve term dominates the FP32 error
+    assert abs(s32["chi2"] - chi2_o) <= 1e-6 * chi2_o
     e.close()
