@@ -116,6 +116,7 @@ template <typename T4>
 __global__ void k_xform(const FrameGeom *__restrict__ geoms, const double4 *__restrict__ vx, int nv,
                         T4 *__restrict__ vt)
 {
+    grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nv) return;
     const FrameGeom &g = geoms[blockIdx.y];
@@ -143,6 +144,7 @@ __global__ void k_bin(const FrameGeom *__restrict__ geoms, int view0, int nf,
                       const T4 *__restrict__ vt, FrameState *__restrict__ states,
                       int *__restrict__ bin_count, int2 *__restrict__ bin_ids, int cap)
 {
+    grid_dep_wait();
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nf) return;
     int v = view0 + blockIdx.y;
@@ -880,6 +882,7 @@ __global__ void __launch_bounds__(CHI2_THREADS) k_chi2_summary(Chi2Args ca, Fina
     __shared__ double red[CHI2_THREADS / 32][6];
     __shared__ __align__(16) unsigned char stage[FUSED_STAGE_BYTES];
     __shared__ int s_last;
+    grid_dep_wait();
     double *s_part = reinterpret_cast<double *>(stage);
     const int nwork = fa.nframes + ca.nitems;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
@@ -981,18 +984,20 @@ void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, 
     k_reset_state<<<blocks, 256, 0, s>>>(st, nviews, bin_count, ntiles);
 }
 
-void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt, cudaStream_t s)
+void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt, cudaStream_t s,
+                      bool pdl)
 {
     dim3 grid((nv + 255) / 256, nviews);
-    k_xform<double4><<<grid, 256, 0, s>>>(g, vx, nv, vt);
+    launch_k(k_xform<double4>, grid, dim3(256), 0, s, pdl, g, vx, nv, vt);
 }
 
 
 void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const double4 *vt,
-                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s)
+                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s, bool pdl)
 {
     dim3 grid((m.nf + 255) / 256, nviews);
-    k_bin<double4><<<grid, 256, 0, s>>>(g, view0, m.nf, m.fvi, m.fn, vt, st, bin_count, bin_ids, cap);
+    launch_k(k_bin<double4>, grid, dim3(256), 0, s, pdl, g, view0, m.nf, (const int4 *)m.fvi, (const double4 *)m.fn,
+             vt, st, bin_count, bin_ids, cap);
 }
 
 
@@ -1062,13 +1067,13 @@ bool chi2_summary_fits(int nframes, int max_frame_items)
 }
 
 void launch_chi2_summary(const Chi2Args &ca, const FinalizeArgs &fa, const SummaryArgs &sa, int *counters,
-                         int fp32, cudaStream_t s)
+                         int fp32, cudaStream_t s, bool pdl)
 {
     const int nwork = fa.nframes + ca.nitems;       // frame outputs, then chunks
     int blocks = nwork < 8 * 148 ? nwork : 8 * 148;
     if (blocks <= 0 || ca.nitems <= 0) return;
-    if (fp32) k_chi2_summary<float><<<blocks, CHI2_THREADS, 0, s>>>(ca, fa, sa, counters);
-    else k_chi2_summary<double><<<blocks, CHI2_THREADS, 0, s>>>(ca, fa, sa, counters);
+    if (fp32) launch_k(k_chi2_summary<float>, dim3(blocks), dim3(CHI2_THREADS), 0, s, pdl, ca, fa, sa, counters);
+    else launch_k(k_chi2_summary<double>, dim3(blocks), dim3(CHI2_THREADS), 0, s, pdl, ca, fa, sa, counters);
 }
 
 void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s)

@@ -614,10 +614,14 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
             }
         }
     } else {
-        launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
+        // graph-captured chain: each kernel after the first is a programmatic
+        // dependent launch of the one before it (stage timing keeps plain
+        // launches so its events separate the stages)
+        const bool pdl = fork;
+        launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s, pdl);
         mark(2);
         if (fork) CK(cudaStreamWaitEvent(s, evf[2], 0));
-        launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s);
+        launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s, pdl);
         if (fork) CK(cudaStreamWaitEvent(s, evf[3], 0));
         mark(3);
         // one CTA per tile, heaviest tiles first (empty tiles sort last and
@@ -628,6 +632,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         // their own. The FP32 form rasters lightcurve views with its exact
         // variant, in a second launch.
         ra.work = d_work_sorted;
+        ra.pdl = pdl ? 1 : 0;
         if (f32) {
             RasterArgs rr = ra, rl = ra;
             rr.nwork = work_radar;
@@ -695,7 +700,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     sa.baddiam = 0;
     sa.baddiam_logfactor = 0.0;
     sa.out = d_summary;
-    if (fused) launch_chi2_summary(ca, fa, sa, d_chi2_counters, f32 ? 1 : 0, s);
+    if (fused) launch_chi2_summary(ca, fa, sa, d_chi2_counters, f32 ? 1 : 0, s, fork);
     else launch_summary(fa, sa, s);
     mark(7);
     CK(cudaGetLastError());

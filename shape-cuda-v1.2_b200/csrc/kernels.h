@@ -9,6 +9,33 @@
 
 namespace shape {
 
+// Programmatic dependent launch (batched forms): a kernel launched with
+// launch_k(..., pdl = true) may be scheduled before the previous kernel on
+// its stream has finished, and waits here, before its first access to that
+// kernel's outputs, until it has (a no-op after an ordinary launch). The
+// previous kernel does not trigger early, so waiting blocks take no SM
+// slots from it; what is saved is the launch latency between the two.
+#ifdef __CUDACC__
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+#endif
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, bool pdl,
+                     Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? at : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 struct ModelDev {
     int nv, nf;
     const double *a, *u, *r, *scale;   // a,u: [nv*3]
@@ -25,6 +52,7 @@ struct RasterArgs {
     int nwork;                 // items
     int grid;                  // CTAs (0: one per item); fewer CTAs stride over the rest
     int exact;                 // FP32 form: the exact variant (lightcurve views)
+    int pdl;                   // programmatic dependent launch (launch_k)
     const void *vt;            // double4 view-frame vertices (both forms)
     const int4 *fvi;
     const double4 *vn;
@@ -51,10 +79,11 @@ void launch_realize(const ModelDev &m, cudaStream_t s);      // launch_realize_v
 void launch_realize_vf(const ModelDev &m, cudaStream_t s);   // vertices, facet normals and areas
 void launch_realize_vn(const ModelDev &m, cudaStream_t s);   // vertex normals (after _vf)
 void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, cudaStream_t s);
+// pdl: programmatic dependent launch (launch_k)
 void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt,
-                      cudaStream_t s);
+                      cudaStream_t s, bool pdl = false);
 void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const double4 *vt,
-                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s);
+                    FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s, bool pdl = false);
 
 struct Chi2Item { int frame; int start; int count; };
 struct Chi2Args {
@@ -183,7 +212,7 @@ constexpr size_t FUSED_STAGE_BYTES = 24 * 1024;
 bool chi2_summary_fits(int nframes, int max_frame_items);
 // counters: nframes + 1 ints, zero before the launch
 void launch_chi2_summary(const Chi2Args &ca, const FinalizeArgs &fa, const SummaryArgs &sa, int *counters,
-                         int fp32, cudaStream_t s);
+                         int fp32, cudaStream_t s, bool pdl = false);
 
 // raster_f64.cu / raster_f32.cu
 void launch_raster_f64(const RasterArgs &a, cudaStream_t s);

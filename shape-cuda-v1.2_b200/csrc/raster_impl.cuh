@@ -777,6 +777,7 @@ template <typename T, bool EXACT>
 __global__ void __launch_bounds__(RASTER_THREADS, sizeof(T) == 8 ? RASTER_MIN_BLOCKS_F64 : RASTER_MIN_BLOCKS)
 k_raster(RasterArgs a)
 {
+    grid_dep_wait();
     extern __shared__ __align__(32) unsigned char smem[];
     // dynamic shared memory: the ranked bin, then the staging area, which
     // holds the facet bitmap, its prefix counts and the raw bin while the bin
@@ -1194,8 +1195,10 @@ inline void launch_raster_t(const RasterArgs &a, cudaStream_t s)
     const int grid = (a.grid > 0 && a.grid < a.nwork) ? a.grid : a.nwork;
     // the FP64 form is exact by construction; the FP32 form runs its exact
     // variant on lightcurve views
-    if (sizeof(T) == 4 && a.exact) k_raster<T, true><<<grid, RASTER_THREADS, b.smem_bytes, s>>>(b);
-    else k_raster<T, false><<<grid, RASTER_THREADS, b.smem_bytes, s>>>(b);
+    if (sizeof(T) == 4 && a.exact)
+        launch_k(k_raster<T, true>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
+    else
+        launch_k(k_raster<T, false>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
 }
 
 }  // namespace shape
