@@ -880,7 +880,7 @@ __global__ void __launch_bounds__(CHI2_THREADS) k_chi2_summary(Chi2Args ca, Fina
                                                                int *counters)
 {
     __shared__ double red[CHI2_THREADS / 32][6];
-    __shared__ __align__(16) unsigned char stage[FUSED_STAGE_BYTES];
+    extern __shared__ __align__(16) unsigned char stage[];   // chi2_summary_smem bytes
     __shared__ int s_last;
     grid_dep_wait();
     double *s_part = reinterpret_cast<double *>(stage);
@@ -1060,20 +1060,25 @@ cudaError_t configure_summary()
     return cudaFuncSetAttribute(k_summary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SUMMARY_SMEM_MAX);
 }
 
+size_t chi2_summary_smem(int nframes, int max_frame_items)
+{
+    const size_t a = (size_t)nframes * 25, b = (size_t)max_frame_items * 6 * sizeof(double);
+    return ((a > b ? a : b) + 15) & ~(size_t)15;
+}
+
 bool chi2_summary_fits(int nframes, int max_frame_items)
 {
-    return nframes > 0 && (size_t)nframes * 25 <= FUSED_STAGE_BYTES &&
-           (size_t)max_frame_items * 6 * sizeof(double) <= FUSED_STAGE_BYTES;
+    return nframes > 0 && chi2_summary_smem(nframes, max_frame_items) <= FUSED_STAGE_BYTES;
 }
 
 void launch_chi2_summary(const Chi2Args &ca, const FinalizeArgs &fa, const SummaryArgs &sa, int *counters,
-                         int fp32, cudaStream_t s, bool pdl)
+                         int fp32, cudaStream_t s, bool pdl, size_t smem)
 {
     const int nwork = fa.nframes + ca.nitems;       // frame outputs, then chunks
     int blocks = nwork < 8 * 148 ? nwork : 8 * 148;
     if (blocks <= 0 || ca.nitems <= 0) return;
-    if (fp32) launch_k(k_chi2_summary<float>, dim3(blocks), dim3(CHI2_THREADS), 0, s, pdl, ca, fa, sa, counters);
-    else launch_k(k_chi2_summary<double>, dim3(blocks), dim3(CHI2_THREADS), 0, s, pdl, ca, fa, sa, counters);
+    if (fp32) launch_k(k_chi2_summary<float>, dim3(blocks), dim3(CHI2_THREADS), smem, s, pdl, ca, fa, sa, counters);
+    else launch_k(k_chi2_summary<double>, dim3(blocks), dim3(CHI2_THREADS), smem, s, pdl, ca, fa, sa, counters);
 }
 
 void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s)

@@ -221,6 +221,7 @@ int EngineImpl::finalize()
         bool every = true;
         for (const FrameHost &h : fh) { max_items = std::max(max_items, h.nitems); every = every && h.nitems > 0; }
         fused_chi2 = every && !chi2_items.empty() && chi2_summary_fits((int)fh.size(), max_items);
+        fused_smem = fused_chi2 ? chi2_summary_smem((int)fh.size(), max_items) : 0;
     }
     // lightcurve points: two views each (src/shape/calc_fits.c:1634-1716)
     const int LC_CHUNK = 4096;
@@ -700,7 +701,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     sa.baddiam = 0;
     sa.baddiam_logfactor = 0.0;
     sa.out = d_summary;
-    if (fused) launch_chi2_summary(ca, fa, sa, d_chi2_counters, f32 ? 1 : 0, s, fork);
+    if (fused) launch_chi2_summary(ca, fa, sa, d_chi2_counters, f32 ? 1 : 0, s, fork, fused_smem);
     else launch_summary(fa, sa, s);
     mark(7);
     CK(cudaGetLastError());

@@ -134,6 +134,7 @@ struct EngineImpl {
     double *d_o2pre = nullptr;        // per chi-square item: o2 partial (model independent)
     int *d_chi2_counters = nullptr;   // fused chi-square / summary: per-frame items done, frames done
     bool fused_chi2 = false;          // batched forms run k_chi2_summary
+    size_t fused_smem = 0;            // its dynamic shared memory
     FrameHost *d_fh = nullptr;
     shape_deldop_result *d_results = nullptr;
     double *d_set_delpp = nullptr, *d_set_doppp = nullptr, *d_dop_extra = nullptr;

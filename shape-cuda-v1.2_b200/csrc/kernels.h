@@ -206,13 +206,15 @@ cudaError_t configure_summary();
 void launch_summary(const FinalizeArgs &fa, const SummaryArgs &a, cudaStream_t s);
 
 // Chi-square partials + per-frame finalize + totals in one launch (the
-// batched forms). Its shared staging holds one frame's partials and then
-// every frame's terms; chi2_summary_fits says whether a dataset fits.
+// batched forms). Its shared staging (chi2_summary_smem bytes of dynamic
+// shared memory) holds one frame's partials and then every frame's terms;
+// chi2_summary_fits says whether a dataset fits in FUSED_STAGE_BYTES.
 constexpr size_t FUSED_STAGE_BYTES = 24 * 1024;
+size_t chi2_summary_smem(int nframes, int max_frame_items);
 bool chi2_summary_fits(int nframes, int max_frame_items);
 // counters: nframes + 1 ints, zero before the launch
 void launch_chi2_summary(const Chi2Args &ca, const FinalizeArgs &fa, const SummaryArgs &sa, int *counters,
-                         int fp32, cudaStream_t s, bool pdl = false);
+                         int fp32, cudaStream_t s, bool pdl, size_t smem);
 
 // raster_f64.cu / raster_f32.cu
 void launch_raster_f64(const RasterArgs &a, cudaStream_t s);

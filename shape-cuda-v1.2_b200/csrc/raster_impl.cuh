@@ -137,9 +137,10 @@ template <typename T> __device__ T radlaw_dev(const RadarLawDev &L, T c)
 // same staged facet: broadcasts, no bank conflicts). FP64 form, posvis's
 // own terms: p0 = (v00, v01, A, B), p1 = (den, C, D, v02),
 // p2 = (E, F, nx, ny). FP32 form, s, t and the depth above the first corner
-// as affine functions of the tile-relative pixel centre (x, y):
-// s = a0 + a1 x + a2 y, t = b0 + b1 x + b2 y, zr = c0 + c1 x + c2 y, with
-// p0 = (a0, a1, a2, b0), p1 = (b1, b2, c0, c1), p2 = (c2, v02, nx, ny).
+// as linear functions of the pixel centre's offset (dx, dy) from that
+// corner (tile-relative coordinates): s = a1 dx + a2 dy, t = b1 dx + b2 dy,
+// zr = c1 dx + c2 dy, with p0 = (v00, v01, a1, a2), p1 = (b1, b2, c1, c2),
+// p2 = (0, v02, nx, ny).
 template <typename T>
 struct Stage {
     typename Vec4<T>::type p0, p1, p2;
@@ -210,27 +211,27 @@ __device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage
         s.p1 = vec4<T>(den, C, D, p0.z);
         (void)ox; (void)oy;
     } else {
-        // the affine coefficients in FP64 from posvis's terms, rounded once
+        // the linear coefficients in FP64 from posvis's terms, rounded once
         const double A = p2.y - p1.y, B = p2.x - p1.x, C = p1.x - p0.x, D = p1.y - p0.y;
         const double Ez = p1.z - p0.z, Fz = p2.z - p1.z;
         const double den = 1.0 / (C * A - B * D);
         const double V0 = p0.x - ox, V1 = p0.y - oy;
-        const double a1 = den * A, a2 = -den * B, a0 = den * (B * V1 - A * V0);
-        const double b1 = -den * D, b2 = den * C, b0 = den * (D * V0 - C * V1);
-        const double c0 = Ez * a0 + Fz * b0, c1 = Ez * a1 + Fz * b1, c2 = Ez * a2 + Fz * b2;
-        s.p0 = vec4<T>((T)a0, (T)a1, (T)a2, (T)b0);
-        s.p1 = vec4<T>((T)b1, (T)b2, (T)c0, (T)c1);
-        E = (T)c2;       // p2 = (c2, v02, nx, ny)
+        const double a1 = den * A, a2 = -den * B;
+        const double b1 = -den * D, b2 = den * C;
+        const double c1 = Ez * a1 + Fz * b1, c2 = Ez * a2 + Fz * b2;
+        s.p0 = vec4<T>((T)V0, (T)V1, (T)a1, (T)a2);
+        s.p1 = vec4<T>((T)b1, (T)b2, (T)c1, (T)c2);
+        E = (T)0;        // p2 = (0, v02, nx, ny)
         F = (T)p0.z;
         // Bounds on the FP32 values' error at any pixel centre of the tile
-        // (x, y in [0, 16 kmpp)): 8 units of 2^-24 of the summed magnitudes
-        // of the terms (rounded coefficients, two fused multiply-adds, the
-        // depth's add); at least 1e-9, so a value past twice its bound
-        // also clears posvis's 1e-10 tolerance.
-        const double xs = 16.0 * g.kmpp, u = 8.0 / 16777216.0;
-        s.es = (float)fmax(1e-9, u * (fabs(a0) + (fabs(a1) + fabs(a2)) * xs));
-        s.et = (float)fmax(1e-9, u * (fabs(b0) + (fabs(b1) + fabs(b2)) * xs));
-        s.ez = (float)(u * (fabs(p0.z) + fabs(c0) + (fabs(c1) + fabs(c2)) * xs));
+        // (x, y in [0, 16 kmpp)): 8 units of 2^-24 of the terms' magnitudes
+        // (the offsets' rounding, the rounded coefficients, a product and a
+        // fused multiply-add; the depth's add); at least 1e-9, so a value
+        // past twice its bound also clears posvis's 1e-10 tolerance.
+        const double xs = 16.0 * g.kmpp + fabs(V0) + fabs(V1), u = 8.0 / 16777216.0;
+        s.es = (float)fmax(1e-9, u * (fabs(a1) + fabs(a2)) * xs);
+        s.et = (float)fmax(1e-9, u * (fabs(b1) + fabs(b2)) * xs);
+        s.ez = (float)(u * (fabs(p0.z) + (fabs(c1) + fabs(c2)) * xs));
     }
     s.f = f;
     if (g.smooth) {
@@ -771,8 +772,7 @@ __device__ inline unsigned long long warp_kmax(unsigned long long k)
 // The tile raster. EXACT (FP32 form, lightcurve views): a pixel with a
 // decision within FP32 error is redone by the FP64 form's rules, so facet
 // assignment, depth and the shadow test's inputs are the FP64 form's;
-// without it (radar views) the FP32 test's tolerance is the staged error
-// bound, which keeps pixels on shared edges covered.
+// without it (radar views) the FP32 test is posvis's with FP32 values.
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(RASTER_THREADS, sizeof(T) == 8 ? RASTER_MIN_BLOCKS_F64 : RASTER_MIN_BLOCKS)
 k_raster(RasterArgs a)
@@ -847,9 +847,10 @@ k_raster(RasterArgs a)
                 const auto p0 = s.p0, p1 = s.p1, p2 = s.p2;
                 const float4 be = *reinterpret_cast<const float4 *>(&s.bb);   // bb, es, et, ez
                 const bool inb = __vcmpgeu4(pxw, __float_as_uint(be.x)) == 0xffffffffu;   // pixel in the facet's bbox
-                sv = fmaf(p0.y, x0, fmaf(p0.z, x1, p0.x));
-                tv = fmaf(p1.x, x0, fmaf(p1.y, x1, p0.w));
-                zr = fmaf(p1.w, x0, fmaf(p2.x, x1, p1.z));
+                const T dx = x0 - p0.x, dy = x1 - p0.y;
+                sv = fmaf(p0.z, dx, p0.w * dy);
+                tv = fmaf(p1.x, dx, p1.y * dy);
+                zr = fmaf(p1.z, dx, p1.w * dy);
                 z = p2.y + zr;
                 const T es = be.y, et = be.z, est = es + et;
                 if constexpr (EXACT) {
@@ -862,7 +863,12 @@ k_raster(RasterArgs a)
                     if (!((z > zz) || (fac < 0))) return;
                     zze = be.w;
                 } else {
-                    const bool in = inb && (sv >= -es) && (sv <= 1 + es) && (tv >= -et) && (tv <= sv + est);
+                    // posvis's own tolerance: a wider one (the error bounds)
+                    // also covers pixels just outside the silhouette, which
+                    // measured worse than the rare pixel on a shared edge
+                    // that both facets' FP32 tests miss
+                    const bool in = inb && (sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL) &&
+                                    (tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL);
                     if (!(in && ((z > zz) || (fac < 0)))) return;
                 }
             }
