@@ -638,6 +638,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
             RasterArgs rr = ra, rl = ra;
             rr.nwork = work_radar;
             rr.grid = nonempty_radar;
+            rr.exact = fp32_exact;
             rl.work = d_work_sorted + work_radar;
             rl.nwork = (int)work.size() - work_radar;
             rl.grid = nonempty_lc;
@@ -1235,6 +1236,19 @@ int shape_engine_stage_times(shape_engine *h, int form, double *ms, int max)
     if (ce != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(ce));
     E.last_form = form;
     return n;
+}
+
+int shape_engine_set_fp32_exact(shape_engine *h, int exact)
+{
+    if (!h || (exact != 0 && exact != 1)) return shape::set_err(SHAPE_E_ARG, "set_fp32_exact: 0 or 1");
+    shape::EngineImpl &E = h->impl;
+    if (E.fp32_exact != exact && E.gexec[SHAPE_FORM_BATCHED_FP32]) {   // the captured graph has the other kernel
+        cudaSetDevice(E.device);
+        cudaGraphExecDestroy(E.gexec[SHAPE_FORM_BATCHED_FP32]);
+        E.gexec[SHAPE_FORM_BATCHED_FP32] = nullptr;
+    }
+    E.fp32_exact = exact;
+    return SHAPE_OK;
 }
 
 int shape_engine_set_bin_capacity(shape_engine *h, int cap)

@@ -1054,7 +1054,7 @@ k_raster(RasterArgs a)
         if constexpr (sizeof(T) == 4) {
             if (fac < 0) {
                 z64 = -SHAPE_HUGENUMBER;
-            } else if (g.kind != VIEW_RADAR) {
+            } else if (EXACT || g.kind != VIEW_RADAR) {
                 const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
                 z64 = facet_depth64(vt, a.fvi[fac], (double)pi * g.kmpp, (double)pj * g.kmpp);
             }

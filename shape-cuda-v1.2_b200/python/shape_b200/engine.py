@@ -109,6 +109,7 @@ def load_library(path=LIB_PATH):
     L.shape_engine_last_time_ms.argtypes = [vp, P(C.c_double)]
     L.shape_engine_stage_times.argtypes = [vp, C.c_int, cd.dptr, C.c_int]
     L.shape_engine_set_bin_capacity.argtypes = [vp, C.c_int]
+    L.shape_engine_set_fp32_exact.argtypes = [vp, C.c_int]
     L.shape_engine_get_tuning.argtypes = [vp, P(C.c_int), C.c_int]
     L.shape_engine_bestfit.argtypes = [vp, P(FitParam), C.c_int, P(FitOptions), P(FitResult), cd.dptr, C.c_int]
     L.shape_engine_get_scale.argtypes = [vp, C.c_int, P(C.c_double)]
@@ -216,6 +217,11 @@ class Engine:
 
     def set_bin_capacity(self, cap):
         _chk(self.L.shape_engine_set_bin_capacity(self.h, int(cap)))
+
+    def set_fp32_exact(self, exact=True):
+        """Batched FP32 form: radar views by the exact raster variant too
+        (facet and depth maps equal to the FP64 form's; slower raster)."""
+        _chk(self.L.shape_engine_set_fp32_exact(self.h, 1 if exact else 0))
 
     def tuning(self):
         out = (C.c_int * 8)()

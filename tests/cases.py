@@ -77,3 +77,10 @@ def radar_law(kind):
     L.diff_R, L.diff_C = 0.08, 1.3
     L.qs_R, L.qs_C, L.qs_cos_cutoff = 0.05, 4.0, math.cos(60 * math.pi / 180)
     return L
+
+
+def scaled_model(m, sc):
+    """A copy of model m with scale factors sc (the oracle reads them from the model)."""
+    mm = m.copy()
+    mm.scale = np.array([float(x) for x in sc])
+    return mm

@@ -93,6 +93,33 @@ def test_config2_fp32_tolerance(cuda_device):
     e.close()
 
 
+@pytest.mark.parametrize("case", ["c1", "c2_12"])
+def test_fp32_exact_option_radar_maps(cuda_device, case):
+    """shape_engine_set_fp32_exact(1): radar views' facet and depth maps in
+    the batched FP32 form equal the oracle's (pixels with a decision within
+    FP32 error redone by the FP64 rules, FP64 depths), at jittered scale
+    factors too; chi-square within the FP32 bar."""
+    m, p, ds = cases.c1() if case == "c1" else cases.c2(12)
+    e = eng.make_engine(m, p, deldops=[ds])
+    e.keep_pos(True)
+    e.set_fp32_exact(True)
+    rng = np.random.default_rng(11)
+    for trial in range(3):
+        sc = [1.0, 1.0, 1.0] if trial == 0 else list(1.0 + 0.02 * rng.uniform(-1, 1, 3))
+        for j in range(3):
+            e.set_scale(j, sc[j])
+        mm = cases.scaled_model(m, sc)
+        o = cases.orc().eval_deldop(mm, ds, p, keep_pos=True)
+        s = e.evaluate(eng.FORM_BATCHED_FP32)
+        for f in range(ds.nframes):
+            pg, po = e.pos(f), o["pos"][f]
+            assert np.array_equal(pg["f"], po["f"]), (trial, f, "facet map")
+            assert np.array_equal(pg["z"], po["z"]), (trial, f, "z map")
+        chi2_o = sum(r["chi2"] for r in o["results"])
+        assert abs(s["chi2"] - chi2_o) <= FP32_CHI2_RTOL * chi2_o, (trial, s["chi2"], chi2_o)
+    e.close()
+
+
 def test_lightcurve_fp64_exact(cuda_device):
     m, p, sets = cases.c3(12, 2)
     o = cases.orc()
