@@ -514,6 +514,17 @@ def main():
     kpe = E.kernels_per_eval(form)
     stages = E.stage_times(form if form != eng.FORM_PLAIN_FP64 else eng.FORM_BATCHED_FP64)
 
+    # the FP32 form with shape_engine_set_fp32_exact(1) (facet and depth maps
+    # of every view equal to the FP64 form's), a short run beside the default
+    exact = None
+    if form == eng.FORM_BATCHED_FP32 and not lcs:
+        E.set_fp32_exact(True)
+        chi32x = E.evaluate(form)["chi2"]
+        ex_ms, _ = run(form, max(20, min(args.steps, 100)), 3, False)
+        E.set_fp32_exact(False)
+        exact = {"frame_evals_per_s": nu / (statistics.mean(ex_ms) / 1e3), "ms_per_step": statistics.mean(ex_ms),
+                 "dchi2_rel_fp32_vs_fp64": abs(chi32x - chi64) / abs(chi64)}
+
     total_dev = sum(dev_ms)
     total_host = sum(host_ms)
     units_all = ws * nu
@@ -555,6 +566,7 @@ def main():
                    "dchi2_rel_fp32_vs_fp64": dchi,
                    "plain_fp64_frame_evals_per_s": plain_rate,
                    "batched_over_plain_fp64": value / ws / plain_rate,
+                   "fp32_exact_option": exact,
                    "p50_ms": statistics.median(dev_ms), "p99_ms": float(np.percentile(dev_ms, 99)),
                    "stage_ms": stages,
                    "step_algorithmic_bytes": step_bytes,
