@@ -803,9 +803,11 @@ __device__ void summary_totals(const SummaryArgs &a, Term term)
 }
 
 // One item's chi-square partial sums (the body of k_chi2_partials), left by
-// thread 0 in part[0..5]. With a.o2pre set, o2 is the item's precomputed
-// partial and obs / 1/var are read only where the fit is nonzero: a zero
-// fit bin adds exact zeros to m2 and om, so the sums keep their values.
+// thread 0 in part[0..5]: each thread sums its bins in order, the threads'
+// sums merge with compensation (warp shuffles, then the block's warps in
+// order). With a.o2pre set, o2 is the item's precomputed partial and obs /
+// 1/var are read only where the fit is nonzero: a zero fit bin adds exact
+// zeros to m2 and om, so the sums keep their values.
 template <typename T>
 __device__ void chi2_item_partials(const Chi2Args &a, int it, const Chi2Item &item, double (*red)[6], double *part)
 {
@@ -814,27 +816,32 @@ __device__ void chi2_item_partials(const Chi2Args &a, int it, const Chi2Item &it
     const T *fit = static_cast<const T *>(a.fit) + base;
     const double *obs = a.obs + base, *oov = a.oov + base;
     const bool pre = a.o2pre != nullptr;
-    KSum o2 = {0, 0}, m2 = {0, 0}, om = {0, 0};
-    double ob[CHI2_ITEMS], wv[CHI2_ITEMS], ft[CHI2_ITEMS];
+    T ft[CHI2_ITEMS];
+    double ob[CHI2_ITEMS], wv[CHI2_ITEMS];
 #pragma unroll
     for (int j = 0; j < CHI2_ITEMS; j++) {
         const int k = threadIdx.x + j * CHI2_THREADS;
-        ft[j] = (k < item.count) ? (double)fit[k] : 0.0;
+        ft[j] = (k < item.count) ? fit[k] : (T)0;
     }
 #pragma unroll
     for (int j = 0; j < CHI2_ITEMS; j++) {
         const int k = threadIdx.x + j * CHI2_THREADS;
-        const bool in = (k < item.count) && (!pre || ft[j] != 0.0);
+        const bool in = (k < item.count) && (!pre || ft[j] != (T)0);
         ob[j] = in ? obs[k] : 0.0;
         wv[j] = in ? oov[k] : 0.0;
     }
+    // a thread's own bins (at most CHI2_ITEMS) summed in bin order in plain
+    // FP64; the compensated sums start where the threads' sums merge
+    double so2 = 0.0, sm2 = 0.0, som = 0.0;
 #pragma unroll
     for (int j = 0; j < CHI2_ITEMS; j++) {
         if (threadIdx.x + j * CHI2_THREADS >= item.count) break;
-        if (!pre) o2.add(ob[j] * ob[j] * wv[j]);
-        m2.add(ft[j] * ft[j] * wv[j]);
-        om.add(ft[j] * ob[j] * wv[j]);
+        const double f = (double)ft[j];
+        if (!pre) so2 += ob[j] * ob[j] * wv[j];
+        sm2 += f * f * wv[j];
+        som += f * ob[j] * wv[j];
     }
+    KSum o2 = {so2, 0}, m2 = {sm2, 0}, om = {som, 0};
     for (int off = 16; off > 0; off >>= 1) {
         o2.merge(shfl_ksum(o2, off));
         m2.merge(shfl_ksum(m2, off));
