@@ -600,33 +600,39 @@ __device__ inline void red_row_f32(float4 *base, const float (&w)[FAST_COLS], fl
 // FP32 delay-Doppler scatter without a shared-memory accumulator: the same
 // weights as pixel_dd_scatter's fast path, added to the fit image in HBM by
 // 16-byte vector reductions (at most 2 rows x 3 per pixel instead of 16
-// scalar atomics); footprints beyond FAST_ROWS x FAST_COLS take the generic
-// path with scalar atomics.
+// scalar atomics); footprints beyond FAST_ROWS x FAST_COLS and frames with
+// other responses take the generic path with scalar atomics.
 __device__ inline void pixel_dd_scatter_f32_direct(const RasterArgs &a, const FrameGeom &g, const DDC<float> &k,
                                             float cose, const PixDD<float> &d, float *fit)
 {
     const int nr = d.idel_max - d.idel_min + 1, nc = d.idop_max - d.idop_min + 1;
-    if (nr > FAST_ROWS || nc > FAST_COLS) {
+    // the vector path serves the common responses (delay: tri2 of the
+    // scaled offset, as LONG_ORIG or spb = 1 give; Doppler: one point per
+    // pixel, nsinc2 = 1), written out without the general responses'
+    // branches; other frames and larger footprints take the general path
+    const bool lean = (g.nsinc2 == 1) && (g.codemethod == SHAPE_CODE_LONG_ORIG || g.spb == 1);
+    if (!lean || nr > FAST_ROWS || nc > FAST_COLS) {
         pixel_dd_scatter<float>(a, g, k, cose, d, fit, 1, 1, g.ndop);
         return;
     }
-    float s2u = 0.0f;
-    if (g.nsinc2 == 1) {
-        const float su = sinf(3.141592653589793f * d.dfrac);
-        s2u = su * su;
-    }
+    const float su = sinf(3.141592653589793f * d.dfrac);
+    const float s2u = su * su;
     const float rl = radlaw_dev<float>(a.laws[g.law], cose) * k.kmpp * k.kmpp * d.codefactor;
     float dc[FAST_ROWS], pc[FAST_COLS];
     float sdel = 0.0f, sdop = 0.0f;
     const float ddel0 = d.ddel0, ddop0 = d.ddop0;
+    // del_resp / dop_resp of these cases (delay offset over spb/stride for
+    // LONG_ORIG, over 1 for spb = 1)
+    const float sos = (g.codemethod == SHAPE_CODE_LONG_ORIG) ? k.spb_over_stride : 1.0f;
 #pragma unroll
     for (int r = 0; r < FAST_ROWS; r++) {
-        dc[r] = (r < nr) ? del_resp<float>(g, k, d.delPOS, ddel0 - (float)r, d.idel_min + r) : 0.0f;
+        dc[r] = (r < nr) ? tri2<float>(__fdividef(ddel0 - (float)r, sos)) : 0.0f;
         if (r < nr) sdel += dc[r];
     }
 #pragma unroll
     for (int c = 0; c < FAST_COLS; c++) {
-        pc[c] = (c < nc) ? dop_resp<float>(g, k, d.dopPOS, ddop0 - (float)c, s2u, d.idop_min + c) : 0.0f;
+        const float t = fabsf(3.141592653589793f * (ddop0 - (float)c));
+        pc[c] = (c < nc) ? ((t > 1.0e-4f) ? __fdividef(s2u, t * t) : 1.0f) : 0.0f;
         if (c < nc) sdop += pc[c];
     }
     const float amp = __fdividef(rl, sdel * sdop);

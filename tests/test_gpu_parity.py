@@ -178,6 +178,24 @@ def test_codemethods_fp64(cuda_device, codemethod, spb, stride, nsinc2):
     e.close()
 
 
+@pytest.mark.parametrize("codemethod,spb,stride,nsinc2", [
+    (0, 1, 1, 1), (2, 1, 1, 1), (2, 2, 1, 2), (2, 3, 1, 3), (1, 2, 2, 1), (0, 4, 2, 2)])
+def test_codemethods_fp32(cuda_device, codemethod, spb, stride, nsinc2):
+    """Batched FP32 over the code methods: the vector path (LONG_ORIG or
+    spb = 1, nsinc2 = 1) and the general path (the others) within the FP32
+    chi-square bar."""
+    m = cases.c2_model()
+    p = synth.eval_params(nsinc2=nsinc2, sinc2width=7)
+    ds = cases.small_frames(m, p, 3, (61, 101), codemethod=codemethod, spb=spb, stride=stride)
+    ds.set.dopfftlen = 64
+    o = cases.orc().eval_deldop(m, ds, p)
+    chi2_o = sum(r["chi2"] for r in o["results"])
+    e = eng.make_engine(m, p, deldops=[ds])
+    s = e.evaluate(eng.FORM_BATCHED_FP32)
+    assert abs(s["chi2"] - chi2_o) <= FP32_CHI2_RTOL * chi2_o, (s["chi2"], chi2_o)
+    e.close()
+
+
 @pytest.mark.parametrize("law", [2, 3, 4, 5, 6, 7])
 def test_radar_laws_fp64(cuda_device, law):
     m = cases.c2_model()
