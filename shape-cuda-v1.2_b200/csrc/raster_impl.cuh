@@ -534,15 +534,32 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
         T dc[FAST_ROWS], pc[FAST_COLS];
         T sdel = 0, sdop = 0;
         const T ddel0 = delPOS - (T)idel_min, ddop0 = dopPOS - (T)idop_min;
+        // the common responses (LONG_ORIG or spb = 1, nsinc2 = 1) written
+        // out with del_resp / dop_resp's own operations, so the same values
+        if (g.nsinc2 == 1 && (g.codemethod == SHAPE_CODE_LONG_ORIG || g.spb == 1)) {
+            const T sos = (g.codemethod == SHAPE_CODE_LONG_ORIG) ? k.spb_over_stride : (T)1;
 #pragma unroll
-        for (int r = 0; r < FAST_ROWS; r++) {
-            dc[r] = (r < nr) ? del_resp<T>(g, k, delPOS, ddel0 - (T)r, idel_min + r) : (T)0;
-            if (r < nr) sdel += dc[r];
-        }
+            for (int r = 0; r < FAST_ROWS; r++) {
+                dc[r] = (r < nr) ? tri2<T>((ddel0 - (T)r) / sos) : (T)0;
+                if (r < nr) sdel += dc[r];
+            }
 #pragma unroll
-        for (int c = 0; c < FAST_COLS; c++) {
-            pc[c] = (c < nc) ? dop_resp<T>(g, k, dopPOS, ddop0 - (T)c, s2u, idop_min + c) : (T)0;
-            if (c < nc) sdop += pc[c];
+            for (int c = 0; c < FAST_COLS; c++) {
+                const T t = fabs((T)3.141592653589793 * (ddop0 - (T)c));
+                pc[c] = (c < nc) ? ((t > (T)1.0e-4) ? s2u / (t * t) : (T)1.0) : (T)0;
+                if (c < nc) sdop += pc[c];
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < FAST_ROWS; r++) {
+                dc[r] = (r < nr) ? del_resp<T>(g, k, delPOS, ddel0 - (T)r, idel_min + r) : (T)0;
+                if (r < nr) sdel += dc[r];
+            }
+#pragma unroll
+            for (int c = 0; c < FAST_COLS; c++) {
+                pc[c] = (c < nc) ? dop_resp<T>(g, k, dopPOS, ddop0 - (T)c, s2u, idop_min + c) : (T)0;
+                if (c < nc) sdop += pc[c];
+            }
         }
         // sum of del_c*dop_c over the footprint = (sum del_c) * (sum dop_c)
         // (src/shape/pos2deldop.c:462-466)
