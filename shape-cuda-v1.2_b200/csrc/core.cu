@@ -133,6 +133,31 @@ __global__ void k_xform(const FrameGeom *__restrict__ geoms, const double4 *__re
     store_vt(vt, g.vt_base + i, t[0], t[1], t[2]);
 }
 
+// The same transform of vertices realized on the fly (realize_vertex, the
+// operations k_realize_vf uses), so the batched graph can run it beside
+// k_realize_vf instead of after it: the view-frame vertices are identical.
+template <typename T4>
+__global__ void k_xform_realize(const FrameGeom *__restrict__ geoms, const double *__restrict__ a,
+                                const double *__restrict__ u, const double *__restrict__ r,
+                                const double *__restrict__ scale, int nv, T4 *__restrict__ vt)
+{
+    grid_dep_wait();
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const FrameGeom &g = geoms[blockIdx.y];
+    double4 x = realize_vertex(i, a, u, r, scale);
+    double t[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        t[k] = 0.0;
+        t[k] += g.oa[3 * k + 0] * x.x;
+        t[k] += g.oa[3 * k + 1] * x.y;
+        t[k] += g.oa[3 * k + 2] * x.z;
+        t[k] += 0.0;
+    }
+    store_vt(vt, g.vt_base + i, t[0], t[1], t[2]);
+}
+
 // -------------------------------------------------------------- binning
 
 // Facet culling, bounding box, outbnd flag and POSrect bookkeeping of
@@ -989,6 +1014,12 @@ void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, 
     if (blocks > 4 * 148) blocks = 4 * 148;
     if (blocks < (nviews + 255) / 256) blocks = (nviews + 255) / 256;
     k_reset_state<<<blocks, 256, 0, s>>>(st, nviews, bin_count, ntiles);
+}
+
+void launch_xform_realize_f64(const FrameGeom *g, int nviews, const ModelDev &m, double4 *vt, cudaStream_t s)
+{
+    dim3 grid((m.nv + 255) / 256, nviews);
+    k_xform_realize<double4><<<grid, 256, 0, s>>>(g, m.a, m.u, m.r, m.scale, m.nv, vt);
 }
 
 void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt, cudaStream_t s,

@@ -426,6 +426,7 @@ int EngineImpl::finalize()
 
     if (!stream2) {
         CK(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&stream3, cudaStreamNonBlocking));
         for (auto &e : evf) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     CK(configure_raster_f64());
@@ -512,18 +513,22 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     cudaStream_t s = stream;
     const bool f32 = (form == SHAPE_FORM_BATCHED_FP32);
     auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], s); };
-    // The batched forms run the state reset, the image clears and the vertex
-    // normals on a side branch (stream2) that rejoins before binning and
-    // before the raster; the plain form and stage timing run them in line.
+    // The batched forms run two side branches beside the view transform
+    // (which realizes its vertices on the fly): the state reset and image
+    // clears (stream2), and realize with the facet and vertex normals
+    // (stream3); binning waits for the facet normals and the reset, the
+    // raster for the vertex normals. The plain form and stage timing run
+    // them in line.
     const bool fork = (form != SHAPE_FORM_PLAIN_FP64) && !marks;
     cudaStream_t sr = fork ? stream2 : s;
     if (fork) {
         CK(cudaEventRecord(evf[0], s));
         CK(cudaStreamWaitEvent(stream2, evf[0], 0));
-    }
-    if (fork) {
-        launch_realize_vf(md, s);
-        CK(cudaEventRecord(evf[1], s));
+        CK(cudaStreamWaitEvent(stream3, evf[0], 0));
+        launch_realize_vf(md, stream3);
+        CK(cudaEventRecord(evf[1], stream3));        // vertices, facet normals and areas
+        launch_realize_vn(md, stream3);
+        CK(cudaEventRecord(evf[3], stream3));        // vertex normals
     } else {
         launch_realize(md, s);
     }
@@ -538,12 +543,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         CK(cudaMemsetAsync(d_ovf, 0, sizeof(double) * dop_frames.size() * DOP_MAXOVERFLOW, sr));
     const bool fused = fused_chi2 && form != SHAPE_FORM_PLAIN_FP64;
     if (fused) CK(cudaMemsetAsync(d_chi2_counters, 0, sizeof(int) * (fh.size() + 1), sr));
-    if (fork) {
-        CK(cudaEventRecord(evf[2], stream2));        // reset and clears done
-        CK(cudaStreamWaitEvent(stream2, evf[1], 0));  // facet normals exist
-        launch_realize_vn(md, stream2);
-        CK(cudaEventRecord(evf[3], stream2));        // vertex normals done
-    }
+    if (fork) CK(cudaEventRecord(evf[2], stream2));   // reset and clears done
     mark(1);
 
     RasterArgs ra;
@@ -619,9 +619,13 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         // dependent launch of the one before it (stage timing keeps plain
         // launches so its events separate the stages)
         const bool pdl = fork;
-        launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s, pdl);
+        if (fork) launch_xform_realize_f64(d_geoms, nviews, md, d_vt64, s);
+        else launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
         mark(2);
-        if (fork) CK(cudaStreamWaitEvent(s, evf[2], 0));
+        if (fork) {
+            CK(cudaStreamWaitEvent(s, evf[1], 0));
+            CK(cudaStreamWaitEvent(s, evf[2], 0));
+        }
         launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s, pdl);
         if (fork) CK(cudaStreamWaitEvent(s, evf[3], 0));
         mark(3);

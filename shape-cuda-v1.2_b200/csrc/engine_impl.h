@@ -69,7 +69,8 @@ struct EngineImpl {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // side branch of the batched graph (state reset, image clears, vertex
     // normals) and its fork / join events
-    cudaStream_t stream2 = nullptr;
+    cudaStream_t stream2 = nullptr;   // batched graph branches: state reset and clears
+    cudaStream_t stream3 = nullptr;   // ... and realize (vertices, facet and vertex normals)
     cudaEvent_t evf[4] = {nullptr, nullptr, nullptr, nullptr};
     float last_ms = 0.f;
 
@@ -177,6 +178,7 @@ struct EngineImpl {
         for (auto &e : evf)
             if (e) { cudaEventDestroy(e); e = nullptr; }
         if (stream2) { cudaStreamDestroy(stream2); stream2 = nullptr; }
+        if (stream3) { cudaStreamDestroy(stream3); stream3 = nullptr; }
         if (stream) { cudaStreamDestroy(stream); stream = nullptr; }
     }
 

@@ -82,6 +82,8 @@ void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, 
 // pdl: programmatic dependent launch (launch_k)
 void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt,
                       cudaStream_t s, bool pdl = false);
+// the transform of vertices realized on the fly (no dependency on k_realize_vf)
+void launch_xform_realize_f64(const FrameGeom *g, int nviews, const ModelDev &m, double4 *vt, cudaStream_t s);
 void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m, const double4 *vt,
                     FrameState *st, int *bin_count, int2 *bin_ids, int cap, cudaStream_t s, bool pdl = false);
 
