@@ -139,8 +139,10 @@ int shape_engine_get_realized(shape_engine *e, double *x, double *vn, double *fn
  * between stages, and writes the stage times in ms: [0] realize, [1] state
  * reset and image clears, [2] view transforms, [3] facet binning,
  * [4] tile raster + delay-Doppler synthesis, [5] chi-square partials,
- * [6] lightcurve shadowing + photometry, [7] finalize + summary.
- * Returns the number of stages written. */
+ * [6] lightcurve shadowing + photometry, [7] finalize + summary. Datasets
+ * whose chi-square partials, frame results and totals run as one kernel
+ * (every radar frame's chunk list fits its staging) time that kernel in [7]
+ * and leave [5] empty. Returns the number of stages written. */
 int shape_engine_stage_times(shape_engine *e, int form, double *ms, int max);
 
 /* Facet-bin capacity per 16x16 POS tile. 0 (default) lets finalize size it

@@ -283,6 +283,9 @@ class Engine:
     STAGES = ["realize", "reset", "transform", "bin", "raster_synth", "chi2", "lc_photo", "finalize"]
 
     def stage_times(self, form=FORM_BATCHED_FP32):
+        """Stage times in ms of one batched evaluation (shape_engine_stage_times);
+        with the fused chi-square kernel its time is under "finalize" and
+        "chi2" is empty."""
         if isinstance(form, str):
             form = FORMS[form]
         ms = np.zeros(8)
