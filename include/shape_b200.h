@@ -286,6 +286,19 @@ typedef struct shape_server_stats {
     int instances_created, instances_evicted;
     double peak_hbm_bytes;     /* peak device bytes held by instances during the run */
 } shape_server_stats;
+/* Spin realization of one dataset (replaces realize_spin + inteuler,
+ * src/shape/realize_spin.c:41-285, src/shape/inteuler.c:85-117, for
+ * principal-axis rotators): for each of n view epochs t[k] (days), the
+ * ecliptic -> body matrix ae[9k..9k+8] (row-major) and the total spin vector
+ * in ecliptic coordinates spin_out[3k..3k+2] = orbspin[3k..] + ae^T (w + omegaoff),
+ * w being the body-frame spin vector evolved from t0 with the impulses met
+ * on the way. angleoff / omegaoff: the dataset's angle and spin offsets.
+ * Host code; the values equal the reference's (same operations and order).
+ * A non-principal-axis state returns SHAPE_E_UNSUPPORTED, more than
+ * SHAPE_MAX_IMPULSES impulses SHAPE_E_ARG. */
+int shape_realize_spin(const shape_spin_state *spin, const double angleoff[3], const double omegaoff[3], int n,
+                       const double *t, const double *orbspin, double *ae, double *spin_out);
+
 int shape_server_create(int device, size_t hbm_budget_bytes, int max_slots, shape_server **out);
 void shape_server_destroy(shape_server *s);
 /* engine: a configured engine (model and datasets added; it need not be

@@ -154,6 +154,23 @@ typedef struct shape_doppler_set {
 } shape_doppler_set;
 
 /* One calculated lightcurve epoch (struct crvrend_t, src/shape/shape2.h:1344-1356). */
+/* A model's spin state (struct spin_t, src/shape/shape2.h:1007-1020), values
+ * only: Euler angles of the principal axes at epoch t0, the body-frame spin
+ * vector and its rate of change, spin impulses (body frame, applied at their
+ * epochs) and a libration of the third Euler angle. */
+#define SHAPE_MAX_IMPULSES 10     /* MAXIMP, src/shape/shape2.h:1003 */
+typedef struct shape_spin_state {
+    int pa;                       /* 1: principal-axis rotator */
+    double t0;                    /* epoch of the initial conditions (days) */
+    double angle[3];              /* Euler angles phi, theta, psi (rad) */
+    double omega[3];              /* spin vector, body coordinates (rad/day) */
+    double omegadot[3];           /* its rate of change (rad/day^2) */
+    int n_impulse;                /* spin impulses, at most SHAPE_MAX_IMPULSES */
+    double t_impulse[SHAPE_MAX_IMPULSES];
+    double impulse[SHAPE_MAX_IMPULSES][3];
+    double lib_amp, lib_freq, lib_phase;   /* psi libration: amplitude, frequency, phase */
+} shape_spin_state;
+
 typedef struct shape_lghtcrv_point {
     int pos_n;
     double km_per_pixel;

@@ -569,3 +569,68 @@ double ref_brent_abs(double ax, double bx, double cx, ref_objfn fn, double tol, 
 {
     return brent_abs(ax, bx, cx, fn, tol, abstol, xmin);
 }
+
+
+/* The reference's spin realization (realize_spin, src/shape/realize_spin.c)
+ * for n one-view frames of a single delay-Doppler set with view epochs t[]
+ * and orbital spin contributions orbspin[3n]: the check of
+ * shape_realize_spin. Writes each view's ae (row-major) and total spin. */
+int ref_realize_spin_frames(const shape_spin_state *sp, const double angleoff[3], const double omegaoff[3],
+                            int n, const double *t, const double *orbspin, double *ae, double *spin_out)
+{
+    if (sp->n_impulse < 0 || sp->n_impulse > MAXIMP) return -1;
+    struct par_t *par = calloc(1, sizeof *par);
+    struct mod_t *mod = calloc(1, sizeof *mod);
+    struct dat_t *dat = calloc(1, sizeof *dat);
+    par->int_method = BRUTE;
+    par->int_abstol = 1e-7;
+    mod->spin.pa = (unsigned char)sp->pa;
+    mod->spin.t0 = sp->t0;
+    for (int j = 0; j < 3; j++) {
+        mod->spin.angle[j].val = sp->angle[j];
+        mod->spin.omega[j].val = sp->omega[j];
+        mod->spin.omegadot[j].val = sp->omegadot[j];
+        mod->spin.inertia[j].val = 1.0;
+    }
+    mod->spin.n_impulse = sp->n_impulse;
+    for (int k = 0; k < sp->n_impulse; k++) {
+        mod->spin.t_impulse[k] = sp->t_impulse[k];
+        for (int j = 0; j < 3; j++) mod->spin.impulse[k][j].val = sp->impulse[k][j];
+    }
+    mod->spin.lib_amp.val = sp->lib_amp;
+    mod->spin.lib_freq.val = sp->lib_freq;
+    mod->spin.lib_phase.val = sp->lib_phase;
+    dat->nsets = 1;
+    dat->set = calloc(1, sizeof(struct set_t));
+    struct set_t *set = &dat->set[0];
+    set->type = DELAY;
+    for (int j = 0; j < 3; j++) {
+        set->angleoff[j].val = angleoff[j];
+        set->angleoff[j].state = 'c';
+        set->omegaoff[j].val = omegaoff[j];
+        set->omegaoff[j].state = 'c';
+    }
+    struct deldop_t *dd = &set->desc.deldop;
+    dd->nframes = n;
+    dd->nviews = 1;
+    dd->frame = calloc((size_t)(n > 0 ? n : 1), sizeof(struct deldopfrm_t));
+    for (int f = 0; f < n; f++) {
+        dd->frame[f].view = calloc(1, sizeof(struct deldopview_t));
+        dd->frame[f].view[0].t = t[f];
+        for (int j = 0; j < 3; j++) dd->frame[f].view[0].orbspin[j] = orbspin[3 * f + j];
+    }
+    realize_spin(par, mod, dat);
+    for (int f = 0; f < n; f++) {
+        for (int i = 0; i < 3; i++) {
+            for (int j = 0; j < 3; j++) ae[9 * f + 3 * i + j] = dd->frame[f].view[0].ae[i][j];
+            spin_out[3 * f + i] = dd->frame[f].view[0].spin[i];
+        }
+        free(dd->frame[f].view);
+    }
+    free(dd->frame);
+    free(dat->set);
+    free(dat);
+    free(mod);
+    free(par);
+    return 0;
+}

@@ -33,6 +33,7 @@ UNITS = [
     ("noalloc.cu", ["-fmad=false"]),
     ("fit.cu", ["-fmad=false"]),
     ("server.cu", ["-fmad=false"]),
+    ("spin.cu", ["-fmad=false"]),
 ]
 
 HEADERS = ["engine_internal.h", "engine_impl.h", "kernels.h", "raster_impl.cuh"]

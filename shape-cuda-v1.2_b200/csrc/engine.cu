@@ -828,7 +828,8 @@ int shape_abi_sizes(size_t *out, int max)
     size_t v[] = {sizeof(shape_model_desc), sizeof(shape_radar_law), sizeof(shape_optical_law),
                   sizeof(shape_eval_params), sizeof(shape_deldop_frame), sizeof(shape_deldop_set),
                   sizeof(shape_lghtcrv_point), sizeof(shape_lghtcrv_set), sizeof(shape_deldop_result),
-                  sizeof(shape_eval_summary), sizeof(shape_doppler_frame), sizeof(shape_doppler_set)};
+                  sizeof(shape_eval_summary), sizeof(shape_doppler_frame), sizeof(shape_doppler_set),
+                  sizeof(shape_spin_state)};
     int n = (int)(sizeof v / sizeof v[0]);
     for (int i = 0; i < n && i < max; i++) out[i] = v[i];
     return n;

@@ -81,6 +81,20 @@ class DopplerSet(C.Structure):
     ]
 
 
+MAX_IMPULSES = 10
+
+
+class SpinState(C.Structure):
+    """shape_spin_state (include/shape_types.h)."""
+    _fields_ = [
+        ("pa", C.c_int), ("t0", C.c_double),
+        ("angle", C.c_double * 3), ("omega", C.c_double * 3), ("omegadot", C.c_double * 3),
+        ("n_impulse", C.c_int), ("t_impulse", C.c_double * MAX_IMPULSES),
+        ("impulse", (C.c_double * 3) * MAX_IMPULSES),
+        ("lib_amp", C.c_double), ("lib_freq", C.c_double), ("lib_phase", C.c_double),
+    ]
+
+
 class LghtcrvPoint(C.Structure):
     _fields_ = [
         ("pos_n", C.c_int), ("km_per_pixel", C.c_double),

@@ -110,6 +110,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_stage_times.argtypes = [vp, C.c_int, cd.dptr, C.c_int]
     L.shape_engine_set_bin_capacity.argtypes = [vp, C.c_int]
     L.shape_engine_set_fp32_exact.argtypes = [vp, C.c_int]
+    L.shape_realize_spin.argtypes = [P(cd.SpinState), cd.dptr, cd.dptr, C.c_int, cd.dptr, cd.dptr, cd.dptr,
+                                     cd.dptr]
     L.shape_engine_get_tuning.argtypes = [vp, P(C.c_int), C.c_int]
     L.shape_engine_bestfit.argtypes = [vp, P(FitParam), C.c_int, P(FitOptions), P(FitResult), cd.dptr, C.c_int]
     L.shape_engine_get_scale.argtypes = [vp, C.c_int, P(C.c_double)]
@@ -348,6 +350,36 @@ class Engine:
         _chk(self.L.shape_engine_get_realized(self.h, cd.as_dptr(x), cd.as_dptr(vn), cd.as_dptr(fn),
                                               cd.as_dptr(area)))
         return {"x": x, "vn": vn, "fn": fn, "area": area}
+
+
+def spin_state(pa=1, t0=0.0, angle=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), omegadot=(0.0, 0.0, 0.0),
+               impulses=(), lib=(0.0, 0.0, 0.0)):
+    """A shape_spin_state; impulses: (epoch, (wx, wy, wz)) pairs."""
+    s = cd.SpinState()
+    s.pa, s.t0 = int(pa), float(t0)
+    for j in range(3):
+        s.angle[j], s.omega[j], s.omegadot[j] = angle[j], omega[j], omegadot[j]
+    s.n_impulse = len(impulses)
+    for k, (te, w) in enumerate(impulses[:cd.MAX_IMPULSES]):
+        s.t_impulse[k] = te
+        for j in range(3):
+            s.impulse[k][j] = w[j]
+    s.lib_amp, s.lib_freq, s.lib_phase = lib
+    return s
+
+
+def realize_spin(spin, t, orbspin=None, angleoff=(0.0, 0.0, 0.0), omegaoff=(0.0, 0.0, 0.0)):
+    """shape_realize_spin: (ae [n,3,3] ecliptic -> body, total spin [n,3]
+    ecliptic) of a principal-axis spin state at view epochs t."""
+    L = load_library()
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    n = t.size
+    orb = np.zeros((n, 3)) if orbspin is None else np.ascontiguousarray(orbspin, dtype=np.float64).reshape(n, 3)
+    ae, sp = np.zeros((n, 3, 3)), np.zeros((n, 3))
+    ao, oo = np.array(angleoff, dtype=np.float64), np.array(omegaoff, dtype=np.float64)
+    _chk(L.shape_realize_spin(C.byref(spin), cd.as_dptr(ao), cd.as_dptr(oo), n, cd.as_dptr(t), cd.as_dptr(orb),
+                              cd.as_dptr(ae), cd.as_dptr(sp)))
+    return ae, sp
 
 
 def make_engine(model, params, deldops=(), lghtcrvs=(), device=0, dopplers=()):

@@ -41,6 +41,7 @@ def test_struct_layouts_match_compiler():
     assert C.sizeof(eng.EvalSummary) == sizes[len(eng.ABI_ORDER)]
     for k, name in enumerate(("shape_doppler_frame", "shape_doppler_set")):
         assert C.sizeof(cd.STRUCTS[name]) == sizes[len(eng.ABI_ORDER) + 1 + k], name
+    assert C.sizeof(cd.SpinState) == sizes[len(eng.ABI_ORDER) + 3], "shape_spin_state"
 
 
 def test_errors_without_device_are_reported():
