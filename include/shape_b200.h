@@ -287,15 +287,22 @@ typedef struct shape_server_stats {
     double peak_hbm_bytes;     /* peak device bytes held by instances during the run */
 } shape_server_stats;
 /* Spin realization of one dataset (replaces realize_spin + inteuler,
- * src/shape/realize_spin.c:41-285, src/shape/inteuler.c:85-117, for
- * principal-axis rotators): for each of n view epochs t[k] (days), the
- * ecliptic -> body matrix ae[9k..9k+8] (row-major) and the total spin vector
- * in ecliptic coordinates spin_out[3k..3k+2] = orbspin[3k..] + ae^T (w + omegaoff),
- * w being the body-frame spin vector evolved from t0 with the impulses met
- * on the way. angleoff / omegaoff: the dataset's angle and spin offsets.
- * Host code; the values equal the reference's (same operations and order).
- * A non-principal-axis state returns SHAPE_E_UNSUPPORTED, more than
- * SHAPE_MAX_IMPULSES impulses SHAPE_E_ARG. */
+ * src/shape/realize_spin.c:41-285, src/shape/inteuler.c:85-210): for each of
+ * n view epochs t[k] (days), the ecliptic -> body matrix ae[9k..9k+8]
+ * (row-major) and the total spin vector in ecliptic coordinates
+ * spin_out[3k..3k+2] = orbspin[3k..] + ae^T (w + omegaoff), w being the
+ * body-frame spin vector evolved from t0 with the impulses met on the way.
+ * angleoff / omegaoff: the dataset's angle and spin offsets. Host code.
+ * Principal-axis states: the reference's values (same operations and order).
+ * Non-principal-axis states: Euler's equations and the orientation
+ * integrated between impulse epochs by an adaptive Dormand-Prince 5(4)
+ * method at local error 1e-13, in time measured from each interval's start
+ * (the reference's brute-force integration, with its own integrator; its
+ * periodic method is not provided): within ~1e-12 of the exact solution
+ * over days, where the reference's stepping of the absolute epoch leaves
+ * it ~1e-8 away. More than
+ * SHAPE_MAX_IMPULSES impulses, or a non-positive moment of inertia for a
+ * non-principal-axis state, return SHAPE_E_ARG. */
 int shape_realize_spin(const shape_spin_state *spin, const double angleoff[3], const double omegaoff[3], int n,
                        const double *t, const double *orbspin, double *ae, double *spin_out);
 

@@ -169,6 +169,7 @@ typedef struct shape_spin_state {
     double t_impulse[SHAPE_MAX_IMPULSES];
     double impulse[SHAPE_MAX_IMPULSES][3];
     double lib_amp, lib_freq, lib_phase;   /* psi libration: amplitude, frequency, phase */
+    double inertia[3];            /* principal moments of inertia (non-principal-axis rotation) */
 } shape_spin_state;
 
 typedef struct shape_lghtcrv_point {

@@ -204,7 +204,7 @@ class Reference:
                                             cd.dptr, cd.iptr, P(cd.DeldopResult)]
         L.ref_set_scale.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.ref_realize_spin_frames.argtypes = [P(cd.SpinState), cd.dptr, cd.dptr, C.c_int, cd.dptr, cd.dptr,
-                                              cd.dptr, cd.dptr]
+                                              cd.dptr, cd.dptr, C.c_double]
         L.ref_set_r.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.ref_realize.argtypes = [C.c_void_p]
         L.ref_evaluate.restype = C.c_double

@@ -574,23 +574,26 @@ double ref_brent_abs(double ax, double bx, double cx, ref_objfn fn, double tol, 
 /* The reference's spin realization (realize_spin, src/shape/realize_spin.c)
  * for n one-view frames of a single delay-Doppler set with view epochs t[]
  * and orbital spin contributions orbspin[3n]: the check of
- * shape_realize_spin. Writes each view's ae (row-major) and total spin. */
+ * shape_realize_spin. Non-principal-axis states use the reference's
+ * brute-force integration with tolerance int_abstol. Writes each view's ae
+ * (row-major) and total spin. */
 int ref_realize_spin_frames(const shape_spin_state *sp, const double angleoff[3], const double omegaoff[3],
-                            int n, const double *t, const double *orbspin, double *ae, double *spin_out)
+                            int n, const double *t, const double *orbspin, double *ae, double *spin_out,
+                            double int_abstol)
 {
     if (sp->n_impulse < 0 || sp->n_impulse > MAXIMP) return -1;
     struct par_t *par = calloc(1, sizeof *par);
     struct mod_t *mod = calloc(1, sizeof *mod);
     struct dat_t *dat = calloc(1, sizeof *dat);
     par->int_method = BRUTE;
-    par->int_abstol = 1e-7;
+    par->int_abstol = int_abstol;
     mod->spin.pa = (unsigned char)sp->pa;
     mod->spin.t0 = sp->t0;
     for (int j = 0; j < 3; j++) {
         mod->spin.angle[j].val = sp->angle[j];
         mod->spin.omega[j].val = sp->omega[j];
         mod->spin.omegadot[j].val = sp->omegadot[j];
-        mod->spin.inertia[j].val = 1.0;
+        mod->spin.inertia[j].val = sp->inertia[j] > 0.0 ? sp->inertia[j] : 1.0;
     }
     mod->spin.n_impulse = sp->n_impulse;
     for (int k = 0; k < sp->n_impulse; k++) {

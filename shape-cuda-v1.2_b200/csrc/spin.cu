@@ -1,9 +1,13 @@
-// Spin realization of principal-axis rotators on the host: the per-view
-// steps of realize_spin (src/shape/realize_spin.c:41-285) with inteuler's
-// principal-axis branch (src/shape/inteuler.c:85-117) and euler2mat
-// (src/util/euler.c). Each quantity is computed with the reference's
-// operations in the reference's order, so the matrices and spin vectors
-// are the reference's to the last bit.
+// Spin realization on the host: the per-view steps of realize_spin
+// (src/shape/realize_spin.c:41-285) with inteuler (src/shape/inteuler.c) and
+// euler2mat (src/util/euler.c). Principal-axis rotators: each quantity is
+// computed with the reference's operations in the reference's order, so the
+// matrices and spin vectors are the reference's to the last bit.
+// Non-principal-axis rotators: Euler's equations for the body-frame spin
+// vector and the body-frame motion of the ecliptic axes, integrated between
+// impulse epochs with an adaptive Dormand-Prince 5(4) method (Dormand and
+// Prince 1980) to a relative error of 1e-13; the reference integrates the
+// same equations with its own stepper, so values agree to that accuracy.
 #include <cmath>
 
 #include "engine_impl.h"
@@ -63,6 +67,84 @@ int impulse_path(const shape_spin_state &sp, double t, double *te, double (*imp)
     return k + 1;
 }
 
+// Torque-free rotation: y = (w in body coordinates, then the three ecliptic
+// axes in body coordinates, the columns of ae). Euler's equations for w;
+// each fixed axis a moves in the body frame as da/dt = a x w.
+void npa_rhs(const double I[3], const double *y, double *dy)
+{
+    dy[0] = ((I[1] - I[2]) / I[0]) * y[1] * y[2];
+    dy[1] = ((I[2] - I[0]) / I[1]) * y[2] * y[0];
+    dy[2] = ((I[0] - I[1]) / I[2]) * y[0] * y[1];
+    for (int c = 3; c < 12; c += 3) {
+        dy[c + 0] = y[c + 1] * y[2] - y[c + 2] * y[1];
+        dy[c + 1] = y[c + 2] * y[0] - y[c + 0] * y[2];
+        dy[c + 2] = y[c + 0] * y[1] - y[c + 1] * y[0];
+    }
+}
+
+// Integrates y from ta to tb (either direction) with the Dormand-Prince
+// 5(4) pair and step-size control on the local error estimate. Time runs
+// from 0 to tb - ta (exact for epochs within a factor of two of each
+// other): stepping the absolute epoch (~2.5e6 days, ulp ~5e-10 day) would
+// drift the integrated span by the rounding of every step. Returns false if
+// it takes more than a bounded number of steps.
+bool npa_integrate(const double I[3], double *y, double ta, double tb)
+{
+    // stage weights (the right-hand side does not depend on time, so the
+    // stage nodes are not needed)
+    static const double a21 = 1.0 / 5;
+    static const double a31 = 3.0 / 40, a32 = 9.0 / 40;
+    static const double a41 = 44.0 / 45, a42 = -56.0 / 15, a43 = 32.0 / 9;
+    static const double a51 = 19372.0 / 6561, a52 = -25360.0 / 2187, a53 = 64448.0 / 6561, a54 = -212.0 / 729;
+    static const double a61 = 9017.0 / 3168, a62 = -355.0 / 33, a63 = 46732.0 / 5247, a64 = 49.0 / 176,
+                        a65 = -5103.0 / 18656;
+    static const double b1 = 35.0 / 384, b3 = 500.0 / 1113, b4 = 125.0 / 192, b5 = -2187.0 / 6784,
+                        b6 = 11.0 / 84;
+    // differences of the fifth- and fourth-order weights (error estimate)
+    static const double e1 = 35.0 / 384 - 5179.0 / 57600, e3 = 500.0 / 1113 - 7571.0 / 16695,
+                        e4 = 125.0 / 192 - 393.0 / 640, e5 = -2187.0 / 6784 + 92097.0 / 339200,
+                        e6 = 11.0 / 84 - 187.0 / 2100, e7 = -1.0 / 40;
+    const double tol = 1e-13, span = tb - ta;
+    if (span == 0.0) return true;
+    const double dir = span > 0 ? 1.0 : -1.0;
+    double t = 0.0, h = dir * std::fmin(std::fabs(span), 1e-3);
+    double k1[12], k2[12], k3[12], k4[12], k5[12], k6[12], k7[12], yt[12], yn[12];
+    npa_rhs(I, y, k1);
+    for (long it = 0; it < 50000000L; it++) {
+        if (dir * (t + h - span) > 0) h = span - t;
+        for (int i = 0; i < 12; i++) yt[i] = y[i] + h * a21 * k1[i];
+        npa_rhs(I, yt, k2);
+        for (int i = 0; i < 12; i++) yt[i] = y[i] + h * (a31 * k1[i] + a32 * k2[i]);
+        npa_rhs(I, yt, k3);
+        for (int i = 0; i < 12; i++) yt[i] = y[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+        npa_rhs(I, yt, k4);
+        for (int i = 0; i < 12; i++) yt[i] = y[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i] + a54 * k4[i]);
+        npa_rhs(I, yt, k5);
+        for (int i = 0; i < 12; i++)
+            yt[i] = y[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i] + a64 * k4[i] + a65 * k5[i]);
+        npa_rhs(I, yt, k6);
+        for (int i = 0; i < 12; i++)
+            yn[i] = y[i] + h * (b1 * k1[i] + b3 * k3[i] + b4 * k4[i] + b5 * k5[i] + b6 * k6[i]);
+        npa_rhs(I, yn, k7);
+        // error relative to the spin magnitude (w) and to 1 (unit axes)
+        const double wmag = std::sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]) + 1e-300;
+        double err = 0.0;
+        for (int i = 0; i < 12; i++) {
+            const double ei = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i] + e6 * k6[i] + e7 * k7[i]);
+            const double sc = tol * (i < 3 ? wmag : 1.0);
+            err = std::fmax(err, std::fabs(ei) / sc);
+        }
+        if (err <= 1.0) {
+            t += h;
+            for (int i = 0; i < 12; i++) { y[i] = yn[i]; k1[i] = k7[i]; }
+            if (dir * (t - span) >= 0) return true;
+        }
+        const double f = (err == 0.0) ? 5.0 : std::fmin(5.0, std::fmax(0.2, 0.9 * std::pow(err, -0.2)));
+        h *= f;
+    }
+    return false;
+}
+
 }  // namespace
 
 extern "C" int shape_realize_spin(const shape_spin_state *spin, const double angleoff[3], const double omegaoff[3],
@@ -72,29 +154,48 @@ extern "C" int shape_realize_spin(const shape_spin_state *spin, const double ang
         return shape::report_error(SHAPE_E_ARG, "realize_spin: null argument");
     if (spin->n_impulse < 0 || spin->n_impulse > SHAPE_MAX_IMPULSES)
         return shape::report_error(SHAPE_E_ARG, "realize_spin: more than SHAPE_MAX_IMPULSES impulses");
-    if (!spin->pa)
-        return shape::report_error(SHAPE_E_UNSUPPORTED, "realize_spin: non-principal-axis rotation");
+    if (!spin->pa && !(spin->inertia[0] > 0.0 && spin->inertia[1] > 0.0 && spin->inertia[2] > 0.0))
+        return shape::report_error(SHAPE_E_ARG, "realize_spin: non-positive moment of inertia");
     // the dataset's angle offsets are added to the model's Euler angles
     const double phi = spin->angle[0] + angleoff[0], theta = spin->angle[1] + angleoff[1];
     const double psi0 = spin->angle[2] + angleoff[2];
     for (int v = 0; v < n; v++) {
         double te[SHAPE_MAX_IMPULSES + 2], imp[SHAPE_MAX_IMPULSES + 2][3];
         const int ne = impulse_path(*spin, t[v], te, imp);
-        const double dt = te[ne - 1] - te[0];
-        // principal-axis kinematics: psi advances with the z spin, its drift
-        // and the libration; z impulses add to the rate from their epochs
-        double psi = psi0 + spin->omega[2] * dt + 0.5 * spin->omegadot[2] * dt * dt +
-                     spin->lib_amp * std::sin(spin->lib_freq * dt + spin->lib_phase);
-        double w[3];
-        for (int i = 0; i < 2; i++) w[i] = spin->omega[i] + spin->omegadot[i] * dt;
-        w[2] = spin->omega[2] + spin->omegadot[2] * dt +
-               spin->lib_amp * spin->lib_freq * std::cos(spin->lib_freq * dt + spin->lib_phase);
-        for (int k = 0; k < ne; k++) {
-            psi += imp[k][2] * (te[ne - 1] - te[k]);
-            w[2] += imp[k][2];
+        double m[3][3], w[3];
+        if (!spin->pa) {
+            // non-principal-axis: integrate from t0 one impulse interval at a
+            // time (intervals shorter than 1e-6 day are skipped, as the
+            // reference does), adding each impulse after its interval
+            euler_zxz(m, phi, theta, psi0);
+            double y[12];
+            for (int j = 0; j < 3; j++) y[j] = spin->omega[j];
+            for (int j = 0; j < 3; j++)
+                for (int i = 0; i < 3; i++) y[3 + 3 * j + i] = m[i][j];
+            for (int k = 0; k + 1 < ne; k++) {
+                if (std::fabs(te[k + 1] - te[k]) >= 1.0e-6 &&
+                    !npa_integrate(spin->inertia, y, te[k], te[k + 1]))
+                    return shape::report_error(SHAPE_E_STATE, "realize_spin: integration did not converge");
+                for (int j = 0; j < 3; j++) y[j] += imp[k + 1][j];
+            }
+            for (int j = 0; j < 3; j++) w[j] = y[j];
+            for (int j = 0; j < 3; j++)
+                for (int i = 0; i < 3; i++) m[i][j] = y[3 + 3 * j + i];
+        } else {
+            const double dt = te[ne - 1] - te[0];
+            // principal-axis kinematics: psi advances with the z spin, its drift
+            // and the libration; z impulses add to the rate from their epochs
+            double psi = psi0 + spin->omega[2] * dt + 0.5 * spin->omegadot[2] * dt * dt +
+                         spin->lib_amp * std::sin(spin->lib_freq * dt + spin->lib_phase);
+            for (int i = 0; i < 2; i++) w[i] = spin->omega[i] + spin->omegadot[i] * dt;
+            w[2] = spin->omega[2] + spin->omegadot[2] * dt +
+                   spin->lib_amp * spin->lib_freq * std::cos(spin->lib_freq * dt + spin->lib_phase);
+            for (int k = 0; k < ne; k++) {
+                psi += imp[k][2] * (te[ne - 1] - te[k]);
+                w[2] += imp[k][2];
+            }
+            euler_zxz(m, phi, theta, psi);
         }
-        double m[3][3];
-        euler_zxz(m, phi, theta, psi);
         // the dataset's spin offsets (body frame), then body -> ecliptic
         // (transpose of ae), plus the orbital contribution
         for (int j = 0; j < 3; j++) w[j] += omegaoff[j];

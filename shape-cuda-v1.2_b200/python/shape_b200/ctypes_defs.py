@@ -92,6 +92,7 @@ class SpinState(C.Structure):
         ("n_impulse", C.c_int), ("t_impulse", C.c_double * MAX_IMPULSES),
         ("impulse", (C.c_double * 3) * MAX_IMPULSES),
         ("lib_amp", C.c_double), ("lib_freq", C.c_double), ("lib_phase", C.c_double),
+        ("inertia", C.c_double * 3),
     ]
 
 

@@ -353,8 +353,9 @@ class Engine:
 
 
 def spin_state(pa=1, t0=0.0, angle=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), omegadot=(0.0, 0.0, 0.0),
-               impulses=(), lib=(0.0, 0.0, 0.0)):
-    """A shape_spin_state; impulses: (epoch, (wx, wy, wz)) pairs."""
+               impulses=(), lib=(0.0, 0.0, 0.0), inertia=(1.0, 1.0, 1.0)):
+    """A shape_spin_state; impulses: (epoch, (wx, wy, wz)) pairs; inertia:
+    principal moments (non-principal-axis states)."""
     s = cd.SpinState()
     s.pa, s.t0 = int(pa), float(t0)
     for j in range(3):
@@ -365,6 +366,8 @@ def spin_state(pa=1, t0=0.0, angle=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), omega
         for j in range(3):
             s.impulse[k][j] = w[j]
     s.lib_amp, s.lib_freq, s.lib_phase = lib
+    for j in range(3):
+        s.inertia[j] = inertia[j]
     return s
 
 

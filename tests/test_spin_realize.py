@@ -1,9 +1,11 @@
-"""shape_realize_spin (host spin realization of principal-axis rotators)
-against the reference's own realize_spin (oracle/_ref/libshape_ref.so, via
-ref_realize_spin_frames), on the CPU: body matrices and total spin vectors
-equal to the last bit, over seeded random spin states with spin-rate drift,
+"""shape_realize_spin (host spin realization) against the reference's own
+realize_spin (oracle/_ref/libshape_ref.so, via ref_realize_spin_frames), on
+the CPU. Principal-axis rotators: body matrices and total spin vectors equal
+to the last bit, over seeded random spin states with spin-rate drift,
 libration, spin impulses before and after the initial epoch, dataset angle
-and spin offsets, and epochs at t0 and at an impulse epoch."""
+and spin offsets, and epochs at t0 and at an impulse epoch. Non-principal-
+axis rotators: within 1e-7 of the reference's brute-force integration, and
+conserving energy and angular momentum to 1e-11."""
 import ctypes as C
 
 import numpy as np
@@ -19,14 +21,14 @@ def ref():
     return Reference()
 
 
-def _reference(ref, spin, t, orb, angleoff, omegaoff):
+def _reference(ref, spin, t, orb, angleoff, omegaoff, int_abstol=1e-7):
     n = len(t)
     ae, sp = np.zeros((n, 3, 3)), np.zeros((n, 3))
     t = np.ascontiguousarray(t, dtype=np.float64)
     orb = np.ascontiguousarray(orb, dtype=np.float64)
     ao, oo = np.array(angleoff, dtype=np.float64), np.array(omegaoff, dtype=np.float64)
     rc = ref.lib.ref_realize_spin_frames(C.byref(spin), cd.as_dptr(ao), cd.as_dptr(oo), n, cd.as_dptr(t),
-                                         cd.as_dptr(orb), cd.as_dptr(ae), cd.as_dptr(sp))
+                                         cd.as_dptr(orb), cd.as_dptr(ae), cd.as_dptr(sp), int_abstol)
     assert rc == 0
     return ae, sp
 
@@ -85,9 +87,60 @@ def test_realize_spin_no_offsets_is_the_model_rotation(ref):
     assert np.array_equal(ae, ae_r) and np.array_equal(sp, sp_r)
 
 
+@pytest.mark.parametrize("seed", range(4))
+def test_realize_spin_npa_matches_reference_integration(ref, seed):
+    """Non-principal-axis rotators: the Dormand-Prince integration against
+    the reference's brute-force (Bulirsch-Stoer) integration of the same
+    equations at tolerance 1e-12: matrices to 1e-7, spin vectors to 1e-7
+    relative over spans of up to 3 days (tens of rotations), impulses
+    included. The reference steps the absolute epoch (~2.5e6 days), whose
+    rounding leaves it ~1e-8 from the exact solution whatever its tolerance;
+    the invariants test below holds this side to 1e-11."""
+    rng = np.random.default_rng(1700 + seed)
+    t0 = 2458000.0
+    inertia = (1.0, rng.uniform(1.05, 1.4), rng.uniform(1.45, 1.9))
+    omega = tuple(rng.normal(0, 1.0, 3) + np.array([0.0, 0.0, 2 * np.pi / 0.4]))
+    imps = [(t0 + 0.7, tuple(rng.normal(0, 0.05, 3)))] if seed % 2 else []
+    spin = eng.spin_state(0, t0, tuple(rng.uniform(0, 2 * np.pi, 3)), omega, (0, 0, 0), imps, (0, 0, 0), inertia)
+    t = np.sort(t0 + rng.uniform(-3, 3, 10))
+    t[0] = t0
+    orb = rng.normal(0, 1e-2, (10, 3))
+    ao, oo = tuple(rng.normal(0, 1e-2, 3)), tuple(rng.normal(0, 1e-4, 3))
+    ae_r, sp_r = _reference(ref, spin, t, orb, ao, oo, int_abstol=1e-12)
+    ae_g, sp_g = eng.realize_spin(spin, t, orb, ao, oo)
+    assert np.abs(ae_g - ae_r).max() < 1e-7, np.abs(ae_g - ae_r).max()
+    assert np.abs(sp_g - sp_r).max() < 1e-7 * np.abs(sp_r).max(), np.abs(sp_g - sp_r).max()
+    for m in ae_g:
+        assert np.allclose(m @ m.T, np.eye(3), atol=1e-10)
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_realize_spin_npa_invariants(seed):
+    """Torque-free rotation conserves the kinetic energy sum(I w^2) and the
+    angular momentum in the ecliptic frame, ae^T (I w): both to 1e-11
+    relative over 20 days (hundreds of rotations), forward and backward
+    from t0, for a tumbling state well away from principal-axis rotation."""
+    rng = np.random.default_rng(2100 + seed)
+    t0 = 2459000.5
+    inertia = np.array([1.0, rng.uniform(1.1, 1.5), rng.uniform(1.6, 2.2)])
+    omega = rng.normal(0, 1.0, 3) * 2 * np.pi / rng.uniform(0.2, 1.0)
+    spin = eng.spin_state(0, t0, tuple(rng.uniform(0, 2 * np.pi, 3)), tuple(omega), (0, 0, 0), (), (0, 0, 0),
+                          tuple(inertia))
+    t = np.concatenate([[t0], t0 + rng.uniform(-10, 10, 8)])
+    ae, sp = eng.realize_spin(spin, t)
+    w = np.einsum("kij,kj->ki", ae, sp)                 # body-frame spin
+    energy = (inertia * w * w).sum(1)
+    L = np.einsum("kji,kj->ki", ae, inertia * w)       # ecliptic angular momentum
+    assert np.allclose(w[0], omega, rtol=0, atol=1e-12 * np.abs(omega).max())
+    assert np.abs(energy / energy[0] - 1).max() < 1e-11
+    assert np.abs(L - L[0]).max() < 1e-11 * np.linalg.norm(L[0])
+    for m in ae:
+        assert np.allclose(m @ m.T, np.eye(3), atol=1e-11)
+
+
 def test_realize_spin_errors():
     L = eng.load_library()
-    spin = eng.spin_state(0, 0.0, (0, 0, 0), (0, 0, 1.0))          # non-principal-axis
+    spin = eng.spin_state(0, 0.0, (0, 0, 0), (0, 0, 1.0), inertia=(1.0, 0.0, 1.0))   # bad moments
     with pytest.raises(eng.EngineError):
         eng.realize_spin(spin, [0.5])
     spin = eng.spin_state(1, 0.0, (0, 0, 0), (0, 0, 1.0))
