@@ -157,6 +157,27 @@ int shape_engine_set_bin_capacity(shape_engine *e, int cap);
  * depths on radar views too, so every view's facet and depth maps are the
  * FP64 form's (slower raster). Takes effect at the next evaluation. */
 int shape_engine_set_fp32_exact(shape_engine *e, int exact);
+
+/* A new view for radar frame global_frame (delay-Doppler and Doppler frames
+ * numbered across sets in the order they were added), for spin, pole and
+ * delay-correction trials without rebuilding the engine: ae, oe, spin,
+ * deloff and dopoff as in shape_deldop_frame (deloff is ignored for Doppler
+ * frames). The frame's view-dependent constants (posvis's observer <- body
+ * matrix, src/shape/posvis.c:101-122; pos2deldop's Doppler axes, footprint
+ * extents, shifts and badradar term, src/shape/pos2deldop.c:218-288) are
+ * recomputed on the host exactly as at finalize and copied to the device on
+ * the engine's stream, so the next evaluation of every form sees them and
+ * captured graphs stay valid; the results equal those of an engine built
+ * with the new view. Bin capacities keep their tuning (a tile that now
+ * overflows takes the ordered full-scan path). Before finalize the frame's
+ * descriptor is updated. Workloads a server already took from this engine
+ * keep their views. */
+int shape_engine_set_frame_view(shape_engine *e, int global_frame, const double ae[9], const double oe[9],
+                                const double spin[3], double deloff, double dopoff);
+/* The same for lightcurve point `point` (numbered across sets): its ae, oe
+ * and se (src/shape/calc_fits.c:1634-1716). */
+int shape_engine_set_point_view(shape_engine *e, int point, const double ae[9], const double oe[9],
+                                const double se[9]);
 /* Tuning state after finalize: [0] bin capacity, [1] largest tile count of
  * the dry run, [2] non-empty tiles, [3] tiles, [4] tile width in pixels.
  * Returns the number of values written. */

@@ -81,6 +81,69 @@ static int radar_law_index(EngineImpl &E, const shape_radar_law &L)
     return (int)E.laws.size() - 1;
 }
 
+// View-dependent constants of radar frame F (src/shape/pos2deldop.c:218-275,
+// src/shape/posvis.c:101-122): the observer <- body matrix, the Doppler
+// axes and footprint extents, the delay and Doppler shifts and a Doppler
+// spectrum's overflow origin; dx = the Doppler extent term of the frame's
+// bin limits; the badradar flag and log-factor of a footprint wider than
+// MAXBINS. g.nsinc2, g.sinc2width and g.dop1d must be set.
+static void radar_view_geom(FrameGeom &g, FrameHost &h, double &dx, const shape_deldop_frame &F,
+                            const shape_deldop_set &S)
+{
+    mul_bt(g.oa, F.oe, F.ae);
+    double w[3];
+    mv(w, F.oe, F.spin);
+    double dopfact = S.dopscale * SHAPE_KM2HZFACT * F.km_per_pixel * S.Ftx / S.dop_per_pixel;
+    g.ax = -w[1] * dopfact;
+    g.ay = w[0] * dopfact;
+    double km2Hz = sqrt(g.ax * g.ax + g.ay * g.ay) * S.dop_per_pixel / F.km_per_pixel;
+    dx = 0.0;
+    if (w[0] != 0.0 || w[1] != 0.0)
+        dx = km2Hz * 0.5 * F.km_per_pixel * sqrt(w[0] * w[0] + w[1] * w[1]) /
+             std::max(fabs(w[0]), fabs(w[1]));
+    g.xincr = g.ax / g.nsinc2;
+    g.yincr = g.ay / g.nsinc2;
+    g.dopdiff_bl = -(g.nsinc2 - 1) * (g.xincr + g.yincr) / 2;
+    g.dopdiff_max = (g.nsinc2 - 1) * (fabs(g.xincr) + fabs(g.yincr)) / 2;
+    g.delshift = F.delcom_vig + F.deloff;
+    g.dopshift = F.dopcom_vig + F.dopoff + 0.0;
+    g.dopDC_vig = F.dopDC_vig;
+    if (g.dop1d) g.idop0 = DOP_MAXOVERFLOW / 2 - (int)floor(g.dopshift + 0.5);
+    h.badradar = 0;
+    h.badradar_logfactor = 0.0;
+    if (2 * g.dopdiff_max + g.sinc2width + 1 > SHAPE_MAXBINS) {
+        h.badradar = 1;
+        h.badradar_logfactor = log((2 * g.dopdiff_max + g.sinc2width + 1) / SHAPE_MAXBINS);
+    }
+}
+
+// View-dependent constants of lightcurve point P (src/shape/calc_fits.c:
+// 1634-1716): the observer and sun views' body matrices, the sun direction
+// in observer coordinates and the observer -> sun transform of posmask.
+static void lc_view_geom(FrameGeom &go, FrameGeom &gs, LcPointDev &pd, const shape_lghtcrv_point &P)
+{
+    mul_bt(go.oa, P.oe, P.ae);
+    double us[3] = {0.0, 0.0, 1.0};
+    mtv(us, P.se, us);
+    mv(us, P.oe, us);
+    go.usrc[0] = us[0]; go.usrc[1] = us[1]; go.usrc[2] = us[2];
+    mul_bt(gs.oa, P.se, P.ae);
+    mul_bt(pd.so, P.se, P.oe);
+}
+
+// The float copies of a view's constants that the FP32 raster reads.
+static void view_float_consts(FrameGeom &g)
+{
+    const double fv[FDD_N] = {g.delfact, g.delshift, g.ax, g.ay, g.dopshift, g.const1, g.const2,
+                              g.one_over_spb, g.xincr, g.yincr, g.dopdiff_bl, g.dopdiff_max,
+                              g.dopDC_vig, g.dopfftlen, g.kmpp, g.sinc2width / 2.0,
+                              (double)g.spb_over_stride, (double)g.stride, (double)g.spb_sq,
+                              (double)g.nsinc2_sq};
+    for (int k = 0; k < FDD_N; k++) g.fdd[k] = (float)fv[k];
+    for (int k = 0; k < 9; k++) g.foa[k] = (float)g.oa[k];
+    for (int k = 0; k < 3; k++) g.foa[9 + k] = (float)g.usrc[k];
+}
+
 int EngineImpl::finalize()
 {
     if (!have_model) return set_err(SHAPE_E_STATE, "finalize: no model set");
@@ -111,14 +174,7 @@ int EngineImpl::finalize()
         for (int t = 0; t < g.tiles_x * g.tiles_x; t++) work.push_back(make_int2((int)geoms.size(), t));
         tile_base += g.tiles_x * g.tiles_x;
         pos_base += (long long)g.side * g.side;
-        const double fv[FDD_N] = {g.delfact, g.delshift, g.ax, g.ay, g.dopshift, g.const1, g.const2,
-                                  g.one_over_spb, g.xincr, g.yincr, g.dopdiff_bl, g.dopdiff_max,
-                                  g.dopDC_vig, g.dopfftlen, g.kmpp, g.sinc2width / 2.0,
-                                  (double)g.spb_over_stride, (double)g.stride, (double)g.spb_sq,
-                                  (double)g.nsinc2_sq};
-        for (int k = 0; k < FDD_N; k++) g.fdd[k] = (float)fv[k];
-        for (int k = 0; k < 9; k++) g.foa[k] = (float)g.oa[k];
-        for (int k = 0; k < 3; k++) g.foa[9 + k] = (float)g.usrc[k];
+        view_float_consts(g);
         geoms.push_back(g);
     };
 
@@ -137,7 +193,6 @@ int EngineImpl::finalize()
             const shape_deldop_frame &F = frames[fi];
             FrameGeom g;
             memset(&g, 0, sizeof g);
-            mul_bt(g.oa, F.oe, F.ae);
             g.kind = VIEW_RADAR;
             g.smooth = params.pos_smooth;
             g.ndel = F.ndel;
@@ -159,45 +214,23 @@ int EngineImpl::finalize()
             // a Doppler frame's single row: delPOS = z*0 + 1 = 1 exactly, so its
             // delay response tri2(0) is 1 and its weights are pos2doppler's
             g.delfact = dd[s].doppler ? 0.0 : -SHAPE_KM2US / S.del_per_pixel;
-            double w[3];
-            mv(w, F.oe, F.spin);
-            double dopfact = S.dopscale * SHAPE_KM2HZFACT * F.km_per_pixel * S.Ftx / S.dop_per_pixel;
-            g.ax = -w[1] * dopfact;
-            g.ay = w[0] * dopfact;
-            double km2Hz = sqrt(g.ax * g.ax + g.ay * g.ay) * S.dop_per_pixel / F.km_per_pixel;
-            double dx = 0.0;
-            if (w[0] != 0.0 || w[1] != 0.0)
-                dx = km2Hz * 0.5 * F.km_per_pixel * sqrt(w[0] * w[0] + w[1] * w[1]) /
-                     std::max(fabs(w[0]), fabs(w[1]));
-            dop_extra.push_back(dx);
             g.nsinc2 = params.nsinc2;
             g.nsinc2_sq = params.nsinc2 * params.nsinc2;
             g.sinc2width = params.sinc2width;
-            g.xincr = g.ax / params.nsinc2;
-            g.yincr = g.ay / params.nsinc2;
-            g.dopdiff_bl = -(params.nsinc2 - 1) * (g.xincr + g.yincr) / 2;
-            g.dopdiff_max = (params.nsinc2 - 1) * (fabs(g.xincr) + fabs(g.yincr)) / 2;
-            g.delshift = F.delcom_vig + F.deloff;
-            g.dopshift = F.dopcom_vig + F.dopoff + 0.0;
-            g.dopDC_vig = F.dopDC_vig;
             g.dopfftlen = S.dopfftlen;
             g.law = law;
             g.frame_index = fi;
             g.dop1d = dd[s].doppler;
-            if (g.dop1d) {
-                g.idop0 = DOP_MAXOVERFLOW / 2 - (int)floor(g.dopshift + 0.5);
-                g.ovf_base = (long long)dop_frames.size() * DOP_MAXOVERFLOW;
-            }
+            if (g.dop1d) g.ovf_base = (long long)dop_frames.size() * DOP_MAXOVERFLOW;
             FrameHost h;
             memset(&h, 0, sizeof h);
             h.weight = F.weight;
             h.dof = F.dof;
             h.cal_in = F.cal;
             h.cal_floating = F.cal_floating;
-            if (2 * g.dopdiff_max + params.sinc2width + 1 > SHAPE_MAXBINS) {
-                h.badradar = 1;
-                h.badradar_logfactor = log((2 * g.dopdiff_max + params.sinc2width + 1) / SHAPE_MAXBINS);
-            }
+            double dx;
+            radar_view_geom(g, h, dx, F, S);
+            dop_extra.push_back(dx);
             h.view = (int)geoms.size();
             h.set = (int)s;
             h.dop_index = g.dop1d ? (int)dop_frames.size() : -1;
@@ -244,27 +277,20 @@ int EngineImpl::finalize()
             const shape_lghtcrv_point &P = points[lc[s].pt0 + k];
             LcPointDev pd;
             memset(&pd, 0, sizeof pd);
-            FrameGeom go;
+            FrameGeom go, gs;
             memset(&go, 0, sizeof go);
-            mul_bt(go.oa, P.oe, P.ae);
-            double us[3] = {0.0, 0.0, 1.0};
-            mtv(us, P.se, us);
-            mv(us, P.oe, us);
-            go.usrc[0] = us[0]; go.usrc[1] = us[1]; go.usrc[2] = us[2];
+            memset(&gs, 0, sizeof gs);
+            lc_view_geom(go, gs, pd, P);
             go.kind = VIEW_LC_OBS;
             go.smooth = params.pos_smooth;
             go.frame_index = lc[s].pt0 + k;
             pd.obs_view = (int)geoms.size();
             add_view(go, P.pos_n, P.km_per_pixel);
-            FrameGeom gs;
-            memset(&gs, 0, sizeof gs);
-            mul_bt(gs.oa, P.se, P.ae);
             gs.kind = VIEW_LC_SUN;
             gs.smooth = 0;
             gs.frame_index = lc[s].pt0 + k;
             pd.sun_view = (int)geoms.size();
             add_view(gs, P.pos_n, P.km_per_pixel);
-            mul_bt(pd.so, P.se, P.oe);
             pd.set = (int)s;
             pd.law_type = S.law.type;
             pd.intensityfactor = pow(P.km_per_pixel / SHAPE_AU, 2.0);
@@ -439,6 +465,56 @@ int EngineImpl::finalize()
     rc = tune_bins();
     if (rc) return rc;
     finalized = true;
+    return SHAPE_OK;
+}
+
+// A new view for radar frame fi (spin, pole and delay-correction trials):
+// its constants are recomputed as finalize computes them and the changed
+// elements copied to the device on the engine stream, ahead of the next
+// evaluation. Every kernel reads them through the device arrays, so the
+// captured graphs stay valid.
+int EngineImpl::set_frame_view(int fi, const double ae[9], const double oe[9], const double spin[3],
+                               double deloff, double dopoff)
+{
+    if (fi < 0 || fi >= (int)frames.size()) return set_err(SHAPE_E_ARG, "set_frame_view: frame out of range");
+    shape_deldop_frame &F = frames[fi];
+    memcpy(F.ae, ae, sizeof F.ae);
+    memcpy(F.oe, oe, sizeof F.oe);
+    memcpy(F.spin, spin, sizeof F.spin);
+    size_t s = 0;
+    while (!(fi >= dd[s].frame0 && fi < dd[s].frame0 + dd[s].nframes)) s++;
+    F.deloff = dd[s].doppler ? 0.0 : deloff;
+    F.dopoff = dopoff;
+    if (!finalized) return SHAPE_OK;
+    FrameHost &h = fh[fi];
+    FrameGeom &g = geoms[h.view];
+    radar_view_geom(g, h, dop_extra[fi], F, dd[s].set);
+    view_float_consts(g);
+    cudaStream_t st = stream;
+    CK(cudaMemcpyAsync(d_geoms + h.view, &g, sizeof g, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_fh + fi, &h, sizeof h, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_dop_extra + fi, &dop_extra[fi], sizeof(double), cudaMemcpyHostToDevice, st));
+    return SHAPE_OK;
+}
+
+// A new view for lightcurve point pt (same contract as set_frame_view).
+int EngineImpl::set_point_view(int pt, const double ae[9], const double oe[9], const double se[9])
+{
+    if (pt < 0 || pt >= (int)points.size()) return set_err(SHAPE_E_ARG, "set_point_view: point out of range");
+    shape_lghtcrv_point &P = points[pt];
+    memcpy(P.ae, ae, sizeof P.ae);
+    memcpy(P.oe, oe, sizeof P.oe);
+    memcpy(P.se, se, sizeof P.se);
+    if (!finalized) return SHAPE_OK;
+    LcPointDev &pd = lcpts[pt];
+    FrameGeom &go = geoms[pd.obs_view], &gs = geoms[pd.sun_view];
+    lc_view_geom(go, gs, pd, P);
+    view_float_consts(go);
+    view_float_consts(gs);
+    cudaStream_t st = stream;
+    CK(cudaMemcpyAsync(d_geoms + pd.obs_view, &go, sizeof go, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_geoms + pd.sun_view, &gs, sizeof gs, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_lcpts + pt, &pd, sizeof pd, cudaMemcpyHostToDevice, st));
     return SHAPE_OK;
 }
 
@@ -1241,6 +1317,24 @@ int shape_engine_stage_times(shape_engine *h, int form, double *ms, int max)
     if (ce != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(ce));
     E.last_form = form;
     return n;
+}
+
+int shape_engine_set_frame_view(shape_engine *h, int global_frame, const double ae[9], const double oe[9],
+                                const double spin[3], double deloff, double dopoff)
+{
+    if (!h || !ae || !oe || !spin) return shape::set_err(SHAPE_E_ARG, "set_frame_view: null argument");
+    shape::EngineImpl &E = h->impl;
+    if (E.finalized) cudaSetDevice(E.device);
+    return E.set_frame_view(global_frame, ae, oe, spin, deloff, dopoff);
+}
+
+int shape_engine_set_point_view(shape_engine *h, int point, const double ae[9], const double oe[9],
+                                const double se[9])
+{
+    if (!h || !ae || !oe || !se) return shape::set_err(SHAPE_E_ARG, "set_point_view: null argument");
+    shape::EngineImpl &E = h->impl;
+    if (E.finalized) cudaSetDevice(E.device);
+    return E.set_point_view(point, ae, oe, se);
 }
 
 int shape_engine_set_fp32_exact(shape_engine *h, int exact)

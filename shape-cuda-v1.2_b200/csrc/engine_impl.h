@@ -190,6 +190,9 @@ struct EngineImpl {
 
     int finalize();
     int tune_bins();
+    int set_frame_view(int fi, const double ae[9], const double oe[9], const double spin[3], double deloff,
+                       double dopoff);
+    int set_point_view(int pt, const double ae[9], const double oe[9], const double se[9]);
     int enqueue(int form, cudaEvent_t *marks = nullptr);
     int launch(int form);
     int poll();

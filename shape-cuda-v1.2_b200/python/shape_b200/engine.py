@@ -110,6 +110,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_stage_times.argtypes = [vp, C.c_int, cd.dptr, C.c_int]
     L.shape_engine_set_bin_capacity.argtypes = [vp, C.c_int]
     L.shape_engine_set_fp32_exact.argtypes = [vp, C.c_int]
+    L.shape_engine_set_frame_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.dptr, C.c_double, C.c_double]
+    L.shape_engine_set_point_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.dptr]
     L.shape_realize_spin.argtypes = [P(cd.SpinState), cd.dptr, cd.dptr, C.c_int, cd.dptr, cd.dptr, cd.dptr,
                                      cd.dptr]
     L.shape_engine_get_tuning.argtypes = [vp, P(C.c_int), C.c_int]
@@ -224,6 +226,22 @@ class Engine:
         """Batched FP32 form: radar views by the exact raster variant too
         (facet and depth maps equal to the FP64 form's; slower raster)."""
         _chk(self.L.shape_engine_set_fp32_exact(self.h, 1 if exact else 0))
+
+    def set_frame_view(self, frame, ae, oe, spin, deloff=0.0, dopoff=0.0):
+        """New view for radar frame `frame` (numbered across sets): 3x3 ae
+        and oe, the spin vector and the delay / Doppler offsets."""
+        a = np.ascontiguousarray(ae, dtype=np.float64).reshape(9)
+        o = np.ascontiguousarray(oe, dtype=np.float64).reshape(9)
+        w = np.ascontiguousarray(spin, dtype=np.float64).reshape(3)
+        _chk(self.L.shape_engine_set_frame_view(self.h, int(frame), cd.as_dptr(a), cd.as_dptr(o), cd.as_dptr(w),
+                                                float(deloff), float(dopoff)))
+
+    def set_point_view(self, point, ae, oe, se):
+        """New view for lightcurve point `point` (numbered across sets)."""
+        a = np.ascontiguousarray(ae, dtype=np.float64).reshape(9)
+        o = np.ascontiguousarray(oe, dtype=np.float64).reshape(9)
+        q = np.ascontiguousarray(se, dtype=np.float64).reshape(9)
+        _chk(self.L.shape_engine_set_point_view(self.h, int(point), cd.as_dptr(a), cd.as_dptr(o), cd.as_dptr(q)))
 
     def tuning(self):
         out = (C.c_int * 8)()

@@ -1,0 +1,147 @@
+"""View updates between evaluations (shape_engine_set_frame_view and
+shape_engine_set_point_view), as spin, pole and delay-correction trials make
+them: after new views, every form gives what the oracle gives on datasets
+carrying those views, at the parity tests' bars (FP64 forms: facet, z and
+cos(e) maps bit-exact, chi-square to 1e-10; FP32 form: chi-square to 1e-6),
+through graphs captured before the change; setting the old views back
+restores the first results."""
+import copy
+
+import numpy as np
+import pytest
+
+import cases
+import golden_cases as gc
+from shape_b200 import ctypes_defs as cd
+from shape_b200 import engine as eng
+from test_gpu_parity import CHI2_RTOL, FP32_CHI2_RTOL, _frame_checks
+
+pytestmark = pytest.mark.gpu
+
+FORMS = (eng.FORM_PLAIN_FP64, eng.FORM_BATCHED_FP64, eng.FORM_BATCHED_FP32)
+
+
+def _rz(a):
+    c, s = np.cos(a), np.sin(a)
+    return np.array([[c, -s, 0.0], [s, c, 0.0], [0.0, 0.0, 1.0]])
+
+
+def _rx(a):
+    c, s = np.cos(a), np.sin(a)
+    return np.array([[1.0, 0.0, 0.0], [0.0, c, -s], [0.0, s, c]])
+
+
+def _m(v):
+    return np.array(v[:], dtype=np.float64).reshape(3, 3)
+
+
+def _new_view(fr, k):
+    """A spin-phase step, a pole tilt and a faster spin for frame k."""
+    ae = _rz(0.15 + 0.05 * k) @ _m(fr.ae) @ _rx(0.08)
+    spin = 1.08 * (_rx(0.08).T @ np.array(fr.spin[:]))
+    return ae, spin
+
+
+def test_frame_views_deldop(cuda_device):
+    m, p, ds = cases.c2(12)
+    e = eng.make_engine(m, p, deldops=[ds])
+    e.keep_pos(True)
+    base = {f: e.evaluate(f)["chi2"] for f in FORMS}      # tuned, graphs captured
+    ds2 = copy.copy(ds)
+    ds2.frames = []
+    for k, fr in enumerate(ds.frames):
+        g = cd.DeldopFrame.from_buffer_copy(fr)
+        ae, spin = _new_view(fr, k)
+        cd.fill9(g.ae, ae)
+        for j in range(3):
+            g.spin[j] = spin[j]
+        g.deloff, g.dopoff = fr.deloff + 0.37, fr.dopoff - 0.21
+        ds2.frames.append(g)
+        e.set_frame_view(k, ae, _m(fr.oe), spin, g.deloff, g.dopoff)
+    o = cases.orc().eval_deldop(m, ds2, p, keep_pos=True)
+    chi2_o = sum(r["chi2"] for r in o["results"])
+    for form in (eng.FORM_PLAIN_FP64, eng.FORM_BATCHED_FP64):
+        s = e.evaluate(form)
+        _frame_checks(e, o, ds2)
+        assert abs(s["chi2"] - chi2_o) <= CHI2_RTOL * chi2_o, (form, s["chi2"], chi2_o)
+    s = e.evaluate(eng.FORM_BATCHED_FP32)
+    assert abs(s["chi2"] - chi2_o) <= FP32_CHI2_RTOL * chi2_o, (s["chi2"], chi2_o)
+    for k, fr in enumerate(ds.frames):
+        e.set_frame_view(k, _m(fr.ae), _m(fr.oe), fr.spin[:], fr.deloff, fr.dopoff)
+    for form in FORMS:       # FP32: the scatter's float atomics may add in another order
+        c = e.evaluate(form)["chi2"]
+        bar = FP32_CHI2_RTOL if form == eng.FORM_BATCHED_FP32 else CHI2_RTOL
+        assert abs(c - base[form]) <= bar * base[form], (form, c, base[form])
+    with pytest.raises(eng.EngineError):
+        e.set_frame_view(ds.nframes, np.eye(3), np.eye(3), np.zeros(3))
+    e.close()
+
+
+def test_frame_views_doppler(cuda_device):
+    model_fn, ds_fn, p = gc.DOPPLER_CASES["dop_nsinc2"]      # nsinc2 = 2: footprint increments
+    m = model_fn()
+    ds = ds_fn(lambda d, q: cases.orc().eval_doppler(m, d, q)["fits"], p)
+    e = eng.make_engine(m, p, dopplers=[ds])
+    e.keep_pos(True)
+    for f in FORMS:
+        e.evaluate(f)
+    ds2 = copy.copy(ds)
+    ds2.frames = []
+    for k, fr in enumerate(ds.frames):
+        g = cd.DopplerFrame.from_buffer_copy(fr)
+        ae, spin = _new_view(fr, k)
+        cd.fill9(g.ae, ae)
+        for j in range(3):
+            g.spin[j] = spin[j]
+        g.dopoff = fr.dopoff + 0.43
+        ds2.frames.append(g)
+        e.set_frame_view(k, ae, _m(fr.oe), spin, 5.0, g.dopoff)     # deloff: ignored for spectra
+    o = cases.orc().eval_doppler(m, ds2, p, keep_pos=True)
+    chi2_o = sum(r["chi2"] for r in o["results"])
+    for form in (eng.FORM_PLAIN_FP64, eng.FORM_BATCHED_FP64):
+        s = e.evaluate(form)
+        res = e.results()
+        for f in range(len(ds2.frames)):
+            assert np.array_equal(e.pos(f)["f"], o["pos"][f]["f"]), (form, f)
+            assert list(res[f]["idoplim"]) == list(o["results"][f]["idoplim"]), (form, f)
+            assert abs(res[f]["chi2"] - o["results"][f]["chi2"]) <= CHI2_RTOL * abs(o["results"][f]["chi2"])
+        assert abs(s["chi2"] - chi2_o) <= CHI2_RTOL * chi2_o
+    s = e.evaluate(eng.FORM_BATCHED_FP32)
+    assert abs(s["chi2"] - chi2_o) <= FP32_CHI2_RTOL * chi2_o
+    e.close()
+
+
+def test_point_views_lightcurve(cuda_device):
+    m, p, sets = cases.c3(12, 2)
+    e = eng.make_engine(m, p, lghtcrvs=sets)
+    e.keep_pos(True)
+    for f in FORMS:
+        e.evaluate(f)
+    sets2, pt = [], 0
+    for ds in sets:
+        d2 = copy.copy(ds)
+        d2.points = []
+        for i, q in enumerate(ds.points):
+            g = cd.LghtcrvPoint.from_buffer_copy(q)
+            ae = _rz(0.2 + 0.03 * i) @ _m(q.ae)
+            cd.fill9(g.ae, ae)
+            d2.points.append(g)
+            e.set_point_view(pt, ae, _m(q.oe), _m(q.se))
+            pt += 1
+        sets2.append(d2)
+    o = cases.orc()
+    outs = [o.eval_lghtcrv(m, d, p, keep_pos=True) for d in sets2]
+    tot = sum(oo["chi2"] for oo in outs)
+    for form in FORMS:
+        s = e.evaluate(form)
+        for k, d in enumerate(sets2):
+            for i, q in enumerate(d.points):
+                pg, po = e.lghtcrv_pos(k, i, q), outs[k]["pos"][i]
+                assert np.array_equal(pg["f"], po["f"]), (form, k, i)
+                assert np.array_equal(pg["fill"], po["fill"]), (form, k, i)
+            if form != eng.FORM_BATCHED_FP32:
+                g = e.lghtcrv(k, d)
+                np.testing.assert_allclose(g["y"], outs[k]["y"], rtol=1e-12)
+        bar = FP32_CHI2_RTOL if form == eng.FORM_BATCHED_FP32 else CHI2_RTOL
+        assert abs(s["chi2"] - tot) <= bar * tot, (form, s["chi2"], tot)
+    e.close()
