@@ -178,6 +178,26 @@ int shape_engine_set_frame_view(shape_engine *e, int global_frame, const double 
  * and se (src/shape/calc_fits.c:1634-1716). */
 int shape_engine_set_point_view(shape_engine *e, int point, const double ae[9], const double oe[9],
                                 const double se[9]);
+
+/* The spin model of the engine's views, for spin fits (realize_spin,
+ * src/shape/realize_spin.c:41-285): the spin state; each dataset's angle and
+ * spin offsets (3 doubles per dataset, numbered as the add_*_set calls
+ * returned them; NULL = zeros); each radar frame's view epoch (days,
+ * light-time corrected; global frame numbering) and orbital spin
+ * contribution (3 doubles per frame, ecliptic, rad/day; NULL = zeros).
+ * Lightcurve points take their set's calculated epochs x[]. Every view's
+ * ae (and a radar frame's spin vector) is realized now by
+ * shape_realize_spin and replaces the one its dataset gave; oe and se are
+ * kept. All datasets must be added first. */
+int shape_engine_set_spin_model(shape_engine *e, const shape_spin_state *spin, const double *set_angleoff,
+                                const double *set_omegaoff, const double *frame_t,
+                                const double *frame_orbspin);
+/* One spin parameter (SHAPE_PAR_SPIN_* / ANGLEOFF / OMEGAOFF) of the spin
+ * model: set re-realizes every view and copies the view constants to the
+ * device on the engine's stream (the next evaluation, graph replays
+ * included, sees them). */
+int shape_engine_set_spin_param(shape_engine *e, int kind, int index, double value);
+int shape_engine_get_spin_param(shape_engine *e, int kind, int index, double *value);
 /* Tuning state after finalize: [0] bin capacity, [1] largest tile count of
  * the dry run, [2] non-empty tiles, [3] tiles, [4] tile width in pixels.
  * Returns the number of values written. */
@@ -194,6 +214,16 @@ int shape_engine_last_time_ms(shape_engine *e, double *ms);
 /* Free parameter kinds (src/shape/mkparlist.c:218-235). */
 #define SHAPE_PAR_SCALE 1      /* component scale factor index (SIZEPAR) */
 #define SHAPE_PAR_VERTEX_R 2   /* vertex deviation r of vertex index (SHAPEPAR) */
+/* Spin parameters (SPINPAR, src/shape/mkparlist.c:855-950); they need the
+ * engine's spin model (shape_engine_set_spin_model). */
+#define SHAPE_PAR_SPIN_ANGLE 3     /* spin.angle[index] (rad) */
+#define SHAPE_PAR_SPIN_OMEGA 4     /* spin.omega[index] (rad/day) */
+#define SHAPE_PAR_SPIN_INERTIA 5   /* spin.inertia[index] */
+#define SHAPE_PAR_SPIN_OMEGADOT 6  /* spin.omegadot[index] (rad/day^2) */
+#define SHAPE_PAR_SPIN_IMPULSE 7   /* spin.impulse[index / 3][index % 3] (rad/day) */
+#define SHAPE_PAR_SPIN_LIB 8       /* index 0 lib_amp, 1 lib_freq, 2 lib_phase */
+#define SHAPE_PAR_ANGLEOFF 9       /* angleoff[index % 3] of dataset index / 3 (rad) */
+#define SHAPE_PAR_OMEGAOFF 10      /* omegaoff[index % 3] of dataset index / 3 (rad/day) */
 
 /* One free parameter with its step and tolerances (par->fparstep,
  * fpartol, fparabstol; e.g. length_step/length_tol/length_abstol). */

@@ -518,6 +518,108 @@ int EngineImpl::set_point_view(int pt, const double ae[9], const double oe[9], c
     return SHAPE_OK;
 }
 
+int EngineImpl::set_spin_model(const shape_spin_state &sp, const double *ao, const double *oo, const double *t,
+                               const double *orb)
+{
+    if (!t && !frames.empty()) return set_err(SHAPE_E_ARG, "set_spin_model: frame epochs needed");
+    const size_t nsets = setrecs.size(), nfr = frames.size();
+    spin_st = sp;
+    spin_angleoff.assign(ao ? ao : nullptr, ao ? ao + 3 * nsets : nullptr);
+    spin_omegaoff.assign(oo ? oo : nullptr, oo ? oo + 3 * nsets : nullptr);
+    spin_angleoff.resize(3 * nsets, 0.0);
+    spin_omegaoff.resize(3 * nsets, 0.0);
+    frame_t.assign(t ? t : nullptr, t ? t + nfr : nullptr);
+    frame_orbspin.assign(orb ? orb : nullptr, orb ? orb + 3 * nfr : nullptr);
+    frame_orbspin.resize(3 * nfr, 0.0);
+    have_spin = true;
+    return realize_views();
+}
+
+// The field of the spin model that a spin parameter names, or null.
+double *EngineImpl::spin_param(int kind, int index)
+{
+    if (!have_spin || index < 0) return nullptr;
+    const int nsets = (int)(spin_angleoff.size() / 3);
+    switch (kind) {
+    case SHAPE_PAR_SPIN_ANGLE: return index < 3 ? &spin_st.angle[index] : nullptr;
+    case SHAPE_PAR_SPIN_OMEGA: return index < 3 ? &spin_st.omega[index] : nullptr;
+    case SHAPE_PAR_SPIN_INERTIA: return index < 3 ? &spin_st.inertia[index] : nullptr;
+    case SHAPE_PAR_SPIN_OMEGADOT: return index < 3 ? &spin_st.omegadot[index] : nullptr;
+    case SHAPE_PAR_SPIN_IMPULSE:
+        return index < 3 * spin_st.n_impulse ? &spin_st.impulse[index / 3][index % 3] : nullptr;
+    case SHAPE_PAR_SPIN_LIB:
+        return index == 0 ? &spin_st.lib_amp : index == 1 ? &spin_st.lib_freq : index == 2 ? &spin_st.lib_phase
+                                                                                           : nullptr;
+    case SHAPE_PAR_ANGLEOFF: return index < 3 * nsets ? &spin_angleoff[index] : nullptr;
+    case SHAPE_PAR_OMEGAOFF: return index < 3 * nsets ? &spin_omegaoff[index] : nullptr;
+    default: return nullptr;
+    }
+}
+
+// Realizes every view's ae (and a radar frame's spin vector) from the spin
+// model, dataset by dataset, then refreshes the view constants.
+int EngineImpl::realize_views()
+{
+    if (spin_angleoff.size() != 3 * setrecs.size() || frame_t.size() != frames.size())
+        return set_err(SHAPE_E_STATE, "spin model: datasets were added after set_spin_model");
+    std::vector<double> ae, sp, zero;
+    for (size_t r = 0; r < setrecs.size(); r++) {
+        const double *ao = &spin_angleoff[3 * r], *oo = &spin_omegaoff[3 * r];
+        if (setrecs[r].type == 0) {
+            const int f0 = setrecs[r].first, n = setrecs[r].count;
+            ae.resize(9 * (size_t)n);
+            sp.resize(3 * (size_t)n);
+            int rc = shape_realize_spin(&spin_st, ao, oo, n, &frame_t[f0], &frame_orbspin[3 * (size_t)f0],
+                                        ae.data(), sp.data());
+            if (rc) return rc;
+            for (int k = 0; k < n; k++) {
+                memcpy(frames[f0 + k].ae, &ae[9 * (size_t)k], 9 * sizeof(double));
+                memcpy(frames[f0 + k].spin, &sp[3 * (size_t)k], 3 * sizeof(double));
+            }
+        } else {
+            const LcSetHost &L = lc[setrecs[r].first];
+            ae.resize(9 * (size_t)L.npts);
+            sp.resize(3 * (size_t)L.npts);
+            zero.assign(3 * (size_t)L.npts, 0.0);
+            int rc = shape_realize_spin(&spin_st, ao, oo, L.npts, L.x.data(), zero.data(), ae.data(), sp.data());
+            if (rc) return rc;
+            for (int k = 0; k < L.npts; k++) memcpy(points[L.pt0 + k].ae, &ae[9 * (size_t)k], 9 * sizeof(double));
+        }
+    }
+    return refresh_views();
+}
+
+// After finalize: every view's constants recomputed from frames / points and
+// the arrays copied to the device on the engine stream (set_frame_view does
+// the same for one frame).
+int EngineImpl::refresh_views()
+{
+    if (!finalized) return SHAPE_OK;
+    for (size_t s = 0; s < dd.size(); s++)
+        for (int k = 0; k < dd[s].nframes; k++) {
+            const int fi = dd[s].frame0 + k;
+            FrameHost &h = fh[fi];
+            radar_view_geom(geoms[h.view], h, dop_extra[fi], frames[fi], dd[s].set);
+            view_float_consts(geoms[h.view]);
+        }
+    for (size_t pt = 0; pt < lcpts.size(); pt++) {
+        LcPointDev &pd = lcpts[pt];
+        lc_view_geom(geoms[pd.obs_view], geoms[pd.sun_view], pd, points[pt]);
+        view_float_consts(geoms[pd.obs_view]);
+        view_float_consts(geoms[pd.sun_view]);
+    }
+    cudaStream_t st = stream;
+    CK(cudaMemcpyAsync(d_geoms, geoms.data(), sizeof(FrameGeom) * geoms.size(), cudaMemcpyHostToDevice, st));
+    if (!fh.empty()) {
+        CK(cudaMemcpyAsync(d_fh, fh.data(), sizeof(FrameHost) * fh.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_dop_extra, dop_extra.data(), sizeof(double) * dop_extra.size(),
+                           cudaMemcpyHostToDevice, st));
+    }
+    if (!lcpts.empty())
+        CK(cudaMemcpyAsync(d_lcpts, lcpts.data(), sizeof(LcPointDev) * lcpts.size(), cudaMemcpyHostToDevice, st));
+    return SHAPE_OK;
+}
+
 // Bin autotuning from a dry-run binning of the model as loaded: the bin
 // capacity becomes the next power of two above 1.25x the fullest tile (so a
 // fit's small model changes do not overflow into the full-scan path), and
@@ -1335,6 +1437,42 @@ int shape_engine_set_point_view(shape_engine *h, int point, const double ae[9], 
     shape::EngineImpl &E = h->impl;
     if (E.finalized) cudaSetDevice(E.device);
     return E.set_point_view(point, ae, oe, se);
+}
+
+int shape_engine_set_spin_model(shape_engine *h, const shape_spin_state *spin, const double *set_angleoff,
+                                const double *set_omegaoff, const double *frame_t, const double *frame_orbspin)
+{
+    if (!h || !spin) return shape::set_err(SHAPE_E_ARG, "set_spin_model: null argument");
+    shape::EngineImpl &E = h->impl;
+    if (E.finalized) cudaSetDevice(E.device);
+    return E.set_spin_model(*spin, set_angleoff, set_omegaoff, frame_t, frame_orbspin);
+}
+
+int shape_engine_set_spin_param(shape_engine *h, int kind, int index, double value)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "set_spin_param: null argument");
+    shape::EngineImpl &E = h->impl;
+    double *p = E.spin_param(kind, index);
+    if (!p) return shape::set_err(E.have_spin ? SHAPE_E_ARG : SHAPE_E_STATE, "set_spin_param: no such spin parameter");
+    const double old = *p;
+    *p = value;
+    if (E.finalized) cudaSetDevice(E.device);
+    int rc = E.realize_views();
+    if (rc) {                       // keep the last realizable state
+        *p = old;
+        E.realize_views();
+    }
+    return rc;
+}
+
+int shape_engine_get_spin_param(shape_engine *h, int kind, int index, double *value)
+{
+    if (!h || !value) return shape::set_err(SHAPE_E_ARG, "get_spin_param: null argument");
+    double *p = h->impl.spin_param(kind, index);
+    if (!p) return shape::set_err(h->impl.have_spin ? SHAPE_E_ARG : SHAPE_E_STATE,
+                                  "get_spin_param: no such spin parameter");
+    *value = *p;
+    return SHAPE_OK;
 }
 
 int shape_engine_set_fp32_exact(shape_engine *h, int exact)

@@ -193,6 +193,16 @@ struct EngineImpl {
     int set_frame_view(int fi, const double ae[9], const double oe[9], const double spin[3], double deloff,
                        double dopoff);
     int set_point_view(int pt, const double ae[9], const double oe[9], const double se[9]);
+    // spin model of the views (shape_engine_set_spin_model)
+    bool have_spin = false;
+    shape_spin_state spin_st;
+    std::vector<double> spin_angleoff, spin_omegaoff;   // 3 per dataset (setrecs order)
+    std::vector<double> frame_t, frame_orbspin;         // per radar frame
+    int set_spin_model(const shape_spin_state &sp, const double *ao, const double *oo, const double *t,
+                       const double *orb);
+    double *spin_param(int kind, int index);
+    int realize_views();
+    int refresh_views();
     int enqueue(int form, cudaEvent_t *marks = nullptr);
     int launch(int form);
     int poll();

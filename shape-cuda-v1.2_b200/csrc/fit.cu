@@ -199,12 +199,16 @@ struct EngineTarget : FitTarget {
     {
         if (p.kind == SHAPE_PAR_SCALE) return shape_engine_get_scale(e, p.index, v);
         if (p.kind == SHAPE_PAR_VERTEX_R) return shape_engine_get_vertex_r(e, p.index, v);
+        if (p.kind >= SHAPE_PAR_SPIN_ANGLE && p.kind <= SHAPE_PAR_OMEGAOFF)
+            return shape_engine_get_spin_param(e, p.kind, p.index, v);
         return report_error(SHAPE_E_ARG, "bestfit: unknown parameter kind");
     }
     int set(const shape_fit_param &p, int, double v) override
     {
         if (p.kind == SHAPE_PAR_SCALE) return shape_engine_set_scale(e, p.index, v);
         if (p.kind == SHAPE_PAR_VERTEX_R) return shape_engine_set_vertex_r(e, p.index, v);
+        if (p.kind >= SHAPE_PAR_SPIN_ANGLE && p.kind <= SHAPE_PAR_OMEGAOFF)
+            return shape_engine_set_spin_param(e, p.kind, p.index, v);
         return report_error(SHAPE_E_ARG, "bestfit: unknown parameter kind");
     }
     // objective(x) of src/shape/bestfit.c:718-874 without penalties

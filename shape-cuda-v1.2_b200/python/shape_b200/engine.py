@@ -22,6 +22,14 @@ FORMS = {"plain_fp64": 0, "batched_fp64": 1, "batched_fp32": 2}
 
 PAR_SCALE = 1
 PAR_VERTEX_R = 2
+PAR_SPIN_ANGLE = 3
+PAR_SPIN_OMEGA = 4
+PAR_SPIN_INERTIA = 5
+PAR_SPIN_OMEGADOT = 6
+PAR_SPIN_IMPULSE = 7
+PAR_SPIN_LIB = 8
+PAR_ANGLEOFF = 9
+PAR_OMEGAOFF = 10
 
 
 class FitParam(C.Structure):
@@ -112,6 +120,9 @@ def load_library(path=LIB_PATH):
     L.shape_engine_set_fp32_exact.argtypes = [vp, C.c_int]
     L.shape_engine_set_frame_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.dptr, C.c_double, C.c_double]
     L.shape_engine_set_point_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.dptr]
+    L.shape_engine_set_spin_model.argtypes = [vp, P(cd.SpinState), cd.dptr, cd.dptr, cd.dptr, cd.dptr]
+    L.shape_engine_set_spin_param.argtypes = [vp, C.c_int, C.c_int, C.c_double]
+    L.shape_engine_get_spin_param.argtypes = [vp, C.c_int, C.c_int, P(C.c_double)]
     L.shape_realize_spin.argtypes = [P(cd.SpinState), cd.dptr, cd.dptr, C.c_int, cd.dptr, cd.dptr, cd.dptr,
                                      cd.dptr]
     L.shape_engine_get_tuning.argtypes = [vp, P(C.c_int), C.c_int]
@@ -266,6 +277,24 @@ class Engine:
     def get_vertex_r(self, i):
         v = C.c_double()
         _chk(self.L.shape_engine_get_vertex_r(self.h, i, C.byref(v)))
+        return v.value
+
+    def set_spin_model(self, spin, frame_t=None, frame_orbspin=None, angleoff=None, omegaoff=None):
+        """Spin model of the views: a spin_state(), per radar frame its view
+        epoch and orbital spin (nframes x 3), per dataset its angle and spin
+        offsets (nsets x 3). Realizes every view now."""
+        self._spin = spin
+        keep = [None if v is None else np.ascontiguousarray(v, dtype=np.float64).ravel()
+                for v in (angleoff, omegaoff, frame_t, frame_orbspin)]
+        ptrs = [cd.as_dptr(v) if v is not None else None for v in keep]
+        _chk(self.L.shape_engine_set_spin_model(self.h, C.byref(spin), *ptrs))
+
+    def set_spin_param(self, kind, index, value):
+        _chk(self.L.shape_engine_set_spin_param(self.h, int(kind), int(index), float(value)))
+
+    def get_spin_param(self, kind, index):
+        v = C.c_double()
+        _chk(self.L.shape_engine_get_spin_param(self.h, int(kind), int(index), C.byref(v)))
         return v.value
 
     def bestfit(self, params, form=FORM_BATCHED_FP64, term_prec=1e-4, term_maxiter=0, trace_max=0):

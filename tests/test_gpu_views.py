@@ -145,3 +145,116 @@ def test_point_views_lightcurve(cuda_device):
         bar = FP32_CHI2_RTOL if form == eng.FORM_BATCHED_FP32 else CHI2_RTOL
         assert abs(s["chi2"] - tot) <= bar * tot, (form, s["chi2"], tot)
     e.close()
+
+
+def _spin_views(ds, spin, t, angleoff=(0.0, 0.0, 0.0)):
+    """ds with every frame's ae and spin vector realized from `spin` at the
+    view epochs t (shape_realize_spin, checked against the reference's
+    realize_spin on the CPU)."""
+    ae, sp = eng.realize_spin(spin, t, None, angleoff)
+    d2 = copy.copy(ds)
+    d2.frames = []
+    for k, fr in enumerate(ds.frames):
+        g = cd.DeldopFrame.from_buffer_copy(fr)
+        cd.fill9(g.ae, ae[k])
+        for j in range(3):
+            g.spin[j] = sp[k][j]
+        d2.frames.append(g)
+    return d2
+
+
+T0 = 2458000.0
+
+
+def _pa_spin(psi0):
+    return eng.spin_state(1, T0, (0.5, 0.9, psi0), (0.0, 0.0, 2 * np.pi / 0.25))
+
+
+def test_spin_model_deldop(cuda_device):
+    """set_spin_model realizes the views of an engine whose graphs were
+    captured on the dataset's own views; a spin-parameter trial re-realizes
+    them. Both against the oracle on the realized views."""
+    m, p, ds = cases.c2(12)
+    t = T0 + 0.04 * np.arange(ds.nframes)
+    e = eng.make_engine(m, p, deldops=[ds])
+    e.keep_pos(True)
+    for f in FORMS:
+        e.evaluate(f)
+    e.set_spin_model(_pa_spin(0.3), t)
+    for psi0 in (0.3, 0.35):
+        if psi0 != 0.3:
+            e.set_spin_param(eng.PAR_SPIN_ANGLE, 2, psi0)
+        assert e.get_spin_param(eng.PAR_SPIN_ANGLE, 2) == psi0
+        ds2 = _spin_views(ds, _pa_spin(psi0), t)
+        o = cases.orc().eval_deldop(m, ds2, p, keep_pos=True)
+        chi2_o = sum(r["chi2"] for r in o["results"])
+        for form in (eng.FORM_PLAIN_FP64, eng.FORM_BATCHED_FP64):
+            s = e.evaluate(form)
+            _frame_checks(e, o, ds2)
+            assert abs(s["chi2"] - chi2_o) <= CHI2_RTOL * chi2_o, (psi0, form, s["chi2"], chi2_o)
+        s = e.evaluate(eng.FORM_BATCHED_FP32)
+        assert abs(s["chi2"] - chi2_o) <= FP32_CHI2_RTOL * chi2_o, (psi0, s["chi2"], chi2_o)
+    for kind, index in ((eng.PAR_SPIN_ANGLE, 3), (eng.PAR_ANGLEOFF, 3), (eng.PAR_SPIN_IMPULSE, 0), (99, 0)):
+        with pytest.raises(eng.EngineError):
+            e.set_spin_param(kind, index, 0.0)
+    e.close()
+
+
+def test_spin_model_lightcurve_offsets(cuda_device):
+    """Lightcurve points realized at their sets' calculated epochs, with a
+    per-dataset angle offset on the second set."""
+    m, p, sets = cases.c3(12, 2)
+    e = eng.make_engine(m, p, lghtcrvs=sets)
+    e.keep_pos(True)
+    e.evaluate(eng.FORM_BATCHED_FP64)
+    spin = eng.spin_state(1, float(sets[0].x[0]), (0.2, 1.1, 0.4), (0.0, 0.0, 2 * np.pi / 0.3))
+    aoff = np.array([[0.0, 0.0, 0.0], [0.01, -0.02, 0.03]])
+    e.set_spin_model(spin, None, None, aoff)
+    o = cases.orc()
+    tot = 0.0
+    outs, sets2 = [], []
+    for k, ds in enumerate(sets):
+        ae, _ = eng.realize_spin(spin, ds.x, None, tuple(aoff[k]))
+        d2 = copy.copy(ds)
+        d2.points = []
+        for i, q in enumerate(ds.points):
+            g = cd.LghtcrvPoint.from_buffer_copy(q)
+            cd.fill9(g.ae, ae[i])
+            d2.points.append(g)
+        sets2.append(d2)
+        outs.append(o.eval_lghtcrv(m, d2, p, keep_pos=True))
+        tot += outs[-1]["chi2"]
+    for form in (eng.FORM_PLAIN_FP64, eng.FORM_BATCHED_FP64):
+        s = e.evaluate(form)
+        for k, d in enumerate(sets2):
+            np.testing.assert_allclose(e.lghtcrv(k, d)["y"], outs[k]["y"], rtol=1e-12)
+            for i, q in enumerate(d.points):
+                assert np.array_equal(e.lghtcrv_pos(k, i, q)["f"], outs[k]["pos"][i]["f"]), (form, k, i)
+        assert abs(s["chi2"] - tot) <= CHI2_RTOL * tot, (form, s["chi2"], tot)
+    e.close()
+
+
+def test_spin_fit_recovers_rotation_phase(cuda_device):
+    """bestfit over spin.angle[2] (SHAPE_PAR_SPIN_ANGLE) on noise-free data
+    made from a known spin state: every trial is a spin realization of all
+    views plus a graph replay; the fit returns to the true phase."""
+    m, p, ds = cases.c2(12)
+    t = T0 + 0.04 * np.arange(ds.nframes)
+    truth = _spin_views(ds, _pa_spin(0.3), t)
+    fits = cases.orc().eval_deldop(m, truth, p)["fits"]
+    obs = np.concatenate([np.asarray(f, dtype=np.float64).ravel() for f in fits])
+    data = copy.copy(truth)
+    data.obs = obs
+    e = eng.make_engine(m, p, deldops=[data])
+    e.set_spin_model(_pa_spin(0.3), t)
+    at_truth = e.evaluate(eng.FORM_BATCHED_FP64)["chi2"]
+    e.set_spin_param(eng.PAR_SPIN_ANGLE, 2, 0.32)
+    at_start = e.evaluate(eng.FORM_BATCHED_FP64)["chi2"]
+    assert at_truth <= 1e-6 * at_start, (at_truth, at_start)
+    res, trace = e.bestfit([(eng.PAR_SPIN_ANGLE, 2, 0.005, 1e-7, 1e-7)], term_prec=1e-9, term_maxiter=4,
+                           trace_max=400)
+    psi = e.get_spin_param(eng.PAR_SPIN_ANGLE, 2)
+    assert abs(psi - 0.3) < 1e-4, psi
+    assert res["final_objective"] < 1e-3 * res["initial_objective"], res
+    assert len(trace) == res["trace_len"] > 5
+    e.close()
