@@ -57,9 +57,11 @@ typedef struct shape_eval_summary {
     double posbnd_logfactor;   /* par->posbnd_logfactor after /= dat->dof */
     int badradar;              /* par->badradar */
     double badradar_logfactor; /* after /= (dof_deldop + dof_doppler) */
-    double objective;          /* chi2/dof times bad-model factors, as in
-                                  objective() (src/shape/bestfit.c:789-866)
-                                  with no penalties */
+    double objective;          /* (chi2/dof + penalties) times the bad-model
+                                  factors, as objective() computes it
+                                  (src/shape/bestfit.c:789-866) */
+    double penalties;          /* the penalty sum (shape_engine_set_penalties;
+                                  0 with none) */
 } shape_eval_summary;
 
 const char *shape_last_error(void);
@@ -178,6 +180,39 @@ int shape_engine_set_frame_view(shape_engine *e, int global_frame, const double 
  * and se (src/shape/calc_fits.c:1634-1716). */
 int shape_engine_set_point_view(shape_engine *e, int point, const double ae[9], const double oe[9],
                                 const double se[9]);
+
+/* Penalty types (par->pen.type; the reference's numbering, src/shape/const.h). */
+#define SHAPE_PEN_NONSMOOTH 9
+#define SHAPE_PEN_CONCAVITY 10
+#define SHAPE_PEN_RDEV 11
+#define SHAPE_PEN_VOLUME 12
+#define SHAPE_PEN_COMDEV 13
+#define SHAPE_PEN_INERTIADEV 14
+#define SHAPE_PEN_INERTIADEV_UNI 15
+#define SHAPE_PEN_PA3TILT 16
+#define SHAPE_PEN_NONPA 17
+#define SHAPE_PEN_NONPA_UNI 18
+#define SHAPE_PEN_EULEROFFS 19
+#define SHAPE_PEN_FLATTENING 20
+#define SHAPE_PEN_MAXRDEV 21
+#define SHAPE_PEN_IMPULSE 25
+
+/* The penalty terms of the objective (par->pen; penalties,
+ * src/shape/penalties.c:121-1236): n penalties of the given types and
+ * weights (a negative weight takes the reciprocal of the penalty, as in the
+ * reference). From the next evaluation on, the summary's objective is
+ * (chi2/dof + the penalty sum) times the bad-model factors, and bestfit
+ * minimises that. The model's moments and its edge and vertex sums are
+ * reduced on the device after each evaluation (two more launches and a
+ * 128-byte copy), and the penalties follow from them on the host. The
+ * shape penalties need a closed surface. INERTIADEV, NONPA and IMPULSE need
+ * the spin model. The photometric penalties, MAXELLIPDEV, NONCOSINE and
+ * BIFURCATION return SHAPE_E_UNSUPPORTED. n = 0 removes the penalties.
+ * Server workloads ignore them. */
+int shape_engine_set_penalties(shape_engine *e, int n, const int *type, const double *weight);
+/* Each penalty's value after its weight's sign rule (par->pen.base) at the
+ * last evaluation, for up to max penalties; returns the penalty count. */
+int shape_engine_get_penalties(shape_engine *e, double *base, int max);
 
 /* The spin model of the engine's views, for spin fits (realize_spin,
  * src/shape/realize_spin.c:41-285): the spin state; each dataset's angle and

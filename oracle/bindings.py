@@ -215,6 +215,9 @@ class Reference:
         L.ref_evaluate_mt.argtypes = [P(C.c_void_p), C.c_int]
         L.ref_get_realized.argtypes = [C.c_void_p, cd.dptr, cd.dptr, cd.dptr, cd.dptr]
         L.ref_get_flags.argtypes = [C.c_void_p, cd.dptr]
+        L.ref_penalties.argtypes = [C.c_void_p, C.c_int, cd.iptr, cd.dptr, P(cd.SpinState), cd.dptr, cd.dptr,
+                                    cd.dptr]
+        L.ref_penalties.restype = C.c_double
         L.ref_get_seen.argtypes = [C.c_void_p, C.c_char_p]
         L.ref_get_deldop_frame.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr, cd.dptr,
                                            cd.dptr, cd.iptr, P(cd.DeldopResult)]
@@ -277,6 +280,20 @@ class RefSession:
 
     def evaluate(self):
         return self.L.ref_evaluate(self.h)
+
+    def penalties(self, pens, spin=None, angleoff=None, omegaoff=None):
+        """The reference's penalties() for [(type, weight), ...]: (sum, bases)."""
+        n = len(pens)
+        types = np.array([t for t, _ in pens] or [0], dtype=np.int32)
+        w = np.array([x for _, x in pens] or [0.0])
+        base = np.zeros(max(1, n))
+        ao = None if angleoff is None else np.ascontiguousarray(angleoff, dtype=np.float64).ravel()
+        oo = None if omegaoff is None else np.ascontiguousarray(omegaoff, dtype=np.float64).ravel()
+        tot = self.L.ref_penalties(self.h, n, types.ctypes.data_as(cd.iptr), cd.as_dptr(w),
+                                   C.byref(spin) if spin is not None else None,
+                                   cd.as_dptr(ao) if ao is not None else None,
+                                   cd.as_dptr(oo) if oo is not None else None, cd.as_dptr(base))
+        return tot, base[:n].copy()
 
     def realized(self):
         m = self.model

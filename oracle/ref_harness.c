@@ -637,3 +637,50 @@ int ref_realize_spin_frames(const shape_spin_state *sp, const double angleoff[3]
     free(par);
     return 0;
 }
+
+
+/* The reference's penalties(par, mod, dat) (src/shape/penalties.c:121-1236)
+ * after realize_mod, for n penalties of the given types and weights: the
+ * check of the engine's penalty terms. The model's edges come from the
+ * reference's own setupsides (src/shape/read_mod.c:2386). sp (or NULL)
+ * supplies spin.inertia and the spin impulses; angleoff / omegaoff (or
+ * NULL) 3 doubles per dataset. Writes par->pen.base[1..n] to base and
+ * returns the penalty sum. */
+double ref_penalties(void *h, int n, const int *type, const double *weight, const shape_spin_state *sp,
+                     const double *angleoff, const double *omegaoff, double *base)
+{
+    ref_session *S = h;
+    struct vertices_t *real = &S->mod.shape.comp[0].real;
+    if (!real->s) setupsides(real);
+    if (sp) {
+        S->mod.spin.n_impulse = sp->n_impulse;
+        for (int j = 0; j < 3; j++) S->mod.spin.inertia[j].val = sp->inertia[j];
+        for (int k = 0; k < sp->n_impulse; k++)
+            for (int j = 0; j < 3; j++) S->mod.spin.impulse[k][j].val = sp->impulse[k][j];
+    }
+    for (int s = 0; s < S->dat.nsets; s++)
+        for (int j = 0; j < 3; j++) {
+            S->dat.set[s].angleoff[j].val = angleoff ? angleoff[3 * s + j] : 0.0;
+            S->dat.set[s].omegaoff[j].val = omegaoff ? omegaoff[3 * s + j] : 0.0;
+        }
+    realize_mod(&S->par, &S->mod);
+    struct par_t *par = &S->par;
+    par->pen.n = n;
+    par->pen.type = calloc((size_t)n + 1, sizeof(int));
+    par->pen.weight = calloc((size_t)n + 1, sizeof(double));
+    par->pen.base = calloc((size_t)n + 1, sizeof(double));
+    for (int i = 0; i < n; i++) {
+        par->pen.type[i + 1] = type[i];
+        par->pen.weight[i + 1] = weight[i];
+    }
+    par->showstate = 0;
+    double sum = penalties(par, &S->mod, &S->dat);
+    for (int i = 0; i < n; i++) base[i] = par->pen.base[i + 1];
+    free(par->pen.type);
+    free(par->pen.weight);
+    free(par->pen.base);
+    par->pen.n = 0;
+    par->pen.type = NULL;
+    par->pen.weight = par->pen.base = NULL;
+    return sum;
+}

@@ -34,6 +34,7 @@ UNITS = [
     ("fit.cu", ["-fmad=false"]),
     ("server.cu", ["-fmad=false"]),
     ("spin.cu", ["-fmad=false"]),
+    ("penalty.cu", ["-fmad=false"]),
 ]
 
 HEADERS = ["engine_internal.h", "engine_impl.h", "kernels.h", "raster_impl.cuh"]

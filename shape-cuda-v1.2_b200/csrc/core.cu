@@ -824,6 +824,7 @@ __device__ void summary_totals(const SummaryArgs &a, Term term)
     if (posbnd) err *= a.bad_objfactor * exp(out.posbnd_logfactor);
     if (badradar) err *= a.bad_objfactor * exp(out.badradar_logfactor);
     out.objective = err;
+    out.penalties = 0.0;
     *a.out = out;
 }
 

@@ -151,6 +151,7 @@ int EngineImpl::finalize()
     mem.release();
     invalidate_graphs();
     d_work_sorted = nullptr;
+    d_sides = nullptr; d_msum_part = d_msum = nullptr;
     cap = fixed_cap > 0 ? fixed_cap : 512;
     geoms.clear(); fh.clear(); work.clear(); view_work0.clear(); view_nwork.clear();
     chi2_items.clear(); frame_view.clear(); dop_extra.clear(); set_delpp.clear(); set_doppp.clear();
@@ -620,6 +621,213 @@ int EngineImpl::refresh_views()
     return SHAPE_OK;
 }
 
+// ---- penalties (src/shape/penalties.c:121-1236)
+
+static bool pen_needs_spin(int t)
+{
+    return t == SHAPE_PEN_INERTIADEV || t == SHAPE_PEN_NONPA || t == SHAPE_PEN_IMPULSE;
+}
+
+int EngineImpl::set_penalties(int n, const int *type, const double *weight)
+{
+    if (n < 0 || (n > 0 && (!type || !weight))) return set_err(SHAPE_E_ARG, "set_penalties: invalid argument");
+    for (int i = 0; i < n; i++) {
+        switch (type[i]) {
+        case SHAPE_PEN_NONSMOOTH: case SHAPE_PEN_CONCAVITY: case SHAPE_PEN_RDEV: case SHAPE_PEN_VOLUME:
+        case SHAPE_PEN_COMDEV: case SHAPE_PEN_INERTIADEV: case SHAPE_PEN_INERTIADEV_UNI: case SHAPE_PEN_PA3TILT:
+        case SHAPE_PEN_NONPA: case SHAPE_PEN_NONPA_UNI: case SHAPE_PEN_EULEROFFS: case SHAPE_PEN_FLATTENING:
+        case SHAPE_PEN_MAXRDEV: case SHAPE_PEN_IMPULSE:
+            break;
+        default:
+            return set_err(SHAPE_E_UNSUPPORTED, "set_penalties: penalty type not supported");
+        }
+    }
+    pen_type.assign(type, type + n);
+    pen_weight.assign(weight, weight + n);
+    pen_base.assign((size_t)n, 0.0);
+    return SHAPE_OK;
+}
+
+// Before an evaluation with penalties: the spin model where a penalty needs
+// it, the edges of the closed triangulated surface (each with its two
+// facets) and the device buffers of the model sums, built on first use.
+int EngineImpl::prepare_penalties()
+{
+    for (int t : pen_type)
+        if (pen_needs_spin(t) && !have_spin)
+            return set_err(SHAPE_E_STATE, "penalties: inertiadev, nonpa and impulse need the spin model");
+    if (!d_sides) {
+        struct Half { long long key; int f, j; };
+        std::vector<Half> hs;
+        hs.reserve(3 * (size_t)nf);
+        for (int f = 0; f < nf; f++)
+            for (int j = 0; j < 3; j++) {
+                const long long a = fv[3 * f + j], b = fv[3 * f + (j + 1) % 3];
+                hs.push_back(Half{std::min(a, b) * (long long)nv + std::max(a, b), f, j});
+            }
+        std::sort(hs.begin(), hs.end(), [](const Half &x, const Half &y) {
+            return x.key != y.key ? x.key < y.key : x.f < y.f;
+        });
+        std::vector<int4> sides;
+        for (size_t k = 0; k < hs.size(); k += 2) {
+            if (k + 1 >= hs.size() || hs[k + 1].key != hs[k].key || (k + 2 < hs.size() && hs[k + 2].key == hs[k].key))
+                return set_err(SHAPE_E_ARG, "penalties: the model is not a closed surface (an edge without two facets)");
+            const Half &h1 = hs[k];
+            sides.push_back(make_int4(fv[3 * h1.f + h1.j], fv[3 * h1.f + (h1.j + 2) % 3], h1.f, hs[k + 1].f));
+        }
+        nsides = (int)sides.size();
+        int rc;
+        if ((rc = mem.alloc(&d_sides, sides.size())) != SHAPE_OK) return rc;
+        if ((rc = mem.alloc(&d_msum_part, (size_t)model_sums_blocks() * MSUM_N)) != SHAPE_OK) return rc;
+        if ((rc = mem.alloc(&d_msum, (size_t)MSUM_N)) != SHAPE_OK) return rc;
+        if (!h_msum) CK(cudaMallocHost((void **)&h_msum, sizeof(double) * MSUM_N));
+        CK(cudaMemcpyAsync(d_sides, sides.data(), sizeof(int4) * sides.size(), cudaMemcpyHostToDevice, stream));
+    }
+    return SHAPE_OK;
+}
+
+// The two model-sum launches and the copy of the sums to pinned memory, on
+// the engine stream after the evaluation.
+int EngineImpl::enqueue_model_sums()
+{
+    ModelSumArgs a;
+    a.m = md;
+    a.sides = d_sides;
+    a.nsides = nsides;
+    a.part = d_msum_part;
+    a.out = d_msum;
+    launch_model_sums(a, stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_msum, d_msum, sizeof(double) * MSUM_N, cudaMemcpyDeviceToHost, stream));
+    return SHAPE_OK;
+}
+
+// Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations
+// (Jacobi's method; each rotation through the smaller angle, |tan| <= 1), so
+// every eigenvalue stays at the diagonal position it converges from: d =
+// eigenvalues, columns of V = eigenvectors (principal axes in body
+// coordinates). Converges quadratically; 50 sweeps bound it.
+static void jacobi3(const double A[3][3], double d[3], double V[3][3])
+{
+    double a[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) { a[i][j] = A[i][j]; V[i][j] = (i == j) ? 1.0 : 0.0; }
+    for (int sweep = 0; sweep < 50; sweep++) {
+        if (a[0][1] == 0.0 && a[0][2] == 0.0 && a[1][2] == 0.0) break;
+        for (int p = 0; p < 2; p++)
+            for (int q = p + 1; q < 3; q++) {
+                const double apq = a[p][q];
+                if (apq == 0.0) continue;
+                if (std::fabs(apq) <= 1e-18 * std::fabs(a[p][p]) && std::fabs(apq) <= 1e-18 * std::fabs(a[q][q])) {
+                    a[p][q] = a[q][p] = 0.0;        // below the diagonals' rounding
+                    continue;
+                }
+                const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
+                double t = 1.0 / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                if (theta < 0.0) t = -t;
+                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < 3; k++) {        // columns p, q of A J
+                    const double akp = a[k][p], akq = a[k][q];
+                    a[k][p] = c * akp - s * akq;
+                    a[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; k++) {        // rows p, q of J^T (A J)
+                    const double apk = a[p][k], aqk = a[q][k];
+                    a[p][k] = c * apk - s * aqk;
+                    a[q][k] = s * apk + c * aqk;
+                }
+                a[p][q] = a[q][p] = 0.0;
+                for (int k = 0; k < 3; k++) {
+                    const double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - s * vkq;
+                    V[k][q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    for (int i = 0; i < 3; i++) d[i] = a[i][i];
+}
+
+// The penalty sum of the objective from the model sums (each penalty's
+// value as src/shape/penalties.c:149-1220 defines it; weight >= 0 gives
+// |weight| * value, a negative weight |weight| / max(value, 1e-10)).
+double EngineImpl::penalty_sum(const double *ms)
+{
+    const double PIE = 3.141592653589793, R2D = 57.29577951308232;
+    const double V = ms[MSUM_VOLUME];
+    const double com[3] = {ms[MSUM_COM] / V, ms[MSUM_COM + 1] / V, ms[MSUM_COM + 2] / V};
+    const double I[3][3] = {{ms[MSUM_IXX], ms[MSUM_IXY], ms[MSUM_IXZ]},
+                            {ms[MSUM_IXY], ms[MSUM_IYY], ms[MSUM_IYZ]},
+                            {ms[MSUM_IXZ], ms[MSUM_IYZ], ms[MSUM_IZZ]}};
+    const double r_eff = pow(3 * V / (4 * PIE), 1.0 / 3.0);
+    bool got_pa = false;
+    double pm[3] = {0, 0, 0}, ap[3][3];
+    auto principal = [&]() { if (!got_pa) { jacobi3(I, pm, ap); got_pa = true; } };
+    auto inertia_dev = [&](const double *p) {
+        double a = 0.0, b = 0.0, adotb = 0.0;
+        for (int j = 0; j < 3; j++) {
+            a += p[j] * p[j];
+            adotb += p[j] * I[j][j];
+            for (int k = 0; k < 3; k++) b += I[j][k] * I[j][k];
+        }
+        return 1 - adotb / sqrt(a * b);
+    };
+    auto nonpa = [](const double *p) {
+        const double pen = std::max(p[0] / p[2] - 1, p[1] / p[2] - 1) + 0.01;
+        return pen < 0.0 ? 0.0 : pen;
+    };
+    double sum = 0.0;
+    for (size_t i = 0; i < pen_type.size(); i++) {
+        double pen = 0.0;
+        switch (pen_type[i]) {
+        case SHAPE_PEN_NONSMOOTH: pen = ms[MSUM_NONSMOOTH] / nsides; break;
+        case SHAPE_PEN_CONCAVITY: pen = ms[MSUM_CONCAVITY] / nsides; break;
+        case SHAPE_PEN_RDEV: pen = ms[MSUM_RDEV] / (r_eff * r_eff) / nv; break;
+        case SHAPE_PEN_MAXRDEV: pen = ms[MSUM_RDEV_MAX] / (r_eff * r_eff); break;
+        case SHAPE_PEN_VOLUME: pen = V; break;
+        case SHAPE_PEN_COMDEV:
+            for (int k = 0; k < 3; k++) pen += com[k] * com[k];
+            pen /= (r_eff * r_eff);
+            break;
+        case SHAPE_PEN_INERTIADEV: pen = inertia_dev(spin_st.inertia); break;
+        case SHAPE_PEN_INERTIADEV_UNI: principal(); pen = inertia_dev(pm); break;
+        case SHAPE_PEN_PA3TILT: principal(); pen = std::max(0.0, 1 - ap[2][2] * ap[2][2]); break;
+        case SHAPE_PEN_NONPA: pen = nonpa(spin_st.inertia); break;
+        case SHAPE_PEN_NONPA_UNI: principal(); pen = nonpa(pm); break;
+        case SHAPE_PEN_EULEROFFS: {
+            int ntot = 0;
+            for (size_t k = 0; k < setrecs.size(); k++)
+                for (int j = 0; j < 3; j++) {
+                    const double ao = have_spin ? spin_angleoff[3 * k + j] : 0.0;
+                    const double oo = have_spin ? spin_omegaoff[3 * k + j] : 0.0;
+                    pen += ao * ao;
+                    pen += oo * oo;
+                    ntot += 2;
+                }
+            pen *= R2D * R2D / ntot;
+            break;
+        }
+        case SHAPE_PEN_FLATTENING: {
+            principal();
+            const double b_over_c =
+                sqrt(std::min(-pm[0] + pm[1] + pm[2], pm[0] - pm[1] + pm[2]) / (pm[0] + pm[1] - pm[2]));
+            if (b_over_c > 1.0) {
+                const double x = b_over_c - 1;
+                pen = x * x * x * x;
+            }
+            break;
+        }
+        case SHAPE_PEN_IMPULSE:
+            for (int n = 0; n < spin_st.n_impulse; n++)
+                for (int j = 0; j < 3; j++) pen += spin_st.impulse[n][j] * spin_st.impulse[n][j];
+            pen *= R2D * R2D / (3 * spin_st.n_impulse);
+            break;
+        }
+        pen_base[i] = pen_weight[i] >= 0.0 ? pen : 1.0 / std::max(pen, 1.0e-10);
+        sum += fabs(pen_weight[i]) * pen_base[i];
+    }
+    return sum;
+}
+
 // Bin autotuning from a dry-run binning of the model as loaded: the bin
 // capacity becomes the next power of two above 1.25x the fullest tile (so a
 // fit's small model changes do not overflow into the full-scan path), and
@@ -908,6 +1116,7 @@ int EngineImpl::kernels_per_eval(int form) const
     }
     n += lcdev.empty() ? 0 : 1;          // lightcurve finalize
     n += dop_frames.empty() ? 0 : 1;     // Doppler overflow spectra
+    n += pen_type.empty() ? 0 : 2;       // model sums for the penalties
     return n + 1;                        // finalize + summary (with the chi-square partials when fused)
 }
 
@@ -929,12 +1138,17 @@ int EngineImpl::launch(int form)
     fill_params(h_params);
     double sc[3];
     effective_scale(sc, &pending_baddiam, &pending_bdl);
+    if (!pen_type.empty()) {
+        int rc = prepare_penalties();
+        if (rc) return rc;
+    }
     if (form == SHAPE_FORM_PLAIN_FP64) {
         CK(cudaEventRecord(ev0, s));
         CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s));
         int rc = enqueue(form);
         if (rc) return rc;
         CK(cudaMemcpyAsync(h_summary, d_summary, sizeof(shape_eval_summary), cudaMemcpyDeviceToHost, s));
+        if (!pen_type.empty() && (rc = enqueue_model_sums()) != SHAPE_OK) return rc;
         CK(cudaEventRecord(ev1, s));
     } else {
         if (gexec[form] && graph_keep_pos[form] != keep_pos) {
@@ -958,6 +1172,10 @@ int EngineImpl::launch(int form)
         }
         CK(cudaEventRecord(ev0, s));
         CK(cudaGraphLaunch(gexec[form], s));
+        if (!pen_type.empty()) {
+            int rc = enqueue_model_sums();
+            if (rc) return rc;
+        }
         CK(cudaEventRecord(ev1, s));
     }
     last_form = form;
@@ -979,8 +1197,18 @@ int EngineImpl::finish(shape_eval_summary *out)
     CK(cudaEventSynchronize(ev1));
     CK(cudaEventElapsedTime(&last_ms, ev0, ev1));
     shape_eval_summary sm = *h_summary;
-    // bad-diameter factor depends only on the host-side scale factors
-    if (pending_baddiam) {
+    sm.penalties = 0.0;
+    if (!pen_type.empty()) {
+        // objective() (src/shape/bestfit.c:789-866): reduced chi-square plus
+        // penalties, then the bad-model factors
+        sm.penalties = penalty_sum(h_msum);
+        double err = sm.chi2 / sm.dof + sm.penalties;
+        if (pending_baddiam) err *= bad_objfactor * exp(pending_bdl);
+        if (sm.posbnd) err *= bad_objfactor * exp(sm.posbnd_logfactor);
+        if (sm.badradar) err *= bad_objfactor * exp(sm.badradar_logfactor);
+        sm.objective = err;
+    } else if (pending_baddiam) {
+        // bad-diameter factor depends only on the host-side scale factors
         const double bdl = pending_bdl;
         sm.objective = sm.chi2 / sm.dof * (bad_objfactor * exp(bdl));
         if (sm.posbnd) sm.objective *= bad_objfactor * exp(sm.posbnd_logfactor);
@@ -1473,6 +1701,21 @@ int shape_engine_get_spin_param(shape_engine *h, int kind, int index, double *va
                                   "get_spin_param: no such spin parameter");
     *value = *p;
     return SHAPE_OK;
+}
+
+int shape_engine_set_penalties(shape_engine *h, int n, const int *type, const double *weight)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "set_penalties: null argument");
+    return h->impl.set_penalties(n, type, weight);
+}
+
+int shape_engine_get_penalties(shape_engine *h, double *base, int max)
+{
+    if (!h || (max > 0 && !base)) return shape::set_err(SHAPE_E_ARG, "get_penalties: null argument");
+    const EngineImpl &E = h->impl;
+    const int n = std::min<int>(max, (int)E.pen_base.size());
+    for (int i = 0; i < n; i++) base[i] = E.pen_base[i];
+    return (int)E.pen_base.size();
 }
 
 int shape_engine_set_fp32_exact(shape_engine *h, int exact)

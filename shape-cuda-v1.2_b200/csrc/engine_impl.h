@@ -154,6 +154,18 @@ struct EngineImpl {
     double *d_ovf = nullptr, *d_ovf_out = nullptr;
     int *d_dop_frames = nullptr;
 
+    // penalty terms of the objective (shape_engine_set_penalties)
+    std::vector<int> pen_type;
+    std::vector<double> pen_weight, pen_base;
+    int nsides = 0;                         // edges of the closed surface
+    int4 *d_sides = nullptr;                // (v1, f1's third vertex, f1, f2); built on first use
+    double *d_msum_part = nullptr, *d_msum = nullptr;
+    double *h_msum = nullptr;               // pinned [MSUM_N]
+    int set_penalties(int n, const int *type, const double *weight);
+    int prepare_penalties();
+    int enqueue_model_sums();
+    double penalty_sum(const double *ms);
+
     // pinned staging
     double *h_params = nullptr;             // r[nv], scale[3]
     shape_eval_summary *h_summary = nullptr;
@@ -173,6 +185,7 @@ struct EngineImpl {
         mem.release();
         if (h_params) { cudaFreeHost(h_params); h_params = nullptr; }
         if (h_summary) { cudaFreeHost(h_summary); h_summary = nullptr; }
+        if (h_msum) { cudaFreeHost(h_msum); h_msum = nullptr; }
         if (ev0) { cudaEventDestroy(ev0); ev0 = nullptr; }
         if (ev1) { cudaEventDestroy(ev1); ev1 = nullptr; }
         for (auto &e : evf)

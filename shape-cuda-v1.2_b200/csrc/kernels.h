@@ -78,6 +78,21 @@ struct RasterArgs {
 void launch_realize(const ModelDev &m, cudaStream_t s);      // launch_realize_vf + launch_realize_vn
 void launch_realize_vf(const ModelDev &m, cudaStream_t s);   // vertices, facet normals and areas
 void launch_realize_vn(const ModelDev &m, cudaStream_t s);   // vertex normals (after _vf)
+
+// Model sums for the penalty terms (penalty.cu), in this order.
+enum {
+    MSUM_VOLUME, MSUM_COM, MSUM_IXX = MSUM_COM + 3, MSUM_IYY, MSUM_IZZ, MSUM_IXY, MSUM_IXZ, MSUM_IYZ,
+    MSUM_NONSMOOTH, MSUM_CONCAVITY, MSUM_RDEV, MSUM_RDEV_MAX, MSUM_N
+};
+struct ModelSumArgs {
+    ModelDev m;                 // realized model (vx, fn, fv, u, r, scale)
+    const int4 *sides;          // edges: (end vertex v1, f1's third vertex, f1, f2)
+    int nsides;
+    double *part;               // [model_sums_blocks() * MSUM_N]
+    double *out;                // [MSUM_N]
+};
+int model_sums_blocks();
+void launch_model_sums(const ModelSumArgs &a, cudaStream_t s);   // two launches
 void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, cudaStream_t s);
 // pdl: programmatic dependent launch (launch_k)
 void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt,

@@ -31,6 +31,11 @@ PAR_SPIN_LIB = 8
 PAR_ANGLEOFF = 9
 PAR_OMEGAOFF = 10
 
+# penalty types (the reference's numbering)
+PEN_NONSMOOTH, PEN_CONCAVITY, PEN_RDEV, PEN_VOLUME, PEN_COMDEV = 9, 10, 11, 12, 13
+PEN_INERTIADEV, PEN_INERTIADEV_UNI, PEN_PA3TILT, PEN_NONPA, PEN_NONPA_UNI = 14, 15, 16, 17, 18
+PEN_EULEROFFS, PEN_FLATTENING, PEN_MAXRDEV, PEN_IMPULSE = 19, 20, 21, 25
+
 
 class FitParam(C.Structure):
     _fields_ = [("kind", C.c_int), ("index", C.c_int), ("step", C.c_double), ("tol", C.c_double),
@@ -67,7 +72,8 @@ class ServerStats(C.Structure):
 class EvalSummary(C.Structure):
     _fields_ = [("chi2", C.c_double), ("dof", C.c_double), ("chi2_deldop", C.c_double),
                 ("chi2_lghtcrv", C.c_double), ("posbnd", C.c_int), ("posbnd_logfactor", C.c_double),
-                ("badradar", C.c_int), ("badradar_logfactor", C.c_double), ("objective", C.c_double)]
+                ("badradar", C.c_int), ("badradar_logfactor", C.c_double), ("objective", C.c_double),
+                ("penalties", C.c_double)]
 
 
 ABI_ORDER = ["shape_model_desc", "shape_radar_law", "shape_optical_law", "shape_eval_params",
@@ -122,6 +128,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_set_point_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.dptr]
     L.shape_engine_set_spin_model.argtypes = [vp, P(cd.SpinState), cd.dptr, cd.dptr, cd.dptr, cd.dptr]
     L.shape_engine_set_spin_param.argtypes = [vp, C.c_int, C.c_int, C.c_double]
+    L.shape_engine_set_penalties.argtypes = [vp, C.c_int, P(C.c_int), cd.dptr]
+    L.shape_engine_get_penalties.argtypes = [vp, cd.dptr, C.c_int]
     L.shape_engine_get_spin_param.argtypes = [vp, C.c_int, C.c_int, P(C.c_double)]
     L.shape_realize_spin.argtypes = [P(cd.SpinState), cd.dptr, cd.dptr, C.c_int, cd.dptr, cd.dptr, cd.dptr,
                                      cd.dptr]
@@ -288,6 +296,19 @@ class Engine:
                 for v in (angleoff, omegaoff, frame_t, frame_orbspin)]
         ptrs = [cd.as_dptr(v) if v is not None else None for v in keep]
         _chk(self.L.shape_engine_set_spin_model(self.h, C.byref(spin), *ptrs))
+
+    def set_penalties(self, penalties):
+        """penalties: list of (type, weight); [] removes them."""
+        n = len(penalties)
+        types = (C.c_int * max(1, n))(*[int(t) for t, _ in penalties])
+        w = np.array([float(x) for _, x in penalties] or [0.0])
+        _chk(self.L.shape_engine_set_penalties(self.h, n, types, cd.as_dptr(w)))
+
+    def penalties(self):
+        """Each penalty's base value at the last evaluation."""
+        out = np.zeros(64)
+        n = _chk(self.L.shape_engine_get_penalties(self.h, cd.as_dptr(out), 64))
+        return out[:n].copy()
 
     def set_spin_param(self, kind, index, value):
         _chk(self.L.shape_engine_set_spin_param(self.h, int(kind), int(index), float(value)))
