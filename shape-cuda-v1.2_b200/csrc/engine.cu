@@ -1227,7 +1227,7 @@ using shape::EngineImpl;
 extern "C" {
 
 const char *shape_last_error(void) { return shape::g_err.c_str(); }
-const char *shape_version(void) { return "shape-b200 0.1 (sm_100a)"; }
+const char *shape_version(void) { return "shape-b200 0.2 (sm_100a)"; }
 
 int shape_abi_sizes(size_t *out, int max)
 {
