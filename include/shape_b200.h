@@ -392,6 +392,39 @@ typedef struct shape_server_stats {
 int shape_realize_spin(const shape_spin_state *spin, const double angleoff[3], const double omegaoff[3], int n,
                        const double *t, const double *orbspin, double *ae, double *spin_out);
 
+/* ------------------------------------------------------------- model files */
+
+/* A SHAPE model file (.mod) as read_mod reads it (src/shape/read_mod.c:204-227,
+ * read_shape :289-542, read_photo :544-1953, read_spin :1954-2140), for the
+ * models the engine evaluates: one vertex component with zero component
+ * offsets and rotations, radar laws none / cosine / gaussian / hagfors /
+ * cosine_qs / gauss+cosine / hagfors+cosine / cosine+cosine, optical laws
+ * none / lambertian / lommel / kaasalainen, and the spin section. Comments
+ * in curly braces are skipped; numbers must fill their token. Angles come
+ * out in radians, spin rates in rad/day and epochs in Julian days, by
+ * read_spin's operations. Syntax errors return SHAPE_E_ARG and valid but
+ * unsupported content SHAPE_E_UNSUPPORTED, both with the line number in
+ * shape_last_error(). Host code; the handle owns all arrays. */
+typedef struct shape_mod_file shape_mod_file;
+int shape_mod_read(const char *path, shape_mod_file **out);
+void shape_mod_free(shape_mod_file *m);
+/* The shape as shape_engine_set_model takes it (arrays owned by m; the
+ * attached-facet lists in increasing facet order, as setupvertices builds
+ * them). */
+int shape_mod_model(const shape_mod_file *m, shape_model_desc *out);
+/* Law ilaw of the file; returns the number of laws (law = NULL: count
+ * only). A "none" law has type 0. */
+int shape_mod_radar_law(const shape_mod_file *m, int ilaw, shape_radar_law *law);
+int shape_mod_optical_law(const shape_mod_file *m, int ilaw, shape_optical_law *law);
+/* The spin state (pa set as read_spin sets it). */
+int shape_mod_spin(const shape_mod_file *m, shape_spin_state *spin);
+/* The file's floating parameters (state f) that the engine can vary, in the
+ * reference's parameter-list order (src/shape/mkparlist.c): scale factors,
+ * vertex deviations, spin angles, spin rates, moments of inertia, spin-rate
+ * changes, impulses, libration. kind and index are set, step and the
+ * tolerances are 0 (they come from the .par file). Returns the count. */
+int shape_mod_free_params(const shape_mod_file *m, shape_fit_param *out, int max);
+
 int shape_server_create(int device, size_t hbm_budget_bytes, int max_slots, shape_server **out);
 void shape_server_destroy(shape_server *s);
 /* engine: a configured engine (model and datasets added; it need not be

@@ -218,6 +218,13 @@ class Reference:
         L.ref_penalties.argtypes = [C.c_void_p, C.c_int, cd.iptr, cd.dptr, P(cd.SpinState), cd.dptr, cd.dptr,
                                     cd.dptr]
         L.ref_penalties.restype = C.c_double
+        L.ref_mod_read.argtypes = [C.c_char_p]
+        L.ref_mod_read.restype = C.c_void_p
+        L.ref_mod_shape.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), cd.dptr, cd.dptr, cd.dptr, cd.dptr,
+                                    cd.iptr, cd.iptr, cd.iptr]
+        L.ref_mod_radar.argtypes = [C.c_void_p, C.c_int, P(cd.RadarLaw)]
+        L.ref_mod_optical.argtypes = [C.c_void_p, C.c_int, P(cd.OpticalLaw)]
+        L.ref_mod_spin.argtypes = [C.c_void_p, P(cd.SpinState)]
         L.ref_get_seen.argtypes = [C.c_void_p, C.c_char_p]
         L.ref_get_deldop_frame.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr, cd.dptr,
                                            cd.dptr, cd.iptr, P(cd.DeldopResult)]
@@ -257,6 +264,35 @@ class Reference:
             keep.append(arr)
             self.lib.ref_add_lghtcrv_set(h, C.byref(ls.bind()), arr)
         return RefSession(self, h, model, keep)
+
+    def read_mod(self, path):
+        """The reference's read_mod on a model file: (arrays, radar laws,
+        optical laws, spin state), arrays as shape_model_desc holds them."""
+        h = self.lib.ref_mod_read(os.fsencode(path))
+        nv, nf = C.c_int(), C.c_int()
+        self.lib.ref_mod_shape(h, C.byref(nv), C.byref(nf), None, None, None, None, None, None, None)
+        nv, nf = nv.value, nf.value
+        a, u, r, sc = np.zeros(3 * nv), np.zeros(3 * nv), np.zeros(nv), np.zeros(3)
+        fv, ap, ai = np.zeros(3 * nf, np.int32), np.zeros(nv + 1, np.int32), np.zeros(3 * nf, np.int32)
+        i32 = lambda x: x.ctypes.data_as(cd.iptr)
+        self.lib.ref_mod_shape(h, C.byref(C.c_int()), C.byref(C.c_int()), cd.as_dptr(a), cd.as_dptr(u),
+                               cd.as_dptr(r), cd.as_dptr(sc), i32(fv), i32(ap), i32(ai))
+        radar, optical = [], []
+        n = self.lib.ref_mod_radar(h, -1, C.byref(cd.RadarLaw()))
+        for i in range(n):
+            law = cd.RadarLaw()
+            self.lib.ref_mod_radar(h, i, C.byref(law))
+            radar.append(law)
+        n = self.lib.ref_mod_optical(h, -1, C.byref(cd.OpticalLaw()))
+        for i in range(n):
+            olaw = cd.OpticalLaw()
+            self.lib.ref_mod_optical(h, i, C.byref(olaw))
+            optical.append(olaw)
+        spin = cd.SpinState()
+        self.lib.ref_mod_spin(h, C.byref(spin))
+        arrays = {"a": a.reshape(nv, 3), "u": u.reshape(nv, 3), "r": r, "scale": sc, "fv": fv.reshape(nf, 3),
+                  "af_ptr": ap, "af_idx": ai}
+        return arrays, radar, optical, spin
 
     def mnbrak(self, fn, ax, bx):
         cb = OBJFN(fn)

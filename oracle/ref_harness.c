@@ -684,3 +684,106 @@ double ref_penalties(void *h, int n, const int *type, const double *weight, cons
     par->pen.weight = par->pen.base = NULL;
     return sum;
 }
+
+
+/* The reference's read_mod (src/shape/read_mod.c:204-227) on a model file:
+ * the check of shape_mod_read. The ref_mod_* getters copy the result into
+ * the engine's descriptor types. */
+typedef struct { struct par_t par; struct mod_t mod; } ref_modfile;
+
+void *ref_mod_read(const char *path)
+{
+    ref_modfile *F = calloc(1, sizeof *F);
+    F->par.action = FIT;
+    snprintf(F->mod.name, sizeof F->mod.name, "%s", path);
+    read_mod(&F->par, &F->mod);
+    return F;
+}
+
+/* Sizes into nv / nf; the arrays (each may be NULL) as shape_model_desc
+ * holds them. */
+void ref_mod_shape(void *h, int *nv, int *nf, double *a, double *u, double *r, double *scale, int *fv,
+                   int *af_ptr, int *af_idx)
+{
+    ref_modfile *F = h;
+    struct vertices_t *real = &F->mod.shape.comp[0].real;
+    *nv = real->nv;
+    *nf = real->nf;
+    for (int j = 0; j < 3 && scale; j++) scale[j] = real->scalefactor[j].val;
+    int k = 0;
+    for (int i = 0; i < real->nv; i++) {
+        for (int j = 0; j < 3; j++) {
+            if (a) a[3 * i + j] = real->v[i].a[j];
+            if (u) u[3 * i + j] = real->v[i].u[j];
+        }
+        if (r) r[i] = real->v[i].r.val;
+        if (af_ptr) af_ptr[i] = k;
+        for (int q = 0; q < real->v[i].naf; q++, k++)
+            if (af_idx) af_idx[k] = real->v[i].af[q];
+    }
+    if (af_ptr) af_ptr[real->nv] = k;
+    for (int f = 0; f < real->nf && fv; f++)
+        for (int j = 0; j < 3; j++) fv[3 * f + j] = real->f[f].v[j];
+}
+
+int ref_mod_radar(void *h, int i, shape_radar_law *L)
+{
+    ref_modfile *F = h;
+    struct photo_t *ph = &F->mod.photo;
+    memset(L, 0, sizeof *L);
+    if (i < 0 || i >= ph->nradlaws) return ph->nradlaws;      /* count only */
+    L->type = ph->radtype[i] == NOLAW ? 0 : ph->radtype[i];
+    switch (ph->radtype[i]) {
+    case COSINELAW_DIFF:
+        L->diff_R = ph->radar[i].RC.R.val; L->diff_C = ph->radar[i].RC.C.val; break;
+    case GAUSSIANLAW: case HAGFORSLAW: case COSINELAW_QS:
+        L->qs_R = ph->radar[i].quasispec.R.val; L->qs_C = ph->radar[i].quasispec.C.val;
+        L->qs_cos_cutoff = ph->radar[i].quasispec.cos_cutoff; break;
+    case GAUSSIAN_COSINE: case HAGFORS_COSINE: case COSINE_COSINE:
+        L->qs_R = ph->radar[i].hybrid.qs.R.val; L->qs_C = ph->radar[i].hybrid.qs.C.val;
+        L->qs_cos_cutoff = ph->radar[i].hybrid.qs.cos_cutoff;
+        L->diff_R = ph->radar[i].hybrid.diff.R.val; L->diff_C = ph->radar[i].hybrid.diff.C.val; break;
+    default: break;
+    }
+    return ph->nradlaws;
+}
+
+int ref_mod_optical(void *h, int i, shape_optical_law *L)
+{
+    ref_modfile *F = h;
+    struct photo_t *ph = &F->mod.photo;
+    memset(L, 0, sizeof *L);
+    if (i < 0 || i >= ph->noptlaws) return ph->noptlaws;      /* count only */
+    L->type = ph->opttype[i] == NOLAW ? 0 : ph->opttype[i];
+    if (ph->opttype[i] == KAASALAINEN) {
+        L->R = ph->optical[i].kaas.R.val; L->wt = ph->optical[i].kaas.wt.val;
+        L->A0 = ph->optical[i].kaas.A0.val; L->D = ph->optical[i].kaas.D.val;
+        L->k = ph->optical[i].kaas.k.val;
+    } else if (ph->opttype[i] == LAMBERTLAW || ph->opttype[i] == LOMMEL) {
+        L->R = ph->optical[i].R.R.val;
+    }
+    return ph->noptlaws;
+}
+
+void ref_mod_spin(void *h, shape_spin_state *sp)
+{
+    ref_modfile *F = h;
+    const struct spin_t *s = &F->mod.spin;
+    memset(sp, 0, sizeof *sp);
+    sp->pa = s->pa;
+    sp->t0 = s->t0;
+    for (int j = 0; j < 3; j++) {
+        sp->angle[j] = s->angle[j].val;
+        sp->omega[j] = s->omega[j].val;
+        sp->omegadot[j] = s->omegadot[j].val;
+        sp->inertia[j] = s->inertia[j].val;
+    }
+    sp->n_impulse = s->n_impulse;
+    for (int n = 0; n < s->n_impulse && n < SHAPE_MAX_IMPULSES; n++) {
+        sp->t_impulse[n] = s->t_impulse[n];
+        for (int j = 0; j < 3; j++) sp->impulse[n][j] = s->impulse[n][j].val;
+    }
+    sp->lib_amp = s->lib_amp.val;
+    sp->lib_freq = s->lib_freq.val;
+    sp->lib_phase = s->lib_phase.val;
+}

@@ -35,6 +35,7 @@ UNITS = [
     ("server.cu", ["-fmad=false"]),
     ("spin.cu", ["-fmad=false"]),
     ("penalty.cu", ["-fmad=false"]),
+    ("modfile.cu", []),
 ]
 
 HEADERS = ["engine_internal.h", "engine_impl.h", "kernels.h", "raster_impl.cuh"]

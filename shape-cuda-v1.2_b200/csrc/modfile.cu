@@ -1,0 +1,411 @@
+// Reader of SHAPE model files (.mod; read_mod, src/shape/read_mod.c:204-227)
+// for the models the engine evaluates: one vertex component (read_shape,
+// :289-542) with no component offsets, the homogeneous radar and optical
+// scattering laws (read_photo, :544-1953) and the spin section (read_spin,
+// :1954-2140). Host code.
+//
+// The file is a stream of whitespace-separated tokens with comments in
+// curly braces. A parameter is a state token (c, f or =) followed by its
+// value. Numbers are converted with strtod / strtol and must be the whole
+// token (src/util/getdouble.c, getint.c). Angles are stored in radians and
+// spin rates in rad/day, by the same operations as read_spin, and the
+// epochs in Julian days (cal2jd, src/astro/jdcal.c:8-13).
+#include <cerrno>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "shape_b200.h"
+
+namespace shape {
+int report_error(int code, const std::string &msg);   // engine.cu
+}
+
+struct shape_mod_file {
+    std::vector<double> a, u, r;
+    double scale[3];
+    std::vector<int> fv, af_ptr, af_idx;
+    char scale_state[3];
+    std::vector<char> r_state;
+    std::vector<shape_radar_law> radar;
+    std::vector<shape_optical_law> optical;
+    shape_spin_state spin;
+    char angle_state[3], omega_state[3], inertia_state[3], omegadot_state[3], lib_state[3];
+    char impulse_state[SHAPE_MAX_IMPULSES][3];
+};
+
+namespace {
+
+const double D2R = 0.01745329251994330;   // src/shape/const.h
+
+struct ParseError {
+    int code;
+    std::string msg;
+};
+
+class Tokens {
+public:
+    explicit Tokens(std::string text) : t_(std::move(text)) {}
+
+    // The next token, or false at the end of the file.
+    bool next(std::string &tok)
+    {
+        for (;;) {
+            while (p_ < t_.size() && isspace((unsigned char)t_[p_])) {
+                if (t_[p_] == '\n') line_++;
+                p_++;
+            }
+            if (p_ < t_.size() && t_[p_] == '{') {
+                while (p_ < t_.size() && t_[p_] != '}') {
+                    if (t_[p_] == '\n') line_++;
+                    p_++;
+                }
+                if (p_ >= t_.size()) fail("unclosed comment");
+                p_++;
+                continue;
+            }
+            break;
+        }
+        if (p_ >= t_.size()) return false;
+        const size_t b = p_;
+        while (p_ < t_.size() && !isspace((unsigned char)t_[p_]) && t_[p_] != '{') p_++;
+        tok.assign(t_, b, p_ - b);
+        return true;
+    }
+    std::string word(const char *what)
+    {
+        std::string s;
+        if (!next(s)) fail(std::string("end of file instead of ") + what);
+        return s;
+    }
+    int integer(const char *what)
+    {
+        const std::string s = word(what);
+        char *end = nullptr;
+        errno = 0;
+        const long v = strtol(s.c_str(), &end, 10);
+        if (*end != '\0' || errno == ERANGE || v < INT_MIN || v > INT_MAX)
+            fail(std::string("expected an integer (") + what + "), got " + s);
+        return (int)v;
+    }
+    double real(const char *what)
+    {
+        const std::string s = word(what);
+        char *end = nullptr;
+        const double v = strtod(s.c_str(), &end);
+        if (*end != '\0') fail(std::string("expected a number (") + what + "), got " + s);
+        return v;
+    }
+    // state (c, f or =) and value of a parameter
+    double param(const char *what, char *state)
+    {
+        const std::string s = word(what);
+        if (s != "c" && s != "f" && s != "=") fail(std::string("expected c, f or = before ") + what + ", got " + s);
+        if (state) *state = s[0];
+        return real(what);
+    }
+    [[noreturn]] void fail(const std::string &m, int code = SHAPE_E_ARG) const
+    {
+        throw ParseError{code, "model file line " + std::to_string(line_) + ": " + m};
+    }
+
+private:
+    std::string t_;
+    size_t p_ = 0;
+    int line_ = 1;
+};
+
+// Julian day number of a calendar date at noon: Gregorian from 1582
+// October 15 on, Julian before (Fliegel and Van Flandern 1968; the Julian
+// calendar form of the same construction). Integer division truncates.
+long julian_day_number(int yy, int mo, int dd)
+{
+    const bool gregorian = yy > 1582 || (yy == 1582 && (mo > 10 || (mo == 10 && dd >= 15)));
+    const long y = yy, m = mo, d = dd;
+    if (gregorian)
+        return (1461 * (y + 4800 + (m - 14) / 12)) / 4 + (367 * (m - 2 - 12 * ((m - 14) / 12))) / 12 -
+               (3 * ((y + 4900 + (m - 14) / 12) / 100)) / 4 + d - 32075;
+    return 367 * y - (7 * (y + 5001 + (m - 9) / 7)) / 4 + (275 * m) / 9 + d + 1729777;
+}
+
+// Six integers yyyy mm dd hh mm ss -> Julian date (days).
+double read_epoch(Tokens &tk, const char *what)
+{
+    int c[6];
+    for (int i = 0; i < 6; i++) c[i] = tk.integer(what);
+    if (c[0] <= 0 || c[1] < 1 || c[1] > 12 || c[2] < 1 || c[2] > 31) tk.fail(std::string("bad date in ") + what);
+    double jd = (double)julian_day_number(c[0], c[1], c[2]) - 0.5;
+    jd += ((c[3] * 60 + c[4]) * 60 + c[5]) / 86400.0;
+    return jd;
+}
+
+void read_shape(Tokens &tk, shape_mod_file &m)
+{
+    const int ncomp = tk.integer("number of components");
+    if (ncomp != 1) tk.fail("only one-component models are supported", SHAPE_E_UNSUPPORTED);
+    for (int j = 0; j < 6; j++) {
+        char st;
+        const double v = tk.param(j < 3 ? "component offset" : "component rotation", &st);
+        if (v != 0.0 || st == 'f')
+            tk.fail("component offsets and rotations must be held at zero", SHAPE_E_UNSUPPORTED);
+    }
+    const std::string type = tk.word("component type");
+    if (type != "vertex") tk.fail("component type " + type + ": only vertex components are supported",
+                                  SHAPE_E_UNSUPPORTED);
+    const int nv = tk.integer("number of vertices");
+    if (nv < 4) tk.fail("a vertex model needs at least 4 vertices");
+    for (int j = 0; j < 3; j++) m.scale[j] = tk.param("scale factor", &m.scale_state[j]);
+    if (m.scale_state[0] == '=') tk.fail("scale factor 0 cannot take the = state");
+    m.a.resize(3 * (size_t)nv);
+    m.u.resize(3 * (size_t)nv);
+    m.r.resize(nv);
+    m.r_state.resize(nv);
+    for (int v = 0; v < nv; v++) {
+        m.r[v] = tk.param("vertex deviation", &m.r_state[v]);
+        if (m.r_state[v] == '=')
+            tk.fail("mirrored vertex deviations (= state) are not supported", SHAPE_E_UNSUPPORTED);
+        for (int k = 0; k < 3; k++) m.u[3 * (size_t)v + k] = tk.real("vertex direction");
+        for (int k = 0; k < 3; k++) m.a[3 * (size_t)v + k] = tk.real("vertex base point");
+    }
+    const int nf = tk.integer("number of facets");
+    if (nf < 4) tk.fail("a vertex model needs at least 4 facets");
+    m.fv.resize(3 * (size_t)nf);
+    for (size_t k = 0; k < m.fv.size(); k++) {
+        m.fv[k] = tk.integer("facet vertex");
+        if (m.fv[k] < 0 || m.fv[k] >= nv) tk.fail("facet vertex index out of range");
+    }
+    // attached facets of each vertex, in increasing facet order
+    // (setupvertices, src/shape/read_mod.c:2504-2590)
+    m.af_ptr.assign((size_t)nv + 1, 0);
+    for (int v : m.fv) m.af_ptr[v + 1]++;
+    for (int v = 0; v < nv; v++) m.af_ptr[v + 1] += m.af_ptr[v];
+    m.af_idx.resize(m.fv.size());
+    std::vector<int> fill(m.af_ptr.begin(), m.af_ptr.end() - 1);
+    for (int f = 0; f < nf; f++)
+        for (int k = 0; k < 3; k++) m.af_idx[fill[m.fv[3 * (size_t)f + k]]++] = f;
+}
+
+void read_photo(Tokens &tk, shape_mod_file &m)
+{
+    const int nrad = tk.integer("number of radar laws");
+    if (nrad < 0) tk.fail("negative number of radar laws");
+    for (int i = 0; i < nrad; i++) {
+        const std::string s = tk.word("radar law");
+        shape_radar_law L;
+        memset(&L, 0, sizeof L);
+        auto cutoff = [&]() {
+            const double deg = tk.real("cutoff angle");
+            if (deg <= 0.0 || deg > 90.0) tk.fail("cutoff angle must be in (0, 90] deg");
+            return cos(deg * D2R);
+        };
+        if (s == "none") {
+            L.type = 0;
+        } else if (s == "cosine") {
+            L.type = SHAPE_RADLAW_COSINE_DIFF;
+            L.diff_R = tk.param("R", nullptr);
+            L.diff_C = tk.param("C", nullptr);
+        } else if (s == "gaussian" || s == "hagfors" || s == "cosine_qs") {
+            L.type = s == "gaussian" ? SHAPE_RADLAW_GAUSSIAN : s == "hagfors" ? SHAPE_RADLAW_HAGFORS
+                                                                               : SHAPE_RADLAW_COSINE_QS;
+            L.qs_R = tk.param("R", nullptr);
+            L.qs_C = tk.param("C", nullptr);
+            L.qs_cos_cutoff = cutoff();
+        } else if (s == "gauss+cosine" || s == "hagfors+cosine" || s == "cosine+cosine") {
+            L.type = s == "gauss+cosine" ? SHAPE_RADLAW_GAUSSIAN_COSINE
+                     : s == "hagfors+cosine" ? SHAPE_RADLAW_HAGFORS_COSINE : SHAPE_RADLAW_COSINE_COSINE;
+            L.qs_R = tk.param("R", nullptr);
+            L.qs_C = tk.param("C", nullptr);
+            L.qs_cos_cutoff = cutoff();
+            L.diff_R = tk.param("R", nullptr);
+            L.diff_C = tk.param("C", nullptr);
+        } else {
+            tk.fail("radar law " + s + " is not supported", SHAPE_E_UNSUPPORTED);
+        }
+        m.radar.push_back(L);
+    }
+    const int nopt = tk.integer("number of optical laws");
+    if (nopt < 0) tk.fail("negative number of optical laws");
+    for (int i = 0; i < nopt; i++) {
+        const std::string s = tk.word("optical law");
+        shape_optical_law L;
+        memset(&L, 0, sizeof L);
+        if (s == "none") {
+            L.type = 0;
+        } else if (s == "lambertian" || s == "lommel") {
+            L.type = s == "lambertian" ? SHAPE_OPTLAW_LAMBERT : SHAPE_OPTLAW_LOMMEL;
+            L.R = tk.param("R", nullptr);
+        } else if (s == "kaasalainen") {
+            L.type = SHAPE_OPTLAW_KAASALAINEN;
+            L.R = tk.param("R", nullptr);
+            L.wt = tk.param("wt", nullptr);
+            L.A0 = tk.param("A0", nullptr);
+            L.D = tk.param("D", nullptr);
+            L.k = tk.param("k", nullptr);
+            L.D *= D2R;
+            L.k /= D2R;
+        } else {
+            tk.fail("optical law " + s + " is not supported", SHAPE_E_UNSUPPORTED);
+        }
+        m.optical.push_back(L);
+    }
+}
+
+void read_spin(Tokens &tk, shape_mod_file &m)
+{
+    shape_spin_state &sp = m.spin;
+    memset(&sp, 0, sizeof sp);
+    sp.t0 = read_epoch(tk, "spin epoch");
+    for (int i = 0; i < 3; i++) sp.angle[i] = tk.param("spin angle", &m.angle_state[i]);
+    for (int i = 0; i < 3; i++) sp.omega[i] = tk.param("spin rate", &m.omega_state[i]);
+    for (int i = 0; i < 3; i++) sp.inertia[i] = tk.param("moment of inertia", &m.inertia_state[i]);
+    for (int i = 0; i < 3; i++) sp.omegadot[i] = tk.param("spin-rate change", &m.omegadot_state[i]);
+    sp.lib_amp = tk.param("libration amplitude", &m.lib_state[0]);
+    sp.lib_freq = tk.param("libration frequency", &m.lib_state[1]);
+    sp.lib_phase = tk.param("libration phase", &m.lib_state[2]);
+    sp.n_impulse = tk.integer("number of spin impulses");
+    if (sp.n_impulse < 0 || sp.n_impulse > SHAPE_MAX_IMPULSES) tk.fail("too many spin impulses");
+    for (int n = 0; n < sp.n_impulse; n++) {
+        sp.t_impulse[n] = read_epoch(tk, "spin impulse epoch");
+        if (n > 0 && sp.t_impulse[n] <= sp.t_impulse[n - 1])
+            tk.fail("spin impulses must be in increasing chronological order");
+        for (int i = 0; i < 3; i++) sp.impulse[n][i] = tk.param("spin impulse", &m.impulse_state[n][i]);
+    }
+    // principal-axis rotator: x and y spin held at zero and no x/y impulses
+    // (src/shape/read_mod.c:2060-2080)
+    sp.pa = 0;
+    if (sp.omega[0] == 0.0 && m.omega_state[0] == 'c' && sp.omega[1] == 0.0 && m.omega_state[1] == 'c') {
+        sp.pa = 1;
+        for (int n = 0; n < sp.n_impulse && sp.pa; n++)
+            if (sp.impulse[n][0] != 0.0 || m.impulse_state[n][0] == 'f' || sp.impulse[n][1] != 0.0 ||
+                m.impulse_state[n][1] == 'f')
+                sp.pa = 0;
+    }
+    const bool xy_dot = sp.omegadot[0] != 0 || m.omegadot_state[0] == 'f' || sp.omegadot[1] != 0 ||
+                        m.omegadot_state[1] == 'f';
+    if (sp.pa && xy_dot) tk.fail("a principal-axis rotator cannot have x or y spin-rate change");
+    if (!sp.pa && (xy_dot || sp.omegadot[2] != 0 || m.omegadot_state[2] == 'f' || sp.lib_amp != 0 ||
+                   m.lib_state[0] == 'f'))
+        tk.fail("a non-principal-axis rotator cannot have spin-rate change or libration");
+    // Euler angles "over the pole" folded back, all angles into [0, 360)
+    // deg, then radians and rad/day (src/shape/read_mod.c:2113-2135)
+    sp.angle[1] -= 360.0 * floor(sp.angle[1] / 360.0);
+    if (sp.angle[1] > 180.0) {
+        sp.angle[1] = 360.0 - sp.angle[1];
+        sp.angle[0] += 180.0;
+        sp.angle[2] += 180.0;
+    }
+    for (int i = 0; i < 3; i++) {
+        sp.angle[i] -= 360.0 * floor(sp.angle[i] / 360.0);
+        sp.angle[i] *= D2R;
+        sp.omega[i] *= D2R;
+        sp.omegadot[i] *= D2R;
+        for (int n = 0; n < sp.n_impulse; n++) sp.impulse[n][i] *= D2R;
+    }
+    sp.lib_amp *= D2R;
+    sp.lib_freq *= D2R;
+    sp.lib_phase *= D2R;
+}
+
+}  // namespace
+
+extern "C" {
+
+int shape_mod_read(const char *path, shape_mod_file **out)
+{
+    if (!path || !out) return shape::report_error(SHAPE_E_ARG, "mod_read: null argument");
+    *out = nullptr;
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return shape::report_error(SHAPE_E_ARG, std::string("mod_read: cannot open ") + path);
+    std::string text;
+    char buf[1 << 16];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, n);
+    fclose(fp);
+    shape_mod_file *m = new shape_mod_file();
+    memset(m->impulse_state, 'c', sizeof m->impulse_state);
+    try {
+        Tokens tk(std::move(text));
+        read_shape(tk, *m);
+        read_photo(tk, *m);
+        read_spin(tk, *m);
+    } catch (const ParseError &e) {
+        delete m;
+        return shape::report_error(e.code, e.msg);
+    }
+    *out = m;
+    return SHAPE_OK;
+}
+
+void shape_mod_free(shape_mod_file *m) { delete m; }
+
+int shape_mod_model(const shape_mod_file *m, shape_model_desc *out)
+{
+    if (!m || !out) return shape::report_error(SHAPE_E_ARG, "mod_model: null argument");
+    out->nv = (int)m->r.size();
+    out->nf = (int)(m->fv.size() / 3);
+    out->a = m->a.data();
+    out->u = m->u.data();
+    out->r = m->r.data();
+    for (int j = 0; j < 3; j++) out->scale[j] = m->scale[j];
+    out->fv = m->fv.data();
+    out->af_ptr = m->af_ptr.data();
+    out->af_idx = m->af_idx.data();
+    return SHAPE_OK;
+}
+
+int shape_mod_radar_law(const shape_mod_file *m, int ilaw, shape_radar_law *law)
+{
+    if (!m) return shape::report_error(SHAPE_E_ARG, "mod_radar_law: null argument");
+    if (!law) return (int)m->radar.size();
+    if (ilaw < 0 || ilaw >= (int)m->radar.size()) return shape::report_error(SHAPE_E_ARG, "mod_radar_law: no such law");
+    *law = m->radar[ilaw];
+    return (int)m->radar.size();
+}
+
+int shape_mod_optical_law(const shape_mod_file *m, int ilaw, shape_optical_law *law)
+{
+    if (!m) return shape::report_error(SHAPE_E_ARG, "mod_optical_law: null argument");
+    if (!law) return (int)m->optical.size();
+    if (ilaw < 0 || ilaw >= (int)m->optical.size())
+        return shape::report_error(SHAPE_E_ARG, "mod_optical_law: no such law");
+    *law = m->optical[ilaw];
+    return (int)m->optical.size();
+}
+
+int shape_mod_spin(const shape_mod_file *m, shape_spin_state *spin)
+{
+    if (!m || !spin) return shape::report_error(SHAPE_E_ARG, "mod_spin: null argument");
+    *spin = m->spin;
+    return SHAPE_OK;
+}
+
+int shape_mod_free_params(const shape_mod_file *m, shape_fit_param *out, int max)
+{
+    if (!m || (max > 0 && !out)) return shape::report_error(SHAPE_E_ARG, "mod_free_params: null argument");
+    int n = 0;
+    auto add = [&](char state, int kind, int index) {
+        if (state != 'f') return;
+        if (n < max) {
+            out[n].kind = kind;
+            out[n].index = index;
+            out[n].step = out[n].tol = out[n].abstol = 0.0;
+        }
+        n++;
+    };
+    for (int j = 0; j < 3; j++) add(m->scale_state[j], SHAPE_PAR_SCALE, j);
+    for (size_t v = 0; v < m->r_state.size(); v++) add(m->r_state[v], SHAPE_PAR_VERTEX_R, (int)v);
+    for (int i = 0; i < 3; i++) add(m->angle_state[i], SHAPE_PAR_SPIN_ANGLE, i);
+    for (int i = 0; i < 3; i++) add(m->omega_state[i], SHAPE_PAR_SPIN_OMEGA, i);
+    for (int i = 0; i < 3; i++) add(m->inertia_state[i], SHAPE_PAR_SPIN_INERTIA, i);
+    for (int i = 0; i < 3; i++) add(m->omegadot_state[i], SHAPE_PAR_SPIN_OMEGADOT, i);
+    for (int k = 0; k < m->spin.n_impulse; k++)
+        for (int i = 0; i < 3; i++) add(m->impulse_state[k][i], SHAPE_PAR_SPIN_IMPULSE, 3 * k + i);
+    for (int i = 0; i < 3; i++) add(m->lib_state[i], SHAPE_PAR_SPIN_LIB, i);
+    return n;
+}
+
+}  // extern "C"

@@ -129,6 +129,14 @@ def load_library(path=LIB_PATH):
     L.shape_engine_set_spin_model.argtypes = [vp, P(cd.SpinState), cd.dptr, cd.dptr, cd.dptr, cd.dptr]
     L.shape_engine_set_spin_param.argtypes = [vp, C.c_int, C.c_int, C.c_double]
     L.shape_engine_set_penalties.argtypes = [vp, C.c_int, P(C.c_int), cd.dptr]
+    L.shape_mod_read.argtypes = [C.c_char_p, P(vp)]
+    L.shape_mod_free.argtypes = [vp]
+    L.shape_mod_free.restype = None
+    L.shape_mod_model.argtypes = [vp, P(cd.ModelDesc)]
+    L.shape_mod_radar_law.argtypes = [vp, C.c_int, P(cd.RadarLaw)]
+    L.shape_mod_optical_law.argtypes = [vp, C.c_int, P(cd.OpticalLaw)]
+    L.shape_mod_spin.argtypes = [vp, P(cd.SpinState)]
+    L.shape_mod_free_params.argtypes = [vp, P(FitParam), C.c_int]
     L.shape_engine_get_penalties.argtypes = [vp, cd.dptr, C.c_int]
     L.shape_engine_get_spin_param.argtypes = [vp, C.c_int, C.c_int, P(C.c_double)]
     L.shape_realize_spin.argtypes = [P(cd.SpinState), cd.dptr, cd.dptr, C.c_int, cd.dptr, cd.dptr, cd.dptr,
@@ -418,6 +426,66 @@ class Engine:
         _chk(self.L.shape_engine_get_realized(self.h, cd.as_dptr(x), cd.as_dptr(vn), cd.as_dptr(fn),
                                               cd.as_dptr(area)))
         return {"x": x, "vn": vn, "fn": fn, "area": area}
+
+
+class ModFile:
+    """A SHAPE model file read by shape_mod_read (host code, no GPU)."""
+
+    def __init__(self, path):
+        self.L = load_library()
+        self.h = None
+        h = C.c_void_p()
+        _chk(self.L.shape_mod_read(os.fsencode(path), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.L.shape_mod_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def model(self):
+        """The shape as a synth.Model (copies of the arrays)."""
+        from .synth import Model
+        d = cd.ModelDesc()
+        _chk(self.L.shape_mod_model(self.h, C.byref(d)))
+        nv, nf = d.nv, d.nf
+        arr = lambda p, n, dt: np.ctypeslib.as_array(p, shape=(n,)).astype(dt).copy()
+        af_ptr = arr(d.af_ptr, nv + 1, np.int32)
+        return Model(arr(d.a, 3 * nv, np.float64).reshape(nv, 3), arr(d.u, 3 * nv, np.float64).reshape(nv, 3),
+                     arr(d.r, nv, np.float64), arr(d.fv, 3 * nf, np.int32).reshape(nf, 3), af_ptr,
+                     arr(d.af_idx, int(af_ptr[-1]), np.int32), np.array(d.scale[:]))
+
+    def radar_laws(self):
+        n = _chk(self.L.shape_mod_radar_law(self.h, 0, None))
+        out = []
+        for i in range(n):
+            law = cd.RadarLaw()
+            _chk(self.L.shape_mod_radar_law(self.h, i, C.byref(law)))
+            out.append(law)
+        return out
+
+    def optical_laws(self):
+        n = _chk(self.L.shape_mod_optical_law(self.h, 0, None))
+        out = []
+        for i in range(n):
+            law = cd.OpticalLaw()
+            _chk(self.L.shape_mod_optical_law(self.h, i, C.byref(law)))
+            out.append(law)
+        return out
+
+    def spin(self):
+        s = cd.SpinState()
+        _chk(self.L.shape_mod_spin(self.h, C.byref(s)))
+        return s
+
+    def free_params(self):
+        """[(kind, index), ...] in the reference's parameter-list order."""
+        n = _chk(self.L.shape_mod_free_params(self.h, None, 0))
+        arr = (FitParam * max(1, n))()
+        _chk(self.L.shape_mod_free_params(self.h, arr, n))
+        return [(arr[i].kind, arr[i].index) for i in range(n)]
 
 
 def spin_state(pa=1, t0=0.0, angle=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), omegadot=(0.0, 0.0, 0.0),

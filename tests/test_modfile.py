@@ -1,0 +1,186 @@
+"""Model files (.mod): shape_mod_read against the reference's own read_mod
+(oracle/_ref/libshape_ref.so via ref_mod_read), on the CPU. Files are
+written here from seeded models, with comments in curly braces between
+tokens; the shape arrays, the attached-facet lists, the scattering laws and
+the spin state (epochs, angles folded over the pole, rad and rad/day
+conversions, impulses, the principal-axis flag) must equal the
+reference's to the last bit. Unsupported content and syntax errors are
+refused with their line."""
+import numpy as np
+import pytest
+
+import cases
+from oracle.bindings import Reference
+from shape_b200 import engine as eng
+
+KINDS = {"ANGLE": eng.PAR_SPIN_ANGLE, "OMEGA": eng.PAR_SPIN_OMEGA, "IMPULSE": eng.PAR_SPIN_IMPULSE}
+
+
+@pytest.fixture(scope="module")
+def ref():
+    return Reference()
+
+
+class Writer:
+    """Tokens with a comment after some of them (seeded)."""
+
+    def __init__(self, seed):
+        self.rng = np.random.default_rng(seed)
+        self.out = []
+
+    def tok(self, *items):
+        for t in items:
+            self.out.append(t if isinstance(t, str) else repr(t))
+            r = self.rng.random()
+            if r < 0.05:
+                self.out.append("{ a comment\nover two lines }")
+            elif r < 0.1:
+                self.out.append("\n")
+
+    def par(self, state, value):
+        self.tok(state, float(value))
+
+    def text(self):
+        return " ".join(self.out) + "\n"
+
+
+def write_mod(path, m, seed=0, states=None, radar=("cosine", 0.1, 1.0), optical=("kaasalainen",),
+              spin=None, ctype="vertex", rstate="f"):
+    w = Writer(seed)
+    st = states or {}
+    w.tok(1)
+    for _ in range(6):
+        w.par("c", 0.0)
+    w.tok(ctype, m.nv)
+    for j in range(3):
+        w.par(st.get("scale", "fcf")[j], m.scale[j])
+    for v in range(m.nv):
+        w.par(rstate if v % 7 else "c", m.r[v])
+        w.tok(*[float(x) for x in m.u[v]], *[float(x) for x in m.a[v]])
+    w.tok(m.nf)
+    for f in range(m.nf):
+        w.tok(*[int(x) for x in m.fv[f]])
+    w.tok(1, radar[0])
+    if radar[0] == "cosine":
+        w.par("f", radar[1]); w.par("c", radar[2])
+    elif radar[0] in ("gaussian", "hagfors", "cosine_qs"):
+        w.par("f", 0.2); w.par("c", 3.0); w.tok(55.0)
+    else:
+        w.par("f", 0.2); w.par("c", 3.0); w.tok(40.0); w.par("f", 0.05); w.par("c", 1.5)
+    w.tok(2, optical[0])
+    if optical[0] == "kaasalainen":
+        w.par("f", 0.45); w.par("c", 0.3); w.par("c", 0.5); w.par("c", 7.0); w.par("c", -0.004)
+    else:
+        w.par("f", 0.2)
+    w.tok("lommel")
+    w.par("c", 0.1)
+    sp = spin or {}
+    w.tok(*sp.get("t0", (2018, 3, 14, 5, 6, 7)))
+    for a in sp.get("angle", (30.0, 250.0, -10.0)):
+        w.par("f", a)
+    for i, o in enumerate(sp.get("omega", (0.0, 0.0, 1440.0))):
+        w.par(sp.get("omega_state", "ccf")[i], o)
+    for x in sp.get("inertia", (1.0, 1.1, 1.2)):
+        w.par("c", x)
+    for x in sp.get("omegadot", (0.0, 0.0, 1e-6)):
+        w.par("c", x)
+    for x in sp.get("lib", (0.0, 0.0, 0.0)):
+        w.par("c", x)
+    imps = sp.get("impulses", [((2018, 3, 15, 0, 0, 0), (0.0, 0.0, 2.0))])
+    w.tok(len(imps))
+    for date, vec in imps:
+        w.tok(*date)
+        for x in vec:
+            w.par("f" if x else "c", x)
+    path.write_text(w.text())
+
+
+def _compare(path, ref):
+    mf = eng.ModFile(path)
+    m = mf.model()
+    arrays, radar, optical, spin = ref.read_mod(str(path))
+    for k in ("a", "u", "r", "scale"):
+        assert np.array_equal(np.asarray(getattr(m, k)), arrays[k]), k
+    for k in ("fv", "af_ptr", "af_idx"):
+        assert np.array_equal(np.asarray(getattr(m, k)), arrays[k]), k
+    for mine, theirs in zip(mf.radar_laws(), radar):
+        assert bytes(mine) == bytes(theirs)
+    for mine, theirs in zip(mf.optical_laws(), optical):
+        assert bytes(mine) == bytes(theirs)
+    assert len(mf.radar_laws()) == len(radar) and len(mf.optical_laws()) == len(optical)
+    s = mf.spin()
+    for k in ("pa", "t0", "n_impulse", "lib_amp", "lib_freq", "lib_phase"):
+        assert getattr(s, k) == getattr(spin, k), k
+    for k in ("angle", "omega", "omegadot", "inertia"):
+        assert list(getattr(s, k)) == list(getattr(spin, k)), k
+    for n in range(s.n_impulse):
+        assert s.t_impulse[n] == spin.t_impulse[n]
+        assert list(s.impulse[n]) == list(spin.impulse[n])
+    return mf, m
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_mod_matches_reference_read_mod(tmp_path, ref, seed):
+    base = cases.c1()[0]
+    m = base.copy()
+    rng = np.random.default_rng(seed)
+    m.r = rng.normal(0, 0.02, m.nv)
+    m.scale = np.array([1.0, 1.05, 0.95]) + rng.normal(0, 1e-3, 3)
+    radar = [("cosine", 0.1, 1.0), ("hagfors",), ("cosine+cosine",)][seed]
+    spin = {"angle": [(30.0, 250.0, -10.0), (-400.0, 95.0, 720.5), (10.0, 181.0, 3.0)][seed]}
+    path = tmp_path / ("m%d.mod" % seed)
+    write_mod(path, m, seed=seed, radar=radar, optical=[("kaasalainen",), ("lambertian",), ("lommel",)][seed],
+              spin=spin)
+    mf, got = _compare(path, ref)
+    assert np.array_equal(got.a, m.a) and np.array_equal(got.r, m.r) and np.array_equal(got.fv, m.fv)
+    assert mf.spin().pa == 1
+    assert mf.spin().angle[1] <= np.pi
+    # free parameters in the reference's order: scale 0 and 2, the floating
+    # vertex deviations, the three angles, omega z, the z impulse
+    fp = mf.free_params()
+    nr = sum(1 for v in range(m.nv) if v % 7)
+    assert fp[:2] == [(eng.PAR_SCALE, 0), (eng.PAR_SCALE, 2)]
+    assert all(k == eng.PAR_VERTEX_R for k, _ in fp[2:2 + nr]) and len(fp) == 2 + nr + 5
+    assert fp[2 + nr:] == [(eng.PAR_SPIN_ANGLE, 0), (eng.PAR_SPIN_ANGLE, 1), (eng.PAR_SPIN_ANGLE, 2),
+                           (eng.PAR_SPIN_OMEGA, 2), (eng.PAR_SPIN_IMPULSE, 2)]
+    mf.close()
+
+
+def test_mod_non_principal_axis(tmp_path, ref):
+    m = cases.c1()[0]
+    path = tmp_path / "npa.mod"
+    write_mod(path, m, seed=5, spin={"omega": (12.0, -30.0, 900.0), "omega_state": "fff",
+                                     "omegadot": (0.0, 0.0, 0.0), "t0": (1999, 12, 31, 23, 59, 59),
+                                     "impulses": [((2000, 1, 2, 0, 0, 0), (1.0, 0.0, -2.0)),
+                                                  ((2000, 1, 5, 12, 0, 0), (0.0, 0.5, 0.0))]})
+    mf, _ = _compare(path, ref)
+    assert mf.spin().pa == 0 and mf.spin().n_impulse == 2
+
+
+def _err(path):
+    with pytest.raises(eng.EngineError) as ei:
+        eng.ModFile(path)
+    return str(ei.value)
+
+
+def test_mod_refusals(tmp_path):
+    m = cases.c1()[0]
+    p = tmp_path / "e.mod"
+    write_mod(p, m, ctype="ellipse")
+    assert "error -4" in _err(p) and "vertex" in _err(p)
+    write_mod(p, m, rstate="=")
+    assert "error -4" in _err(p)
+    write_mod(p, m, radar=("tabular",))
+    assert "error -4" in _err(p)
+    write_mod(p, m)
+    text = p.read_text()
+    p.write_text(text.replace("vertex", "vertex x", 1))
+    msg = _err(p)
+    assert "error -1" in msg and "line" in msg
+    p.write_text(text + " { unclosed")
+    # the spin section ends before the comment; the reader stops there
+    eng.ModFile(p).close()
+    p.write_text(text.rsplit(" ", 8)[0])
+    assert "end of file" in _err(p)
+    p.write_text("1 c 0 c 0 c 0 c 0 c 0 c 0 vertex 4 { unclosed")
+    assert "unclosed comment" in _err(p)
