@@ -424,6 +424,26 @@ int shape_mod_spin(const shape_mod_file *m, shape_spin_state *spin);
  * changes, impulses, libration. kind and index are set, step and the
  * tolerances are 0 (they come from the .par file). Returns the count. */
 int shape_mod_free_params(const shape_mod_file *m, shape_fit_param *out, int max);
+/* Writes m as a model file that read_mod (and shape_mod_read) reads back:
+ * the parameter states of the file m came from, numbers with 17
+ * significant digits. Shape values round-trip exactly. Angles and rates
+ * are written back in degrees, which can change their last bit. Epochs
+ * become calendar dates to the second, as jd2cal rounds them
+ * (src/astro/jdcal.c:16-33). */
+int shape_mod_write(const shape_mod_file *m, const char *path);
+/* Copies an engine's current scale factors, vertex deviations and (when it
+ * has a spin model) spin parameters into m, as a fit leaves them; m must
+ * describe the engine's model. */
+int shape_mod_take_engine(shape_mod_file *m, shape_engine *e);
+
+/* The listfit output of one radar frame (chi2_deldop with listfit,
+ * src/shape/chi2.c:525-560): ndel*ndop lines "%13.6e" of cal * fit / sdev,
+ * delay-major (fit host memory). */
+int shape_write_fitdat(const char *path, int ndel, int ndop, const double *fit, double cal, double sdev);
+/* The same for radar frame global_frame of the engine's last evaluation:
+ * its fit image and calibration, with the frame's sdev (deldop->frame[f]
+ * .sdev; the engine keeps none for delay-Doppler frames). */
+int shape_engine_write_fitdat(shape_engine *e, int global_frame, double sdev, const char *path);
 
 int shape_server_create(int device, size_t hbm_budget_bytes, int max_slots, shape_server **out);
 void shape_server_destroy(shape_server *s);

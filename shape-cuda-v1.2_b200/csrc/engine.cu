@@ -1506,6 +1506,22 @@ int shape_engine_get_fit(shape_engine *h, int frame, double *fit)
     return SHAPE_OK;
 }
 
+int shape_engine_write_fitdat(shape_engine *h, int frame, double sdev, const char *path)
+{
+    if (!h || !path) return shape::set_err(SHAPE_E_ARG, "write_fitdat: null argument");
+    if (!(sdev > 0.0)) return shape::set_err(SHAPE_E_ARG, "write_fitdat: sdev must be > 0");
+    EngineImpl &E = h->impl;
+    if (frame < 0 || frame >= (int)E.frames.size()) return shape::set_err(SHAPE_E_ARG, "write_fitdat: bad frame");
+    const shape_deldop_frame &F = E.frames[frame];
+    std::vector<double> fit((size_t)F.ndel * F.ndop);
+    int rc = shape_engine_get_fit(h, frame, fit.data());
+    if (rc) return rc;
+    std::vector<shape_deldop_result> res(E.frames.size());
+    rc = shape_engine_get_deldop_results(h, res.data(), (int)res.size());
+    if (rc < 0) return rc;
+    return shape_write_fitdat(path, F.ndel, F.ndop, fit.data(), res[frame].cal, sdev);
+}
+
 int shape_engine_keep_pos(shape_engine *h, int keep)
 {
     if (!h) return shape::set_err(SHAPE_E_ARG, "null engine");

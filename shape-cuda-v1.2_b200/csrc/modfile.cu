@@ -1,8 +1,9 @@
-// Reader of SHAPE model files (.mod; read_mod, src/shape/read_mod.c:204-227)
-// for the models the engine evaluates: one vertex component (read_shape,
-// :289-542) with no component offsets, the homogeneous radar and optical
-// scattering laws (read_photo, :544-1953) and the spin section (read_spin,
-// :1954-2140). Host code.
+// SHAPE model files (.mod; read_mod, src/shape/read_mod.c:204-227) for the
+// models the engine evaluates: one vertex component (read_shape, :289-542)
+// with no component offsets, the homogeneous radar and optical scattering
+// laws (read_photo, :544-1953) and the spin section (read_spin, :1954-2140),
+// read and written; and the listfit output of a radar frame (.fitdat,
+// src/shape/chi2.c:525-560). Host code.
 //
 // The file is a stream of whitespace-separated tokens with comments in
 // curly braces. A parameter is a state token (c, f or =) followed by its
@@ -33,6 +34,7 @@ struct shape_mod_file {
     std::vector<char> r_state;
     std::vector<shape_radar_law> radar;
     std::vector<shape_optical_law> optical;
+    std::vector<std::string> radar_state, optical_state;   // states of each law's parameters, in file order
     shape_spin_state spin;
     char angle_state[3], omega_state[3], inertia_state[3], omegadot_state[3], lib_state[3];
     char impulse_state[SHAPE_MAX_IMPULSES][3];
@@ -143,6 +145,31 @@ double read_epoch(Tokens &tk, const char *what)
     return jd;
 }
 
+// Julian date -> yyyy mm dd hh mm ss (Gregorian; the inverse of
+// julian_day_number, Fliegel and Van Flandern 1968), seconds rounded as
+// jd2cal rounds them (src/astro/jdcal.c:16-33). False before 1582 Oct 15.
+bool calendar(double jd, int c[6])
+{
+    long jdn = (long)floor(jd + 0.5);
+    long secs = (long)floor((jd + 0.5 - (double)jdn) * 86400 + 0.5);
+    if (secs == 86400) { jdn++; secs = 0; }
+    if (jdn < 2299161) return false;
+    long l = jdn + 68569;
+    const long n = 4 * l / 146097;
+    l = l - (146097 * n + 3) / 4;
+    const long i = 4000 * (l + 1) / 1461001;
+    l = l - 1461 * i / 4 + 31;
+    const long j = 80 * l / 2447;
+    c[2] = (int)(l - 2447 * j / 80);
+    l = j / 11;
+    c[1] = (int)(j + 2 - 12 * l);
+    c[0] = (int)(100 * (n - 49) + i + l);
+    c[3] = (int)(secs / 3600);
+    c[4] = (int)((secs % 3600) / 60);
+    c[5] = (int)(secs % 60);
+    return true;
+}
+
 void read_shape(Tokens &tk, shape_mod_file &m)
 {
     const int ncomp = tk.integer("number of components");
@@ -197,6 +224,13 @@ void read_photo(Tokens &tk, shape_mod_file &m)
         const std::string s = tk.word("radar law");
         shape_radar_law L;
         memset(&L, 0, sizeof L);
+        std::string states;
+        auto par = [&](const char *what) {
+            char st;
+            const double v = tk.param(what, &st);
+            states.push_back(st);
+            return v;
+        };
         auto cutoff = [&]() {
             const double deg = tk.real("cutoff angle");
             if (deg <= 0.0 || deg > 90.0) tk.fail("cutoff angle must be in (0, 90] deg");
@@ -206,26 +240,27 @@ void read_photo(Tokens &tk, shape_mod_file &m)
             L.type = 0;
         } else if (s == "cosine") {
             L.type = SHAPE_RADLAW_COSINE_DIFF;
-            L.diff_R = tk.param("R", nullptr);
-            L.diff_C = tk.param("C", nullptr);
+            L.diff_R = par("R");
+            L.diff_C = par("C");
         } else if (s == "gaussian" || s == "hagfors" || s == "cosine_qs") {
             L.type = s == "gaussian" ? SHAPE_RADLAW_GAUSSIAN : s == "hagfors" ? SHAPE_RADLAW_HAGFORS
                                                                                : SHAPE_RADLAW_COSINE_QS;
-            L.qs_R = tk.param("R", nullptr);
-            L.qs_C = tk.param("C", nullptr);
+            L.qs_R = par("R");
+            L.qs_C = par("C");
             L.qs_cos_cutoff = cutoff();
         } else if (s == "gauss+cosine" || s == "hagfors+cosine" || s == "cosine+cosine") {
             L.type = s == "gauss+cosine" ? SHAPE_RADLAW_GAUSSIAN_COSINE
                      : s == "hagfors+cosine" ? SHAPE_RADLAW_HAGFORS_COSINE : SHAPE_RADLAW_COSINE_COSINE;
-            L.qs_R = tk.param("R", nullptr);
-            L.qs_C = tk.param("C", nullptr);
+            L.qs_R = par("R");
+            L.qs_C = par("C");
             L.qs_cos_cutoff = cutoff();
-            L.diff_R = tk.param("R", nullptr);
-            L.diff_C = tk.param("C", nullptr);
+            L.diff_R = par("R");
+            L.diff_C = par("C");
         } else {
             tk.fail("radar law " + s + " is not supported", SHAPE_E_UNSUPPORTED);
         }
         m.radar.push_back(L);
+        m.radar_state.push_back(states);
     }
     const int nopt = tk.integer("number of optical laws");
     if (nopt < 0) tk.fail("negative number of optical laws");
@@ -233,24 +268,32 @@ void read_photo(Tokens &tk, shape_mod_file &m)
         const std::string s = tk.word("optical law");
         shape_optical_law L;
         memset(&L, 0, sizeof L);
+        std::string states;
+        auto par = [&](const char *what) {
+            char st;
+            const double v = tk.param(what, &st);
+            states.push_back(st);
+            return v;
+        };
         if (s == "none") {
             L.type = 0;
         } else if (s == "lambertian" || s == "lommel") {
             L.type = s == "lambertian" ? SHAPE_OPTLAW_LAMBERT : SHAPE_OPTLAW_LOMMEL;
-            L.R = tk.param("R", nullptr);
+            L.R = par("R");
         } else if (s == "kaasalainen") {
             L.type = SHAPE_OPTLAW_KAASALAINEN;
-            L.R = tk.param("R", nullptr);
-            L.wt = tk.param("wt", nullptr);
-            L.A0 = tk.param("A0", nullptr);
-            L.D = tk.param("D", nullptr);
-            L.k = tk.param("k", nullptr);
+            L.R = par("R");
+            L.wt = par("wt");
+            L.A0 = par("A0");
+            L.D = par("D");
+            L.k = par("k");
             L.D *= D2R;
             L.k /= D2R;
         } else {
             tk.fail("optical law " + s + " is not supported", SHAPE_E_UNSUPPORTED);
         }
         m.optical.push_back(L);
+        m.optical_state.push_back(states);
     }
 }
 
@@ -406,6 +449,135 @@ int shape_mod_free_params(const shape_mod_file *m, shape_fit_param *out, int max
         for (int i = 0; i < 3; i++) add(m->impulse_state[k][i], SHAPE_PAR_SPIN_IMPULSE, 3 * k + i);
     for (int i = 0; i < 3; i++) add(m->lib_state[i], SHAPE_PAR_SPIN_LIB, i);
     return n;
+}
+
+// Writes m as a model file that read_mod reads back: one vertex component
+// with zero offsets, its laws and the spin section, the parameter states of
+// the file it came from, numbers with 17 significant digits (shape values
+// exactly; angles and rates back in degrees, which rounds their last bit).
+int shape_mod_write(const shape_mod_file *m, const char *path)
+{
+    if (!m || !path) return shape::report_error(SHAPE_E_ARG, "mod_write: null argument");
+    int t0[6], ti[SHAPE_MAX_IMPULSES][6];
+    const shape_spin_state &sp = m->spin;
+    bool ok = calendar(sp.t0, t0);
+    for (int n = 0; n < sp.n_impulse; n++) ok = ok && calendar(sp.t_impulse[n], ti[n]);
+    if (!ok) return shape::report_error(SHAPE_E_UNSUPPORTED, "mod_write: epoch before the Gregorian calendar");
+    FILE *fp = fopen(path, "w");
+    if (!fp) return shape::report_error(SHAPE_E_ARG, std::string("mod_write: cannot create ") + path);
+    auto par = [&](char st, double v) { fprintf(fp, " %c %.17g", st, v); };
+    const int nv = (int)m->r.size(), nf = (int)(m->fv.size() / 3);
+    fprintf(fp, "{SHAPE model file written by shape-b200}\n\n{shape}\n1 {component}\n");
+    fprintf(fp, " c 0 c 0 c 0 {linear offsets (km)}\n c 0 c 0 c 0 {rotation offsets (deg)}\n");
+    fprintf(fp, "vertex\n%d {vertices}\n", nv);
+    for (int j = 0; j < 3; j++) par(m->scale_state[j], m->scale[j]);
+    fprintf(fp, " {scale factors}\n");
+    for (int v = 0; v < nv; v++) {
+        par(m->r_state[v], m->r[v]);
+        for (int k = 0; k < 3; k++) fprintf(fp, " %.17g", m->u[3 * (size_t)v + k]);
+        for (int k = 0; k < 3; k++) fprintf(fp, " %.17g", m->a[3 * (size_t)v + k]);
+        fprintf(fp, "\n");
+    }
+    fprintf(fp, "%d {facets}\n", nf);
+    for (int f = 0; f < nf; f++)
+        fprintf(fp, "%d %d %d\n", m->fv[3 * (size_t)f], m->fv[3 * (size_t)f + 1], m->fv[3 * (size_t)f + 2]);
+    fprintf(fp, "\n{photometry}\n%d {radar laws}\n", (int)m->radar.size());
+    for (size_t i = 0; i < m->radar.size(); i++) {
+        const shape_radar_law &L = m->radar[i];
+        const std::string &st = m->radar_state[i];
+        const double cut = acos(L.qs_cos_cutoff) / D2R;
+        switch (L.type) {
+        case SHAPE_RADLAW_COSINE_DIFF:
+            fprintf(fp, "cosine"); par(st[0], L.diff_R); par(st[1], L.diff_C); break;
+        case SHAPE_RADLAW_GAUSSIAN: case SHAPE_RADLAW_HAGFORS: case SHAPE_RADLAW_COSINE_QS:
+            fprintf(fp, L.type == SHAPE_RADLAW_GAUSSIAN ? "gaussian" : L.type == SHAPE_RADLAW_HAGFORS ? "hagfors"
+                                                                                                       : "cosine_qs");
+            par(st[0], L.qs_R); par(st[1], L.qs_C); fprintf(fp, " %.17g", cut); break;
+        case SHAPE_RADLAW_GAUSSIAN_COSINE: case SHAPE_RADLAW_HAGFORS_COSINE: case SHAPE_RADLAW_COSINE_COSINE:
+            fprintf(fp, L.type == SHAPE_RADLAW_GAUSSIAN_COSINE ? "gauss+cosine"
+                        : L.type == SHAPE_RADLAW_HAGFORS_COSINE ? "hagfors+cosine" : "cosine+cosine");
+            par(st[0], L.qs_R); par(st[1], L.qs_C); fprintf(fp, " %.17g", cut);
+            par(st[2], L.diff_R); par(st[3], L.diff_C); break;
+        default:
+            fprintf(fp, "none");
+        }
+        fprintf(fp, "\n");
+    }
+    fprintf(fp, "%d {optical laws}\n", (int)m->optical.size());
+    for (size_t i = 0; i < m->optical.size(); i++) {
+        const shape_optical_law &L = m->optical[i];
+        const std::string &st = m->optical_state[i];
+        if (L.type == SHAPE_OPTLAW_LAMBERT || L.type == SHAPE_OPTLAW_LOMMEL) {
+            fprintf(fp, L.type == SHAPE_OPTLAW_LAMBERT ? "lambertian" : "lommel");
+            par(st[0], L.R);
+        } else if (L.type == SHAPE_OPTLAW_KAASALAINEN) {
+            fprintf(fp, "kaasalainen");
+            par(st[0], L.R); par(st[1], L.wt); par(st[2], L.A0); par(st[3], L.D / D2R); par(st[4], L.k * D2R);
+        } else {
+            fprintf(fp, "none");
+        }
+        fprintf(fp, "\n");
+    }
+    fprintf(fp, "\n{spin}\n%d %d %d %d %d %d {t0}\n", t0[0], t0[1], t0[2], t0[3], t0[4], t0[5]);
+    for (int i = 0; i < 3; i++) par(m->angle_state[i], sp.angle[i] / D2R);
+    fprintf(fp, " {angles (deg)}\n");
+    for (int i = 0; i < 3; i++) par(m->omega_state[i], sp.omega[i] / D2R);
+    fprintf(fp, " {spin (deg/day)}\n");
+    for (int i = 0; i < 3; i++) par(m->inertia_state[i], sp.inertia[i]);
+    fprintf(fp, " {moments of inertia}\n");
+    for (int i = 0; i < 3; i++) par(m->omegadot_state[i], sp.omegadot[i] / D2R);
+    fprintf(fp, " {spin change (deg/day/day)}\n");
+    par(m->lib_state[0], sp.lib_amp / D2R);
+    par(m->lib_state[1], sp.lib_freq / D2R);
+    par(m->lib_state[2], sp.lib_phase / D2R);
+    fprintf(fp, " {libration}\n%d {spin impulses}\n", sp.n_impulse);
+    for (int n = 0; n < sp.n_impulse; n++) {
+        fprintf(fp, "%d %d %d %d %d %d", ti[n][0], ti[n][1], ti[n][2], ti[n][3], ti[n][4], ti[n][5]);
+        for (int i = 0; i < 3; i++) par(m->impulse_state[n][i], sp.impulse[n][i] / D2R);
+        fprintf(fp, "\n");
+    }
+    const int bad = ferror(fp);
+    if (fclose(fp) != 0 || bad) return shape::report_error(SHAPE_E_ARG, std::string("mod_write: write failed: ") + path);
+    return SHAPE_OK;
+}
+
+// The engine's current scale factors, vertex deviations and (with a spin
+// model) spin parameters into m, as a fit leaves them.
+int shape_mod_take_engine(shape_mod_file *m, shape_engine *e)
+{
+    if (!m || !e) return shape::report_error(SHAPE_E_ARG, "mod_take_engine: null argument");
+    for (int j = 0; j < 3; j++)
+        if (int rc = shape_engine_get_scale(e, j, &m->scale[j])) return rc;
+    for (size_t v = 0; v < m->r.size(); v++)
+        if (int rc = shape_engine_get_vertex_r(e, (int)v, &m->r[v])) return rc;
+    double x;
+    if (shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_ANGLE, 0, &x) != SHAPE_OK) return SHAPE_OK;   // no spin model
+    shape_spin_state &sp = m->spin;
+    for (int i = 0; i < 3; i++) {
+        shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_ANGLE, i, &sp.angle[i]);
+        shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_OMEGA, i, &sp.omega[i]);
+        shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_INERTIA, i, &sp.inertia[i]);
+        shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_OMEGADOT, i, &sp.omegadot[i]);
+    }
+    for (int k = 0; k < 3 * sp.n_impulse; k++)
+        shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_IMPULSE, k, &sp.impulse[k / 3][k % 3]);
+    shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_LIB, 0, &sp.lib_amp);
+    shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_LIB, 1, &sp.lib_freq);
+    shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_LIB, 2, &sp.lib_phase);
+    return SHAPE_OK;
+}
+
+// The listfit output of a radar frame (src/shape/chi2.c:555-558): one line
+// "%13.6e" of cal * fit / sdev per bin, delay-major.
+int shape_write_fitdat(const char *path, int ndel, int ndop, const double *fit, double cal, double sdev)
+{
+    if (!path || !fit || ndel < 1 || ndop < 1) return shape::report_error(SHAPE_E_ARG, "write_fitdat: invalid argument");
+    FILE *fp = fopen(path, "w");
+    if (!fp) return shape::report_error(SHAPE_E_ARG, std::string("write_fitdat: cannot create ") + path);
+    for (size_t k = 0; k < (size_t)ndel * ndop; k++) fprintf(fp, "%13.6e\n", cal * fit[k] / sdev);
+    const int bad = ferror(fp);
+    if (fclose(fp) != 0 || bad) return shape::report_error(SHAPE_E_ARG, std::string("write_fitdat: write failed: ") + path);
+    return SHAPE_OK;
 }
 
 }  // extern "C"

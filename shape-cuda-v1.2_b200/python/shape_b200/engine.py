@@ -137,6 +137,10 @@ def load_library(path=LIB_PATH):
     L.shape_mod_optical_law.argtypes = [vp, C.c_int, P(cd.OpticalLaw)]
     L.shape_mod_spin.argtypes = [vp, P(cd.SpinState)]
     L.shape_mod_free_params.argtypes = [vp, P(FitParam), C.c_int]
+    L.shape_mod_write.argtypes = [vp, C.c_char_p]
+    L.shape_mod_take_engine.argtypes = [vp, vp]
+    L.shape_write_fitdat.argtypes = [C.c_char_p, C.c_int, C.c_int, cd.dptr, C.c_double, C.c_double]
+    L.shape_engine_write_fitdat.argtypes = [vp, C.c_int, C.c_double, C.c_char_p]
     L.shape_engine_get_penalties.argtypes = [vp, cd.dptr, C.c_int]
     L.shape_engine_get_spin_param.argtypes = [vp, C.c_int, C.c_int, P(C.c_double)]
     L.shape_realize_spin.argtypes = [P(cd.SpinState), cd.dptr, cd.dptr, C.c_int, cd.dptr, cd.dptr, cd.dptr,
@@ -318,6 +322,9 @@ class Engine:
         n = _chk(self.L.shape_engine_get_penalties(self.h, cd.as_dptr(out), 64))
         return out[:n].copy()
 
+    def write_fitdat(self, frame, sdev, path):
+        _chk(self.L.shape_engine_write_fitdat(self.h, int(frame), float(sdev), os.fsencode(path)))
+
     def set_spin_param(self, kind, index, value):
         _chk(self.L.shape_engine_set_spin_param(self.h, int(kind), int(index), float(value)))
 
@@ -428,6 +435,13 @@ class Engine:
         return {"x": x, "vn": vn, "fn": fn, "area": area}
 
 
+def write_fitdat(path, fit, cal, sdev):
+    """The listfit file of one radar frame: cal * fit / sdev, one "%13.6e" per line."""
+    f = np.ascontiguousarray(fit, dtype=np.float64)
+    ndel, ndop = f.shape if f.ndim == 2 else (1, f.size)
+    _chk(load_library().shape_write_fitdat(os.fsencode(path), ndel, ndop, cd.as_dptr(f), float(cal), float(sdev)))
+
+
 class ModFile:
     """A SHAPE model file read by shape_mod_read (host code, no GPU)."""
 
@@ -479,6 +493,13 @@ class ModFile:
         s = cd.SpinState()
         _chk(self.L.shape_mod_spin(self.h, C.byref(s)))
         return s
+
+    def write(self, path):
+        _chk(self.L.shape_mod_write(self.h, os.fsencode(path)))
+
+    def take_engine(self, engine):
+        """The engine's current shape and spin parameters into this model."""
+        _chk(self.L.shape_mod_take_engine(self.h, engine.h))
 
     def free_params(self):
         """[(kind, index), ...] in the reference's parameter-list order."""

@@ -1,0 +1,40 @@
+"""Model and fit files with the engine: a model read from a .mod file
+evaluates exactly like the same model given directly; after parameter
+changes, shape_mod_take_engine carries the engine's values into the file
+written next; shape_engine_write_fitdat writes the frame's listfit file
+(cal * fit / sdev, "%13.6e" per line) from the last evaluation."""
+import numpy as np
+import pytest
+
+import cases
+from shape_b200 import engine as eng
+from test_modfile import write_mod
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mod_file_engine_round_trip(cuda_device, tmp_path):
+    m, p, ds = cases.c1()
+    path = tmp_path / "c1.mod"
+    write_mod(path, m, seed=2)
+    mf = eng.ModFile(path)
+    e1 = eng.make_engine(mf.model(), p, deldops=[ds])
+    e2 = eng.make_engine(m, p, deldops=[ds])
+    for form in (eng.FORM_PLAIN_FP64, eng.FORM_BATCHED_FP64):
+        assert e1.evaluate(form)["chi2"] == e2.evaluate(form)["chi2"]
+    e1.set_scale(1, 1.07)
+    e1.set_vertex_r(5, 0.0123)
+    mf.take_engine(e1)
+    out = tmp_path / "fitted.mod"
+    mf.write(out)
+    back = eng.ModFile(out).model()
+    assert back.scale[1] == 1.07 and back.r[5] == 0.0123 and np.array_equal(back.fv, m.fv)
+    s = e1.evaluate(eng.FORM_BATCHED_FP64)
+    sdev = 0.8
+    e1.write_fitdat(0, sdev, tmp_path / "f0.fitdat")
+    cal = e1.results()[0]["cal"]
+    want = ["%13.6e" % (cal * x / sdev) for x in np.asarray(e1.fit(0)).ravel()]
+    assert (tmp_path / "f0.fitdat").read_text().splitlines() == want
+    assert s["chi2"] > 0.0
+    e1.close()
+    e2.close()

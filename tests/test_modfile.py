@@ -13,8 +13,6 @@ import cases
 from oracle.bindings import Reference
 from shape_b200 import engine as eng
 
-KINDS = {"ANGLE": eng.PAR_SPIN_ANGLE, "OMEGA": eng.PAR_SPIN_OMEGA, "IMPULSE": eng.PAR_SPIN_IMPULSE}
-
 
 @pytest.fixture(scope="module")
 def ref():
@@ -184,3 +182,45 @@ def test_mod_refusals(tmp_path):
     assert "end of file" in _err(p)
     p.write_text("1 c 0 c 0 c 0 c 0 c 0 c 0 vertex 4 { unclosed")
     assert "unclosed comment" in _err(p)
+
+
+def test_mod_write_round_trip(tmp_path, ref):
+    """shape_mod_write: the written file reads back (with this reader and
+    with the reference's read_mod, identically) to the same shape, states,
+    epochs and impulses; angles, rates and law constants written in degrees
+    return to within a few ulps."""
+    m = cases.c1()[0].copy()
+    m.r = np.random.default_rng(9).normal(0, 0.02, m.nv)
+    a, b = tmp_path / "a.mod", tmp_path / "b.mod"
+    write_mod(a, m, seed=4, radar=("gauss+cosine",),
+              spin={"angle": (33.3, 120.7, 359.9), "lib": (0.5, 20.0, 45.0),
+                    "impulses": [((2019, 5, 6, 7, 8, 9), (0.0, 0.0, 1.25)),
+                                 ((2019, 6, 1, 23, 59, 59), (0.0, 0.0, -0.5))]})
+    ma = eng.ModFile(a)
+    ma.write(b)
+    mb, gb = _compare(b, ref)
+    ga = ma.model()
+    for k in ("a", "u", "r", "scale", "fv", "af_ptr", "af_idx"):
+        assert np.array_equal(np.asarray(getattr(ga, k)), np.asarray(getattr(gb, k))), k
+    assert mb.free_params() == ma.free_params()
+    sa, sb = ma.spin(), mb.spin()
+    assert sa.t0 == sb.t0 and sa.n_impulse == sb.n_impulse and sa.pa == sb.pa
+    assert [sa.t_impulse[n] for n in range(2)] == [sb.t_impulse[n] for n in range(2)]
+    for k in ("angle", "omega", "omegadot", "inertia"):
+        np.testing.assert_allclose(list(getattr(sb, k)), list(getattr(sa, k)), rtol=4e-16, atol=1e-300)
+    np.testing.assert_allclose([sb.impulse[n][2] for n in range(2)], [sa.impulse[n][2] for n in range(2)],
+                               rtol=4e-16)
+    for x, y in zip(ma.radar_laws() + ma.optical_laws(), mb.radar_laws() + mb.optical_laws()):
+        assert x.type == y.type
+        for f, _ in type(x)._fields_[1:]:
+            assert abs(getattr(x, f) - getattr(y, f)) <= 4e-16 * abs(getattr(x, f)) + 1e-300, f
+
+
+def test_fitdat_format(tmp_path):
+    rng = np.random.default_rng(3)
+    fit = rng.normal(0, 1, (7, 11)) * 10.0 ** rng.integers(-8, 8, (7, 11))
+    cal, sdev = 1.7342, 0.913
+    p = tmp_path / "f.fitdat"
+    eng.write_fitdat(p, fit, cal, sdev)
+    lines = p.read_text().splitlines()
+    assert lines == ["%13.6e" % (cal * x / sdev) for x in fit.ravel()]
