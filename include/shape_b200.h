@@ -436,6 +436,23 @@ int shape_mod_write(const shape_mod_file *m, const char *path);
  * describe the engine's model. */
 int shape_mod_take_engine(shape_mod_file *m, shape_engine *e);
 
+/* One radar data file into a frame's obs and 1/variance arrays (read_deldop
+ * / read_doppler, src/shape/read_dat.c:800-856, 1150-1176, 2074-2260): a
+ * stored image of ndel x ndop (a Doppler spectrum: ndel = 1) in raw
+ * float32, RDF (header lines up to one starting with '.', then float32) or
+ * ASCII, told apart by the first 128 bytes as the reference does (FITS
+ * returns SHAPE_E_UNSUPPORTED). Each value is rounded to float, the window
+ * idel_use x idop_use (1-based, inclusive) is kept, delay-major, and
+ * multiplied by sdev. gamma != 1 applies the delay-Doppler gamma transform
+ * (par->dd_gamma; pass 1 for Doppler data). 1/variance is 1/sdev^2, or
+ * with nlooks > 0 (par->speckle) 1/(sdev^2 + (obs/sqrt(nlooks))^2), times
+ * pixweight (a full-size weight image, or NULL). big_endian: the data's
+ * byte order for float32 files (par->endian; the reference's default is
+ * big-endian). Host code. */
+int shape_read_radar_data(const char *path, int ndel, int ndop, const int idel_use[2], const int idop_use[2],
+                          int big_endian, double sdev, double gamma, double nlooks, const double *pixweight,
+                          double *obs, double *oneovervar);
+
 /* The listfit output of one radar frame (chi2_deldop with listfit,
  * src/shape/chi2.c:525-560): ndel*ndop lines "%13.6e" of cal * fit / sdev,
  * delay-major (fit host memory). */

@@ -225,6 +225,8 @@ class Reference:
         L.ref_mod_radar.argtypes = [C.c_void_p, C.c_int, P(cd.RadarLaw)]
         L.ref_mod_optical.argtypes = [C.c_void_p, C.c_int, P(cd.OpticalLaw)]
         L.ref_mod_spin.argtypes = [C.c_void_p, P(cd.SpinState)]
+        L.ref_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int,
+                                          C.c_double, cd.dptr]
         L.ref_get_seen.argtypes = [C.c_void_p, C.c_char_p]
         L.ref_get_deldop_frame.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr, cd.dptr,
                                            cd.dptr, cd.iptr, P(cd.DeldopResult)]
@@ -293,6 +295,15 @@ class Reference:
         arrays = {"a": a.reshape(nv, 3), "u": u.reshape(nv, 3), "r": r, "scale": sc, "fv": fv.reshape(nf, 3),
                   "af_ptr": ap, "af_idx": ai}
         return arrays, radar, optical, spin
+
+    def read_radar_data(self, path, kind, ndel, ndop, idel_use, idop_use, swap, sdev):
+        """The reference's reader of one data file (kind 0-2 delay-Doppler
+        ascii / binary / rdf, 3-5 Doppler): the window's obs values."""
+        obs = np.zeros((idel_use[1] - idel_use[0] + 1) * (idop_use[1] - idop_use[0] + 1))
+        rc = self.lib.ref_read_radar_data(os.fsencode(path), kind, ndel, ndop, (C.c_int * 2)(*idel_use),
+                                          (C.c_int * 2)(*idop_use), swap, sdev, cd.as_dptr(obs))
+        assert rc == 0
+        return obs
 
     def mnbrak(self, fn, ax, bx):
         cb = OBJFN(fn)

@@ -787,3 +787,57 @@ void ref_mod_spin(void *h, shape_spin_state *sp)
     sp->lib_freq = s->lib_freq.val;
     sp->lib_phase = s->lib_phase.val;
 }
+
+
+/* The reference's data-file readers (read_deldop_ascii / _binary / _rdf
+ * and read_doppler_*, src/shape/read_dat.c:2074-2260) on one file: kind 0-2
+ * delay-Doppler ascii / binary / rdf, 3-5 the Doppler ones (ndel = 1).
+ * obs receives the window idel_use x idop_use, delay-major. */
+void read_deldop_ascii(FILE *fin, struct deldop_t *deldop, int iframe, int idel_use[2], int idop_use[2]);
+void read_deldop_binary(FILE *fin, struct deldop_t *deldop, int iframe, int idel_use[2], int idop_use[2],
+                        int swap_bytes);
+void read_deldop_rdf(FILE *fin, struct deldop_t *deldop, int iframe, int idel_use[2], int idop_use[2],
+                     int swap_bytes);
+void read_doppler_ascii(FILE *fin, struct doppler_t *doppler, int iframe, int idop_use[2]);
+void read_doppler_binary(FILE *fin, struct doppler_t *doppler, int iframe, int idop_use[2], int swap_bytes);
+void read_doppler_rdf(FILE *fin, struct doppler_t *doppler, int iframe, int idop_use[2], int swap_bytes);
+
+int ref_read_radar_data(const char *path, int kind, int ndel, int ndop, const int *idel_in, const int *idop_in,
+                        int swap, double sdev, double *obs)
+{
+    int idel_use[2] = {idel_in[0], idel_in[1]}, idop_use[2] = {idop_in[0], idop_in[1]};
+    const int wdel = idel_use[1] - idel_use[0] + 1, wdop = idop_use[1] - idop_use[0] + 1;
+    FILE *fin = fopen(path, "rb");
+    if (!fin) return -1;
+    if (kind < 3) {
+        struct deldop_t *dd = calloc(1, sizeof *dd);      /* 32 MB: not on the stack */
+        dd->ndel = ndel;
+        dd->ndop = ndop;
+        dd->frame = calloc(1, sizeof(struct deldopfrm_t));
+        dd->frame[0].sdev = sdev;
+        dd->frame[0].obs = matrix(1, wdel, 1, wdop);
+        if (kind == 0) read_deldop_ascii(fin, dd, 0, idel_use, idop_use);
+        else if (kind == 1) read_deldop_binary(fin, dd, 0, idel_use, idop_use, swap);
+        else read_deldop_rdf(fin, dd, 0, idel_use, idop_use, swap);
+        for (int j = 1; j <= wdel; j++)
+            for (int k = 1; k <= wdop; k++) obs[(j - 1) * wdop + (k - 1)] = dd->frame[0].obs[j][k];
+        free_matrix(dd->frame[0].obs, 1, wdel, 1, wdop);
+        free(dd->frame);
+        free(dd);
+    } else {
+        struct doppler_t *dp = calloc(1, sizeof *dp);
+        dp->ndop = ndop;
+        dp->frame = calloc(1, sizeof(struct dopfrm_t));
+        dp->frame[0].sdev = sdev;
+        dp->frame[0].obs = vector(1, wdop);
+        if (kind == 3) read_doppler_ascii(fin, dp, 0, idop_use);
+        else if (kind == 4) read_doppler_binary(fin, dp, 0, idop_use, swap);
+        else read_doppler_rdf(fin, dp, 0, idop_use, swap);
+        for (int k = 1; k <= wdop; k++) obs[k - 1] = dp->frame[0].obs[k];
+        free_vector(dp->frame[0].obs, 1, wdop);
+        free(dp->frame);
+        free(dp);
+    }
+    fclose(fin);
+    return 0;
+}

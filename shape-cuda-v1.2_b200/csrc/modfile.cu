@@ -2,8 +2,10 @@
 // models the engine evaluates: one vertex component (read_shape, :289-542)
 // with no component offsets, the homogeneous radar and optical scattering
 // laws (read_photo, :544-1953) and the spin section (read_spin, :1954-2140),
-// read and written; and the listfit output of a radar frame (.fitdat,
-// src/shape/chi2.c:525-560). Host code.
+// read and written; the data files of radar frames (delay-Doppler images
+// and Doppler spectra, src/shape/read_dat.c:800-856, 1150-1176, 2074-2260);
+// and the listfit output of a radar frame (.fitdat, src/shape/chi2.c:
+// 525-560). Host code.
 //
 // The file is a stream of whitespace-separated tokens with comments in
 // curly braces. A parameter is a state token (c, f or =) followed by its
@@ -11,7 +13,10 @@
 // token (src/util/getdouble.c, getint.c). Angles are stored in radians and
 // spin rates in rad/day, by the same operations as read_spin, and the
 // epochs in Julian days (cal2jd, src/astro/jdcal.c:8-13).
+#include <algorithm>
+#include <cctype>
 #include <cerrno>
+#include <cstdint>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -564,6 +569,89 @@ int shape_mod_take_engine(shape_mod_file *m, shape_engine *e)
     shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_LIB, 0, &sp.lib_amp);
     shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_LIB, 1, &sp.lib_freq);
     shape_engine_get_spin_param(e, SHAPE_PAR_SPIN_LIB, 2, &sp.lib_phase);
+    return SHAPE_OK;
+}
+
+// One radar data file (a delay-Doppler image of ndel x ndop, or a Doppler
+// spectrum as ndel = 1), as read_deldop / read_doppler read it
+// (src/shape/read_dat.c:800-856, 1150-1176): the type from the first 128
+// bytes (any byte >= 128: raw float32; "SIMPLE": FITS, not supported;
+// "type" in any case: an RDF header, lines up to one that starts with '.',
+// then float32; otherwise ASCII numbers with comments in curly braces),
+// each value rounded to float, the window idel_use x idop_use (1-based,
+// inclusive) kept and multiplied by sdev; then per kept pixel the gamma
+// transform (value > 0: value^(1/gamma); delay-Doppler data only) and
+// 1/variance = 1/sdev^2, or 1/(sdev^2 + (obs/sqrt(nlooks))^2) with speckle
+// (nlooks > 0), times pixweight of the pixel (full-size array, or null).
+int shape_read_radar_data(const char *path, int ndel, int ndop, const int idel_use[2], const int idop_use[2],
+                          int big_endian, double sdev, double gamma, double nlooks, const double *pixweight,
+                          double *obs, double *oneovervar)
+{
+    if (!path || !idel_use || !idop_use || !obs || !oneovervar || ndel < 1 || ndop < 1 ||
+        idel_use[0] < 1 || idel_use[1] > ndel || idel_use[0] > idel_use[1] || idop_use[0] < 1 ||
+        idop_use[1] > ndop || idop_use[0] > idop_use[1] || !(gamma > 0.0))
+        return shape::report_error(SHAPE_E_ARG, "read_radar_data: invalid argument");
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return shape::report_error(SHAPE_E_ARG, std::string("read_radar_data: cannot open ") + path);
+    std::string text;
+    char buf[1 << 16];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, n);
+    fclose(fp);
+    if (text.size() < 128) return shape::report_error(SHAPE_E_ARG, "read_radar_data: file shorter than 128 bytes");
+    bool binary = false;
+    for (int j = 0; j < 128; j++) binary = binary || (unsigned char)text[j] >= 128;
+    std::string head(text.data(), strnlen(text.data(), 128));
+    const bool fits = !binary && head.find("SIMPLE") != std::string::npos;
+    for (char &c : head) c = (char)tolower((unsigned char)c);
+    const bool rdf = !binary && !fits && head.find("type") != std::string::npos;
+    if (fits) return shape::report_error(SHAPE_E_UNSUPPORTED, "read_radar_data: FITS data files are not supported");
+    const int wdop = idop_use[1] - idop_use[0] + 1;
+    const size_t total = (size_t)ndel * ndop;
+    std::vector<float> px(total);
+    if (binary || rdf) {
+        size_t off = 0;
+        if (rdf) {                                   // header lines, read as fgets reads them (199 bytes at most)
+            for (;;) {
+                if (off >= text.size()) return shape::report_error(SHAPE_E_ARG, "read_radar_data: RDF header without end");
+                const size_t nl = text.find('\n', off);
+                const size_t end = std::min(nl == std::string::npos ? text.size() : nl + 1, off + 199);
+                const char first = text[off];
+                off = end;
+                if (first == '.') break;
+            }
+        }
+        if (text.size() - off < total * sizeof(float))
+            return shape::report_error(SHAPE_E_ARG, "read_radar_data: data file too short");
+        memcpy(px.data(), text.data() + off, total * sizeof(float));
+        const uint16_t one = 1;
+        const bool little_host = *(const unsigned char *)&one == 1;
+        if (little_host == (big_endian != 0))
+            for (float &v : px) {
+                unsigned char *b = (unsigned char *)&v;
+                std::swap(b[0], b[3]);
+                std::swap(b[1], b[2]);
+            }
+    } else {
+        try {
+            Tokens tk(std::move(text));
+            for (size_t k = 0; k < total; k++) px[k] = (float)tk.real("data value");
+        } catch (const ParseError &e) {
+            return shape::report_error(e.code, "read_radar_data: " + e.msg);
+        }
+    }
+    const double lookfact = nlooks > 0.0 ? 1 / sqrt(nlooks) : 0.0;
+    for (int j = idel_use[0]; j <= idel_use[1]; j++)
+        for (int k = idop_use[0]; k <= idop_use[1]; k++) {
+            const size_t src = (size_t)(j - 1) * ndop + (k - 1);
+            const size_t dst = (size_t)(j - idel_use[0]) * wdop + (k - idop_use[0]);
+            double o = px[src] * sdev;
+            if (gamma != 1.0 && o > 0.0) o = pow(o, 1 / gamma);
+            obs[dst] = o;
+            double w = nlooks > 0.0 ? 1 / (pow(sdev, 2.0) + pow(lookfact * o, 2.0)) : 1 / pow(sdev, 2.0);
+            if (pixweight) w *= pixweight[src];
+            oneovervar[dst] = w;
+        }
     return SHAPE_OK;
 }
 

@@ -140,6 +140,8 @@ def load_library(path=LIB_PATH):
     L.shape_mod_write.argtypes = [vp, C.c_char_p]
     L.shape_mod_take_engine.argtypes = [vp, vp]
     L.shape_write_fitdat.argtypes = [C.c_char_p, C.c_int, C.c_int, cd.dptr, C.c_double, C.c_double]
+    L.shape_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int, C.c_double,
+                                        C.c_double, C.c_double, cd.dptr, cd.dptr, cd.dptr]
     L.shape_engine_write_fitdat.argtypes = [vp, C.c_int, C.c_double, C.c_char_p]
     L.shape_engine_get_penalties.argtypes = [vp, cd.dptr, C.c_int]
     L.shape_engine_get_spin_param.argtypes = [vp, C.c_int, C.c_int, P(C.c_double)]
@@ -433,6 +435,23 @@ class Engine:
         _chk(self.L.shape_engine_get_realized(self.h, cd.as_dptr(x), cd.as_dptr(vn), cd.as_dptr(fn),
                                               cd.as_dptr(area)))
         return {"x": x, "vn": vn, "fn": fn, "area": area}
+
+
+def read_radar_data(path, ndel, ndop, idel_use=None, idop_use=None, big_endian=True, sdev=1.0, gamma=1.0,
+                    nlooks=0.0, pixweight=None):
+    """One radar data file (shape_read_radar_data): (obs, 1/variance) of the
+    window idel_use x idop_use (1-based, inclusive; default the whole
+    stored image), each [rows, cols]."""
+    dl = idel_use or (1, ndel)
+    dp = idop_use or (1, ndop)
+    wd, wp = dl[1] - dl[0] + 1, dp[1] - dp[0] + 1
+    obs, oov = np.zeros(max(1, wd * wp)), np.zeros(max(1, wd * wp))
+    pw = None if pixweight is None else np.ascontiguousarray(pixweight, dtype=np.float64).ravel()
+    _chk(load_library().shape_read_radar_data(os.fsencode(path), ndel, ndop, (C.c_int * 2)(*dl), (C.c_int * 2)(*dp),
+                                              1 if big_endian else 0, float(sdev), float(gamma), float(nlooks),
+                                              cd.as_dptr(pw) if pw is not None else None, cd.as_dptr(obs),
+                                              cd.as_dptr(oov)))
+    return obs.reshape(wd, wp), oov.reshape(wd, wp)
 
 
 def write_fitdat(path, fit, cal, sdev):
