@@ -453,6 +453,15 @@ int shape_read_radar_data(const char *path, int ndel, int ndop, const int idel_u
                           int big_endian, double sdev, double gamma, double nlooks, const double *pixweight,
                           double *obs, double *oneovervar);
 
+/* A lightcurve data file (read_lghtcrv, src/shape/read_dat.c:1925-1956):
+ * n points of epoch (JD), magnitude and magnitude error, whitespace-
+ * separated with comments in curly braces. Writes each point's epoch, its
+ * intensity relative to the Sun exp(-0.4 ln10 (mag - sun_appmag)) and
+ * 1/variance with the error 0.4 ln10 magerr intensity, in the reference's
+ * operation order. Host code. */
+int shape_read_lghtcrv_data(const char *path, int n, double sun_appmag, double *t, double *obs,
+                            double *oneovervar);
+
 /* The listfit output of one radar frame (chi2_deldop with listfit,
  * src/shape/chi2.c:525-560): ndel*ndop lines "%13.6e" of cal * fit / sdev,
  * delay-major (fit host memory). */

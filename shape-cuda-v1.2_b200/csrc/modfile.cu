@@ -655,6 +655,41 @@ int shape_read_radar_data(const char *path, int ndel, int ndop, const int idel_u
     return SHAPE_OK;
 }
 
+// A lightcurve data file (read_lghtcrv, src/shape/read_dat.c:1925-1956): n
+// points of (epoch JD, magnitude, magnitude error) as tokens; intensity
+// relative to the Sun exp(-0.4 ln10 (mag - sun_appmag)), its error
+// 0.4 ln10 magerr intensity, and 1/variance.
+int shape_read_lghtcrv_data(const char *path, int n, double sun_appmag, double *t, double *obs,
+                            double *oneovervar)
+{
+    if (!path || n < 1 || !t || !obs || !oneovervar)
+        return shape::report_error(SHAPE_E_ARG, "read_lghtcrv_data: invalid argument");
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return shape::report_error(SHAPE_E_ARG, std::string("read_lghtcrv_data: cannot open ") + path);
+    std::string text;
+    char buf[1 << 16];
+    size_t got;
+    while ((got = fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, got);
+    fclose(fp);
+    const double LN10 = 2.302585092994046;   // src/shape/const.h
+    try {
+        Tokens tk(std::move(text));
+        for (int i = 0; i < n; i++) {
+            const double epoch = tk.real("epoch");
+            const double mag = tk.real("magnitude");
+            const double magerr = tk.real("magnitude error");
+            const double intens = exp(-0.4 * LN10 * (mag - sun_appmag));
+            const double err = (0.4 * LN10 * magerr) * intens;
+            t[i] = epoch;
+            obs[i] = intens;
+            oneovervar[i] = 1.0 / (err * err);
+        }
+    } catch (const ParseError &e) {
+        return shape::report_error(e.code, "read_lghtcrv_data: " + e.msg);
+    }
+    return SHAPE_OK;
+}
+
 // The listfit output of a radar frame (src/shape/chi2.c:555-558): one line
 // "%13.6e" of cal * fit / sdev per bin, delay-major.
 int shape_write_fitdat(const char *path, int ndel, int ndop, const double *fit, double cal, double sdev)

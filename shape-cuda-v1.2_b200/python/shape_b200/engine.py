@@ -140,6 +140,7 @@ def load_library(path=LIB_PATH):
     L.shape_mod_write.argtypes = [vp, C.c_char_p]
     L.shape_mod_take_engine.argtypes = [vp, vp]
     L.shape_write_fitdat.argtypes = [C.c_char_p, C.c_int, C.c_int, cd.dptr, C.c_double, C.c_double]
+    L.shape_read_lghtcrv_data.argtypes = [C.c_char_p, C.c_int, C.c_double, cd.dptr, cd.dptr, cd.dptr]
     L.shape_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int, C.c_double,
                                         C.c_double, C.c_double, cd.dptr, cd.dptr, cd.dptr]
     L.shape_engine_write_fitdat.argtypes = [vp, C.c_int, C.c_double, C.c_char_p]
@@ -452,6 +453,14 @@ def read_radar_data(path, ndel, ndop, idel_use=None, idop_use=None, big_endian=T
                                               cd.as_dptr(pw) if pw is not None else None, cd.as_dptr(obs),
                                               cd.as_dptr(oov)))
     return obs.reshape(wd, wp), oov.reshape(wd, wp)
+
+
+def read_lghtcrv_data(path, n, sun_appmag):
+    """A lightcurve data file (shape_read_lghtcrv_data): (t, obs, 1/variance)."""
+    t, obs, oov = np.zeros(n), np.zeros(n), np.zeros(n)
+    _chk(load_library().shape_read_lghtcrv_data(os.fsencode(path), n, float(sun_appmag), cd.as_dptr(t),
+                                                cd.as_dptr(obs), cd.as_dptr(oov)))
+    return t, obs, oov
 
 
 def write_fitdat(path, fit, cal, sdev):

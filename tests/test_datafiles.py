@@ -101,3 +101,23 @@ def test_radar_data_refusals(tmp_path):
         eng.read_radar_data(p, 5, 40)
     with pytest.raises(eng.EngineError):
         eng.read_radar_data(p, 4, 40, (0, 4), (1, 40))
+
+
+def test_lightcurve_data(tmp_path):
+    """read_lghtcrv's conversion (src/shape/read_dat.c:1925-1956), restated
+    with the same operations: magnitudes to intensities relative to the Sun
+    and their 1/variance."""
+    rng = np.random.default_rng(8)
+    n, sun = 40, -26.74
+    rows = [(2458000.0 + 0.01 * i + rng.uniform(0, 1e-3), rng.uniform(12, 16), rng.uniform(0.005, 0.05))
+            for i in range(n)]
+    p = tmp_path / "lc.dat"
+    p.write_text("{ JD mag err }\n" + "".join("%r %r %r\n" % r for r in rows))
+    t, obs, oov = eng.read_lghtcrv_data(p, n, sun)
+    ln10 = 2.302585092994046
+    for i, (jd, mag, err) in enumerate(rows):
+        intens = math.exp(-0.4 * ln10 * (mag - sun))
+        e = (0.4 * ln10 * err) * intens
+        assert t[i] == jd and obs[i] == intens and oov[i] == 1.0 / (e * e)
+    with pytest.raises(eng.EngineError, match="end of file"):
+        eng.read_lghtcrv_data(p, n + 1, sun)
