@@ -69,7 +69,7 @@ const char *shape_version(void);
 /* sizeof() of every struct in shape_types.h, in the order
  * model_desc, radar_law, optical_law, eval_params, deldop_frame,
  * deldop_set, lghtcrv_point, lghtcrv_set, deldop_result, eval_summary,
- * doppler_frame, doppler_set;
+ * doppler_frame, doppler_set, spin_state, ephem_point;
  * lets bindings verify their layouts. Returns the number written. */
 int shape_abi_sizes(size_t *out, int max);
 
@@ -391,6 +391,20 @@ typedef struct shape_server_stats {
  * non-principal-axis state, return SHAPE_E_ARG. */
 int shape_realize_spin(const shape_spin_state *spin, const double angleoff[3], const double omegaoff[3], int n,
                        const double *t, const double *orbspin, double *ae, double *spin_out);
+
+/* A view's geometry from ephemerides at epoch t (ephem2mat,
+ * src/shape/ephem2mat.c:33-228), with the reference's operations: RA, Dec
+ * and distance interpolated linearly in the asteroid ephemeris (nast >= 2
+ * entries, ascending t; RA across the 0/360 line), the ecliptic ->
+ * observer matrix oe (row-major), the plane-of-sky motion's contribution s
+ * to the apparent spin vector (ecliptic, rad/day), and the distance (AU).
+ * With a solar ephemeris (sun non-NULL; the bistatic case) also the
+ * ecliptic -> solar matrix se, the solar phase angle and the azimuth of the
+ * Sun in the plane of the sky; otherwise both angles are 0. An epoch
+ * outside a table returns SHAPE_E_ARG. Host code. */
+int shape_ephem_view(const shape_ephem_point *ast, int nast, const shape_ephem_point *sun, int nsun, double t,
+                     double oe[9], double se[9], double s[3], double *solar_phase, double *solar_azimuth,
+                     double *dist);
 
 /* ------------------------------------------------------------- model files */
 

@@ -158,7 +158,14 @@ typedef struct shape_doppler_set {
  * only: Euler angles of the principal axes at epoch t0, the body-frame spin
  * vector and its rate of change, spin impulses (body frame, applied at their
  * epochs) and a libration of the third Euler angle. */
-#define SHAPE_MAX_IMPULSES 10     /* MAXIMP, src/shape/shape2.h:1003 */
+#define SHAPE_MAX_IMPULSES 10
+
+/* One ephemeris entry (struct ephpnt_t, src/shape/shape2.h:1047-1052). */
+typedef struct shape_ephem_point {
+    double t;               /* Julian date */
+    double ra, dec;         /* equatorial right ascension, declination (rad) */
+    double dist;            /* distance (AU) */
+} shape_ephem_point;     /* MAXIMP, src/shape/shape2.h:1003 */
 typedef struct shape_spin_state {
     int pa;                       /* 1: principal-axis rotator */
     double t0;                    /* epoch of the initial conditions (days) */

@@ -225,6 +225,9 @@ class Reference:
         L.ref_mod_radar.argtypes = [C.c_void_p, C.c_int, P(cd.RadarLaw)]
         L.ref_mod_optical.argtypes = [C.c_void_p, C.c_int, P(cd.OpticalLaw)]
         L.ref_mod_spin.argtypes = [C.c_void_p, P(cd.SpinState)]
+        L.ref_ephem2mat.argtypes = [cd.dptr, C.c_int, cd.dptr, C.c_int, C.c_double, cd.dptr, cd.dptr, cd.dptr,
+                                    cd.dptr]
+        L.ref_ephem2mat.restype = C.c_double
         L.ref_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int,
                                           C.c_double, cd.dptr]
         L.ref_get_seen.argtypes = [C.c_void_p, C.c_char_p]

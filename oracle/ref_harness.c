@@ -841,3 +841,23 @@ int ref_read_radar_data(const char *path, int kind, int ndel, int ndop, const in
     fclose(fin);
     return 0;
 }
+
+
+/* The reference's ephem2mat (src/shape/ephem2mat.c:33-228) on ephemeris
+ * tables given as (t, ra, dec, dist) quadruples: the check of
+ * shape_ephem_view. nsun = 0: monostatic. */
+double ref_ephem2mat(const double *ast, int nast, const double *sun, int nsun, double t, double *oe, double *se,
+                     double *s, double *phase_az)
+{
+    struct ephem_t A, S;
+    A.n = nast;
+    A.pnt = (struct ephpnt_t *)ast;
+    S.n = nsun;
+    S.pnt = (struct ephpnt_t *)sun;
+    double o[3][3], e[3][3];
+    memset(e, 0, sizeof e);
+    double dist = ephem2mat(A, S, t, o, e, s, &phase_az[0], &phase_az[1], nsun > 0);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) { oe[3 * i + j] = o[i][j]; se[3 * i + j] = e[i][j]; }
+    return dist;
+}

@@ -1235,7 +1235,7 @@ int shape_abi_sizes(size_t *out, int max)
                   sizeof(shape_eval_params), sizeof(shape_deldop_frame), sizeof(shape_deldop_set),
                   sizeof(shape_lghtcrv_point), sizeof(shape_lghtcrv_set), sizeof(shape_deldop_result),
                   sizeof(shape_eval_summary), sizeof(shape_doppler_frame), sizeof(shape_doppler_set),
-                  sizeof(shape_spin_state)};
+                  sizeof(shape_spin_state), sizeof(shape_ephem_point)};
     int n = (int)(sizeof v / sizeof v[0]);
     for (int i = 0; i < n && i < max; i++) out[i] = v[i];
     return n;

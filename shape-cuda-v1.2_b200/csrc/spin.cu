@@ -211,3 +211,126 @@ extern "C" int shape_realize_spin(const shape_spin_state *spin, const double ang
     }
     return SHAPE_OK;
 }
+
+namespace {
+
+// Unit vector in place (normalize, src/util/normalize.c): divided by its
+// length unless that is zero.
+void unit(double u[3])
+{
+    double norm = 0.0;
+    for (int i = 0; i < 3; i++) norm += u[i] * u[i];
+    norm = std::sqrt(norm);
+    if (norm != 0.0)
+        for (int i = 0; i < 3; i++) u[i] /= norm;
+}
+
+void cross3(double z[3], const double x[3], const double y[3])
+{
+    const double a = x[1] * y[2] - x[2] * y[1], b = x[2] * y[0] - x[0] * y[2], c = x[0] * y[1] - x[1] * y[0];
+    z[0] = a; z[1] = b; z[2] = c;
+}
+
+// Equatorial -> ecliptic (J2000 obliquity; the cosine and sine of
+// src/astro/eq2ec.c).
+void eq_to_ecl(double u[3])
+{
+    const double COSEPS = 0.9174821430652418, SINEPS = 0.3977769691126060;
+    const double tmp = u[1] * COSEPS + u[2] * SINEPS;
+    u[2] = u[2] * COSEPS - u[1] * SINEPS;
+    u[1] = tmp;
+}
+
+// Linear interpolation of an ephemeris at t: RA (across the 0/360 line),
+// Dec and distance with their rates; false if t is outside the table.
+bool interpolate(const shape_ephem_point *e, int n, double t, double *ra, double *dec, double *dist,
+                 double *rarate, double *decrate)
+{
+    const double PIE = 3.141592653589793;
+    if (n < 2 || e[0].t > t) return false;
+    int i = 0;
+    while (e[i + 1].t < t) {
+        ++i;
+        if (i == n - 1) return false;
+    }
+    const double Dt = e[i + 1].t - e[i].t, dt = t - e[i].t;
+    const double delta_ra = e[i + 1].ra - e[i].ra, twopi = 2 * PIE;
+    if (delta_ra > PIE)
+        *rarate = (e[i + 1].ra - (e[i].ra + twopi)) / Dt;
+    else if (delta_ra < -PIE)
+        *rarate = ((e[i + 1].ra + twopi) - e[i].ra) / Dt;
+    else
+        *rarate = (e[i + 1].ra - e[i].ra) / Dt;
+    *ra = e[i].ra + *rarate * dt;
+    *ra = *ra - twopi * floor(*ra / twopi);
+    *decrate = (e[i + 1].dec - e[i].dec) / Dt;
+    *dec = e[i].dec + *decrate * dt;
+    const double distrate = (e[i + 1].dist - e[i].dist) / Dt;
+    *dist = e[i].dist + distrate * dt;
+    return true;
+}
+
+}  // namespace
+
+extern "C" int shape_ephem_view(const shape_ephem_point *ast, int nast, const shape_ephem_point *sun, int nsun,
+                                double t, double oe_out[9], double se_out[9], double s[3], double *solar_phase,
+                                double *solar_azimuth, double *dist)
+{
+    const double PIE = 3.141592653589793;
+    if (!ast || !oe_out || !s || !solar_phase || !solar_azimuth || !dist || (sun && !se_out))
+        return shape::report_error(SHAPE_E_ARG, "ephem_view: null argument");
+    double ra, dec, rarate, decrate;
+    if (!interpolate(ast, nast, t, &ra, &dec, dist, &rarate, &decrate))
+        return shape::report_error(SHAPE_E_ARG, "ephem_view: epoch outside the asteroid ephemeris");
+    // observer axes: z toward the observer, x along -RA (pole x z), y = z x x
+    double oe[3][3], ee[3], edot[3];
+    oe[2][0] = -cos(dec) * cos(ra);
+    oe[2][1] = -cos(dec) * sin(ra);
+    oe[2][2] = -sin(dec);
+    for (int i = 0; i < 3; i++) ee[i] = oe[2][i] * *dist;
+    oe[0][0] = -oe[2][1];
+    oe[0][1] = oe[2][0];
+    oe[0][2] = 0.0;
+    unit(oe[0]);
+    cross3(oe[1], oe[2], oe[0]);
+    for (int i = 0; i < 3; i++) eq_to_ecl(oe[i]);
+    // plane-of-sky motion's contribution to the apparent spin: edot x z
+    edot[0] = decrate * sin(dec) * cos(ra) + rarate * cos(dec) * sin(ra);
+    edot[1] = decrate * sin(dec) * sin(ra) - rarate * cos(dec) * cos(ra);
+    edot[2] = -decrate * cos(dec);
+    eq_to_ecl(edot);
+    cross3(s, edot, oe[2]);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) oe_out[3 * i + j] = oe[i][j];
+    if (!sun) {
+        *solar_phase = 0.0;
+        *solar_azimuth = 0.0;
+        return SHAPE_OK;
+    }
+    double ra_s, dec_s, dist_s, rr, dr;
+    if (!interpolate(sun, nsun, t, &ra_s, &dec_s, &dist_s, &rr, &dr))
+        return shape::report_error(SHAPE_E_ARG, "ephem_view: epoch outside the solar ephemeris");
+    double ss[3] = {cos(dec_s) * cos(ra_s) * dist_s, cos(dec_s) * sin(ra_s) * dist_s, sin(dec_s) * dist_s};
+    for (int i = 0; i < 3; i++) ss[i] = ss[i] + ee[i];   // asteroid -> Sun
+    eq_to_ecl(ss);
+    unit(ss);
+    const double theta = acos(ss[2]), phi = atan2(ss[1], ss[0]) + PIE / 2;
+    double se[3][3];
+    euler_zxz(se, phi, theta, 0.0);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) se_out[3 * i + j] = se[i][j];
+    double so[3];
+    for (int i = 0; i < 3; i++) {
+        so[i] = 0.0;
+        for (int j = 0; j < 3; j++) so[i] += oe[i][j] * ss[j];
+    }
+    unit(so);
+    *solar_phase = acos(so[2]);
+    if (so[0] == 0.0 && so[1] == 0.0) {
+        *solar_azimuth = 0.0;
+    } else {
+        *solar_azimuth = atan2(so[1], so[0]) - PIE / 2;
+        if (*solar_azimuth < 0.0) *solar_azimuth += 2 * PIE;
+    }
+    return SHAPE_OK;
+}

@@ -84,6 +84,10 @@ class DopplerSet(C.Structure):
 MAX_IMPULSES = 10
 
 
+class EphemPoint(C.Structure):
+    _fields_ = [("t", C.c_double), ("ra", C.c_double), ("dec", C.c_double), ("dist", C.c_double)]
+
+
 class SpinState(C.Structure):
     """shape_spin_state (include/shape_types.h)."""
     _fields_ = [

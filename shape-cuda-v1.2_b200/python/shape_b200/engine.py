@@ -140,6 +140,8 @@ def load_library(path=LIB_PATH):
     L.shape_mod_write.argtypes = [vp, C.c_char_p]
     L.shape_mod_take_engine.argtypes = [vp, vp]
     L.shape_write_fitdat.argtypes = [C.c_char_p, C.c_int, C.c_int, cd.dptr, C.c_double, C.c_double]
+    L.shape_ephem_view.argtypes = [P(cd.EphemPoint), C.c_int, P(cd.EphemPoint), C.c_int, C.c_double, cd.dptr,
+                                   cd.dptr, cd.dptr, P(C.c_double), P(C.c_double), P(C.c_double)]
     L.shape_read_lghtcrv_data.argtypes = [C.c_char_p, C.c_int, C.c_double, cd.dptr, cd.dptr, cd.dptr]
     L.shape_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int, C.c_double,
                                         C.c_double, C.c_double, cd.dptr, cd.dptr, cd.dptr]
@@ -453,6 +455,23 @@ def read_radar_data(path, ndel, ndop, idel_use=None, idop_use=None, big_endian=T
                                               cd.as_dptr(pw) if pw is not None else None, cd.as_dptr(obs),
                                               cd.as_dptr(oov)))
     return obs.reshape(wd, wp), oov.reshape(wd, wp)
+
+
+def ephem_view(ast, t, sun=None):
+    """View geometry at epoch t from ephemeris rows (t, ra, dec, dist):
+    dict of oe (3x3), se (3x3, bistatic), s, solar_phase, solar_azimuth,
+    dist."""
+    def table(rows):
+        a = np.ascontiguousarray(rows, dtype=np.float64).reshape(-1, 4)
+        return (cd.EphemPoint * len(a))(*[cd.EphemPoint(*r) for r in a]), len(a)
+    A, na = table(ast)
+    S, ns = table(sun) if sun is not None else (None, 0)
+    oe, se, s = np.zeros(9), np.zeros(9), np.zeros(3)
+    ph, az, d = C.c_double(), C.c_double(), C.c_double()
+    _chk(load_library().shape_ephem_view(A, na, S, ns, float(t), cd.as_dptr(oe), cd.as_dptr(se), cd.as_dptr(s),
+                                         C.byref(ph), C.byref(az), C.byref(d)))
+    return {"oe": oe.reshape(3, 3), "se": se.reshape(3, 3), "s": s, "solar_phase": ph.value,
+            "solar_azimuth": az.value, "dist": d.value}
 
 
 def read_lghtcrv_data(path, n, sun_appmag):

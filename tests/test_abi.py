@@ -42,6 +42,7 @@ def test_struct_layouts_match_compiler():
     for k, name in enumerate(("shape_doppler_frame", "shape_doppler_set")):
         assert C.sizeof(cd.STRUCTS[name]) == sizes[len(eng.ABI_ORDER) + 1 + k], name
     assert C.sizeof(cd.SpinState) == sizes[len(eng.ABI_ORDER) + 3], "shape_spin_state"
+    assert C.sizeof(cd.EphemPoint) == sizes[len(eng.ABI_ORDER) + 4], "shape_ephem_point"
 
 
 def test_errors_without_device_are_reported():
