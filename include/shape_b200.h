@@ -406,6 +406,16 @@ int shape_ephem_view(const shape_ephem_point *ast, int nast, const shape_ephem_p
                      double oe[9], double se[9], double s[3], double *solar_phase, double *solar_azimuth,
                      double *dist);
 
+/* A radar view's epoch and geometry as the reference's dataset reader sets
+ * them (src/shape/read_dat.c:866-900): shape_ephem_view at t_obs (the
+ * view's epoch from the .obs file), then, with perform_ltc
+ * (par->perform_ltc), the epoch less the one-way light time (5.775518328e-3
+ * day per AU of the distance found) and the ephemeris evaluated again.
+ * Writes the view epoch (for shape_realize_spin), oe and the orbital spin
+ * contribution. */
+int shape_ephem_radar_view(const shape_ephem_point *ast, int nast, double t_obs, int perform_ltc, double *t_view,
+                           double oe[9], double orbspin[3]);
+
 /* ------------------------------------------------------------- model files */
 
 /* A SHAPE model file (.mod) as read_mod reads it (src/shape/read_mod.c:204-227,

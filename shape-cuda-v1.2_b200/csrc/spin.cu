@@ -334,3 +334,20 @@ extern "C" int shape_ephem_view(const shape_ephem_point *ast, int nast, const sh
     }
     return SHAPE_OK;
 }
+
+// A radar view's epoch and geometry as read_deldop / read_doppler set them
+// (src/shape/read_dat.c:866-900): the ephemeris at the uncorrected epoch
+// gives the distance; with light-time correction the one-way light time
+// (DAYSPERAU = 5.775518328e-3 day per AU, src/shape/const.h) is taken off
+// the epoch and the ephemeris evaluated again there.
+extern "C" int shape_ephem_radar_view(const shape_ephem_point *ast, int nast, double t_obs, int perform_ltc,
+                                      double *t_view, double oe[9], double orbspin[3])
+{
+    if (!t_view) return shape::report_error(SHAPE_E_ARG, "ephem_radar_view: null argument");
+    double ph, az, dist;
+    *t_view = t_obs;
+    int rc = shape_ephem_view(ast, nast, nullptr, 0, *t_view, oe, nullptr, orbspin, &ph, &az, &dist);
+    if (rc || !perform_ltc) return rc;
+    *t_view -= 5.775518328e-3 * dist;
+    return shape_ephem_view(ast, nast, nullptr, 0, *t_view, oe, nullptr, orbspin, &ph, &az, &dist);
+}

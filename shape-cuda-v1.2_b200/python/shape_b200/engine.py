@@ -142,6 +142,8 @@ def load_library(path=LIB_PATH):
     L.shape_write_fitdat.argtypes = [C.c_char_p, C.c_int, C.c_int, cd.dptr, C.c_double, C.c_double]
     L.shape_ephem_view.argtypes = [P(cd.EphemPoint), C.c_int, P(cd.EphemPoint), C.c_int, C.c_double, cd.dptr,
                                    cd.dptr, cd.dptr, P(C.c_double), P(C.c_double), P(C.c_double)]
+    L.shape_ephem_radar_view.argtypes = [P(cd.EphemPoint), C.c_int, C.c_double, C.c_int, P(C.c_double), cd.dptr,
+                                         cd.dptr]
     L.shape_read_lghtcrv_data.argtypes = [C.c_char_p, C.c_int, C.c_double, cd.dptr, cd.dptr, cd.dptr]
     L.shape_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int, C.c_double,
                                         C.c_double, C.c_double, cd.dptr, cd.dptr, cd.dptr]
@@ -472,6 +474,16 @@ def ephem_view(ast, t, sun=None):
                                          C.byref(ph), C.byref(az), C.byref(d)))
     return {"oe": oe.reshape(3, 3), "se": se.reshape(3, 3), "s": s, "solar_phase": ph.value,
             "solar_azimuth": az.value, "dist": d.value}
+
+
+def ephem_radar_view(ast, t_obs, perform_ltc=True):
+    """(view epoch, oe 3x3, orbital spin) of a radar view (shape_ephem_radar_view)."""
+    a = np.ascontiguousarray(ast, dtype=np.float64).reshape(-1, 4)
+    A = (cd.EphemPoint * len(a))(*[cd.EphemPoint(*r) for r in a])
+    tv, oe, s = C.c_double(), np.zeros(9), np.zeros(3)
+    _chk(load_library().shape_ephem_radar_view(A, len(a), float(t_obs), 1 if perform_ltc else 0, C.byref(tv),
+                                               cd.as_dptr(oe), cd.as_dptr(s)))
+    return tv.value, oe.reshape(3, 3), s
 
 
 def read_lghtcrv_data(path, n, sun_appmag):

@@ -62,3 +62,18 @@ def test_ephem_view_out_of_range():
         eng.ephem_view(ast, ast[-1, 0] + 0.1)
     with pytest.raises(eng.EngineError):
         eng.ephem_view(ast[:1], ast[0, 0])
+
+
+def test_radar_view_light_time(ref):
+    """The light-time-corrected view: the reference's sequence of two
+    ephem2mat calls with the epoch moved by 5.775518328e-3 day per AU."""
+    rng = np.random.default_rng(77)
+    ast = _table(rng, 10, 2458000.0, 2.0, 0.03)
+    for t in rng.uniform(ast[1, 0], ast[-1, 0], 8):
+        _, _, _, _, d = _ref(ref, ast, None, t)
+        tl = t - 5.775518328e-3 * d
+        oe, _, s, _, _ = _ref(ref, ast, None, tl)
+        tv, goe, gs = eng.ephem_radar_view(ast, t, True)
+        assert tv == tl and np.array_equal(goe, oe) and np.array_equal(gs, s)
+        tv0, goe0, _ = eng.ephem_radar_view(ast, t, False)
+        assert tv0 == t and np.array_equal(goe0, _ref(ref, ast, None, t)[0])
