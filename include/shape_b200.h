@@ -416,6 +416,16 @@ int shape_ephem_view(const shape_ephem_point *ast, int nast, const shape_ephem_p
 int shape_ephem_radar_view(const shape_ephem_point *ast, int nast, double t_obs, int perform_ltc, double *t_view,
                            double oe[9], double orbspin[3]);
 
+/* A view's delay and Doppler offsets (bins) from its dataset's
+ * delay-correction polynomial (deldopoffs, src/shape/deldopoffs.c:17-42):
+ * a[0..n] in usec and usec/day^k about epoch t0; deloff = (a0 + sum a_k
+ * (t - t0)^k) / del_per_pixel, dopoff = -(d delay / dt) Ftx /
+ * (dop_per_pixel 86400), in the reference's operation order. These are the
+ * shape_deldop_frame / shape_engine_set_frame_view offsets; a Doppler set
+ * uses dopoff only. */
+int shape_delcor_offsets(const double *a, int n, double t0, double t_view, double del_per_pixel,
+                         double dop_per_pixel, double Ftx, double *deloff, double *dopoff);
+
 /* ------------------------------------------------------------- model files */
 
 /* A SHAPE model file (.mod) as read_mod reads it (src/shape/read_mod.c:204-227,

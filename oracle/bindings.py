@@ -228,6 +228,9 @@ class Reference:
         L.ref_ephem2mat.argtypes = [cd.dptr, C.c_int, cd.dptr, C.c_int, C.c_double, cd.dptr, cd.dptr, cd.dptr,
                                     cd.dptr]
         L.ref_ephem2mat.restype = C.c_double
+        L.ref_deldopoffs.argtypes = [cd.dptr, C.c_int, C.c_double, C.c_int, cd.dptr, C.c_double, C.c_double,
+                                     C.c_double, cd.dptr, cd.dptr]
+        L.ref_deldopoffs.restype = None
         L.ref_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int,
                                           C.c_double, cd.dptr]
         L.ref_get_seen.argtypes = [C.c_void_p, C.c_char_p]

@@ -861,3 +861,36 @@ double ref_ephem2mat(const double *ast, int nast, const double *sun, int nsun, d
         for (int j = 0; j < 3; j++) { oe[3 * i + j] = o[i][j]; se[3 * i + j] = e[i][j]; }
     return dist;
 }
+
+
+/* The reference's deldopoffs (src/shape/deldopoffs.c:17-42) for nv single-
+ * view frames at epochs t[]: the check of shape_delcor_offsets. */
+void deldopoffs(struct deldop_t *deldop);
+void ref_deldopoffs(const double *a, int n, double t0, int nv, const double *t, double delpp, double doppp,
+                    double Ftx, double *deloff, double *dopoff)
+{
+    struct deldop_t *dd = calloc(1, sizeof *dd);
+    dd->nframes = nv;
+    dd->nviews = 1;
+    dd->del_per_pixel = delpp;
+    dd->dop_per_pixel = doppp;
+    dd->Ftx = Ftx;
+    dd->delcor.t0 = t0;
+    dd->delcor.n = n;
+    dd->delcor.a = calloc((size_t)n + 1, sizeof(struct param_t));
+    for (int i = 0; i <= n; i++) dd->delcor.a[i].val = a[i];
+    dd->frame = calloc((size_t)nv, sizeof(struct deldopfrm_t));
+    for (int f = 0; f < nv; f++) {
+        dd->frame[f].view = calloc(1, sizeof(struct deldopview_t));
+        dd->frame[f].view[0].t = t[f];
+    }
+    deldopoffs(dd);
+    for (int f = 0; f < nv; f++) {
+        deloff[f] = dd->frame[f].view[0].deloff;
+        dopoff[f] = dd->frame[f].view[0].dopoff;
+        free(dd->frame[f].view);
+    }
+    free(dd->frame);
+    free(dd->delcor.a);
+    free(dd);
+}

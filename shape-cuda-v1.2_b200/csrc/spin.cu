@@ -351,3 +351,23 @@ extern "C" int shape_ephem_radar_view(const shape_ephem_point *ast, int nast, do
     *t_view -= 5.775518328e-3 * dist;
     return shape_ephem_view(ast, nast, nullptr, 0, *t_view, oe, nullptr, orbspin, &ph, &az, &dist);
 }
+
+// Delay and Doppler offsets of a view from its dataset's delay-correction
+// polynomial (deldopoffs, src/shape/deldopoffs.c:17-42): delay (usec)
+// a0 + sum a_n (t - t0)^n in bins of del_per_pixel, and its rate (usec/day)
+// as a Doppler offset -rate Ftx / (dop_per_pixel 86400) in bins.
+extern "C" int shape_delcor_offsets(const double *a, int n, double t0, double t_view, double del_per_pixel,
+                                    double dop_per_pixel, double Ftx, double *deloff, double *dopoff)
+{
+    if (!a || n < 0 || !deloff || !dopoff || !(del_per_pixel != 0.0) || !(dop_per_pixel != 0.0))
+        return shape::report_error(SHAPE_E_ARG, "delcor_offsets: invalid argument");
+    double x = 1.0, dop = 0.0, del = a[0];
+    const double arg = t_view - t0;
+    for (int k = 1; k <= n; k++) {
+        dop += k * a[k] * x;
+        del += a[k] * (x *= arg);
+    }
+    *deloff = del / del_per_pixel;
+    *dopoff = -dop * Ftx / (dop_per_pixel * 86400.0);
+    return SHAPE_OK;
+}

@@ -144,6 +144,8 @@ def load_library(path=LIB_PATH):
                                    cd.dptr, cd.dptr, P(C.c_double), P(C.c_double), P(C.c_double)]
     L.shape_ephem_radar_view.argtypes = [P(cd.EphemPoint), C.c_int, C.c_double, C.c_int, P(C.c_double), cd.dptr,
                                          cd.dptr]
+    L.shape_delcor_offsets.argtypes = [cd.dptr, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, P(C.c_double), P(C.c_double)]
     L.shape_read_lghtcrv_data.argtypes = [C.c_char_p, C.c_int, C.c_double, cd.dptr, cd.dptr, cd.dptr]
     L.shape_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int, C.c_double,
                                         C.c_double, C.c_double, cd.dptr, cd.dptr, cd.dptr]
@@ -484,6 +486,16 @@ def ephem_radar_view(ast, t_obs, perform_ltc=True):
     _chk(load_library().shape_ephem_radar_view(A, len(a), float(t_obs), 1 if perform_ltc else 0, C.byref(tv),
                                                cd.as_dptr(oe), cd.as_dptr(s)))
     return tv.value, oe.reshape(3, 3), s
+
+
+def delcor_offsets(a, t0, t_view, del_per_pixel, dop_per_pixel, Ftx):
+    """(deloff, dopoff) of a view from a delay-correction polynomial a[0..n]."""
+    c = np.ascontiguousarray(a, dtype=np.float64)
+    d, p = C.c_double(), C.c_double()
+    _chk(load_library().shape_delcor_offsets(cd.as_dptr(c), len(c) - 1, float(t0), float(t_view),
+                                             float(del_per_pixel), float(dop_per_pixel), float(Ftx), C.byref(d),
+                                             C.byref(p)))
+    return d.value, p.value
 
 
 def read_lghtcrv_data(path, n, sun_appmag):

@@ -77,3 +77,17 @@ def test_radar_view_light_time(ref):
         assert tv == tl and np.array_equal(goe, oe) and np.array_equal(gs, s)
         tv0, goe0, _ = eng.ephem_radar_view(ast, t, False)
         assert tv0 == t and np.array_equal(goe0, _ref(ref, ast, None, t)[0])
+
+
+@pytest.mark.parametrize("order", [0, 1, 3])
+def test_delcor_offsets_match_reference(ref, order):
+    rng = np.random.default_rng(40 + order)
+    a = rng.normal(0, 1, order + 1) * 10.0 ** -np.arange(order + 1)
+    t0 = 2458000.5
+    t = t0 + rng.uniform(-3, 3, 9)
+    delpp, doppp, ftx = 0.125, 0.0763, 2380.0
+    d_ref, p_ref = np.zeros(9), np.zeros(9)
+    ref.lib.ref_deldopoffs(cd.as_dptr(a), order, t0, 9, cd.as_dptr(t), delpp, doppp, ftx, cd.as_dptr(d_ref),
+                           cd.as_dptr(p_ref))
+    for k in range(9):
+        assert eng.delcor_offsets(a, t0, t[k], delpp, doppp, ftx) == (d_ref[k], p_ref[k])
