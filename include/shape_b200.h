@@ -496,6 +496,42 @@ int shape_read_radar_data(const char *path, int ndel, int ndop, const int idel_u
 int shape_read_lghtcrv_data(const char *path, int n, double sun_appmag, double *t, double *obs,
                             double *oneovervar);
 
+/* ------------------------------------------------------------- .obs files */
+
+/* The switches of the .par file that the dataset reader uses. */
+typedef struct shape_obs_options {
+    int perform_ltc;        /* par->perform_ltc: light-time correction of view epochs */
+    double dd_gamma;        /* par->dd_gamma (1: none) */
+    int speckle;            /* par->speckle */
+    int big_endian;         /* par->endian == BIG_ENDIAN_DATA (the reference's default) */
+} shape_obs_options;
+
+/* A SHAPE observation file (.obs; read_dat, src/shape/read_dat.c:409-527)
+ * whose datasets are delay-Doppler sets (read_deldop, :528-900) with one
+ * view per frame and no pixel-weighting masks or gzipped data files (those,
+ * and the other dataset types, return SHAPE_E_UNSUPPORTED). Host code. */
+typedef struct shape_obs_file shape_obs_file;
+int shape_obs_read(const char *path, shape_obs_file **out);
+void shape_obs_free(shape_obs_file *o);
+int shape_obs_nsets(const shape_obs_file *o);
+/* Set s's radar setup (set->law is kept: take it from the model's radar
+ * law iradlaw), its frame count, angle and spin offsets (rad, rad/day) and
+ * the number of data elements of its frames. */
+int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *iradlaw, int *nframes,
+                  double angleoff[3], double omegaoff[3], size_t *nelem);
+/* Set s's frames for shape_engine_add_deldop_set: each view's epoch and oe
+ * from the ephemeris (shape_ephem_radar_view), deloff and dopoff from the
+ * delay-correction polynomial (shape_delcor_offsets), ae and the spin
+ * vector from the spin state (shape_realize_spin, with the set's offsets
+ * and the orbital spin), the data file read from the set's directory
+ * (shape_read_radar_data), the weight, dof and calibration. pos_n and
+ * km_per_pixel come from the .par file. obs and oneovervar receive each
+ * frame's image in frame order (nelem doubles); sdev (or NULL) each
+ * frame's sdev. */
+int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
+                     const shape_obs_options *opt, shape_deldop_frame *frames, double *obs, double *oneovervar,
+                     double *sdev);
+
 /* The listfit output of one radar frame (chi2_deldop with listfit,
  * src/shape/chi2.c:525-560): ndel*ndop lines "%13.6e" of cal * fit / sdev,
  * delay-major (fit host memory). */

@@ -894,3 +894,61 @@ void ref_deldopoffs(const double *a, int n, double t0, int nv, const double *t, 
     free(dd->delcor.a);
     free(dd);
 }
+
+
+/* The reference's read_mod + read_dat + realize_delcor + realize_spin on a
+ * model file and an observation file (paths relative to the current
+ * directory, as the reference opens them): the check of shape_obs_read /
+ * shape_obs_frames. ref_obs_frame copies one delay-Doppler frame's view
+ * and data out. */
+typedef struct { struct par_t par; struct mod_t mod; struct dat_t dat; } ref_obsfile;
+
+void *ref_obs_read(const char *modpath, const char *obspath, int perform_ltc, double dd_gamma, int speckle,
+                   int big_endian)
+{
+    ref_obsfile *F = calloc(1, sizeof *F);
+    F->par.action = FIT;
+    F->par.perform_ltc = (unsigned char)perform_ltc;
+    F->par.dd_gamma = dd_gamma;
+    F->par.speckle = (unsigned char)speckle;
+    F->par.endian = big_endian ? BIG_ENDIAN_DATA : LITTLE_ENDIAN_DATA;
+    F->par.int_method = BRUTE;
+    F->par.int_abstol = 1e-7;
+    F->par.pos_scope = LOCAL;              /* POS sizing in read_dat (set_up_pos) */
+    F->par.pos_pixels = 151;
+    F->par.pos_width = 2.25;
+    snprintf(F->mod.name, sizeof F->mod.name, "%s", modpath);
+    snprintf(F->dat.name, sizeof F->dat.name, "%s", obspath);
+    read_mod(&F->par, &F->mod);
+    read_dat(&F->par, &F->mod, &F->dat);
+    realize_delcor(&F->dat, 0.0, 0);
+    realize_spin(&F->par, &F->mod, &F->dat);
+    return F;
+}
+
+/* geom: t, oe[9], orbspin[3], ae[9], spin[3], deloff, dopoff, delcom_vig,
+ * dopcom_vig, dopDC_vig, weight, dof, cal, sdev (34 doubles); ndel/ndop of
+ * the window; obs and oneovervar delay-major (either may be NULL). */
+void ref_obs_frame(void *h, int s, int f, double *geom, int *nd, double *obs, double *oov)
+{
+    ref_obsfile *F = h;
+    struct deldop_t *dd = &F->dat.set[s].desc.deldop;
+    struct deldopfrm_t *fr = &dd->frame[f];
+    struct deldopview_t *v = &fr->view[0];
+    double *g = geom;
+    *g++ = v->t;
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) *g++ = v->oe[i][j];
+    for (int i = 0; i < 3; i++) *g++ = v->orbspin[i];
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) *g++ = v->ae[i][j];
+    for (int i = 0; i < 3; i++) *g++ = v->spin[i];
+    *g++ = v->deloff; *g++ = v->dopoff;
+    *g++ = fr->delcom_vig; *g++ = fr->dopcom_vig; *g++ = fr->dopDC_vig;
+    *g++ = fr->weight; *g++ = fr->dof; *g++ = fr->cal.val; *g++ = fr->sdev;
+    nd[0] = fr->ndel;
+    nd[1] = fr->ndop;
+    for (int j = 1; j <= fr->ndel; j++)
+        for (int k = 1; k <= fr->ndop; k++) {
+            if (obs) obs[(j - 1) * fr->ndop + (k - 1)] = fr->obs[j][k];
+            if (oov) oov[(j - 1) * fr->ndop + (k - 1)] = fr->oneovervar[j][k];
+        }
+}

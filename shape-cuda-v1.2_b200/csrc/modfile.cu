@@ -690,6 +690,203 @@ int shape_read_lghtcrv_data(const char *path, int n, double sun_appmag, double *
     return SHAPE_OK;
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------------- .obs files
+
+struct shape_obs_file {
+    struct Frame {
+        std::string name;
+        double t0, sdev, cal, nlooks, delcom, weight;
+        char cal_state;
+    };
+    struct Set {
+        int iradlaw;
+        double angleoff[3], omegaoff[3];
+        std::vector<shape_ephem_point> ephem;
+        shape_deldop_set dd;
+        int ndel, ndop;
+        double dopcom, dopDC;
+        double delcor_t0;
+        std::vector<double> delcor;
+        std::string dir;
+        std::vector<Frame> frames;
+    };
+    std::vector<Set> sets;
+};
+
+extern "C" {
+
+int shape_obs_read(const char *path, shape_obs_file **out)
+{
+    if (!path || !out) return shape::report_error(SHAPE_E_ARG, "obs_read: null argument");
+    *out = nullptr;
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return shape::report_error(SHAPE_E_ARG, std::string("obs_read: cannot open ") + path);
+    std::string text;
+    char buf[1 << 16];
+    size_t got;
+    while ((got = fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, got);
+    fclose(fp);
+    shape_obs_file *o = new shape_obs_file();
+    try {
+        Tokens tk(std::move(text));
+        const int nsets = tk.integer("number of datasets");
+        if (nsets < 1) tk.fail("no datasets");
+        for (int s = 0; s < nsets; s++) {
+            shape_obs_file::Set S;
+            tk.integer("input node");
+            // dataset angle offsets wrapped to [-180, 180) deg, then radians
+            // (src/shape/read_dat.c:436-446)
+            for (int i = 0; i < 3; i++) {
+                double v = tk.param("angle offset", nullptr);
+                v += 360.0 * floor((180.0 - v) / 360.0);
+                S.angleoff[i] = v * D2R;
+            }
+            for (int i = 0; i < 3; i++) S.omegaoff[i] = tk.param("spin offset", nullptr) * D2R;
+            const std::string type = tk.word("dataset type");
+            if (type != "delay-doppler") tk.fail("dataset type " + type + " is not supported", SHAPE_E_UNSUPPORTED);
+            // read_deldop header (src/shape/read_dat.c:528-640)
+            S.iradlaw = tk.integer("radar law");
+            const int ne = tk.integer("ephemeris points");
+            if (ne < 2) tk.fail("an ephemeris needs at least 2 points");
+            for (int i = 0; i < ne; i++) {
+                shape_ephem_point e;
+                e.t = read_epoch(tk, "ephemeris epoch");
+                e.ra = tk.real("RA") * D2R;
+                e.dec = tk.real("Dec") * D2R;
+                e.dist = tk.real("distance");
+                S.ephem.push_back(e);
+            }
+            memset(&S.dd, 0, sizeof S.dd);
+            S.dd.Ftx = tk.real("Ftx");
+            S.ndel = tk.integer("delay bins");
+            S.dd.del_per_pixel = tk.real("delay resolution");
+            S.dd.spb = tk.integer("samples per baud");
+            S.dd.stride = tk.integer("stride");
+            if (S.dd.spb < 1 || S.dd.stride < 1 || S.dd.spb % S.dd.stride != 0)
+                tk.fail("stride must divide evenly into spb");
+            const std::string code = tk.word("code method");
+            if (code == "short") S.dd.codemethod = SHAPE_CODE_SHORT;
+            else if (code == "long1" || code == "long_orig") S.dd.codemethod = SHAPE_CODE_LONG_ORIG;
+            else if (code == "long2" || code == "long_mod") S.dd.codemethod = SHAPE_CODE_LONG_MOD;
+            else tk.fail("code method " + code + " is not known");
+            S.ndop = tk.integer("Doppler bins");
+            S.dd.dop_per_pixel = tk.real("Doppler resolution");
+            S.dopcom = tk.real("Doppler COM bin");
+            S.dopDC = tk.real("Doppler DC bin");
+            S.dd.dopfftlen = tk.integer("Doppler FFT length");
+            S.delcor_t0 = read_epoch(tk, "delay-correction epoch");
+            const int nd = tk.integer("delay-correction order");
+            if (nd < 0) tk.fail("negative delay-correction order");
+            for (int i = 0; i <= nd; i++) S.delcor.push_back(tk.param("delay-correction coefficient", nullptr));
+            S.dd.dopscale = tk.param("dopscale", nullptr);
+            const int nviews = tk.integer("views per frame");
+            tk.real("view interval");
+            const std::string smear = tk.word("smearing mode");
+            if (smear != "center" && smear != "first") tk.fail("smearing mode " + smear + " is not known");
+            if (nviews != 1) tk.fail("smeared frames (more than one view) are not supported", SHAPE_E_UNSUPPORTED);
+            S.dir = tk.word("data directory");
+            const int nf = tk.integer("number of frames");
+            if (nf < 1) tk.fail("no frames");
+            for (int i = 0; i < nf; i++) {
+                shape_obs_file::Frame F;
+                F.name = tk.word("data file");
+                F.t0 = read_epoch(tk, "frame epoch");
+                F.sdev = tk.real("sdev");
+                F.cal = tk.param("calibration", &F.cal_state);
+                if (F.cal <= 0.0 && F.cal_state == 'c') tk.fail("a fixed calibration must be > 0");
+                F.nlooks = tk.real("looks");
+                F.delcom = tk.real("delay COM bin");
+                F.weight = tk.real("weight");
+                if (tk.integer("pixel weighting") != 0)
+                    tk.fail("pixel-weighting masks are not supported", SHAPE_E_UNSUPPORTED);
+                if (F.name.size() >= 3 && F.name.compare(F.name.size() - 3, 3, ".gz") == 0)
+                    tk.fail("gzipped data files are not supported", SHAPE_E_UNSUPPORTED);
+                S.frames.push_back(F);
+            }
+            o->sets.push_back(std::move(S));
+        }
+    } catch (const ParseError &e) {
+        delete o;
+        return shape::report_error(e.code, "obs_read: " + e.msg);
+    }
+    *out = o;
+    return SHAPE_OK;
+}
+
+void shape_obs_free(shape_obs_file *o) { delete o; }
+
+int shape_obs_nsets(const shape_obs_file *o) { return o ? (int)o->sets.size() : shape::report_error(SHAPE_E_ARG, "obs_nsets: null argument"); }
+
+int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *iradlaw, int *nframes,
+                  double angleoff[3], double omegaoff[3], size_t *nelem)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size()) return shape::report_error(SHAPE_E_ARG, "obs_set: no such set");
+    const shape_obs_file::Set &S = o->sets[s];
+    if (set) {
+        shape_radar_law law = set->law;
+        *set = S.dd;
+        set->law = law;
+    }
+    if (iradlaw) *iradlaw = S.iradlaw;
+    if (nframes) *nframes = (int)S.frames.size();
+    for (int i = 0; i < 3; i++) {
+        if (angleoff) angleoff[i] = S.angleoff[i];
+        if (omegaoff) omegaoff[i] = S.omegaoff[i];
+    }
+    if (nelem) *nelem = S.frames.size() * (size_t)S.ndel * S.ndop;
+    return SHAPE_OK;
+}
+
+int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
+                     const shape_obs_options *opt, shape_deldop_frame *frames, double *obs, double *oneovervar,
+                     double *sdev)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size() || !spin || !opt || !frames || !obs || !oneovervar)
+        return shape::report_error(SHAPE_E_ARG, "obs_frames: invalid argument");
+    const shape_obs_file::Set &S = o->sets[s];
+    const int nf = (int)S.frames.size();
+    const size_t D = (size_t)S.ndel * S.ndop;
+    std::vector<double> t(nf), orb(3 * (size_t)nf), ae(9 * (size_t)nf), sp(3 * (size_t)nf);
+    for (int f = 0; f < nf; f++) {
+        const shape_obs_file::Frame &F = S.frames[f];
+        shape_deldop_frame &G = frames[f];
+        memset(&G, 0, sizeof G);
+        G.pos_n = pos_n;
+        G.km_per_pixel = km_per_pixel;
+        if (int rc = shape_ephem_radar_view(S.ephem.data(), (int)S.ephem.size(), F.t0, opt->perform_ltc, &t[f],
+                                            G.oe, &orb[3 * (size_t)f]))
+            return rc;
+        if (int rc = shape_delcor_offsets(S.delcor.data(), (int)S.delcor.size() - 1, S.delcor_t0, t[f],
+                                          S.dd.del_per_pixel, S.dd.dop_per_pixel, S.dd.Ftx, &G.deloff, &G.dopoff))
+            return rc;
+        G.ndel = S.ndel;
+        G.ndop = S.ndop;
+        G.delcom_vig = F.delcom;                 // no mask: the window is the whole image
+        G.dopcom_vig = S.dopcom;
+        G.dopDC_vig = S.dopDC;
+        G.weight = F.weight;
+        G.dof = F.weight * S.ndel * S.ndop;
+        G.cal_floating = F.cal_state == 'f';
+        G.cal = F.cal;
+        if (sdev) sdev[f] = F.sdev;
+        const std::string full = S.dir + "/" + F.name;
+        const int dl[2] = {1, S.ndel}, dp[2] = {1, S.ndop};
+        if (int rc = shape_read_radar_data(full.c_str(), S.ndel, S.ndop, dl, dp, opt->big_endian, F.sdev,
+                                           opt->dd_gamma, opt->speckle ? F.nlooks : 0.0, nullptr, obs + f * D,
+                                           oneovervar + f * D))
+            return rc;
+    }
+    if (int rc = shape_realize_spin(spin, S.angleoff, S.omegaoff, nf, t.data(), orb.data(), ae.data(), sp.data()))
+        return rc;
+    for (int f = 0; f < nf; f++) {
+        memcpy(frames[f].ae, &ae[9 * (size_t)f], sizeof frames[f].ae);
+        memcpy(frames[f].spin, &sp[3 * (size_t)f], sizeof frames[f].spin);
+    }
+    return SHAPE_OK;
+}
+
 // The listfit output of a radar frame (src/shape/chi2.c:555-558): one line
 // "%13.6e" of cal * fit / sdev per bin, delay-major.
 int shape_write_fitdat(const char *path, int ndel, int ndop, const double *fit, double cal, double sdev)

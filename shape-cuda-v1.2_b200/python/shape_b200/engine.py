@@ -146,6 +146,14 @@ def load_library(path=LIB_PATH):
                                          cd.dptr]
     L.shape_delcor_offsets.argtypes = [cd.dptr, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                        C.c_double, P(C.c_double), P(C.c_double)]
+    L.shape_obs_read.argtypes = [C.c_char_p, P(vp)]
+    L.shape_obs_free.argtypes = [vp]
+    L.shape_obs_free.restype = None
+    L.shape_obs_nsets.argtypes = [vp]
+    L.shape_obs_set.argtypes = [vp, C.c_int, P(cd.DeldopSet), P(C.c_int), P(C.c_int), cd.dptr, cd.dptr,
+                                P(C.c_size_t)]
+    L.shape_obs_frames.argtypes = [vp, C.c_int, P(cd.SpinState), C.c_int, C.c_double, P(ObsOptions),
+                                   P(cd.DeldopFrame), cd.dptr, cd.dptr, cd.dptr]
     L.shape_read_lghtcrv_data.argtypes = [C.c_char_p, C.c_int, C.c_double, cd.dptr, cd.dptr, cd.dptr]
     L.shape_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int, C.c_double,
                                         C.c_double, C.c_double, cd.dptr, cd.dptr, cd.dptr]
@@ -511,6 +519,49 @@ def write_fitdat(path, fit, cal, sdev):
     f = np.ascontiguousarray(fit, dtype=np.float64)
     ndel, ndop = f.shape if f.ndim == 2 else (1, f.size)
     _chk(load_library().shape_write_fitdat(os.fsencode(path), ndel, ndop, cd.as_dptr(f), float(cal), float(sdev)))
+
+
+class ObsOptions(C.Structure):
+    _fields_ = [("perform_ltc", C.c_int), ("dd_gamma", C.c_double), ("speckle", C.c_int), ("big_endian", C.c_int)]
+
+
+class ObsFile:
+    """A SHAPE observation file read by shape_obs_read (delay-Doppler sets)."""
+
+    def __init__(self, path):
+        self.L = load_library()
+        self.h = None
+        h = C.c_void_p()
+        _chk(self.L.shape_obs_read(os.fsencode(path), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.L.shape_obs_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def nsets(self):
+        return _chk(self.L.shape_obs_nsets(self.h))
+
+    def set_info(self, s):
+        st, law, nf, ne = cd.DeldopSet(), C.c_int(), C.c_int(), C.c_size_t()
+        ao, oo = np.zeros(3), np.zeros(3)
+        _chk(self.L.shape_obs_set(self.h, s, C.byref(st), C.byref(law), C.byref(nf), cd.as_dptr(ao), cd.as_dptr(oo),
+                                  C.byref(ne)))
+        return {"set": st, "iradlaw": law.value, "nframes": nf.value, "angleoff": ao, "omegaoff": oo,
+                "nelem": ne.value}
+
+    def frames(self, s, spin, pos_n, km_per_pixel, perform_ltc=1, dd_gamma=1.0, speckle=0, big_endian=1):
+        info = self.set_info(s)
+        nf = info["nframes"]
+        fr = (cd.DeldopFrame * nf)()
+        obs, oov, sdev = np.zeros(info["nelem"]), np.zeros(info["nelem"]), np.zeros(nf)
+        opt = ObsOptions(perform_ltc, dd_gamma, speckle, big_endian)
+        _chk(self.L.shape_obs_frames(self.h, s, C.byref(spin), int(pos_n), float(km_per_pixel), C.byref(opt), fr,
+                                     cd.as_dptr(obs), cd.as_dptr(oov), cd.as_dptr(sdev)))
+        return list(fr), obs, oov, sdev
 
 
 class ModFile:

@@ -1,0 +1,96 @@
+"""Observation files (.obs): shape_obs_read + shape_obs_frames against the
+reference's own read_dat, realize_delcor and realize_spin (via
+ref_obs_read) on the CPU, for a delay-Doppler set with an ephemeris, a
+delay-correction polynomial, dataset angle and spin offsets and ASCII and
+big-endian binary data files: every frame's observer and body matrices,
+spin vector, delay and Doppler offsets, COM bins, weight, dof,
+calibration, sdev, and its obs and 1/variance images, bit for bit."""
+import numpy as np
+import pytest
+
+import cases
+from oracle.bindings import Reference
+from shape_b200 import ctypes_defs as cd
+from shape_b200 import engine as eng
+from test_modfile import write_mod
+
+OBS = """{ one delay-Doppler set }
+1
+0
+c 0.5 c -0.3 c 190.0   { angle offsets (deg) }
+c 0 c 0 c 0.2          { spin offsets (deg/day) }
+delay-doppler
+0                      { radar law }
+3
+2018 3 14 0 0 0  359.5 10.2 0.031
+2018 3 15 0 0 0  0.4 10.0 0.030
+2018 3 16 0 0 0  1.1 9.8 0.029
+2380.0 20 0.5 1 1 long_orig
+30 0.1 15.5 15.0 64
+2018 3 14 12 0 0  2 c 0.25 c 0.01 c -0.002
+c 1.0
+1 0.0 center
+d
+3
+f0.dat 2018 3 14 5 6 7  1.5  f 1.0  4 10.0 1.0 0
+f1.dat 2018 3 14 17 0 0  1.2  c 2.0  0  9.5 0.8 0
+f2.dat 2018 3 15 9 30 0  0.9  f 1.0  9 11.0 1.2 0
+"""
+
+
+@pytest.mark.parametrize("ltc,gamma,speckle", [(1, 1.0, 0), (0, 1.4, 1)])
+def test_obs_matches_reference(tmp_path, monkeypatch, ltc, gamma, speckle):
+    monkeypatch.chdir(tmp_path)
+    m = cases.c1()[0]
+    write_mod(tmp_path / "m.mod", m, seed=3)
+    (tmp_path / "d").mkdir()
+    rng = np.random.default_rng(12)
+    for f in range(3):
+        img = rng.normal(0, 1, (20, 30))
+        img[0, 0] = -1.5
+        if f == 2:
+            (tmp_path / "d" / "f2.dat").write_bytes(img.astype(">f4").tobytes())
+        else:
+            (tmp_path / "d" / ("f%d.dat" % f)).write_text("\n".join(repr(float(x)) for x in img.ravel()) + "\n")
+    (tmp_path / "t.obs").write_text(OBS)
+    spin = eng.ModFile("m.mod").spin()
+    o = eng.ObsFile("t.obs")
+    info = o.set_info(0)
+    assert o.nsets() == 1 and info["nframes"] == 3 and info["iradlaw"] == 0
+    assert info["set"].codemethod == 1 and info["set"].Ftx == 2380.0
+    frames, obs, oov, sdev = o.frames(0, spin, 75, 0.02, perform_ltc=ltc, dd_gamma=gamma, speckle=speckle)
+    ref = Reference()
+    h = ref.lib.ref_obs_read(b"m.mod", b"t.obs", ltc, gamma, speckle, 1)
+    D = 20 * 30
+    for f in range(3):
+        g, nd = np.zeros(34), (eng.C.c_int * 2)()
+        ro, rv = np.zeros(D), np.zeros(D)
+        ref.lib.ref_obs_frame(h, 0, f, cd.as_dptr(g), nd, cd.as_dptr(ro), cd.as_dptr(rv))
+        fr = frames[f]
+        assert (nd[0], nd[1]) == (fr.ndel, fr.ndop) == (20, 30)
+        assert list(fr.oe) == list(g[1:10]), f
+        assert list(fr.ae) == list(g[13:22]), f
+        assert list(fr.spin) == list(g[22:25]), f
+        assert (fr.deloff, fr.dopoff) == (g[25], g[26]), f
+        assert (fr.delcom_vig, fr.dopcom_vig, fr.dopDC_vig) == (g[27], g[28], g[29])
+        assert (fr.weight, fr.dof, fr.cal, sdev[f]) == (g[30], g[31], g[32], g[33])
+        assert fr.cal_floating == (f != 1)
+        assert np.array_equal(obs[f * D:(f + 1) * D], ro) and np.array_equal(oov[f * D:(f + 1) * D], rv), f
+        assert fr.pos_n == 75 and fr.km_per_pixel == 0.02
+
+
+def test_obs_refusals(tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    p = tmp_path / "u.obs"
+    p.write_text(OBS.replace("delay-doppler", "lightcurve"))
+    with pytest.raises(eng.EngineError, match="error -4"):
+        eng.ObsFile(p)
+    p.write_text(OBS.replace("1 0.0 center", "3 60.0 center"))
+    with pytest.raises(eng.EngineError, match="error -4"):
+        eng.ObsFile(p)
+    p.write_text(OBS.replace("1.0 0\nf1", "1.0 1\nf1"))
+    with pytest.raises(eng.EngineError, match="error -4"):
+        eng.ObsFile(p)
+    p.write_text(OBS.replace("long_orig", "long9"))
+    with pytest.raises(eng.EngineError, match="error -1"):
+        eng.ObsFile(p)
