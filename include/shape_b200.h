@@ -507,13 +507,17 @@ typedef struct shape_obs_options {
 } shape_obs_options;
 
 /* A SHAPE observation file (.obs; read_dat, src/shape/read_dat.c:409-527)
- * whose datasets are delay-Doppler sets (read_deldop, :528-900) with one
- * view per frame and no pixel-weighting masks or gzipped data files (those,
- * and the other dataset types, return SHAPE_E_UNSUPPORTED). Host code. */
+ * whose datasets are delay-Doppler sets (read_deldop, :528-900) or Doppler
+ * sets (read_doppler, :920-1180) with one view per frame and no
+ * pixel-weighting masks or gzipped data files (those, and the other
+ * dataset types, return SHAPE_E_UNSUPPORTED). Host code. */
 typedef struct shape_obs_file shape_obs_file;
 int shape_obs_read(const char *path, shape_obs_file **out);
 void shape_obs_free(shape_obs_file *o);
 int shape_obs_nsets(const shape_obs_file *o);
+/* 0: set s is a delay-Doppler set (shape_obs_set / shape_obs_frames);
+ * 1: a Doppler set (shape_obs_doppler). */
+int shape_obs_set_type(const shape_obs_file *o, int s);
 /* Set s's radar setup (set->law is kept: take it from the model's radar
  * law iradlaw), its frame count, angle and spin offsets (rad, rad/day) and
  * the number of data elements of its frames. */
@@ -531,6 +535,15 @@ int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *ir
 int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
                      const shape_obs_options *opt, shape_deldop_frame *frames, double *obs, double *oneovervar,
                      double *sdev);
+
+/* A Doppler set's setup (set->law is kept) and frames for
+ * shape_engine_add_doppler_set, built as shape_obs_frames builds
+ * delay-Doppler frames (dopoff from the delay-correction polynomial's
+ * rate, src/shape/dopoffs.c:19-40). obs and oneovervar receive each
+ * frame's spectrum in frame order. */
+int shape_obs_doppler(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
+                      const shape_obs_options *opt, shape_doppler_set *set, shape_doppler_frame *frames, double *obs,
+                      double *oneovervar);
 
 /* The listfit output of one radar frame (chi2_deldop with listfit,
  * src/shape/chi2.c:525-560): ndel*ndop lines "%13.6e" of cal * fit / sdev,

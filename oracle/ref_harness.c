@@ -952,3 +952,27 @@ void ref_obs_frame(void *h, int s, int f, double *geom, int *nd, double *obs, do
             if (oov) oov[(j - 1) * fr->ndop + (k - 1)] = fr->oneovervar[j][k];
         }
 }
+
+/* A Doppler frame of ref_obs_read's data: geom = t, oe[9], orbspin[3],
+ * ae[9], spin[3], dopoff, dopcom_vig, weight, dof, cal, sdev (31 doubles);
+ * ndop of the window; the spectrum and its 1/variance. */
+void ref_obs_doppler_frame(void *h, int s, int f, double *geom, int *ndop, double *obs, double *oov)
+{
+    ref_obsfile *F = h;
+    struct doppler_t *dp = &F->dat.set[s].desc.doppler;
+    struct dopfrm_t *fr = &dp->frame[f];
+    struct dopview_t *v = &fr->view[0];
+    double *g = geom;
+    *g++ = v->t;
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) *g++ = v->oe[i][j];
+    for (int i = 0; i < 3; i++) *g++ = v->orbspin[i];
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) *g++ = v->ae[i][j];
+    for (int i = 0; i < 3; i++) *g++ = v->spin[i];
+    *g++ = v->dopoff;
+    *g++ = fr->dopcom_vig; *g++ = fr->weight; *g++ = fr->dof; *g++ = fr->cal.val; *g++ = fr->sdev;
+    *ndop = fr->ndop;
+    for (int k = 1; k <= fr->ndop; k++) {
+        obs[k - 1] = fr->obs[k];
+        oov[k - 1] = fr->oneovervar[k];
+    }
+}

@@ -701,6 +701,7 @@ struct shape_obs_file {
         char cal_state;
     };
     struct Set {
+        int doppler = 0;                 // 1: a Doppler set (read_doppler)
         int iradlaw;
         double angleoff[3], omegaoff[3];
         std::vector<shape_ephem_point> ephem;
@@ -745,8 +746,10 @@ int shape_obs_read(const char *path, shape_obs_file **out)
             }
             for (int i = 0; i < 3; i++) S.omegaoff[i] = tk.param("spin offset", nullptr) * D2R;
             const std::string type = tk.word("dataset type");
-            if (type != "delay-doppler") tk.fail("dataset type " + type + " is not supported", SHAPE_E_UNSUPPORTED);
-            // read_deldop header (src/shape/read_dat.c:528-640)
+            if (type != "delay-doppler" && type != "doppler")
+                tk.fail("dataset type " + type + " is not supported", SHAPE_E_UNSUPPORTED);
+            S.doppler = type == "doppler";
+            // read_deldop / read_doppler headers (src/shape/read_dat.c:528-640, 920-1000)
             S.iradlaw = tk.integer("radar law");
             const int ne = tk.integer("ephemeris points");
             if (ne < 2) tk.fail("an ephemeris needs at least 2 points");
@@ -760,6 +763,15 @@ int shape_obs_read(const char *path, shape_obs_file **out)
             }
             memset(&S.dd, 0, sizeof S.dd);
             S.dd.Ftx = tk.real("Ftx");
+            if (S.doppler) {
+                S.ndel = 1;
+                S.ndop = tk.integer("Doppler bins");
+                S.dd.dop_per_pixel = tk.real("Doppler bin width");
+                S.dopcom = tk.real("Doppler COM bin");
+                S.dd.del_per_pixel = 1.0;
+                S.dd.spb = S.dd.stride = 1;
+                S.dd.codemethod = SHAPE_CODE_LONG_ORIG;
+            } else {
             S.ndel = tk.integer("delay bins");
             S.dd.del_per_pixel = tk.real("delay resolution");
             S.dd.spb = tk.integer("samples per baud");
@@ -776,6 +788,7 @@ int shape_obs_read(const char *path, shape_obs_file **out)
             S.dopcom = tk.real("Doppler COM bin");
             S.dopDC = tk.real("Doppler DC bin");
             S.dd.dopfftlen = tk.integer("Doppler FFT length");
+            }
             S.delcor_t0 = read_epoch(tk, "delay-correction epoch");
             const int nd = tk.integer("delay-correction order");
             if (nd < 0) tk.fail("negative delay-correction order");
@@ -797,7 +810,7 @@ int shape_obs_read(const char *path, shape_obs_file **out)
                 F.cal = tk.param("calibration", &F.cal_state);
                 if (F.cal <= 0.0 && F.cal_state == 'c') tk.fail("a fixed calibration must be > 0");
                 F.nlooks = tk.real("looks");
-                F.delcom = tk.real("delay COM bin");
+                F.delcom = S.doppler ? 1.0 : tk.real("delay COM bin");
                 F.weight = tk.real("weight");
                 if (tk.integer("pixel weighting") != 0)
                     tk.fail("pixel-weighting masks are not supported", SHAPE_E_UNSUPPORTED);
@@ -818,6 +831,12 @@ int shape_obs_read(const char *path, shape_obs_file **out)
 void shape_obs_free(shape_obs_file *o) { delete o; }
 
 int shape_obs_nsets(const shape_obs_file *o) { return o ? (int)o->sets.size() : shape::report_error(SHAPE_E_ARG, "obs_nsets: null argument"); }
+
+int shape_obs_set_type(const shape_obs_file *o, int s)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size()) return shape::report_error(SHAPE_E_ARG, "obs_set_type: no such set");
+    return o->sets[s].doppler;
+}
 
 int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *iradlaw, int *nframes,
                   double angleoff[3], double omegaoff[3], size_t *nelem)
@@ -846,6 +865,7 @@ int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spi
     if (!o || s < 0 || s >= (int)o->sets.size() || !spin || !opt || !frames || !obs || !oneovervar)
         return shape::report_error(SHAPE_E_ARG, "obs_frames: invalid argument");
     const shape_obs_file::Set &S = o->sets[s];
+    if (S.doppler) return shape::report_error(SHAPE_E_ARG, "obs_frames: a Doppler set (use shape_obs_doppler)");
     const int nf = (int)S.frames.size();
     const size_t D = (size_t)S.ndel * S.ndop;
     std::vector<double> t(nf), orb(3 * (size_t)nf), ae(9 * (size_t)nf), sp(3 * (size_t)nf);
@@ -876,6 +896,61 @@ int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spi
         if (int rc = shape_read_radar_data(full.c_str(), S.ndel, S.ndop, dl, dp, opt->big_endian, F.sdev,
                                            opt->dd_gamma, opt->speckle ? F.nlooks : 0.0, nullptr, obs + f * D,
                                            oneovervar + f * D))
+            return rc;
+    }
+    if (int rc = shape_realize_spin(spin, S.angleoff, S.omegaoff, nf, t.data(), orb.data(), ae.data(), sp.data()))
+        return rc;
+    for (int f = 0; f < nf; f++) {
+        memcpy(frames[f].ae, &ae[9 * (size_t)f], sizeof frames[f].ae);
+        memcpy(frames[f].spin, &sp[3 * (size_t)f], sizeof frames[f].spin);
+    }
+    return SHAPE_OK;
+}
+
+// A Doppler set's setup and frames (read_doppler, src/shape/read_dat.c:
+// 920-1180; dopoffs, src/shape/dopoffs.c:19-40), as shape_obs_frames does
+// for delay-Doppler sets.
+int shape_obs_doppler(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
+                      const shape_obs_options *opt, shape_doppler_set *set, shape_doppler_frame *frames, double *obs,
+                      double *oneovervar)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size() || !spin || !opt || !set || !frames || !obs || !oneovervar)
+        return shape::report_error(SHAPE_E_ARG, "obs_doppler: invalid argument");
+    const shape_obs_file::Set &S = o->sets[s];
+    if (!S.doppler) return shape::report_error(SHAPE_E_ARG, "obs_doppler: not a Doppler set");
+    const shape_radar_law law = set->law;
+    memset(set, 0, sizeof *set);
+    set->dop_per_bin = S.dd.dop_per_pixel;
+    set->Ftx = S.dd.Ftx;
+    set->dopscale = S.dd.dopscale;
+    set->law = law;
+    const int nf = (int)S.frames.size();
+    std::vector<double> t(nf), orb(3 * (size_t)nf), ae(9 * (size_t)nf), sp(3 * (size_t)nf);
+    for (int f = 0; f < nf; f++) {
+        const shape_obs_file::Frame &F = S.frames[f];
+        shape_doppler_frame &G = frames[f];
+        memset(&G, 0, sizeof G);
+        G.pos_n = pos_n;
+        G.km_per_pixel = km_per_pixel;
+        if (int rc = shape_ephem_radar_view(S.ephem.data(), (int)S.ephem.size(), F.t0, opt->perform_ltc, &t[f],
+                                            G.oe, &orb[3 * (size_t)f]))
+            return rc;
+        double deloff;
+        if (int rc = shape_delcor_offsets(S.delcor.data(), (int)S.delcor.size() - 1, S.delcor_t0, t[f], 1.0,
+                                          S.dd.dop_per_pixel, S.dd.Ftx, &deloff, &G.dopoff))
+            return rc;
+        G.ndop = S.ndop;
+        G.dopcom_vig = S.dopcom;                 // no mask: the whole spectrum
+        G.weight = F.weight;
+        G.dof = F.weight * S.ndop;
+        G.cal_floating = F.cal_state == 'f';
+        G.cal = F.cal;
+        G.sdev = F.sdev;
+        const std::string full = S.dir + "/" + F.name;
+        const int dl[2] = {1, 1}, dp[2] = {1, S.ndop};
+        if (int rc = shape_read_radar_data(full.c_str(), 1, S.ndop, dl, dp, opt->big_endian, F.sdev, 1.0,
+                                           opt->speckle ? F.nlooks : 0.0, nullptr, obs + (size_t)f * S.ndop,
+                                           oneovervar + (size_t)f * S.ndop))
             return rc;
     }
     if (int rc = shape_realize_spin(spin, S.angleoff, S.omegaoff, nf, t.data(), orb.data(), ae.data(), sp.data()))

@@ -150,6 +150,9 @@ def load_library(path=LIB_PATH):
     L.shape_obs_free.argtypes = [vp]
     L.shape_obs_free.restype = None
     L.shape_obs_nsets.argtypes = [vp]
+    L.shape_obs_set_type.argtypes = [vp, C.c_int]
+    L.shape_obs_doppler.argtypes = [vp, C.c_int, P(cd.SpinState), C.c_int, C.c_double, P(ObsOptions),
+                                    P(cd.DopplerSet), P(cd.DopplerFrame), cd.dptr, cd.dptr]
     L.shape_obs_set.argtypes = [vp, C.c_int, P(cd.DeldopSet), P(C.c_int), P(C.c_int), cd.dptr, cd.dptr,
                                 P(C.c_size_t)]
     L.shape_obs_frames.argtypes = [vp, C.c_int, P(cd.SpinState), C.c_int, C.c_double, P(ObsOptions),
@@ -552,6 +555,20 @@ class ObsFile:
                                   C.byref(ne)))
         return {"set": st, "iradlaw": law.value, "nframes": nf.value, "angleoff": ao, "omegaoff": oo,
                 "nelem": ne.value}
+
+    def set_type(self, s):
+        """0: delay-Doppler set, 1: Doppler set."""
+        return _chk(self.L.shape_obs_set_type(self.h, s))
+
+    def doppler(self, s, spin, pos_n, km_per_pixel, nframes, ndop, perform_ltc=1, speckle=0, big_endian=1):
+        """A Doppler set: (shape_doppler_set, frames, obs, 1/variance)."""
+        st = cd.DopplerSet()
+        fr = (cd.DopplerFrame * nframes)()
+        obs, oov = np.zeros(nframes * ndop), np.zeros(nframes * ndop)
+        opt = ObsOptions(perform_ltc, 1.0, speckle, big_endian)
+        _chk(self.L.shape_obs_doppler(self.h, s, C.byref(spin), int(pos_n), float(km_per_pixel), C.byref(opt),
+                                      C.byref(st), fr, cd.as_dptr(obs), cd.as_dptr(oov)))
+        return st, list(fr), obs, oov
 
     def frames(self, s, spin, pos_n, km_per_pixel, perform_ltc=1, dd_gamma=1.0, speckle=0, big_endian=1):
         info = self.set_info(s)

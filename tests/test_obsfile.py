@@ -79,6 +79,57 @@ def test_obs_matches_reference(tmp_path, monkeypatch, ltc, gamma, speckle):
         assert fr.pos_n == 75 and fr.km_per_pixel == 0.02
 
 
+DOPPLER_SET = """0
+c 0 c 0 c 0
+c 0 c 0 c -0.1
+doppler
+0
+2
+2018 3 14 0 0 0  359.5 10.2 0.031
+2018 3 16 0 0 0  1.1 9.8 0.029
+2380.0 64 0.25 31.5
+2018 3 14 12 0 0  1 c 0.25 c 0.03
+f 1.0
+1 0.0 first
+d
+2
+s0.dat 2018 3 14 8 0 0  1.1  f 1.0  6  1.0 0
+s1.dat 2018 3 15 2 0 0  0.7  c 1.5  0  0.5 0
+"""
+
+
+@pytest.mark.parametrize("speckle", [0, 1])
+def test_obs_doppler_set_matches_reference(tmp_path, monkeypatch, speckle):
+    """A delay-Doppler set followed by a Doppler set: the Doppler frames'
+    view, offsets and spectra against the reference's read_doppler,
+    dopoffs and realize_spin."""
+    monkeypatch.chdir(tmp_path)
+    write_mod(tmp_path / "m.mod", cases.c1()[0], seed=3)
+    (tmp_path / "d").mkdir()
+    rng = np.random.default_rng(5)
+    for f in range(3):
+        (tmp_path / "d" / ("f%d.dat" % f)).write_bytes(rng.normal(0, 1, (20, 30)).astype(">f4").tobytes())
+    (tmp_path / "d" / "s0.dat").write_text("\n".join(repr(float(x)) for x in rng.normal(0, 1, 64)) + "\n")
+    (tmp_path / "d" / "s1.dat").write_bytes((-np.abs(rng.normal(0, 1, 64))).astype(">f4").tobytes())
+    (tmp_path / "t.obs").write_text(OBS.replace("{ one delay-Doppler set }\n1\n", "2\n", 1) + DOPPLER_SET)
+    o = eng.ObsFile("t.obs")
+    assert o.nsets() == 2 and o.set_type(0) == 0 and o.set_type(1) == 1
+    spin = eng.ModFile("m.mod").spin()
+    st, frames, obs, oov = o.doppler(1, spin, 60, 0.03, 2, 64, perform_ltc=1, speckle=speckle)
+    assert st.dop_per_bin == 0.25 and st.Ftx == 2380.0 and st.dopscale == 1.0
+    ref = Reference()
+    h = ref.lib.ref_obs_read(b"m.mod", b"t.obs", 1, 1.0, speckle, 1)
+    for f in range(2):
+        g, nd = np.zeros(31), (eng.C.c_int * 1)()
+        ro, rv = np.zeros(64), np.zeros(64)
+        ref.lib.ref_obs_doppler_frame(h, 1, f, cd.as_dptr(g), nd, cd.as_dptr(ro), cd.as_dptr(rv))
+        fr = frames[f]
+        assert nd[0] == fr.ndop == 64
+        assert list(fr.oe) == list(g[1:10]) and list(fr.ae) == list(g[13:22]) and list(fr.spin) == list(g[22:25])
+        assert (fr.dopoff, fr.dopcom_vig, fr.weight, fr.dof, fr.cal, fr.sdev) == tuple(g[25:31]), f
+        assert np.array_equal(obs[64 * f:64 * (f + 1)], ro) and np.array_equal(oov[64 * f:64 * (f + 1)], rv), f
+
+
 def test_obs_refusals(tmp_path, monkeypatch):
     monkeypatch.chdir(tmp_path)
     p = tmp_path / "u.obs"
