@@ -8,15 +8,16 @@
  * src/shape/posvis.c:84, src/shape/pos2deldop.c:176,
  * src/shape/posmask.c:58, src/shape/apply_photo.c:78,
  * src/shape/calc_fits.c:340, src/shape/chi2.c:240) with device-resident
- * model and frame state. A shim in the reference converts
- * struct mod_t / dat_t / par_t into the plain descriptions of shape_types.h
- * once, then calls shape_engine_evaluate where objective() called
- * calc_fits + chi2 (src/shape/bestfit.c:789-790).
+ * model and frame state. A shim compiled into the reference program
+ * converts struct mod_t / dat_t / par_t into the plain descriptions of
+ * shape_types.h once, then calls shape_engine_evaluate where objective()
+ * called calc_fits + chi2 (src/shape/bestfit.c:789-790).
  *
  * Conventions: every function returns SHAPE_OK (0) or a negative
  * SHAPE_E_* status; shape_last_error() gives a message for the calling
- * thread. Host pointers are plain host memory (pinned or not); nothing in
- * the ABI exposes device pointers. An engine handle is bound to one CUDA
+ * thread. Pointer arguments are plain host memory (pinned or not), except
+ * the d_-prefixed arguments of shape_chi2_frames_noalloc, which are device
+ * pointers the caller owns; no call returns a device pointer. An engine handle is bound to one CUDA
  * device and one stream; it is not thread-safe (use one handle per thread),
  * which matches the reference's single-threaded calc_fits.
  */
@@ -327,7 +328,8 @@ int shape_brent_minimize(shape_objective_fn f, void *user, double ax, double bx,
  * array (about 3.5 MB per device, kept until the process exits); the first
  * call on a device looks up its address, so make that first call outside
  * any stream capture. Kernels run on the legacy default stream and the call
- * returns after the results reach host memory. Calls share the scratch
+ * returns after the results reach host memory; the caller's current device
+ * is current again on return. Calls share the scratch
  * array: calls that overlap on the GPU (from several threads or streams)
  * race on it. */
 int shape_chi2_frames_noalloc(int device, int nframes, const long long *frame_offsets,
@@ -510,7 +512,12 @@ typedef struct shape_obs_options {
  * whose datasets are delay-Doppler sets (read_deldop, :528-900) or Doppler
  * sets (read_doppler, :920-1180) with one view per frame and no
  * pixel-weighting masks or gzipped data files (those, and the other
- * dataset types, return SHAPE_E_UNSUPPORTED). Host code. */
+ * dataset types, return SHAPE_E_UNSUPPORTED). The '=' state of angle and
+ * spin offsets and of delay-correction polynomials takes the last earlier
+ * set's value, as the reference's realize_angleoff, realize_omegaoff and
+ * realize_delcor do (src/shape/realize_spin.c:283-337,
+ * src/shape/realize_delcor.c:60-146); '=' on the first set, or a tied
+ * polynomial of another degree or epoch, is SHAPE_E_ARG. Host code. */
 typedef struct shape_obs_file shape_obs_file;
 int shape_obs_read(const char *path, shape_obs_file **out);
 void shape_obs_free(shape_obs_file *o);
@@ -520,7 +527,10 @@ int shape_obs_nsets(const shape_obs_file *o);
 int shape_obs_set_type(const shape_obs_file *o, int s);
 /* Set s's radar setup (set->law is kept: take it from the model's radar
  * law iradlaw), its frame count, angle and spin offsets (rad, rad/day) and
- * the number of data elements of its frames. */
+ * the number of data elements of its frames. iradlaw is >= 0 (a negative
+ * index fails in shape_obs_read); the file does not know the model, so the
+ * caller checks iradlaw < the model's number of radar laws, as
+ * read_deldop does (src/shape/read_dat.c:557-562). */
 int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *iradlaw, int *nframes,
                   double angleoff[3], double omegaoff[3], size_t *nelem);
 /* Set s's frames for shape_engine_add_deldop_set: each view's epoch and oe

@@ -70,6 +70,9 @@ class Oracle:
         L.orc_splint.argtypes = [cd.dptr, cd.dptr, cd.dptr, C.c_int, C.c_double]
         L.orc_radlaw.restype = C.c_double
         L.orc_radlaw.argtypes = [P(cd.RadarLaw), C.c_double]
+        L.orc_chi2_frame.argtypes = [cd.dptr, cd.dptr, cd.dptr, C.c_int, C.c_double, C.c_int, C.c_double,
+                                     P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double),
+                                     P(C.c_double)]
 
     def realize(self, model):
         d = model.desc()

@@ -10,7 +10,7 @@
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REPO="$(cd "$HERE/.." && pwd)"
-REF_ROOT="${REF_ROOT:-/root/reference}"
+REF_ROOT="${REF_ROOT:-$(cd "$REPO/.." && pwd)/reference}"
 SRC="$REF_ROOT/src"
 OUT="$HERE/_ref"
 OBJ="$OUT/obj"

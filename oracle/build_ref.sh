@@ -3,7 +3,8 @@
 # (test infrastructure: the checker and the CPU baseline, never the product).
 #
 # The reference's C sources are compiled where they lie under the reference
-# tree (REF_ROOT, default /root/reference); nothing is copied. Each source is
+# tree (REF_ROOT; by default the reference checkout beside this repository,
+# ../reference); nothing is copied. Each source is
 # compiled with -I- so that its own directory is not searched for quoted
 # includes, which lets oracle/refshim/shape/head.h stand in for the
 # reference's head.h (that one includes an absent cfitsio by absolute path and
@@ -14,7 +15,7 @@
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REPO="$(cd "$HERE/.." && pwd)"
-REF_ROOT="${REF_ROOT:-/root/reference}"
+REF_ROOT="${REF_ROOT:-$(cd "$REPO/.." && pwd)/reference}"
 SRC="$REF_ROOT/src"
 OUT="$HERE/_ref"
 OBJ="$OUT/obj"

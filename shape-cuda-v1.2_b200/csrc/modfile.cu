@@ -117,13 +117,16 @@ public:
     }
     [[noreturn]] void fail(const std::string &m, int code = SHAPE_E_ARG) const
     {
-        throw ParseError{code, "model file line " + std::to_string(line_) + ": " + m};
+        throw ParseError{code, kind_ + " line " + std::to_string(line_) + ": " + m};
     }
+    // the kind of file named in error messages
+    void set_kind(const char *kind) { kind_ = kind; }
 
 private:
     std::string t_;
     size_t p_ = 0;
     int line_ = 1;
+    std::string kind_ = "model file";
 };
 
 // Julian day number of a calendar date at noon: Gregorian from 1582
@@ -704,6 +707,8 @@ struct shape_obs_file {
         int doppler = 0;                 // 1: a Doppler set (read_doppler)
         int iradlaw;
         double angleoff[3], omegaoff[3];
+        char angle_state[3], omega_state[3];   // c, f or = (= ties to an earlier set)
+        char delcor_state;                     // state of the first delay-correction coefficient
         std::vector<shape_ephem_point> ephem;
         shape_deldop_set dd;
         int ndel, ndop;
@@ -715,6 +720,43 @@ struct shape_obs_file {
     };
     std::vector<Set> sets;
 };
+
+// The '=' state ties a set's value to the last earlier set that gives its
+// own: each component of the angle and spin offsets on its own
+// (realize_angleoff / realize_omegaoff, src/shape/realize_spin.c:283-337),
+// and the whole delay-correction polynomial with its epoch when the first
+// coefficient has it (realize_delcor, src/shape/realize_delcor.c:60-146).
+// The first set cannot take '='; a tied polynomial must have the earlier
+// one's degree and an epoch within half a second of it.
+static void tie_obs_sets(std::vector<shape_obs_file::Set> &sets, const Tokens &tk)
+{
+    constexpr double HALF_SECOND_DAYS = 5.8e-6;
+    for (int j = 0; j < 3; j++) {
+        int sa = -1, so = -1;
+        for (size_t s = 0; s < sets.size(); s++) {
+            shape_obs_file::Set &S = sets[s];
+            if (S.angle_state[j] != '=') sa = (int)s;
+            else if (sa < 0) tk.fail("the first dataset's angle offsets cannot take the = state");
+            else S.angleoff[j] = sets[sa].angleoff[j];
+            if (S.omega_state[j] != '=') so = (int)s;
+            else if (so < 0) tk.fail("the first dataset's spin offsets cannot take the = state");
+            else S.omegaoff[j] = sets[so].omegaoff[j];
+        }
+    }
+    int sd = -1;
+    for (size_t s = 0; s < sets.size(); s++) {
+        shape_obs_file::Set &S = sets[s];
+        if (S.delcor_state != '=') { sd = (int)s; continue; }
+        if (sd < 0) tk.fail("the first delay-correction polynomial cannot take the = state");
+        const shape_obs_file::Set &T = sets[sd];
+        if (S.delcor.size() != T.delcor.size())
+            tk.fail("delay-correction polynomials tied by = must have the same degree");
+        if (fabs(S.delcor_t0 - T.delcor_t0) > HALF_SECOND_DAYS)
+            tk.fail("delay-correction polynomials tied by = must have the same epoch");
+        S.delcor_t0 = T.delcor_t0;
+        S.delcor = T.delcor;
+    }
+}
 
 extern "C" {
 
@@ -732,6 +774,7 @@ int shape_obs_read(const char *path, shape_obs_file **out)
     shape_obs_file *o = new shape_obs_file();
     try {
         Tokens tk(std::move(text));
+        tk.set_kind("observation file");
         const int nsets = tk.integer("number of datasets");
         if (nsets < 1) tk.fail("no datasets");
         for (int s = 0; s < nsets; s++) {
@@ -740,17 +783,18 @@ int shape_obs_read(const char *path, shape_obs_file **out)
             // dataset angle offsets wrapped to [-180, 180) deg, then radians
             // (src/shape/read_dat.c:436-446)
             for (int i = 0; i < 3; i++) {
-                double v = tk.param("angle offset", nullptr);
+                double v = tk.param("angle offset", &S.angle_state[i]);
                 v += 360.0 * floor((180.0 - v) / 360.0);
                 S.angleoff[i] = v * D2R;
             }
-            for (int i = 0; i < 3; i++) S.omegaoff[i] = tk.param("spin offset", nullptr) * D2R;
+            for (int i = 0; i < 3; i++) S.omegaoff[i] = tk.param("spin offset", &S.omega_state[i]) * D2R;
             const std::string type = tk.word("dataset type");
             if (type != "delay-doppler" && type != "doppler")
                 tk.fail("dataset type " + type + " is not supported", SHAPE_E_UNSUPPORTED);
             S.doppler = type == "doppler";
             // read_deldop / read_doppler headers (src/shape/read_dat.c:528-640, 920-1000)
             S.iradlaw = tk.integer("radar law");
+            if (S.iradlaw < 0) tk.fail("negative radar law index");
             const int ne = tk.integer("ephemeris points");
             if (ne < 2) tk.fail("an ephemeris needs at least 2 points");
             for (int i = 0; i < ne; i++) {
@@ -792,7 +836,11 @@ int shape_obs_read(const char *path, shape_obs_file **out)
             S.delcor_t0 = read_epoch(tk, "delay-correction epoch");
             const int nd = tk.integer("delay-correction order");
             if (nd < 0) tk.fail("negative delay-correction order");
-            for (int i = 0; i <= nd; i++) S.delcor.push_back(tk.param("delay-correction coefficient", nullptr));
+            for (int i = 0; i <= nd; i++) {
+                char st;
+                S.delcor.push_back(tk.param("delay-correction coefficient", &st));
+                if (i == 0) S.delcor_state = st;
+            }
             S.dd.dopscale = tk.param("dopscale", nullptr);
             const int nviews = tk.integer("views per frame");
             tk.real("view interval");
@@ -820,6 +868,7 @@ int shape_obs_read(const char *path, shape_obs_file **out)
             }
             o->sets.push_back(std::move(S));
         }
+        tie_obs_sets(o->sets, tk);
     } catch (const ParseError &e) {
         delete o;
         return shape::report_error(e.code, "obs_read: " + e.msg);

@@ -158,6 +158,23 @@ static double *g_addr[MAX_DEVICES];          // device address of g_noalloc_scra
 // Errors go to the message shape_last_error() returns (engine.cu).
 static int fail(int code, const std::string &m) { return shape::report_error(code, m); }
 
+// Makes `device` current for the call and gives the caller's current device
+// back on every return path.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t set(int device)
+    {
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) { prev = -1; return e; }
+        return prev == device ? cudaSuccess : cudaSetDevice(device);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace noalloc
 }  // namespace shape
 
@@ -185,7 +202,8 @@ extern "C" int shape_chi2_frames_noalloc(int device, int nframes, const long lon
                                      " elements exceed the maximum of " +
                                      std::to_string((long long)MAX_ITEMS * CHI2_BLOCK));
     if (device < 0 || device >= MAX_DEVICES) return fail(SHAPE_E_ARG, "shape_chi2_frames_noalloc: bad device");
-    cudaError_t e = cudaSetDevice(device);
+    DeviceGuard dg;
+    cudaError_t e = dg.set(device);
     if (e != cudaSuccess) return fail(SHAPE_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     double *base;
     {

@@ -34,6 +34,17 @@
 #ifndef RASTER_MIN_BLOCKS_F64
 #define RASTER_MIN_BLOCKS_F64 4
 #endif
+#ifndef RASTER_RADAR_Z64
+#define RASTER_RADAR_Z64 1
+#endif
+#ifndef RASTER_RARE_NOINLINE
+#define RASTER_RARE_NOINLINE 0
+#endif
+#if RASTER_RARE_NOINLINE
+#define RARE_FN __noinline__
+#else
+#define RARE_FN __forceinline__
+#endif
 
 namespace shape {
 
@@ -592,6 +603,16 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
     }
 }
 
+// The FP32 raster's general scatter (footprints beyond the fast path's, or
+// responses other than its two), kept out of line so its arrays and
+// constants do not raise the fast path's register use.
+static __device__ RARE_FN void pixel_dd_scatter_f32_generic(const RasterArgs &a, const FrameGeom &g,
+                                                           const DDC<float> &k, float cose, const PixDD<float> &d,
+                                                           float *fit)
+{
+    pixel_dd_scatter<float>(a, g, k, cose, d, fit, 1, 1, g.ndop);
+}
+
 // One footprint row of the FP32 raster straight into the frame's fit image:
 // the row's FAST_COLS-wide weights (zero beyond the footprint) are shifted
 // by the misalignment m of the first bin (0..3 floats) into the 16-byte
@@ -629,7 +650,7 @@ __device__ inline void pixel_dd_scatter_f32_direct(const RasterArgs &a, const Fr
     // branches; other frames and larger footprints take the general path
     const bool lean = (g.nsinc2 == 1) && (g.codemethod == SHAPE_CODE_LONG_ORIG || g.spb == 1);
     if (!lean || nr > FAST_ROWS || nc > FAST_COLS) {
-        pixel_dd_scatter<float>(a, g, k, cose, d, fit, 1, 1, g.ndop);
+        pixel_dd_scatter_f32_generic(a, g, k, cose, d, fit);
         return;
     }
     const float su = sinf(3.141592653589793f * d.dfrac);
@@ -668,7 +689,7 @@ __device__ inline void pixel_dd_scatter_f32_direct(const RasterArgs &a, const Fr
 // the same weights as pixel_dd_scatter's generic path (one row, delay
 // response 1), bins clipped to the overflow spectrum.
 template <typename T>
-__device__ void pixel_dop_overflow(const RasterArgs &a, const FrameGeom &g, const DDC<T> &k, T cose,
+__device__ RARE_FN void pixel_dop_overflow(const RasterArgs &a, const FrameGeom &g, const DDC<T> &k, T cose,
                                    const PixDD<T> &d)
 {
     const int idop_min = d.idop_min, idop_max = d.idop_max;
@@ -719,7 +740,7 @@ __device__ inline double facet_depth64(const double4 *vt, int4 c, double x0, dou
 // ids: the bin's (facet, packed tile bbox) entries, sorted; (li, lj): the
 // pixel in the tile; (x0, y0): its centre. Returns the winner's facet
 // (-1: none) and writes its FP32 depth and the cos(e) state.
-static __device__ __forceinline__ int pixel_posvis64(const RasterArgs &a, const FrameGeom &g, const int2 *ids,
+static __device__ RARE_FN int pixel_posvis64(const RasterArgs &a, const FrameGeom &g, const int2 *ids,
                                                   int count, int li, int lj, double x0, double y0, float *zz,
                                                   bool *good, float *gm)
 {
@@ -1077,7 +1098,7 @@ k_raster(RasterArgs a)
         if constexpr (sizeof(T) == 4) {
             if (fac < 0) {
                 z64 = -SHAPE_HUGENUMBER;
-            } else if (EXACT || g.kind != VIEW_RADAR) {
+            } else if ((EXACT && (RASTER_RADAR_Z64 || writes_pos)) || g.kind != VIEW_RADAR) {
                 const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
                 z64 = facet_depth64(vt, a.fvi[fac], (double)pi * g.kmpp, (double)pj * g.kmpp);
             }

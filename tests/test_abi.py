@@ -62,10 +62,10 @@ def test_dropin_compiles_against_reference_headers(tmp_path):
     definitions and exports calc_fits (signature of src/shape/shape2.h:1451)
     and calc_fits_chi2_b200 under their default names."""
     import pytest
-    ref_src = os.environ.get("REF_ROOT", "/root/reference") + "/src"
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    ref_src = os.environ.get("REF_ROOT", os.path.join(os.path.dirname(repo), "reference")) + "/src"
     if not os.path.isdir(os.path.join(ref_src, "shape")):
         pytest.skip("reference headers not present")
-    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     inc = ["-I" + os.path.join(ref_src, d) for d in ("shape", "util", "nr", "astro", "pgm",
                                                      "HostMultiThreading")]
     obj = str(tmp_path / "dropin.o")

@@ -145,3 +145,74 @@ def test_obs_refusals(tmp_path, monkeypatch):
     p.write_text(OBS.replace("long_orig", "long9"))
     with pytest.raises(eng.EngineError, match="error -1"):
         eng.ObsFile(p)
+
+
+TIED_DOPPLER_SET = """0
+= 0 c 0.3 = 0
+= 0 c 0 = 0
+doppler
+0
+2
+2018 3 14 0 0 0  359.5 10.2 0.031
+2018 3 16 0 0 0  1.1 9.8 0.029
+2380.0 64 0.25 31.5
+2018 3 14 12 0 0  2 = 9.0 = 9.0 = 9.0
+f 1.0
+1 0.0 first
+d
+2
+s0.dat 2018 3 14 8 0 0  1.1  f 1.0  6  1.0 0
+s1.dat 2018 3 15 2 0 0  0.7  c 1.5  0  0.5 0
+"""
+
+
+def test_obs_tied_sets_match_reference(tmp_path, monkeypatch):
+    """A Doppler set that ties components of its angle and spin offsets and
+    its delay-correction polynomial (same epoch) to the delay-Doppler
+    set before it with the = state: the tied values are the earlier set's,
+    as the reference's realize_angleoff / realize_omegaoff / realize_delcor
+    make them, so the Doppler frames' body matrices, spin vectors and
+    Doppler offsets equal the reference's bit for bit."""
+    monkeypatch.chdir(tmp_path)
+    write_mod(tmp_path / "m.mod", cases.c1()[0], seed=3)
+    (tmp_path / "d").mkdir()
+    rng = np.random.default_rng(8)
+    for f in range(3):
+        (tmp_path / "d" / ("f%d.dat" % f)).write_bytes(rng.normal(0, 1, (20, 30)).astype(">f4").tobytes())
+    for f in range(2):
+        (tmp_path / "d" / ("s%d.dat" % f)).write_bytes(rng.normal(0, 1, 64).astype(">f4").tobytes())
+    (tmp_path / "t.obs").write_text(OBS.replace("{ one delay-Doppler set }\n1\n", "2\n", 1) + TIED_DOPPLER_SET)
+    o = eng.ObsFile("t.obs")
+    a0, a1 = o.set_info(0), o.set_info(1)
+    assert a1["angleoff"][0] == a0["angleoff"][0] and a1["angleoff"][2] == a0["angleoff"][2]
+    assert a1["omegaoff"][0] == a0["omegaoff"][0] and a1["omegaoff"][2] == a0["omegaoff"][2]
+    assert a1["angleoff"][1] != a0["angleoff"][1]
+    spin = eng.ModFile("m.mod").spin()
+    st, frames, obs, oov = o.doppler(1, spin, 60, 0.03, 2, 64, perform_ltc=1)
+    ref = Reference()
+    h = ref.lib.ref_obs_read(b"m.mod", b"t.obs", 1, 1.0, 0, 1)
+    for f in range(2):
+        g, nd = np.zeros(31), (eng.C.c_int * 1)()
+        ro, rv = np.zeros(64), np.zeros(64)
+        ref.lib.ref_obs_doppler_frame(h, 1, f, cd.as_dptr(g), nd, cd.as_dptr(ro), cd.as_dptr(rv))
+        fr = frames[f]
+        assert list(fr.oe) == list(g[1:10]) and list(fr.ae) == list(g[13:22]) and list(fr.spin) == list(g[22:25])
+        assert (fr.dopoff, fr.dopcom_vig, fr.weight, fr.dof, fr.cal, fr.sdev) == tuple(g[25:31]), f
+
+
+def test_obs_tie_refusals(tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    p = tmp_path / "u.obs"
+    p.write_text(OBS.replace("c 0.5 c -0.3 c 190.0", "= 0.5 c -0.3 c 190.0"))
+    with pytest.raises(eng.EngineError, match="first dataset's angle offsets"):
+        eng.ObsFile(p)
+    two = OBS.replace("{ one delay-Doppler set }\n1\n", "2\n", 1)
+    p.write_text(two + TIED_DOPPLER_SET.replace("2 = 9.0 = 9.0 = 9.0", "1 = 9.0 = 9.0"))
+    with pytest.raises(eng.EngineError, match="same degree"):
+        eng.ObsFile(p)
+    p.write_text(two + TIED_DOPPLER_SET.replace("12 0 0  2 =", "12 0 1  2 ="))
+    with pytest.raises(eng.EngineError, match="same epoch"):
+        eng.ObsFile(p)
+    p.write_text(OBS.replace("0                      { radar law }", "-1"))
+    with pytest.raises(eng.EngineError, match="observation file line .*negative radar law"):
+        eng.ObsFile(p)
