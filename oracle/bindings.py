@@ -194,6 +194,7 @@ class Reference:
     def __init__(self):
         L = self.lib = _load(REF_SO, "oracle/build_ref.sh")
         P = C.POINTER
+        L.ref_spline_eval.argtypes = [cd.dptr, cd.dptr, C.c_int, cd.dptr, C.c_int, cd.dptr]
         L.ref_new.restype = C.c_void_p
         L.ref_new.argtypes = [P(cd.ModelDesc), P(cd.EvalParams), C.c_int]
         L.ref_set_radar_law.argtypes = [C.c_void_p, P(cd.RadarLaw)]
@@ -319,6 +320,13 @@ class Reference:
                                           (C.c_int * 2)(*idop_use), swap, sdev, cd.as_dptr(obs))
         assert rc == 0
         return obs
+
+    def spline_eval(self, x, y, t):
+        """The reference's spline() + splint() at epochs t (natural ends)."""
+        x, y, t = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, t))
+        out = np.zeros(len(t))
+        self.lib.ref_spline_eval(cd.as_dptr(x), cd.as_dptr(y), len(x), cd.as_dptr(t), len(t), cd.as_dptr(out))
+        return out
 
     def mnbrak(self, fn, ax, bx):
         cb = OBJFN(fn)

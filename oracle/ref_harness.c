@@ -463,6 +463,20 @@ void ref_get_doppler_frame(void *h, int s, int f, double *fit, double *z, double
     }
 }
 
+/* The reference's natural cubic spline as calc_lghtcrv uses it
+ * (src/shape/calc_fits.c:1923-1933): spline() over the n knots (x, y) with
+ * both end derivatives 2e30, then splint() at each of the m epochs t. */
+void ref_spline_eval(const double *x, const double *y, int n, const double *t, int m, double *out)
+{
+    double *xv = vector(1, n), *yv = vector(1, n), *y2 = vector(1, n);
+    for (int i = 1; i <= n; i++) { xv[i] = x[i - 1]; yv[i] = y[i - 1]; }
+    spline(xv, yv, n, 2.0e30, 2.0e30, y2);
+    for (int k = 0; k < m; k++) splint(xv, yv, y2, n, t[k], &out[k]);
+    free_vector(xv, 1, n);
+    free_vector(yv, 1, n);
+    free_vector(y2, 1, n);
+}
+
 /* Outputs of a lightcurve set after ref_evaluate: y[ncalc], fit[n], [cal, chi2]. */
 void ref_get_lghtcrv(void *h, int s, double *y, double *fit, double out[2])
 {

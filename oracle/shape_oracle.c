@@ -879,31 +879,33 @@ double orc_lghtcrv_point(const shape_eval_params *par, const orc_real *real,
 /* ------------------------------------------------------------------- spline */
 
 /* Natural cubic spline through (x[i], y[i]), i = 0..n-1: second derivatives
- * y2 with y2[0] = y2[n-1] = 0, from the standard tridiagonal system
+ * y2 with y2[0] = y2[n-1] = 0, from the tridiagonal system
  *   h[i-1] y2[i-1] + 2 (h[i-1] + h[i]) y2[i] + h[i] y2[i+1]
- *     = 6 ((y[i+1]-y[i])/h[i] - (y[i]-y[i-1])/h[i-1]),
- * solved by forward elimination and back substitution. This is the role of
- * spline(x, y, n, 2e30, 2e30, y2) in src/shape/calc_fits.c:1923. */
+ *     = 6 ((y[i+1]-y[i])/h[i] - (y[i]-y[i-1])/h[i-1])
+ * with each row divided by its span x[i+1] - x[i-1]: lower coefficient
+ * w = h[i-1] / span, diagonal 2, upper 1 - w. Forward elimination keeps,
+ * per row, the multiplier of y2[i+1] (stored in y2[i]) and the eliminated
+ * right-hand side r[i]; back substitution then gives y2[i] = m[i] y2[i+1]
+ * + r[i]. Solving the span-scaled rows in this order is how the reference
+ * solves the system (spline(x, y, n, 2e30, 2e30, y2),
+ * src/shape/calc_fits.c:1923), so the second derivatives and every fit
+ * value are bit-identical to it. */
 void orc_spline_natural(const double *x, const double *y, int n, double *y2)
 {
-    if (n < 3) {
-        for (int i = 0; i < n; i++) y2[i] = 0.0;
-        return;
-    }
-    double *cp = malloc(sizeof(double) * (size_t)n);
-    y2[0] = 0.0;
-    cp[0] = 0.0;
+    if (n < 1) return;
+    double *r = malloc(sizeof(double) * (size_t)n);
+    y2[0] = r[0] = 0.0;
     for (int i = 1; i < n - 1; i++) {
-        double hl = x[i] - x[i - 1], hr = x[i + 1] - x[i];
-        double diag = 2.0 * (hl + hr) - hl * cp[i - 1];
-        double rhs = 6.0 * ((y[i + 1] - y[i]) / hr - (y[i] - y[i - 1]) / hl) - hl * y2[i - 1];
-        cp[i] = hr / diag;
-        y2[i] = rhs / diag;
+        const double span = x[i + 1] - x[i - 1];
+        const double w = (x[i] - x[i - 1]) / span;
+        const double piv = w * y2[i - 1] + 2.0;
+        y2[i] = (w - 1.0) / piv;
+        const double dslope = (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]);
+        r[i] = (6.0 * dslope / span - w * r[i - 1]) / piv;
     }
-    y2[n - 1] = 0.0;
-    for (int i = n - 2; i >= 1; i--)
-        y2[i] -= cp[i] * y2[i + 1];
-    free(cp);
+    if (n > 1) y2[n - 1] = 0.0;
+    for (int i = n - 2; i >= 0; i--) y2[i] = y2[i] * y2[i + 1] + r[i];
+    free(r);
 }
 
 /* Cubic spline evaluation at t: locate the bracketing knots by bisection

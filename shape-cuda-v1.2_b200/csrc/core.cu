@@ -593,27 +593,30 @@ __device__ double view_logfactor(const FrameGeom &g, const FrameState &st)
     return log(xfactor * yfactor);
 }
 
-// Natural cubic spline second derivatives (tridiagonal system solved by
-// forward elimination / back substitution) and evaluation; the role of
-// spline/splint in src/shape/calc_fits.c:1923-1933.
-__device__ void spline_natural_dev(const double *x, const double *y, int n, double *y2, double *cp)
+// Natural cubic spline second derivatives and evaluation (the role of
+// spline/splint in src/shape/calc_fits.c:1923-1933). The tridiagonal system
+//   h[i-1] y2[i-1] + 2 (h[i-1] + h[i]) y2[i] + h[i] y2[i+1]
+//     = 6 ((y[i+1]-y[i])/h[i] - (y[i]-y[i-1])/h[i-1]),   y2[0] = y2[n-1] = 0,
+// is solved with each row divided by its span x[i+1] - x[i-1] (lower
+// coefficient w = h[i-1]/span, diagonal 2, upper 1 - w): forward
+// elimination keeps each row's multiplier of y2[i+1] in y2[i] and its
+// eliminated right-hand side in r[i], back substitution forms
+// y2[i] = y2[i] y2[i+1] + r[i]. The reference solves the span-scaled rows in
+// this order, so the FP64 fits are bit-identical to its.
+__device__ void spline_natural_dev(const double *x, const double *y, int n, double *y2, double *r)
 {
-    if (n < 3) {
-        for (int i = 0; i < n; i++) y2[i] = 0.0;
-        return;
-    }
-    y2[0] = 0.0;
-    cp[0] = 0.0;
+    if (n < 1) return;
+    y2[0] = r[0] = 0.0;
     for (int i = 1; i < n - 1; i++) {
-        double hl = x[i] - x[i - 1], hr = x[i + 1] - x[i];
-        double diag = 2.0 * (hl + hr) - hl * cp[i - 1];
-        double rhs = 6.0 * ((y[i + 1] - y[i]) / hr - (y[i] - y[i - 1]) / hl) - hl * y2[i - 1];
-        cp[i] = hr / diag;
-        y2[i] = rhs / diag;
+        const double span = x[i + 1] - x[i - 1];
+        const double w = (x[i] - x[i - 1]) / span;
+        const double piv = w * y2[i - 1] + 2.0;
+        y2[i] = (w - 1.0) / piv;
+        const double dslope = (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]);
+        r[i] = (6.0 * dslope / span - w * r[i - 1]) / piv;
     }
-    y2[n - 1] = 0.0;
-    for (int i = n - 2; i >= 1; i--)
-        y2[i] -= cp[i] * y2[i + 1];
+    if (n > 1) y2[n - 1] = 0.0;
+    for (int i = n - 2; i >= 0; i--) y2[i] = y2[i] * y2[i + 1] + r[i];
 }
 
 __device__ double splint_dev(const double *x, const double *y, const double *y2, int n, double t)

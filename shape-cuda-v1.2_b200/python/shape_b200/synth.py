@@ -490,11 +490,19 @@ def doppler_dataset(nframes=8, pos_range=(101, 301), ndop_range=(64, 256), synth
 
 
 def lightcurve_dataset(npoints=200, pos_range=(129, 257), synthesize=None, params=None,
-                       seed=7, set_index=0, radius=1.05, law_type=11):
+                       seed=7, set_index=0, radius=1.05, law_type=11, obs_between=False):
     """Config 3: one lightcurve of `npoints` points, solar phase uniform in
     5-60 deg, odd POS sides uniform in pos_range, Kaasalainen law with
     wt=0.3 (Lommel-Seeliger 0.7 + Lambert 0.3), A0=0, k=0; calc epochs equal
-    observation epochs; 1% Gaussian noise."""
+    observation epochs; 1% Gaussian noise.
+
+    obs_between: the npoints epochs are the calculated ones only, and the
+    npoints - 1 observation epochs lie strictly between consecutive calc
+    epochs (at 20-80 % of each gap), so every fit value is the natural
+    spline of the calculated brightnesses evaluated off its knots
+    (src/shape/calc_fits.c:1923-1933); the observed values are the
+    synthesized brightnesses interpolated linearly to those epochs, with the
+    same 1% noise."""
     params = params or eval_params()
     rng = np.random.default_rng(seed + 101 * set_index)
     pole = ecl_dir(30.0, 60.0)
@@ -517,20 +525,26 @@ def lightcurve_dataset(npoints=200, pos_range=(129, 257), synthesize=None, param
         cd.fill9(p.se, se)
         p.solar_phase = alpha
         pts.append(p)
+    x = t.copy()
+    if obs_between:
+        frac = np.random.default_rng(seed + 7 + 101 * set_index).uniform(0.2, 0.8, npoints - 1)
+        t = x[:-1] + frac * (x[1:] - x[:-1])
+    nobs = len(t)
     ls = cd.LghtcrvSet()
-    ls.ncalc = ls.n = npoints
-    ls.weight, ls.dof = 1.0, float(npoints)
+    ls.ncalc, ls.n = npoints, nobs
+    ls.weight, ls.dof = 1.0, float(nobs)
     ls.cal_floating, ls.cal = 1, 1.0
     law = cd.OpticalLaw()
     law.type, law.R, law.wt, law.A0, law.D, law.k = law_type, 1.0, 0.3, 0.0, 0.1, 0.0
     ls.law = law
-    x = t.copy()
-    obs = np.ones(npoints)
-    ds = LightcurveDataset(ls, pts, x, t.copy(), obs, np.ones(npoints))
+    obs = np.ones(nobs)
+    ds = LightcurveDataset(ls, pts, x, t.copy(), obs, np.ones(nobs))
     if synthesize is not None:
         y = np.asarray(synthesize(ds, params), dtype=np.float64)
+        if obs_between:
+            y = np.interp(t, x, y)
         nrng = np.random.default_rng(1234 + set_index)
-        ds.obs = y * (1.0 + 0.01 * nrng.standard_normal(npoints))
+        ds.obs = y * (1.0 + 0.01 * nrng.standard_normal(nobs))
         ds.oneovervar = 1.0 / (0.01 * ds.obs) ** 2
     ds.bind()
     return ds

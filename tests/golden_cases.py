@@ -70,6 +70,11 @@ LGHTCRV_CASES = {
                synth.eval_params(mask_tol=0.002)),
     "c3_short": (synth.harmonic_model, lambda s, p: synth.lightcurve_dataset(4, (129, 141), s, p, seed=7),
                  synth.eval_params(mask_tol=0.0)),
+    # observation epochs strictly between the calculated ones: the fit is
+    # the natural spline off its knots (NR spline / splint in the reference)
+    "kaasalainen_off_knots": (octa3_model,
+                              lambda s, p: synth.lightcurve_dataset(9, (41, 61), s, p, seed=13, obs_between=True),
+                              synth.eval_params(mask_tol=0.0)),
 }
 
 

@@ -257,3 +257,32 @@ def test_param_update_graph_replay(cuda_device):
         vals.append(a)
     assert len(set(vals)) == 3
     e.close()
+
+
+@pytest.mark.parametrize("form", [eng.FORM_PLAIN_FP64, eng.FORM_BATCHED_FP64, eng.FORM_BATCHED_FP32])
+def test_lightcurve_off_knots(cuda_device, form):
+    """Observation epochs strictly between the calculated ones (the golden
+    case kaasalainen_off_knots, pinned bit-exact to the reference's
+    calc_lghtcrv): every fit value is the natural spline off its knots.
+    FP64 forms: y and fit to rtol 1e-12, chi-square 1e-10 against the oracle;
+    FP32 form: per-point and chi-square error below 1e-6."""
+    import golden_cases as gc
+    model_fn, ds_fn, params = gc.LGHTCRV_CASES["kaasalainen_off_knots"]
+    m = model_fn()
+    o = cases.orc()
+    ds = ds_fn(lambda d, p: o.eval_lghtcrv(m, d, p)["y"], params)
+    assert ds.set.n == ds.set.ncalc - 1 and np.all((ds.t > ds.x[:-1]) & (ds.t < ds.x[1:]))
+    oo = o.eval_lghtcrv(m, ds, params)
+    e = eng.make_engine(m, params, lghtcrvs=[ds])
+    s = e.evaluate(form)
+    g = e.lghtcrv(0, ds)
+    if form == eng.FORM_BATCHED_FP32:
+        err = np.max(np.abs(g["fit"] - oo["fit"]) / np.abs(oo["fit"]))
+        print("FP32 off-knot worst per-point relative error %.3e" % err)
+        assert err < 1e-6
+        assert abs(s["chi2"] - oo["chi2"]) <= FP32_CHI2_RTOL * abs(oo["chi2"])
+    else:
+        np.testing.assert_allclose(g["y"], oo["y"], rtol=1e-12)
+        np.testing.assert_allclose(g["fit"], oo["fit"], rtol=1e-12)
+        assert abs(s["chi2"] - oo["chi2"]) <= CHI2_RTOL * abs(oo["chi2"])
+    e.close()

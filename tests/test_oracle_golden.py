@@ -141,18 +141,23 @@ def test_lightcurve_bit_exact(orc, name):
 
 
 def test_spline_matches_reference_off_knots(orc):
-    """Natural spline between knots against the closed form for a cubic
-    with zero end curvature is hard to pin; instead check the defining
-    properties: interpolation at knots and C2 continuity."""
-    x = np.linspace(0.0, 1.0, 9) ** 1.3
-    y = np.sin(3 * x) + x
-    t = np.concatenate([x, (x[:-1] + x[1:]) / 2])
-    fit = orc.spline_fit(x, y, t)
-    assert np.array_equal(fit[:len(x)], y)
-    h = 1e-6
-    for xi in x[1:-1]:
-        d2l = (orc.spline_fit(x, y, [xi - 2 * h])[0] - 2 * orc.spline_fit(x, y, [xi - h])[0]
-               + orc.spline_fit(x, y, [xi])[0]) / h ** 2
-        d2r = (orc.spline_fit(x, y, [xi])[0] - 2 * orc.spline_fit(x, y, [xi + h])[0]
-               + orc.spline_fit(x, y, [xi + 2 * h])[0]) / h ** 2
-        assert abs(d2l - d2r) < 1e-2 * (1 + abs(d2l))
+    """The oracle's natural cubic spline against the reference's own NR
+    spline/splint (compiled from the reference sources, oracle/_ref), bit
+    for bit, at the knots and strictly between them, on uneven knots. The
+    committed golden case kaasalainen_off_knots pins the same path inside
+    calc_lghtcrv without the reference tree."""
+    try:
+        from oracle.bindings import Reference
+        ref = Reference()
+    except RuntimeError:
+        pytest.skip("reference CPU build (oracle/_ref) not present")
+    rng = np.random.default_rng(3)
+    for n in (2, 3, 9, 40):
+        x = np.sort(rng.uniform(0.0, 1.0, n)) + 2458000.0
+        y = np.sin(7 * x) + rng.uniform(0.5, 1.5, n)
+        mids = x[:-1] + rng.uniform(0.05, 0.95, n - 1) * np.diff(x)
+        t = np.concatenate([x, mids])
+        got = orc.spline_fit(x, y, t)
+        want = ref.spline_eval(x, y, t)
+        assert np.array_equal(got, want), n
+        assert np.array_equal(got[:n], y)
