@@ -337,6 +337,78 @@ int shape_chi2_frames_noalloc(int device, int nframes, const long long *frame_of
                               const double *d_fit, const double *weight,
                               const int *cal_floating, const double *cal, double *out);
 
+/* ---- One plane-of-sky view per call, on the caller's host images ----
+ *
+ * The device forms of the reference's posvis, pos2deldop, posmask,
+ * apply_photo and posclr for callers that drive the plane of sky themselves
+ * (the write / view / map actions, multi-component models, binary systems),
+ * reached through the reference-signature wrappers of
+ * shape-cuda-v1.2_b200/dropin/shape_b200_pos.c. Images are the caller's
+ * host arrays of (2n+1)^2 elements in [i][j] order: element [i][j],
+ * i, j in [-n, n], at (i+n)*(2n+1) + (j+n). Each call uploads what it reads,
+ * runs on the device (FP64, the engine's kernels) and copies back what it
+ * writes; calls on one device run one at a time. */
+
+/* The plane-of-sky frame: struct pos_t's geometry (src/shape/shape2.h:1061-1094). */
+typedef struct shape_pos_view {
+    int n;                      /* pos->n */
+    double km_per_pixel;        /* pos->km_per_pixel */
+    double ae[9], oe[9], se[9]; /* pos->ae, pos->oe, pos->se (row-major) */
+    int bistatic;               /* pos->bistatic */
+} shape_pos_view;
+
+/* struct pos_t's images and limits; an operation reads or writes only the
+ * members it names, the others may be NULL. */
+typedef struct shape_pos_images {
+    double *b, *cose, *cosi, *z;    /* pos->b, cose, cosi, z */
+    int *body, *comp, *f;           /* pos->body, comp, f */
+    double *cosill, *zill;          /* sun view (bistatic) */
+    int *bodyill, *compill, *fill;
+    int xlim[2], ylim[2];           /* pos->xlim, ylim */
+    int xlim2[2], ylim2[2];         /* pos->xlim2, ylim2 */
+    double posbnd_logfactor;        /* pos->posbnd_logfactor */
+} shape_pos_images;
+
+/* posvis (src/shape/posvis.c:84-364; declared at src/shape/shape2.h:1503):
+ * one model component (x, vn: nv x 3 vertex positions and normals; fv, fn:
+ * nf x 3 facet corners and normals; body-fixed) seen from the observer
+ * (src = 0: z, cose, f, and cosi when bistatic) or from the sun (src = 1:
+ * zill, cosill, fill), accumulating over what the images hold: a pixel
+ * changes only where this component is nearer. Pixels it assigns get
+ * body and comp; xlim/ylim (xlim2/ylim2) widen as POSrect widens them;
+ * posbnd_logfactor is set. Returns outbnd (0 or 1) or a negative status. */
+int shape_posvis(int device, const shape_pos_view *view, shape_pos_images *img, int nv, const double *x,
+                 const double *vn, int nf, const int *fv, const double *fn, const double orbit_offset[3],
+                 int smooth, int src, int body, int comp);
+
+/* pos2deldop (src/shape/pos2deldop.c:176-581; src/shape/shape2.h:1495):
+ * adds the radar cross-section of every lit pixel of `body` within xlim /
+ * ylim to fit (ndel x ndop, delay-row major) for the frame's view (oe,
+ * spin, deloff, dopoff, COM and DC bins of `frame`; its km_per_pixel is
+ * the view's), sets res's delay / Doppler limits and badradar terms and
+ * *km2Hz (may be NULL). Returns badradar (0 or 1) or a negative status. */
+int shape_pos2deldop(int device, const shape_pos_view *view, const shape_pos_images *img,
+                     const shape_eval_params *par, const shape_deldop_set *set, const shape_deldop_frame *frame,
+                     double orbit_xoff, double orbit_yoff, double orbit_dopoff, int body, double *fit,
+                     shape_deldop_result *res, double *km2Hz);
+
+/* posmask (src/shape/posmask.c:58-174; src/shape/shape2.h:1502): zeroes
+ * cose where the sun view shows another facet, component or body nearer
+ * the sun than the pixel by more than tol (reads z, f, comp, body and the
+ * sun view's zill, fill, compill, bodyill). */
+int shape_posmask(int device, const shape_pos_view *view, shape_pos_images *img, double tol);
+
+/* apply_photo (src/shape/apply_photo.c:78-309; src/shape/shape2.h:1446)
+ * for the Lambert, Lommel-Seeliger and Kaasalainen laws: writes b for every
+ * lit pixel of `body` within xlim / ylim and *sum = their sum in the
+ * reference's order (TINY, 1e-40, when 0). */
+int shape_apply_photo(int device, const shape_optical_law *law, double phase, double intensityfactor,
+                      const shape_pos_view *view, shape_pos_images *img, int body, double *sum);
+
+/* posclr (src/shape/posclr.c:24-67; src/shape/shape2.h:1501): blank images
+ * and empty limits. Host only. */
+int shape_posclr(const shape_pos_view *view, shape_pos_images *img);
+
 /* Continuous-batching evaluation server (one device). It has no counterpart
  * in the reference, whose fits evaluate one model at a time in one process;
  * it serves many fits (workloads) from one GPU. A workload is the host

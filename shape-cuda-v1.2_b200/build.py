@@ -31,6 +31,7 @@ UNITS = [
     ("raster_f32.cu", []),
     ("engine.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
+    ("posview.cu", ["-fmad=false"]),
     ("fit.cu", ["-fmad=false"]),
     ("server.cu", ["-fmad=false"]),
     ("spin.cu", ["-fmad=false"]),
@@ -38,7 +39,7 @@ UNITS = [
     ("modfile.cu", []),
 ]
 
-HEADERS = ["engine_internal.h", "engine_impl.h", "kernels.h", "raster_impl.cuh"]
+HEADERS = ["engine_internal.h", "engine_impl.h", "kernels.h", "raster_impl.cuh", "posmask_dev.cuh"]
 
 
 def _newer(src_list, target):

@@ -12,6 +12,7 @@
 #include <climits>
 
 #include "kernels.h"
+#include "posmask_dev.cuh"
 
 namespace shape {
 
@@ -111,7 +112,7 @@ __device__ inline void store_vt(double4 *vt, int i, double x, double y, double z
 }
 
 // Vertex coordinates in each view's frame: cotrans(v, oa, x, 1) then
-// += orbit_offset (= 0.0) (src/shape/posvis.c:159-166).
+// += orbit_offset (src/shape/posvis.c:159-166; 0.0 for the engine's views).
 template <typename T4>
 __global__ void k_xform(const FrameGeom *__restrict__ geoms, const double4 *__restrict__ vx, int nv,
                         T4 *__restrict__ vt)
@@ -128,7 +129,7 @@ __global__ void k_xform(const FrameGeom *__restrict__ geoms, const double4 *__re
         t[r] += g.oa[3 * r + 0] * x.x;
         t[r] += g.oa[3 * r + 1] * x.y;
         t[r] += g.oa[3 * r + 2] * x.z;
-        t[r] += 0.0;
+        t[r] += g.off[r];
     }
     store_vt(vt, g.vt_base + i, t[0], t[1], t[2]);
 }
@@ -153,7 +154,7 @@ __global__ void k_xform_realize(const FrameGeom *__restrict__ geoms, const doubl
         t[k] += g.oa[3 * k + 0] * x.x;
         t[k] += g.oa[3 * k + 1] * x.y;
         t[k] += g.oa[3 * k + 2] * x.z;
-        t[k] += 0.0;
+        t[k] += g.off[k];
     }
     store_vt(vt, g.vt_base + i, t[0], t[1], t[2]);
 }
@@ -469,8 +470,6 @@ __global__ void k_doppler_overflow(DopOvfArgs a)
 
 // ------------------------------------------------------------ lightcurves
 
-__device__ inline int iround_(double x) { return (x < 0.0) ? (int)(x - 0.5) : (int)(x + 0.5); }
-
 // posmask (src/shape/posmask.c:58-174) and apply_photo
 // (src/shape/apply_photo.c:85-133, 226-248) per POS pixel of one
 // lightcurve point; brightness summed per work item (fixed order within a
@@ -514,35 +513,7 @@ __global__ void k_lc_photo(LcArgs a)
 #define ZILL(a_, b_) ((double)ZI[(long long)((a_) + n) * side + ((b_) + n)])
             if (fabs(i0) < n && fabs(j0) < n && ZILL(im, jm) > -bignum &&
                 F[p] != FI[(long long)(im + n) * side + (jm + n)]) {
-                int i1 = (int)floor(i0), j1 = (int)floor(j0);
-                double zill;
-                if (ZILL(i1, j1) > -bignum && ZILL(i1 + 1, j1) > -bignum &&
-                    ZILL(i1, j1 + 1) > -bignum && ZILL(i1 + 1, j1 + 1) > -bignum) {
-                    double t = i0 - i1, u = j0 - j1;
-                    zill = (1 - t) * (1 - u) * ZILL(i1, j1) + t * (1 - u) * ZILL(i1 + 1, j1)
-                           + t * u * ZILL(i1 + 1, j1 + 1) + (1 - t) * u * ZILL(i1, j1 + 1);
-                } else {
-                    zill = ZILL(im, jm);
-                    int i_sign = (i0 >= im) ? 1 : -1;
-                    int i2 = im + i_sign;
-                    if (abs(i2) <= n && ZILL(i2, jm) > -bignum) {
-                        zill += fabs(i0 - im) * (ZILL(i2, jm) - ZILL(im, jm));
-                    } else {
-                        i2 = im - i_sign;
-                        if (abs(i2) <= n && ZILL(i2, jm) > -bignum)
-                            zill -= fabs(i0 - im) * (ZILL(i2, jm) - ZILL(im, jm));
-                    }
-                    int j_sign = (j0 >= jm) ? 1 : -1;
-                    int j2 = jm + j_sign;
-                    if (abs(j2) <= n && ZILL(im, j2) > -bignum) {
-                        zill += fabs(j0 - jm) * (ZILL(im, j2) - ZILL(im, jm));
-                    } else {
-                        j2 = jm - j_sign;
-                        if (abs(j2) <= n && ZILL(im, j2) > -bignum)
-                            zill -= fabs(j0 - jm) * (ZILL(im, j2) - ZILL(im, jm));
-                    }
-                }
-                if (zill - x[2] > P.mask_tol) {
+                if (posmask_zill(ZI, n, side, i0, j0, im, jm) - x[2] > P.mask_tol) {
                     cose = 0.0;
                     CE[p] = (T)0;
                 }

@@ -41,7 +41,7 @@ int report_error(int code, const std::string &msg) { return set_err(code, msg); 
     } while (0)
 
 // y = A x with A row-major (cotrans dir=1, src/util/cotrans.c)
-static void mv(double y[3], const double *A, const double x[3])
+void mv(double y[3], const double *A, const double x[3])
 {
     double t[3];
     for (int i = 0; i < 3; i++) {
@@ -51,7 +51,7 @@ static void mv(double y[3], const double *A, const double x[3])
     y[0] = t[0]; y[1] = t[1]; y[2] = t[2];
 }
 // y = A^T x (cotrans dir=-1)
-static void mtv(double y[3], const double *A, const double x[3])
+void mtv(double y[3], const double *A, const double x[3])
 {
     double t[3];
     for (int i = 0; i < 3; i++) {
@@ -61,7 +61,7 @@ static void mtv(double y[3], const double *A, const double x[3])
     y[0] = t[0]; y[1] = t[1]; y[2] = t[2];
 }
 // M = B * A^T (mtrnsps + mmmul as in src/shape/posvis.c:101-122)
-static void mul_bt(double *M, const double *B, const double *A)
+void mul_bt(double *M, const double *B, const double *A)
 {
     double t[9];
     for (int i = 0; i < 3; i++)
@@ -81,14 +81,42 @@ static int radar_law_index(EngineImpl &E, const shape_radar_law &L)
     return (int)E.laws.size() - 1;
 }
 
+// Set-level constants of pos2deldop for a radar view
+// (src/shape/pos2deldop.c:201-240): the code method's delay response
+// extents, the delay scale, the sinc^2 sampling and the law index. A Doppler
+// frame is a single row: delPOS = z*0 + 1 = 1 exactly, so its delay response
+// tri2(0) is 1 and its weights are pos2doppler's.
+void radar_set_consts(FrameGeom &g, const shape_deldop_set &S, const shape_eval_params &P, int law, int doppler)
+{
+    g.codemethod = S.codemethod;
+    g.spb = S.spb;
+    g.stride = S.stride;
+    g.spb_over_stride = S.spb / S.stride;
+    g.one_over_spb = 1.0 / S.spb;
+    g.spb_sq = S.spb * S.spb;
+    if (S.codemethod != SHAPE_CODE_LONG_ORIG) {
+        g.const1 = (3 * S.spb - 1) / (2.0 * S.stride);
+        g.const2 = (S.spb - 1) / (2.0 * S.stride);
+    } else {
+        g.const1 = (double)g.spb_over_stride;
+        g.const2 = 0.0;
+    }
+    g.delfact = doppler ? 0.0 : -SHAPE_KM2US / S.del_per_pixel;
+    g.nsinc2 = P.nsinc2;
+    g.nsinc2_sq = P.nsinc2 * P.nsinc2;
+    g.sinc2width = P.sinc2width;
+    g.dopfftlen = S.dopfftlen;
+    g.law = law;
+}
+
 // View-dependent constants of radar frame F (src/shape/pos2deldop.c:218-275,
 // src/shape/posvis.c:101-122): the observer <- body matrix, the Doppler
 // axes and footprint extents, the delay and Doppler shifts and a Doppler
 // spectrum's overflow origin; dx = the Doppler extent term of the frame's
 // bin limits; the badradar flag and log-factor of a footprint wider than
 // MAXBINS. g.nsinc2, g.sinc2width and g.dop1d must be set.
-static void radar_view_geom(FrameGeom &g, FrameHost &h, double &dx, const shape_deldop_frame &F,
-                            const shape_deldop_set &S)
+void radar_view_geom(FrameGeom &g, FrameHost &h, double &dx, const shape_deldop_frame &F,
+                     const shape_deldop_set &S)
 {
     mul_bt(g.oa, F.oe, F.ae);
     double w[3];
@@ -199,27 +227,7 @@ int EngineImpl::finalize()
             g.ndel = F.ndel;
             g.ndop = F.ndop;
             g.fit_base = frame_off[fi];
-            g.codemethod = S.codemethod;
-            g.spb = S.spb;
-            g.stride = S.stride;
-            g.spb_over_stride = S.spb / S.stride;
-            g.one_over_spb = 1.0 / S.spb;
-            g.spb_sq = S.spb * S.spb;
-            if (S.codemethod != SHAPE_CODE_LONG_ORIG) {
-                g.const1 = (3 * S.spb - 1) / (2.0 * S.stride);
-                g.const2 = (S.spb - 1) / (2.0 * S.stride);
-            } else {
-                g.const1 = (double)g.spb_over_stride;
-                g.const2 = 0.0;
-            }
-            // a Doppler frame's single row: delPOS = z*0 + 1 = 1 exactly, so its
-            // delay response tri2(0) is 1 and its weights are pos2doppler's
-            g.delfact = dd[s].doppler ? 0.0 : -SHAPE_KM2US / S.del_per_pixel;
-            g.nsinc2 = params.nsinc2;
-            g.nsinc2_sq = params.nsinc2 * params.nsinc2;
-            g.sinc2width = params.sinc2width;
-            g.dopfftlen = S.dopfftlen;
-            g.law = law;
+            radar_set_consts(g, S, params, law, dd[s].doppler);
             g.frame_index = fi;
             g.dop1d = dd[s].doppler;
             if (g.dop1d) g.ovf_base = (long long)dop_frames.size() * DOP_MAXOVERFLOW;

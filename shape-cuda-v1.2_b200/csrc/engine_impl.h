@@ -17,6 +17,16 @@ namespace shape {
 
 int report_error(int code, const std::string &msg);   // engine.cu
 
+// Host geometry shared by the engine and the one-view operations
+// (engine.cu, FP64 in the reference's operation order): y = A x, y = A^T x,
+// M = B A^T, and a radar view's set- and view-level pos2deldop constants.
+void mv(double y[3], const double *A, const double x[3]);
+void mtv(double y[3], const double *A, const double x[3]);
+void mul_bt(double *M, const double *B, const double *A);
+void radar_set_consts(FrameGeom &g, const shape_deldop_set &S, const shape_eval_params &P, int law, int doppler);
+void radar_view_geom(FrameGeom &g, FrameHost &h, double &dx, const shape_deldop_frame &F,
+                     const shape_deldop_set &S);
+
 struct DevMem {
     std::vector<void *> ptrs;
     std::vector<size_t> sizes;

@@ -32,10 +32,12 @@ constexpr int DOP_MAXOVERFLOW = 2000;   // Doppler overflow spectrum bins (MAXOV
 constexpr int VIEW_RADAR = 0;       // delay-Doppler frame, observer view
 constexpr int VIEW_LC_OBS = 1;      // lightcurve point, observer view (bistatic)
 constexpr int VIEW_LC_SUN = 2;      // lightcurve point, sun view (src = 1)
+constexpr int VIEW_POS = 3;         // a plane-of-sky view of its own (monostatic observer view, no synthesis)
 
 struct FrameGeom {
     double oa[9];        // observer(or sun) <- body, row-major, reference op order
     double usrc[3];      // sun direction in observer coords (VIEW_LC_OBS)
+    double off[3];       // orbit offset added to the view-frame vertices (posvis's orbit_offset; 0 here otherwise)
     double kmpp;
     int n, side;         // POS half width, 2n+1
     int tiles_x;         // tiles per POS side

@@ -72,6 +72,12 @@ struct RasterArgs {
     int keep_pos;
     double *ovf;               // Doppler overflow spectra (DOP_MAXOVERFLOW per Doppler frame)
     size_t smem_bytes;         // dynamic shared memory of the raster CTA (set by the launcher)
+    // FP64 raster of a single view into images that already hold earlier
+    // calls' results (posvis accumulating over model components): each pixel
+    // starts from its z / facet / cos(e) / cos(i), and won[p] is set to 1
+    // where this launch assigned pixel p. 0 for the engine's evaluations.
+    int accumulate;
+    unsigned char *won;
 };
 
 // core.cu (FP64, no FMA contraction)

@@ -858,6 +858,17 @@ k_raster(RasterArgs a)
         const T x1 = (sizeof(T) == 8) ? (T)pj * (T)g.kmpp : (T)((double)lj * g.kmpp);
         T zz = (T)(-SHAPE_HUGENUMBER), cosa = 0, cosb = 0;
         int fac = -1;
+        if constexpr (sizeof(T) == 8) {
+            // a single view accumulating over earlier calls (posvis over
+            // model components): the pixel starts from what the images hold
+            if (a.accumulate && inframe) {
+                const long long p = g.pos_base + (long long)(pi + n) * g.side + (pj + n);
+                zz = static_cast<const double *>(a.pos_z)[p];
+                fac = a.pos_f[p];
+                cosa = static_cast<const T *>(a.pos_cose)[p];
+                if (g.kind != VIEW_LC_SUN) cosb = static_cast<const T *>(a.pos_cosi)[p];
+            }
+        }
         T zze = 0;       // FP32 form: the winner's depth error bound
         bool amb = false;   // FP32 form: a decision within FP32 error (pixel_posvis64 redoes it)
         bool good = false;
@@ -1089,7 +1100,7 @@ k_raster(RasterArgs a)
         }
 
         // ---- outputs of this tile
-        const bool covered = inframe && fac >= 0;
+        bool covered = inframe && fac >= 0;
         // FP64 depth. FP32 form: a radar pixel keeps its FP32 depth (about
         // 1e-7 km, 1e-5 of a delay bin); a lightcurve view recomputes the
         // winning facet's depth in FP64 (facet_depth64), because posmask's
@@ -1107,6 +1118,15 @@ k_raster(RasterArgs a)
             long long p = g.pos_base + (long long)(pi + n) * g.side + (pj + n);
             double *Z = static_cast<double *>(a.pos_z);
             T *CE = static_cast<T *>(a.pos_cose), *CI = static_cast<T *>(a.pos_cosi);
+            if constexpr (sizeof(T) == 8) {
+                if (a.accumulate) {
+                    // assigned by this launch: a win always changes the facet
+                    // (the pixel was blank) or raises the depth
+                    const bool won = (Z[p] != z64) || (a.pos_f[p] != fac);
+                    a.won[p] = won ? 1 : 0;
+                    covered = won;
+                }
+            }
             Z[p] = z64;
             a.pos_f[p] = fac;
             CE[p] = cosa;                        // cos(e), or cos(i) in the sun view (pos->cosill)

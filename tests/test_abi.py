@@ -73,6 +73,7 @@ def test_dropin_compiles_against_reference_headers(tmp_path):
                     os.path.join(repo, "oracle", "refshim", "shape"), "-I-",
                     "-I" + os.path.join(repo, "oracle", "refshim", "shape")] + inc +
                    ["-I/usr/local/cuda/include", "-I" + os.path.join(repo, "include"),
+                    "-I" + os.path.join(repo, "shape-cuda-v1.2_b200", "dropin"),
                     os.path.join(repo, "shape-cuda-v1.2_b200", "dropin", "shape_b200_dropin.c"), "-o", obj],
                    check=True)
     syms = subprocess.run(["nm", "-g", "--defined-only", obj], capture_output=True, text=True,
