@@ -415,14 +415,24 @@ int shape_posclr(const shape_pos_view *view, shape_pos_images *img);
  * description of a configured engine (model, switches, datasets), copied at
  * registration. The server keeps device-resident instances of workloads, at
  * most hbm_budget_bytes of device memory in total, and runs up to max_slots
- * requests at once, each on its instance's stream. shape_server_run replays
- * a request trace: each request is admitted, in arrival order, once its
- * arrival time (seconds after the call starts) has passed, a slot is free
- * and an idle instance of its workload exists or fits in the budget (idle
- * instances of other workloads are evicted, least recently used first, to
- * make room). A request evaluates its workload at its own scale factors;
- * its result is the same as a lone shape_engine_evaluate of that workload at
- * those scale factors. */
+ * requests at once, each on its instance's stream. A scheduler thread
+ * serves the requests: it admits every waiting request it can, oldest
+ * first, to an idle instance of its workload or to a new one when the
+ * budget allows (idle instances of other workloads are evicted, least
+ * recently used first, to make room); a request that cannot start does not
+ * hold up those behind it, unless it has waited more than 20 ms, after
+ * which later requests only get instances that already exist. A request
+ * evaluates its workload at its own scale factors; its result is the same
+ * as a lone shape_engine_evaluate of that workload at those scale factors.
+ *
+ * Online use: shape_server_start, then shape_server_submit as requests
+ * arrive (any thread) and shape_server_poll / shape_server_wait for their
+ * results; shape_server_stats_get covers the requests since start;
+ * shape_server_stop finishes what was submitted and ends the thread.
+ * shape_server_run replays a whole trace through the same scheduler: each
+ * request is submitted at its arrival time (seconds after the call starts)
+ * and its latency counts from then; its requests leave the ticket table
+ * when it returns. */
 typedef struct shape_server shape_server;
 typedef struct shape_request {
     int workload;              /* index returned by shape_server_add_workload */
@@ -646,6 +656,23 @@ int shape_server_add_workload(shape_server *s, shape_engine *engine, int form);
 int shape_server_workload_bytes(shape_server *s, int w, size_t *bytes);
 int shape_server_run(shape_server *s, const shape_request *req, int n, shape_request_result *res,
                      shape_server_stats *stats);
+/* Starts the scheduler thread (and a statistics window). */
+int shape_server_start(shape_server *s);
+/* Queues one request of workload w at scale factors scale[3] (NULL: 1, 1,
+ * 1); *ticket identifies it. Its arrival time is the time of the call. */
+int shape_server_submit(shape_server *s, int w, const double scale[3], long long *ticket);
+/* 1 and *res when the request is done, 0 while it is not (poll), or a
+ * negative status; shape_server_wait waits up to timeout_s seconds and
+ * returns SHAPE_E_TIMEOUT if it is still not done. Result times are
+ * seconds on the server's clock (since shape_server_create). After a
+ * device failure every open request reports the failure's status. */
+int shape_server_poll(shape_server *s, long long ticket, shape_request_result *res);
+int shape_server_wait(shape_server *s, long long ticket, double timeout_s, shape_request_result *res);
+/* Throughput and latency percentiles of the requests completed since
+ * shape_server_start. */
+int shape_server_stats_get(shape_server *s, shape_server_stats *stats);
+/* Completes every submitted request, then ends the scheduler thread. */
+int shape_server_stop(shape_server *s);
 
 #ifdef __cplusplus
 }

@@ -176,6 +176,12 @@ def load_library(path=LIB_PATH):
     L.shape_server_add_workload.argtypes = [vp, vp, C.c_int]
     L.shape_server_workload_bytes.argtypes = [vp, C.c_int, P(C.c_size_t)]
     L.shape_server_run.argtypes = [vp, P(Request), C.c_int, P(RequestResult), P(ServerStats)]
+    L.shape_server_start.argtypes = [vp]
+    L.shape_server_submit.argtypes = [vp, C.c_int, cd.dptr, P(C.c_longlong)]
+    L.shape_server_poll.argtypes = [vp, C.c_longlong, P(RequestResult)]
+    L.shape_server_wait.argtypes = [vp, C.c_longlong, C.c_double, P(RequestResult)]
+    L.shape_server_stats_get.argtypes = [vp, P(ServerStats)]
+    L.shape_server_stop.argtypes = [vp]
     _lib = L
     return L
 
@@ -773,6 +779,37 @@ class Server:
         _chk(self.L.shape_server_run(self.h, req, n, res, C.byref(st)))
         out = [{k: getattr(r, k) for k, _ in RequestResult._fields_} for r in res]
         return out, {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    # online use: requests submitted as they arrive, results collected later
+    def start(self):
+        _chk(self.L.shape_server_start(self.h))
+
+    def submit(self, workload, scale=(1.0, 1.0, 1.0)):
+        """Queues one request; returns its ticket."""
+        t = C.c_longlong()
+        sc = np.ascontiguousarray(scale, dtype=np.float64)
+        _chk(self.L.shape_server_submit(self.h, workload, cd.as_dptr(sc), C.byref(t)))
+        return t.value
+
+    def poll(self, ticket):
+        """The result dict of a finished request, or None while it runs."""
+        r = RequestResult()
+        if _chk(self.L.shape_server_poll(self.h, ticket, C.byref(r))) == 0:
+            return None
+        return {k: getattr(r, k) for k, _ in RequestResult._fields_}
+
+    def wait(self, ticket, timeout_s=60.0):
+        r = RequestResult()
+        _chk(self.L.shape_server_wait(self.h, ticket, float(timeout_s), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in RequestResult._fields_}
+
+    def stats(self):
+        st = ServerStats()
+        _chk(self.L.shape_server_stats_get(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def stop(self):
+        _chk(self.L.shape_server_stop(self.h))
 
 
 PARAM_OBJECTIVE = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int),

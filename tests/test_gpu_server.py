@@ -79,3 +79,65 @@ def test_budget_evictions_keep_results(cuda_device):
     assert st["peak_hbm_bytes"] <= budget
     _check(engines, trace, res)
     srv.close()
+
+
+def test_online_submit_poll(cuda_device):
+    """Online use: requests submitted from two threads while others run,
+    results collected by polling and waiting; each equals a lone evaluation.
+    """
+    import threading
+    import time
+    engines = _workloads()
+    srv = eng.Server(device=0, hbm_budget_bytes=8 << 30, max_slots=4)
+    for e, form in engines:
+        srv.add_workload(e, form)
+    srv.start()
+    trace = eng.poisson_trace(48, 1500.0, len(engines), seed=9)
+    tickets = [None] * len(trace)
+
+    def submitter(lo, hi):
+        for i in range(lo, hi):
+            w, _, sc = trace[i]
+            tickets[i] = srv.submit(w, sc)
+            time.sleep(0.0005)
+    th = [threading.Thread(target=submitter, args=(0, 24)), threading.Thread(target=submitter, args=(24, 48))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    res = []
+    for i, tk in enumerate(tickets):
+        r = srv.poll(tk) if i % 2 else None
+        res.append(r if r is not None else srv.wait(tk, 60.0))
+    st = srv.stats()
+    srv.stop()
+    assert st["requests_per_s"] > 0 and st["p99_latency_s"] >= st["p50_latency_s"] > 0.0
+    _check(engines, trace, res)
+    with pytest.raises(eng.EngineError):
+        srv.submit(0)                      # stopped: no scheduler to serve it
+    srv.close()
+
+
+def test_no_head_of_line_blocking(cuda_device):
+    """A request that cannot be admitted (its workload's instance is busy
+    and the budget has no room for a second one) does not hold up a later
+    request of a workload with an idle instance."""
+    m2, p2, d2 = cases.c2(64)
+    m1, p1, d1 = cases.c1()
+    big = eng.make_engine(m2, p2, deldops=[d2])
+    small = eng.make_engine(m1, p1, deldops=[d1])
+    probe = eng.Server(device=0, hbm_budget_bytes=8 << 30, max_slots=4)
+    wb = probe.add_workload(big, eng.FORM_BATCHED_FP64)
+    ws = probe.add_workload(small, eng.FORM_PLAIN_FP64)
+    need_big, need_small = probe.workload_bytes(wb), probe.workload_bytes(ws)
+    probe.close()
+    # one instance of each fits, a second instance of the big workload does not
+    srv = eng.Server(device=0, hbm_budget_bytes=need_big + need_small + need_small // 2, max_slots=4)
+    srv.add_workload(big, eng.FORM_BATCHED_FP64)
+    srv.add_workload(small, eng.FORM_PLAIN_FP64)
+    trace = [(0, 0.0, (1.0, 1.0, 1.0)), (0, 0.0, (1.01, 1.0, 1.0)), (1, 0.0, (1.0, 1.0, 1.0))]
+    res, st = srv.run(trace)
+    # the small request started before the second big one
+    assert res[2]["t_start"] < res[1]["t_start"], [r["t_start"] for r in res]
+    _check([(big, eng.FORM_BATCHED_FP64), (small, eng.FORM_PLAIN_FP64)], trace, res)
+    srv.close()
