@@ -153,12 +153,14 @@ int shape_engine_stage_times(shape_engine *e, int form, double *ms, int max);
  * fullest tile); tiles whose bin overflows are rasterized by an ordered scan
  * of all facets, which is exact but slow. Takes effect at the next finalize. */
 int shape_engine_set_bin_capacity(shape_engine *e, int cap);
-/* Batched FP32 form, radar views: 0 (default) tests coverage and depth
- * order in FP32 (a pixel within FP32 error of a facet edge or of a depth tie
- * may take another facet than the FP64 form; lightcurve views are always
- * exact); 1 redoes such pixels by the FP64 form's rules and takes FP64
- * depths on radar views too, so every view's facet and depth maps are the
- * FP64 form's (slower raster). Takes effect at the next evaluation. */
+/* Batched FP32 form, radar views: 1 (default) redoes every pixel whose
+ * coverage or depth-order decision lies within FP32 error by the FP64
+ * form's rules, so facet maps are the FP64 form's (kept POS maps also get
+ * the FP64 form's depths); 0 takes the FP32 decisions as they are (a pixel
+ * within FP32 error of a facet edge or of a depth tie may take another
+ * facet than the FP64 form: a faster raster, and a small frame's
+ * chi-square may move by ~1e-4 when that happens). Lightcurve views are
+ * always exact. Takes effect at the next evaluation. */
 int shape_engine_set_fp32_exact(shape_engine *e, int exact);
 
 /* A new view for radar frame global_frame (delay-Doppler and Doppler frames

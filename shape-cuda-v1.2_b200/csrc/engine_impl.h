@@ -257,7 +257,7 @@ struct EngineImpl {
     // (nonempty_lc non-empty at tuning)
     int work_radar = 0, nonempty_radar = 0, nonempty_lc = 0;
     int fixed_cap = 0;            // > 0: bin capacity set by the caller, no autotuning
-    int fp32_exact = 0;           // batched FP32: radar views by the exact raster variant too
+    int fp32_exact = 1;           // batched FP32: radar views by the exact raster variant too
     int evaluate(int form, shape_eval_summary *out);
     int kernels_per_eval(int form) const;
     void fill_params(double *dst) const

@@ -34,9 +34,6 @@
 #ifndef RASTER_MIN_BLOCKS_F64
 #define RASTER_MIN_BLOCKS_F64 4
 #endif
-#ifndef RASTER_RADAR_Z64
-#define RASTER_RADAR_Z64 1
-#endif
 #ifndef RASTER_RARE_NOINLINE
 #define RASTER_RARE_NOINLINE 0
 #endif
@@ -151,7 +148,7 @@ template <typename T> __device__ T radlaw_dev(const RadarLawDev &L, T c)
 // as linear functions of the pixel centre's offset (dx, dy) from that
 // corner (tile-relative coordinates): s = a1 dx + a2 dy, t = b1 dx + b2 dy,
 // zr = c1 dx + c2 dy, with p0 = (v00, v01, a1, a2), p1 = (b1, b2, c1, c2),
-// p2 = (0, v02, nx, ny).
+// p2 = (v02 lo, v02 hi, nx, ny), v02 = hi + lo to about 2^-48 of itself.
 template <typename T>
 struct Stage {
     typename Vec4<T>::type p0, p1, p2;
@@ -232,8 +229,10 @@ __device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage
         const double c1 = Ez * a1 + Fz * b1, c2 = Ez * a2 + Fz * b2;
         s.p0 = vec4<T>((T)V0, (T)V1, (T)a1, (T)a2);
         s.p1 = vec4<T>((T)b1, (T)b2, (T)c1, (T)c2);
-        E = (T)0;        // p2 = (0, v02, nx, ny)
+        // p2 = (v02 lo, v02 hi, nx, ny): the corner depth as a float pair,
+        // the rounded value and its rounding error
         F = (T)p0.z;
+        E = (T)(p0.z - (double)F);
         // Bounds on the FP32 values' error at any pixel centre of the tile
         // (x, y in [0, 16 kmpp)): 8 units of 2^-24 of the terms' magnitudes
         // (the offsets' rounding, the rounded coefficients, a product and a
@@ -739,9 +738,9 @@ __device__ inline double facet_depth64(const double4 *vt, int4 c, double x0, dou
 // and order-dependent smoothed normal), over the tile's bin in facet order.
 // ids: the bin's (facet, packed tile bbox) entries, sorted; (li, lj): the
 // pixel in the tile; (x0, y0): its centre. Returns the winner's facet
-// (-1: none) and writes its FP32 depth and the cos(e) state.
+// (-1: none) and writes its FP64 depth and the cos(e) state.
 static __device__ RARE_FN int pixel_posvis64(const RasterArgs &a, const FrameGeom &g, const int2 *ids,
-                                                  int count, int li, int lj, double x0, double y0, float *zz,
+                                                  int count, int li, int lj, double x0, double y0, double *zz,
                                                   bool *good, float *gm)
 {
     const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
@@ -791,7 +790,7 @@ static __device__ RARE_FN int pixel_posvis64(const RasterArgs &a, const FrameGeo
             *good = true; gm[0] = (float)nn[0]; gm[1] = (float)nn[1]; gm[2] = (float)nn[2];
         }
     }
-    *zz = (float)zw;
+    *zz = zw;
     return fac;
 }
 
@@ -870,6 +869,7 @@ k_raster(RasterArgs a)
             }
         }
         T zze = 0;       // FP32 form: the winner's depth error bound
+        T zlo = 0;       // FP32 form: the winner's depth is zz + zlo (two floats)
         bool amb = false;   // FP32 form: a decision within FP32 error (pixel_posvis64 redoes it)
         bool good = false;
         T gm0 = 0, gm1 = 0, gm2 = 0;
@@ -930,6 +930,13 @@ k_raster(RasterArgs a)
             const auto p2 = s.p2;
             zz = z;
             fac = s.f;
+            if constexpr (sizeof(T) == 4) {
+                // the depth as a float pair: the rounding error of v02 hi + zr
+                // (two-sum) plus v02's low part, so radar views get their
+                // depth to a few 1e-9 km without an FP64 recomputation
+                const float bv = z - p2.y;
+                zlo = ((p2.y - (z - bv)) + (zr - bv)) + p2.x;
+            }
             // cos(e) changes only when the smoothed normal faces the viewer
             // (posvis.c:265). Its sign is that of the view-z component before
             // normalization, so a win records the body-frame interpolated
@@ -1066,9 +1073,12 @@ k_raster(RasterArgs a)
         if constexpr (sizeof(T) == 4 && EXACT) {
             if (amb && count > 0 && count <= a.cap) {
                 float gmv[3] = {0.0f, 0.0f, 0.0f};
+                double zw;
                 good = false;
-                fac = pixel_posvis64(a, g, ids, count, li, lj, (double)pi * g.kmpp, (double)pj * g.kmpp, &zz,
+                fac = pixel_posvis64(a, g, ids, count, li, lj, (double)pi * g.kmpp, (double)pj * g.kmpp, &zw,
                                      &good, gmv);
+                zz = (float)zw;
+                zlo = (float)(zw - (double)zz);
                 gm0 = gmv[0]; gm1 = gmv[1]; gm2 = gmv[2];
             }
         }
@@ -1101,17 +1111,21 @@ k_raster(RasterArgs a)
 
         // ---- outputs of this tile
         bool covered = inframe && fac >= 0;
-        // FP64 depth. FP32 form: a radar pixel keeps its FP32 depth (about
-        // 1e-7 km, 1e-5 of a delay bin); a lightcurve view recomputes the
-        // winning facet's depth in FP64 (facet_depth64), because posmask's
-        // shadow test compares it with the sun view's to a few 1e-8 km.
+        // FP64 depth. FP32 form: a radar pixel takes its float-pair depth
+        // (a few 1e-9 km, 1e-7 of a delay bin); a lightcurve view, and an
+        // exact radar view whose maps are kept, recompute the winning facet's
+        // depth in FP64 with the FP64 form's operations (facet_depth64),
+        // because posmask's shadow test compares it with the sun view's to a
+        // few 1e-8 km and the kept maps are the FP64 form's.
         double z64 = (double)zz;
         if constexpr (sizeof(T) == 4) {
             if (fac < 0) {
                 z64 = -SHAPE_HUGENUMBER;
-            } else if ((EXACT && (RASTER_RADAR_Z64 || writes_pos)) || g.kind != VIEW_RADAR) {
+            } else if (g.kind != VIEW_RADAR || (EXACT && writes_pos)) {
                 const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
                 z64 = facet_depth64(vt, a.fvi[fac], (double)pi * g.kmpp, (double)pj * g.kmpp);
+            } else {
+                z64 = (double)zz + (double)zlo;
             }
         }
         if (inframe && writes_pos) {

@@ -280,8 +280,9 @@ class Engine:
         _chk(self.L.shape_engine_set_bin_capacity(self.h, int(cap)))
 
     def set_fp32_exact(self, exact=True):
-        """Batched FP32 form: radar views by the exact raster variant too
-        (facet and depth maps equal to the FP64 form's; slower raster)."""
+        """Batched FP32 form, radar views: True (the default) redoes pixels
+        whose decisions lie within FP32 error by the FP64 rules; False keeps
+        the FP32 decisions (faster raster)."""
         _chk(self.L.shape_engine_set_fp32_exact(self.h, 1 if exact else 0))
 
     def set_frame_view(self, frame, ae, oe, spin, deloff=0.0, dopoff=0.0):
