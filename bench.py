@@ -421,6 +421,75 @@ def sweep_cpu(model, dds, params, k=5):
             "kind": "reference", "sample": "first %d parameters of the sweep: %d trials" % (k, count[0])}
 
 
+def per_config(lrank, flush, budget_cpu_s=3.0):
+    """Configs 1 and 3 (one evaluation per step) and config 4 (a short
+    vertex sweep, each trial a graph replay) beside the config-2 headline:
+    batched FP32 frame-evals/s (CUDA events, L2 flushed before each step),
+    the raster kernel's roofline fraction, the FP32 form's worst
+    delta-chi2/chi2 against the FP64 form over jittered trials, and the
+    reference CPU code's rate on a bounded sample of the same workload."""
+    import torch
+    from shape_b200 import engine as eng
+    peak, _ = peak_hbm()
+    out = {}
+    dd_syn = lambda m: eng.engine_synthesizer(m, lrank)[0]
+    lc_syn = lambda m: eng.engine_synthesizer(m, lrank)[1]
+    for name, steps in (("c1", 200), ("c3", 20), ("c4", 40)):
+        params = synth.eval_params()
+        model, dds, lcs, desc = workload(name, dd_syn, lc_syn, params)
+        nu = units(dds, lcs)
+        E = eng.make_engine(model, params, deldops=dds, lghtcrvs=lcs, device=lrank)
+        rng = np.random.default_rng(17)
+        worst = 0.0
+        for k in range(4):
+            sc = [1.0, 1.0, 1.0] if k == 0 else list(1.0 + 0.02 * rng.uniform(-1, 1, 3))
+            for j in range(3):
+                E.set_scale(j, sc[j])
+            c64 = E.evaluate(eng.FORM_BATCHED_FP64)["chi2"]
+            c32 = E.evaluate(eng.FORM_BATCHED_FP32)["chi2"]
+            worst = max(worst, abs(c32 - c64) / abs(c64))
+        for j in range(3):
+            E.set_scale(j, 1.0)
+        for k in range(3):
+            E.evaluate(eng.FORM_BATCHED_FP32)
+        dev = []
+        for k in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            E.set_scale(0, 1.0 + 1e-3 * math.sin(0.7 * k))
+            E.evaluate(eng.FORM_BATCHED_FP32)
+            dev.append(E.last_ms())
+        st = E.stage_times(eng.FORM_BATCHED_FP32)
+        E.close()
+        _, _, _, rs_bytes = algorithmic_bytes(model, dds, lcs, 4)
+        rs_ms = st.get("raster_synth", float("nan"))
+        ms = statistics.mean(dev)
+        cpu = cpu_baseline(model, dds, lcs, params, budget_s=budget_cpu_s)
+        out[name] = {"workload": desc, "frame_evals_per_s": nu / (ms / 1e3), "ms_per_step": ms,
+                     "p50_ms": statistics.median(dev), "p99_ms": float(np.percentile(dev, 99)),
+                     "raster_ms": rs_ms, "roofline_frac": rs_bytes / (rs_ms / 1e3) / 1e9 / peak,
+                     "max_dchi2_rel_fp32_vs_fp64": worst,
+                     "cpu_reference_frame_evals_per_s": cpu["value"], "cpu_cores": cpu["cores"]}
+    # config 4: the vertex-deviation sweep over its first parameters
+    params = synth.eval_params()
+    model, dds, lcs, desc = workload("c4", dd_syn, None, params)
+    E = eng.make_engine(model, params, deldops=dds, device=lrank)
+    E.evaluate(eng.FORM_BATCHED_FP32)
+    npar = 100
+    fit_params = [(eng.PAR_VERTEX_R, i, SWEEP_STEP, SWEEP_TOL, SWEEP_ABSTOL) for i in range(npar)]
+    t0 = time.perf_counter()
+    res, _ = E.bestfit(fit_params, form=eng.FORM_BATCHED_FP32, term_prec=1e-4, term_maxiter=1)
+    dt = time.perf_counter() - t0
+    E.close()
+    cpu = sweep_cpu(model, dds, params, k=2)
+    out["c4_sweep"] = {"workload": desc + "; one bestfit sweep over the first %d vertex deviations" % npar,
+                       "trials_per_s": res["evaluations"] / dt, "trials": res["evaluations"],
+                       "frame_evals_per_s": res["evaluations"] * dds[0].nframes / dt,
+                       "cpu_reference_trials_per_s": cpu["value"], "cpu_sample": cpu["sample"],
+                       "cpu_cores": cpu["cores"]}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -433,6 +502,7 @@ def main():
     ap.add_argument("--params", type=int, default=2000, help="vertex parameters of the sweep mode")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-mix measurement")
+    ap.add_argument("--no-per-config", action="store_true", help="skip the configs 1, 3, 4 block")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, ws, lrank, dist = dist_setup()
@@ -514,18 +584,18 @@ def main():
     kpe = E.kernels_per_eval(form)
     stages = E.stage_times(form if form != eng.FORM_PLAIN_FP64 else eng.FORM_BATCHED_FP64)
 
-    # the FP32 form with shape_engine_set_fp32_exact(1) (facet and depth maps
-    # of every view equal to the FP64 form's), a short run beside the default
-    exact = None
+    # the FP32 form with shape_engine_set_fp32_exact(0) (radar views keep
+    # their FP32 coverage decisions), a short run beside the default
+    fast = None
     if form == eng.FORM_BATCHED_FP32 and not lcs:
-        E.set_fp32_exact(True)
-        ex_ms, _ = run(form, max(20, min(args.steps, 100)), 3, False)
+        E.set_fp32_exact(False)
+        fx_ms, _ = run(form, max(20, min(args.steps, 100)), 3, False)
         E.set_scale(0, trial(0))           # both forms at the same scale factors
         c64 = E.evaluate(eng.FORM_BATCHED_FP64)["chi2"]
-        c32x = E.evaluate(form)["chi2"]
-        E.set_fp32_exact(False)
-        exact = {"frame_evals_per_s": nu / (statistics.mean(ex_ms) / 1e3), "ms_per_step": statistics.mean(ex_ms),
-                 "dchi2_rel_fp32_vs_fp64": abs(c32x - c64) / abs(c64)}
+        c32f = E.evaluate(form)["chi2"]
+        E.set_fp32_exact(True)
+        fast = {"frame_evals_per_s": nu / (statistics.mean(fx_ms) / 1e3), "ms_per_step": statistics.mean(fx_ms),
+                "dchi2_rel_fp32_vs_fp64": abs(c32f - c64) / abs(c64)}
 
     total_dev = sum(dev_ms)
     total_host = sum(host_ms)
@@ -548,11 +618,15 @@ def main():
     # dominant kernel: the fused tile raster (+ delay-Doppler synthesis)
     rs_ms = stages.get("raster_synth", float("nan"))
     achieved = rs_bytes / (rs_ms / 1e3) / 1e9
-    traffic = None
+    # DRAM traffic and issue-slot use of this kernel cannot be read inside
+    # the run: they come from the ncu capture summarized in profiles/ (its
+    # command and build named there), per launch of the same workload
+    traffic, issue, prof_src = None, None, None
     traffic_path = os.path.join(REPO, "profiles", "raster_traffic.json")
     if os.path.exists(traffic_path):
         try:
-            traffic = json.load(open(traffic_path)).get(args.workload + "_" + args.form)
+            rec = json.load(open(traffic_path)).get(args.workload + "_" + args.form) or {}
+            traffic, issue, prof_src = rec.get("dram_bytes"), rec.get("issue_active_pct"), rec.get("source")
         except Exception:
             traffic = None
     step_bytes = b_model + b_pos + b_dd
@@ -568,14 +642,15 @@ def main():
                    "dchi2_rel_fp32_vs_fp64": dchi,
                    "plain_fp64_frame_evals_per_s": plain_rate,
                    "batched_over_plain_fp64": value / ws / plain_rate,
-                   "fp32_exact_option": exact,
+                   "fp32_fast_option": fast,
                    "p50_ms": statistics.median(dev_ms), "p99_ms": float(np.percentile(dev_ms, 99)),
                    "stage_ms": stages,
                    "step_algorithmic_bytes": step_bytes,
                    "step_achieved_gbs": step_bytes / (ms_step / 1e3) / 1e9},
         "roofline": {"bound": "hbm", "kernel": "k_raster (tile raster + delay-Doppler synthesis)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_src, "traffic": traffic,
+                     "peak_source": peak_src, "traffic": traffic, "traffic_source": prof_src,
+                     "issue_active_pct": issue,
                      "algorithmic_bytes_per_launch": rs_bytes},
         "e2e": {"value": e2e, "unit": "frame-evals/s", "h2d_bytes_per_step": 8 * (model.nv + 3),
                 "d2h_bytes_per_step": 72,
@@ -587,6 +662,8 @@ def main():
     E.close()
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(model, dds, lcs, params)
+    if ws == 1 and not args.no_per_config and args.workload == "c2":
+        line["per_config"] = per_config(lrank, flush)
     if ws == 1 and not args.no_serve and args.workload == "c2":
         line["serving"] = serving_bench(lrank)
     if dist:
