@@ -34,6 +34,17 @@
 #ifndef RASTER_MIN_BLOCKS_F64
 #define RASTER_MIN_BLOCKS_F64 4
 #endif
+// The warp-independent raster (k_raster_w): its shared memory allows 6
+// CTAs per SM in FP32 (40 registers) and 3 in FP64.
+#ifndef RASTER_W_MIN_BLOCKS
+#define RASTER_W_MIN_BLOCKS 6
+#endif
+#ifndef RASTER_W_MIN_BLOCKS_F64
+#define RASTER_W_MIN_BLOCKS_F64 3
+#endif
+#ifndef RASTER_WARP
+#define RASTER_WARP 0
+#endif
 #ifndef RASTER_RARE_NOINLINE
 #define RASTER_RARE_NOINLINE 0
 #endif
@@ -1240,6 +1251,334 @@ k_raster(RasterArgs a)
     }
 }
 
+// ------------------------------------------------------------------------
+// Warp-independent tile raster. The CTA still takes one 16x16 tile (its bin
+// read once into L1), but each of its 8 warps works its 4x8 block on its own,
+// with no CTA-wide barrier: a warp collects the bin's facets whose bbox
+// meets its block, sorts them by facet index, stages and replays them 32 at
+// a time, then finalizes, writes and scatters its own 32 pixels and moves
+// the frame limits with atomics it skips when they cannot change anything.
+// Blocks of one tile differ in work by about 2x on average, so the CTA-wide
+// barriers of k_raster kept the faster warps of a tile idle.
+constexpr int WARP_LIST = 128;       // facets a warp block sorts in shared memory
+
+template <typename T>
+struct WarpArea {
+    int2 ids[WARP_LIST];             // the block's bin entries, in facet order
+    Stage<T> st[32];                 // the chunk being replayed
+};
+
+template <typename T, bool EXACT>
+__global__ void __launch_bounds__(RASTER_THREADS, sizeof(T) == 8 ? RASTER_W_MIN_BLOCKS_F64 : RASTER_W_MIN_BLOCKS)
+k_raster_w(RasterArgs a)
+{
+    grid_dep_wait();
+    extern __shared__ __align__(32) unsigned char smem[];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    WarpArea<T> &wa = reinterpret_cast<WarpArea<T> *>(smem)[wid];
+    int2 *ids = wa.ids;
+    Stage<T> *st = wa.st;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    // warp wid owns a 4x8 block of the 16x16 tile
+    const int bi0 = 4 * (wid >> 1), bj0 = 8 * (wid & 1);
+    const int li = bi0 + (lane >> 3), lj = bj0 + (lane & 7);
+
+    for (int w = blockIdx.x; w < a.nwork; w += gridDim.x) {
+        const int2 item = a.work[w];
+        const FrameGeom &g = a.geoms[item.x];
+        const int tile = item.y;
+        const int tx = tile / g.tiles_x, ty = tile % g.tiles_x;
+        const int n = g.n;
+        const int ti0 = -n + tx * TILE_W, tj0 = -n + ty * TILE_W;
+        const int ti1 = min(ti0 + TILE_W - 1, n), tj1 = min(tj0 + TILE_W - 1, n);
+        const int pi = ti0 + li, pj = tj0 + lj;
+        const bool inframe = (pi <= n) && (pj <= n);
+        const int count = a.bin_count[g.tile_base + tile];
+        const bool writes_pos = (g.kind != VIEW_RADAR) || a.keep_pos;
+        if (count == 0 && !writes_pos) continue;
+        // a block wholly outside the frame (the tile's last rows or columns)
+        if (bi0 > ti1 - ti0 || bj0 > tj1 - tj0) continue;
+
+        const double ox = (double)ti0 * g.kmpp, oy = (double)tj0 * g.kmpp;
+        const T x0 = (sizeof(T) == 8) ? (T)pi * (T)g.kmpp : (T)((double)li * g.kmpp);
+        const T x1 = (sizeof(T) == 8) ? (T)pj * (T)g.kmpp : (T)((double)lj * g.kmpp);
+        T zz = (T)(-SHAPE_HUGENUMBER), cosa = 0, cosb = 0;
+        int fac = -1;
+        if constexpr (sizeof(T) == 8) {
+            if (a.accumulate && inframe) {
+                const long long p = g.pos_base + (long long)(pi + n) * g.side + (pj + n);
+                zz = static_cast<const double *>(a.pos_z)[p];
+                fac = a.pos_f[p];
+                cosa = static_cast<const T *>(a.pos_cose)[p];
+                if (g.kind != VIEW_LC_SUN) cosb = static_cast<const T *>(a.pos_cosi)[p];
+            }
+        }
+        T zze = 0, zlo = 0;
+        bool amb = false, good = false;
+        T gm0 = 0, gm1 = 0, gm2 = 0;
+        const bool smooth = g.smooth != 0;
+        const bool bistatic_obs = (g.kind == VIEW_LC_OBS);
+        const T oa6 = (T)g.oa[6], oa7 = (T)g.oa[7], oa8 = (T)g.oa[8];
+        const unsigned pxw = pack_px(li, lj);
+        auto visit = [&](const Stage<T> &s) {
+            T sv, tv, z, zr = 0;
+            if constexpr (sizeof(T) == 8) {
+                if (__vcmpgeu4(pxw, s.bb) != 0xffffffffu) return;
+                const auto p0 = s.p0, p1 = s.p1;
+                const T dx = x0 - p0.x, dy = x1 - p0.y;
+                sv = (dx * p0.z - p0.w * dy) * p1.x;
+                if (!((sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL))) return;
+                tv = (p1.y * dy - dx * p1.z) * p1.x;
+                if (!((tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL))) return;
+                const auto p2 = s.p2;
+                z = p1.w + sv * p2.x + tv * p2.y;
+                if (!((z > zz) || (fac < 0))) return;
+            } else {
+                const auto p0 = s.p0, p1 = s.p1, p2 = s.p2;
+                const float4 be = *reinterpret_cast<const float4 *>(&s.bb);
+                const bool inb = __vcmpgeu4(pxw, __float_as_uint(be.x)) == 0xffffffffu;
+                const T dx = x0 - p0.x, dy = x1 - p0.y;
+                sv = fmaf(p0.z, dx, p0.w * dy);
+                tv = fmaf(p1.x, dx, p1.y * dy);
+                zr = fmaf(p1.z, dx, p1.w * dy);
+                z = p2.y + zr;
+                const T es = be.y, et = be.z, est = es + et;
+                if constexpr (EXACT) {
+                    const bool out = !inb || (sv < -2 * es) || (sv > 1 + 2 * es) || (tv < -2 * et) ||
+                                     (tv > sv + 2 * est);
+                    if (out) return;
+                    const bool sure = (sv >= es) && (sv <= 1 - es) && (tv >= et) && (tv <= sv - est);
+                    const bool near = (fac >= 0) && (fabsf(z - zz) <= be.w + zze);
+                    amb = amb || !sure || near;
+                    if (!((z > zz) || (fac < 0))) return;
+                    zze = be.w;
+                } else {
+                    const bool in = inb && (sv >= (T)-SHAPE_SMALLVAL) && (sv <= (T)1.0 + (T)SHAPE_SMALLVAL) &&
+                                    (tv >= (T)-SHAPE_SMALLVAL) && (tv <= sv + (T)SHAPE_SMALLVAL);
+                    if (!(in && ((z > zz) || (fac < 0)))) return;
+                }
+            }
+            const auto p2 = s.p2;
+            zz = z;
+            fac = s.f;
+            if constexpr (sizeof(T) == 4) {
+                const float bv = z - p2.y;
+                zlo = ((p2.y - (z - bv)) + (zr - bv)) + p2.x;
+            }
+            if (smooth) {
+                const T m0 = s.q[0] + sv * (s.q[3] - s.q[0]) + tv * (s.q[6] - s.q[3]);
+                const T m1 = s.q[1] + sv * (s.q[4] - s.q[1]) + tv * (s.q[7] - s.q[4]);
+                const T m2 = s.q[2] + sv * (s.q[5] - s.q[2]) + tv * (s.q[8] - s.q[5]);
+                T r2 = 0;
+                r2 += oa6 * m0; r2 += oa7 * m1; r2 += oa8 * m2;
+                if constexpr (sizeof(T) == 4 && EXACT)
+                    amb = amb || (fabsf(r2) <= 4 * (s.es + s.et) + 1e-6f * (fabsf(m0) + fabsf(m1) + fabsf(m2)));
+                if (r2 > (T)0) { good = true; gm0 = m0; gm1 = m1; gm2 = m2; }
+            } else {
+                good = true; gm0 = p2.z; gm1 = p2.w; gm2 = s.nz;
+            }
+        };
+
+        // the block's facets: bin entries whose tile bbox meets the block
+        int nb = 0;
+        bool listed = (count > 0 && count <= a.cap);
+        if (listed) {
+            const int2 *bin = a.bin_ids + (size_t)(g.tile_base + tile) * a.cap;
+            for (int base = 0; base < count; base += 32) {
+                const int k = base + lane;
+                int2 e = make_int2(0, 0);
+                bool hit = false;
+                if (k < count) {
+                    e = bin[k];
+                    const int b = e.y;
+                    hit = (b & 15) <= bi0 + 3 && ((b >> 4) & 15) >= bi0 && ((b >> 8) & 15) <= bj0 + 7 &&
+                          ((b >> 12) & 15) >= bj0;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                const int pos = nb + __popc(m & lt_mask);
+                if (hit && pos < WARP_LIST) ids[pos] = e;
+                nb += __popc(m);
+            }
+            __syncwarp();
+            listed = nb <= WARP_LIST;
+        }
+        if (listed && nb > 0) {
+            // facet order (posvis walks facets in index order): a facet's rank
+            // is the number of listed facets with a smaller index
+            int2 mine[WARP_LIST / 32];
+            int rank[WARP_LIST / 32];
+#pragma unroll
+            for (int r = 0; r < WARP_LIST / 32; r++) {
+                const int k = lane + 32 * r;
+                rank[r] = -1;
+                if (k < nb) {
+                    mine[r] = ids[k];
+                    int c = 0;
+                    for (int j = 0; j < nb; j++) c += (ids[j].x < mine[r].x);
+                    rank[r] = c;
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < WARP_LIST / 32; r++)
+                if (rank[r] >= 0) ids[rank[r]] = mine[r];
+            __syncwarp();
+            for (int c0 = 0; c0 < nb; c0 += 32) {
+                const int nst = min(32, nb - c0);
+                if (lane < nst) {
+                    const int2 e = ids[c0 + lane];
+                    Stage<T> sf;
+                    const int bb = e.y;
+                    sf.bb = pack_bb(bb & 15, (bb >> 4) & 15, (bb >> 8) & 15, (bb >> 12) & 15);
+                    sf.wmask = 0;
+                    stage_fill<T>(a, g, e.x, sf, ox, oy);
+                    st[lane] = sf;
+                }
+                __syncwarp();
+                for (int b = 0; b < nst; b++) visit(st[b]);
+                __syncwarp();
+            }
+        } else if (count > 0 && !listed) {
+            // bin or block list overflow: every facet of the model in index
+            // order, keeping those that overlap this tile
+            for (int c0 = 0; c0 < a.nf; c0 += 32) {
+                Stage<T> sf;
+                bool ok = false;
+                if (c0 + lane < a.nf) ok = stage_facet<T>(a, g, c0 + lane, ti0, ti1, tj0, tj1, sf, ox, oy);
+                const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                if (ok) st[__popc(bal & lt_mask)] = sf;
+                __syncwarp();
+                const int tot = __popc(bal);
+                for (int b = 0; b < tot; b++) visit(st[b]);
+                __syncwarp();
+            }
+        }
+
+        // FP32 form: a pixel with a decision within FP32 error is redone by
+        // the FP64 form's rules over the block's sorted list (an overflowing
+        // block, which has none, keeps its FP32 decisions)
+        if constexpr (sizeof(T) == 4 && EXACT) {
+            if (amb && listed && nb > 0) {
+                float gmv[3] = {0.0f, 0.0f, 0.0f};
+                double zw;
+                good = false;
+                fac = pixel_posvis64(a, g, ids, nb, li, lj, (double)pi * g.kmpp, (double)pj * g.kmpp, &zw, &good,
+                                     gmv);
+                zz = (float)zw;
+                zlo = (float)(zw - (double)zz);
+                gm0 = gmv[0]; gm1 = gmv[1]; gm2 = gmv[2];
+            }
+        }
+
+        if (good) {
+            T n0 = gm0, n1 = gm1, n2 = gm2;
+            T oa[12];
+            load_oa<T>(g, oa);
+            if (smooth) {
+                T r0 = 0, r1 = 0, r2 = 0;
+                r0 += oa[0] * gm0; r0 += oa[1] * gm1; r0 += oa[2] * gm2;
+                r1 += oa[3] * gm0; r1 += oa[4] * gm1; r1 += oa[5] * gm2;
+                r2 += oa6 * gm0; r2 += oa7 * gm1; r2 += oa8 * gm2;
+                T norm = 0;
+                norm += r0 * r0; norm += r1 * r1; norm += r2 * r2;
+                norm = sqrt(norm);
+                if (norm != (T)0) { r0 /= norm; r1 /= norm; r2 /= norm; }
+                n0 = r0; n1 = r1; n2 = r2;
+            }
+            if (n2 > (T)0) {
+                cosa = n2;
+                if (bistatic_obs) {
+                    cosb = n0 * oa[9] + n1 * oa[10] + n2 * oa[11];
+                    if (cosb <= (T)0) cosa = 0;
+                }
+            }
+        }
+
+        bool covered = inframe && fac >= 0;
+        double z64 = (double)zz;
+        if constexpr (sizeof(T) == 4) {
+            if (fac < 0) {
+                z64 = -SHAPE_HUGENUMBER;
+            } else if (g.kind != VIEW_RADAR || (EXACT && writes_pos)) {
+                const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
+                z64 = facet_depth64(vt, a.fvi[fac], (double)pi * g.kmpp, (double)pj * g.kmpp);
+            } else {
+                z64 = (double)zz + (double)zlo;
+            }
+        }
+        if (inframe && writes_pos) {
+            long long p = g.pos_base + (long long)(pi + n) * g.side + (pj + n);
+            double *Z = static_cast<double *>(a.pos_z);
+            T *CE = static_cast<T *>(a.pos_cose), *CI = static_cast<T *>(a.pos_cosi);
+            if constexpr (sizeof(T) == 8) {
+                if (a.accumulate) {
+                    const bool won = (Z[p] != z64) || (a.pos_f[p] != fac);
+                    a.won[p] = won ? 1 : 0;
+                    covered = won;
+                }
+            }
+            Z[p] = z64;
+            a.pos_f[p] = fac;
+            CE[p] = cosa;
+            if (g.kind != VIEW_LC_SUN) CI[p] = cosb;
+        }
+        FrameState &S = a.states[item.x];
+        // covered-pixel bbox (POSrect with (i,i,j,j), posvis.c:278-280); an
+        // atomic only where it can move the frame's value
+        {
+            const int cimin = warp_min(covered ? pi : INT_MAX), cimax = warp_max(covered ? pi : INT_MIN);
+            const int cjmin = warp_min(covered ? pj : INT_MAX), cjmax = warp_max(covered ? pj : INT_MIN);
+            if (lane == 0 && cimin != INT_MAX) {
+                if (cimin < *(volatile int *)&S.cov_i[0]) atomicMin(&S.cov_i[0], cimin);
+                if (cimax > *(volatile int *)&S.cov_i[1]) atomicMax(&S.cov_i[1], cimax);
+                if (cjmin < *(volatile int *)&S.cov_j[0]) atomicMin(&S.cov_j[0], cjmin);
+                if (cjmax > *(volatile int *)&S.cov_j[1]) atomicMax(&S.cov_j[1], cjmax);
+            }
+        }
+        if (g.kind == VIEW_RADAR) {
+            if (covered && a.mark_seen && (double)cosa > a.mincosine_seen) a.seen[fac] = 1;
+            const DDC<T> kc = load_ddc<T>(g);
+            PixPos pp = {0.0, 0.0};
+            PixDD<T> dd;
+            dd.ok = false;
+            const bool lit = covered && cosa > (T)0;
+            if (lit) {
+                if constexpr (sizeof(T) == 4)
+                    dd = pixel_dd_setup_x(g, pi, pj, z64, pp);
+                else
+                    dd = pixel_dd_setup<T>(g, kc, pi, pj, z64, pp);
+            }
+            // delay / Doppler extremes of the lit pixels as dkey keys
+            const unsigned long long kd = dkey(pp.del), kp = dkey(pp.dop);
+            const unsigned long long k0 = warp_kmin(lit ? kd : ~0ull), k1 = warp_kmax(lit ? kd : 0ull);
+            const unsigned long long k2 = warp_kmin(lit ? kp : ~0ull), k3 = warp_kmax(lit ? kp : 0ull);
+            if (lane == 0 && k0 != ~0ull) {
+                int l[4];
+                dd_bin_limits(g, dkey_inv(k0), dkey_inv(k1), dkey_inv(k2), dkey_inv(k3), l);
+                if (l[0] < *(volatile int *)&S.idellim[0]) atomicMin(&S.idellim[0], l[0]);
+                if (l[1] > *(volatile int *)&S.idellim[1]) atomicMax(&S.idellim[1], l[1]);
+                if (l[2] < *(volatile int *)&S.idoplim[0]) atomicMin(&S.idoplim[0], l[2]);
+                if (l[3] > *(volatile int *)&S.idoplim[1]) atomicMax(&S.idoplim[1], l[3]);
+                if (k0 < *(volatile unsigned long long *)&S.dellim[0]) atomicMin(&S.dellim[0], k0);
+                if (k1 > *(volatile unsigned long long *)&S.dellim[1]) atomicMax(&S.dellim[1], k1);
+                if (k2 < *(volatile unsigned long long *)&S.doplim[0]) atomicMin(&S.doplim[0], k2);
+                if (k3 > *(volatile unsigned long long *)&S.doplim[1]) atomicMax(&S.doplim[1], k3);
+                if (!*(volatile int *)&S.any_lit) S.any_lit = 1;
+            }
+            if (dd.ok) {
+                if constexpr (sizeof(T) == 4)
+                    pixel_dd_scatter_f32_direct(a, g, kc, cosa, dd, static_cast<float *>(a.fit) + g.fit_base);
+                else
+                    pixel_dd_scatter<T>(a, g, kc, cosa, dd, static_cast<T *>(a.fit) + g.fit_base, 1, 1, g.ndop);
+            } else if (g.dop1d && lit) {
+                S.any_overflow = 1;
+                pixel_dop_overflow<T>(a, g, kc, cosa, dd);
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // Dynamic shared memory of a raster CTA: the ranked bin, then the staging
 // area, large enough for the staged facets and for the rank's scratch (the
 // bitmap and prefix counts, 8 bytes per 32 facets, plus the raw bin).
@@ -1252,15 +1591,22 @@ inline size_t raster_smem_bytes(int cap, int nf)
 }
 
 // Called once per device before any launch (not inside stream capture).
-// Both kernels run several CTAs per SM (8 FP32, 4 FP64), which needs the
-// largest shared-memory carveout.
+// Both kernels run several CTAs per SM, which needs the largest
+// shared-memory carveout.
 template <typename T, bool EXACT>
 inline cudaError_t configure_raster_one()
 {
     cudaError_t e = cudaFuncSetAttribute(k_raster<T, EXACT>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_raster<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_raster<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_raster_w<T, EXACT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_raster_w<T, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(RASTER_THREADS / 32 * sizeof(WarpArea<T>)));
+    return e;
 }
 template <typename T>
 inline cudaError_t configure_raster_t()
@@ -1275,10 +1621,18 @@ inline void launch_raster_t(const RasterArgs &a, cudaStream_t s)
 {
     if (a.nwork <= 0) return;
     RasterArgs b = a;
-    b.smem_bytes = raster_smem_bytes<T>(a.cap, a.nf);
     const int grid = (a.grid > 0 && a.grid < a.nwork) ? a.grid : a.nwork;
     // the FP64 form is exact by construction; the FP32 form runs its exact
-    // variant on lightcurve views
+    // variant unless radar views are asked for their FP32 decisions
+    if (RASTER_WARP) {
+        b.smem_bytes = RASTER_THREADS / 32 * sizeof(WarpArea<T>);
+        if (sizeof(T) == 4 && a.exact)
+            launch_k(k_raster_w<T, true>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
+        else
+            launch_k(k_raster_w<T, false>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
+        return;
+    }
+    b.smem_bytes = raster_smem_bytes<T>(a.cap, a.nf);
     if (sizeof(T) == 4 && a.exact)
         launch_k(k_raster<T, true>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
     else
