@@ -594,9 +594,10 @@ typedef struct shape_obs_options {
 
 /* A SHAPE observation file (.obs; read_dat, src/shape/read_dat.c:409-527)
  * whose datasets are delay-Doppler sets (read_deldop, :528-900) or Doppler
- * sets (read_doppler, :920-1180) with one view per frame and no
- * pixel-weighting masks or gzipped data files (those, and the other
- * dataset types, return SHAPE_E_UNSUPPORTED). The '=' state of angle and
+ * sets (read_doppler, :920-1180) or lightcurve / heliocurve sets
+ * (read_lghtcrv, :1667-2063) with one view per frame or point and no
+ * pixel-weighting masks or gzipped data files (those, and plane-of-sky
+ * sets, return SHAPE_E_UNSUPPORTED). The '=' state of angle and
  * spin offsets and of delay-correction polynomials takes the last earlier
  * set's value, as the reference's realize_angleoff, realize_omegaoff and
  * realize_delcor do (src/shape/realize_spin.c:283-337,
@@ -607,7 +608,8 @@ int shape_obs_read(const char *path, shape_obs_file **out);
 void shape_obs_free(shape_obs_file *o);
 int shape_obs_nsets(const shape_obs_file *o);
 /* 0: set s is a delay-Doppler set (shape_obs_set / shape_obs_frames);
- * 1: a Doppler set (shape_obs_doppler). */
+ * 1: a Doppler set (shape_obs_doppler); 2: a lightcurve or heliocurve set
+ * (shape_obs_lghtcrv_info / shape_obs_lghtcrv). */
 int shape_obs_set_type(const shape_obs_file *o, int s);
 /* Set s's radar setup (set->law is kept: take it from the model's radar
  * law iradlaw), its frame count, angle and spin offsets (rad, rad/day) and
@@ -638,6 +640,26 @@ int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spi
 int shape_obs_doppler(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
                       const shape_obs_options *opt, shape_doppler_set *set, shape_doppler_frame *frames, double *obs,
                       double *oneovervar);
+
+/* Lightcurve set s (read_lghtcrv, src/shape/read_dat.c:1667-2063; its data
+ * file, named in the .obs file relative to the current directory, is read
+ * by shape_obs_read): the index of its optical law in the model, and its
+ * numbers of calculated and observed points. One view per point. A
+ * heliocurve set is read as the reference reads it: as a lightcurve set,
+ * its two tables taken as the asteroid's and the Sun's ephemerides
+ * (src/shape/read_dat.c:495-502 passes the lightcurve type). */
+int shape_obs_lghtcrv_info(const shape_obs_file *o, int s, int *ioptlaw, int *ncalc, int *n);
+/* The set ready for shape_engine_add_lghtcrv_set: set (its law member is
+ * kept: take it from the model's optical law ioptlaw), ncalc points, the
+ * calculated epochs x[ncalc] (light-time corrected with perform_ltc) with
+ * each point's observer, Sun and body matrices and solar phase, and the
+ * observation epochs t[n], intensities obs[n] (magnitudes relative to
+ * sun_appmag, the .par file's sun_appmag for this law) and 1/variance; set
+ * points at the caller's x, t, obs and oneovervar arrays. As read_lghtcrv
+ * and realize_spin give them (src/shape/realize_spin.c:223-260). */
+int shape_obs_lghtcrv(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
+                      const shape_obs_options *opt, double sun_appmag, shape_lghtcrv_set *set,
+                      shape_lghtcrv_point *points, double *x, double *t, double *obs, double *oneovervar);
 
 /* The listfit output of one radar frame (chi2_deldop with listfit,
  * src/shape/chi2.c:525-560): ndel*ndop lines "%13.6e" of cal * fit / sdev,

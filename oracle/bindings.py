@@ -195,6 +195,9 @@ class Reference:
         L = self.lib = _load(REF_SO, "oracle/build_ref.sh")
         P = C.POINTER
         L.ref_spline_eval.argtypes = [cd.dptr, cd.dptr, C.c_int, cd.dptr, C.c_int, cd.dptr]
+        L.ref_obs_lghtcrv.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), cd.dptr, cd.dptr, cd.dptr, cd.dptr,
+                                      cd.dptr, cd.dptr]
+        L.ref_obs_lghtcrv_ephem.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr]
         L.ref_new.restype = C.c_void_p
         L.ref_new.argtypes = [P(cd.ModelDesc), P(cd.EvalParams), C.c_int]
         L.ref_set_radar_law.argtypes = [C.c_void_p, P(cd.RadarLaw)]

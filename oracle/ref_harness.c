@@ -931,6 +931,7 @@ void *ref_obs_read(const char *modpath, const char *obspath, int perform_ltc, do
     F->par.pos_scope = LOCAL;              /* POS sizing in read_dat (set_up_pos) */
     F->par.pos_pixels = 151;
     F->par.pos_width = 2.25;
+    for (int k = 0; k < MAXSUNMAGS; k++) F->par.sun_appmag[k] = -26.75;
     snprintf(F->mod.name, sizeof F->mod.name, "%s", modpath);
     snprintf(F->dat.name, sizeof F->dat.name, "%s", obspath);
     read_mod(&F->par, &F->mod);
@@ -965,6 +966,52 @@ void ref_obs_frame(void *h, int s, int f, double *geom, int *nd, double *obs, do
             if (obs) obs[(j - 1) * fr->ndop + (k - 1)] = fr->obs[j][k];
             if (oov) oov[(j - 1) * fr->ndop + (k - 1)] = fr->oneovervar[j][k];
         }
+}
+
+/* A lightcurve set of ref_obs_read's data: sizes = ioptlaw, ncalc, n (x
+ * NULL: sizes only); x[ncalc]; per calculated point i, pt[28 i ..] =
+ * oe[9], se[9], ae[9], solar_phase; t[n] (first view), obs[n], oov[n];
+ * tail = weight, dof, cal. */
+void ref_obs_lghtcrv(void *h, int s, int *sizes, double *x, double *pt, double *t, double *obs, double *oov,
+                     double *tail)
+{
+    ref_obsfile *F = h;
+    struct lghtcrv_t *lc = &F->dat.set[s].desc.lghtcrv;
+    sizes[0] = lc->ioptlaw;
+    sizes[1] = lc->ncalc;
+    sizes[2] = lc->n;
+    if (!x) return;
+    for (int i = 1; i <= lc->ncalc; i++) {
+        x[i - 1] = lc->x[i];
+        double *g = pt + 28 * (size_t)(i - 1);
+        for (int a = 0; a < 3; a++) for (int b = 0; b < 3; b++) *g++ = lc->rend[i].oe[a][b];
+        for (int a = 0; a < 3; a++) for (int b = 0; b < 3; b++) *g++ = lc->rend[i].se[a][b];
+        for (int a = 0; a < 3; a++) for (int b = 0; b < 3; b++) *g++ = lc->rend[i].ae[a][b];
+        *g++ = lc->solar_phase[i];
+    }
+    for (int i = 1; i <= lc->n; i++) {
+        t[i - 1] = lc->t[i][0];
+        obs[i - 1] = lc->obs[i];
+        oov[i - 1] = lc->oneovervar[i];
+    }
+    tail[0] = lc->weight;
+    tail[1] = lc->dof;
+    tail[2] = lc->cal.val;
+}
+
+/* The asteroid (which = 0) or solar (1) ephemeris of lightcurve set s as
+ * ref_obs_read's read_dat left it: per entry t, ra, dec, dist; returns n. */
+int ref_obs_lghtcrv_ephem(void *h, int s, int which, double *out)
+{
+    ref_obsfile *F = h;
+    struct lghtcrv_t *lc = &F->dat.set[s].desc.lghtcrv;
+    struct ephem_t *e = which ? &lc->solephem : &lc->astephem;
+    if (out)
+        for (int i = 0; i < e->n; i++) {
+            out[4 * i] = e->pnt[i].t; out[4 * i + 1] = e->pnt[i].ra;
+            out[4 * i + 2] = e->pnt[i].dec; out[4 * i + 3] = e->pnt[i].dist;
+        }
+    return e->n;
 }
 
 /* A Doppler frame of ref_obs_read's data: geom = t, oe[9], orbspin[3],

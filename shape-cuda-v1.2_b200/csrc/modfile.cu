@@ -705,6 +705,7 @@ struct shape_obs_file {
     };
     struct Set {
         int doppler = 0;                 // 1: a Doppler set (read_doppler)
+        int lightcurve = 0;              // 1: a lightcurve or heliocurve set (read_lghtcrv)
         int iradlaw;
         double angleoff[3], omegaoff[3];
         char angle_state[3], omega_state[3];   // c, f or = (= ties to an earlier set)
@@ -717,9 +718,101 @@ struct shape_obs_file {
         std::vector<double> delcor;
         std::string dir;
         std::vector<Frame> frames;
+        // lightcurve sets (read_lghtcrv, src/shape/read_dat.c:1667-2063)
+        int ioptlaw = 0;
+        std::vector<shape_ephem_point> solephem;   // the Sun as seen by the observer
+        std::vector<double> x0;                    // calculated epochs before light-time correction
+        std::string lcname;                        // data file
+        char lc_cal_state = 'c';
+        double lc_cal = 0.0, lc_weight = 0.0;
+        std::vector<double> lc_t0, lc_mag, lc_magerr;   // the data file's points
     };
     std::vector<Set> sets;
 };
+
+// An ephemeris table: a count, then per entry an epoch (yyyy mm dd hh mm
+// ss), RA and Dec in degrees and distance in AU.
+static std::vector<shape_ephem_point> read_ephem(Tokens &tk, const char *what)
+{
+    const int ne = tk.integer(what);
+    if (ne < 2) tk.fail(std::string(what) + ": an ephemeris needs at least 2 points");
+    std::vector<shape_ephem_point> v(ne);
+    for (int i = 0; i < ne; i++) {
+        v[i].t = read_epoch(tk, "ephemeris epoch");
+        v[i].ra = tk.real("RA") * D2R;
+        v[i].dec = tk.real("Dec") * D2R;
+        v[i].dist = tk.real("distance");
+    }
+    return v;
+}
+
+// The body of a lightcurve or heliocurve set (read_lghtcrv,
+// src/shape/read_dat.c:1667-1956): optical law, the asteroid's and the
+// Sun's ephemerides, the calculated epochs (a list, a start / stop / step,
+// or the observation epochs), one view per point, the data file and its
+// calibration and weight; the data file is read here, as read_dat reads
+// it, so a set whose calculated epochs are its observation epochs knows
+// them. A heliocurve set is read exactly as a lightcurve set: read_dat
+// gives read_lghtcrv the set type LGHTCRV for both (:487-502), so the
+// reference never takes read_lghtcrv's heliocentric branch (:1740-1786)
+// and uses the two tables as written.
+static void read_lghtcrv_set(Tokens &tk, shape_obs_file::Set &S)
+{
+    S.lightcurve = 1;
+    S.delcor_state = 'c';
+    memset(&S.dd, 0, sizeof S.dd);
+    S.ndel = S.ndop = 0;
+    S.iradlaw = 0;
+    S.ioptlaw = tk.integer("optical law");
+    if (S.ioptlaw < 0) tk.fail("negative optical law index");
+    S.ephem = read_ephem(tk, "asteroid ephemeris points");
+    S.solephem = read_ephem(tk, "solar ephemeris points");
+    const int np = tk.integer("calculation epochs");
+    if (np > 0) {
+        for (int i = 0; i < np; i++) {
+            S.x0.push_back(tk.real("calculation epoch"));
+            if (i > 0 && S.x0[i] <= S.x0[i - 1]) tk.fail("calculation epochs must increase");
+        }
+    } else if (np == 0) {
+        const double t1 = tk.real("start epoch"), t2 = tk.real("stop epoch"), dt = tk.real("epoch step");
+        if (t2 < t1 || dt <= 0) tk.fail("calculation epochs: need stop >= start and step > 0");
+        const int nc = ((int)floor((t2 - t1) / dt)) + 1;
+        for (int i = 1; i <= nc; i++) S.x0.push_back(t1 + (i - 1) * dt);
+    }
+    const int nviews = tk.integer("views per point");
+    tk.real("view interval");
+    const std::string smear = tk.word("smearing mode");
+    if (smear != "center" && smear != "first") tk.fail("smearing mode " + smear + " is not known");
+    if (nviews != 1) tk.fail("smeared points (more than one view) are not supported", SHAPE_E_UNSUPPORTED);
+    const int n = tk.integer("lightcurve points");
+    if (n < 1) tk.fail("a lightcurve needs at least one point");
+    S.lcname = tk.word("lightcurve data file");
+    S.lc_cal = tk.param("calibration", &S.lc_cal_state);
+    S.lc_weight = tk.real("weight");
+    FILE *fp = fopen(S.lcname.c_str(), "rb");
+    if (!fp) tk.fail("cannot open lightcurve data file " + S.lcname);
+    std::string text;
+    char buf[1 << 16];
+    size_t got;
+    while ((got = fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, got);
+    fclose(fp);
+    Tokens dt(std::move(text));
+    dt.set_kind("lightcurve data file");
+    for (int i = 0; i < n; i++) {
+        S.lc_t0.push_back(dt.real("epoch"));
+        S.lc_mag.push_back(dt.real("magnitude"));
+        S.lc_magerr.push_back(dt.real("magnitude error"));
+    }
+    std::string extra;
+    if (dt.next(extra)) tk.fail("lightcurve data file " + S.lcname + " has more than the points listed");
+    if (np < 0) {
+        // the sorted distinct observation epochs (src/shape/read_dat.c:1990-2004)
+        std::vector<double> e = S.lc_t0;
+        std::sort(e.begin(), e.end());
+        for (size_t i = 0; i < e.size(); i++)
+            if (i == 0 || e[i] > e[i - 1]) S.x0.push_back(e[i]);
+    }
+}
 
 // The '=' state ties a set's value to the last earlier set that gives its
 // own: each component of the angle and spin offsets on its own
@@ -746,6 +839,7 @@ static void tie_obs_sets(std::vector<shape_obs_file::Set> &sets, const Tokens &t
     int sd = -1;
     for (size_t s = 0; s < sets.size(); s++) {
         shape_obs_file::Set &S = sets[s];
+        if (S.lightcurve) continue;              // no delay polynomial
         if (S.delcor_state != '=') { sd = (int)s; continue; }
         if (sd < 0) tk.fail("the first delay-correction polynomial cannot take the = state");
         const shape_obs_file::Set &T = sets[sd];
@@ -789,6 +883,11 @@ int shape_obs_read(const char *path, shape_obs_file **out)
             }
             for (int i = 0; i < 3; i++) S.omegaoff[i] = tk.param("spin offset", &S.omega_state[i]) * D2R;
             const std::string type = tk.word("dataset type");
+            if (type == "lightcurve" || type == "heliocurve") {
+                read_lghtcrv_set(tk, S);
+                o->sets.push_back(std::move(S));
+                continue;
+            }
             if (type != "delay-doppler" && type != "doppler")
                 tk.fail("dataset type " + type + " is not supported", SHAPE_E_UNSUPPORTED);
             S.doppler = type == "doppler";
@@ -884,7 +983,7 @@ int shape_obs_nsets(const shape_obs_file *o) { return o ? (int)o->sets.size() : 
 int shape_obs_set_type(const shape_obs_file *o, int s)
 {
     if (!o || s < 0 || s >= (int)o->sets.size()) return shape::report_error(SHAPE_E_ARG, "obs_set_type: no such set");
-    return o->sets[s].doppler;
+    return o->sets[s].lightcurve ? 2 : o->sets[s].doppler;
 }
 
 int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *iradlaw, int *nframes,
@@ -914,6 +1013,7 @@ int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spi
     if (!o || s < 0 || s >= (int)o->sets.size() || !spin || !opt || !frames || !obs || !oneovervar)
         return shape::report_error(SHAPE_E_ARG, "obs_frames: invalid argument");
     const shape_obs_file::Set &S = o->sets[s];
+    if (S.lightcurve) return shape::report_error(SHAPE_E_ARG, "obs_frames: a lightcurve set (use shape_obs_lghtcrv)");
     if (S.doppler) return shape::report_error(SHAPE_E_ARG, "obs_frames: a Doppler set (use shape_obs_doppler)");
     const int nf = (int)S.frames.size();
     const size_t D = (size_t)S.ndel * S.ndop;
@@ -1008,6 +1108,87 @@ int shape_obs_doppler(const shape_obs_file *o, int s, const shape_spin_state *sp
         memcpy(frames[f].ae, &ae[9 * (size_t)f], sizeof frames[f].ae);
         memcpy(frames[f].spin, &sp[3 * (size_t)f], sizeof frames[f].spin);
     }
+    return SHAPE_OK;
+}
+
+int shape_obs_lghtcrv_info(const shape_obs_file *o, int s, int *ioptlaw, int *ncalc, int *n)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size() || !o->sets[s].lightcurve)
+        return shape::report_error(SHAPE_E_ARG, "obs_lghtcrv_info: not a lightcurve set");
+    const shape_obs_file::Set &S = o->sets[s];
+    if (ioptlaw) *ioptlaw = S.ioptlaw;
+    if (ncalc) *ncalc = (int)S.x0.size();
+    if (n) *n = (int)S.lc_t0.size();
+    return SHAPE_OK;
+}
+
+// A lightcurve set ready for shape_engine_add_lghtcrv_set, as read_lghtcrv
+// and realize_spin leave it (src/shape/read_dat.c:1856-1956, 2010-2029;
+// src/shape/realize_spin.c:223-260): each calculated epoch light-time
+// corrected through the ephemerides (x = x0 - DAYSPERAU * distance, the
+// view taken again there), its observer and Sun matrices and solar phase,
+// its body matrix from the spin state with the set's angle and spin
+// offsets; each observation's magnitude turned into an intensity relative
+// to the Sun's (sun_appmag, the .par file's value for this set's optical
+// law) and its epoch light-time corrected the same way.
+int shape_obs_lghtcrv(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
+                      const shape_obs_options *opt, double sun_appmag, shape_lghtcrv_set *set,
+                      shape_lghtcrv_point *points, double *x, double *t, double *obs, double *oneovervar)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size() || !o->sets[s].lightcurve || !spin || !opt || !set || !points ||
+        !x || !t || !obs || !oneovervar)
+        return shape::report_error(SHAPE_E_ARG, "obs_lghtcrv: invalid argument");
+    const shape_obs_file::Set &S = o->sets[s];
+    const double DAYSPERAU = 5.775518328e-3;   // src/shape/const.h:144
+    const double LN10 = 2.302585092994046;     // src/shape/const.h:133
+    const int nc = (int)S.x0.size(), n = (int)S.lc_t0.size();
+    const shape_ephem_point *A = S.ephem.data(), *U = S.solephem.data();
+    const int na = (int)S.ephem.size(), nu = (int)S.solephem.size();
+    std::vector<double> orb(3 * (size_t)nc), ae(9 * (size_t)nc), sp(3 * (size_t)nc);
+    for (int i = 0; i < nc; i++) {
+        shape_lghtcrv_point &P = points[i];
+        memset(&P, 0, sizeof P);
+        P.pos_n = pos_n;
+        P.km_per_pixel = km_per_pixel;
+        double az, dist;
+        x[i] = S.x0[i];
+        if (int rc = shape_ephem_view(A, na, U, nu, x[i], P.oe, P.se, &orb[3 * (size_t)i], &P.solar_phase, &az, &dist))
+            return rc;
+        if (opt->perform_ltc) {
+            x[i] = S.x0[i] - DAYSPERAU * dist;
+            if (int rc = shape_ephem_view(A, na, U, nu, x[i], P.oe, P.se, &orb[3 * (size_t)i], &P.solar_phase, &az,
+                                          &dist))
+                return rc;
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        const double intens = exp(-0.4 * LN10 * (S.lc_mag[i] - sun_appmag));
+        const double err = (0.4 * LN10 * S.lc_magerr[i]) * intens;
+        obs[i] = intens;
+        oneovervar[i] = 1.0 / (err * err);
+        t[i] = S.lc_t0[i];
+        if (opt->perform_ltc) {
+            double oe[9], se[9], os[3], ph, az, dist;
+            if (int rc = shape_ephem_view(A, na, U, nu, t[i], oe, se, os, &ph, &az, &dist)) return rc;
+            t[i] -= DAYSPERAU * dist;
+        }
+    }
+    if (int rc = shape_realize_spin(spin, S.angleoff, S.omegaoff, nc, x, orb.data(), ae.data(), sp.data()))
+        return rc;
+    for (int i = 0; i < nc; i++) memcpy(points[i].ae, &ae[9 * (size_t)i], sizeof points[i].ae);
+    shape_optical_law law = set->law;
+    memset(set, 0, sizeof *set);
+    set->law = law;
+    set->ncalc = nc;
+    set->n = n;
+    set->x = x;
+    set->t = t;
+    set->obs = obs;
+    set->oneovervar = oneovervar;
+    set->weight = S.lc_weight;
+    set->dof = S.lc_weight * n;
+    set->cal_floating = S.lc_cal_state == 'f';
+    set->cal = S.lc_cal;
     return SHAPE_OK;
 }
 

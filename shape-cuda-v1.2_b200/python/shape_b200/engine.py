@@ -151,6 +151,9 @@ def load_library(path=LIB_PATH):
     L.shape_obs_free.restype = None
     L.shape_obs_nsets.argtypes = [vp]
     L.shape_obs_set_type.argtypes = [vp, C.c_int]
+    L.shape_obs_lghtcrv_info.argtypes = [vp, C.c_int, P(C.c_int), P(C.c_int), P(C.c_int)]
+    L.shape_obs_lghtcrv.argtypes = [vp, C.c_int, P(cd.SpinState), C.c_int, C.c_double, P(ObsOptions), C.c_double,
+                                    P(cd.LghtcrvSet), P(cd.LghtcrvPoint), cd.dptr, cd.dptr, cd.dptr, cd.dptr]
     L.shape_obs_doppler.argtypes = [vp, C.c_int, P(cd.SpinState), C.c_int, C.c_double, P(ObsOptions),
                                     P(cd.DopplerSet), P(cd.DopplerFrame), cd.dptr, cd.dptr]
     L.shape_obs_set.argtypes = [vp, C.c_int, P(cd.DeldopSet), P(C.c_int), P(C.c_int), cd.dptr, cd.dptr,
@@ -564,8 +567,31 @@ class ObsFile:
                 "nelem": ne.value}
 
     def set_type(self, s):
-        """0: delay-Doppler set, 1: Doppler set."""
+        """0: delay-Doppler set, 1: Doppler set, 2: lightcurve set."""
         return _chk(self.L.shape_obs_set_type(self.h, s))
+
+    def lghtcrv_info(self, s):
+        law, nc, n = C.c_int(), C.c_int(), C.c_int()
+        _chk(self.L.shape_obs_lghtcrv_info(self.h, s, C.byref(law), C.byref(nc), C.byref(n)))
+        return {"ioptlaw": law.value, "ncalc": nc.value, "n": n.value}
+
+    def lghtcrv(self, s, spin, pos_n, km_per_pixel, sun_appmag=-26.75, perform_ltc=1, law=None):
+        """A lightcurve set: synth.LightcurveDataset ready for the engine."""
+        from . import synth
+        info = self.lghtcrv_info(s)
+        nc, n = info["ncalc"], info["n"]
+        st = cd.LghtcrvSet()
+        if law is not None:
+            st.law = law
+        pts = (cd.LghtcrvPoint * nc)()
+        x, t, obs, oov = np.zeros(nc), np.zeros(n), np.zeros(n), np.zeros(n)
+        opt = ObsOptions(perform_ltc, 1.0, 0, 1)
+        _chk(self.L.shape_obs_lghtcrv(self.h, s, C.byref(spin), int(pos_n), float(km_per_pixel), C.byref(opt),
+                                      float(sun_appmag), C.byref(st), pts, cd.as_dptr(x), cd.as_dptr(t),
+                                      cd.as_dptr(obs), cd.as_dptr(oov)))
+        ds = synth.LightcurveDataset(st, list(pts), x, t, obs, oov)
+        ds.bind()
+        return ds
 
     def doppler(self, s, spin, pos_n, km_per_pixel, nframes, ndop, perform_ltc=1, speckle=0, big_endian=1):
         """A Doppler set: (shape_doppler_set, frames, obs, 1/variance)."""

@@ -133,7 +133,7 @@ def test_obs_doppler_set_matches_reference(tmp_path, monkeypatch, speckle):
 def test_obs_refusals(tmp_path, monkeypatch):
     monkeypatch.chdir(tmp_path)
     p = tmp_path / "u.obs"
-    p.write_text(OBS.replace("delay-doppler", "lightcurve"))
+    p.write_text(OBS.replace("delay-doppler", "plane-of-sky"))
     with pytest.raises(eng.EngineError, match="error -4"):
         eng.ObsFile(p)
     p.write_text(OBS.replace("1 0.0 center", "3 60.0 center"))
@@ -216,3 +216,91 @@ def test_obs_tie_refusals(tmp_path, monkeypatch):
     p.write_text(OBS.replace("0                      { radar law }", "-1"))
     with pytest.raises(eng.EngineError, match="observation file line .*negative radar law"):
         eng.ObsFile(p)
+
+
+LC_SETS = """0
+c 0 c 0 c 10.0
+c 0 c 0 c 0.05
+lightcurve
+0
+3
+2018 3 14 0 0 0  359.5 10.2 0.031
+2018 3 15 0 0 0  0.4 10.0 0.030
+2018 3 16 0 0 0  1.1 9.8 0.029
+3
+2018 3 14 0 0 0  170.0 -5.0 0.99
+2018 3 15 0 0 0  171.0 -5.4 0.99
+2018 3 16 0 0 0  172.0 -5.8 0.99
+{CALC}
+1 0.0 center
+5 lc{K}.dat f 1.0 1.5
+"""
+
+HELIO_SET = """0
+= 0 c -2.0 c 0
+c 0 c 0 c 0
+heliocurve
+1
+3
+2018 3 14 0 0 0  10.0 2.0 1.02
+2018 3 15 0 0 0  10.5 2.1 1.02
+2018 3 16 0 0 0  11.0 2.2 1.02
+3
+2018 3 14 0 0 0  8.0 1.0 1.0
+2018 3 15 0 0 0  8.9 1.1 1.0
+2018 3 16 0 0 0  9.8 1.2 1.0
+-1
+1 0.0 first
+5 lc9.dat c 2.5 0.8
+"""
+
+
+@pytest.mark.parametrize("ltc", [1, 0])
+def test_obs_lightcurve_sets_match_reference(tmp_path, monkeypatch, ltc):
+    """Lightcurve sets with explicit, evenly spaced and observation-derived
+    calculated epochs, and a heliocurve set, against the reference's
+    read_lghtcrv and realize_spin (which read a heliocurve set's tables as a
+    lightcurve set's): epochs, observer / Sun / body matrices,
+    solar phases, intensities, 1/variance, weight, dof and calibration bit
+    for bit."""
+    monkeypatch.chdir(tmp_path)
+    write_mod(tmp_path / "m.mod", cases.c1()[0], seed=3)
+    rng = np.random.default_rng(31)
+    calcs = ["3\n2458191.8 2458192.3 2458192.9", "0\n2458191.75 2458193.0 0.25", "-1"]
+    text = "%d\n" % (len(calcs) + 1)
+    for k, calc in enumerate(calcs):
+        ep = np.sort(rng.uniform(2458191.8, 2458192.8, 5))
+        if k == 2:
+            ep[3] = ep[2]                       # a repeated epoch: calculated once
+        (tmp_path / ("lc%d.dat" % k)).write_text("".join("%.9f %.6f %.6f\n" % (e, 14 + rng.normal(0, 0.2), 0.02)
+                                                      for e in ep))
+        text += LC_SETS.replace("{CALC}", calc).replace("{K}", str(k))
+    (tmp_path / "lc9.dat").write_text("".join("%.9f %.6f %.6f\n" % (e, 13.5, 0.03)
+                                              for e in np.sort(rng.uniform(2458191.8, 2458192.8, 5))))
+    text += HELIO_SET
+    (tmp_path / "t.obs").write_text(text)
+    o = eng.ObsFile("t.obs")
+    spin = eng.ModFile("m.mod").spin()
+    ref = Reference()
+    h = ref.lib.ref_obs_read(b"m.mod", b"t.obs", ltc, 1.0, 0, 1)
+    for s in range(4):
+        assert o.set_type(s) == 2
+        info = o.lghtcrv_info(s)
+        sizes = (eng.C.c_int * 3)()
+        ref.lib.ref_obs_lghtcrv(h, s, sizes, None, None, None, None, None, None)
+        assert (info["ioptlaw"], info["ncalc"], info["n"]) == tuple(sizes), s
+        nc, n = info["ncalc"], info["n"]
+        x, pt, t, ob, ov, tail = (np.zeros(nc), np.zeros(28 * nc), np.zeros(n), np.zeros(n), np.zeros(n),
+                                  np.zeros(3))
+        ref.lib.ref_obs_lghtcrv(h, s, sizes, cd.as_dptr(x), cd.as_dptr(pt), cd.as_dptr(t), cd.as_dptr(ob),
+                                cd.as_dptr(ov), cd.as_dptr(tail))
+        ds = o.lghtcrv(s, spin, 60, 0.03, sun_appmag=-26.75, perform_ltc=ltc)
+        assert np.array_equal(ds.x, x), s
+        assert np.array_equal(ds.t, t) and np.array_equal(ds.obs, ob) and np.array_equal(ds.oneovervar, ov), s
+        for i, p in enumerate(ds.points):
+            g = pt[28 * i:28 * (i + 1)]
+            assert list(p.oe) == list(g[0:9]) and list(p.se) == list(g[9:18]) and list(p.ae) == list(g[18:27]), (s, i)
+            assert p.solar_phase == g[27], (s, i)
+        assert (ds.set.weight, ds.set.dof, ds.set.cal) == tuple(tail), s
+        assert ds.set.cal_floating == (s < 3)
+    assert o.lghtcrv_info(2)["ncalc"] == 4          # five epochs, one repeated
