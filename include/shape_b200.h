@@ -86,6 +86,20 @@ int shape_engine_set_params(shape_engine *e, const shape_eval_params *p);
 int shape_engine_add_deldop_set(shape_engine *e, const shape_deldop_set *set,
                                 int nframes, const shape_deldop_frame *frames,
                                 const double *obs, const double *oneovervar);
+/* Appends a delay-Doppler set whose frames are each rendered from nviews
+ * views (smearing, src/shape/calc_fits.c:475-594; the views of read_dat's
+ * deldopview_t, src/shape/read_dat.c:868-899). views[f*nviews + k] is frame
+ * f's k-th view in the reference's rendering order (v0+1 .. v0+nviews modulo
+ * nviews), so the last one is the view at the frame's epoch; each view gives
+ * ae, oe, spin, deloff and dopoff, and the epoch view gives the frame's other
+ * fields. The fit image is the mean over the views; posbnd, the image limits
+ * and the seen marks are the epoch view's; each view whose footprint is too
+ * wide adds dof * log-factor / nviews to the badradar term. A frame with
+ * several views refuses shape_engine_set_frame_view, and an engine holding
+ * one refuses shape_engine_set_spin_model (SHAPE_E_UNSUPPORTED). */
+int shape_engine_add_deldop_set_views(shape_engine *e, const shape_deldop_set *set, int nframes, int nviews,
+                                      const shape_deldop_frame *views, const double *obs,
+                                      const double *oneovervar);
 int shape_engine_add_lghtcrv_set(shape_engine *e, const shape_lghtcrv_set *set,
                                  const shape_lghtcrv_point *points);
 /* Appends a Doppler set (calc_doppler / pos2doppler / chi2_doppler,

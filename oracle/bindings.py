@@ -58,6 +58,10 @@ class Oracle:
         L.orc_deldop_frame.argtypes = [P(cd.EvalParams), P(OrcReal), P(cd.DeldopSet),
                                        P(cd.DeldopFrame), cd.dptr, cd.dptr, P(OrcPos),
                                        cd.dptr, C.c_char_p, P(cd.DeldopResult)]
+        L.orc_deldop_frame_views.argtypes = [P(cd.EvalParams), P(OrcReal), P(cd.DeldopSet), C.c_int,
+                                             P(cd.DeldopFrame), cd.dptr, cd.dptr, P(OrcPos),
+                                             cd.dptr, C.c_char_p, P(cd.DeldopResult), P(C.c_int),
+                                             P(C.c_double)]
         L.orc_doppler_frame.argtypes = [P(cd.EvalParams), P(OrcReal), P(cd.DopplerSet),
                                         P(cd.DopplerFrame), cd.dptr, cd.dptr, P(OrcPos),
                                         cd.dptr, C.c_char_p, P(cd.DeldopResult)]
@@ -114,11 +118,22 @@ class Oracle:
             res = cd.DeldopResult()
             obs = np.ascontiguousarray(ds.frame_obs(f))
             oov = np.ascontiguousarray(ds.oneovervar[ds.offsets[f]:ds.offsets[f + 1]])
-            self.lib.orc_deldop_frame(C.byref(params), C.byref(R), C.byref(ds.set), C.byref(fr),
-                                      cd.as_dptr(obs), cd.as_dptr(oov), C.byref(pos),
-                                      cd.as_dptr(fit), seen, C.byref(res))
+            if getattr(ds, "views", None):
+                va = (cd.DeldopFrame * ds.nviews)(*ds.views[f])
+                bany, bterm = C.c_int(0), C.c_double(0.0)
+                self.lib.orc_deldop_frame_views(C.byref(params), C.byref(R), C.byref(ds.set), ds.nviews, va,
+                                                cd.as_dptr(obs), cd.as_dptr(oov), C.byref(pos),
+                                                cd.as_dptr(fit), seen, C.byref(res), C.byref(bany),
+                                                C.byref(bterm))
+                rd = cd.result_to_dict(res)
+                rd["badradar_any"], rd["badradar_term"] = bany.value, bterm.value
+            else:
+                self.lib.orc_deldop_frame(C.byref(params), C.byref(R), C.byref(ds.set), C.byref(fr),
+                                          cd.as_dptr(obs), cd.as_dptr(oov), C.byref(pos),
+                                          cd.as_dptr(fit), seen, C.byref(res))
+                rd = cd.result_to_dict(res)
             fits.append(fit)
-            results.append(cd.result_to_dict(res))
+            results.append(rd)
             if keep_pos:
                 poss.append(self.pos_arrays(pos))
             self.lib.orc_pos_free(C.byref(pos))
@@ -204,6 +219,8 @@ class Reference:
         L.ref_set_optical_law.argtypes = [C.c_void_p, P(cd.OpticalLaw)]
         L.ref_add_deldop_set.argtypes = [C.c_void_p, P(cd.DeldopSet), C.c_int,
                                          P(cd.DeldopFrame), cd.dptr, cd.dptr]
+        L.ref_add_deldop_set_views.argtypes = [C.c_void_p, P(cd.DeldopSet), C.c_int, C.c_int, C.c_int,
+                                               P(cd.DeldopFrame), cd.dptr, cd.dptr]
         L.ref_add_lghtcrv_set.argtypes = [C.c_void_p, P(cd.LghtcrvSet), P(cd.LghtcrvPoint)]
         L.ref_add_doppler_set.argtypes = [C.c_void_p, P(cd.DopplerSet), C.c_int,
                                           P(cd.DopplerFrame), cd.dptr, cd.dptr]
@@ -271,6 +288,12 @@ class Reference:
         if lghtcrvs:
             self.lib.ref_set_optical_law(h, C.byref(optical_law or lghtcrvs[0].set.law))
         for ds in deldops:
+            if getattr(ds, "views", None):
+                arr = ds.view_array()
+                keep.append(arr)
+                self.lib.ref_add_deldop_set_views(h, C.byref(ds.set), ds.nframes, ds.nviews, ds.v0, arr,
+                                                  cd.as_dptr(ds.obs), cd.as_dptr(ds.oneovervar))
+                continue
             arr = ds.frame_array()
             keep.append(arr)
             self.lib.ref_add_deldop_set(h, C.byref(ds.set), ds.nframes, arr,

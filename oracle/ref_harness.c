@@ -152,9 +152,14 @@ static void ref_copy_rm(double out[3][3], const double *in)
     for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) out[i][j] = in[3 * i + j];
 }
 
-int ref_add_deldop_set(void *h, const shape_deldop_set *ds, int nframes,
-                       const shape_deldop_frame *frames, const double *obs_all,
-                       const double *oov_all)
+/* A delay-Doppler set with nviews views per frame (smearing): views[f *
+ * nviews + k] is frame f's k-th view in rendering order, which calc_fits
+ * walks as v = (v0 + 1 + k) % nviews (src/shape/calc_fits.c:489-490), so it
+ * is stored at the reference's view index v; the frame-level fields come from
+ * the last (epoch) view, index v0. */
+int ref_add_deldop_set_views(void *h, const shape_deldop_set *ds, int nframes, int nviews, int v0,
+                             const shape_deldop_frame *views, const double *obs_all,
+                             const double *oov_all)
 {
     ref_session *S = h;
     if (S->dat.nsets >= S->nsets_cap) return -1;
@@ -170,14 +175,15 @@ int ref_add_deldop_set(void *h, const shape_deldop_set *ds, int nframes,
     dd->spb = ds->spb;
     dd->stride = ds->stride;
     dd->dopfftlen = ds->dopfftlen;
-    dd->nviews = 1;
-    dd->v0 = 0;
+    if (nviews < 1 || v0 < 0 || v0 >= nviews) return -1;
+    dd->nviews = nviews;
+    dd->v0 = v0;
     dd->nframes = nframes;
     dd->frame = calloc((size_t)nframes, sizeof(struct deldopfrm_t));
     size_t off = 0;
     double dof = 0.0;
     for (int f = 0; f < nframes; f++) {
-        const shape_deldop_frame *F = &frames[f];
+        const shape_deldop_frame *F = &views[(size_t)f * nviews + nviews - 1];
         struct deldopfrm_t *fr = &dd->frame[f];
         fr->ndel = F->ndel; fr->ndop = F->ndop;
         fr->delcom_vig = F->delcom_vig; fr->dopcom_vig = F->dopcom_vig;
@@ -197,12 +203,16 @@ int ref_add_deldop_set(void *h, const shape_deldop_set *ds, int nframes,
                 fr->fit[i][j] = 0.0;
             }
         off += (size_t)F->ndel * F->ndop;
-        fr->view = calloc(1, sizeof(struct deldopview_t));
-        ref_copy_rm(fr->view[0].ae, F->ae);
-        ref_copy_rm(fr->view[0].oe, F->oe);
-        for (int j = 0; j < 3; j++) fr->view[0].spin[j] = F->spin[j];
-        fr->view[0].deloff = F->deloff;
-        fr->view[0].dopoff = F->dopoff;
+        fr->view = calloc((size_t)nviews, sizeof(struct deldopview_t));
+        for (int k = 0; k < nviews; k++) {
+            const shape_deldop_frame *V = &views[(size_t)f * nviews + k];
+            struct deldopview_t *w = &fr->view[(v0 + 1 + k) % nviews];
+            ref_copy_rm(w->ae, V->ae);
+            ref_copy_rm(w->oe, V->oe);
+            for (int j = 0; j < 3; j++) w->spin[j] = V->spin[j];
+            w->deloff = V->deloff;
+            w->dopoff = V->dopoff;
+        }
         ref_alloc_pos(&fr->pos, F->pos_n, F->km_per_pixel, 0);
         dof += F->dof;
     }
@@ -211,6 +221,13 @@ int ref_add_deldop_set(void *h, const shape_deldop_set *ds, int nframes,
     S->dat.dof_deldop += dof;
     S->dat.dof += dof;
     return S->dat.nsets - 1;
+}
+
+int ref_add_deldop_set(void *h, const shape_deldop_set *ds, int nframes,
+                       const shape_deldop_frame *frames, const double *obs_all,
+                       const double *oov_all)
+{
+    return ref_add_deldop_set_views(h, ds, nframes, 1, 0, frames, obs_all, oov_all);
 }
 
 /* A Doppler set (struct doppler_t, src/shape/shape2.h:1266-1287) with one

@@ -807,6 +807,80 @@ void orc_deldop_frame(const shape_eval_params *par, const orc_real *real,
                    &res->cal, &res->chi2);
 }
 
+/* A smeared frame (src/shape/calc_fits.c:475-594): views[0..nviews-1] in
+ * rendering order (v0+1 .. v0+nviews modulo nviews, the epoch view last),
+ * each cleared, rendered by posvis and mapped by pos2deldop into its own fit;
+ * the frame's fit is the sum over views divided by nviews (summed in view
+ * order). posbnd, the seen marks and the limits are the epoch view's; each
+ * view whose footprint is too wide adds dof * log-factor / nviews to
+ * *badradar_term in view order, and sets *badradar_any. res holds the epoch
+ * view's own flags and the chi-square of the mean fit. */
+void orc_deldop_frame_views(const shape_eval_params *par, const orc_real *real,
+                            const shape_deldop_set *set, int nviews, const shape_deldop_frame *views,
+                            const double *obs, const double *oneovervar,
+                            orc_pos *pos, double *fit, unsigned char *seen,
+                            shape_deldop_result *res, int *badradar_any, double *badradar_term)
+{
+    const double zero3[3] = {0.0, 0.0, 0.0};
+    const shape_deldop_frame *ep = &views[nviews - 1];
+    const size_t D = (size_t)ep->ndel * (size_t)ep->ndop;
+    double *store = calloc(D, sizeof(double));
+    *badradar_any = 0;
+    *badradar_term = 0.0;
+    for (int k = 0; k < nviews; k++) {
+        const shape_deldop_frame *V = &views[k];
+        const int epoch = (k == nviews - 1);
+        memcpy(pos->ae, V->ae, sizeof pos->ae);
+        memcpy(pos->oe, V->oe, sizeof pos->oe);
+        pos->kmpp = ep->km_per_pixel;
+        pos->bistatic = 0;
+        orc_posclr(pos);
+        int ob = orc_posvis(real, zero3, pos, par->pos_smooth, 0);
+        if (epoch) {
+            res->outbnd = ob;
+            res->posbnd_logfactor = pos->posbnd_logfactor;
+        }
+        const int n = pos->n, side = 2 * n + 1;
+        if (epoch && seen && par->mark_seen)
+            for (int i = pos->xlim[0]; i <= pos->xlim[1]; i++)
+                for (int l = pos->ylim[0]; l <= pos->ylim[1]; l++) {
+                    size_t p = (size_t)(i + n) * side + (size_t)(l + n);
+                    if (pos->cose[p] > par->mincosine_seen && pos->f[p] >= 0)
+                        seen[pos->f[p]] = 1;
+                }
+        /* the view's own fields with the frame's sizes and COM bins */
+        shape_deldop_frame fv = *ep;
+        memcpy(fv.ae, V->ae, sizeof fv.ae);
+        memcpy(fv.oe, V->oe, sizeof fv.oe);
+        memcpy(fv.spin, V->spin, sizeof fv.spin);
+        fv.deloff = V->deloff;
+        fv.dopoff = V->dopoff;
+        shape_deldop_result rv = *res;
+        memset(fit, 0, sizeof(double) * D);
+        orc_pos2deldop(par, set, &fv, pos, fit, &rv);
+        if (rv.badradar) {
+            *badradar_any = 1;
+            *badradar_term += ep->dof * rv.badradar_logfactor / nviews;
+        }
+        res->badradar = rv.badradar;
+        res->badradar_logfactor = rv.badradar_logfactor;
+        for (size_t i = 0; i < D; i++) store[i] += fit[i];
+        if (epoch) {
+            res->xlim[0] = pos->xlim[0]; res->xlim[1] = pos->xlim[1];
+            res->ylim[0] = pos->ylim[0]; res->ylim[1] = pos->ylim[1];
+            memcpy(res->idellim, rv.idellim, sizeof res->idellim);
+            memcpy(res->idoplim, rv.idoplim, sizeof res->idoplim);
+            memcpy(res->dellim, rv.dellim, sizeof res->dellim);
+            memcpy(res->doplim, rv.doplim, sizeof res->doplim);
+        }
+    }
+    for (size_t i = 0; i < D; i++) fit[i] = store[i] / nviews;
+    free(store);
+    orc_chi2_frame(obs, oneovervar, fit, ep->ndel * ep->ndop, ep->weight,
+                   ep->cal_floating, ep->cal, &res->o2, &res->m2, &res->om,
+                   &res->cal, &res->chi2);
+}
+
 /* calc_doppler for one frame (src/shape/calc_fits.c:860-935) then its chi2. */
 void orc_doppler_frame(const shape_eval_params *par, const orc_real *real,
                        const shape_doppler_set *set, const shape_doppler_frame *frm,

@@ -85,6 +85,17 @@ void orc_deldop_frame(const shape_eval_params *par, const orc_real *real,
                       orc_pos *pos, double *fit, unsigned char *seen,
                       shape_deldop_result *res);
 
+/* A smeared delay-Doppler frame (src/shape/calc_fits.c:475-594): views in
+ * rendering order, the epoch view last; fit receives the mean over the
+ * views. *badradar_term is the frame's badradar contribution (dof *
+ * log-factor / nviews summed over the views flagged) and *badradar_any its
+ * flag; res holds the epoch view's posbnd, limits and the chi-square terms. */
+void orc_deldop_frame_views(const shape_eval_params *par, const orc_real *real,
+                            const shape_deldop_set *set, int nviews, const shape_deldop_frame *views,
+                            const double *obs, const double *oneovervar,
+                            orc_pos *pos, double *fit, unsigned char *seen,
+                            shape_deldop_result *res, int *badradar_any, double *badradar_term);
+
 /* One calculated lightcurve point of calc_lghtcrv
  * (src/shape/calc_fits.c:1629-1716): returns y[i]. outbnd_logsum receives the
  * 0.5-weighted posbnd log-factor sum for this point and *outbnd the flag. */

@@ -547,6 +547,19 @@ __global__ void k_lc_photo(LcArgs a)
     }
 }
 
+// A radar frame's badradar term of the objective (src/shape/calc_fits.c:
+// 545-550): dof * log-factor / views, summed over the views whose
+// footprint was too wide; the flag when any of them was. One view: the
+// frame's own result (which includes a Doppler frame's overflow term).
+__device__ inline double frame_blog(const FrameHost &h, double frame_lf)
+{
+    return h.nviews > 1 ? h.dof * h.badradar_lfsum / h.nviews : h.dof * frame_lf / 1;
+}
+__device__ inline bool frame_bad(const FrameHost &h, int frame_bad)
+{
+    return frame_bad || (h.nviews > 1 && h.badradar_any);
+}
+
 // posbnd_logfactor of one POS view (src/shape/posvis.c:301-307).
 __device__ double view_logfactor(const FrameGeom &g, const FrameState &st)
 {
@@ -733,8 +746,8 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
         if (use_sm) {
             s_chi2[fr] = r.chi2;
             s_plog[fr] = a.fh[fr].dof * r.posbnd_logfactor;
-            s_blog[fr] = a.fh[fr].dof * r.badradar_logfactor / 1;
-            s_flag[fr] = (r.outbnd ? 1 : 0) | (r.badradar ? 2 : 0);
+            s_blog[fr] = frame_blog(a.fh[fr], r.badradar_logfactor);
+            s_flag[fr] = (r.outbnd ? 1 : 0) | (frame_bad(a.fh[fr], r.badradar) ? 2 : 0);
         }
     }
     __syncthreads();
@@ -748,8 +761,8 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
             const shape_deldop_result &r = a.results[f];
             c = r.chi2;
             pl = a.fh[f].dof * r.posbnd_logfactor;
-            bl = a.fh[f].dof * r.badradar_logfactor / 1;
-            fl = (r.outbnd ? 1 : 0) | (r.badradar ? 2 : 0);
+            bl = frame_blog(a.fh[f], r.badradar_logfactor);
+            fl = (r.outbnd ? 1 : 0) | (frame_bad(a.fh[f], r.badradar) ? 2 : 0);
         });
 }
 
@@ -945,8 +958,8 @@ __global__ void __launch_bounds__(CHI2_THREADS) k_chi2_summary(Chi2Args ca, Fina
                     const shape_deldop_result *r = fa.results + f;
                     s_chi2[f] = __ldcg(&r->chi2);
                     s_plog[f] = fa.fh[f].dof * __ldcg(&r->posbnd_logfactor);
-                    s_blog[f] = fa.fh[f].dof * __ldcg(&r->badradar_logfactor) / 1;
-                    s_flag[f] = (__ldcg(&r->outbnd) ? 1 : 0) | (__ldcg(&r->badradar) ? 2 : 0);
+                    s_blog[f] = frame_blog(fa.fh[f], __ldcg(&r->badradar_logfactor));
+                    s_flag[f] = (__ldcg(&r->outbnd) ? 1 : 0) | (frame_bad(fa.fh[f], __ldcg(&r->badradar)) ? 2 : 0);
                 }
                 __syncthreads();
                 if (threadIdx.x == 0)

@@ -187,7 +187,8 @@ int EngineImpl::finalize()
 
     const int nframes = (int)frames.size();
     const int npts = (int)points.size();
-    nviews = nframes + 2 * npts;
+    nviews = 2 * npts;
+    for (int fi = 0; fi < nframes; fi++) nviews += fviews[fi].empty() ? 1 : (int)fviews[fi].size();
     int tile_base = 0;
     long long pos_base = 0;
     auto add_view = [&](FrameGeom &g, int n, double kmpp) {
@@ -237,8 +238,33 @@ int EngineImpl::finalize()
             h.dof = F.dof;
             h.cal_in = F.cal;
             h.cal_floating = F.cal_floating;
+            // a smeared frame's views in the reference's order, its epoch
+            // view last (src/shape/calc_fits.c:489-490): each rasterized
+            // into the same fit image at 1/views of its cross-section; the
+            // frame's limits, posbnd and seen marks are the epoch view's
+            const std::vector<shape_deldop_frame> &V = fviews[fi];
+            const int nview = V.empty() ? 1 : (int)V.size();
+            h.nviews = nview;
+            for (int k2 = 0; k2 + 1 < nview; k2++) {
+                FrameGeom gv = g;
+                FrameHost hv = h;
+                double dxv;
+                radar_view_geom(gv, hv, dxv, V[k2], S);
+                gv.wscale = 1.0 / nview;
+                gv.no_seen = 1;
+                if (hv.badradar) {
+                    h.badradar_any = 1;
+                    h.badradar_lfsum += hv.badradar_logfactor;
+                }
+                add_view(gv, F.pos_n, F.km_per_pixel);
+            }
             double dx;
             radar_view_geom(g, h, dx, F, S);
+            g.wscale = 1.0 / nview;
+            if (h.badradar) {
+                h.badradar_any = 1;
+                h.badradar_lfsum += h.badradar_logfactor;
+            }
             dop_extra.push_back(dx);
             h.view = (int)geoms.size();
             h.set = (int)s;
@@ -289,6 +315,7 @@ int EngineImpl::finalize()
             FrameGeom go, gs;
             memset(&go, 0, sizeof go);
             memset(&gs, 0, sizeof gs);
+            go.wscale = gs.wscale = 1.0;
             lc_view_geom(go, gs, pd, P);
             go.kind = VIEW_LC_OBS;
             go.smooth = params.pos_smooth;
@@ -486,6 +513,8 @@ int EngineImpl::set_frame_view(int fi, const double ae[9], const double oe[9], c
                                double deloff, double dopoff)
 {
     if (fi < 0 || fi >= (int)frames.size()) return set_err(SHAPE_E_ARG, "set_frame_view: frame out of range");
+    if (!fviews[fi].empty())
+        return set_err(SHAPE_E_UNSUPPORTED, "set_frame_view: the frame has several views (smearing)");
     shape_deldop_frame &F = frames[fi];
     memcpy(F.ae, ae, sizeof F.ae);
     memcpy(F.oe, oe, sizeof F.oe);
@@ -571,6 +600,8 @@ int EngineImpl::realize_views()
 {
     if (spin_angleoff.size() != 3 * setrecs.size() || frame_t.size() != frames.size())
         return set_err(SHAPE_E_STATE, "spin model: datasets were added after set_spin_model");
+    for (const auto &V : fviews)
+        if (!V.empty()) return set_err(SHAPE_E_UNSUPPORTED, "spin model: a frame has several views (smearing)");
     std::vector<double> ae, sp, zero;
     for (size_t r = 0; r < setrecs.size(); r++) {
         const double *ao = &spin_angleoff[3 * r], *oo = &spin_omegaoff[3 * r];
@@ -991,7 +1022,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
             rv.nwork = view_nwork[v];
             launch_raster_f64(rv, s);
             const FrameGeom &g = geoms[v];
-            if (g.kind == VIEW_RADAR) {
+            if (g.kind == VIEW_RADAR && fh[g.frame_index].view == v) {
                 const FrameHost &h = fh[g.frame_index];
                 Chi2Args cv = ca;
                 cv.items = d_chi2_items + h.item0;
@@ -1114,7 +1145,8 @@ int EngineImpl::kernels_per_eval(int form) const
     int n = 2 + 1;                       // realize (vertices + facets, vertex normals), state reset
     if (form == SHAPE_FORM_PLAIN_FP64) {
         for (int v = 0; v < nviews; v++)
-            n += 3 + (geoms[v].kind == VIEW_RADAR || geoms[v].kind == VIEW_LC_SUN ? 1 : 0);
+            n += 3 + ((geoms[v].kind == VIEW_RADAR && fh[geoms[v].frame_index].view == v) ||
+                              geoms[v].kind == VIEW_LC_SUN ? 1 : 0);
     } else {
         n += 3;                          // transform, bin, raster
         if (form == SHAPE_FORM_BATCHED_FP32 && work_radar > 0 && work_radar < (int)work.size())
@@ -1331,6 +1363,7 @@ int shape_engine_add_deldop_set(shape_engine *h, const shape_deldop_set *set, in
         E.oov.insert(E.oov.end(), oov + off, oov + off + D);
         off += D;
         E.frames.push_back(F);
+        E.fviews.emplace_back();
         E.frame_sdev.push_back(0.0);
         E.dof += F.dof;
         E.dof_deldop += F.dof;
@@ -1339,6 +1372,43 @@ int shape_engine_add_deldop_set(shape_engine *h, const shape_deldop_set *set, in
     E.dd.push_back(d);
     E.finalized = false;
     return (int)E.setrecs.size() - 1;
+}
+
+// A delay-Doppler set whose frames are each rendered from several views
+// (smearing, src/shape/calc_fits.c:475-594): views[f * nviews + k] is frame
+// f's k-th view in the order the reference renders them, v0+1 .. v0+nviews
+// modulo nviews, so the last is the view at the frame's epoch. A view
+// supplies ae, oe, spin, deloff and dopoff (struct deldopview_t); the frame's
+// other fields (sizes, weight, dof, calibration, COM and DC bins) are the
+// epoch view's.
+int shape_engine_add_deldop_set_views(shape_engine *h, const shape_deldop_set *set, int nframes, int nviews,
+                                      const shape_deldop_frame *views, const double *obs, const double *oov)
+{
+    if (!h || !set || nframes <= 0 || nviews < 1 || !views || !obs || !oov)
+        return shape::set_err(SHAPE_E_ARG, "add_deldop_set_views: invalid argument");
+    std::vector<shape_deldop_frame> ep((size_t)nframes);
+    for (int k = 0; k < nframes; k++) ep[k] = views[(size_t)k * nviews + nviews - 1];
+    EngineImpl &E = h->impl;
+    const int f0 = (int)E.frames.size();
+    int rc = shape_engine_add_deldop_set(h, set, nframes, ep.data(), obs, oov);
+    if (rc < 0 || nviews == 1) return rc;
+    E.dd.back().nviews = nviews;
+    for (int k = 0; k < nframes; k++) {
+        const shape_deldop_frame *V = views + (size_t)k * nviews;
+        std::vector<shape_deldop_frame> &fv = E.fviews[f0 + k];
+        fv.assign(V, V + nviews);
+        for (shape_deldop_frame &w : fv) {
+            // the frame-level fields are the epoch view's
+            shape_deldop_frame x = ep[k];
+            memcpy(x.ae, w.ae, sizeof x.ae);
+            memcpy(x.oe, w.oe, sizeof x.oe);
+            memcpy(x.spin, w.spin, sizeof x.spin);
+            x.deloff = w.deloff;
+            x.dopoff = w.dopoff;
+            w = x;
+        }
+    }
+    return rc;
 }
 
 // A Doppler set runs as a delay-Doppler set of one-row frames (LONG_ORIG,
@@ -1382,6 +1452,7 @@ int shape_engine_add_doppler_set(shape_engine *h, const shape_doppler_set *set, 
         E.oov.insert(E.oov.end(), oov + off, oov + off + P.ndop);
         off += (size_t)P.ndop;
         E.frames.push_back(F);
+        E.fviews.emplace_back();
         E.frame_sdev.push_back(P.sdev);
         E.dof += P.dof;
         E.dof_doppler += P.dof;

@@ -66,6 +66,7 @@ struct DdSetHost {
     shape_deldop_set set;       // a Doppler set is held as a one-row delay-Doppler set
     int frame0, nframes;
     int doppler = 0;            // 1: Doppler spectra (shape_engine_add_doppler_set)
+    int nviews = 1;             // views per frame (smearing); frames[] holds each frame's epoch view
 };
 struct LcSetHost {
     shape_lghtcrv_set set;
@@ -96,6 +97,9 @@ struct EngineImpl {
     // datasets (host)
     std::vector<DdSetHost> dd;
     std::vector<shape_deldop_frame> frames;
+    // per frame: its views in the order the reference renders them (the
+    // epoch view last); empty for a frame with one view
+    std::vector<std::vector<shape_deldop_frame>> fviews;
     std::vector<long long> frame_off;   // element offsets into obs/oov/fit
     std::vector<double> obs, oov;
     std::vector<LcSetHost> lc;
@@ -242,6 +246,7 @@ struct EngineImpl {
         fv = o.fv; af_ptr = o.af_ptr; af_idx = o.af_idx; have_model = o.have_model;
         params = o.params; bad_objfactor = o.bad_objfactor;
         dd = o.dd; frames = o.frames; frame_off = o.frame_off; obs = o.obs; oov = o.oov;
+        fviews = o.fviews;
         lc = o.lc; points = o.points; setrecs = o.setrecs;
         dof = o.dof; dof_deldop = o.dof_deldop; dof_doppler = o.dof_doppler; dof_lghtcrv = o.dof_lghtcrv;
         frame_sdev = o.frame_sdev;

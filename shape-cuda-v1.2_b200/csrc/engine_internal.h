@@ -38,6 +38,8 @@ struct FrameGeom {
     double oa[9];        // observer(or sun) <- body, row-major, reference op order
     double usrc[3];      // sun direction in observer coords (VIEW_LC_OBS)
     double off[3];       // orbit offset added to the view-frame vertices (posvis's orbit_offset; 0 here otherwise)
+    double wscale;       // weight of this view's cross-section in its frame: 1 / views of a smeared frame
+    int no_seen;         // 1: a smeared frame's view other than the frame's epoch view (marks no seen facets)
     double kmpp;
     int n, side;         // POS half width, 2n+1
     int tiles_x;         // tiles per POS side

@@ -132,6 +132,13 @@ struct FrameHost {             // per radar frame constants for finalize
     int item0, nitems;
     int dop_index;             // Doppler frame: index of its overflow terms, else -1
     double sdev;               // Doppler frame: receiver noise sdev (overflow variance)
+    // smeared frames (src/shape/calc_fits.c:475-594): views, whether any
+    // view's footprint was too wide, and the sum of those views'
+    // badradar log-factors (the objective adds dof * sum / views); the
+    // frame's own badradar and badradar_logfactor are its epoch view's
+    int nviews;
+    int badradar_any;
+    double badradar_lfsum;
 };
 struct FinalizeArgs {
     int nframes;

@@ -171,6 +171,7 @@ static int posvis_impl(int device, const shape_pos_view *view, shape_pos_images 
     g.side = side;
     g.tiles_x = tiles_x;
     g.kind = src ? VIEW_LC_SUN : (view->bistatic ? VIEW_LC_OBS : VIEW_POS);
+    g.wscale = 1.0;
     g.smooth = smooth ? 1 : 0;
 
     // model arrays in the engine's layout
@@ -327,8 +328,8 @@ __global__ void k_pos2deldop(P2dArgs a)
         d.dopPOS = kc.ax * ((double)xi - a.xoff) + kc.ay * ((double)yj - a.yoff) + kc.dopshift;
         d.idop_min = (int)floor(d.dopPOS - kc.dopdiff_max + 1 - kc.half_w);
         d.idop_max = (int)floor(d.dopPOS + kc.dopdiff_max + kc.half_w);
-        d.codefactor = (g.codemethod == SHAPE_CODE_SHORT) ? sinc2<double>((d.dopPOS - kc.dopDC_vig) / kc.dopfftlen)
-                                                          : 1.0;
+        d.codefactor = ((g.codemethod == SHAPE_CODE_SHORT) ? sinc2<double>((d.dopPOS - kc.dopDC_vig) / kc.dopfftlen)
+                                                           : 1.0) * g.wscale;
         pp.dop = d.dopPOS;
         d.ok = (d.idel_min >= 1) && (d.idel_max <= g.ndel) && (d.idop_min >= 1) && (d.idop_max <= g.ndop) &&
                (d.idel_max - d.idel_min + 1 <= SHAPE_MAXBINS);
@@ -371,6 +372,7 @@ static int pos2deldop_impl(int device, const shape_pos_view *view, const shape_p
     FrameGeom g;
     memset(&g, 0, sizeof g);
     g.kind = VIEW_RADAR;
+    g.wscale = 1.0;
     g.n = n;
     g.side = side;
     g.kmpp = view->km_per_pixel;

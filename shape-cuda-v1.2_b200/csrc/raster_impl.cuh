@@ -404,8 +404,10 @@ __device__ PixDD<T> pixel_dd_setup(const FrameGeom &g, const DDC<T> &k, int x, i
     const T half_w = k.half_w;
     d.idop_min = (int)floor(d.dopPOS - dopdiff_max + 1 - half_w);
     d.idop_max = (int)floor(d.dopPOS + dopdiff_max + half_w);
-    d.codefactor = (g.codemethod == SHAPE_CODE_SHORT)
-                       ? sinc2<T>((d.dopPOS - k.dopDC_vig) / k.dopfftlen) : (T)1;
+    // a smeared frame's view adds 1/views of its cross-section (wscale; 1
+    // for a frame of one view)
+    d.codefactor = ((g.codemethod == SHAPE_CODE_SHORT)
+                       ? sinc2<T>((d.dopPOS - k.dopDC_vig) / k.dopfftlen) : (T)1) * (T)g.wscale;
     pp.del = (double)d.delPOS;
     pp.dop = (double)d.dopPOS;
     d.ok = (d.idel_min >= 1) && (d.idel_max <= g.ndel) && (d.idop_min >= 1) && (d.idop_max <= g.ndop) &&
@@ -432,8 +434,8 @@ __device__ inline PixDD<float> pixel_dd_setup_x(const FrameGeom &g, int x, int y
     d.ddel0 = (float)(del - (double)d.idel_min);
     d.ddop0 = (float)(dop - (double)d.idop_min);
     d.dfrac = (float)(dop - floor(dop));
-    d.codefactor = (g.codemethod == SHAPE_CODE_SHORT) ? sinc2<float>((float)((dop - g.dopDC_vig) / g.dopfftlen))
-                                                       : 1.0f;
+    d.codefactor = ((g.codemethod == SHAPE_CODE_SHORT) ? sinc2<float>((float)((dop - g.dopDC_vig) / g.dopfftlen))
+                                                        : 1.0f) * (float)g.wscale;
     pp.del = del;
     pp.dop = dop;
     d.ok = (d.idel_min >= 1) && (d.idel_max <= g.ndel) && (d.idop_min >= 1) && (d.idop_max <= g.ndop) &&
@@ -1168,7 +1170,7 @@ k_raster(RasterArgs a)
         dd.ok = false;
         T scose = 0;
         if (g.kind == VIEW_RADAR && covered) {
-            if (a.mark_seen && (double)cosa > a.mincosine_seen)
+            if (a.mark_seen && !g.no_seen && (double)cosa > a.mincosine_seen)
                 a.seen[fac] = 1;
         }
         const DDC<T> kc = load_ddc<T>(g);
@@ -1536,7 +1538,7 @@ k_raster_w(RasterArgs a)
             }
         }
         if (g.kind == VIEW_RADAR) {
-            if (covered && a.mark_seen && (double)cosa > a.mincosine_seen) a.seen[fac] = 1;
+            if (covered && a.mark_seen && !g.no_seen && (double)cosa > a.mincosine_seen) a.seen[fac] = 1;
             const DDC<T> kc = load_ddc<T>(g);
             PixPos pp = {0.0, 0.0};
             PixDD<T> dd;

@@ -102,6 +102,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_set_params.argtypes = [vp, P(cd.EvalParams)]
     L.shape_engine_add_deldop_set.argtypes = [vp, P(cd.DeldopSet), C.c_int, P(cd.DeldopFrame),
                                               cd.dptr, cd.dptr]
+    L.shape_engine_add_deldop_set_views.argtypes = [vp, P(cd.DeldopSet), C.c_int, C.c_int, P(cd.DeldopFrame),
+                                                    cd.dptr, cd.dptr]
     L.shape_engine_add_lghtcrv_set.argtypes = [vp, P(cd.LghtcrvSet), P(cd.LghtcrvPoint)]
     L.shape_engine_add_doppler_set.argtypes = [vp, P(cd.DopplerSet), C.c_int, P(cd.DopplerFrame),
                                                cd.dptr, cd.dptr]
@@ -243,10 +245,17 @@ class Engine:
         _chk(self.L.shape_engine_set_params(self.h, C.byref(params)))
 
     def add_deldop(self, ds):
-        arr = ds.frame_array()
-        self._keep.append(arr)
-        idx = _chk(self.L.shape_engine_add_deldop_set(self.h, C.byref(ds.set), ds.nframes, arr,
-                                                      cd.as_dptr(ds.obs), cd.as_dptr(ds.oneovervar)))
+        if getattr(ds, "views", None):
+            arr = ds.view_array()
+            self._keep.append(arr)
+            idx = _chk(self.L.shape_engine_add_deldop_set_views(self.h, C.byref(ds.set), ds.nframes, ds.nviews,
+                                                                arr, cd.as_dptr(ds.obs),
+                                                                cd.as_dptr(ds.oneovervar)))
+        else:
+            arr = ds.frame_array()
+            self._keep.append(arr)
+            idx = _chk(self.L.shape_engine_add_deldop_set(self.h, C.byref(ds.set), ds.nframes, arr,
+                                                          cd.as_dptr(ds.obs), cd.as_dptr(ds.oneovervar)))
         self.deldops.append(ds)
         self.set_index.append(("deldop", len(self.deldops) - 1))
         return idx

@@ -269,14 +269,27 @@ class DeldopDataset:
     obs: np.ndarray          # concatenated [sum ndel*ndop]
     oneovervar: np.ndarray
     offsets: np.ndarray      # [nframes+1] element offsets into obs
+    # smearing: per frame, its views in rendering order (the epoch view,
+    # frames[f], last); None for one view per frame
+    views: list = None
+    v0: int = 0              # the epoch view's index among the reference's views
 
     @property
     def nframes(self):
         return len(self.frames)
 
+    @property
+    def nviews(self):
+        return len(self.views[0]) if self.views else 1
+
     def frame_array(self):
         arr = (cd.DeldopFrame * len(self.frames))(*self.frames)
         return arr
+
+    def view_array(self):
+        """Every frame's views back to back (frame-major, rendering order)."""
+        flat = [v for fv in self.views for v in fv]
+        return (cd.DeldopFrame * len(flat))(*flat)
 
     def frame_obs(self, f):
         return self.obs[self.offsets[f]:self.offsets[f + 1]]
@@ -421,6 +434,42 @@ def batched_dataset(nframes=64, pos_range=(101, 301), ndel_range=(64, 256),
         delcom = 0.5 * ndel + 0.5 * (KM2US * radius / dset.del_per_pixel)
         frames.append(_frame(n, kmpp, ae, oe, omega * pole, ndel, ndop, delcom, 0.5 * ndop + 0.5))
     return _finish_deldop(dset, frames, synthesize, 20.0, 1.0, 1234, params)
+
+
+def smeared_dataset(nframes=4, nviews=3, v0=1, view_interval=0.004, pos_n=75, synthesize=None,
+                    params=None, seed=11):
+    """Delay-Doppler frames rendered from nviews views each (smearing): view k
+    of the reference's numbering sits at t0 + (k - v0) * view_interval days
+    (src/shape/read_dat.c:868-873), so its body rotates by omega times that;
+    each view carries its own small delay / Doppler correction. The views are
+    listed in rendering order, v0+1 .. v0+nviews modulo nviews, ending with
+    the epoch view."""
+    params = params or eval_params()
+    rng = np.random.default_rng(seed)
+    pole = ecl_dir(30.0, 60.0)
+    omega = 2 * math.pi / 0.25
+    to_earth = ecl_dir(0.0, 10.0)
+    oe = observer_matrix(to_earth)
+    dset = cd.DeldopSet()
+    dset.del_per_pixel, dset.dop_per_pixel = 0.1, 0.1
+    dset.Ftx, dset.dopscale = 2380.0, 1.0
+    dset.codemethod, dset.spb, dset.stride, dset.dopfftlen = 1, 1, 1, 64
+    dset.law = radar_cosine()
+    frames, views = [], []
+    for f in range(nframes):
+        phase0 = 0.7 + 2 * math.pi * f / nframes
+        fv = [None] * nviews
+        for k in range(nviews):
+            fr = _frame(pos_n, 2.25 / 150.0, body_matrix(pole, phase0 + omega * (k - v0) * view_interval),
+                        oe, omega * pole, 100, 100, 70.0, 50.5)
+            fr.deloff, fr.dopoff = rng.uniform(-0.3, 0.3, 2)
+            fv[k] = fr
+        order = [(v0 + 1 + j) % nviews for j in range(nviews)]
+        views.append([fv[k] for k in order])
+        frames.append(fv[v0])
+    ds = _finish_deldop(dset, frames, synthesize, 20.0, 1.0, 1234 + nviews, params)
+    ds.views, ds.v0 = views, v0
+    return ds
 
 
 def config2_dataset(synthesize=None, params=None):
