@@ -80,6 +80,16 @@ void *dh_pos_new(int n, double kmpp, const double *ae, const double *oe, const d
     pos->cosill = matrix(-n, n, -n, n); pos->zill = matrix(-n, n, -n, n);
     pos->bodyill = imatrix(-n, n, -n, n); pos->compill = imatrix(-n, n, -n, n); pos->fill = imatrix(-n, n, -n, n);
     pos->bistatic = bistatic;
+    /* matrix() leaves the rows uninitialized and posclr only clears the
+     * sun view's images of a bistatic frame: a fixed fill makes two frames
+     * comparable, and shows any write to images the routines must not touch */
+    for (int i = -n; i <= n; i++)
+        for (int j = -n; j <= n; j++) {
+            pos->b[i][j] = pos->cose[i][j] = pos->cosi[i][j] = pos->z[i][j] = 0.25;
+            pos->cosill[i][j] = pos->zill[i][j] = 0.25;
+            pos->body[i][j] = pos->comp[i][j] = pos->f[i][j] = -7;
+            pos->bodyill[i][j] = pos->compill[i][j] = pos->fill[i][j] = -7;
+        }
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) {
             pos->ae[i][j] = ae[3 * i + j]; pos->oe[i][j] = oe[3 * i + j]; pos->se[i][j] = se[3 * i + j];
