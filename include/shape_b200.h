@@ -641,10 +641,22 @@ int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *ir
  * (shape_read_radar_data), the weight, dof and calibration. pos_n and
  * km_per_pixel come from the .par file. obs and oneovervar receive each
  * frame's image in frame order (nelem doubles); sdev (or NULL) each
- * frame's sdev. */
+ * frame's sdev. A set with several views per frame (smearing) returns
+ * SHAPE_E_UNSUPPORTED here: read it with shape_obs_frames_views. */
 int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
                      const shape_obs_options *opt, shape_deldop_frame *frames, double *obs, double *oneovervar,
                      double *sdev);
+/* Views per frame of set s and the index v0 of the view at the frame's
+ * epoch (smearing mode center: nviews / 2, first: 0; src/shape/read_dat.c:
+ * 635-646). */
+int shape_obs_views(const shape_obs_file *o, int s, int *nviews, int *v0);
+/* Set s's frames for shape_engine_add_deldop_set_views: nframes * nviews
+ * views, each built as shape_obs_frames builds a frame at the view's epoch
+ * t0 + (k - v0) * view interval (src/shape/read_dat.c:868-899), listed per
+ * frame in rendering order (views (v0+1+j) % nviews, the epoch view last). */
+int shape_obs_frames_views(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n,
+                           double km_per_pixel, const shape_obs_options *opt, shape_deldop_frame *views, double *obs,
+                           double *oneovervar, double *sdev);
 
 /* A Doppler set's setup (set->law is kept) and frames for
  * shape_engine_add_doppler_set, built as shape_obs_frames builds

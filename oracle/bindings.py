@@ -259,6 +259,11 @@ class Reference:
         L.ref_obs_read.restype = C.c_void_p
         L.ref_obs_frame.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr, P(C.c_int), cd.dptr, cd.dptr]
         L.ref_obs_frame.restype = None
+        L.ref_obs_frame_view.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, cd.dptr, P(C.c_int), cd.dptr,
+                                         cd.dptr]
+        L.ref_obs_frame_view.restype = None
+        L.ref_obs_views.argtypes = [C.c_void_p, C.c_int, P(C.c_int)]
+        L.ref_obs_views.restype = None
         L.ref_obs_doppler_frame.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr, P(C.c_int), cd.dptr, cd.dptr]
         L.ref_obs_doppler_frame.restype = None
         L.ref_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int,

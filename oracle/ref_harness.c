@@ -961,12 +961,12 @@ void *ref_obs_read(const char *modpath, const char *obspath, int perform_ltc, do
 /* geom: t, oe[9], orbspin[3], ae[9], spin[3], deloff, dopoff, delcom_vig,
  * dopcom_vig, dopDC_vig, weight, dof, cal, sdev (34 doubles); ndel/ndop of
  * the window; obs and oneovervar delay-major (either may be NULL). */
-void ref_obs_frame(void *h, int s, int f, double *geom, int *nd, double *obs, double *oov)
+void ref_obs_frame_view(void *h, int s, int f, int k, double *geom, int *nd, double *obs, double *oov)
 {
     ref_obsfile *F = h;
     struct deldop_t *dd = &F->dat.set[s].desc.deldop;
     struct deldopfrm_t *fr = &dd->frame[f];
-    struct deldopview_t *v = &fr->view[0];
+    struct deldopview_t *v = &fr->view[k];
     double *g = geom;
     *g++ = v->t;
     for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) *g++ = v->oe[i][j];
@@ -983,6 +983,20 @@ void ref_obs_frame(void *h, int s, int f, double *geom, int *nd, double *obs, do
             if (obs) obs[(j - 1) * fr->ndop + (k - 1)] = fr->obs[j][k];
             if (oov) oov[(j - 1) * fr->ndop + (k - 1)] = fr->oneovervar[j][k];
         }
+}
+
+/* View 0 of a frame (the only one of an unsmeared set). */
+void ref_obs_frame(void *h, int s, int f, double *geom, int *nd, double *obs, double *oov)
+{
+    ref_obs_frame_view(h, s, f, 0, geom, nd, obs, oov);
+}
+
+/* Views per frame and the epoch view's index of delay-Doppler set s. */
+void ref_obs_views(void *h, int s, int *out)
+{
+    ref_obsfile *F = h;
+    out[0] = F->dat.set[s].desc.deldop.nviews;
+    out[1] = F->dat.set[s].desc.deldop.v0;
 }
 
 /* A lightcurve set of ref_obs_read's data: sizes = ioptlaw, ncalc, n (x

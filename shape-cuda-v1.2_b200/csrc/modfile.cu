@@ -718,6 +718,10 @@ struct shape_obs_file {
         std::vector<double> delcor;
         std::string dir;
         std::vector<Frame> frames;
+        // smearing (src/shape/read_dat.c:635-646): views per frame, the
+        // epoch view's index and the interval between views in days
+        int nviews = 1, v0 = 0;
+        double view_interval = 0.0;
         // lightcurve sets (read_lghtcrv, src/shape/read_dat.c:1667-2063)
         int ioptlaw = 0;
         std::vector<shape_ephem_point> solephem;   // the Sun as seen by the observer
@@ -942,10 +946,14 @@ int shape_obs_read(const char *path, shape_obs_file **out)
             }
             S.dd.dopscale = tk.param("dopscale", nullptr);
             const int nviews = tk.integer("views per frame");
-            tk.real("view interval");
+            S.view_interval = tk.real("view interval") / 86400.0;
             const std::string smear = tk.word("smearing mode");
             if (smear != "center" && smear != "first") tk.fail("smearing mode " + smear + " is not known");
-            if (nviews != 1) tk.fail("smeared frames (more than one view) are not supported", SHAPE_E_UNSUPPORTED);
+            if (nviews < 1) tk.fail("views per frame must be >= 1");
+            if (nviews != 1 && S.doppler)
+                tk.fail("smeared Doppler frames (more than one view) are not supported", SHAPE_E_UNSUPPORTED);
+            S.nviews = nviews;
+            S.v0 = smear == "center" ? nviews / 2 : 0;
             S.dir = tk.word("data directory");
             const int nf = tk.integer("number of frames");
             if (nf < 1) tk.fail("no frames");
@@ -1006,30 +1014,35 @@ int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *ir
     return SHAPE_OK;
 }
 
-int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
-                     const shape_obs_options *opt, shape_deldop_frame *frames, double *obs, double *oneovervar,
-                     double *sdev)
+int shape_obs_views(const shape_obs_file *o, int s, int *nviews, int *v0)
 {
-    if (!o || s < 0 || s >= (int)o->sets.size() || !spin || !opt || !frames || !obs || !oneovervar)
-        return shape::report_error(SHAPE_E_ARG, "obs_frames: invalid argument");
-    const shape_obs_file::Set &S = o->sets[s];
-    if (S.lightcurve) return shape::report_error(SHAPE_E_ARG, "obs_frames: a lightcurve set (use shape_obs_lghtcrv)");
-    if (S.doppler) return shape::report_error(SHAPE_E_ARG, "obs_frames: a Doppler set (use shape_obs_doppler)");
-    const int nf = (int)S.frames.size();
-    const size_t D = (size_t)S.ndel * S.ndop;
-    std::vector<double> t(nf), orb(3 * (size_t)nf), ae(9 * (size_t)nf), sp(3 * (size_t)nf);
+    if (!o || s < 0 || s >= (int)o->sets.size() || !nviews)
+        return shape::report_error(SHAPE_E_ARG, "obs_views: invalid argument");
+    *nviews = o->sets[s].nviews;
+    if (v0) *v0 = o->sets[s].v0;
+    return SHAPE_OK;
+}
+
+// Every view of every frame of delay-Doppler set S (read_deldop,
+// src/shape/read_dat.c:860-905; deldopoffs, src/shape/deldopoffs.c:19-45;
+// realize_spin, src/shape/realize_spin.c:130-185): view k of frame f (the
+// reference's numbering) sits at t0 + (k - v0) * view interval, light-time
+// corrected; views[f * nviews + j] receives view (v0 + 1 + j) % nviews, the
+// order calc_deldop renders them, so the epoch view v0 closes each frame.
+static int obs_deldop_views(const shape_obs_file::Set &S, const shape_spin_state *spin, int pos_n,
+                            double km_per_pixel, const shape_obs_options *opt, shape_deldop_frame *views,
+                            double *obs, double *oneovervar, double *sdev)
+{
+    const int nf = (int)S.frames.size(), nv = S.nviews;
+    const size_t D = (size_t)S.ndel * S.ndop, N = (size_t)nf * nv;
+    std::vector<double> t(N), orb(3 * N), ae(9 * N), sp(3 * N);
+    std::vector<shape_deldop_frame> vk(N);     // reference view order
     for (int f = 0; f < nf; f++) {
         const shape_obs_file::Frame &F = S.frames[f];
-        shape_deldop_frame &G = frames[f];
+        shape_deldop_frame G;
         memset(&G, 0, sizeof G);
         G.pos_n = pos_n;
         G.km_per_pixel = km_per_pixel;
-        if (int rc = shape_ephem_radar_view(S.ephem.data(), (int)S.ephem.size(), F.t0, opt->perform_ltc, &t[f],
-                                            G.oe, &orb[3 * (size_t)f]))
-            return rc;
-        if (int rc = shape_delcor_offsets(S.delcor.data(), (int)S.delcor.size() - 1, S.delcor_t0, t[f],
-                                          S.dd.del_per_pixel, S.dd.dop_per_pixel, S.dd.Ftx, &G.deloff, &G.dopoff))
-            return rc;
         G.ndel = S.ndel;
         G.ndop = S.ndop;
         G.delcom_vig = F.delcom;                 // no mask: the window is the whole image
@@ -1039,6 +1052,19 @@ int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spi
         G.dof = F.weight * S.ndel * S.ndop;
         G.cal_floating = F.cal_state == 'f';
         G.cal = F.cal;
+        for (int k = 0; k < nv; k++) {
+            const size_t i = (size_t)f * nv + k;
+            shape_deldop_frame &V = vk[i];
+            V = G;
+            const double tk = nv == 1 ? F.t0 : F.t0 + (k - S.v0) * S.view_interval;
+            if (int rc = shape_ephem_radar_view(S.ephem.data(), (int)S.ephem.size(), tk, opt->perform_ltc, &t[i],
+                                                V.oe, &orb[3 * i]))
+                return rc;
+            if (int rc = shape_delcor_offsets(S.delcor.data(), (int)S.delcor.size() - 1, S.delcor_t0, t[i],
+                                              S.dd.del_per_pixel, S.dd.dop_per_pixel, S.dd.Ftx, &V.deloff,
+                                              &V.dopoff))
+                return rc;
+        }
         if (sdev) sdev[f] = F.sdev;
         const std::string full = S.dir + "/" + F.name;
         const int dl[2] = {1, S.ndel}, dp[2] = {1, S.ndop};
@@ -1047,13 +1073,41 @@ int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spi
                                            oneovervar + f * D))
             return rc;
     }
-    if (int rc = shape_realize_spin(spin, S.angleoff, S.omegaoff, nf, t.data(), orb.data(), ae.data(), sp.data()))
+    if (int rc = shape_realize_spin(spin, S.angleoff, S.omegaoff, (int)N, t.data(), orb.data(), ae.data(), sp.data()))
         return rc;
-    for (int f = 0; f < nf; f++) {
-        memcpy(frames[f].ae, &ae[9 * (size_t)f], sizeof frames[f].ae);
-        memcpy(frames[f].spin, &sp[3 * (size_t)f], sizeof frames[f].spin);
+    for (size_t i = 0; i < N; i++) {
+        memcpy(vk[i].ae, &ae[9 * i], sizeof vk[i].ae);
+        memcpy(vk[i].spin, &sp[3 * i], sizeof vk[i].spin);
     }
+    for (int f = 0; f < nf; f++)
+        for (int j = 0; j < nv; j++) views[(size_t)f * nv + j] = vk[(size_t)f * nv + (S.v0 + 1 + j) % nv];
     return SHAPE_OK;
+}
+
+int shape_obs_frames_views(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n,
+                           double km_per_pixel, const shape_obs_options *opt, shape_deldop_frame *views, double *obs,
+                           double *oneovervar, double *sdev)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size() || !spin || !opt || !views || !obs || !oneovervar)
+        return shape::report_error(SHAPE_E_ARG, "obs_frames_views: invalid argument");
+    const shape_obs_file::Set &S = o->sets[s];
+    if (S.lightcurve || S.doppler)
+        return shape::report_error(SHAPE_E_ARG, "obs_frames_views: not a delay-Doppler set");
+    return obs_deldop_views(S, spin, pos_n, km_per_pixel, opt, views, obs, oneovervar, sdev);
+}
+
+int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
+                     const shape_obs_options *opt, shape_deldop_frame *frames, double *obs, double *oneovervar,
+                     double *sdev)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size() || !spin || !opt || !frames || !obs || !oneovervar)
+        return shape::report_error(SHAPE_E_ARG, "obs_frames: invalid argument");
+    const shape_obs_file::Set &S = o->sets[s];
+    if (S.lightcurve) return shape::report_error(SHAPE_E_ARG, "obs_frames: a lightcurve set (use shape_obs_lghtcrv)");
+    if (S.doppler) return shape::report_error(SHAPE_E_ARG, "obs_frames: a Doppler set (use shape_obs_doppler)");
+    if (S.nviews != 1)
+        return shape::report_error(SHAPE_E_UNSUPPORTED, "obs_frames: smeared frames (use shape_obs_frames_views)");
+    return obs_deldop_views(S, spin, pos_n, km_per_pixel, opt, frames, obs, oneovervar, sdev);
 }
 
 // A Doppler set's setup and frames (read_doppler, src/shape/read_dat.c:

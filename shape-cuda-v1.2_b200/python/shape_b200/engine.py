@@ -162,6 +162,9 @@ def load_library(path=LIB_PATH):
                                 P(C.c_size_t)]
     L.shape_obs_frames.argtypes = [vp, C.c_int, P(cd.SpinState), C.c_int, C.c_double, P(ObsOptions),
                                    P(cd.DeldopFrame), cd.dptr, cd.dptr, cd.dptr]
+    L.shape_obs_views.argtypes = [vp, C.c_int, P(C.c_int), P(C.c_int)]
+    L.shape_obs_frames_views.argtypes = [vp, C.c_int, P(cd.SpinState), C.c_int, C.c_double, P(ObsOptions),
+                                         P(cd.DeldopFrame), cd.dptr, cd.dptr, cd.dptr]
     L.shape_read_lghtcrv_data.argtypes = [C.c_char_p, C.c_int, C.c_double, cd.dptr, cd.dptr, cd.dptr]
     L.shape_read_radar_data.argtypes = [C.c_char_p, C.c_int, C.c_int, P(C.c_int), P(C.c_int), C.c_int, C.c_double,
                                         C.c_double, C.c_double, cd.dptr, cd.dptr, cd.dptr]
@@ -621,6 +624,26 @@ class ObsFile:
         _chk(self.L.shape_obs_frames(self.h, s, C.byref(spin), int(pos_n), float(km_per_pixel), C.byref(opt), fr,
                                      cd.as_dptr(obs), cd.as_dptr(oov), cd.as_dptr(sdev)))
         return list(fr), obs, oov, sdev
+
+    def views(self, s):
+        """(views per frame, index of the epoch view) of set s."""
+        nv, v0 = C.c_int(), C.c_int()
+        _chk(self.L.shape_obs_views(self.h, s, C.byref(nv), C.byref(v0)))
+        return nv.value, v0.value
+
+    def frame_views(self, s, spin, pos_n, km_per_pixel, perform_ltc=1, dd_gamma=1.0, speckle=0, big_endian=1):
+        """A delay-Doppler set of any views per frame: (views per frame in
+        rendering order, the epoch view last; obs, 1/variance, sdev)."""
+        info = self.set_info(s)
+        nf = info["nframes"]
+        nv, _ = self.views(s)
+        fr = (cd.DeldopFrame * (nf * nv))()
+        obs, oov, sdev = np.zeros(info["nelem"]), np.zeros(info["nelem"]), np.zeros(nf)
+        opt = ObsOptions(perform_ltc, dd_gamma, speckle, big_endian)
+        _chk(self.L.shape_obs_frames_views(self.h, s, C.byref(spin), int(pos_n), float(km_per_pixel), C.byref(opt),
+                                           fr, cd.as_dptr(obs), cd.as_dptr(oov), cd.as_dptr(sdev)))
+        fl = list(fr)
+        return [fl[f * nv:(f + 1) * nv] for f in range(nf)], obs, oov, sdev
 
 
 class ModFile:

@@ -136,7 +136,10 @@ def test_obs_refusals(tmp_path, monkeypatch):
     p.write_text(OBS.replace("delay-doppler", "plane-of-sky"))
     with pytest.raises(eng.EngineError, match="error -4"):
         eng.ObsFile(p)
-    p.write_text(OBS.replace("1 0.0 center", "3 60.0 center"))
+    p.write_text(OBS.replace("1 0.0 center", "0 60.0 center"))
+    with pytest.raises(eng.EngineError, match="error -1"):
+        eng.ObsFile(p)
+    p.write_text("1\n" + DOPPLER_SET.replace("1 0.0 first", "3 60.0 first"))
     with pytest.raises(eng.EngineError, match="error -4"):
         eng.ObsFile(p)
     p.write_text(OBS.replace("1.0 0\nf1", "1.0 1\nf1"))
@@ -304,3 +307,56 @@ def test_obs_lightcurve_sets_match_reference(tmp_path, monkeypatch, ltc):
         assert (ds.set.weight, ds.set.dof, ds.set.cal) == tuple(tail), s
         assert ds.set.cal_floating == (s < 3)
     assert o.lghtcrv_info(2)["ncalc"] == 4          # five epochs, one repeated
+
+
+def _smeared_files(tmp_path, mode, nviews):
+    m = cases.c1()[0]
+    write_mod(tmp_path / "m.mod", m, seed=3)
+    (tmp_path / "d").mkdir()
+    rng = np.random.default_rng(21)
+    for f in range(3):
+        img = rng.normal(0, 1, (20, 30))
+        if f == 2:
+            (tmp_path / "d" / "f2.dat").write_bytes(img.astype(">f4").tobytes())
+        else:
+            (tmp_path / "d" / ("f%d.dat" % f)).write_text("\n".join(repr(float(x)) for x in img.ravel()) + "\n")
+    (tmp_path / "t.obs").write_text(OBS.replace("1 0.0 center", "%d 1800.0 %s" % (nviews, mode)))
+    return m
+
+
+@pytest.mark.parametrize("mode,nviews,ltc", [("center", 3, 1), ("first", 4, 0), ("center", 4, 1)])
+def test_obs_smeared_views_match_reference(tmp_path, monkeypatch, mode, nviews, ltc):
+    """Every view of every frame of a smeared set (read_deldop's view
+    epochs t0 + (k - v0) * interval, light-time corrected, each view's
+    observer matrix, orbital spin, delay / Doppler offsets and realized
+    spin), listed in rendering order, bit for bit against read_dat."""
+    monkeypatch.chdir(tmp_path)
+    _smeared_files(tmp_path, mode, nviews)
+    spin = eng.ModFile("m.mod").spin()
+    o = eng.ObsFile("t.obs")
+    nv, v0 = o.views(0)
+    assert nv == nviews and v0 == (nviews // 2 if mode == "center" else 0)
+    with pytest.raises(eng.EngineError, match="error -4"):
+        o.frames(0, spin, 75, 0.02, perform_ltc=ltc)
+    views, obs, oov, sdev = o.frame_views(0, spin, 75, 0.02, perform_ltc=ltc)
+    ref = Reference()
+    h = ref.lib.ref_obs_read(b"m.mod", b"t.obs", ltc, 1.0, 0, 1)
+    rv = (eng.C.c_int * 2)()
+    ref.lib.ref_obs_views(h, 0, rv)
+    assert (rv[0], rv[1]) == (nv, v0)
+    D = 20 * 30
+    for f in range(3):
+        assert len(views[f]) == nv
+        for j, V in enumerate(views[f]):
+            k = (v0 + 1 + j) % nv
+            g, nd = np.zeros(34), (eng.C.c_int * 2)()
+            ro, rvv = np.zeros(D), np.zeros(D)
+            ref.lib.ref_obs_frame_view(h, 0, f, k, cd.as_dptr(g), nd, cd.as_dptr(ro), cd.as_dptr(rvv))
+            assert list(V.oe) == list(g[1:10]), (f, k)
+            assert list(V.ae) == list(g[13:22]), (f, k)
+            assert list(V.spin) == list(g[22:25]), (f, k)
+            assert (V.deloff, V.dopoff) == (g[25], g[26]), (f, k)
+            assert (V.delcom_vig, V.dopcom_vig, V.dopDC_vig, V.weight, V.dof, V.cal) == tuple(g[27:33])
+            assert np.array_equal(obs[f * D:(f + 1) * D], ro) and np.array_equal(oov[f * D:(f + 1) * D], rvv)
+        # the epoch view closes the list, and the views differ
+        assert list(views[f][-1].ae) != list(views[f][0].ae)
