@@ -176,6 +176,22 @@ int shape_engine_set_bin_capacity(shape_engine *e, int cap);
  * chi-square may move by ~1e-4 when that happens). Lightcurve views are
  * always exact. Takes effect at the next evaluation. */
 int shape_engine_set_fp32_exact(shape_engine *e, int exact);
+/* Raster kernel of the batched forms. mode -1 (default): the first batched
+ * evaluation of each form times four candidates on this engine's datasets
+ * (the tile-per-CTA kernel and the warp-independent kernel, each with one
+ * CTA per non-empty tile or a persistent grid of resident CTAs on every
+ * SM striding over the tiles) and keeps the fastest; the choice is
+ * remembered for engines of the same size class in the process. mode 0 /
+ * 1: that kernel, one CTA per tile, no timing. Every candidate computes the
+ * same images. Lightcurve views always use the tile-per-CTA kernel (in the
+ * FP32 form their own launch; in the FP64 form an engine with lightcurve
+ * points tunes the grid only). */
+int shape_engine_set_raster_tuning(shape_engine *e, int mode);
+/* The raster choice of a form: *variant (0 tile-per-CTA, 1 warp-
+ * independent), *persistent, and ms[4] (may be NULL) the measured raster
+ * times of the candidates variant*2 + persistent (0 where not measured).
+ * Returns 1 once the form is tuned, 0 before its first evaluation. */
+int shape_engine_get_raster_tuning(shape_engine *e, int form, int *variant, int *persistent, double *ms);
 
 /* A new view for radar frame global_frame (delay-Doppler and Doppler frames
  * numbered across sets in the order they were added), for spin, pole and

@@ -12,7 +12,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "engine_impl.h"
@@ -178,6 +181,7 @@ int EngineImpl::finalize()
     if (dd.empty() && lc.empty()) return set_err(SHAPE_E_STATE, "finalize: no datasets");
     mem.release();
     invalidate_graphs();
+    for (int f = 0; f < 3; f++) tuned[f] = 0;
     d_work_sorted = nullptr;
     d_sides = nullptr; d_msum_part = d_msum = nullptr;
     cap = fixed_cap > 0 ? fixed_cap : 512;
@@ -1063,20 +1067,22 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         // variant, in a second launch.
         ra.work = d_work_sorted;
         ra.pdl = pdl ? 1 : 0;
+        ra.variant = raster_variant[form];
         if (f32) {
             RasterArgs rr = ra, rl = ra;
             rr.nwork = work_radar;
-            rr.grid = nonempty_radar;
             rr.exact = fp32_exact;
+            rr.grid = raster_grid(form, nonempty_radar, rr, true);
             rl.work = d_work_sorted + work_radar;
             rl.nwork = (int)work.size() - work_radar;
-            rl.grid = nonempty_lc;
             rl.exact = 1;
+            rl.variant = 0;       // lightcurve views: the tile-per-CTA kernel
+            rl.grid = raster_grid(form, nonempty_lc, rl, true);
             launch_raster_f32(rr, s);
             launch_raster_f32(rl, s);
         } else {
             ra.nwork = (int)work.size();
-            ra.grid = tuned_nonempty;
+            ra.grid = raster_grid(form, tuned_nonempty, ra, false);
             launch_raster_f64(ra, s);
         }
         mark(4);
@@ -1196,6 +1202,16 @@ int EngineImpl::launch(int form)
             gexec[form] = nullptr;
         }
         if (!gexec[form]) {
+            if (!tuned[form]) {
+                if (tune_mode < 0) {
+                    int rc = autotune(form);
+                    if (rc) return rc;
+                } else {
+                    raster_variant[form] = (form == SHAPE_FORM_BATCHED_FP64 && !lcpts.empty()) ? 0 : tune_mode;
+                    raster_persistent[form] = 0;
+                    tuned[form] = 1;
+                }
+            }
             // baddiam factors are baked into the summary launch: graphs are
             // rebuilt if the flag changes (rare: a scale factor <= 0.01).
             cudaGraph_t graph;
@@ -1219,6 +1235,95 @@ int EngineImpl::launch(int form)
         CK(cudaEventRecord(ev1, s));
     }
     last_form = form;
+    return SHAPE_OK;
+}
+
+// The raster grid of a batched launch: one CTA per tile that was non-empty
+// at bin tuning, or (persistent) the kernel's resident CTAs on every SM,
+// each striding over the sorted tiles.
+int EngineImpl::raster_grid(int form, int nonempty, const RasterArgs &a, bool f32) const
+{
+    if (!raster_persistent[form] || nonempty <= 0) return nonempty;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
+        return nonempty;
+    const int occ = f32 ? raster_occupancy_f32(a) : raster_occupancy_f64(a);
+    if (occ <= 0) return nonempty;
+    return std::min(nonempty, occ * sms);
+}
+
+namespace {
+// Raster choices by size class, shared by the engines of the process (the
+// server's clones of one dataset tune once).
+struct TuneKey {
+    int device, form, exact, nviews, nf, nonempty, maxcount;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(device, form, exact, nviews, nf, nonempty, maxcount) <
+               std::tie(o.device, o.form, o.exact, o.nviews, o.nf, o.nonempty, o.maxcount);
+    }
+};
+struct TuneChoice {
+    int variant, persistent;
+    double ms[4];
+};
+std::mutex tune_mu;
+std::map<TuneKey, TuneChoice> tune_cache;
+}  // namespace
+
+// Measures the raster stage of this form with each kernel and grid (one
+// untimed and three timed eager runs each, the minimum kept) and keeps the
+// fastest. Runs outside any capture, before the form's graph is built.
+int EngineImpl::autotune(int form)
+{
+    const TuneKey key{device, form, form == SHAPE_FORM_BATCHED_FP32 ? fp32_exact : 0, nviews, nf,
+                      tuned_nonempty, tuned_max_count / 16};
+    {
+        std::lock_guard<std::mutex> lk(tune_mu);
+        auto it = tune_cache.find(key);
+        if (it != tune_cache.end()) {
+            raster_variant[form] = it->second.variant;
+            raster_persistent[form] = it->second.persistent;
+            memcpy(tune_ms[form], it->second.ms, sizeof tune_ms[form]);
+            tuned[form] = 1;
+            return SHAPE_OK;
+        }
+    }
+    cudaStream_t s = stream;
+    CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s));
+    cudaEvent_t ev[8];
+    for (auto &x : ev) CK(cudaEventCreate(&x));
+    int best = 0, rc = SHAPE_OK;
+    double best_ms = 1e300;
+    // the warp-independent kernel is a candidate for radar views only: a
+    // batched FP64 launch that also holds lightcurve views keeps the
+    // tile-per-CTA kernel
+    const int ncand = (form == SHAPE_FORM_BATCHED_FP64 && !lcpts.empty()) ? 2 : 4;
+    for (int c = 0; c < ncand && rc == SHAPE_OK; c++) {
+        raster_variant[form] = c >> 1;
+        raster_persistent[form] = c & 1;
+        double m = 1e300;
+        for (int rep = 0; rep < 4 && rc == SHAPE_OK; rep++) {
+            rc = enqueue(form, ev);
+            if (rc) break;
+            cudaError_t ce = cudaStreamSynchronize(s);
+            if (ce != cudaSuccess) { rc = set_err(SHAPE_E_CUDA, cudaGetErrorString(ce)); break; }
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[3], ev[4]);     // after bin -> after raster
+            if (rep > 0) m = std::min(m, (double)t);
+        }
+        tune_ms[form][c] = m;
+        if (m < best_ms) { best_ms = m; best = c; }
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (rc) return rc;
+    raster_variant[form] = best >> 1;
+    raster_persistent[form] = best & 1;
+    tuned[form] = 1;
+    std::lock_guard<std::mutex> lk(tune_mu);
+    TuneChoice ch{raster_variant[form], raster_persistent[form], {}};
+    memcpy(ch.ms, tune_ms[form], sizeof ch.ms);
+    tune_cache[key] = ch;
     return SHAPE_OK;
 }
 
@@ -1822,8 +1927,31 @@ int shape_engine_set_fp32_exact(shape_engine *h, int exact)
         cudaGraphExecDestroy(E.gexec[SHAPE_FORM_BATCHED_FP32]);
         E.gexec[SHAPE_FORM_BATCHED_FP32] = nullptr;
     }
+    if (E.fp32_exact != exact) E.tuned[SHAPE_FORM_BATCHED_FP32] = 0;
     E.fp32_exact = exact;
     return SHAPE_OK;
+}
+
+int shape_engine_set_raster_tuning(shape_engine *h, int mode)
+{
+    if (!h || mode < -1 || mode > 1) return shape::set_err(SHAPE_E_ARG, "set_raster_tuning: -1, 0 or 1");
+    shape::EngineImpl &E = h->impl;
+    if (E.finalized) cudaSetDevice(E.device);
+    E.invalidate_graphs();
+    E.tune_mode = mode;
+    for (int f = 0; f < 3; f++) E.tuned[f] = 0;
+    return SHAPE_OK;
+}
+
+int shape_engine_get_raster_tuning(shape_engine *h, int form, int *variant, int *persistent, double *ms)
+{
+    if (!h || form < 0 || form > 2) return shape::set_err(SHAPE_E_ARG, "get_raster_tuning: bad argument");
+    const shape::EngineImpl &E = h->impl;
+    if (variant) *variant = E.raster_variant[form];
+    if (persistent) *persistent = E.raster_persistent[form];
+    if (ms)
+        for (int c = 0; c < 4; c++) ms[c] = E.tune_ms[form][c];
+    return E.tuned[form];
 }
 
 int shape_engine_set_bin_capacity(shape_engine *h, int cap)

@@ -252,6 +252,7 @@ struct EngineImpl {
         frame_sdev = o.frame_sdev;
         fixed_cap = o.fixed_cap;
         fp32_exact = o.fp32_exact;
+        tune_mode = o.tune_mode;
         finalized = false;
     }
     // bin tuning results
@@ -263,6 +264,19 @@ struct EngineImpl {
     int work_radar = 0, nonempty_radar = 0, nonempty_lc = 0;
     int fixed_cap = 0;            // > 0: bin capacity set by the caller, no autotuning
     int fp32_exact = 1;           // batched FP32: radar views by the exact raster variant too
+    // Raster kernel per form (RasterArgs::variant) and grid (0: one CTA per
+    // tile that was non-empty at bin tuning; 1: persistent, resident CTAs x
+    // SMs striding over the tiles). tune_mode -1: the first batched
+    // evaluation of a form measures the four candidates on this engine's
+    // datasets and keeps the fastest (remembered per size class for other
+    // engines of the process); 0 / 1: that kernel, one CTA per tile.
+    int tune_mode = -1;
+    int raster_variant[3] = {0, 0, 0};
+    int raster_persistent[3] = {0, 0, 0};
+    int tuned[3] = {0, 0, 0};
+    double tune_ms[3][4] = {};    // raster ms of candidates (variant * 2 + persistent); 0: not measured
+    int autotune(int form);
+    int raster_grid(int form, int nonempty, const RasterArgs &a, bool f32) const;
     int evaluate(int form, shape_eval_summary *out);
     int kernels_per_eval(int form) const;
     void fill_params(double *dst) const

@@ -78,6 +78,10 @@ struct RasterArgs {
     // where this launch assigned pixel p. 0 for the engine's evaluations.
     int accumulate;
     unsigned char *won;
+    // 0: the tile-per-CTA kernel (k_raster: the CTA's warps share one
+    // sorted facet list and meet at block barriers); 1: the warp-independent
+    // kernel (k_raster_w: each warp sorts and replays its own block's list)
+    int variant;
 };
 
 // core.cu (FP64, no FMA contraction)
@@ -249,6 +253,9 @@ void launch_chi2_summary(const Chi2Args &ca, const FinalizeArgs &fa, const Summa
 // raster_f64.cu / raster_f32.cu
 void launch_raster_f64(const RasterArgs &a, cudaStream_t s);
 void launch_raster_f32(const RasterArgs &a, cudaStream_t s);
+// resident CTAs per SM of the raster kernel these arguments select
+int raster_occupancy_f64(const RasterArgs &a);
+int raster_occupancy_f32(const RasterArgs &a);
 cudaError_t configure_raster_f64();
 cudaError_t configure_raster_f32();
 

@@ -4,5 +4,6 @@
 
 namespace shape {
 void launch_raster_f64(const RasterArgs &a, cudaStream_t s) { launch_raster_t<double>(a, s); }
+int raster_occupancy_f64(const RasterArgs &a) { return raster_occupancy_t<double>(a); }
 cudaError_t configure_raster_f64() { return configure_raster_t<double>(); }
 }  // namespace shape

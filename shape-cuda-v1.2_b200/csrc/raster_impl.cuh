@@ -42,9 +42,6 @@
 #ifndef RASTER_W_MIN_BLOCKS_F64
 #define RASTER_W_MIN_BLOCKS_F64 3
 #endif
-#ifndef RASTER_WARP
-#define RASTER_WARP 0
-#endif
 #ifndef RASTER_RARE_NOINLINE
 #define RASTER_RARE_NOINLINE 0
 #endif
@@ -1626,7 +1623,7 @@ inline void launch_raster_t(const RasterArgs &a, cudaStream_t s)
     const int grid = (a.grid > 0 && a.grid < a.nwork) ? a.grid : a.nwork;
     // the FP64 form is exact by construction; the FP32 form runs its exact
     // variant unless radar views are asked for their FP32 decisions
-    if (RASTER_WARP) {
+    if (a.variant == 1) {
         b.smem_bytes = RASTER_THREADS / 32 * sizeof(WarpArea<T>);
         if (sizeof(T) == 4 && a.exact)
             launch_k(k_raster_w<T, true>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
@@ -1639,6 +1636,27 @@ inline void launch_raster_t(const RasterArgs &a, cudaStream_t s)
         launch_k(k_raster<T, true>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
     else
         launch_k(k_raster<T, false>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
+}
+
+// Resident CTAs per SM of the kernel launch_raster_t would launch for a
+// (0 when the query fails): the persistent grid is this times the SM count.
+template <typename T>
+inline int raster_occupancy_t(const RasterArgs &a)
+{
+    int n = 0;
+    cudaError_t e;
+    if (a.variant == 1) {
+        const size_t sm = RASTER_THREADS / 32 * sizeof(WarpArea<T>);
+        e = (sizeof(T) == 4 && a.exact)
+                ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raster_w<T, true>, RASTER_THREADS, sm)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raster_w<T, false>, RASTER_THREADS, sm);
+    } else {
+        const size_t sm = raster_smem_bytes<T>(a.cap, a.nf);
+        e = (sizeof(T) == 4 && a.exact)
+                ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raster<T, true>, RASTER_THREADS, sm)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raster<T, false>, RASTER_THREADS, sm);
+    }
+    return e == cudaSuccess ? n : 0;
 }
 
 }  // namespace shape

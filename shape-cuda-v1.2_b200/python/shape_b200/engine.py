@@ -126,6 +126,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_stage_times.argtypes = [vp, C.c_int, cd.dptr, C.c_int]
     L.shape_engine_set_bin_capacity.argtypes = [vp, C.c_int]
     L.shape_engine_set_fp32_exact.argtypes = [vp, C.c_int]
+    L.shape_engine_set_raster_tuning.argtypes = [vp, C.c_int]
+    L.shape_engine_get_raster_tuning.argtypes = [vp, C.c_int, P(C.c_int), P(C.c_int), cd.dptr]
     L.shape_engine_set_frame_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.dptr, C.c_double, C.c_double]
     L.shape_engine_set_point_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.dptr]
     L.shape_engine_set_spin_model.argtypes = [vp, P(cd.SpinState), cd.dptr, cd.dptr, cd.dptr, cd.dptr]
@@ -299,6 +301,20 @@ class Engine:
         whose decisions lie within FP32 error by the FP64 rules; False keeps
         the FP32 decisions (faster raster)."""
         _chk(self.L.shape_engine_set_fp32_exact(self.h, 1 if exact else 0))
+
+    def set_raster_tuning(self, mode=-1):
+        """-1: time the raster candidates at each batched form's first
+        evaluation and keep the fastest; 0 / 1: the tile-per-CTA / warp-
+        independent kernel, one CTA per tile."""
+        _chk(self.L.shape_engine_set_raster_tuning(self.h, int(mode)))
+
+    def raster_tuning(self, form):
+        """{'tuned', 'variant', 'persistent', 'ms': [4 candidate times]}."""
+        if isinstance(form, str):
+            form = FORMS[form]
+        v, p, ms = C.c_int(), C.c_int(), np.zeros(4)
+        t = _chk(self.L.shape_engine_get_raster_tuning(self.h, form, C.byref(v), C.byref(p), cd.as_dptr(ms)))
+        return {"tuned": bool(t), "variant": v.value, "persistent": p.value, "ms": ms.tolist()}
 
     def set_frame_view(self, frame, ae, oe, spin, deloff=0.0, dopoff=0.0):
         """New view for radar frame `frame` (numbered across sets): 3x3 ae
