@@ -260,6 +260,22 @@ int shape_engine_get_penalties(shape_engine *e, double *base, int max);
 int shape_engine_set_spin_model(shape_engine *e, const shape_spin_state *spin, const double *set_angleoff,
                                 const double *set_omegaoff, const double *frame_t,
                                 const double *frame_orbspin);
+/* Spin realization inside each evaluation (principal-axis rotators): with
+ * on = 1 the evaluation graph copies the spin state and dataset offsets
+ * from pinned memory and a kernel realizes every radar frame's and
+ * lightcurve point's ae (and a frame's spin vector) and view constants
+ * before the raster, as shape_realize_spin and the host setup do (the
+ * device's sin and cos may differ from the C library's in the last place).
+ * shape_engine_set_spin_param then only records the value: a spin trial is
+ * a graph replay with no host realization or view upload. Needs the spin
+ * model (SHAPE_E_STATE without it) of a principal-axis rotator and single-
+ * view frames (SHAPE_E_UNSUPPORTED otherwise); set_frame_view and
+ * set_point_view are refused while it is on. on = 0 realizes on the host
+ * again (the default). */
+int shape_engine_set_spin_device(shape_engine *e, int on);
+/* A radar frame's current ae (9, row-major) and spin vector (3): the
+ * device-realized ones of the last evaluation in device spin mode. */
+int shape_engine_get_frame_view(shape_engine *e, int global_frame, double ae[9], double spin[3]);
 /* One spin parameter (SHAPE_PAR_SPIN_* / ANGLEOFF / OMEGAOFF) of the spin
  * model: set re-realizes every view and copies the view constants to the
  * device on the engine's stream (the next evaluation, graph replays

@@ -39,7 +39,8 @@ UNITS = [
     ("modfile.cu", []),
 ]
 
-HEADERS = ["engine_internal.h", "engine_impl.h", "kernels.h", "raster_impl.cuh", "posmask_dev.cuh"]
+HEADERS = ["engine_internal.h", "engine_impl.h", "kernels.h", "raster_impl.cuh", "posmask_dev.cuh", "viewgeom.cuh",
+           "spin_impl.cuh"]
 
 
 def _newer(src_list, target):

@@ -43,38 +43,6 @@ int report_error(int code, const std::string &msg) { return set_err(code, msg); 
                            std::string(#call) + ": " + cudaGetErrorString(e_));            \
     } while (0)
 
-// y = A x with A row-major (cotrans dir=1, src/util/cotrans.c)
-void mv(double y[3], const double *A, const double x[3])
-{
-    double t[3];
-    for (int i = 0; i < 3; i++) {
-        t[i] = 0.0;
-        for (int k = 0; k < 3; k++) t[i] += A[3 * i + k] * x[k];
-    }
-    y[0] = t[0]; y[1] = t[1]; y[2] = t[2];
-}
-// y = A^T x (cotrans dir=-1)
-void mtv(double y[3], const double *A, const double x[3])
-{
-    double t[3];
-    for (int i = 0; i < 3; i++) {
-        t[i] = 0.0;
-        for (int k = 0; k < 3; k++) t[i] += A[3 * k + i] * x[k];
-    }
-    y[0] = t[0]; y[1] = t[1]; y[2] = t[2];
-}
-// M = B * A^T (mtrnsps + mmmul as in src/shape/posvis.c:101-122)
-void mul_bt(double *M, const double *B, const double *A)
-{
-    double t[9];
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) {
-            t[3 * i + j] = 0.0;
-            for (int k = 0; k < 3; k++) t[3 * i + j] += B[3 * i + k] * A[3 * j + k];
-        }
-    memcpy(M, t, sizeof t);
-}
-
 static int radar_law_index(EngineImpl &E, const shape_radar_law &L)
 {
     if (L.type < SHAPE_RADLAW_COSINE_DIFF || L.type > SHAPE_RADLAW_COSINE_COSINE) return -1;
@@ -110,69 +78,6 @@ void radar_set_consts(FrameGeom &g, const shape_deldop_set &S, const shape_eval_
     g.sinc2width = P.sinc2width;
     g.dopfftlen = S.dopfftlen;
     g.law = law;
-}
-
-// View-dependent constants of radar frame F (src/shape/pos2deldop.c:218-275,
-// src/shape/posvis.c:101-122): the observer <- body matrix, the Doppler
-// axes and footprint extents, the delay and Doppler shifts and a Doppler
-// spectrum's overflow origin; dx = the Doppler extent term of the frame's
-// bin limits; the badradar flag and log-factor of a footprint wider than
-// MAXBINS. g.nsinc2, g.sinc2width and g.dop1d must be set.
-void radar_view_geom(FrameGeom &g, FrameHost &h, double &dx, const shape_deldop_frame &F,
-                     const shape_deldop_set &S)
-{
-    mul_bt(g.oa, F.oe, F.ae);
-    double w[3];
-    mv(w, F.oe, F.spin);
-    double dopfact = S.dopscale * SHAPE_KM2HZFACT * F.km_per_pixel * S.Ftx / S.dop_per_pixel;
-    g.ax = -w[1] * dopfact;
-    g.ay = w[0] * dopfact;
-    double km2Hz = sqrt(g.ax * g.ax + g.ay * g.ay) * S.dop_per_pixel / F.km_per_pixel;
-    dx = 0.0;
-    if (w[0] != 0.0 || w[1] != 0.0)
-        dx = km2Hz * 0.5 * F.km_per_pixel * sqrt(w[0] * w[0] + w[1] * w[1]) /
-             std::max(fabs(w[0]), fabs(w[1]));
-    g.xincr = g.ax / g.nsinc2;
-    g.yincr = g.ay / g.nsinc2;
-    g.dopdiff_bl = -(g.nsinc2 - 1) * (g.xincr + g.yincr) / 2;
-    g.dopdiff_max = (g.nsinc2 - 1) * (fabs(g.xincr) + fabs(g.yincr)) / 2;
-    g.delshift = F.delcom_vig + F.deloff;
-    g.dopshift = F.dopcom_vig + F.dopoff + 0.0;
-    g.dopDC_vig = F.dopDC_vig;
-    if (g.dop1d) g.idop0 = DOP_MAXOVERFLOW / 2 - (int)floor(g.dopshift + 0.5);
-    h.badradar = 0;
-    h.badradar_logfactor = 0.0;
-    if (2 * g.dopdiff_max + g.sinc2width + 1 > SHAPE_MAXBINS) {
-        h.badradar = 1;
-        h.badradar_logfactor = log((2 * g.dopdiff_max + g.sinc2width + 1) / SHAPE_MAXBINS);
-    }
-}
-
-// View-dependent constants of lightcurve point P (src/shape/calc_fits.c:
-// 1634-1716): the observer and sun views' body matrices, the sun direction
-// in observer coordinates and the observer -> sun transform of posmask.
-static void lc_view_geom(FrameGeom &go, FrameGeom &gs, LcPointDev &pd, const shape_lghtcrv_point &P)
-{
-    mul_bt(go.oa, P.oe, P.ae);
-    double us[3] = {0.0, 0.0, 1.0};
-    mtv(us, P.se, us);
-    mv(us, P.oe, us);
-    go.usrc[0] = us[0]; go.usrc[1] = us[1]; go.usrc[2] = us[2];
-    mul_bt(gs.oa, P.se, P.ae);
-    mul_bt(pd.so, P.se, P.oe);
-}
-
-// The float copies of a view's constants that the FP32 raster reads.
-static void view_float_consts(FrameGeom &g)
-{
-    const double fv[FDD_N] = {g.delfact, g.delshift, g.ax, g.ay, g.dopshift, g.const1, g.const2,
-                              g.one_over_spb, g.xincr, g.yincr, g.dopdiff_bl, g.dopdiff_max,
-                              g.dopDC_vig, g.dopfftlen, g.kmpp, g.sinc2width / 2.0,
-                              (double)g.spb_over_stride, (double)g.stride, (double)g.spb_sq,
-                              (double)g.nsinc2_sq};
-    for (int k = 0; k < FDD_N; k++) g.fdd[k] = (float)fv[k];
-    for (int k = 0; k < 9; k++) g.foa[k] = (float)g.oa[k];
-    for (int k = 0; k < 3; k++) g.foa[9 + k] = (float)g.usrc[k];
 }
 
 int EngineImpl::finalize()
@@ -504,6 +409,8 @@ int EngineImpl::finalize()
     md.fv = d_fv; md.af_ptr = d_afp; md.af_idx = d_afi;
     rc = tune_bins();
     if (rc) return rc;
+    rc = setup_spin_device();
+    if (rc) return rc;
     finalized = true;
     return SHAPE_OK;
 }
@@ -519,6 +426,7 @@ int EngineImpl::set_frame_view(int fi, const double ae[9], const double oe[9], c
     if (fi < 0 || fi >= (int)frames.size()) return set_err(SHAPE_E_ARG, "set_frame_view: frame out of range");
     if (!fviews[fi].empty())
         return set_err(SHAPE_E_UNSUPPORTED, "set_frame_view: the frame has several views (smearing)");
+    if (spin_device) return set_err(SHAPE_E_STATE, "set_frame_view: views are realized on the device from the spin model");
     shape_deldop_frame &F = frames[fi];
     memcpy(F.ae, ae, sizeof F.ae);
     memcpy(F.oe, oe, sizeof F.oe);
@@ -543,6 +451,7 @@ int EngineImpl::set_frame_view(int fi, const double ae[9], const double oe[9], c
 int EngineImpl::set_point_view(int pt, const double ae[9], const double oe[9], const double se[9])
 {
     if (pt < 0 || pt >= (int)points.size()) return set_err(SHAPE_E_ARG, "set_point_view: point out of range");
+    if (spin_device) return set_err(SHAPE_E_STATE, "set_point_view: views are realized on the device from the spin model");
     shape_lghtcrv_point &P = points[pt];
     memcpy(P.ae, ae, sizeof P.ae);
     memcpy(P.oe, oe, sizeof P.oe);
@@ -574,7 +483,9 @@ int EngineImpl::set_spin_model(const shape_spin_state &sp, const double *ao, con
     frame_orbspin.assign(orb ? orb : nullptr, orb ? orb + 3 * nfr : nullptr);
     frame_orbspin.resize(3 * nfr, 0.0);
     have_spin = true;
-    return realize_views();
+    int rc = realize_views();
+    if (rc == SHAPE_OK && finalized && spin_device) rc = setup_spin_device();
+    return rc;
 }
 
 // The field of the spin model that a spin parameter names, or null.
@@ -631,6 +542,101 @@ int EngineImpl::realize_views()
         }
     }
     return refresh_views();
+}
+
+// Spin realization inside the evaluation: one source per radar frame and
+// lightcurve point (its epoch, dataset record and orbital spin), device
+// copies of the frames, points and delay-Doppler sets it rebuilds views
+// from, and the pinned spin state and offsets the graph copies in.
+int EngineImpl::setup_spin_device()
+{
+    n_spin_src = 0;
+    if (!spin_device) return SHAPE_OK;
+    if (!have_spin) return set_err(SHAPE_E_STATE, "device spin realization: no spin model");
+    if (!spin_st.pa)
+        return set_err(SHAPE_E_UNSUPPORTED, "device spin realization: principal-axis rotators only");
+    for (const auto &V : fviews)
+        if (!V.empty()) return set_err(SHAPE_E_UNSUPPORTED, "device spin realization: a frame has several views");
+    std::vector<SpinViewSrc> src;
+    for (size_t r = 0; r < setrecs.size(); r++) {
+        if (setrecs[r].type == 0) {
+            int ds = 0;
+            while (ds < (int)dd.size() && dd[ds].frame0 != setrecs[r].first) ds++;
+            for (int k = 0; k < setrecs[r].count; k++) {
+                const int fi = setrecs[r].first + k;
+                SpinViewSrc v{0, fi, (int)r, ds, frame_t[fi], {0.0, 0.0, 0.0}};
+                for (int j = 0; j < 3; j++) v.orb[j] = frame_orbspin[3 * (size_t)fi + j];
+                src.push_back(v);
+            }
+        } else {
+            const LcSetHost &L = lc[setrecs[r].first];
+            for (int k = 0; k < L.npts; k++) src.push_back(SpinViewSrc{1, L.pt0 + k, (int)r, 0, L.x[k], {0.0, 0.0, 0.0}});
+        }
+    }
+    std::vector<shape_deldop_set> sets;
+    for (const DdSetHost &D : dd) sets.push_back(D.set);
+    const size_t nrec = setrecs.size();
+    int rc;
+    for (void *p : {(void *)d_spin_src, (void *)d_spin, (void *)d_spin_off, (void *)d_frames_dev,
+                    (void *)d_ddsets, (void *)d_points_dev})
+        if (p) mem.release_one(p);
+    d_spin_src = nullptr; d_spin = nullptr; d_spin_off = nullptr;
+    d_frames_dev = nullptr; d_ddsets = nullptr; d_points_dev = nullptr;
+    if ((rc = mem.alloc(&d_spin_src, std::max<size_t>(1, src.size()))) != SHAPE_OK) return rc;
+    if ((rc = mem.alloc(&d_spin, 1)) != SHAPE_OK) return rc;
+    if ((rc = mem.alloc(&d_spin_off, 6 * std::max<size_t>(1, nrec))) != SHAPE_OK) return rc;
+    if ((rc = mem.alloc(&d_frames_dev, std::max<size_t>(1, frames.size()))) != SHAPE_OK) return rc;
+    if ((rc = mem.alloc(&d_ddsets, std::max<size_t>(1, sets.size()))) != SHAPE_OK) return rc;
+    if ((rc = mem.alloc(&d_points_dev, std::max<size_t>(1, points.size()))) != SHAPE_OK) return rc;
+    if (h_spin_off) cudaFreeHost(h_spin_off);
+    h_spin_off = nullptr;
+    if (!h_spin) CK(cudaMallocHost((void **)&h_spin, sizeof(shape_spin_state)));
+    CK(cudaMallocHost((void **)&h_spin_off, sizeof(double) * 6 * std::max<size_t>(1, nrec)));
+    cudaStream_t st = stream;
+    if (!src.empty())
+        CK(cudaMemcpyAsync(d_spin_src, src.data(), sizeof(SpinViewSrc) * src.size(), cudaMemcpyHostToDevice, st));
+    if (!frames.empty())
+        CK(cudaMemcpyAsync(d_frames_dev, frames.data(), sizeof(shape_deldop_frame) * frames.size(),
+                           cudaMemcpyHostToDevice, st));
+    if (!sets.empty())
+        CK(cudaMemcpyAsync(d_ddsets, sets.data(), sizeof(shape_deldop_set) * sets.size(), cudaMemcpyHostToDevice, st));
+    if (!points.empty())
+        CK(cudaMemcpyAsync(d_points_dev, points.data(), sizeof(shape_lghtcrv_point) * points.size(),
+                           cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    n_spin_src = (int)src.size();
+    invalidate_graphs();
+    return SHAPE_OK;
+}
+
+// The spin state and offsets of the next evaluation, into pinned memory.
+void EngineImpl::fill_spin()
+{
+    if (!spin_device || !h_spin) return;
+    *h_spin = spin_st;
+    for (size_t r = 0; r < setrecs.size(); r++)
+        for (int j = 0; j < 3; j++) {
+            h_spin_off[6 * r + j] = spin_angleoff[3 * r + j];
+            h_spin_off[6 * r + 3 + j] = spin_omegaoff[3 * r + j];
+        }
+}
+
+// First step of an evaluation in device spin mode: the state copy and the
+// view realization (before the transform reads the views).
+int EngineImpl::enqueue_spin()
+{
+    if (!spin_device || n_spin_src == 0) return SHAPE_OK;
+    cudaStream_t st = stream;
+    CK(cudaMemcpyAsync(d_spin, h_spin, sizeof(shape_spin_state), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_spin_off, h_spin_off, sizeof(double) * 6 * std::max<size_t>(1, setrecs.size()),
+                       cudaMemcpyHostToDevice, st));
+    SpinRealizeArgs a;
+    a.n = n_spin_src;
+    a.src = d_spin_src; a.spin = d_spin; a.off = d_spin_off;
+    a.frames = d_frames_dev; a.ddsets = d_ddsets; a.points = d_points_dev;
+    a.geoms = d_geoms; a.fh = d_fh; a.dop_extra = d_dop_extra; a.lcpts = d_lcpts;
+    launch_realize_views(a, st);
+    return SHAPE_OK;
 }
 
 // After finalize: every view's constants recomputed from frames / points and
@@ -950,6 +956,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     // them in line.
     const bool fork = (form != SHAPE_FORM_PLAIN_FP64) && !marks;
     cudaStream_t sr = fork ? stream2 : s;
+    if (int rc = enqueue_spin()) return rc;
     if (fork) {
         CK(cudaEventRecord(evf[0], s));
         CK(cudaStreamWaitEvent(stream2, evf[0], 0));
@@ -1149,6 +1156,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
 int EngineImpl::kernels_per_eval(int form) const
 {
     int n = 2 + 1;                       // realize (vertices + facets, vertex normals), state reset
+    n += (spin_device && n_spin_src > 0) ? 1 : 0;   // view realization from the spin state
     if (form == SHAPE_FORM_PLAIN_FP64) {
         for (int v = 0; v < nviews; v++)
             n += 3 + ((geoms[v].kind == VIEW_RADAR && fh[geoms[v].frame_index].view == v) ||
@@ -1182,6 +1190,7 @@ int EngineImpl::launch(int form)
     if (form < 0 || form > 2) return set_err(SHAPE_E_ARG, "unknown form");
     cudaStream_t s = stream;
     fill_params(h_params);
+    fill_spin();
     double sc[3];
     effective_scale(sc, &pending_baddiam, &pending_bdl);
     if (!pen_type.empty()) {
@@ -1830,6 +1839,7 @@ int shape_engine_stage_times(shape_engine *h, int form, double *ms, int max)
     cudaEvent_t ev[9];
     for (auto &x : ev) cudaEventCreate(&x);
     E.fill_params(E.h_params);
+    E.fill_spin();
     cudaMemcpyAsync(E.d_r, E.h_params, sizeof(double) * (E.nv + 3), cudaMemcpyHostToDevice, E.stream);
     cudaEventRecord(ev[0], E.stream);
     int rc = E.enqueue(form, ev + 1);
@@ -1884,6 +1894,7 @@ int shape_engine_set_spin_param(shape_engine *h, int kind, int index, double val
     if (!p) return shape::set_err(E.have_spin ? SHAPE_E_ARG : SHAPE_E_STATE, "set_spin_param: no such spin parameter");
     const double old = *p;
     *p = value;
+    if (E.spin_device && E.finalized) return SHAPE_OK;   // realized by the next evaluation
     if (E.finalized) cudaSetDevice(E.device);
     int rc = E.realize_views();
     if (rc) {                       // keep the last realizable state
@@ -1929,6 +1940,44 @@ int shape_engine_set_fp32_exact(shape_engine *h, int exact)
     }
     if (E.fp32_exact != exact) E.tuned[SHAPE_FORM_BATCHED_FP32] = 0;
     E.fp32_exact = exact;
+    return SHAPE_OK;
+}
+
+int shape_engine_set_spin_device(shape_engine *h, int on)
+{
+    if (!h || (on != 0 && on != 1)) return shape::set_err(SHAPE_E_ARG, "set_spin_device: 0 or 1");
+    shape::EngineImpl &E = h->impl;
+    if (E.finalized) cudaSetDevice(E.device);
+    if (on == E.spin_device) return SHAPE_OK;
+    E.invalidate_graphs();
+    E.spin_device = on;
+    if (!E.finalized) return SHAPE_OK;
+    if (on) {
+        int rc = E.setup_spin_device();
+        if (rc) E.spin_device = 0;
+        return rc;
+    }
+    // back to host realization: the host copies of the views are brought
+    // up to date and uploaded
+    E.n_spin_src = 0;
+    return E.have_spin ? E.realize_views() : SHAPE_OK;
+}
+
+int shape_engine_get_frame_view(shape_engine *h, int global_frame, double ae[9], double spin[3])
+{
+    if (!h || !ae || !spin) return shape::set_err(SHAPE_E_ARG, "get_frame_view: null argument");
+    shape::EngineImpl &E = h->impl;
+    if (global_frame < 0 || global_frame >= (int)E.frames.size())
+        return shape::set_err(SHAPE_E_ARG, "get_frame_view: frame out of range");
+    shape_deldop_frame F = E.frames[global_frame];
+    if (E.spin_device && E.finalized && E.n_spin_src > 0) {
+        cudaSetDevice(E.device);
+        cudaError_t ce = cudaMemcpyAsync(&F, E.d_frames_dev + global_frame, sizeof F, cudaMemcpyDeviceToHost, E.stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(E.stream);
+        if (ce != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, cudaGetErrorString(ce));
+    }
+    memcpy(ae, F.ae, sizeof F.ae);
+    memcpy(spin, F.spin, sizeof F.spin);
     return SHAPE_OK;
 }
 

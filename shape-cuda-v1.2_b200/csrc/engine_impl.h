@@ -12,20 +12,15 @@
 
 #include "kernels.h"
 #include "shape_b200.h"
+#include "viewgeom.cuh"
 
 namespace shape {
 
 int report_error(int code, const std::string &msg);   // engine.cu
 
-// Host geometry shared by the engine and the one-view operations
-// (engine.cu, FP64 in the reference's operation order): y = A x, y = A^T x,
-// M = B A^T, and a radar view's set- and view-level pos2deldop constants.
-void mv(double y[3], const double *A, const double x[3]);
-void mtv(double y[3], const double *A, const double x[3]);
-void mul_bt(double *M, const double *B, const double *A);
+// A radar view's set-level pos2deldop constants (engine.cu); the
+// view-level ones are in viewgeom.cuh.
 void radar_set_consts(FrameGeom &g, const shape_deldop_set &S, const shape_eval_params &P, int law, int doppler);
-void radar_view_geom(FrameGeom &g, FrameHost &h, double &dx, const shape_deldop_frame &F,
-                     const shape_deldop_set &S);
 
 struct DevMem {
     std::vector<void *> ptrs;
@@ -200,6 +195,8 @@ struct EngineImpl {
         if (h_params) { cudaFreeHost(h_params); h_params = nullptr; }
         if (h_summary) { cudaFreeHost(h_summary); h_summary = nullptr; }
         if (h_msum) { cudaFreeHost(h_msum); h_msum = nullptr; }
+        if (h_spin) { cudaFreeHost(h_spin); h_spin = nullptr; }
+        if (h_spin_off) { cudaFreeHost(h_spin_off); h_spin_off = nullptr; }
         if (ev0) { cudaEventDestroy(ev0); ev0 = nullptr; }
         if (ev1) { cudaEventDestroy(ev1); ev1 = nullptr; }
         for (auto &e : evf)
@@ -230,6 +227,20 @@ struct EngineImpl {
     double *spin_param(int kind, int index);
     int realize_views();
     int refresh_views();
+    // spin realization inside each evaluation (principal-axis rotators):
+    // the graph copies the spin state and offsets from pinned memory and
+    // k_realize_views rebuilds every view from them
+    int spin_device = 0;
+    int n_spin_src = 0;
+    SpinViewSrc *d_spin_src = nullptr;
+    shape_spin_state *d_spin = nullptr, *h_spin = nullptr;
+    double *d_spin_off = nullptr, *h_spin_off = nullptr;
+    shape_deldop_frame *d_frames_dev = nullptr;
+    shape_deldop_set *d_ddsets = nullptr;
+    shape_lghtcrv_point *d_points_dev = nullptr;
+    int setup_spin_device();
+    void fill_spin();
+    int enqueue_spin();
     int enqueue(int form, cudaEvent_t *marks = nullptr);
     int launch(int form);
     int poll();
@@ -253,6 +264,10 @@ struct EngineImpl {
         fixed_cap = o.fixed_cap;
         fp32_exact = o.fp32_exact;
         tune_mode = o.tune_mode;
+        have_spin = o.have_spin; spin_st = o.spin_st;
+        spin_angleoff = o.spin_angleoff; spin_omegaoff = o.spin_omegaoff;
+        frame_t = o.frame_t; frame_orbspin = o.frame_orbspin;
+        spin_device = o.spin_device;
         finalized = false;
     }
     // bin tuning results

@@ -215,6 +215,33 @@ size_t lc_finalize_smem(int npts, int n);
 cudaError_t configure_lc_finalize();
 void launch_lc_finalize(const LcFinalizeArgs &a, cudaStream_t s);
 
+// Spin realization inside an evaluation (spin.cu; principal-axis
+// rotators): one thread per radar frame (its epoch view) or lightcurve point
+// realizes ae (and a frame's spin vector) from the device spin state and
+// its dataset's offsets, then the view constants as the host sets them.
+struct SpinViewSrc {
+    int kind;                   // 0 radar frame, 1 lightcurve point
+    int index;                  // global radar frame or point index
+    int rec;                    // dataset record: offsets at off[6 rec ..]
+    int dd;                     // delay-Doppler set of a radar frame
+    double t;                   // epoch (light-time corrected)
+    double orb[3];              // orbital spin contribution (radar frames)
+};
+struct SpinRealizeArgs {
+    int n;
+    const SpinViewSrc *src;
+    const shape_spin_state *spin;
+    const double *off;                 // per record: angleoff[3], omegaoff[3]
+    shape_deldop_frame *frames;        // ae and spin written
+    const shape_deldop_set *ddsets;
+    shape_lghtcrv_point *points;       // ae written
+    FrameGeom *geoms;
+    FrameHost *fh;
+    double *dop_extra;
+    LcPointDev *lcpts;
+};
+void launch_realize_views(const SpinRealizeArgs &a, cudaStream_t s);
+
 struct SetRec { int type; int first; int count; };   // type 0 deldop (frames), 1 lightcurve (set index)
 struct SummaryArgs {
     int nsets;

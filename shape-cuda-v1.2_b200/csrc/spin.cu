@@ -11,61 +11,14 @@
 #include <cmath>
 
 #include "engine_impl.h"
+#include "spin_impl.cuh"
+
+using shape::euler_zxz;
+using shape::impulse_path;
+using shape::spin_pa_body;
+using shape::spin_to_ecliptic;
 
 namespace {
-
-// Rotation from ecliptic to body axes for z-x-z Euler angles (phi, theta,
-// psi): rows are the body axes in ecliptic coordinates.
-void euler_zxz(double m[3][3], double phi, double theta, double psi)
-{
-    const double ct = std::cos(theta), st = std::sin(theta);
-    const double cf = std::cos(phi), sf = std::sin(phi);
-    const double cp = std::cos(psi), sp = std::sin(psi);
-    m[0][0] = cp * cf - ct * sf * sp;
-    m[1][0] = -sp * cf - ct * sf * cp;
-    m[2][0] = st * sf;
-    m[0][1] = cp * sf + ct * cf * sp;
-    m[1][1] = -sp * sf + ct * cf * cp;
-    m[2][1] = -st * cf;
-    m[0][2] = sp * st;
-    m[1][2] = cp * st;
-    m[2][2] = ct;
-}
-
-// Epochs from t0 to t with the impulses met on the way (negated when t is
-// before t0), as the reference lists them (realize_impulse).
-int impulse_path(const shape_spin_state &sp, double t, double *te, double (*imp)[3])
-{
-    int k = 0;
-    te[0] = sp.t0;
-    imp[0][0] = imp[0][1] = imp[0][2] = 0.0;
-    if (t >= sp.t0) {
-        for (int n = 0; n < sp.n_impulse; n++)
-            if (sp.t_impulse[n] > sp.t0 && sp.t_impulse[n] <= t) {
-                k++;
-                te[k] = sp.t_impulse[n];
-                for (int j = 0; j < 3; j++) imp[k][j] = sp.impulse[n][j];
-            }
-        if (te[k] < t) {
-            k++;
-            te[k] = t;
-            imp[k][0] = imp[k][1] = imp[k][2] = 0.0;
-        }
-    } else {
-        for (int n = sp.n_impulse - 1; n >= 0; n--)
-            if (sp.t_impulse[n] < sp.t0 && sp.t_impulse[n] >= t) {
-                k++;
-                te[k] = sp.t_impulse[n];
-                for (int j = 0; j < 3; j++) imp[k][j] = -sp.impulse[n][j];
-            }
-        if (te[k] > t) {
-            k++;
-            te[k] = t;
-            imp[k][0] = imp[k][1] = imp[k][2] = 0.0;
-        }
-    }
-    return k + 1;
-}
 
 // Torque-free rotation: y = (w in body coordinates, then the three ecliptic
 // axes in body coordinates, the columns of ae). Euler's equations for w;
@@ -182,32 +135,9 @@ extern "C" int shape_realize_spin(const shape_spin_state *spin, const double ang
             for (int j = 0; j < 3; j++)
                 for (int i = 0; i < 3; i++) m[i][j] = y[3 + 3 * j + i];
         } else {
-            const double dt = te[ne - 1] - te[0];
-            // principal-axis kinematics: psi advances with the z spin, its drift
-            // and the libration; z impulses add to the rate from their epochs
-            double psi = psi0 + spin->omega[2] * dt + 0.5 * spin->omegadot[2] * dt * dt +
-                         spin->lib_amp * std::sin(spin->lib_freq * dt + spin->lib_phase);
-            for (int i = 0; i < 2; i++) w[i] = spin->omega[i] + spin->omegadot[i] * dt;
-            w[2] = spin->omega[2] + spin->omegadot[2] * dt +
-                   spin->lib_amp * spin->lib_freq * std::cos(spin->lib_freq * dt + spin->lib_phase);
-            for (int k = 0; k < ne; k++) {
-                psi += imp[k][2] * (te[ne - 1] - te[k]);
-                w[2] += imp[k][2];
-            }
-            euler_zxz(m, phi, theta, psi);
+            spin_pa_body(*spin, phi, theta, psi0, te, imp, ne, m, w);
         }
-        // the dataset's spin offsets (body frame), then body -> ecliptic
-        // (transpose of ae), plus the orbital contribution
-        for (int j = 0; j < 3; j++) w[j] += omegaoff[j];
-        double e[3];
-        for (int i = 0; i < 3; i++) {
-            e[i] = 0.0;
-            for (int j = 0; j < 3; j++) e[i] += m[j][i] * w[j];
-        }
-        for (int i = 0; i < 3; i++) {
-            for (int j = 0; j < 3; j++) ae[9 * (size_t)v + 3 * i + j] = m[i][j];
-            spin_out[3 * (size_t)v + i] = orbspin[3 * (size_t)v + i] + e[i];
-        }
+        spin_to_ecliptic(m, w, omegaoff, &orbspin[3 * (size_t)v], &ae[9 * (size_t)v], &spin_out[3 * (size_t)v]);
     }
     return SHAPE_OK;
 }
@@ -371,3 +301,49 @@ extern "C" int shape_delcor_offsets(const double *a, int n, double t0, double t_
     *dopoff = -dop * Ftx / (dop_per_pixel * 86400.0);
     return SHAPE_OK;
 }
+
+namespace shape {
+
+__global__ void k_realize_views(SpinRealizeArgs a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const SpinViewSrc v = a.src[i];
+    const double *ao = a.off + 6 * (size_t)v.rec, *oo = ao + 3;
+    if (v.kind == 0) {
+        shape_deldop_frame F = a.frames[v.index];
+        realize_spin_pa(*a.spin, ao, oo, v.t, v.orb, F.ae, F.spin);
+        for (int k = 0; k < 9; k++) a.frames[v.index].ae[k] = F.ae[k];
+        for (int k = 0; k < 3; k++) a.frames[v.index].spin[k] = F.spin[k];
+        FrameHost h = a.fh[v.index];
+        FrameGeom g = a.geoms[h.view];
+        double dx;
+        radar_view_geom(g, h, dx, F, a.ddsets[v.dd]);
+        view_float_consts(g);
+        a.geoms[h.view] = g;
+        a.fh[v.index] = h;
+        a.dop_extra[v.index] = dx;
+    } else {
+        shape_lghtcrv_point P = a.points[v.index];
+        const double zero[3] = {0.0, 0.0, 0.0};
+        double unused[3];
+        realize_spin_pa(*a.spin, ao, oo, v.t, zero, P.ae, unused);
+        for (int k = 0; k < 9; k++) a.points[v.index].ae[k] = P.ae[k];
+        LcPointDev pd = a.lcpts[v.index];
+        FrameGeom go = a.geoms[pd.obs_view], gs = a.geoms[pd.sun_view];
+        lc_view_geom(go, gs, pd, P);
+        view_float_consts(go);
+        view_float_consts(gs);
+        a.geoms[pd.obs_view] = go;
+        a.geoms[pd.sun_view] = gs;
+        a.lcpts[v.index] = pd;
+    }
+}
+
+void launch_realize_views(const SpinRealizeArgs &a, cudaStream_t s)
+{
+    if (a.n <= 0) return;
+    k_realize_views<<<(a.n + 63) / 64, 64, 0, s>>>(a);
+}
+
+}  // namespace shape

@@ -127,6 +127,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_set_bin_capacity.argtypes = [vp, C.c_int]
     L.shape_engine_set_fp32_exact.argtypes = [vp, C.c_int]
     L.shape_engine_set_raster_tuning.argtypes = [vp, C.c_int]
+    L.shape_engine_set_spin_device.argtypes = [vp, C.c_int]
+    L.shape_engine_get_frame_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr]
     L.shape_engine_get_raster_tuning.argtypes = [vp, C.c_int, P(C.c_int), P(C.c_int), cd.dptr]
     L.shape_engine_set_frame_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.dptr, C.c_double, C.c_double]
     L.shape_engine_set_point_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr, cd.dptr]
@@ -301,6 +303,17 @@ class Engine:
         whose decisions lie within FP32 error by the FP64 rules; False keeps
         the FP32 decisions (faster raster)."""
         _chk(self.L.shape_engine_set_fp32_exact(self.h, 1 if exact else 0))
+
+    def set_spin_device(self, on=True):
+        """Realize the views from the spin model inside each evaluation
+        (principal-axis rotators): spin trials replay the graph only."""
+        _chk(self.L.shape_engine_set_spin_device(self.h, 1 if on else 0))
+
+    def frame_view(self, frame):
+        """(ae 3x3, spin vector) of radar frame `frame` as last realized."""
+        ae, sp = np.zeros(9), np.zeros(3)
+        _chk(self.L.shape_engine_get_frame_view(self.h, int(frame), cd.as_dptr(ae), cd.as_dptr(sp)))
+        return ae.reshape(3, 3), sp
 
     def set_raster_tuning(self, mode=-1):
         """-1: time the raster candidates at each batched form's first

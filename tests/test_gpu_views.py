@@ -258,3 +258,85 @@ def test_spin_fit_recovers_rotation_phase(cuda_device):
     assert res["final_objective"] < 1e-3 * res["initial_objective"], res
     assert len(trace) == res["trace_len"] > 5
     e.close()
+
+
+def test_device_spin_matches_host_realization(cuda_device):
+    """shape_engine_set_spin_device: views realized inside the evaluation
+    graph from the spin state. Against host realization (shape_realize_spin,
+    bit-exact with the reference) of the same trials: ae and spin vectors to
+    a few units in the last place (CUDA's sin / cos against the C
+    library's), chi-square to 1e-10 in the FP64 forms and 1e-6 in FP32, and
+    a spin trial costs no host realization (set_spin_param only records the
+    value)."""
+    m, p, ds = cases.c2(12)
+    t = T0 + 0.04 * np.arange(ds.nframes)
+    host = eng.make_engine(m, p, deldops=[ds])
+    dev = eng.make_engine(m, p, deldops=[ds])
+    for e in (host, dev):
+        e.set_spin_model(_pa_spin(0.3), t, None, None)
+    dev.set_spin_device(True)
+    n0 = host.kernels_per_eval(eng.FORM_BATCHED_FP64)
+    assert dev.kernels_per_eval(eng.FORM_BATCHED_FP64) == n0 + 1
+    trials = [(eng.PAR_SPIN_ANGLE, 2, 0.37), (eng.PAR_SPIN_OMEGA, 2, 2 * np.pi / 0.26),
+              (eng.PAR_SPIN_ANGLE, 0, 0.55), (eng.PAR_ANGLEOFF, 1, 0.01), (eng.PAR_OMEGAOFF, 2, 0.2)]
+    for kind, index, value in [(None, None, None)] + trials:
+        if kind is not None:
+            host.set_spin_param(kind, index, value)
+            dev.set_spin_param(kind, index, value)
+        for form in FORMS:
+            sh, sd = host.evaluate(form), dev.evaluate(form)
+            tol = FP32_CHI2_RTOL if form == eng.FORM_BATCHED_FP32 else CHI2_RTOL
+            assert abs(sd["chi2"] - sh["chi2"]) <= tol * abs(sh["chi2"]), (kind, index, form)
+        for f in range(ds.nframes):
+            ah, wh = host.frame_view(f)
+            ad, wd = dev.frame_view(f)
+            assert np.max(np.abs(ad - ah)) <= 4e-16, (kind, f)
+            assert np.max(np.abs(wd - wh)) <= 4e-15 * np.max(np.abs(wh)), (kind, f)
+    with pytest.raises(eng.EngineError, match="realized on the device"):
+        dev.set_frame_view(0, np.eye(3), np.eye(3), np.zeros(3))
+    # back to host realization: the host views catch up with the trials
+    dev.set_spin_device(False)
+    a, b = dev.evaluate(eng.FORM_BATCHED_FP64)["chi2"], host.evaluate(eng.FORM_BATCHED_FP64)["chi2"]
+    assert abs(a - b) <= 1e-12 * abs(b)
+    for f in range(ds.nframes):
+        assert np.array_equal(dev.frame_view(f)[0], host.frame_view(f)[0])
+    host.close()
+    dev.close()
+
+
+def test_device_spin_lightcurves(cuda_device):
+    """Device spin realization of lightcurve points (observer and sun views)
+    against host realization, with dataset angle offsets."""
+    m, p, sets = cases.c3(12, 2)
+    spin = eng.spin_state(1, float(sets[0].x[0]), (0.2, 1.1, 0.4), (0.0, 0.0, 2 * np.pi / 0.3))
+    aoff = np.array([[0.0, 0.0, 0.0], [0.01, -0.02, 0.03]])
+    host = eng.make_engine(m, p, lghtcrvs=sets)
+    dev = eng.make_engine(m, p, lghtcrvs=sets)
+    for e in (host, dev):
+        e.set_spin_model(spin, None, None, aoff)
+    dev.set_spin_device(True)
+    for kind, index, value in [(None, None, None), (eng.PAR_SPIN_ANGLE, 2, 0.45), (eng.PAR_ANGLEOFF, 4, -0.01)]:
+        if kind is not None:
+            host.set_spin_param(kind, index, value)
+            dev.set_spin_param(kind, index, value)
+        for form in FORMS:
+            sh, sd = host.evaluate(form), dev.evaluate(form)
+            tol = FP32_CHI2_RTOL if form == eng.FORM_BATCHED_FP32 else CHI2_RTOL
+            assert abs(sd["chi2"] - sh["chi2"]) <= tol * abs(sh["chi2"]), (kind, form)
+            for k, d in enumerate(sets):
+                np.testing.assert_allclose(dev.lghtcrv(k, d)["y"], host.lghtcrv(k, d)["y"], rtol=1e-12)
+    host.close()
+    dev.close()
+
+
+def test_device_spin_refusals(cuda_device):
+    m, p, ds = cases.c2(4)
+    e = eng.make_engine(m, p, deldops=[ds])
+    with pytest.raises(eng.EngineError, match="no spin model"):
+        e.set_spin_device(True)
+    t = T0 + 0.04 * np.arange(ds.nframes)
+    npa = eng.spin_state(0, T0, (0.5, 0.9, 0.3), (0.1, 0.2, 2 * np.pi / 0.25), inertia=(1.0, 1.1, 1.2))
+    e.set_spin_model(npa, t)
+    with pytest.raises(eng.EngineError, match="principal-axis"):
+        e.set_spin_device(True)
+    e.close()
