@@ -673,5 +673,16 @@ def main():
     return 0
 
 
+def _json_stdout():
+    """Keeps stdout for the JSON line: the reference's C code prints per-point
+    lines to fd 1 (chi2_lghtcrv, src/shape/chi2.c:1147), so fd 1 is pointed
+    at stderr and Python's stdout writes to a copy of the original fd 1."""
+    real = os.dup(1)
+    sys.stdout.flush()
+    os.dup2(2, 1)
+    sys.stdout = os.fdopen(real, "w", buffering=1)
+
+
 if __name__ == "__main__":
+    _json_stdout()
     sys.exit(main())

@@ -5,8 +5,9 @@ runs the fastest, and a second engine of the same size class reuses the
 choice without timing again.
 
 Bars: facet, z and cos(e) maps bit-exact between candidates (FP64 batched
-form, and the FP32 form's exact variant); chi-square to relative 1e-12 (the
-scatter-add order differs between kernels)."""
+form, and the FP32 form's exact variant); fit images and chi-square to
+relative 1e-12 in FP64 and 1e-5 / 1e-6 in FP32 (the scatter-add order
+differs between kernels and launches, and FP32 images round each add)."""
 import numpy as np
 import pytest
 
@@ -45,12 +46,13 @@ def test_candidates_agree(cuda_device, form):
         if ref is None:
             ref = (s, maps, fits)
             continue
+        fit_tol, chi2_tol = (1e-5, 1e-6) if form == eng.FORM_BATCHED_FP32 else (1e-12, 1e-12)
         for f in range(ds.nframes):
             for k in ("f", "z", "cose"):
                 assert np.array_equal(maps[f][k], ref[1][f][k]), (mode, f, k)
             scale = max(np.abs(ref[2][f]).max(), 1e-300)
-            assert np.abs(fits[f] - ref[2][f]).max() <= 1e-12 * scale, (mode, f)
-        assert abs(s["chi2"] - ref[0]["chi2"]) <= 1e-12 * abs(ref[0]["chi2"]), mode
+            assert np.abs(fits[f] - ref[2][f]).max() <= fit_tol * scale, (mode, f)
+        assert abs(s["chi2"] - ref[0]["chi2"]) <= chi2_tol * abs(ref[0]["chi2"]), mode
 
 
 def test_choice_is_shared_by_size_class(cuda_device):
@@ -62,8 +64,9 @@ def test_choice_is_shared_by_size_class(cuda_device):
     e2.evaluate(eng.FORM_BATCHED_FP32)
     b = e2.raster_tuning(eng.FORM_BATCHED_FP32)
     assert a == b
-    # the same datasets through both engines: the same chi-square
+    # the same datasets through both engines: the same chi-square to the
+    # FP32 images' scatter-order rounding
     assert e1.evaluate(eng.FORM_BATCHED_FP32)["chi2"] == pytest.approx(
-        e2.evaluate(eng.FORM_BATCHED_FP32)["chi2"], rel=1e-12)
+        e2.evaluate(eng.FORM_BATCHED_FP32)["chi2"], rel=1e-6)
     e1.close()
     e2.close()
