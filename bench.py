@@ -503,6 +503,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-mix measurement")
     ap.add_argument("--no-per-config", action="store_true", help="skip the configs 1, 3, 4 block")
+    ap.add_argument("--raster-tuning", type=int, default=-1, choices=[-1, 0, 1],
+                    help="-1: autotune the raster kernel; 0 / 1: the tile-per-CTA / warp kernel (profiling)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, ws, lrank, dist = dist_setup()
@@ -530,6 +533,7 @@ def main():
         dds = [shard.shard_dataset(glob, rank, ws)[0]]
         desc += "; %d frames in all, frame blocks balanced by POS + delay-Doppler pixels" % (64 * ws)
     E = eng.make_engine(model, params, deldops=dds, lghtcrvs=lcs, device=lrank)
+    E.set_raster_tuning(args.raster_tuning)
     form = eng.FORMS[args.form]
     nu = units(dds, lcs)
     flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device="cuda")
@@ -575,7 +579,7 @@ def main():
         return dev_ms, host_ms
 
     # plain FP64 GPU path (the metric's comparison point), a few steps
-    plain_dev, _ = run(eng.FORM_PLAIN_FP64, max(3, min(args.steps, 10)), 2, False)
+    plain_dev = [float("nan")] if args.no_plain else run(eng.FORM_PLAIN_FP64, max(3, min(args.steps, 10)), 2, False)[0]
     clocks = ClockSampler(lrank)
     clocks.start()
     time.sleep(0.3)
@@ -587,7 +591,7 @@ def main():
     # the FP32 form with shape_engine_set_fp32_exact(0) (radar views keep
     # their FP32 coverage decisions), a short run beside the default
     fast = None
-    if form == eng.FORM_BATCHED_FP32 and not lcs:
+    if form == eng.FORM_BATCHED_FP32 and not lcs and not args.no_plain:
         E.set_fp32_exact(False)
         fx_ms, _ = run(form, max(20, min(args.steps, 100)), 3, False)
         E.set_scale(0, trial(0))           # both forms at the same scale factors
