@@ -24,12 +24,19 @@
 
 #include "kernels.h"
 
-// Resident CTAs per SM the register allocation must allow (FP32 / FP64).
-// Both rasters are latency-bound: FP32 at 8 CTAs (32 registers, spills to
-// L1) measured faster than 6 (40), 5 (48) and 4 (64); FP64 at 4 CTAs (64
-// registers) faster than 3 (80).
+// Resident CTAs per SM the register allocation must allow (FP32 / FP32
+// exact variant / FP64). The rasters are latency-bound: the FP32 kernel at
+// 8 CTAs (32 registers, spills to L1) measured faster than 6 (40), 5 (48)
+// and 4 (64) on 64 uneven frames (0.188 ms against 0.195 / 0.194 / 0.210);
+// its exact variant, with the error bounds live through the replay, is
+// fastest at 6 (0.207 ms against 0.264 at 8, 0.214 at 5, 0.225 at 4; 16
+// frames of 511x511: 0.295 against 0.311); FP64 at 4 CTAs (64 registers)
+// faster than 3 (80).
 #ifndef RASTER_MIN_BLOCKS
 #define RASTER_MIN_BLOCKS 8
+#endif
+#ifndef RASTER_MIN_BLOCKS_EXACT
+#define RASTER_MIN_BLOCKS_EXACT 6
 #endif
 #ifndef RASTER_MIN_BLOCKS_F64
 #define RASTER_MIN_BLOCKS_F64 4
@@ -827,7 +834,8 @@ __device__ inline unsigned long long warp_kmax(unsigned long long k)
 // assignment, depth and the shadow test's inputs are the FP64 form's;
 // without it (radar views) the FP32 test is posvis's with FP32 values.
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(RASTER_THREADS, sizeof(T) == 8 ? RASTER_MIN_BLOCKS_F64 : RASTER_MIN_BLOCKS)
+__global__ void __launch_bounds__(RASTER_THREADS, sizeof(T) == 8 ? RASTER_MIN_BLOCKS_F64
+                                                  : (EXACT ? RASTER_MIN_BLOCKS_EXACT : RASTER_MIN_BLOCKS))
 k_raster(RasterArgs a)
 {
     grid_dep_wait();
