@@ -1101,7 +1101,8 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         if (!lc_items.empty()) {
             la.items = d_lc_items;
             la.nitems = (int)lc_items.size();
-            launch_lc_photo(la, f32 ? 1 : 0, s);
+            // lightcurve views hold FP64 cosines in both forms
+            launch_lc_photo(la, 0, s);
         }
         mark(6);
     }
@@ -1732,7 +1733,7 @@ static int copy_pos(EngineImpl &E, int view, double *z, double *cose, double *co
     for (int k = 0; k < 3; k++) {
         if (!bufs[k]) continue;
         cudaError_t e;
-        if (f32 && k > 0) {        // depth maps are FP64 in both forms
+        if (f32 && k > 0 && g.kind == shape::VIEW_RADAR) {   // depth maps, and lightcurve views' cosines, are FP64 in both forms
             std::vector<float> tmp(np);
             e = cudaMemcpy(tmp.data(), (float *)src[k] + g.pos_base, sizeof(float) * np, cudaMemcpyDeviceToHost);
             for (size_t i = 0; i < np; i++) bufs[k][i] = tmp[i];

@@ -750,6 +750,72 @@ __device__ inline double facet_depth64(const double4 *vt, int4 c, double x0, dou
     return __dadd_rn(__dadd_rn(p0.z, __dmul_rn(sv, E)), __dmul_rn(tv, F));
 }
 
+// FP32 form, lightcurve views: cos(e) and cos(i) of a pixel from its good
+// facet gf (the last winner whose smoothed normal faced the viewer; the
+// winner itself without smoothing) with the FP64 form's values and
+// operations, rounded op by op: the interpolated vertex normal at the pixel
+// centre, its view coordinates, normalization and the sun direction
+// (src/shape/posvis.c:250-274). The brightness sums then equal the FP64
+// form's: a lightcurve's chi-square is a small difference of large sums
+// (floating calibration, 1 % noise), which magnifies FP32 cosines' rounding.
+static __device__ void lc_cos64(const RasterArgs &a, const FrameGeom &g, int gf, double x0, double y0,
+                                bool smooth, bool bistatic_obs, double *ce, double *ci)
+{
+    double n0, n1, n2;
+    if (smooth) {
+        const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
+        const int4 c = a.fvi[gf];
+        const double4 p0 = vt[c.x], p1 = vt[c.y], p2 = vt[c.z];
+        const double A = __dsub_rn(p2.y, p1.y), B = __dsub_rn(p2.x, p1.x);
+        const double C = __dsub_rn(p1.x, p0.x), D = __dsub_rn(p1.y, p0.y);
+        const double den = 1.0 / __dsub_rn(__dmul_rn(C, A), __dmul_rn(B, D));
+        const double dx = __dsub_rn(x0, p0.x), dy = __dsub_rn(y0, p0.y);
+        const double sv = __dmul_rn(__dsub_rn(__dmul_rn(dx, A), __dmul_rn(B, dy)), den);
+        const double tv = __dmul_rn(__dsub_rn(__dmul_rn(C, dy), __dmul_rn(dx, D)), den);
+        const double4 q0 = a.vn[c.x], q1 = a.vn[c.y], q2 = a.vn[c.z];
+        const double m0 = __dadd_rn(__dadd_rn(q0.x, __dmul_rn(sv, __dsub_rn(q1.x, q0.x))),
+                                    __dmul_rn(tv, __dsub_rn(q2.x, q1.x)));
+        const double m1 = __dadd_rn(__dadd_rn(q0.y, __dmul_rn(sv, __dsub_rn(q1.y, q0.y))),
+                                    __dmul_rn(tv, __dsub_rn(q2.y, q1.y)));
+        const double m2 = __dadd_rn(__dadd_rn(q0.z, __dmul_rn(sv, __dsub_rn(q1.z, q0.z))),
+                                    __dmul_rn(tv, __dsub_rn(q2.z, q1.z)));
+        double r[3];
+        for (int k = 0; k < 3; k++)
+            r[k] = __dadd_rn(__dadd_rn(__dmul_rn(g.oa[3 * k], m0), __dmul_rn(g.oa[3 * k + 1], m1)),
+                             __dmul_rn(g.oa[3 * k + 2], m2));
+        const double norm = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(r[0], r[0]), __dmul_rn(r[1], r[1])),
+                                                 __dmul_rn(r[2], r[2])));
+        if (norm != 0.0)
+            for (int k = 0; k < 3; k++) r[k] = __ddiv_rn(r[k], norm);
+        n0 = r[0]; n1 = r[1]; n2 = r[2];
+    } else {
+        const double4 nb = a.fn[gf];
+        double nn[3];
+        for (int k = 0; k < 3; k++)
+            nn[k] = __dadd_rn(__dadd_rn(__dmul_rn(g.oa[3 * k], nb.x), __dmul_rn(g.oa[3 * k + 1], nb.y)),
+                              __dmul_rn(g.oa[3 * k + 2], nb.z));
+        n0 = nn[0]; n1 = nn[1]; n2 = nn[2];
+    }
+    *ce = 0.0;
+    *ci = 0.0;
+    if (n2 > 0.0) {
+        *ce = n2;
+        if (bistatic_obs) {
+            *ci = __dadd_rn(__dadd_rn(__dmul_rn(n0, g.usrc[0]), __dmul_rn(n1, g.usrc[1])), __dmul_rn(n2, g.usrc[2]));
+            if (*ci <= 0.0) *ce = 0.0;
+        }
+    }
+}
+
+// The first smoothed-normal component of a good winner, or (FP32 form,
+// lightcurve views: lcv) the winner's facet index in its bits.
+template <typename T>
+__device__ inline T good_tag(bool lcv, int f, T v)
+{
+    if constexpr (sizeof(T) == 4) return lcv ? __int_as_float(f) : v;
+    else return v;
+}
+
 // FP32 form, rare path: posvis at one pixel by the FP64 form's rules (the
 // FP64 visit's s, t, depth and tolerance, rounded op by op; its update rule
 // and order-dependent smoothed normal), over the tile's bin in facet order.
@@ -758,7 +824,7 @@ __device__ inline double facet_depth64(const double4 *vt, int4 c, double x0, dou
 // (-1: none) and writes its FP64 depth and the cos(e) state.
 static __device__ RARE_FN int pixel_posvis64(const RasterArgs &a, const FrameGeom &g, const int2 *ids,
                                                   int count, int li, int lj, double x0, double y0, double *zz,
-                                                  bool *good, float *gm)
+                                                  bool *good, float *gm, int *gf)
 {
     const double4 *vt = static_cast<const double4 *>(a.vt) + g.vt_base;
     double zw = -SHAPE_HUGENUMBER;
@@ -794,7 +860,7 @@ static __device__ RARE_FN int pixel_posvis64(const RasterArgs &a, const FrameGeo
             r2 = __dadd_rn(r2, __dmul_rn(g.oa[6], m0));
             r2 = __dadd_rn(r2, __dmul_rn(g.oa[7], m1));
             r2 = __dadd_rn(r2, __dmul_rn(g.oa[8], m2));
-            if (r2 > 0.0) { *good = true; gm[0] = (float)m0; gm[1] = (float)m1; gm[2] = (float)m2; }
+            if (r2 > 0.0) { *good = true; gm[0] = (float)m0; gm[1] = (float)m1; gm[2] = (float)m2; *gf = e.x; }
         } else {
             const double4 nb = a.fn[e.x];
             double nn[3];
@@ -804,7 +870,7 @@ static __device__ RARE_FN int pixel_posvis64(const RasterArgs &a, const FrameGeo
                 nn[r] = __dadd_rn(nn[r], __dmul_rn(g.oa[3 * r + 1], nb.y));
                 nn[r] = __dadd_rn(nn[r], __dmul_rn(g.oa[3 * r + 2], nb.z));
             }
-            *good = true; gm[0] = (float)nn[0]; gm[1] = (float)nn[1]; gm[2] = (float)nn[2];
+            *good = true; gm[0] = (float)nn[0]; gm[1] = (float)nn[1]; gm[2] = (float)nn[2]; *gf = e.x;
         }
     }
     *zz = zw;
@@ -893,6 +959,9 @@ k_raster(RasterArgs a)
         T gm0 = 0, gm1 = 0, gm2 = 0;
         const bool smooth = g.smooth != 0;
         const bool bistatic_obs = (g.kind == VIEW_LC_OBS);
+        // FP32 form, lightcurve views: the good facet's index rides in gm0's
+        // bits, and the cosines are recomputed from it in FP64 (lc_cos64)
+        const bool lcv = (sizeof(T) == 4) && EXACT && (g.kind != VIEW_RADAR);
         const T oa6 = (T)g.oa[6], oa7 = (T)g.oa[7], oa8 = (T)g.oa[8];
 
         // Apply posvis's update rule for one staged facet at this pixel.
@@ -967,9 +1036,9 @@ k_raster(RasterArgs a)
                 r2 += oa6 * m0; r2 += oa7 * m1; r2 += oa8 * m2;
                 if constexpr (sizeof(T) == 4 && EXACT)     // the sign of r2 within FP32 error
                     amb = amb || (fabsf(r2) <= 4 * (s.es + s.et) + 1e-6f * (fabsf(m0) + fabsf(m1) + fabsf(m2)));
-                if (r2 > (T)0) { good = true; gm0 = m0; gm1 = m1; gm2 = m2; }
+                if (r2 > (T)0) { good = true; gm0 = good_tag<T>(lcv, s.f, m0); gm1 = m1; gm2 = m2; }
             } else {
-                good = true; gm0 = p2.z; gm1 = p2.w; gm2 = s.nz;
+                good = true; gm0 = good_tag<T>(lcv, s.f, p2.z); gm1 = p2.w; gm2 = s.nz;
             }
         };
         // Each warp walks only the staged facets whose bbox meets its block,
@@ -1093,17 +1162,24 @@ k_raster(RasterArgs a)
                 float gmv[3] = {0.0f, 0.0f, 0.0f};
                 double zw;
                 good = false;
+                int gfv = -1;
                 fac = pixel_posvis64(a, g, ids, count, li, lj, (double)pi * g.kmpp, (double)pj * g.kmpp, &zw,
-                                     &good, gmv);
+                                     &good, gmv, &gfv);
                 zz = (float)zw;
                 zlo = (float)(zw - (double)zz);
-                gm0 = gmv[0]; gm1 = gmv[1]; gm2 = gmv[2];
+                gm0 = good_tag<T>(lcv, gfv, gmv[0]); gm1 = gmv[1]; gm2 = gmv[2];
             }
         }
 
         // cos(e) / cos(i) of the last winner whose smoothed normal faced the
         // viewer: cotrans + normalize (posvis.c:250-274), once per pixel
-        if (good) {
+        double ce64 = 0.0, ci64 = 0.0;      // lcv: the FP64 cosines
+        if (good && lcv) {
+            lc_cos64(a, g, __float_as_int((float)gm0), (double)pi * g.kmpp, (double)pj * g.kmpp, smooth,
+                     bistatic_obs, &ce64, &ci64);
+            cosa = (T)ce64;
+            cosb = (T)ci64;
+        } else if (good) {
             T n0 = gm0, n1 = gm1, n2 = gm2;
             T oa[12];
             load_oa<T>(g, oa);
@@ -1161,8 +1237,13 @@ k_raster(RasterArgs a)
             }
             Z[p] = z64;
             a.pos_f[p] = fac;
-            CE[p] = cosa;                        // cos(e), or cos(i) in the sun view (pos->cosill)
-            if (g.kind != VIEW_LC_SUN) CI[p] = cosb;
+            if (lcv) {                           // FP32 form, lightcurve views: FP64 cosines
+                static_cast<double *>(a.pos_cose)[p] = ce64;
+                if (g.kind != VIEW_LC_SUN) static_cast<double *>(a.pos_cosi)[p] = ci64;
+            } else {
+                CE[p] = cosa;                    // cos(e), or cos(i) in the sun view (pos->cosill)
+                if (g.kind != VIEW_LC_SUN) CI[p] = cosb;
+            }
         }
         // covered-pixel bbox (POSrect with (i,i,j,j), posvis.c:278-280)
         int cimin = covered ? pi : INT_MAX, cimax = covered ? pi : INT_MIN;
@@ -1469,8 +1550,9 @@ k_raster_w(RasterArgs a)
                 float gmv[3] = {0.0f, 0.0f, 0.0f};
                 double zw;
                 good = false;
+                int gfv = -1;
                 fac = pixel_posvis64(a, g, ids, nb, li, lj, (double)pi * g.kmpp, (double)pj * g.kmpp, &zw, &good,
-                                     gmv);
+                                     gmv, &gfv);
                 zz = (float)zw;
                 zlo = (float)(zw - (double)zz);
                 gm0 = gmv[0]; gm1 = gmv[1]; gm2 = gmv[2];
