@@ -325,7 +325,20 @@ def serving_bench(lrank, nreq=4000, rate=2000.0, budget=64 << 30, slots=16):
                 "instances_evicted_in_run": st["instances_evicted"],
                 "peak_hbm_gb": st["peak_hbm_bytes"] / 1e9}
 
+    # the step byte model of each workload (bytes per request, by form): the
+    # served requests' bytes over the run's time give the serving mix's
+    # achieved bandwidth beside the measured HBM peak
+    peak, _ = peak_hbm()
+
+    def req_bytes(s_elem):
+        out_b = []
+        for (_, m, dd_, lc_) in work:
+            bm, bp, bd, _ = algorithmic_bytes(m, dd_, lc_, s_elem)
+            out_b.append(bm + bp + bd)
+        return out_b
+
     for name, form in (("fp32", eng.FORM_BATCHED_FP32), ("fp64", eng.FORM_BATCHED_FP64)):
+        wbytes = req_bytes(4 if name == "fp32" else 8)
         srv = eng.Server(lrank, budget, slots)
         t0 = time.perf_counter()
         eng.register_workloads(srv, work, params, form, lrank)
@@ -334,6 +347,10 @@ def serving_bench(lrank, nreq=4000, rate=2000.0, budget=64 << 30, slots=16):
         res, st = srv.run(trace)
         chi[name] = np.array([r["chi2"] for r in res])
         out[name] = {"offered": stats(st), "registration_s": t_reg}
+        mean_b = float(np.mean([wbytes[w] for (w, _, _) in trace]))
+        gbs = mean_b * st["requests_per_s"] / 1e9
+        out[name]["offered"]["roofline"] = {"bound": "hbm", "achieved_gbs": gbs, "peak_gbs": peak,
+                                            "frac": gbs / peak, "bytes_per_request": mean_b}
         if sus_rate is None:
             sus_rate = 0.6 * st["requests_per_s"]
         tr2 = synth.serving_trace(cats, int(sus_rate * 3.0), sus_rate, seed=2027)

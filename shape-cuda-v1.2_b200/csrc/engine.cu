@@ -1084,6 +1084,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
             rl.nwork = (int)work.size() - work_radar;
             rl.exact = 1;
             rl.variant = 0;       // lightcurve views: the tile-per-CTA kernel
+            rl.lc_views = 1;
             rl.grid = raster_grid(form, nonempty_lc, rl, true);
             launch_raster_f32(rr, s);
             launch_raster_f32(rl, s);

@@ -82,6 +82,10 @@ struct RasterArgs {
     // sorted facet list and meet at block barriers); 1: the warp-independent
     // kernel (k_raster_w: each warp sorts and replays its own block's list)
     int variant;
+    // FP32 form: the launch holds only lightcurve views, whose cosines the
+    // exact variant recomputes in FP64 (a separate instantiation, so radar
+    // launches carry none of it)
+    int lc_views;
 };
 
 // core.cu (FP64, no FMA contraction)

@@ -899,7 +899,7 @@ __device__ inline unsigned long long warp_kmax(unsigned long long k)
 // decision within FP32 error is redone by the FP64 form's rules, so facet
 // assignment, depth and the shadow test's inputs are the FP64 form's;
 // without it (radar views) the FP32 test is posvis's with FP32 values.
-template <typename T, bool EXACT>
+template <typename T, bool EXACT, bool LCV = false>
 __global__ void __launch_bounds__(RASTER_THREADS, sizeof(T) == 8 ? RASTER_MIN_BLOCKS_F64
                                                   : (EXACT ? RASTER_MIN_BLOCKS_EXACT : RASTER_MIN_BLOCKS))
 k_raster(RasterArgs a)
@@ -959,9 +959,10 @@ k_raster(RasterArgs a)
         T gm0 = 0, gm1 = 0, gm2 = 0;
         const bool smooth = g.smooth != 0;
         const bool bistatic_obs = (g.kind == VIEW_LC_OBS);
-        // FP32 form, lightcurve views: the good facet's index rides in gm0's
-        // bits, and the cosines are recomputed from it in FP64 (lc_cos64)
-        const bool lcv = (sizeof(T) == 4) && EXACT && (g.kind != VIEW_RADAR);
+        // FP32 form, lightcurve views (their own launch, LCV): the good
+        // facet's index rides in gm0's bits, and the cosines are recomputed
+        // from it in FP64 (lc_cos64); radar launches compile this out
+        const bool lcv = (sizeof(T) == 4) && EXACT && LCV && (g.kind != VIEW_RADAR);
         const T oa6 = (T)g.oa[6], oa7 = (T)g.oa[7], oa8 = (T)g.oa[8];
 
         // Apply posvis's update rule for one staged facet at this pixel.
@@ -1702,7 +1703,13 @@ inline cudaError_t configure_raster_t()
 {
     cudaError_t e = configure_raster_one<T, false>();
     if (e != cudaSuccess || sizeof(T) == 8) return e;
-    return configure_raster_one<T, true>();
+    e = configure_raster_one<T, true>();
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_raster<T, true, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_raster<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    return e;
 }
 
 template <typename T>
@@ -1722,7 +1729,9 @@ inline void launch_raster_t(const RasterArgs &a, cudaStream_t s)
         return;
     }
     b.smem_bytes = raster_smem_bytes<T>(a.cap, a.nf);
-    if (sizeof(T) == 4 && a.exact)
+    if (sizeof(T) == 4 && a.exact && a.lc_views)
+        launch_k(k_raster<T, true, true>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
+    else if (sizeof(T) == 4 && a.exact)
         launch_k(k_raster<T, true>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
     else
         launch_k(k_raster<T, false>, dim3(grid), dim3(RASTER_THREADS), b.smem_bytes, s, a.pdl != 0, b);
@@ -1742,7 +1751,9 @@ inline int raster_occupancy_t(const RasterArgs &a)
                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raster_w<T, false>, RASTER_THREADS, sm);
     } else {
         const size_t sm = raster_smem_bytes<T>(a.cap, a.nf);
-        e = (sizeof(T) == 4 && a.exact)
+        e = (sizeof(T) == 4 && a.exact && a.lc_views)
+                ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raster<T, true, true>, RASTER_THREADS, sm)
+            : (sizeof(T) == 4 && a.exact)
                 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raster<T, true>, RASTER_THREADS, sm)
                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_raster<T, false>, RASTER_THREADS, sm);
     }
