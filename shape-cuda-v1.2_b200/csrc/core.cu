@@ -161,11 +161,18 @@ __global__ void k_xform_realize(const FrameGeom *__restrict__ geoms, const doubl
 
 // -------------------------------------------------------------- binning
 
+// Resident 256-thread blocks per SM the binning kernel's registers must
+// allow: it waits on dependent loads (normal and corners, then the bin
+// atomics), so more blocks in flight hide more of that latency.
+#ifndef BIN_MIN_BLOCKS
+#define BIN_MIN_BLOCKS 6
+#endif
+
 // Facet culling, bounding box, outbnd flag and POSrect bookkeeping of
 // posvis (src/shape/posvis.c:142-199, 322-364), then one bin entry per
 // overlapped 16x16 tile. Bin order is arbitrary; the raster kernel sorts.
 template <typename T4>
-__global__ void k_bin(const FrameGeom *__restrict__ geoms, int view0, int nf,
+__global__ void __launch_bounds__(256, BIN_MIN_BLOCKS) k_bin(const FrameGeom *__restrict__ geoms, int view0, int nf,
                       const int4 *__restrict__ fvi, const double4 *__restrict__ fn,
                       const T4 *__restrict__ vt, FrameState *__restrict__ states,
                       int *__restrict__ bin_count, int2 *__restrict__ bin_ids, int cap)
@@ -175,13 +182,15 @@ __global__ void k_bin(const FrameGeom *__restrict__ geoms, int view0, int nf,
     if (f >= nf) return;
     int v = view0 + blockIdx.y;
     const FrameGeom &g = geoms[v];
-    double4 nb = fn[f];
+    // the normal and the corner indices load together (the culling test
+    // does not wait for the indices); the corners follow
+    const double4 nb = fn[f];
+    const int4 c = fvi[f];
     double nz = 0.0;
     nz += g.oa[6] * nb.x;
     nz += g.oa[7] * nb.y;
     nz += g.oa[8] * nb.z;
     if (!(nz > 0.0)) return;
-    int4 c = fvi[f];
     T4 p0 = vt[g.vt_base + c.x], p1 = vt[g.vt_base + c.y], p2 = vt[g.vt_base + c.z];
     const double kmpp = g.kmpp;
     const int n = g.n;
@@ -310,41 +319,103 @@ __device__ inline KSum shfl_ksum(KSum a, int off)
 // o2 = sum obs^2/var, m2 = sum fit^2/var, om = sum fit*obs/var, each
 // product in the reference's order, accumulated with compensation.
 template <typename T>
-__device__ void chi2_item_partials(const Chi2Args &a, int it, const Chi2Item &item, double (*red)[6], double *part);
+__device__ void chi2_item_warp(const Chi2Args &a, int it, const Chi2Item &item, double *part);
 
+// Resident 256-thread blocks per SM of the chi-square kernels: a warp keeps
+// its item's 48 loads in flight, so residency trades against registers.
+#ifndef CHI2_MIN_BLOCKS
+#define CHI2_MIN_BLOCKS 2
+#endif
+
+// One warp per item, items in grid-stride order over the block's warps.
 template <typename T>
-__global__ void k_chi2_partials(Chi2Args a)
+__global__ void __launch_bounds__(CHI2_THREADS, CHI2_MIN_BLOCKS) k_chi2_partials(Chi2Args a)
 {
-    __shared__ double red[CHI2_THREADS / 32][6];
-    for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
-        chi2_item_partials<T>(a, it, a.items[it], red, a.partials + (size_t)it * 6);
-        __syncthreads();
+    const int wpb = blockDim.x >> 5;
+    for (int it = blockIdx.x * wpb + (threadIdx.x >> 5); it < a.nitems; it += gridDim.x * wpb)
+        chi2_item_warp<T>(a, it, a.items[it], a.partials + (size_t)it * 6);
+}
+
+// A frame's three sums from its item partials (6 per item: o2, m2, om, each
+// a compensated sum and its compensation) in one fixed order: lane l of a
+// warp merges items l, l+32, l+64, ... in turn, then the lanes' sums merge
+// pairwise (l with l+16, l+8, ..., l+1), and the frame's start values (a
+// Doppler frame's overflow o2 and m2, else 0) take the result last.
+// frame_sums_warp does this with the 32 lanes; frame_sums_serial computes
+// the same numbers in one thread, so the batched and plain forms agree
+// bit for bit.
+__device__ inline void ksum_take(KSum &q, const double *p)
+{
+    q.add(p[0]);
+    q.c += p[1];
+}
+__device__ void frame_sums_warp(const double *part, int nitems, const double start[3], KSum out[3], bool via_l2)
+{
+    const int lane = threadIdx.x & 31;
+    KSum q[3] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int it = lane; it < nitems; it += 32)
+        for (int k = 0; k < 3; k++) {
+            double p[2];
+            p[0] = via_l2 ? __ldcg(part + (size_t)it * 6 + 2 * k) : part[(size_t)it * 6 + 2 * k];
+            p[1] = via_l2 ? __ldcg(part + (size_t)it * 6 + 2 * k + 1) : part[(size_t)it * 6 + 2 * k + 1];
+            ksum_take(q[k], p);
+        }
+    for (int off = 16; off > 0; off >>= 1)
+        for (int k = 0; k < 3; k++) q[k].merge(shfl_ksum(q[k], off));
+    for (int k = 0; k < 3; k++) {
+        out[k].s = start[k];
+        out[k].c = 0.0;
+        out[k].merge(q[k]);
+    }
+}
+__device__ void frame_sums_serial(const double *part, int nitems, const double start[3], KSum out[3])
+{
+    KSum q[32][3];
+    for (int l = 0; l < 32; l++)
+        for (int k = 0; k < 3; k++) q[l][k] = KSum{0, 0};
+    for (int it = 0; it < nitems; it++)
+        for (int k = 0; k < 3; k++) ksum_take(q[it & 31][k], part + (size_t)it * 6 + 2 * k);
+    for (int off = 16; off > 0; off >>= 1)
+        for (int l = 0; l < off; l++)
+            for (int k = 0; k < 3; k++) q[l][k].merge(q[l + off][k]);
+    for (int k = 0; k < 3; k++) {
+        out[k].s = start[k];
+        out[k].c = 0.0;
+        out[k].merge(q[0][k]);
     }
 }
 
 // A frame's chi-square terms: chi2_deldop's sums, calibration and
 // chi-square (src/shape/chi2.c:436-460) from the frame's item partials.
 // part: the chi-square partials (6 per item), in global or shared memory;
-// part0: the index of the frame's first item in part.
-__device__ void finalize_frame_chi2(const FinalizeArgs &a, int fr, const double *part, int part0,
-                                    shape_deldop_result &r)
+// part0: the index of the frame's first item in part. One thread.
+__device__ inline void frame_start(const FinalizeArgs &a, const FrameHost &h, double start[3])
 {
-    const FrameHost &h = a.fh[fr];
     // a Doppler frame's sums start from its overflow spectrum's o2 and m2
     // (src/shape/chi2.c:745-747)
     const double *ovf = (h.dop_index >= 0) ? a.ovf_out + (size_t)h.dop_index * DOP_OVF_TERMS : nullptr;
-    KSum q[3] = {{ovf ? ovf[0] : 0.0, 0}, {ovf ? ovf[1] : 0.0, 0}, {0, 0}};
-    for (int it = 0; it < h.nitems; it++)
-        for (int k = 0; k < 3; k++) {
-            q[k].add(part[(size_t)(part0 + it) * 6 + 2 * k]);
-            q[k].c += part[(size_t)(part0 + it) * 6 + 2 * k + 1];
-        }
+    start[0] = ovf ? ovf[0] : 0.0;
+    start[1] = ovf ? ovf[1] : 0.0;
+    start[2] = 0.0;
+}
+__device__ void frame_chi2_from_sums(const FrameHost &h, const KSum q[3], shape_deldop_result &r)
+{
     double o2 = q[0].value(), m2 = q[1].value(), om = q[2].value();
     double cal = h.cal_in;
     if (h.cal_floating)
         cal = (om > 0.0) ? om / m2 : SHAPE_TINYCALFACT;
     r.o2 = o2; r.m2 = m2; r.om = om; r.cal = cal;
     r.chi2 = h.weight * (o2 - 2 * cal * om + cal * cal * m2);
+}
+__device__ void finalize_frame_chi2(const FinalizeArgs &a, int fr, const double *part, int part0,
+                                    shape_deldop_result &r)
+{
+    const FrameHost &h = a.fh[fr];
+    double start[3];
+    frame_start(a, h, start);
+    KSum q[3];
+    frame_sums_serial(part + (size_t)part0 * 6, h.nitems, start, q);
+    frame_chi2_from_sums(h, q, r);
 }
 
 // A frame's posvis / pos2deldop outputs (limits, flags, log-factors), which
@@ -815,40 +886,40 @@ __device__ void summary_totals(const SummaryArgs &a, Term term)
     *a.out = out;
 }
 
-// One item's chi-square partial sums (the body of k_chi2_partials), left by
-// thread 0 in part[0..5]: each thread sums its bins in order, the threads'
-// sums merge with compensation (warp shuffles, then the block's warps in
-// order). With a.o2pre set, o2 is the item's precomputed partial and obs /
-// 1/var are read only where the fit is nonzero: a zero fit bin adds exact
-// zeros to m2 and om, so the sums keep their values.
+// One item's chi-square partial sums, left by lane 0 of the calling warp in
+// part[0..5]: each lane sums its 16 bins (lane, lane + 32, ...) in order in
+// plain FP64, then the lanes' sums merge with compensation by warp shuffles
+// (pairwise: l with l+16, l+8, ..., l+1). With a.o2pre set, o2 is the item's
+// precomputed partial and obs / 1/var are read only where the fit is
+// nonzero: a zero fit bin adds exact zeros to m2 and om, so the sums keep
+// their values.
 template <typename T>
-__device__ void chi2_item_partials(const Chi2Args &a, int it, const Chi2Item &item, double (*red)[6], double *part)
+__device__ void chi2_item_warp(const Chi2Args &a, int it, const Chi2Item &item, double *part)
 {
+    const int lane = threadIdx.x & 31;
     const FrameGeom &g = a.geoms[a.frame_view[item.frame]];
     const long long base = g.fit_base + item.start;
     const T *fit = static_cast<const T *>(a.fit) + base;
     const double *obs = a.obs + base, *oov = a.oov + base;
     const bool pre = a.o2pre != nullptr;
-    T ft[CHI2_ITEMS];
-    double ob[CHI2_ITEMS], wv[CHI2_ITEMS];
+    T ft[CHI2_LANE];
 #pragma unroll
-    for (int j = 0; j < CHI2_ITEMS; j++) {
-        const int k = threadIdx.x + j * CHI2_THREADS;
+    for (int j = 0; j < CHI2_LANE; j++) {
+        const int k = lane + 32 * j;
         ft[j] = (k < item.count) ? fit[k] : (T)0;
     }
+    double ob[CHI2_LANE], wv[CHI2_LANE];
 #pragma unroll
-    for (int j = 0; j < CHI2_ITEMS; j++) {
-        const int k = threadIdx.x + j * CHI2_THREADS;
+    for (int j = 0; j < CHI2_LANE; j++) {
+        const int k = lane + 32 * j;
         const bool in = (k < item.count) && (!pre || ft[j] != (T)0);
         ob[j] = in ? obs[k] : 0.0;
         wv[j] = in ? oov[k] : 0.0;
     }
-    // a thread's own bins (at most CHI2_ITEMS) summed in bin order in plain
-    // FP64; the compensated sums start where the threads' sums merge
     double so2 = 0.0, sm2 = 0.0, som = 0.0;
 #pragma unroll
-    for (int j = 0; j < CHI2_ITEMS; j++) {
-        if (threadIdx.x + j * CHI2_THREADS >= item.count) break;
+    for (int j = 0; j < CHI2_LANE; j++) {
+        if (lane + 32 * j >= item.count) break;
         const double f = (double)ft[j];
         if (!pre) so2 += ob[j] * ob[j] * wv[j];
         sm2 += f * f * wv[j];
@@ -860,115 +931,83 @@ __device__ void chi2_item_partials(const Chi2Args &a, int it, const Chi2Item &it
         m2.merge(shfl_ksum(m2, off));
         om.merge(shfl_ksum(om, off));
     }
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-        red[w][0] = o2.s; red[w][1] = o2.c; red[w][2] = m2.s;
-        red[w][3] = m2.c; red[w][4] = om.s; red[w][5] = om.c;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        KSum r[3] = {{0, 0}, {0, 0}, {0, 0}};
-        for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++)
-            for (int q = 0; q < 3; q++) {
-                r[q].add(red[ww][2 * q]);
-                r[q].c += red[ww][2 * q + 1];
-            }
+    if (lane == 0) {
         if (pre) {
-            r[0].s = a.o2pre[2 * (size_t)it];
-            r[0].c = a.o2pre[2 * (size_t)it + 1];
+            o2.s = a.o2pre[2 * (size_t)it];
+            o2.c = a.o2pre[2 * (size_t)it + 1];
         }
-        for (int q = 0; q < 3; q++) {
-            part[2 * q] = r[q].s;
-            part[2 * q + 1] = r[q].c;
-        }
+        part[0] = o2.s; part[1] = o2.c;
+        part[2] = m2.s; part[3] = m2.c;
+        part[4] = om.s; part[5] = om.c;
     }
 }
 
-// Chi-square partials, per-frame results and totals in one launch. Blocks
-// first fill each frame's chi-square-independent outputs (limits, flags,
-// log-factors: finalize_frame_geom), one frame per block, then compute
-// chunks (items) as k_chi2_partials does. A frame's counter takes one count
-// for its outputs and one per item; the block that makes the last count
-// adds the frame's chi-square terms from its items' partials in item order,
-// and the block that completes the last frame computes the totals in
-// dataset order. The sums and their order are those of k_chi2_partials +
-// k_summary, so the results are the same. Values another block wrote in
-// this launch are read through L2 (__ldcg) after a fence. counters:
-// [nframes] per frame, then the finished frames; zero before the launch.
+// Chi-square partials, per-frame results and totals in one launch, warp by
+// warp with no block barrier: each warp takes (frame, 512-bin) items in
+// grid-stride order. A frame's counter takes one count per item; the warp
+// that makes the frame's last count merges the frame's item partials
+// (frame_sums_warp, the order k_summary's frame_sums_serial reproduces) and
+// writes the frame's results (limits, flags, log-factors and chi-square
+// terms), and the warp that completes the last frame computes the totals in
+// dataset order, as k_chi2_partials + k_summary do. Values another warp
+// wrote in this launch are read through L2 (__ldcg) after a fence.
+// counters: [nframes] per frame, then the finished frames; zero before the
+// launch.
 template <typename T>
-__global__ void __launch_bounds__(CHI2_THREADS) k_chi2_summary(Chi2Args ca, FinalizeArgs fa, SummaryArgs sa,
+__global__ void __launch_bounds__(CHI2_THREADS, CHI2_MIN_BLOCKS) k_chi2_summary(Chi2Args ca, FinalizeArgs fa, SummaryArgs sa,
                                                                int *counters)
 {
-    __shared__ double red[CHI2_THREADS / 32][6];
-    extern __shared__ __align__(16) unsigned char stage[];   // chi2_summary_smem bytes
-    __shared__ int s_last;
+    extern __shared__ __align__(16) unsigned char stage[];   // chi2_summary_smem bytes (the totals)
     grid_dep_wait();
-    double *s_part = reinterpret_cast<double *>(stage);
-    const int nwork = fa.nframes + ca.nitems;
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        int fr;
-        if (w < fa.nframes) {                                 // a frame's outputs
-            fr = w;
-            if (threadIdx.x == 0) {
-                shape_deldop_result r;
-                finalize_frame_geom(fa, fr, r);
-                shape_deldop_result *out = fa.results + fr;
-                out->xlim[0] = r.xlim[0]; out->xlim[1] = r.xlim[1];
-                out->ylim[0] = r.ylim[0]; out->ylim[1] = r.ylim[1];
-                out->outbnd = r.outbnd; out->posbnd_logfactor = r.posbnd_logfactor;
-                out->badradar = r.badradar; out->badradar_logfactor = r.badradar_logfactor;
-                out->idellim[0] = r.idellim[0]; out->idellim[1] = r.idellim[1];
-                out->idoplim[0] = r.idoplim[0]; out->idoplim[1] = r.idoplim[1];
-                out->dellim[0] = r.dellim[0]; out->dellim[1] = r.dellim[1];
-                out->doplim[0] = r.doplim[0]; out->doplim[1] = r.doplim[1];
-            }
-        } else {                                              // a chunk's partials
-            const int it = w - fa.nframes;
-            const Chi2Item item = ca.items[it];
-            chi2_item_partials<T>(ca, it, item, red, ca.partials + (size_t)it * 6);
-            fr = item.frame;
-        }
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (int it = blockIdx.x * wpb + (threadIdx.x >> 5); it < ca.nitems; it += gridDim.x * wpb) {
+        const Chi2Item item = ca.items[it];
+        chi2_item_warp<T>(ca, it, item, ca.partials + (size_t)it * 6);
+        const int fr = item.frame;
         const FrameHost &h = fa.fh[fr];
-        if (threadIdx.x == 0) {
-            __threadfence();                                  // outputs / partials before the count
-            s_last = (atomicAdd(&counters[fr], 1) == h.nitems);
+        int last = 0;
+        if (lane == 0) {
+            __threadfence();                                  // the partials before the count
+            last = (atomicAdd(&counters[fr], 1) == h.nitems - 1);
         }
-        __syncthreads();
-        if (s_last) {                                         // block-uniform
-            __threadfence();
-            // the frame's partials to shared memory, then its chi-square terms
-            for (int k = threadIdx.x; k < 6 * h.nitems; k += blockDim.x)
-                s_part[k] = __ldcg(ca.partials + (size_t)h.item0 * 6 + k);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                shape_deldop_result r;
-                finalize_frame_chi2(fa, fr, s_part, 0, r);
-                shape_deldop_result *out = fa.results + fr;
-                out->o2 = r.o2; out->m2 = r.m2; out->om = r.om; out->cal = r.cal; out->chi2 = r.chi2;
-                __threadfence();                              // results before the count
-                s_last = (atomicAdd(&counters[fa.nframes], 1) == fa.nframes - 1);
-            }
-            __syncthreads();
-            if (s_last) {
-                __threadfence();
-                double *s_chi2 = reinterpret_cast<double *>(stage);
-                double *s_plog = s_chi2 + fa.nframes, *s_blog = s_plog + fa.nframes;
-                unsigned char *s_flag = reinterpret_cast<unsigned char *>(s_blog + fa.nframes);
-                for (int f = threadIdx.x; f < fa.nframes; f += blockDim.x) {
-                    const shape_deldop_result *r = fa.results + f;
-                    s_chi2[f] = __ldcg(&r->chi2);
-                    s_plog[f] = fa.fh[f].dof * __ldcg(&r->posbnd_logfactor);
-                    s_blog[f] = frame_blog(fa.fh[f], __ldcg(&r->badradar_logfactor));
-                    s_flag[f] = (__ldcg(&r->outbnd) ? 1 : 0) | (frame_bad(fa.fh[f], __ldcg(&r->badradar)) ? 2 : 0);
-                }
-                __syncthreads();
-                if (threadIdx.x == 0)
-                    summary_totals(sa, [&](int f, double &c, double &pl, double &bl, int &fl) {
-                        c = s_chi2[f]; pl = s_plog[f]; bl = s_blog[f]; fl = s_flag[f];
-                    });
-            }
+        last = __shfl_sync(full, last, 0);
+        if (!last) continue;                                  // warp-uniform
+        __threadfence();
+        double start[3];
+        frame_start(fa, h, start);
+        KSum q[3];
+        frame_sums_warp(ca.partials + (size_t)h.item0 * 6, h.nitems, start, q, true);
+        int lastf = 0;
+        if (lane == 0) {
+            shape_deldop_result r;
+            finalize_frame_geom(fa, fr, r);
+            frame_chi2_from_sums(h, q, r);
+            fa.results[fr] = r;
+            __threadfence();                                  // the results before the count
+            lastf = (atomicAdd(&counters[fa.nframes], 1) == fa.nframes - 1);
         }
-        __syncthreads();
+        lastf = __shfl_sync(full, lastf, 0);
+        if (!lastf) continue;
+        // the totals: this warp stages every frame's terms in shared memory
+        // (the only warp of the grid that uses it), then lane 0 sums them in
+        // dataset order
+        __threadfence();
+        double *s_chi2 = reinterpret_cast<double *>(stage);
+        double *s_plog = s_chi2 + fa.nframes, *s_blog = s_plog + fa.nframes;
+        unsigned char *s_flag = reinterpret_cast<unsigned char *>(s_blog + fa.nframes);
+        for (int f = lane; f < fa.nframes; f += 32) {
+            const shape_deldop_result *r = fa.results + f;
+            s_chi2[f] = __ldcg(&r->chi2);
+            s_plog[f] = fa.fh[f].dof * __ldcg(&r->posbnd_logfactor);
+            s_blog[f] = frame_blog(fa.fh[f], __ldcg(&r->badradar_logfactor));
+            s_flag[f] = (__ldcg(&r->outbnd) ? 1 : 0) | (frame_bad(fa.fh[f], __ldcg(&r->badradar)) ? 2 : 0);
+        }
+        __syncwarp();
+        if (lane == 0)
+            summary_totals(sa, [&](int f, double &c, double &pl, double &bl, int &fl) {
+                c = s_chi2[f]; pl = s_plog[f]; bl = s_blog[f]; fl = s_flag[f];
+            });
     }
 }
 
@@ -1029,7 +1068,9 @@ void launch_bin_f64(const FrameGeom *g, int view0, int nviews, const ModelDev &m
 
 void launch_chi2_partials(const Chi2Args &a, int fp32, cudaStream_t s)
 {
-    int blocks = a.nitems < 8 * 148 ? a.nitems : 8 * 148;
+    const int wpb = CHI2_THREADS / 32;               // one warp per item
+    const int need = (a.nitems + wpb - 1) / wpb;
+    int blocks = need < 8 * 148 ? need : 8 * 148;
     if (blocks <= 0) return;
     if (fp32) k_chi2_partials<float><<<blocks, CHI2_THREADS, 0, s>>>(a);
     else k_chi2_partials<double><<<blocks, CHI2_THREADS, 0, s>>>(a);
@@ -1088,8 +1129,8 @@ cudaError_t configure_summary()
 
 size_t chi2_summary_smem(int nframes, int max_frame_items)
 {
-    const size_t a = (size_t)nframes * 25, b = (size_t)max_frame_items * 6 * sizeof(double);
-    return ((a > b ? a : b) + 15) & ~(size_t)15;
+    (void)max_frame_items;          // a frame's partials merge in registers
+    return ((size_t)nframes * 25 + 15) & ~(size_t)15;
 }
 
 bool chi2_summary_fits(int nframes, int max_frame_items)
@@ -1100,8 +1141,9 @@ bool chi2_summary_fits(int nframes, int max_frame_items)
 void launch_chi2_summary(const Chi2Args &ca, const FinalizeArgs &fa, const SummaryArgs &sa, int *counters,
                          int fp32, cudaStream_t s, bool pdl, size_t smem)
 {
-    const int nwork = fa.nframes + ca.nitems;       // frame outputs, then chunks
-    int blocks = nwork < 8 * 148 ? nwork : 8 * 148;
+    const int wpb = CHI2_THREADS / 32;               // one warp per item
+    const int need = (ca.nitems + wpb - 1) / wpb;
+    const int blocks = need < 8 * 148 ? need : 8 * 148;
     if (blocks <= 0 || ca.nitems <= 0) return;
     if (fp32) launch_k(k_chi2_summary<float>, dim3(blocks), dim3(CHI2_THREADS), smem, s, pdl, ca, fa, sa, counters);
     else launch_k(k_chi2_summary<double>, dim3(blocks), dim3(CHI2_THREADS), smem, s, pdl, ca, fa, sa, counters);

@@ -182,7 +182,7 @@ int EngineImpl::finalize()
             if (g.dop1d) dop_frames.push_back(fi);
             frame_view.push_back(h.view);
             h.item0 = (int)chi2_items.size();
-            int D = F.ndel * F.ndop, chunk = CHI2_THREADS * CHI2_ITEMS;
+            int D = F.ndel * F.ndop, chunk = CHI2_ITEM;
             for (int st = 0; st < D; st += chunk)
                 chi2_items.push_back(Chi2Item{fi, st, std::min(chunk, D - st)});
             h.nitems = (int)chi2_items.size() - h.item0;

@@ -24,7 +24,8 @@ constexpr int TILE_PIX = TILE_W * TILE_W;
 constexpr int RASTER_THREADS = TILE_PIX;
 constexpr int STAGE_FACETS = 128;   // facets staged in shared memory per pass
 constexpr int CHI2_THREADS = 256;
-constexpr int CHI2_ITEMS = 8;       // elements per thread per chi2 block
+constexpr int CHI2_LANE = 16;       // bins per lane of a chi-square item
+constexpr int CHI2_ITEM = 32 * CHI2_LANE;   // bins per item: one warp's
 constexpr int FIT32_PAD = 16;       // FP32 fit arena padding (vector reductions, k_raster)
 constexpr int DOP_MAXOVERFLOW = 2000;   // Doppler overflow spectrum bins (MAXOVERFLOW, src/shape/const.h:181)
 
