@@ -322,9 +322,11 @@ template <typename T>
 __device__ void chi2_item_warp(const Chi2Args &a, int it, const Chi2Item &item, double *part);
 
 // Resident 256-thread blocks per SM of the chi-square kernels: a warp keeps
-// its item's 48 loads in flight, so residency trades against registers.
+// its item's 48 loads in flight, so residency trades against registers (on
+// 64 uneven frames: 3 blocks, 80 registers, 28.6 us; 2 blocks, 120
+// registers, 31.5 us; 4 blocks, 64 registers, 30.7 us).
 #ifndef CHI2_MIN_BLOCKS
-#define CHI2_MIN_BLOCKS 2
+#define CHI2_MIN_BLOCKS 3
 #endif
 
 // One warp per item, items in grid-stride order over the block's warps.
