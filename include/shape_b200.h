@@ -641,9 +641,16 @@ typedef struct shape_obs_options {
 /* A SHAPE observation file (.obs; read_dat, src/shape/read_dat.c:409-527)
  * whose datasets are delay-Doppler sets (read_deldop, :528-900) or Doppler
  * sets (read_doppler, :920-1180) or lightcurve / heliocurve sets
- * (read_lghtcrv, :1667-2063) with one view per frame or point and no
- * pixel-weighting masks or gzipped data files (those, and plane-of-sky
- * sets, return SHAPE_E_UNSUPPORTED). The '=' state of angle and
+ * (read_lghtcrv, :1667-2063); smeared delay-Doppler frames and
+ * pixel-weighting masks are read, gzipped data files, smeared Doppler
+ * frames or lightcurve points and plane-of-sky sets return
+ * SHAPE_E_UNSUPPORTED. A frame with a pixel-weighting mask
+ * (mask_SS_FF.txt, FFF for sets of more than 100 frames, in the set's data
+ * directory unless shape_obs_set_maskdir names another) keeps the window
+ * of its positive weights: its ndel x ndop, COM and DC bins count from the
+ * window, its dof is weight x the positive weights, and its 1/variance is
+ * multiplied by the weights (src/shape/read_dat.c:696-762, 845-852,
+ * 1059-1118). The '=' state of angle and
  * spin offsets and of delay-correction polynomials takes the last earlier
  * set's value, as the reference's realize_angleoff, realize_omegaoff and
  * realize_delcor do (src/shape/realize_spin.c:283-337,
@@ -651,6 +658,9 @@ typedef struct shape_obs_options {
  * polynomial of another degree or epoch, is SHAPE_E_ARG. Host code. */
 typedef struct shape_obs_file shape_obs_file;
 int shape_obs_read(const char *path, shape_obs_file **out);
+/* The .par file's mask directory (par->maskdir): the masks of every
+ * weighted frame are read again from dir (a missing file is SHAPE_E_ARG). */
+int shape_obs_set_maskdir(shape_obs_file *o, const char *dir);
 void shape_obs_free(shape_obs_file *o);
 int shape_obs_nsets(const shape_obs_file *o);
 /* 0: set s is a delay-Doppler set (shape_obs_set / shape_obs_frames);

@@ -702,6 +702,15 @@ struct shape_obs_file {
         std::string name;
         double t0, sdev, cal, nlooks, delcom, weight;
         char cal_state;
+        // pixel-weighting mask (src/shape/read_dat.c:696-762, 1059-1118):
+        // its weights (delay-major, the full image), or empty when the
+        // frame has none or its mask file is not loaded; the window of
+        // positive weights (1-based, inclusive: delay, then Doppler) and
+        // the frame's dof
+        int weighted = 0;
+        std::vector<double> mask;
+        int win[4] = {1, 1, 1, 1};
+        double dof = 0.0;
     };
     struct Set {
         int doppler = 0;                 // 1: a Doppler set (read_doppler)
@@ -732,6 +741,7 @@ struct shape_obs_file {
         std::vector<double> lc_t0, lc_mag, lc_magerr;   // the data file's points
     };
     std::vector<Set> sets;
+    std::string maskdir;                 // "" : the sets' data directories
 };
 
 // An ephemeris table: a count, then per entry an epoch (yyyy mm dd hh mm
@@ -858,6 +868,89 @@ static void tie_obs_sets(std::vector<shape_obs_file::Set> &sets, const Tokens &t
 
 extern "C" {
 
+// The frames' windows and dof, and the pixel-weighting masks of set s
+// (read_deldop / read_doppler, src/shape/read_dat.c:696-762, 1059-1118):
+// mask_SS_FF.txt (FFF when the set has more than 100 frames) in the mask
+// directory, or the set's data directory without one; ndel x ndop weights
+// (ndop for a Doppler set) whose positive entries give the frame's window
+// and its dof (the frame's weight per positive entry). A frame without a
+// mask keeps the whole image and weight x pixels of dof. A missing mask
+// file is an error only when required (shape_obs_set_maskdir); otherwise the
+// frame stays unloaded and the set's accessors report it.
+static int load_masks(shape_obs_file &o, int s, bool required)
+{
+    shape_obs_file::Set &S = o.sets[s];
+    if (S.lightcurve) return SHAPE_OK;
+    const int nf = (int)S.frames.size();
+    const int nd = S.doppler ? 1 : S.ndel, np = S.ndop;
+    const std::string dir = o.maskdir.empty() ? S.dir : o.maskdir;
+    for (int f = 0; f < nf; f++) {
+        shape_obs_file::Frame &F = S.frames[f];
+        F.mask.clear();
+        if (!F.weighted) {
+            F.win[0] = 1; F.win[1] = nd; F.win[2] = 1; F.win[3] = np;
+            F.dof = F.weight * nd * np;
+            continue;
+        }
+        char name[64];
+        snprintf(name, sizeof name, nf > 100 ? "mask_%02d_%03d.txt" : "mask_%02d_%02d.txt", s, f);
+        const std::string path = dir + "/" + name;
+        FILE *fp = fopen(path.c_str(), "rb");
+        if (!fp) {
+            if (required) return shape::report_error(SHAPE_E_ARG, "obs: cannot open mask file " + path);
+            continue;
+        }
+        std::string text;
+        char buf[1 << 16];
+        size_t got;
+        while ((got = fread(buf, 1, sizeof buf, fp)) > 0) text.append(buf, got);
+        fclose(fp);
+        std::vector<double> w;
+        try {
+            Tokens tk(std::move(text));
+            const std::string kind = "mask file " + path;
+            tk.set_kind(kind.c_str());
+            std::string t;
+            while (tk.next(t)) {
+                char *end = nullptr;
+                const double v = strtod(t.c_str(), &end);
+                if (*end != '\0') tk.fail("expected a number (mask weight), got " + t);
+                w.push_back(v);
+            }
+        } catch (const ParseError &e) {
+            return shape::report_error(e.code, "obs: " + e.msg);
+        }
+        if ((long long)w.size() != (long long)nd * np)
+            return shape::report_error(SHAPE_E_ARG, "obs: mask file " + path + " holds " + std::to_string(w.size()) +
+                                                        " weights, expected " + std::to_string((long long)nd * np));
+        int d0 = nd + 1, d1 = 0, p0 = np + 1, p1 = 0;
+        double dof = 0.0;
+        for (int j = 1; j <= nd; j++)
+            for (int k = 1; k <= np; k++)
+                if (w[(size_t)(j - 1) * np + (k - 1)] > 0.0) {
+                    dof += F.weight;
+                    d0 = std::min(d0, j); d1 = std::max(d1, j);
+                    p0 = std::min(p0, k); p1 = std::max(p1, k);
+                }
+        if (d1 < d0) return shape::report_error(SHAPE_E_ARG, "obs: mask file " + path + " has no positive weight");
+        F.win[0] = d0; F.win[1] = d1; F.win[2] = p0; F.win[3] = p1;
+        F.dof = dof;
+        F.mask = std::move(w);
+    }
+    return SHAPE_OK;
+}
+
+// Set s's frames all have their masks (loaded at shape_obs_read or by
+// shape_obs_set_maskdir).
+static int masks_ready(const shape_obs_file::Set &S, const char *what)
+{
+    for (const shape_obs_file::Frame &F : S.frames)
+        if (F.weighted && F.mask.empty())
+            return shape::report_error(SHAPE_E_ARG, std::string(what) + ": the mask of frame " + F.name +
+                                                        " was not found (shape_obs_set_maskdir)");
+    return SHAPE_OK;
+}
+
 int shape_obs_read(const char *path, shape_obs_file **out)
 {
     if (!path || !out) return shape::report_error(SHAPE_E_ARG, "obs_read: null argument");
@@ -967,8 +1060,7 @@ int shape_obs_read(const char *path, shape_obs_file **out)
                 F.nlooks = tk.real("looks");
                 F.delcom = S.doppler ? 1.0 : tk.real("delay COM bin");
                 F.weight = tk.real("weight");
-                if (tk.integer("pixel weighting") != 0)
-                    tk.fail("pixel-weighting masks are not supported", SHAPE_E_UNSUPPORTED);
+                F.weighted = tk.integer("pixel weighting") != 0;
                 if (F.name.size() >= 3 && F.name.compare(F.name.size() - 3, 3, ".gz") == 0)
                     tk.fail("gzipped data files are not supported", SHAPE_E_UNSUPPORTED);
                 S.frames.push_back(F);
@@ -980,7 +1072,17 @@ int shape_obs_read(const char *path, shape_obs_file **out)
         delete o;
         return shape::report_error(e.code, "obs_read: " + e.msg);
     }
+    for (size_t s = 0; s < o->sets.size(); s++) load_masks(*o, (int)s, false);
     *out = o;
+    return SHAPE_OK;
+}
+
+int shape_obs_set_maskdir(shape_obs_file *o, const char *dir)
+{
+    if (!o || !dir) return shape::report_error(SHAPE_E_ARG, "obs_set_maskdir: null argument");
+    o->maskdir = dir;
+    for (size_t s = 0; s < o->sets.size(); s++)
+        if (int rc = load_masks(*o, (int)s, true)) return rc;
     return SHAPE_OK;
 }
 
@@ -1010,7 +1112,15 @@ int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *ir
         if (angleoff) angleoff[i] = S.angleoff[i];
         if (omegaoff) omegaoff[i] = S.omegaoff[i];
     }
-    if (nelem) *nelem = S.frames.size() * (size_t)S.ndel * S.ndop;
+    if (nelem) {
+        // each frame's window of positive mask weights (the whole image
+        // without a mask)
+        if (int rc = masks_ready(S, "obs_set")) return rc;
+        size_t n = 0;
+        for (const shape_obs_file::Frame &F : S.frames)
+            n += (size_t)(F.win[1] - F.win[0] + 1) * (size_t)(F.win[3] - F.win[2] + 1);
+        *nelem = n;
+    }
     return SHAPE_OK;
 }
 
@@ -1033,8 +1143,10 @@ static int obs_deldop_views(const shape_obs_file::Set &S, const shape_spin_state
                             double km_per_pixel, const shape_obs_options *opt, shape_deldop_frame *views,
                             double *obs, double *oneovervar, double *sdev)
 {
+    if (int rc = masks_ready(S, "obs_frames")) return rc;
     const int nf = (int)S.frames.size(), nv = S.nviews;
-    const size_t D = (size_t)S.ndel * S.ndop, N = (size_t)nf * nv;
+    const size_t N = (size_t)nf * nv;
+    size_t off = 0;
     std::vector<double> t(N), orb(3 * N), ae(9 * N), sp(3 * N);
     std::vector<shape_deldop_frame> vk(N);     // reference view order
     for (int f = 0; f < nf; f++) {
@@ -1043,13 +1155,15 @@ static int obs_deldop_views(const shape_obs_file::Set &S, const shape_spin_state
         memset(&G, 0, sizeof G);
         G.pos_n = pos_n;
         G.km_per_pixel = km_per_pixel;
-        G.ndel = S.ndel;
-        G.ndop = S.ndop;
-        G.delcom_vig = F.delcom;                 // no mask: the window is the whole image
-        G.dopcom_vig = S.dopcom;
-        G.dopDC_vig = S.dopDC;
+        // the window of the frame's positive mask weights (the whole image
+        // without a mask), its COM and DC bins counted from the window
+        G.ndel = F.win[1] - F.win[0] + 1;
+        G.ndop = F.win[3] - F.win[2] + 1;
+        G.delcom_vig = F.delcom - F.win[0] + 1;
+        G.dopcom_vig = S.dopcom - F.win[2] + 1;
+        G.dopDC_vig = S.dopDC - F.win[2] + 1;
         G.weight = F.weight;
-        G.dof = F.weight * S.ndel * S.ndop;
+        G.dof = F.dof;
         G.cal_floating = F.cal_state == 'f';
         G.cal = F.cal;
         for (int k = 0; k < nv; k++) {
@@ -1067,11 +1181,12 @@ static int obs_deldop_views(const shape_obs_file::Set &S, const shape_spin_state
         }
         if (sdev) sdev[f] = F.sdev;
         const std::string full = S.dir + "/" + F.name;
-        const int dl[2] = {1, S.ndel}, dp[2] = {1, S.ndop};
+        const int dl[2] = {F.win[0], F.win[1]}, dp[2] = {F.win[2], F.win[3]};
         if (int rc = shape_read_radar_data(full.c_str(), S.ndel, S.ndop, dl, dp, opt->big_endian, F.sdev,
-                                           opt->dd_gamma, opt->speckle ? F.nlooks : 0.0, nullptr, obs + f * D,
-                                           oneovervar + f * D))
+                                           opt->dd_gamma, opt->speckle ? F.nlooks : 0.0,
+                                           F.weighted ? F.mask.data() : nullptr, obs + off, oneovervar + off))
             return rc;
+        off += (size_t)G.ndel * G.ndop;
     }
     if (int rc = shape_realize_spin(spin, S.angleoff, S.omegaoff, (int)N, t.data(), orb.data(), ae.data(), sp.data()))
         return rc;
@@ -1127,7 +1242,9 @@ int shape_obs_doppler(const shape_obs_file *o, int s, const shape_spin_state *sp
     set->Ftx = S.dd.Ftx;
     set->dopscale = S.dd.dopscale;
     set->law = law;
+    if (int rc = masks_ready(S, "obs_doppler")) return rc;
     const int nf = (int)S.frames.size();
+    size_t off = 0;
     std::vector<double> t(nf), orb(3 * (size_t)nf), ae(9 * (size_t)nf), sp(3 * (size_t)nf);
     for (int f = 0; f < nf; f++) {
         const shape_obs_file::Frame &F = S.frames[f];
@@ -1142,19 +1259,22 @@ int shape_obs_doppler(const shape_obs_file *o, int s, const shape_spin_state *sp
         if (int rc = shape_delcor_offsets(S.delcor.data(), (int)S.delcor.size() - 1, S.delcor_t0, t[f], 1.0,
                                           S.dd.dop_per_pixel, S.dd.Ftx, &deloff, &G.dopoff))
             return rc;
-        G.ndop = S.ndop;
-        G.dopcom_vig = S.dopcom;                 // no mask: the whole spectrum
+        // the window of the frame's positive mask weights (the whole
+        // spectrum without a mask), its COM bin counted from the window
+        G.ndop = F.win[3] - F.win[2] + 1;
+        G.dopcom_vig = S.dopcom - F.win[2] + 1;
         G.weight = F.weight;
-        G.dof = F.weight * S.ndop;
+        G.dof = F.dof;
         G.cal_floating = F.cal_state == 'f';
         G.cal = F.cal;
         G.sdev = F.sdev;
         const std::string full = S.dir + "/" + F.name;
-        const int dl[2] = {1, 1}, dp[2] = {1, S.ndop};
+        const int dl[2] = {1, 1}, dp[2] = {F.win[2], F.win[3]};
         if (int rc = shape_read_radar_data(full.c_str(), 1, S.ndop, dl, dp, opt->big_endian, F.sdev, 1.0,
-                                           opt->speckle ? F.nlooks : 0.0, nullptr, obs + (size_t)f * S.ndop,
-                                           oneovervar + (size_t)f * S.ndop))
+                                           opt->speckle ? F.nlooks : 0.0, F.weighted ? F.mask.data() : nullptr,
+                                           obs + off, oneovervar + off))
             return rc;
+        off += (size_t)G.ndop;
     }
     if (int rc = shape_realize_spin(spin, S.angleoff, S.omegaoff, nf, t.data(), orb.data(), ae.data(), sp.data()))
         return rc;

@@ -167,6 +167,7 @@ def load_library(path=LIB_PATH):
     L.shape_obs_frames.argtypes = [vp, C.c_int, P(cd.SpinState), C.c_int, C.c_double, P(ObsOptions),
                                    P(cd.DeldopFrame), cd.dptr, cd.dptr, cd.dptr]
     L.shape_obs_views.argtypes = [vp, C.c_int, P(C.c_int), P(C.c_int)]
+    L.shape_obs_set_maskdir.argtypes = [vp, C.c_char_p]
     L.shape_obs_frames_views.argtypes = [vp, C.c_int, P(cd.SpinState), C.c_int, C.c_double, P(ObsOptions),
                                          P(cd.DeldopFrame), cd.dptr, cd.dptr, cd.dptr]
     L.shape_read_lghtcrv_data.argtypes = [C.c_char_p, C.c_int, C.c_double, cd.dptr, cd.dptr, cd.dptr]
@@ -634,11 +635,19 @@ class ObsFile:
         ds.bind()
         return ds
 
-    def doppler(self, s, spin, pos_n, km_per_pixel, nframes, ndop, perform_ltc=1, speckle=0, big_endian=1):
-        """A Doppler set: (shape_doppler_set, frames, obs, 1/variance)."""
+    def set_maskdir(self, path):
+        """The .par file's mask directory: weighted frames' masks read from it."""
+        _chk(self.L.shape_obs_set_maskdir(self.h, os.fsencode(str(path))))
+
+    def doppler(self, s, spin, pos_n, km_per_pixel, nframes=None, ndop=None, perform_ltc=1, speckle=0,
+                big_endian=1):
+        """A Doppler set: (shape_doppler_set, frames, obs, 1/variance); each
+        frame's spectrum is its mask window (the whole spectrum without one)."""
+        info = self.set_info(s)
+        nframes = info["nframes"]
         st = cd.DopplerSet()
         fr = (cd.DopplerFrame * nframes)()
-        obs, oov = np.zeros(nframes * ndop), np.zeros(nframes * ndop)
+        obs, oov = np.zeros(info["nelem"]), np.zeros(info["nelem"])
         opt = ObsOptions(perform_ltc, 1.0, speckle, big_endian)
         _chk(self.L.shape_obs_doppler(self.h, s, C.byref(spin), int(pos_n), float(km_per_pixel), C.byref(opt),
                                       C.byref(st), fr, cd.as_dptr(obs), cd.as_dptr(oov)))

@@ -142,9 +142,11 @@ def test_obs_refusals(tmp_path, monkeypatch):
     p.write_text("1\n" + DOPPLER_SET.replace("1 0.0 first", "3 60.0 first"))
     with pytest.raises(eng.EngineError, match="error -4"):
         eng.ObsFile(p)
+    # a weighted frame whose mask file is missing: refused when its sizes
+    # are asked for
     p.write_text(OBS.replace("1.0 0\nf1", "1.0 1\nf1"))
-    with pytest.raises(eng.EngineError, match="error -4"):
-        eng.ObsFile(p)
+    with pytest.raises(eng.EngineError, match="mask"):
+        eng.ObsFile(p).set_info(0)
     p.write_text(OBS.replace("long_orig", "long9"))
     with pytest.raises(eng.EngineError, match="error -1"):
         eng.ObsFile(p)
@@ -360,3 +362,79 @@ def test_obs_smeared_views_match_reference(tmp_path, monkeypatch, mode, nviews, 
             assert np.array_equal(obs[f * D:(f + 1) * D], ro) and np.array_equal(oov[f * D:(f + 1) * D], rvv)
         # the epoch view closes the list, and the views differ
         assert list(views[f][-1].ae) != list(views[f][0].ae)
+
+
+def _mask(nd, np_, rng, rows, cols):
+    w = np.zeros((nd, np_))
+    w[rows[0]:rows[1], cols[0]:cols[1]] = rng.uniform(0.2, 1.5, (rows[1] - rows[0], cols[1] - cols[0]))
+    w[min(rows[0] + 1, nd - 1), cols[0] + 2] = 0.0     # a hole inside the window
+    return w
+
+
+def test_obs_masks_match_reference(tmp_path, monkeypatch):
+    """Pixel-weighting masks (mask_SS_FF.txt in the data directory) on two
+    of three delay-Doppler frames and on one Doppler frame: each frame's
+    window of positive weights, its COM and DC bins counted from the window,
+    dof (weight per positive weight) and 1/variance times the weights, bit
+    for bit against read_dat; then the same masks from a mask directory."""
+    monkeypatch.chdir(tmp_path)
+    m = cases.c1()[0]
+    write_mod(tmp_path / "m.mod", m, seed=3)
+    (tmp_path / "d").mkdir()
+    rng = np.random.default_rng(31)
+    for f in range(3):
+        img = rng.normal(0, 1, (20, 30))
+        (tmp_path / "d" / ("f%d.dat" % f)).write_text("\n".join(repr(float(x)) for x in img.ravel()) + "\n")
+    for f in range(2):
+        spec = rng.normal(0, 1, 64)
+        (tmp_path / "d" / ("s%d.dat" % f)).write_text("\n".join(repr(float(x)) for x in spec) + "\n")
+    masks = {(0, 0): _mask(20, 30, rng, (3, 15), (4, 27)), (0, 2): _mask(20, 30, rng, (0, 20), (10, 30)),
+             (1, 1): _mask(1, 64, np.random.default_rng(2), (0, 1), (5, 50))}
+    mdir = tmp_path / "masks"
+    mdir.mkdir()
+    for (s_, f), w in masks.items():
+        txt = "{ weights }\n" + "\n".join("%.6f" % x for x in w.ravel()) + "\n"
+        (tmp_path / "d" / ("mask_%02d_%02d.txt" % (s_, f))).write_text(txt)
+        (mdir / ("mask_%02d_%02d.txt" % (s_, f))).write_text(txt)
+    def swap(t, a, b):
+        assert t.count(a) == 1, a
+        return t.replace(a, b)
+    obs = swap(OBS, "f0.dat 2018 3 14 5 6 7  1.5  f 1.0  4 10.0 1.0 0", "f0.dat 2018 3 14 5 6 7  1.5  f 1.0  4 10.0 1.0 1")
+    obs = swap(obs, "9 11.0 1.2 0", "9 11.0 1.2 1")
+    dop = swap(DOPPLER_SET, "s1.dat 2018 3 15 2 0 0  0.7  c 1.5  0  0.5 0", "s1.dat 2018 3 15 2 0 0  0.7  c 1.5  0  0.5 1")
+    text = obs.replace("{ one delay-Doppler set }\n1\n", "{ two sets }\n2\n") + dop
+    (tmp_path / "t.obs").write_text(text)
+    spin = eng.ModFile("m.mod").spin()
+    ref = Reference()
+    h = ref.lib.ref_obs_read(b"m.mod", b"t.obs", 1, 1.0, 0, 1)
+    for maskdir in (None, mdir):
+        o = eng.ObsFile("t.obs")
+        if maskdir is not None:
+            o.set_maskdir(maskdir)
+        frames, ob, ov, sdev = o.frames(0, spin, 75, 0.02)
+        off = 0
+        for f in range(3):
+            g, nd = np.zeros(34), (eng.C.c_int * 2)()
+            D = 20 * 30
+            ro, rv = np.zeros(D), np.zeros(D)
+            ref.lib.ref_obs_frame(h, 0, f, cd.as_dptr(g), nd, cd.as_dptr(ro), cd.as_dptr(rv))
+            fr = frames[f]
+            n = nd[0] * nd[1]
+            assert (fr.ndel, fr.ndop) == (nd[0], nd[1]), f
+            assert (fr.delcom_vig, fr.dopcom_vig, fr.dopDC_vig) == (g[27], g[28], g[29]), f
+            assert (fr.weight, fr.dof) == (g[30], g[31]), f
+            assert np.array_equal(ob[off:off + n], ro[:n]) and np.array_equal(ov[off:off + n], rv[:n]), f
+            off += n
+        assert (frames[0].ndel, frames[0].ndop) == (12, 23) and frames[1].ndel == 20
+        st, dfr, dob, dov = o.doppler(1, spin, 75, 0.02)
+        off = 0
+        for f in range(2):
+            g, nd = np.zeros(31), (eng.C.c_int * 1)()
+            ro, rv = np.zeros(64), np.zeros(64)
+            ref.lib.ref_obs_doppler_frame(h, 1, f, cd.as_dptr(g), nd, cd.as_dptr(ro), cd.as_dptr(rv))
+            n = nd[0]
+            assert dfr[f].ndop == n
+            assert (dfr[f].dopcom_vig, dfr[f].dof) == (g[26], g[28]), f
+            assert np.array_equal(dob[off:off + n], ro[:n]) and np.array_equal(dov[off:off + n], rv[:n]), f
+            off += n
+        assert dfr[1].ndop == 45
