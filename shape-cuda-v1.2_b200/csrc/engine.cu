@@ -307,7 +307,6 @@ int EngineImpl::finalize()
         AL(d_ovf_out, dop_frames.size() * DOP_OVF_TERMS);
         AL(d_dop_frames, dop_frames.size());
     }
-    AL(d_summary, 1);
     size_t lc_tot_pts = points.size(), lc_tot_n = 0;
     for (auto &L : lc) lc_tot_n += L.set.n;
     AL(d_lc_x, lc_tot_pts); AL(d_lc_y, lc_tot_pts); AL(d_lc_y2, lc_tot_pts);
@@ -319,7 +318,10 @@ int EngineImpl::finalize()
         cudaFreeHost(h_params);
         CK(cudaMallocHost((void **)&h_params, sizeof(double) * ((size_t)nv + 3)));
     }
-    if (!h_summary) CK(cudaMallocHost((void **)&h_summary, sizeof(shape_eval_summary)));
+    if (!h_summary) {
+        CK(cudaHostAlloc((void **)&h_summary, sizeof(shape_eval_summary), cudaHostAllocMapped));
+        CK(cudaHostGetDevicePointer((void **)&d_summary_map, h_summary, 0));
+    }
 
     // ---- uploads (once)
     cudaStream_t s = stream;
@@ -1145,7 +1147,9 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     // applied by evaluate(), so captured graphs stay valid when it changes
     sa.baddiam = 0;
     sa.baddiam_logfactor = 0.0;
-    sa.out = d_summary;
+    // the summary kernel writes the pinned host summary directly (mapped
+    // memory), so an evaluation needs no device-to-host copy after it
+    sa.out = d_summary_map;
     if (fused) launch_chi2_summary(ca, fa, sa, d_chi2_counters, f32 ? 1 : 0, s, fork, fused_smem);
     else launch_summary(fa, sa, s);
     mark(7);
@@ -1204,7 +1208,6 @@ int EngineImpl::launch(int form)
         CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s));
         int rc = enqueue(form);
         if (rc) return rc;
-        CK(cudaMemcpyAsync(h_summary, d_summary, sizeof(shape_eval_summary), cudaMemcpyDeviceToHost, s));
         if (!pen_type.empty() && (rc = enqueue_model_sums()) != SHAPE_OK) return rc;
         CK(cudaEventRecord(ev1, s));
     } else {
@@ -1229,7 +1232,6 @@ int EngineImpl::launch(int form)
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s);
             int rc = enqueue(form);
-            cudaMemcpyAsync(h_summary, d_summary, sizeof(shape_eval_summary), cudaMemcpyDeviceToHost, s);
             cudaError_t ce = cudaStreamEndCapture(s, &graph);
             if (rc) { if (ce == cudaSuccess) cudaGraphDestroy(graph); return rc; }
             CK(ce);

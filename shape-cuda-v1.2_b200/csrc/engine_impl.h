@@ -157,7 +157,7 @@ struct EngineImpl {
     double *d_lc_y = nullptr, *d_lc_y2 = nullptr, *d_lc_fit = nullptr, *d_lc_out = nullptr;
     double *d_lc_dof = nullptr, *d_lc_npts = nullptr;
     SetRec *d_setrecs = nullptr;
-    shape_eval_summary *d_summary = nullptr;
+    shape_eval_summary *d_summary_map = nullptr;   // device address of the mapped pinned h_summary
     std::vector<LcSetDev> lcdev;
     std::vector<int> dop_frames;        // global indices of the Doppler frames
     double *d_ovf = nullptr, *d_ovf_out = nullptr;
