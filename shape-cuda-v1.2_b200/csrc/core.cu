@@ -355,21 +355,13 @@ __device__ void frame_sums_warp(const double *part, int nitems, const double sta
 {
     const int lane = threadIdx.x & 31;
     KSum q[3] = {{0, 0}, {0, 0}, {0, 0}};
-    // four of the lane's items loaded before they are summed, in item order
-    for (int it0 = lane; it0 < nitems; it0 += 4 * 32) {
-        double p[4][6];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int it = it0 + 32 * u;
-#pragma unroll
-            for (int j = 0; j < 6; j++)
-                p[u][j] = it < nitems ? (via_l2 ? __ldcg(part + (size_t)it * 6 + j) : part[(size_t)it * 6 + j]) : 0.0;
+    for (int it = lane; it < nitems; it += 32)
+        for (int k = 0; k < 3; k++) {
+            double p[2];
+            p[0] = via_l2 ? __ldcg(part + (size_t)it * 6 + 2 * k) : part[(size_t)it * 6 + 2 * k];
+            p[1] = via_l2 ? __ldcg(part + (size_t)it * 6 + 2 * k + 1) : part[(size_t)it * 6 + 2 * k + 1];
+            ksum_take(q[k], p);
         }
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-            if (it0 + 32 * u < nitems)
-                for (int k = 0; k < 3; k++) ksum_take(q[k], &p[u][2 * k]);
-    }
     for (int off = 16; off > 0; off >>= 1)
         for (int k = 0; k < 3; k++) q[k].merge(shfl_ksum(q[k], off));
     for (int k = 0; k < 3; k++) {
