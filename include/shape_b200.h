@@ -176,7 +176,28 @@ int shape_engine_set_bin_capacity(shape_engine *e, int cap);
  * chi-square may move by ~1e-4 when that happens). Lightcurve views are
  * always exact. Takes effect at the next evaluation. */
 int shape_engine_set_fp32_exact(shape_engine *e, int exact);
-/* Raster kernel of the batched forms. mode -1 (default): the first batched
+/* vary_params (src/shape/vary_params.c:84-327): the four means the
+ * reference computes for its joint adjustments of the 0th delay-correction
+ * coefficient, the radar and optical albedos and the Doppler scale, from an
+ * FP64 evaluation of the current model (the call evaluates with the POS maps
+ * kept, so the last results are that evaluation's). As the reference does,
+ * only the first dataset contributes (its loop over datasets ends after set
+ * 0, vary_params.c:106), and the weight sums are read_dat's over every
+ * dataset. vary_* are par->vary_delcor0 / vary_radalb / vary_optalb /
+ * vary_dopscale (0 = VARY_NONE); delcor0_free and dopscale_free (per
+ * dataset in add order, or NULL = none) tell whether a set's 0th
+ * delay-correction coefficient and Doppler scale float (state != 'c'); a
+ * frame or lightcurve counts as fixed-calibration when cal_floating is 0.
+ * out = deldop_zmax, rad_xsec, opt_brightness, cos_subradarlat. A smeared
+ * first dataset returns SHAPE_E_UNSUPPORTED. */
+typedef struct shape_vary_options {
+    int vary_delcor0, vary_radalb, vary_optalb, vary_dopscale;
+    const int *delcor0_free;
+    const int *dopscale_free;
+} shape_vary_options;
+int shape_engine_vary_params(shape_engine *e, const shape_vary_options *opt, double out[4]);
+
+/* Raster kernel of the batched forms./* Raster kernel of the batched forms. mode -1 (default): the first batched
  * evaluation of each form times four candidates on this engine's datasets
  * (the tile-per-CTA kernel and the warp-independent kernel, each with one
  * CTA per non-empty tile or a persistent grid of resident CTAs on every

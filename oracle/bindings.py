@@ -230,6 +230,8 @@ class Reference:
         L.ref_realize_spin_frames.argtypes = [P(cd.SpinState), cd.dptr, cd.dptr, C.c_int, cd.dptr, cd.dptr,
                                               cd.dptr, cd.dptr, C.c_double]
         L.ref_set_r.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        L.ref_vary_params.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), P(C.c_int), cd.dptr]
+        L.ref_vary_params.restype = None
         L.ref_realize.argtypes = [C.c_void_p]
         L.ref_evaluate.restype = C.c_double
         L.ref_evaluate.argtypes = [C.c_void_p]
@@ -413,6 +415,15 @@ class RefSession:
         buf = C.create_string_buffer(self.model.nf)
         self.L.ref_get_seen(self.h, buf)
         return np.frombuffer(buf.raw, dtype=np.uint8).copy()
+
+    def vary_params(self, flags, delcor0_free, dopscale_free):
+        """The reference's vary_params after evaluate(): the four means."""
+        fl = (C.c_int * 4)(*[int(x) for x in flags])
+        a = (C.c_int * len(delcor0_free))(*[int(x) for x in delcor0_free])
+        b = (C.c_int * len(dopscale_free))(*[int(x) for x in dopscale_free])
+        out = np.zeros(4)
+        self.L.ref_vary_params(self.h, fl, a, b, cd.as_dptr(out))
+        return out
 
     def deldop_frame(self, s, f, fr):
         side = 2 * fr.pos_n + 1

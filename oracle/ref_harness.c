@@ -369,6 +369,64 @@ double ref_evaluate(void *h)
     return chi2(&S->par, &S->dat, 0);
 }
 
+/* The reference's vary_params (src/shape/vary_params.c:84-327) on the
+ * session after ref_evaluate: flags = par->vary_delcor0, vary_radalb,
+ * vary_optalb, vary_dopscale (0 = VARY_NONE); delcor0_free / dopscale_free
+ * per dataset give the states of the 0th delay-correction coefficient and of
+ * the Doppler scale factor ('f' when set, else 'c'). The datasets' and
+ * dat's weight sums are formed as read_dat forms them
+ * (src/shape/read_dat.c:421-501, 686-692, 1051-1056, 1900-1906). out = the
+ * four means deldop_zmax, rad_xsec, opt_brightness, cos_subradarlat. */
+void ref_vary_params(void *h, const int *flags, const int *delcor0_free, const int *dopscale_free, double *out)
+{
+    ref_session *S = h;
+    struct dat_t *dat = &S->dat;
+    S->par.vary_delcor0 = (unsigned char)flags[0];
+    S->par.vary_radalb = (unsigned char)flags[1];
+    S->par.vary_optalb = (unsigned char)flags[2];
+    S->par.vary_dopscale = (unsigned char)flags[3];
+    dat->sum_deldop_zmax_weights = dat->sum_rad_xsec_weights = 0.0;
+    dat->sum_opt_brightness_weights = dat->sum_cos_subradarlat_weights = 0.0;
+    for (int s = 0; s < dat->nsets; s++) {
+        struct set_t *set = &dat->set[s];
+        if (set->type == DELAY) {
+            struct deldop_t *dd = &set->desc.deldop;
+            if (!dd->delcor.a) {
+                dd->delcor.n = 0;
+                dd->delcor.a = calloc(1, sizeof(struct param_t));
+            }
+            dd->delcor.a[0].state = delcor0_free[s] ? 'f' : 'c';
+            dd->dopscale.state = dopscale_free[s] ? 'f' : 'c';
+            dd->sum_deldop_zmax_weights = dd->sum_rad_xsec_weights = dd->sum_cos_subradarlat_weights = 0.0;
+            for (int f = 0; f < dd->nframes; f++) {
+                const double w = dd->frame[f].weight;
+                if (dd->delcor.a[0].state != 'c') dd->sum_deldop_zmax_weights += w;
+                if (dd->frame[f].cal.state == 'c') dd->sum_rad_xsec_weights += w;
+                if (dd->dopscale.state != 'c') dd->sum_cos_subradarlat_weights += w;
+            }
+            dat->sum_deldop_zmax_weights += dd->sum_deldop_zmax_weights;
+            dat->sum_rad_xsec_weights += dd->sum_rad_xsec_weights;
+            dat->sum_cos_subradarlat_weights += dd->sum_cos_subradarlat_weights;
+        } else if (set->type == DOPPLER) {
+            struct doppler_t *dp = &set->desc.doppler;
+            dp->dopscale.state = dopscale_free[s] ? 'f' : 'c';
+            dp->sum_rad_xsec_weights = dp->sum_cos_subradarlat_weights = 0.0;
+            for (int f = 0; f < dp->nframes; f++) {
+                const double w = dp->frame[f].weight;
+                if (dp->frame[f].cal.state == 'c') dp->sum_rad_xsec_weights += w;
+                if (dp->dopscale.state != 'c') dp->sum_cos_subradarlat_weights += w;
+            }
+            dat->sum_rad_xsec_weights += dp->sum_rad_xsec_weights;
+            dat->sum_cos_subradarlat_weights += dp->sum_cos_subradarlat_weights;
+        } else if (set->type == LGHTCRV) {
+            struct lghtcrv_t *lc = &set->desc.lghtcrv;
+            lc->sum_opt_brightness_weights = (lc->cal.state == 'c') ? lc->weight * lc->n : 0.0;
+            dat->sum_opt_brightness_weights += lc->sum_opt_brightness_weights;
+        }
+    }
+    vary_params(&S->par, &S->mod, dat, S->par.action, &out[0], &out[1], &out[2], &out[3]);
+}
+
 /* calc_fits + chi2 without re-realizing (model already realized). */
 double ref_calc_chi2(void *h)
 {

@@ -1985,6 +1985,112 @@ int shape_engine_get_frame_view(shape_engine *h, int global_frame, double ae[9],
     return SHAPE_OK;
 }
 
+// vary_params (src/shape/vary_params.c:84-327) from an FP64 evaluation of
+// the current model: for the first dataset only, as the reference's loop
+// over datasets stops after set 0 (vary_params.c:106), the dof-free sums of
+// the subradar point's distance (delay-Doppler frames whose 0th
+// delay-correction coefficient floats), the radar cross sections of frames
+// with a fixed calibration, the lightcurve's fitted brightnesses when its
+// calibration is fixed, and cos(subradar latitude) of frames whose Doppler
+// scale floats, each weighted by the frame's (set's) weight; divided by the
+// weight sums read_dat forms over every dataset
+// (src/shape/read_dat.c:421-501, 686-692, 1051-1056, 1900-1906).
+int shape_engine_vary_params(shape_engine *h, const shape_vary_options *opt, double out[4])
+{
+    if (!h || !opt || !out) return shape::set_err(SHAPE_E_ARG, "vary_params: null argument");
+    EngineImpl &E = h->impl;
+    if (!E.finalized) return shape::set_err(SHAPE_E_STATE, "vary_params before finalize");
+    const int nsets = (int)E.setrecs.size();
+    auto dfree = [&](const int *a, int s) { return a ? a[s] != 0 : false; };
+    // the weight sums over every dataset
+    double w_zmax = 0.0, w_xsec = 0.0, w_opt = 0.0, w_cos = 0.0;
+    for (int s = 0; s < nsets; s++) {
+        const shape::SetRec &R = E.setrecs[s];
+        if (R.type == 0) {
+            int ds = 0;
+            while (ds < (int)E.dd.size() && E.dd[ds].frame0 != R.first) ds++;
+            const bool dop = E.dd[ds].doppler != 0;
+            for (int f = R.first; f < R.first + R.count; f++) {
+                const shape_deldop_frame &F = E.frames[f];
+                if (!dop && dfree(opt->delcor0_free, s)) w_zmax += F.weight;
+                if (!F.cal_floating) w_xsec += F.weight;
+                if (dfree(opt->dopscale_free, s)) w_cos += F.weight;
+            }
+        } else {
+            const shape::LcSetHost &L = E.lc[R.first];
+            if (!L.set.cal_floating) w_opt += L.set.weight * L.set.n;
+        }
+    }
+    double sum_zmax = 0.0, sum_xsec = 0.0, sum_opt = 0.0, sum_cos = 0.0;
+    if (nsets > 0) {
+        const shape::SetRec &R = E.setrecs[0];
+        if (R.type == 0 && !E.fviews[R.first].empty())
+            return shape::set_err(SHAPE_E_UNSUPPORTED, "vary_params: the first dataset has smeared frames");
+        const int keep = E.keep_pos;
+        if (E.finalized) cudaSetDevice(E.device);
+        E.keep_pos = 1;
+        shape_eval_summary sm;
+        int rc = E.evaluate(SHAPE_FORM_PLAIN_FP64, &sm);
+        E.keep_pos = keep;
+        if (rc) return rc;
+        if (R.type == 0) {
+            int ds = 0;
+            while (ds < (int)E.dd.size() && E.dd[ds].frame0 != R.first) ds++;
+            const bool dop = E.dd[ds].doppler != 0;
+            const int nfr = (int)E.frames.size();
+            std::vector<shape_deldop_result> res(nfr);
+            if ((rc = shape_engine_get_deldop_results(h, res.data(), nfr)) < 0) return rc;
+            std::vector<double> ovf(4 * (size_t)nfr);
+            if ((rc = shape_engine_get_radar_overflow(h, ovf.data(), nfr)) < 0) return rc;
+            for (int f = R.first; f < R.first + R.count; f++) {
+                const shape_deldop_frame &F = E.frames[f];
+                const bool zmax_on = opt->vary_delcor0 && !dop && dfree(opt->delcor0_free, 0);
+                const bool xsec_on = opt->vary_radalb && !F.cal_floating;
+                if (zmax_on) {
+                    const int side = 2 * F.pos_n + 1;
+                    std::vector<double> z((size_t)side * side), ce((size_t)side * side);
+                    if ((rc = shape_engine_get_pos(h, f, z.data(), ce.data(), nullptr)) != SHAPE_OK) return rc;
+                    double zmax = -SHAPE_HUGENUMBER;
+                    const shape_deldop_result &r = res[f];
+                    for (int x = r.xlim[0]; x <= r.xlim[1]; x++)
+                        for (int y = r.ylim[0]; y <= r.ylim[1]; y++) {
+                            const size_t p = (size_t)(x + F.pos_n) * side + (size_t)(y + F.pos_n);
+                            if (ce[p] > 0.0) zmax = std::max(zmax, z[p]);
+                        }
+                    sum_zmax += zmax * F.weight;
+                }
+                if (xsec_on) {
+                    std::vector<double> fit((size_t)F.ndel * F.ndop);
+                    if ((rc = shape_engine_get_fit(h, f, fit.data())) != SHAPE_OK) return rc;
+                    double xs = dop ? ovf[4 * (size_t)f + 2] : 0.0;    // overflow_xsec
+                    for (double v : fit) xs += v;
+                    xs *= res[f].cal;
+                    sum_xsec += xs * F.weight;
+                }
+                if (opt->vary_dopscale && dfree(opt->dopscale_free, 0)) {
+                    double oa[9];
+                    shape::mul_bt(oa, F.oe, F.ae);
+                    const double cd = sqrt(oa[6] * oa[6] + oa[7] * oa[7]);
+                    sum_cos += cd * F.weight;
+                }
+            }
+        } else if (opt->vary_optalb) {
+            const shape::LcSetHost &L = E.lc[R.first];
+            if (!L.set.cal_floating) {
+                std::vector<double> y(L.set.ncalc), fit(L.set.n);
+                double cal, chi2;
+                if ((rc = shape_engine_get_lghtcrv(h, 0, y.data(), fit.data(), &cal, &chi2)) != SHAPE_OK) return rc;
+                for (int i = 0; i < L.set.n; i++) sum_opt += fit[i] * L.set.weight;
+            }
+        }
+    }
+    out[0] = w_zmax > 0.0 ? sum_zmax / w_zmax : 0.0;
+    out[1] = w_xsec > 0.0 ? sum_xsec / w_xsec : 0.0;
+    out[2] = w_opt > 0.0 ? sum_opt / w_opt : 0.0;
+    out[3] = w_cos > 0.0 ? sum_cos / w_cos : 0.0;
+    return SHAPE_OK;
+}
+
 int shape_engine_set_raster_tuning(shape_engine *h, int mode)
 {
     if (!h || mode < -1 || mode > 1) return shape::set_err(SHAPE_E_ARG, "set_raster_tuning: -1, 0 or 1");

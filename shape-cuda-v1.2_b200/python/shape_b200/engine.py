@@ -127,6 +127,7 @@ def load_library(path=LIB_PATH):
     L.shape_engine_set_bin_capacity.argtypes = [vp, C.c_int]
     L.shape_engine_set_fp32_exact.argtypes = [vp, C.c_int]
     L.shape_engine_set_raster_tuning.argtypes = [vp, C.c_int]
+    L.shape_engine_vary_params.argtypes = [vp, P(VaryOptions), cd.dptr]
     L.shape_engine_set_spin_device.argtypes = [vp, C.c_int]
     L.shape_engine_get_frame_view.argtypes = [vp, C.c_int, cd.dptr, cd.dptr]
     L.shape_engine_get_raster_tuning.argtypes = [vp, C.c_int, P(C.c_int), P(C.c_int), cd.dptr]
@@ -315,6 +316,22 @@ class Engine:
         ae, sp = np.zeros(9), np.zeros(3)
         _chk(self.L.shape_engine_get_frame_view(self.h, int(frame), cd.as_dptr(ae), cd.as_dptr(sp)))
         return ae.reshape(3, 3), sp
+
+    def vary_params(self, flags, delcor0_free=None, dopscale_free=None):
+        """shape_engine_vary_params: flags = (vary_delcor0, vary_radalb,
+        vary_optalb, vary_dopscale); per dataset free flags. Returns the four
+        means (deldop_zmax, rad_xsec, opt_brightness, cos_subradarlat)."""
+        o = VaryOptions()
+        o.vary_delcor0, o.vary_radalb, o.vary_optalb, o.vary_dopscale = (int(x) for x in flags)
+        keep = []
+        for name, v in (("delcor0_free", delcor0_free), ("dopscale_free", dopscale_free)):
+            if v is not None:
+                a = (C.c_int * len(v))(*[int(x) for x in v])
+                keep.append(a)
+                setattr(o, name, C.cast(a, C.POINTER(C.c_int)))
+        out = np.zeros(4)
+        _chk(self.L.shape_engine_vary_params(self.h, C.byref(o), cd.as_dptr(out)))
+        return out
 
     def set_raster_tuning(self, mode=-1):
         """-1: time the raster candidates at each batched form's first
@@ -574,6 +591,12 @@ def write_fitdat(path, fit, cal, sdev):
     f = np.ascontiguousarray(fit, dtype=np.float64)
     ndel, ndop = f.shape if f.ndim == 2 else (1, f.size)
     _chk(load_library().shape_write_fitdat(os.fsencode(path), ndel, ndop, cd.as_dptr(f), float(cal), float(sdev)))
+
+
+class VaryOptions(C.Structure):
+    _fields_ = [("vary_delcor0", C.c_int), ("vary_radalb", C.c_int), ("vary_optalb", C.c_int),
+                ("vary_dopscale", C.c_int), ("delcor0_free", C.POINTER(C.c_int)),
+                ("dopscale_free", C.POINTER(C.c_int))]
 
 
 class ObsOptions(C.Structure):
