@@ -115,8 +115,9 @@ int shape_engine_add_doppler_set(shape_engine *e, const shape_doppler_set *set,
 /* Allocates device state for everything added so far. */
 int shape_engine_finalize(shape_engine *e);
 
-/* Free parameters (src/shape/mkparlist.c:218-235): component scale factor j
- * (SIZEPAR) and vertex deviation r of vertex i (SHAPEPAR). */
+/* Free parameters (src/shape/mkparlist.c:218-235): scale factor j (SIZEPAR;
+ * j = 3 * component + axis for a model of several components) and vertex
+ * deviation r of vertex i (SHAPEPAR; model-wide vertex index). */
 int shape_engine_set_scale(shape_engine *e, int j, double value);
 int shape_engine_set_vertex_r(shape_engine *e, int i, double value);
 int shape_engine_get_vertex_r(shape_engine *e, int i, double *value);

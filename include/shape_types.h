@@ -67,6 +67,21 @@ typedef struct shape_model_desc {
     const int *fv;          /* [nf][3] facet corner vertex indices (facet_t.v) */
     const int *af_ptr;      /* [nv+1] CSR offsets into af_idx */
     const int *af_idx;      /* attached-facet lists (vertex_t.af), in model-file order */
+    /* Several VERTEX components (shape_t.comp, src/shape/shape2.h:812-826):
+     * ncomp > 1 lists them back to back in a/u/r (comp_nv vertices each)
+     * and fv (comp_nf facets each), fv and af_idx holding model-wide
+     * indices. Each component has its scale factors (comp_scale, replacing
+     * scale[] above), rotation offsets (comp_rot: Euler angles, rad) and
+     * translation offsets (comp_off, km): realize_mod scales, rotates and
+     * translates its vertices (src/shape/realize_mod.c:444-512), and posvis
+     * renders the components in order (src/shape/calc_fits.c:507-513).
+     * ncomp 0 or 1: one component, scale[] above (the other fields unused). */
+    int ncomp;
+    const int *comp_nv;     /* [ncomp] */
+    const int *comp_nf;     /* [ncomp] */
+    const double *comp_scale;   /* [ncomp][3] */
+    const double *comp_rot;     /* [ncomp][3] */
+    const double *comp_off;     /* [ncomp][3] */
 } shape_model_desc;
 
 /* Radar scattering law parameters (union radscat_t, src/shape/shape2.h:852-900). */

@@ -68,41 +68,52 @@ void *ref_new(const shape_model_desc *m, const shape_eval_params *ep, int max_se
     par->warn_badradar = 0;
     par->pos_scope = LOCAL;
 
-    mod->shape.ncomp = 1;
-    mod->shape.comp = calloc(1, sizeof(struct comp_t));
-    struct comp_t *c = &mod->shape.comp[0];
-    c->type = VERTEX;
-    struct vertices_t *real = &c->real;
-    real->nv = c->desc.ver.nv = m->nv;
-    real->nf = c->desc.ver.nf = m->nf;
-    real->v = calloc((size_t)m->nv, sizeof(struct vertex_t));
-    real->f = calloc((size_t)m->nf, sizeof(struct facet_t));
-    for (int j = 0; j < 3; j++) {
-        c->desc.ver.scalefactor[j].state = 'f';
-        c->desc.ver.scalefactor[j].val = m->scale[j];
-        real->scalefactor[j] = c->desc.ver.scalefactor[j];
-        c->off[j].state = c->rot[j].state = 'c';
-        c->off[j].val = c->rot[j].val = 0.0;
+    /* one VERTEX component, or m->ncomp of them back to back (model-wide
+     * facet and attached-facet indices turned into the component's own) */
+    const int nc = m->ncomp > 1 ? m->ncomp : 1;
+    mod->shape.ncomp = nc;
+    mod->shape.comp = calloc((size_t)nc, sizeof(struct comp_t));
+    int v0 = 0, f0 = 0;
+    for (int k = 0; k < nc; k++) {
+        const int nvk = nc > 1 ? m->comp_nv[k] : m->nv, nfk = nc > 1 ? m->comp_nf[k] : m->nf;
+        struct comp_t *c = &mod->shape.comp[k];
+        c->type = VERTEX;
+        struct vertices_t *real = &c->real;
+        real->nv = c->desc.ver.nv = nvk;
+        real->nf = c->desc.ver.nf = nfk;
+        real->v = calloc((size_t)nvk, sizeof(struct vertex_t));
+        real->f = calloc((size_t)nfk, sizeof(struct facet_t));
+        for (int j = 0; j < 3; j++) {
+            c->desc.ver.scalefactor[j].state = 'f';
+            c->desc.ver.scalefactor[j].val = nc > 1 ? m->comp_scale[3 * k + j] : m->scale[j];
+            real->scalefactor[j] = c->desc.ver.scalefactor[j];
+            c->off[j].state = c->rot[j].state = 'c';
+            c->off[j].val = nc > 1 ? m->comp_off[3 * k + j] : 0.0;
+            c->rot[j].val = nc > 1 ? m->comp_rot[3 * k + j] : 0.0;
+        }
+        for (int i = 0; i < nvk; i++) {
+            const int g = v0 + i;
+            struct vertex_t *v = &real->v[i];
+            for (int j = 0; j < 3; j++) { v->a[j] = m->a[3 * g + j]; v->u[j] = m->u[3 * g + j]; }
+            v->r.state = 'f';
+            v->r.val = m->r[g];
+            v->naf = m->af_ptr[g + 1] - m->af_ptr[g];
+            v->af = malloc(sizeof(int) * (size_t)(v->naf > 0 ? v->naf : 1));
+            for (int q = 0; q < v->naf; q++) v->af[q] = m->af_idx[m->af_ptr[g] + q] - f0;
+            v->act = 1;
+            v->v_mirror = i;
+        }
+        for (int f = 0; f < nfk; f++) {
+            for (int j = 0; j < 3; j++) real->f[f].v[j] = m->fv[3 * (f0 + f) + j] - v0;
+            real->f[f].act = 1;
+        }
+        /* the vertex description shares the realization's arrays (VERTEX
+         * type is its own realization, src/shape/realize_mod.c:455-458) */
+        c->desc.ver.v = real->v;
+        c->desc.ver.f = real->f;
+        v0 += nvk;
+        f0 += nfk;
     }
-    for (int i = 0; i < m->nv; i++) {
-        struct vertex_t *v = &real->v[i];
-        for (int j = 0; j < 3; j++) { v->a[j] = m->a[3 * i + j]; v->u[j] = m->u[3 * i + j]; }
-        v->r.state = 'f';
-        v->r.val = m->r[i];
-        v->naf = m->af_ptr[i + 1] - m->af_ptr[i];
-        v->af = malloc(sizeof(int) * (size_t)(v->naf > 0 ? v->naf : 1));
-        for (int k = 0; k < v->naf; k++) v->af[k] = m->af_idx[m->af_ptr[i] + k];
-        v->act = 1;
-        v->v_mirror = i;
-    }
-    for (int f = 0; f < m->nf; f++) {
-        for (int j = 0; j < 3; j++) real->f[f].v[j] = m->fv[3 * f + j];
-        real->f[f].act = 1;
-    }
-    /* the vertex description shares the realization's arrays (VERTEX type is
-     * its own realization, src/shape/realize_mod.c:455-458) */
-    c->desc.ver.v = real->v;
-    c->desc.ver.f = real->f;
 
     S->dat.set = calloc((size_t)max_sets, sizeof(struct set_t));
     S->nsets_cap = max_sets;
@@ -342,14 +353,16 @@ int ref_add_lghtcrv_set(void *h, const shape_lghtcrv_set *ls, const shape_lghtcr
 void ref_set_scale(void *h, int j, double val)
 {
     ref_session *S = h;
-    S->mod.shape.comp[0].desc.ver.scalefactor[j].val = val;
+    S->mod.shape.comp[j / 3].desc.ver.scalefactor[j % 3].val = val;
 }
 
 /* Vertex deviation r of vertex i (a SHAPEPAR free parameter, src/shape/mkparlist.c:227-233). */
 void ref_set_r(void *h, int i, double val)
 {
     ref_session *S = h;
-    S->mod.shape.comp[0].real.v[i].r.val = val;
+    int c = 0;
+    while (i >= S->mod.shape.comp[c].real.nv) i -= S->mod.shape.comp[c++].real.nv;
+    S->mod.shape.comp[c].real.v[i].r.val = val;
 }
 
 void ref_realize(void *h)
@@ -438,12 +451,20 @@ double ref_calc_chi2(void *h)
 void ref_get_realized(void *h, double *x, double *vn, double *fn, double *area)
 {
     ref_session *S = h;
-    struct vertices_t *real = &S->mod.shape.comp[0].real;
-    for (int i = 0; i < real->nv; i++)
-        for (int j = 0; j < 3; j++) { x[3 * i + j] = real->v[i].x[j]; vn[3 * i + j] = real->v[i].n[j]; }
-    for (int f = 0; f < real->nf; f++) {
-        for (int j = 0; j < 3; j++) fn[3 * f + j] = real->f[f].n[j];
-        area[f] = real->f[f].area;
+    int v0 = 0, f0 = 0;
+    for (int c = 0; c < S->mod.shape.ncomp; c++) {
+        struct vertices_t *real = &S->mod.shape.comp[c].real;
+        for (int i = 0; i < real->nv; i++)
+            for (int j = 0; j < 3; j++) {
+                x[3 * (v0 + i) + j] = real->v[i].x[j];
+                vn[3 * (v0 + i) + j] = real->v[i].n[j];
+            }
+        for (int f = 0; f < real->nf; f++) {
+            for (int j = 0; j < 3; j++) fn[3 * (f0 + f) + j] = real->f[f].n[j];
+            area[f0 + f] = real->f[f].area;
+        }
+        v0 += real->nv;
+        f0 += real->nf;
     }
 }
 
@@ -458,12 +479,24 @@ void ref_get_flags(void *h, double out[4])
 void ref_get_seen(void *h, unsigned char *seen)
 {
     ref_session *S = h;
-    struct vertices_t *real = &S->mod.shape.comp[0].real;
-    for (int f = 0; f < real->nf; f++) seen[f] = real->f[f].seen;
+    int f0 = 0;
+    for (int c = 0; c < S->mod.shape.ncomp; c++) {
+        struct vertices_t *real = &S->mod.shape.comp[c].real;
+        for (int f = 0; f < real->nf; f++) seen[f0 + f] = real->f[f].seen;
+        f0 += real->nf;
+    }
 }
 
-static void ref_copy_pos_out(const struct pos_t *pos, double *z, double *cose, double *cosi,
-                             int *f, double *zill, int *fill, int lims[8])
+/* The model-wide index of component c's facet f (components back to back). */
+static int ref_global_facet(const struct mod_t *mod, int c, int f)
+{
+    if (!mod || f < 0) return f;
+    for (int k = 0; k < c; k++) f += mod->shape.comp[k].real.nf;
+    return f;
+}
+
+static void ref_copy_pos_out(const struct mod_t *mod, const struct pos_t *pos, double *z, double *cose,
+                             double *cosi, int *f, double *zill, int *fill, int lims[8])
 {
     int n = pos->n, side = 2 * n + 1;
     for (int i = -n; i <= n; i++)
@@ -472,9 +505,9 @@ static void ref_copy_pos_out(const struct pos_t *pos, double *z, double *cose, d
             if (z) z[p] = pos->z[i][j];
             if (cose) cose[p] = pos->cose[i][j];
             if (cosi) cosi[p] = pos->cosi[i][j];
-            if (f) f[p] = pos->f[i][j];
+            if (f) f[p] = ref_global_facet(mod, pos->comp[i][j], pos->f[i][j]);
             if (zill) zill[p] = pos->zill[i][j];
-            if (fill) fill[p] = pos->fill[i][j];
+            if (fill) fill[p] = ref_global_facet(mod, pos->bistatic ? pos->compill[i][j] : 0, pos->fill[i][j]);
         }
     if (lims) {
         lims[0] = pos->xlim[0]; lims[1] = pos->xlim[1];
@@ -497,7 +530,7 @@ void ref_get_deldop_frame(void *h, int s, int f, double *fit, double *z, double 
             for (int j = 1; j <= fr->ndop; j++)
                 fit[(size_t)(i - 1) * fr->ndop + (size_t)(j - 1)] = fr->fit[i][j];
     int lims[8];
-    ref_copy_pos_out(&fr->pos, z, cose, NULL, fac, NULL, NULL, lims);
+    ref_copy_pos_out(&S->mod, &fr->pos, z, cose, NULL, fac, NULL, NULL, lims);
     if (res) {
         memset(res, 0, sizeof *res);
         res->xlim[0] = lims[0]; res->xlim[1] = lims[1];
@@ -522,7 +555,7 @@ void ref_get_doppler_frame(void *h, int s, int f, double *fit, double *z, double
     if (fit)
         for (int j = 1; j <= fr->ndop; j++) fit[j - 1] = fr->fit[j];
     int lims[8];
-    ref_copy_pos_out(&fr->pos, z, cose, NULL, fac, NULL, NULL, lims);
+    ref_copy_pos_out(&S->mod, &fr->pos, z, cose, NULL, fac, NULL, NULL, lims);
     if (res) {
         memset(res, 0, sizeof *res);
         res->xlim[0] = lims[0]; res->xlim[1] = lims[1];
@@ -568,7 +601,7 @@ void ref_get_lghtcrv_pos(void *h, int s, int i, double *z, double *cose, double 
                          int *fac, double *zill, int *fill, int lims[8])
 {
     ref_session *S = h;
-    ref_copy_pos_out(&S->dat.set[s].desc.lghtcrv.rend[i].pos, z, cose, cosi, fac, zill, fill, lims);
+    ref_copy_pos_out(&S->mod, &S->dat.set[s].desc.lghtcrv.rend[i].pos, z, cose, cosi, fac, zill, fill, lims);
 }
 
 double ref_set_chi2(void *h, int s)
@@ -612,9 +645,11 @@ void ref_free(void *h)
         }
     }
     free(S->dat.set);
-    struct vertices_t *real = &S->mod.shape.comp[0].real;
-    for (int i = 0; i < real->nv; i++) free(real->v[i].af);
-    free(real->v); free(real->f);
+    for (int c = 0; c < S->mod.shape.ncomp; c++) {
+        struct vertices_t *real = &S->mod.shape.comp[c].real;
+        for (int i = 0; i < real->nv; i++) free(real->v[i].af);
+        free(real->v); free(real->f);
+    }
     free(S->mod.shape.comp);
     free(S);
 }

@@ -29,13 +29,37 @@ __device__ inline int clamp_hi(double v) { return (v > (double)INT_MAX) ? INT_MA
 // ---------------------------------------------------------------- realize
 
 // x = scale * (u*r + a)  (src/shape/realize_mod.c:471-479)
+// Several components (vcomp and cxf non-null): vertex i takes its
+// component's scale factors, then the component's rotation (comp.m, when
+// its rotation offsets are not all zero) and translation (when its offsets
+// are not all zero), as realize_mod does (src/shape/realize_mod.c:474-512).
+// cxf holds per component m (9, row-major), off (3) and the two flags.
 __device__ inline double4 realize_vertex(int i, const double *__restrict__ a, const double *__restrict__ u,
-                                         const double *__restrict__ r, const double *__restrict__ scale)
+                                         const double *__restrict__ r, const double *__restrict__ scale,
+                                         const int *__restrict__ vcomp, const double *__restrict__ cxf)
 {
+    const int c = vcomp ? vcomp[i] : 0;
+    const double *sc = scale + 3 * c;
     double ri = r[i];
-    double x0 = scale[0] * (u[3 * i + 0] * ri + a[3 * i + 0]);
-    double x1 = scale[1] * (u[3 * i + 1] * ri + a[3 * i + 1]);
-    double x2 = scale[2] * (u[3 * i + 2] * ri + a[3 * i + 2]);
+    double x0 = sc[0] * (u[3 * i + 0] * ri + a[3 * i + 0]);
+    double x1 = sc[1] * (u[3 * i + 1] * ri + a[3 * i + 1]);
+    double x2 = sc[2] * (u[3 * i + 2] * ri + a[3 * i + 2]);
+    if (cxf) {
+        const double *T = cxf + CXF_N * c;
+        if (T[12] != 0.0) {
+            double y[3];
+            for (int j = 0; j < 3; j++) {
+                y[j] = 0.0;
+                y[j] += T[3 * j + 0] * x0;
+                y[j] += T[3 * j + 1] * x1;
+                y[j] += T[3 * j + 2] * x2;
+            }
+            x0 = y[0]; x1 = y[1]; x2 = y[2];
+        }
+        if (T[13] != 0.0) {
+            x0 += T[9]; x1 += T[10]; x2 += T[11];
+        }
+    }
     return make_double4(x0, x1, x2, 0.0);
 }
 
@@ -67,6 +91,7 @@ __device__ inline void realize_facet(int f, const int *__restrict__ fv, double4 
 // [nf, nf + nv) realize the vertices for the later stages.
 __global__ void k_realize_vf(int nv, int nf, const double *__restrict__ a, const double *__restrict__ u,
                              const double *__restrict__ r, const double *__restrict__ scale,
+                             const int *__restrict__ vcomp, const double *__restrict__ cxf,
                              const int *__restrict__ fv, double4 *__restrict__ vx, double4 *__restrict__ fn,
                              double *__restrict__ area, int4 *__restrict__ fvi)
 {
@@ -74,10 +99,11 @@ __global__ void k_realize_vf(int nv, int nf, const double *__restrict__ a, const
     if (k < nf) {
         int i0 = fv[3 * k + 0], i1 = fv[3 * k + 1], i2 = fv[3 * k + 2];
         fvi[k] = make_int4(i0, i1, i2, 0);
-        realize_facet(k, fv, realize_vertex(i0, a, u, r, scale), realize_vertex(i1, a, u, r, scale),
-                      realize_vertex(i2, a, u, r, scale), fn, area);
+        realize_facet(k, fv, realize_vertex(i0, a, u, r, scale, vcomp, cxf),
+                      realize_vertex(i1, a, u, r, scale, vcomp, cxf), realize_vertex(i2, a, u, r, scale, vcomp, cxf),
+                      fn, area);
     } else if (k < nf + nv) {
-        vx[k - nf] = realize_vertex(k - nf, a, u, r, scale);
+        vx[k - nf] = realize_vertex(k - nf, a, u, r, scale, vcomp, cxf);
     }
 }
 
@@ -140,13 +166,14 @@ __global__ void k_xform(const FrameGeom *__restrict__ geoms, const double4 *__re
 template <typename T4>
 __global__ void k_xform_realize(const FrameGeom *__restrict__ geoms, const double *__restrict__ a,
                                 const double *__restrict__ u, const double *__restrict__ r,
-                                const double *__restrict__ scale, int nv, T4 *__restrict__ vt)
+                                const double *__restrict__ scale, const int *__restrict__ vcomp,
+                                const double *__restrict__ cxf, int nv, T4 *__restrict__ vt)
 {
     grid_dep_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nv) return;
     const FrameGeom &g = geoms[blockIdx.y];
-    double4 x = realize_vertex(i, a, u, r, scale);
+    double4 x = realize_vertex(i, a, u, r, scale, vcomp, cxf);
     double t[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -1020,8 +1047,8 @@ __global__ void __launch_bounds__(CHI2_THREADS, CHI2_MIN_BLOCKS) k_chi2_summary(
 void launch_realize_vf(const ModelDev &m, cudaStream_t s)
 {
     const int B = 256;
-    k_realize_vf<<<(m.nf + m.nv + B - 1) / B, B, 0, s>>>(m.nv, m.nf, m.a, m.u, m.r, m.scale, m.fv, m.vx,
-                                                          m.fn, m.area, m.fvi);
+    k_realize_vf<<<(m.nf + m.nv + B - 1) / B, B, 0, s>>>(m.nv, m.nf, m.a, m.u, m.r, m.scale, m.vcomp, m.cxf, m.fv,
+                                                          m.vx, m.fn, m.area, m.fvi);
 }
 
 void launch_realize_vn(const ModelDev &m, cudaStream_t s)
@@ -1048,7 +1075,7 @@ void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, 
 void launch_xform_realize_f64(const FrameGeom *g, int nviews, const ModelDev &m, double4 *vt, cudaStream_t s)
 {
     dim3 grid((m.nv + 255) / 256, nviews);
-    k_xform_realize<double4><<<grid, 256, 0, s>>>(g, m.a, m.u, m.r, m.scale, m.nv, vt);
+    k_xform_realize<double4><<<grid, 256, 0, s>>>(g, m.a, m.u, m.r, m.scale, m.vcomp, m.cxf, m.nv, vt);
 }
 
 void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt, cudaStream_t s,

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "engine_impl.h"
+#include "spin_impl.cuh"
 #include "kernels.h"
 #include "shape_b200.h"
 
@@ -270,7 +271,7 @@ int EngineImpl::finalize()
     // ---- device allocations
     int rc;
 #define AL(p, n) if ((rc = mem.alloc(&(p), (n))) != SHAPE_OK) return rc
-    AL(d_a, (size_t)3 * nv); AL(d_u, (size_t)3 * nv); AL(d_r, (size_t)nv + 3);
+    AL(d_a, (size_t)3 * nv); AL(d_u, (size_t)3 * nv); AL(d_r, (size_t)npar());
     d_scale = d_r + nv;
     AL(d_fv, (size_t)3 * nf); AL(d_afp, (size_t)nv + 1); AL(d_afi, af_idx.size());
     AL(md.vx, (size_t)nv); AL(md.vn, (size_t)nv); AL(md.fn, (size_t)nf); AL(md.area, (size_t)nf);
@@ -313,10 +314,10 @@ int EngineImpl::finalize()
     AL(d_lc_t, lc_tot_n); AL(d_lc_obs, lc_tot_n); AL(d_lc_oov, lc_tot_n);
     AL(d_lc_fit, lc_tot_n + lc_tot_pts);
 #undef AL
-    if (!h_params) CK(cudaMallocHost((void **)&h_params, sizeof(double) * ((size_t)nv + 3)));
+    if (!h_params) CK(cudaMallocHost((void **)&h_params, sizeof(double) * (size_t)npar()));
     else {
         cudaFreeHost(h_params);
-        CK(cudaMallocHost((void **)&h_params, sizeof(double) * ((size_t)nv + 3)));
+        CK(cudaMallocHost((void **)&h_params, sizeof(double) * (size_t)npar()));
     }
     if (!h_summary) {
         CK(cudaHostAlloc((void **)&h_summary, sizeof(shape_eval_summary), cudaHostAllocMapped));
@@ -408,6 +409,16 @@ int EngineImpl::finalize()
     CK(configure_summary());
     md.nv = nv; md.nf = nf;
     md.a = d_a; md.u = d_u; md.r = d_r; md.scale = d_scale;
+    md.vcomp = nullptr;
+    md.cxf = nullptr;
+    if (ncomp > 1) {
+        if ((rc = mem.alloc(&d_vcomp, (size_t)nv)) != SHAPE_OK) return rc;
+        if ((rc = mem.alloc(&d_cxf, cxf.size())) != SHAPE_OK) return rc;
+        CK(cudaMemcpyAsync(d_vcomp, vcomp.data(), sizeof(int) * (size_t)nv, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_cxf, cxf.data(), sizeof(double) * cxf.size(), cudaMemcpyHostToDevice, stream));
+        md.vcomp = d_vcomp;
+        md.cxf = d_cxf;
+    }
     md.fv = d_fv; md.af_ptr = d_afp; md.af_idx = d_afi;
     rc = tune_bins();
     if (rc) return rc;
@@ -704,6 +715,8 @@ int EngineImpl::set_penalties(int n, const int *type, const double *weight)
 // facets) and the device buffers of the model sums, built on first use.
 int EngineImpl::prepare_penalties()
 {
+    if (ncomp > 1)
+        return set_err(SHAPE_E_UNSUPPORTED, "penalties: models of several components (check_surface's active flags)");
     for (int t : pen_type)
         if (pen_needs_spin(t) && !have_spin)
             return set_err(SHAPE_E_STATE, "penalties: inertiadev, nonpa and impulse need the spin model");
@@ -888,7 +901,7 @@ int EngineImpl::tune_bins()
 {
     cudaStream_t s = stream;
     fill_params(h_params);
-    CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * npar(), cudaMemcpyHostToDevice, s));
     launch_realize(md, s);
     launch_reset_state(d_states, nviews, d_bin_count, ntiles, s);
     launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
@@ -1197,15 +1210,15 @@ int EngineImpl::launch(int form)
     cudaStream_t s = stream;
     fill_params(h_params);
     fill_spin();
-    double sc[3];
-    effective_scale(sc, &pending_baddiam, &pending_bdl);
+    std::vector<double> sc(3 * (size_t)ncomp);
+    effective_scale(sc.data(), &pending_baddiam, &pending_bdl);
     if (!pen_type.empty()) {
         int rc = prepare_penalties();
         if (rc) return rc;
     }
     if (form == SHAPE_FORM_PLAIN_FP64) {
         CK(cudaEventRecord(ev0, s));
-        CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * npar(), cudaMemcpyHostToDevice, s));
         int rc = enqueue(form);
         if (rc) return rc;
         if (!pen_type.empty() && (rc = enqueue_model_sums()) != SHAPE_OK) return rc;
@@ -1230,7 +1243,7 @@ int EngineImpl::launch(int form)
             // rebuilt if the flag changes (rare: a scale factor <= 0.01).
             cudaGraph_t graph;
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s);
+            cudaMemcpyAsync(d_r, h_params, sizeof(double) * npar(), cudaMemcpyHostToDevice, s);
             int rc = enqueue(form);
             cudaError_t ce = cudaStreamEndCapture(s, &graph);
             if (rc) { if (ce == cudaSuccess) cudaGraphDestroy(graph); return rc; }
@@ -1303,7 +1316,7 @@ int EngineImpl::autotune(int form)
         }
     }
     cudaStream_t s = stream;
-    CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * (nv + 3), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_r, h_params, sizeof(double) * npar(), cudaMemcpyHostToDevice, s));
     cudaEvent_t ev[8];
     for (auto &x : ev) CK(cudaEventCreate(&x));
     int best = 0, rc = SHAPE_OK;
@@ -1436,7 +1449,45 @@ int shape_engine_set_model(shape_engine *h, const shape_model_desc *m)
     E.a.assign(m->a, m->a + 3 * (size_t)m->nv);
     E.u.assign(m->u, m->u + 3 * (size_t)m->nv);
     E.r.assign(m->r, m->r + m->nv);
-    for (int j = 0; j < 3; j++) E.scale[j] = m->scale[j];
+    // components: one (scale[]) or several (comp_*), each vertex's component
+    // and each component's rotation matrix (euler2mat of its rotation
+    // offsets, src/util/euler.c) and translation
+    if (m->ncomp > 1) {
+        if (!m->comp_nv || !m->comp_nf || !m->comp_scale || !m->comp_rot || !m->comp_off)
+            return shape::set_err(SHAPE_E_ARG, "set_model: component arrays missing");
+        long long sv = 0, sf = 0;
+        for (int c = 0; c < m->ncomp; c++) {
+            if (m->comp_nv[c] < 1 || m->comp_nf[c] < 1)
+                return shape::set_err(SHAPE_E_ARG, "set_model: a component without vertices or facets");
+            sv += m->comp_nv[c];
+            sf += m->comp_nf[c];
+        }
+        if (sv != m->nv || sf != m->nf)
+            return shape::set_err(SHAPE_E_ARG, "set_model: component sizes do not add up to nv / nf");
+        E.ncomp = m->ncomp;
+        E.scale.assign(m->comp_scale, m->comp_scale + 3 * (size_t)m->ncomp);
+        E.vcomp.resize(m->nv);
+        E.cxf.assign((size_t)shape::CXF_N * m->ncomp, 0.0);
+        int v0 = 0;
+        for (int c = 0; c < m->ncomp; c++) {
+            for (int i = 0; i < m->comp_nv[c]; i++) E.vcomp[v0 + i] = c;
+            v0 += m->comp_nv[c];
+            double mm[3][3];
+            const double *rot = m->comp_rot + 3 * (size_t)c, *off = m->comp_off + 3 * (size_t)c;
+            shape::euler_zxz(mm, rot[0], rot[1], rot[2]);
+            double *T = &E.cxf[(size_t)shape::CXF_N * c];
+            for (int j = 0; j < 3; j++)
+                for (int k = 0; k < 3; k++) T[3 * j + k] = mm[j][k];
+            for (int j = 0; j < 3; j++) T[9 + j] = off[j];
+            T[12] = (rot[0] == 0 && rot[1] == 0 && rot[2] == 0) ? 0.0 : 1.0;
+            T[13] = (off[0] == 0.0 && off[1] == 0.0 && off[2] == 0.0) ? 0.0 : 1.0;
+        }
+    } else {
+        E.ncomp = 1;
+        E.scale.assign(m->scale, m->scale + 3);
+        E.vcomp.clear();
+        E.cxf.clear();
+    }
     E.fv.assign(m->fv, m->fv + 3 * (size_t)m->nf);
     for (int k = 0; k < 3 * m->nf; k++)
         if (E.fv[k] < 0 || E.fv[k] >= m->nv) return shape::set_err(SHAPE_E_ARG, "set_model: facet vertex out of range");
@@ -1637,14 +1688,14 @@ int shape_engine_finalize(shape_engine *h)
 
 int shape_engine_set_scale(shape_engine *h, int j, double value)
 {
-    if (!h || j < 0 || j > 2) return shape::set_err(SHAPE_E_ARG, "set_scale: bad index");
+    if (!h || j < 0 || j >= 3 * h->impl.ncomp) return shape::set_err(SHAPE_E_ARG, "set_scale: bad index");
     h->impl.scale[j] = value;
     return SHAPE_OK;
 }
 
 int shape_engine_get_scale(shape_engine *h, int j, double *value)
 {
-    if (!h || !value || j < 0 || j > 2) return shape::set_err(SHAPE_E_ARG, "get_scale: bad index");
+    if (!h || !value || j < 0 || j >= 3 * h->impl.ncomp) return shape::set_err(SHAPE_E_ARG, "get_scale: bad index");
     *value = h->impl.scale[j];
     return SHAPE_OK;
 }
@@ -1844,7 +1895,7 @@ int shape_engine_stage_times(shape_engine *h, int form, double *ms, int max)
     for (auto &x : ev) cudaEventCreate(&x);
     E.fill_params(E.h_params);
     E.fill_spin();
-    cudaMemcpyAsync(E.d_r, E.h_params, sizeof(double) * (E.nv + 3), cudaMemcpyHostToDevice, E.stream);
+    cudaMemcpyAsync(E.d_r, E.h_params, sizeof(double) * E.npar(), cudaMemcpyHostToDevice, E.stream);
     cudaEventRecord(ev[0], E.stream);
     int rc = E.enqueue(form, ev + 1);
     cudaError_t ce = cudaStreamSynchronize(E.stream);

@@ -83,7 +83,15 @@ struct EngineImpl {
     // model (host)
     int nv = 0, nf = 0;
     std::vector<double> a, u, r;
-    double scale[3] = {1, 1, 1};
+    // scale factors, 3 per component; several components: each vertex's
+    // component and each component's transform (CXF_N doubles)
+    int ncomp = 1;
+    std::vector<double> scale = std::vector<double>(3, 1.0);
+    std::vector<int> vcomp;
+    std::vector<double> cxf;
+    int *d_vcomp = nullptr;
+    double *d_cxf = nullptr;
+    int npar() const { return nv + 3 * ncomp; }   // free parameters uploaded per evaluation
     std::vector<int> fv, af_ptr, af_idx;
     bool have_model = false;
     shape_eval_params params{1, 1, 7, 0.0, 0.0, 1};
@@ -247,13 +255,13 @@ struct EngineImpl {
     int finish(shape_eval_summary *out);
     int pending_baddiam = 0;
     double pending_bdl = 0.0;
-    size_t footprint() const { return mem.bytes + sizeof(double) * ((size_t)nv + 3) + sizeof(shape_eval_summary); }
+    size_t footprint() const { return mem.bytes + sizeof(double) * (size_t)npar() + sizeof(shape_eval_summary); }
     // copies the host description (model, switches, datasets) of another
     // engine; finalize() then builds this engine's own device state
     void clone_host_state(const EngineImpl &o)
     {
         nv = o.nv; nf = o.nf; a = o.a; u = o.u; r = o.r;
-        for (int j = 0; j < 3; j++) scale[j] = o.scale[j];
+        scale = o.scale; ncomp = o.ncomp; vcomp = o.vcomp; cxf = o.cxf;
         fv = o.fv; af_ptr = o.af_ptr; af_idx = o.af_idx; have_model = o.have_model;
         params = o.params; bad_objfactor = o.bad_objfactor;
         dd = o.dd; frames = o.frames; frame_off = o.frame_off; obs = o.obs; oov = o.oov;
@@ -297,9 +305,7 @@ struct EngineImpl {
     void fill_params(double *dst) const
     {
         memcpy(dst, r.data(), sizeof(double) * nv);
-        double sc[3];
-        effective_scale(sc, nullptr, nullptr);
-        memcpy(dst + nv, sc, sizeof sc);
+        effective_scale(dst + nv, nullptr, nullptr);
     }
     // scale factors after realize_coordinates' SMALLRATIO guard
     // (src/shape/realize_mod.c:458-470; SMALLRATIO = 0.01, :138)
@@ -307,7 +313,7 @@ struct EngineImpl {
     {
         int bd = 0;
         double lf = 0.0;
-        for (int j = 0; j < 3; j++) {
+        for (int j = 0; j < 3 * ncomp; j++) {
             double v = scale[j];
             if (v <= 0.01) {
                 bd = 1;

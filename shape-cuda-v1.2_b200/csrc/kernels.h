@@ -36,9 +36,16 @@ inline void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
     cudaLaunchKernelEx(&cfg, kern, args...);
 }
 
+// Per-component transform of a model with several components: the rotation
+// matrix (9, row-major), the translation (3), whether to rotate and whether
+// to translate (nonzero offsets), two spare slots.
+constexpr int CXF_N = 16;
+
 struct ModelDev {
     int nv, nf;
-    const double *a, *u, *r, *scale;   // a,u: [nv*3]
+    const double *a, *u, *r, *scale;   // a,u: [nv*3]; scale: 3 per component
+    const int *vcomp;                  // [nv] component of each vertex (null: one component)
+    const double *cxf;                 // [ncomp * CXF_N] component transforms (null: one component)
     const int *fv;                     // [nf*3]
     const int *af_ptr, *af_idx;
     double4 *vx, *vn, *fn;             // realized

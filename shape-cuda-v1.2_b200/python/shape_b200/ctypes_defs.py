@@ -17,6 +17,9 @@ class ModelDesc(C.Structure):
         ("a", dptr), ("u", dptr), ("r", dptr),
         ("scale", C.c_double * 3),
         ("fv", iptr), ("af_ptr", iptr), ("af_idx", iptr),
+        ("ncomp", C.c_int),
+        ("comp_nv", iptr), ("comp_nf", iptr),
+        ("comp_scale", dptr), ("comp_rot", dptr), ("comp_off", dptr),
     ]
 
 

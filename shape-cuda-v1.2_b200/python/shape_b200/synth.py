@@ -33,6 +33,18 @@ class Model:
     af_idx: np.ndarray     # int32
     scale: np.ndarray = field(default_factory=lambda: np.ones(3))
     name: str = ""
+    # several components (comp_nv / comp_nf vertices and facets each, back to
+    # back; comp_scale replaces scale; comp_rot Euler angles, comp_off
+    # translations): None for one component
+    comp_nv: np.ndarray = None
+    comp_nf: np.ndarray = None
+    comp_scale: np.ndarray = None
+    comp_rot: np.ndarray = None
+    comp_off: np.ndarray = None
+
+    @property
+    def ncomp(self):
+        return 1 if self.comp_nv is None else len(self.comp_nv)
 
     @property
     def nv(self):
@@ -43,8 +55,10 @@ class Model:
         return self.fv.shape[0]
 
     def copy(self):
+        cp = lambda v: None if v is None else v.copy()
         return Model(self.a.copy(), self.u.copy(), self.r.copy(), self.fv.copy(),
-                     self.af_ptr.copy(), self.af_idx.copy(), self.scale.copy(), self.name)
+                     self.af_ptr.copy(), self.af_idx.copy(), self.scale.copy(), self.name,
+                     cp(self.comp_nv), cp(self.comp_nf), cp(self.comp_scale), cp(self.comp_rot), cp(self.comp_off))
 
     def desc(self):
         """ctypes shape_model_desc pointing into this model's arrays."""
@@ -58,6 +72,15 @@ class Model:
         for j in range(3):
             d.scale[j] = float(self.scale[j])
         d.fv, d.af_ptr, d.af_idx = cd.as_iptr(self.fv), cd.as_iptr(self.af_ptr), cd.as_iptr(self.af_idx)
+        if self.comp_nv is not None:
+            self.comp_nv = np.ascontiguousarray(self.comp_nv, dtype=np.int32)
+            self.comp_nf = np.ascontiguousarray(self.comp_nf, dtype=np.int32)
+            for k in ("comp_scale", "comp_rot", "comp_off"):
+                setattr(self, k, np.ascontiguousarray(getattr(self, k), dtype=np.float64))
+            d.ncomp = len(self.comp_nv)
+            d.comp_nv, d.comp_nf = cd.as_iptr(self.comp_nv), cd.as_iptr(self.comp_nf)
+            d.comp_scale, d.comp_rot = cd.as_dptr(self.comp_scale), cd.as_dptr(self.comp_rot)
+            d.comp_off = cd.as_dptr(self.comp_off)
         return d
 
 
@@ -195,6 +218,31 @@ def ellipsoid_model(semi=(1.0, 0.8, 0.6), nrings=23, nper=50):
     base = dirs * np.asarray(semi)[None, :]
     u = base / np.linalg.norm(base, axis=1)[:, None]
     return make_model(u, fv, None, base=base, name="ellipsoid-%d" % fv.shape[0])
+
+
+def two_component_model(rot=(0.3, 0.5, -0.2), off=(0.6, -0.1, 0.05), radius=0.35):
+    """A contact-binary-like two-component VERTEX model: the config-1
+    ellipsoid (1152 vertices) and a smaller sphere (602 vertices) that it
+    partly hides, rotated by Euler angles rot and translated by off (km),
+    scale factors per component."""
+    m1 = ellipsoid_model()
+    dirs, fv2 = ring_sphere(15, 40)
+    base2 = radius * dirs
+    m2 = make_model(dirs, fv2, None, base=base2, name="sphere")
+    nv1 = m1.nv
+    a = np.concatenate([m1.a, m2.a])
+    u = np.concatenate([m1.u, m2.u])
+    r = np.concatenate([m1.r, m2.r])
+    fv = np.concatenate([m1.fv, m2.fv + nv1]).astype(np.int32)
+    af_ptr = np.concatenate([m1.af_ptr[:-1], m2.af_ptr + m1.af_ptr[-1]]).astype(np.int32)
+    af_idx = np.concatenate([m1.af_idx, m2.af_idx + m1.nf]).astype(np.int32)
+    m = Model(a, u, r, fv, af_ptr, af_idx, np.ones(3), "two-component")
+    m.comp_nv = np.array([m1.nv, m2.nv], dtype=np.int32)
+    m.comp_nf = np.array([m1.nf, m2.nf], dtype=np.int32)
+    m.comp_scale = np.array([[1.0, 1.0, 1.0], [1.05, 0.95, 1.0]])
+    m.comp_rot = np.array([[0.0, 0.0, 0.0], list(rot)])
+    m.comp_off = np.array([[0.0, 0.0, 0.0], list(off)])
+    return m
 
 
 def harmonic_model(nrings=40, nper=100, lmax=8, amp=0.05, seed=42):
