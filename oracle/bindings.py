@@ -248,6 +248,8 @@ class Reference:
         L.ref_mod_read.restype = C.c_void_p
         L.ref_mod_shape.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), cd.dptr, cd.dptr, cd.dptr, cd.dptr,
                                     cd.iptr, cd.iptr, cd.iptr]
+        L.ref_mod_comp.argtypes = [C.c_void_p, C.c_int, P(C.c_int), P(C.c_int), cd.dptr, cd.dptr, cd.dptr]
+        L.ref_mod_comp.restype = C.c_int
         L.ref_mod_radar.argtypes = [C.c_void_p, C.c_int, P(cd.RadarLaw)]
         L.ref_mod_optical.argtypes = [C.c_void_p, C.c_int, P(cd.OpticalLaw)]
         L.ref_mod_spin.argtypes = [C.c_void_p, P(cd.SpinState)]
@@ -341,8 +343,16 @@ class Reference:
             optical.append(olaw)
         spin = cd.SpinState()
         self.lib.ref_mod_spin(h, C.byref(spin))
+        comps = []
+        ncomp = self.lib.ref_mod_comp(h, -1, C.byref(C.c_int()), C.byref(C.c_int()), None, None, None)
+        for c in range(ncomp):
+            cnv, cnf = C.c_int(), C.c_int()
+            csc, coff, crot = np.zeros(3), np.zeros(3), np.zeros(3)
+            self.lib.ref_mod_comp(h, c, C.byref(cnv), C.byref(cnf), cd.as_dptr(csc), cd.as_dptr(coff),
+                                  cd.as_dptr(crot))
+            comps.append({"nv": cnv.value, "nf": cnf.value, "scale": csc, "off": coff, "rot": crot})
         arrays = {"a": a.reshape(nv, 3), "u": u.reshape(nv, 3), "r": r, "scale": sc, "fv": fv.reshape(nf, 3),
-                  "af_ptr": ap, "af_idx": ai}
+                  "af_ptr": ap, "af_idx": ai, "comps": comps}
         return arrays, radar, optical, spin
 
     def read_radar_data(self, path, kind, ndel, ndop, idel_use, idop_use, swap, sdev):

@@ -826,28 +826,54 @@ void *ref_mod_read(const char *path)
 
 /* Sizes into nv / nf; the arrays (each may be NULL) as shape_model_desc
  * holds them. */
+/* The model's vertex components back to back: vertex and facet indices made
+ * model-wide (a component's local index plus the vertices or facets of the
+ * components before it); scale holds component 0's factors. */
 void ref_mod_shape(void *h, int *nv, int *nf, double *a, double *u, double *r, double *scale, int *fv,
                    int *af_ptr, int *af_idx)
 {
     ref_modfile *F = h;
-    struct vertices_t *real = &F->mod.shape.comp[0].real;
-    *nv = real->nv;
-    *nf = real->nf;
-    for (int j = 0; j < 3 && scale; j++) scale[j] = real->scalefactor[j].val;
-    int k = 0;
-    for (int i = 0; i < real->nv; i++) {
-        for (int j = 0; j < 3; j++) {
-            if (a) a[3 * i + j] = real->v[i].a[j];
-            if (u) u[3 * i + j] = real->v[i].u[j];
+    int v0 = 0, f0 = 0, k = 0;
+    for (int c = 0; c < F->mod.shape.ncomp; c++) {
+        struct vertices_t *real = &F->mod.shape.comp[c].real;
+        if (c == 0)
+            for (int j = 0; j < 3 && scale; j++) scale[j] = real->scalefactor[j].val;
+        for (int i = 0; i < real->nv; i++) {
+            const int g = v0 + i;
+            for (int j = 0; j < 3; j++) {
+                if (a) a[3 * g + j] = real->v[i].a[j];
+                if (u) u[3 * g + j] = real->v[i].u[j];
+            }
+            if (r) r[g] = real->v[i].r.val;
+            if (af_ptr) af_ptr[g] = k;
+            for (int q = 0; q < real->v[i].naf; q++, k++)
+                if (af_idx) af_idx[k] = f0 + real->v[i].af[q];
         }
-        if (r) r[i] = real->v[i].r.val;
-        if (af_ptr) af_ptr[i] = k;
-        for (int q = 0; q < real->v[i].naf; q++, k++)
-            if (af_idx) af_idx[k] = real->v[i].af[q];
+        for (int f = 0; f < real->nf && fv; f++)
+            for (int j = 0; j < 3; j++) fv[3 * (f0 + f) + j] = v0 + real->f[f].v[j];
+        v0 += real->nv;
+        f0 += real->nf;
     }
-    if (af_ptr) af_ptr[real->nv] = k;
-    for (int f = 0; f < real->nf && fv; f++)
-        for (int j = 0; j < 3; j++) fv[3 * f + j] = real->f[f].v[j];
+    *nv = v0;
+    *nf = f0;
+    if (af_ptr) af_ptr[v0] = k;
+}
+
+/* Component c's vertex and facet counts, scale factors, linear offsets (km)
+ * and rotation offsets (radians); returns the number of components. */
+int ref_mod_comp(void *h, int c, int *nv, int *nf, double *scale, double *off, double *rot)
+{
+    ref_modfile *F = h;
+    if (c < 0 || c >= F->mod.shape.ncomp) return F->mod.shape.ncomp;
+    struct comp_t *cm = &F->mod.shape.comp[c];
+    *nv = cm->real.nv;
+    *nf = cm->real.nf;
+    for (int j = 0; j < 3; j++) {
+        scale[j] = cm->real.scalefactor[j].val;
+        off[j] = cm->off[j].val;
+        rot[j] = cm->rot[j].val;
+    }
+    return F->mod.shape.ncomp;
 }
 
 int ref_mod_radar(void *h, int i, shape_radar_law *L)

@@ -33,9 +33,14 @@ int report_error(int code, const std::string &msg);   // engine.cu
 
 struct shape_mod_file {
     std::vector<double> a, u, r;
-    double scale[3];
+    // components back to back: vertices and facets of each, its scale
+    // factors (3 each, with their states), linear offsets (km) and rotation
+    // offsets (the file's degrees wrapped into (-180, 180], and in radians)
+    std::vector<double> scale;
+    std::vector<char> scale_state;
+    std::vector<int> comp_nv, comp_nf;
+    std::vector<double> comp_off, comp_rot, comp_rot_deg;
     std::vector<int> fv, af_ptr, af_idx;
-    char scale_state[3];
     std::vector<char> r_state;
     std::vector<shape_radar_law> radar;
     std::vector<shape_optical_law> optical;
@@ -181,40 +186,62 @@ bool calendar(double jd, int c[6])
 void read_shape(Tokens &tk, shape_mod_file &m)
 {
     const int ncomp = tk.integer("number of components");
-    if (ncomp != 1) tk.fail("only one-component models are supported", SHAPE_E_UNSUPPORTED);
-    for (int j = 0; j < 6; j++) {
-        char st;
-        const double v = tk.param(j < 3 ? "component offset" : "component rotation", &st);
-        if (v != 0.0 || st == 'f')
-            tk.fail("component offsets and rotations must be held at zero", SHAPE_E_UNSUPPORTED);
-    }
-    const std::string type = tk.word("component type");
-    if (type != "vertex") tk.fail("component type " + type + ": only vertex components are supported",
-                                  SHAPE_E_UNSUPPORTED);
-    const int nv = tk.integer("number of vertices");
-    if (nv < 4) tk.fail("a vertex model needs at least 4 vertices");
-    for (int j = 0; j < 3; j++) m.scale[j] = tk.param("scale factor", &m.scale_state[j]);
-    if (m.scale_state[0] == '=') tk.fail("scale factor 0 cannot take the = state");
-    m.a.resize(3 * (size_t)nv);
-    m.u.resize(3 * (size_t)nv);
-    m.r.resize(nv);
-    m.r_state.resize(nv);
-    for (int v = 0; v < nv; v++) {
-        m.r[v] = tk.param("vertex deviation", &m.r_state[v]);
-        if (m.r_state[v] == '=')
-            tk.fail("mirrored vertex deviations (= state) are not supported", SHAPE_E_UNSUPPORTED);
-        for (int k = 0; k < 3; k++) m.u[3 * (size_t)v + k] = tk.real("vertex direction");
-        for (int k = 0; k < 3; k++) m.a[3 * (size_t)v + k] = tk.real("vertex base point");
-    }
-    const int nf = tk.integer("number of facets");
-    if (nf < 4) tk.fail("a vertex model needs at least 4 facets");
-    m.fv.resize(3 * (size_t)nf);
-    for (size_t k = 0; k < m.fv.size(); k++) {
-        m.fv[k] = tk.integer("facet vertex");
-        if (m.fv[k] < 0 || m.fv[k] >= nv) tk.fail("facet vertex index out of range");
+    if (ncomp < 1) tk.fail("a model needs at least one component");
+    for (int c = 0; c < ncomp; c++) {
+        double off[3], deg[3];
+        for (int j = 0; j < 6; j++) {
+            char st;
+            double v = tk.param(j < 3 ? "component offset" : "component rotation", &st);
+            if (st != 'c')
+                tk.fail("component offsets and rotations must be held constant (c)", SHAPE_E_UNSUPPORTED);
+            // angles wrapped into (-180, 180] before the conversion
+            // (src/shape/read_mod.c:314-320)
+            if (j >= 3) v += 360.0 * floor((180.0 - v) / 360.0);
+            if (j < 3) off[j] = v; else deg[j - 3] = v;
+        }
+        const std::string type = tk.word("component type");
+        if (type != "vertex") tk.fail("component type " + type + ": only vertex components are supported",
+                                      SHAPE_E_UNSUPPORTED);
+        const int nv = tk.integer("number of vertices");
+        if (nv < 4) tk.fail("a vertex model needs at least 4 vertices");
+        const int v0 = (int)m.r.size(), f0 = (int)(m.fv.size() / 3);
+        for (int j = 0; j < 3; j++) {
+            char st;
+            m.scale.push_back(tk.param("scale factor", &st));
+            m.scale_state.push_back(st);
+        }
+        if (m.scale_state[3 * c] == '=') tk.fail("scale factor 0 cannot take the = state");
+        m.a.resize(3 * (size_t)(v0 + nv));
+        m.u.resize(3 * (size_t)(v0 + nv));
+        m.r.resize(v0 + nv);
+        m.r_state.resize(v0 + nv);
+        for (int v = v0; v < v0 + nv; v++) {
+            m.r[v] = tk.param("vertex deviation", &m.r_state[v]);
+            if (m.r_state[v] == '=')
+                tk.fail("mirrored vertex deviations (= state) are not supported", SHAPE_E_UNSUPPORTED);
+            for (int k = 0; k < 3; k++) m.u[3 * (size_t)v + k] = tk.real("vertex direction");
+            for (int k = 0; k < 3; k++) m.a[3 * (size_t)v + k] = tk.real("vertex base point");
+        }
+        const int nf = tk.integer("number of facets");
+        if (nf < 4) tk.fail("a vertex model needs at least 4 facets");
+        m.fv.resize(3 * (size_t)(f0 + nf));
+        for (size_t k = 3 * (size_t)f0; k < m.fv.size(); k++) {
+            const int v = tk.integer("facet vertex");
+            if (v < 0 || v >= nv) tk.fail("facet vertex index out of range");
+            m.fv[k] = v0 + v;                  // model-wide vertex index
+        }
+        m.comp_nv.push_back(nv);
+        m.comp_nf.push_back(nf);
+        for (int j = 0; j < 3; j++) {
+            m.comp_off.push_back(off[j]);
+            m.comp_rot_deg.push_back(deg[j]);
+            m.comp_rot.push_back(deg[j] * D2R);
+        }
     }
     // attached facets of each vertex, in increasing facet order
-    // (setupvertices, src/shape/read_mod.c:2504-2590)
+    // (setupvertices, src/shape/read_mod.c:2504-2590); a component's
+    // vertices only touch its own facets
+    const int nv = (int)m.r.size(), nf = (int)(m.fv.size() / 3);
     m.af_ptr.assign((size_t)nv + 1, 0);
     for (int v : m.fv) m.af_ptr[v + 1]++;
     for (int v = 0; v < nv; v++) m.af_ptr[v + 1] += m.af_ptr[v];
@@ -405,6 +432,13 @@ int shape_mod_model(const shape_mod_file *m, shape_model_desc *out)
     out->fv = m->fv.data();
     out->af_ptr = m->af_ptr.data();
     out->af_idx = m->af_idx.data();
+    const int nc = (int)m->comp_nv.size();
+    out->ncomp = nc > 1 ? nc : 0;
+    out->comp_nv = nc > 1 ? m->comp_nv.data() : nullptr;
+    out->comp_nf = nc > 1 ? m->comp_nf.data() : nullptr;
+    out->comp_scale = nc > 1 ? m->scale.data() : nullptr;
+    out->comp_rot = nc > 1 ? m->comp_rot.data() : nullptr;
+    out->comp_off = nc > 1 ? m->comp_off.data() : nullptr;
     return SHAPE_OK;
 }
 
@@ -447,8 +481,12 @@ int shape_mod_free_params(const shape_mod_file *m, shape_fit_param *out, int max
         }
         n++;
     };
-    for (int j = 0; j < 3; j++) add(m->scale_state[j], SHAPE_PAR_SCALE, j);
-    for (size_t v = 0; v < m->r_state.size(); v++) add(m->r_state[v], SHAPE_PAR_VERTEX_R, (int)v);
+    // per component its scale factors, then its vertex deviations
+    // (src/shape/mkparlist.c:109-235)
+    for (size_t c = 0, v0 = 0; c < m->comp_nv.size(); v0 += m->comp_nv[c], c++) {
+        for (int j = 0; j < 3; j++) add(m->scale_state[3 * c + j], SHAPE_PAR_SCALE, (int)(3 * c + j));
+        for (size_t v = v0; v < v0 + m->comp_nv[c]; v++) add(m->r_state[v], SHAPE_PAR_VERTEX_R, (int)v);
+    }
     for (int i = 0; i < 3; i++) add(m->angle_state[i], SHAPE_PAR_SPIN_ANGLE, i);
     for (int i = 0; i < 3; i++) add(m->omega_state[i], SHAPE_PAR_SPIN_OMEGA, i);
     for (int i = 0; i < 3; i++) add(m->inertia_state[i], SHAPE_PAR_SPIN_INERTIA, i);
@@ -459,8 +497,8 @@ int shape_mod_free_params(const shape_mod_file *m, shape_fit_param *out, int max
     return n;
 }
 
-// Writes m as a model file that read_mod reads back: one vertex component
-// with zero offsets, its laws and the spin section, the parameter states of
+// Writes m as a model file that read_mod reads back: its vertex components
+// with their offsets, its laws and the spin section, the parameter states of
 // the file it came from, numbers with 17 significant digits (shape values
 // exactly; angles and rates back in degrees, which rounds their last bit).
 int shape_mod_write(const shape_mod_file *m, const char *path)
@@ -474,21 +512,31 @@ int shape_mod_write(const shape_mod_file *m, const char *path)
     FILE *fp = fopen(path, "w");
     if (!fp) return shape::report_error(SHAPE_E_ARG, std::string("mod_write: cannot create ") + path);
     auto par = [&](char st, double v) { fprintf(fp, " %c %.17g", st, v); };
-    const int nv = (int)m->r.size(), nf = (int)(m->fv.size() / 3);
-    fprintf(fp, "{SHAPE model file written by shape-b200}\n\n{shape}\n1 {component}\n");
-    fprintf(fp, " c 0 c 0 c 0 {linear offsets (km)}\n c 0 c 0 c 0 {rotation offsets (deg)}\n");
-    fprintf(fp, "vertex\n%d {vertices}\n", nv);
-    for (int j = 0; j < 3; j++) par(m->scale_state[j], m->scale[j]);
-    fprintf(fp, " {scale factors}\n");
-    for (int v = 0; v < nv; v++) {
-        par(m->r_state[v], m->r[v]);
-        for (int k = 0; k < 3; k++) fprintf(fp, " %.17g", m->u[3 * (size_t)v + k]);
-        for (int k = 0; k < 3; k++) fprintf(fp, " %.17g", m->a[3 * (size_t)v + k]);
-        fprintf(fp, "\n");
+    const int ncomp = (int)m->comp_nv.size();
+    fprintf(fp, "{SHAPE model file written by shape-b200}\n\n{shape}\n%d {components}\n", ncomp);
+    int v0 = 0, f0 = 0;
+    for (int c = 0; c < ncomp; c++) {
+        const int nv = m->comp_nv[c], nf = m->comp_nf[c];
+        for (int j = 0; j < 3; j++) par('c', m->comp_off[3 * (size_t)c + j]);
+        fprintf(fp, " {linear offsets (km)}\n");
+        for (int j = 0; j < 3; j++) par('c', m->comp_rot_deg[3 * (size_t)c + j]);
+        fprintf(fp, " {rotation offsets (deg)}\n");
+        fprintf(fp, "vertex\n%d {vertices}\n", nv);
+        for (int j = 0; j < 3; j++) par(m->scale_state[3 * (size_t)c + j], m->scale[3 * (size_t)c + j]);
+        fprintf(fp, " {scale factors}\n");
+        for (int v = v0; v < v0 + nv; v++) {
+            par(m->r_state[v], m->r[v]);
+            for (int k = 0; k < 3; k++) fprintf(fp, " %.17g", m->u[3 * (size_t)v + k]);
+            for (int k = 0; k < 3; k++) fprintf(fp, " %.17g", m->a[3 * (size_t)v + k]);
+            fprintf(fp, "\n");
+        }
+        fprintf(fp, "%d {facets}\n", nf);
+        for (int f = f0; f < f0 + nf; f++)
+            fprintf(fp, "%d %d %d\n", m->fv[3 * (size_t)f] - v0, m->fv[3 * (size_t)f + 1] - v0,
+                    m->fv[3 * (size_t)f + 2] - v0);
+        v0 += nv;
+        f0 += nf;
     }
-    fprintf(fp, "%d {facets}\n", nf);
-    for (int f = 0; f < nf; f++)
-        fprintf(fp, "%d %d %d\n", m->fv[3 * (size_t)f], m->fv[3 * (size_t)f + 1], m->fv[3 * (size_t)f + 2]);
     fprintf(fp, "\n{photometry}\n%d {radar laws}\n", (int)m->radar.size());
     for (size_t i = 0; i < m->radar.size(); i++) {
         const shape_radar_law &L = m->radar[i];
@@ -554,8 +602,8 @@ int shape_mod_write(const shape_mod_file *m, const char *path)
 int shape_mod_take_engine(shape_mod_file *m, shape_engine *e)
 {
     if (!m || !e) return shape::report_error(SHAPE_E_ARG, "mod_take_engine: null argument");
-    for (int j = 0; j < 3; j++)
-        if (int rc = shape_engine_get_scale(e, j, &m->scale[j])) return rc;
+    for (size_t j = 0; j < m->scale.size(); j++)
+        if (int rc = shape_engine_get_scale(e, (int)j, &m->scale[j])) return rc;
     for (size_t v = 0; v < m->r.size(); v++)
         if (int rc = shape_engine_get_vertex_r(e, (int)v, &m->r[v])) return rc;
     double x;

@@ -732,9 +732,16 @@ class ModFile:
         nv, nf = d.nv, d.nf
         arr = lambda p, n, dt: np.ctypeslib.as_array(p, shape=(n,)).astype(dt).copy()
         af_ptr = arr(d.af_ptr, nv + 1, np.int32)
-        return Model(arr(d.a, 3 * nv, np.float64).reshape(nv, 3), arr(d.u, 3 * nv, np.float64).reshape(nv, 3),
-                     arr(d.r, nv, np.float64), arr(d.fv, 3 * nf, np.int32).reshape(nf, 3), af_ptr,
-                     arr(d.af_idx, int(af_ptr[-1]), np.int32), np.array(d.scale[:]))
+        m = Model(arr(d.a, 3 * nv, np.float64).reshape(nv, 3), arr(d.u, 3 * nv, np.float64).reshape(nv, 3),
+                  arr(d.r, nv, np.float64), arr(d.fv, 3 * nf, np.int32).reshape(nf, 3), af_ptr,
+                  arr(d.af_idx, int(af_ptr[-1]), np.int32), np.array(d.scale[:]))
+        if d.ncomp > 1:
+            nc = d.ncomp
+            m.comp_nv, m.comp_nf = arr(d.comp_nv, nc, np.int32), arr(d.comp_nf, nc, np.int32)
+            m.comp_scale = arr(d.comp_scale, 3 * nc, np.float64).reshape(nc, 3)
+            m.comp_rot = arr(d.comp_rot, 3 * nc, np.float64).reshape(nc, 3)
+            m.comp_off = arr(d.comp_off, 3 * nc, np.float64).reshape(nc, 3)
+        return m
 
     def radar_laws(self):
         n = _chk(self.L.shape_mod_radar_law(self.h, 0, None))

@@ -43,21 +43,25 @@ class Writer:
 
 
 def write_mod(path, m, seed=0, states=None, radar=("cosine", 0.1, 1.0), optical=("kaasalainen",),
-              spin=None, ctype="vertex", rstate="f"):
+              spin=None, ctype="vertex", rstate="f", comps=None):
+    """comps: several components, (model, offset km, rotation deg, scale
+    states) each, in place of m."""
     w = Writer(seed)
     st = states or {}
-    w.tok(1)
-    for _ in range(6):
-        w.par("c", 0.0)
-    w.tok(ctype, m.nv)
-    for j in range(3):
-        w.par(st.get("scale", "fcf")[j], m.scale[j])
-    for v in range(m.nv):
-        w.par(rstate if v % 7 else "c", m.r[v])
-        w.tok(*[float(x) for x in m.u[v]], *[float(x) for x in m.a[v]])
-    w.tok(m.nf)
-    for f in range(m.nf):
-        w.tok(*[int(x) for x in m.fv[f]])
+    comps = comps or [(m, (0.0,) * 3, (0.0,) * 3, st.get("scale", "fcf"))]
+    w.tok(len(comps))
+    for cm, off, rot, sst in comps:
+        for x in tuple(off) + tuple(rot):
+            w.par("c", x)
+        w.tok(ctype, cm.nv)
+        for j in range(3):
+            w.par(sst[j], cm.scale[j])
+        for v in range(cm.nv):
+            w.par(rstate if v % 7 else "c", cm.r[v])
+            w.tok(*[float(x) for x in cm.u[v]], *[float(x) for x in cm.a[v]])
+        w.tok(cm.nf)
+        for f in range(cm.nf):
+            w.tok(*[int(x) for x in cm.fv[f]])
     w.tok(1, radar[0])
     if radar[0] == "cosine":
         w.par("f", radar[1]); w.par("c", radar[2])
@@ -142,6 +146,49 @@ def test_mod_matches_reference_read_mod(tmp_path, ref, seed):
     assert fp[2 + nr:] == [(eng.PAR_SPIN_ANGLE, 0), (eng.PAR_SPIN_ANGLE, 1), (eng.PAR_SPIN_ANGLE, 2),
                            (eng.PAR_SPIN_OMEGA, 2), (eng.PAR_SPIN_IMPULSE, 2)]
     mf.close()
+
+
+def test_mod_two_components(tmp_path, ref):
+    """Two vertex components: vertices, facets and attached-facet lists
+    concatenated with model-wide indices, each component's scale factors,
+    offsets and rotations (degrees wrapped into (-180, 180], then radians)
+    equal to the reference's; free parameters per component (its scale
+    factors, then its vertex deviations); the file written back reads the
+    same."""
+    from shape_b200 import synth
+    m1 = cases.c1()[0].copy()
+    m1.r = np.random.default_rng(1).normal(0, 0.02, m1.nv)
+    dirs, fv2 = synth.ring_sphere(6, 10)
+    m2 = synth.make_model(dirs, fv2, None, base=0.3 * dirs, name="small")
+    m2.scale = np.array([1.05, 0.97, 1.0])
+    comps = [(m1, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), "fcc"),
+             (m2, (0.6, -0.1, 0.05), (200.0, -190.0, 30.5), "cff")]
+    path = tmp_path / "two.mod"
+    write_mod(path, None, seed=11, comps=comps)
+    mf, got = _compare(path, ref)
+    arrays = ref.read_mod(str(path))[0]
+    assert got.ncomp == 2 and len(arrays["comps"]) == 2
+    for c, rc in enumerate(arrays["comps"]):
+        assert got.comp_nv[c] == rc["nv"] and got.comp_nf[c] == rc["nf"]
+        assert np.array_equal(got.comp_scale[c], rc["scale"])
+        assert np.array_equal(got.comp_off[c], rc["off"])
+        assert np.array_equal(got.comp_rot[c], rc["rot"])
+    assert got.comp_rot[1][0] < 0 and got.comp_rot[1][1] > 0
+    assert np.array_equal(got.fv[m1.nf:], m2.fv + m1.nv)
+    fp = mf.free_params()
+    n1 = sum(1 for v in range(m1.nv) if v % 7)
+    n2 = sum(1 for v in range(m2.nv) if v % 7)
+    assert fp[0] == (eng.PAR_SCALE, 0)
+    assert fp[1 + n1:3 + n1] == [(eng.PAR_SCALE, 4), (eng.PAR_SCALE, 5)]
+    assert fp[3 + n1][1] == m1.nv + 1 and len(fp) == 3 + n1 + n2 + 5
+    out = tmp_path / "two_back.mod"
+    mf.write(out)
+    mb, back = _compare(out, ref)
+    for k in ("a", "u", "r", "fv", "af_ptr", "af_idx", "comp_nv", "comp_nf", "comp_scale", "comp_off", "comp_rot"):
+        assert np.array_equal(np.asarray(getattr(back, k)), np.asarray(getattr(got, k))), k
+    assert mb.free_params() == fp
+    mf.close()
+    mb.close()
 
 
 def test_mod_non_principal_axis(tmp_path, ref):
