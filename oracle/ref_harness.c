@@ -37,6 +37,10 @@ static void ref_alloc_pos(struct pos_t *pos, int n, double kmpp, int bistatic)
     pos->compill = imatrix(-n, n, -n, n);
     pos->fill = imatrix(-n, n, -n, n);
     pos->bistatic = bistatic;
+    /* defined contents before any routine writes them: a drop-in that
+     * writes only some maps leaves the others as the reference's posclr
+     * sets them, not as malloc left them */
+    posclr(pos);
 }
 
 static void ref_free_pos(struct pos_t *pos)
@@ -490,7 +494,7 @@ void ref_get_seen(void *h, unsigned char *seen)
 /* The model-wide index of component c's facet f (components back to back). */
 static int ref_global_facet(const struct mod_t *mod, int c, int f)
 {
-    if (!mod || f < 0) return f;
+    if (!mod || f < 0 || c < 0 || c >= mod->shape.ncomp) return f;
     for (int k = 0; k < c; k++) f += mod->shape.comp[k].real.nf;
     return f;
 }

@@ -2077,12 +2077,16 @@ int shape_engine_vary_params(shape_engine *h, const shape_vary_options *opt, dou
         const shape::SetRec &R = E.setrecs[0];
         if (R.type == 0 && !E.fviews[R.first].empty())
             return shape::set_err(SHAPE_E_UNSUPPORTED, "vary_params: the first dataset has smeared frames");
-        const int keep = E.keep_pos;
         if (E.finalized) cudaSetDevice(E.device);
+        // the evaluation keeps its POS maps for the reads below; the
+        // caller's setting comes back on every return path
+        struct KeepPos {
+            decltype(E.keep_pos) &ref, old;
+            ~KeepPos() { ref = old; }
+        } keep_guard{E.keep_pos, E.keep_pos};
         E.keep_pos = 1;
         shape_eval_summary sm;
         int rc = E.evaluate(SHAPE_FORM_PLAIN_FP64, &sm);
-        E.keep_pos = keep;
         if (rc) return rc;
         if (R.type == 0) {
             int ds = 0;

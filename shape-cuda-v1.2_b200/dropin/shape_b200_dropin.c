@@ -192,12 +192,14 @@ static void b200_build(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
     for (int f = 0; f < nf; f++)
         for (int j = 0; j < 3; j++) fv[3 * f + j] = real->f[f].v[j];
     shape_model_desc m;
+    memset(&m, 0, sizeof m);
     m.nv = nv; m.nf = nf; m.a = a; m.u = u; m.r = r; m.fv = fv; m.af_ptr = afp; m.af_idx = afi;
     for (int j = 0; j < 3; j++) m.scale[j] = c->desc.ver.scalefactor[j].val;
     b200_check(shape_engine_set_model(g_eng, &m), "set_model");
     free(a); free(u); free(r); free(fv); free(afp); free(afi);
 
     shape_eval_params ep;
+    memset(&ep, 0, sizeof ep);
     ep.pos_smooth = par->pos_smooth;
     ep.nsinc2 = par->nsinc2;
     ep.sinc2width = par->sinc2width;
@@ -212,6 +214,7 @@ static void b200_build(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
             struct deldop_t *dd = &set->desc.deldop;
             if (dd->nviews != 1) b200_unsupported("delay-Doppler smearing (nviews > 1)");
             shape_deldop_set S;
+            memset(&S, 0, sizeof S);
             S.del_per_pixel = dd->del_per_pixel; S.dop_per_pixel = dd->dop_per_pixel;
             S.Ftx = dd->Ftx; S.dopscale = dd->dopscale.val; S.codemethod = dd->codemethod;
             S.spb = dd->spb; S.stride = dd->stride; S.dopfftlen = dd->dopfftlen;
@@ -249,6 +252,7 @@ static void b200_build(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
             struct doppler_t *dp = &set->desc.doppler;
             if (dp->nviews != 1) b200_unsupported("Doppler smearing (nviews > 1)");
             shape_doppler_set S;
+            memset(&S, 0, sizeof S);
             S.dop_per_bin = dp->dop_per_bin; S.Ftx = dp->Ftx; S.dopscale = dp->dopscale.val;
             S.law = radar_law_of(&mod->photo, dp->iradlaw);
             shape_doppler_frame *F = calloc((size_t)dp->nframes, sizeof *F);
@@ -281,6 +285,7 @@ static void b200_build(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
             struct lghtcrv_t *lc = &set->desc.lghtcrv;
             if (lc->nviews != 1) b200_unsupported("lightcurve smearing (nviews > 1)");
             shape_lghtcrv_set L;
+            memset(&L, 0, sizeof L);
             double *x = malloc(sizeof(double) * lc->ncalc), *t = malloc(sizeof(double) * lc->n);
             double *obs = malloc(sizeof(double) * lc->n), *oov = malloc(sizeof(double) * lc->n);
             for (int i = 1; i <= lc->ncalc; i++) x[i - 1] = lc->x[i];
@@ -421,6 +426,7 @@ static void copy_frame_results(struct dat_t *dat, int with_chi2)
 void SHAPE_B200_CALC_FITS(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
 {
     shape_eval_summary sm;
+    memset(&sm, 0, sizeof sm);
     b200_evaluate(par, mod, dat, &sm);
     copy_frame_results(dat, 0);
     size_t maxd = 1;
@@ -496,6 +502,7 @@ void SHAPE_B200_CALC_FITS(struct par_t *par, struct mod_t *mod, struct dat_t *da
 double SHAPE_B200_CALC_FITS_CHI2(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
 {
     shape_eval_summary sm;
+    memset(&sm, 0, sizeof sm);
     b200_evaluate(par, mod, dat, &sm);
     copy_frame_results(dat, 1);
     for (int s = 0; s < dat->nsets; s++) {

@@ -119,6 +119,7 @@ int B200_NAME(posvis)(struct vertices_t *verts, double orbit_offset[3], struct p
     for (int f = 0; f < nf; f++)
         for (int k = 0; k < 3; k++) { fn[3 * f + k] = verts->f[f].n[k]; fv[3 * f + k] = verts->f[f].v[k]; }
     shape_pos_view view;
+    memset(&view, 0, sizeof view);
     pos_view_of(pos, &view);
     shape_pos_images im;
     memset(&im, 0, sizeof im);
@@ -163,6 +164,7 @@ int B200_NAME(pos2deldop)(struct par_t *par, struct photo_t *photo, double orbit
     struct pos_t *pos = &frame->pos;
     const int n = pos->n, ndel = frame->ndel, ndop = frame->ndop;
     shape_pos_view view;
+    memset(&view, 0, sizeof view);
     pos_view_of(pos, &view);
     shape_pos_images im;
     memset(&im, 0, sizeof im);
@@ -256,6 +258,7 @@ void B200_NAME(posmask)(struct pos_t *pos, double tol)
 {
     const int n = pos->n;
     shape_pos_view view;
+    memset(&view, 0, sizeof view);
     pos_view_of(pos, &view);
     shape_pos_images im;
     memset(&im, 0, sizeof im);
@@ -278,6 +281,7 @@ double B200_NAME(apply_photo)(struct mod_t *mod, int ilaw, double phase, double 
     const int n = pos->n;
     shape_optical_law law = optical_law_of(&mod->photo, ilaw);
     shape_pos_view view;
+    memset(&view, 0, sizeof view);
     pos_view_of(pos, &view);
     shape_pos_images im;
     memset(&im, 0, sizeof im);
