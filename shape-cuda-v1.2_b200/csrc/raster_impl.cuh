@@ -63,6 +63,10 @@ namespace shape {
 // Largest facet bitmap (32-bit words) the bin rank uses: models up to 262144
 // facets; larger ones rank by comparisons.
 constexpr int BITMAP_MAX_WORDS = 8192;
+// Bins of at most STAGE_FACETS facets of models up to this many bitmap
+// words (65536 facets) are ranked and staged in one pass (k_raster's fused
+// path), with the bitmap in its own shared-memory area.
+constexpr int FUSED_RANK_MAX_WORDS = 2048;
 
 // Bytes of the ranked bin at the start of a raster CTA's shared memory,
 // rounded up so the staging area after it starts on a 32-byte boundary.
@@ -170,8 +174,11 @@ struct Stage {
     // one 16-byte group, read with one vector load per visit
     unsigned bb;         // pixel bbox in the tile as byte bounds (pack_bb)
     float es, et, ez;    // FP32 form: error bounds of the FP32 s, t and depth over the tile
-    T nz;                // facet normal in view coordinates: (p2.z, p2.w, nz), views without smoothing
-    T q[9];              // body-frame vertex normals of the three corners (smoothing)
+    T nz;                // FP64 form: facet normal in view coordinates (p2.z, p2.w, nz), views without smoothing
+    // smoothing: FP64 form, the body-frame vertex normals of the three
+    // corners; FP32 form, the view-z component of the interpolated normal
+    // as r0 + s r1 + t r2 (its sign decides whether cos(e) changes)
+    T q[sizeof(T) == 8 ? 9 : 3];
     int wmask, f;
 };
 static_assert(offsetof(Stage<float>, bb) % 16 == 0 && offsetof(Stage<double>, bb) % 16 == 0,
@@ -261,9 +268,24 @@ __device__ void stage_fill(const RasterArgs &a, const FrameGeom &g, int f, Stage
     s.f = f;
     if (g.smooth) {
         double4 q0 = a.vn[c.x], q1 = a.vn[c.y], q2 = a.vn[c.z];
-        s.q[0] = (T)q0.x; s.q[1] = (T)q0.y; s.q[2] = (T)q0.z;
-        s.q[3] = (T)q1.x; s.q[4] = (T)q1.y; s.q[5] = (T)q1.z;
-        s.q[6] = (T)q2.x; s.q[7] = (T)q2.y; s.q[8] = (T)q2.z;
+        if constexpr (sizeof(T) == 8) {
+            s.q[0] = (T)q0.x; s.q[1] = (T)q0.y; s.q[2] = (T)q0.z;
+            s.q[3] = (T)q1.x; s.q[4] = (T)q1.y; s.q[5] = (T)q1.z;
+            s.q[6] = (T)q2.x; s.q[7] = (T)q2.y; s.q[8] = (T)q2.z;
+        } else {
+            // the interpolated normal is linear in (s, t), so is its view-z
+            // component: the corners' view-z components in FP64, rounded once
+            const double z0 = g.oa[6] * q0.x + g.oa[7] * q0.y + g.oa[8] * q0.z;
+            const double z1 = g.oa[6] * q1.x + g.oa[7] * q1.y + g.oa[8] * q1.z;
+            const double z2 = g.oa[6] * q2.x + g.oa[7] * q2.y + g.oa[8] * q2.z;
+            s.q[0] = (T)z0; s.q[1] = (T)(z1 - z0); s.q[2] = (T)(z2 - z1);
+        }
+    } else if constexpr (sizeof(T) == 4) {
+        // the FP32 form takes the good facet's normal after the replay
+        // (good_normal_f32)
+        s.p2 = vec4<T>(E, F, (T)0, (T)0);
+        s.nz = (T)0;
+        return;
     } else {
         double4 nb = a.fn[f];
         double nn[3];
@@ -807,13 +829,35 @@ static __device__ void lc_cos64(const RasterArgs &a, const FrameGeom &g, int gf,
     }
 }
 
-// The first smoothed-normal component of a good winner, or (FP32 form,
-// lightcurve views: lcv) the winner's facet index in its bits.
-template <typename T>
-__device__ inline T good_tag(bool lcv, int f, T v)
+// FP32 form: the normal of a pixel's good facet gf at its barycentric
+// coordinates (sv, tv) of that visit: the interpolated body-frame vertex
+// normal with the raster's rounded corner normals (smoothing), or the facet
+// normal in view coordinates as staging rounds it. The replay keeps only
+// (gf, sv, tv) per pixel, so a visit costs two multiply-adds for the sign.
+__device__ inline void good_normal_f32(const RasterArgs &a, const FrameGeom &g, int gf, float sv, float tv,
+                                       bool smooth, float &m0, float &m1, float &m2)
 {
-    if constexpr (sizeof(T) == 4) return lcv ? __int_as_float(f) : v;
-    else return v;
+    if (smooth) {
+        const int4 c = a.fvi[gf];
+        const double4 q0 = a.vn[c.x], q1 = a.vn[c.y], q2 = a.vn[c.z];
+        const float ax = (float)q0.x, ay = (float)q0.y, az = (float)q0.z;
+        const float bx = (float)q1.x, by = (float)q1.y, bz = (float)q1.z;
+        const float cx = (float)q2.x, cy = (float)q2.y, cz = (float)q2.z;
+        m0 = ax + sv * (bx - ax) + tv * (cx - bx);
+        m1 = ay + sv * (by - ay) + tv * (cy - by);
+        m2 = az + sv * (bz - az) + tv * (cz - bz);
+    } else {
+        const double4 nb = a.fn[gf];
+        double nn[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            nn[r] = 0.0;
+            nn[r] += g.oa[3 * r + 0] * nb.x;
+            nn[r] += g.oa[3 * r + 1] * nb.y;
+            nn[r] += g.oa[3 * r + 2] * nb.z;
+        }
+        m0 = (float)nn[0]; m1 = (float)nn[1]; m2 = (float)nn[2];
+    }
 }
 
 // FP32 form, rare path: posvis at one pixel by the FP64 form's rules (the
@@ -895,6 +939,18 @@ __device__ inline unsigned long long warp_kmax(unsigned long long k)
     return ((unsigned long long)hi << 32) | lo;
 }
 
+// Bytes of the staging area after the ranked bin (32-byte multiple): the
+// staged facets, or while a bin is ranked the unfused path's bitmap, prefix
+// counts and raw bin. The fused path's bitmap follows it.
+template <typename T>
+__host__ __device__ inline size_t raster_stage_bytes(int cap, int nf)
+{
+    const size_t nw = ((size_t)nf + 31) / 32;
+    const size_t scratch = (nw <= (size_t)BITMAP_MAX_WORDS ? 8 * nw : 0) + (size_t)cap * sizeof(int2);
+    const size_t st = (size_t)STAGE_FACETS * sizeof(Stage<T>);
+    return ((st > scratch ? st : scratch) + 31) & ~(size_t)31;
+}
+
 // The tile raster. EXACT (FP32 form, lightcurve views): a pixel with a
 // decision within FP32 error is redone by the FP64 form's rules, so facet
 // assignment, depth and the shadow test's inputs are the FP64 form's;
@@ -914,6 +970,7 @@ k_raster(RasterArgs a)
     __shared__ int s_red[RASTER_THREADS / 32][4];
     __shared__ unsigned long long s_redk[RASTER_THREADS / 32][4];
     __shared__ int s_scan[RASTER_THREADS / 32];
+    __shared__ unsigned char s_perm[STAGE_FACETS];
     __shared__ double s_pz[TILE_PIX];
     __shared__ T s_pc[TILE_PIX];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -957,6 +1014,9 @@ k_raster(RasterArgs a)
         bool amb = false;   // FP32 form: a decision within FP32 error (pixel_posvis64 redoes it)
         bool good = false;
         T gm0 = 0, gm1 = 0, gm2 = 0;
+        int gfac = -1;             // FP32 form: the good facet and its (s, t) at this pixel
+        float gsv = 0.0f, gtv = 0.0f;
+        bool gready = false;       // FP32 form: gm0..2 already set (the FP64 redo)
         const bool smooth = g.smooth != 0;
         const bool bistatic_obs = (g.kind == VIEW_LC_OBS);
         // FP32 form, lightcurve views (their own launch, LCV): the good
@@ -1029,36 +1089,107 @@ k_raster(RasterArgs a)
             // (posvis.c:265). Its sign is that of the view-z component before
             // normalization, so a win records the body-frame interpolated
             // normal and the last qualifying one is normalized once, below.
-            if (smooth) {
+            if constexpr (sizeof(T) == 4) {
+                // FP32: the sign of the normal's view-z component from the
+                // staged linear form (the coefficients' rounding, the s and t
+                // errors times coefficients below 2, and two multiply-adds
+                // stay inside the bound); the normal itself is formed once,
+                // after the replay, from (facet, s, t)
+                if (smooth) {
+                    const T r2 = s.q[0] + sv * s.q[1] + tv * s.q[2];
+                    if constexpr (EXACT) amb = amb || (fabsf(r2) <= 4 * (s.es + s.et) + 3e-6f);
+                    if (r2 > (T)0) { good = true; gfac = s.f; gsv = sv; gtv = tv; }
+                } else {
+                    good = true; gfac = s.f;
+                }
+            } else if (smooth) {
                 const T m0 = s.q[0] + sv * (s.q[3] - s.q[0]) + tv * (s.q[6] - s.q[3]);
                 const T m1 = s.q[1] + sv * (s.q[4] - s.q[1]) + tv * (s.q[7] - s.q[4]);
                 const T m2 = s.q[2] + sv * (s.q[5] - s.q[2]) + tv * (s.q[8] - s.q[5]);
                 T r2 = 0;
                 r2 += oa6 * m0; r2 += oa7 * m1; r2 += oa8 * m2;
-                if constexpr (sizeof(T) == 4 && EXACT)     // the sign of r2 within FP32 error
-                    amb = amb || (fabsf(r2) <= 4 * (s.es + s.et) + 1e-6f * (fabsf(m0) + fabsf(m1) + fabsf(m2)));
-                if (r2 > (T)0) { good = true; gm0 = good_tag<T>(lcv, s.f, m0); gm1 = m1; gm2 = m2; }
+                if (r2 > (T)0) { good = true; gm0 = m0; gm1 = m1; gm2 = m2; }
             } else {
-                good = true; gm0 = good_tag<T>(lcv, s.f, p2.z); gm1 = p2.w; gm2 = s.nz;
+                good = true; gm0 = p2.z; gm1 = p2.w; gm2 = s.nz;
             }
         };
         // Each warp walks only the staged facets whose bbox meets its block,
         // in staging (= facet index) order.
-        auto replay = [&](int nst) {
+        // order: the staged slots in facet-index order (fused path), or
+        // null when the slots are already in that order
+        auto replay = [&](int nst, const unsigned char *order) {
             for (int base = 0; base < nst; base += 32) {
                 const int k = base + lane;
-                const bool hit = (k < nst) && ((st[k].wmask >> wid) & 1);
+                const int slot = (k < nst) ? (order ? (int)order[k] : k) : 0;
+                const bool hit = (k < nst) && ((st[slot].wmask >> wid) & 1);
                 unsigned m = __ballot_sync(0xffffffffu, hit);
                 while (m) {
                     const int b = __ffs(m) - 1;
                     m &= m - 1;
-                    visit(st[base + b]);
+                    visit(st[__shfl_sync(0xffffffffu, slot, b)]);
                 }
             }
         };
 
         if (count > 0 && count <= a.cap) {
             const int2 *bin = a.bin_ids + (size_t)(g.tile_base + tile) * a.cap;
+            const int nw = (a.nf + 31) >> 5;
+            if (count <= STAGE_FACETS && nw <= FUSED_RANK_MAX_WORDS) {
+            // Fused rank and staging (a bin that fits one staging pass): each
+            // of the first `count` threads loads one bin entry, marks its
+            // facet in a bitmap of the bin's facets and stages the facet in
+            // its own slot, so the staging loads overlap the marking; the
+            // bitmap's prefix counts then give each facet its rank (the
+            // number of the bin's facets below it), and the replay walks the
+            // slots in rank order, which is facet-index order.
+            unsigned *W = reinterpret_cast<unsigned *>(smem + raster_ids_bytes(a.cap) +
+                                                       raster_stage_bytes<T>(a.cap, a.nf));
+            int *P = reinterpret_cast<int *>(W + nw);
+            for (int w = tid; w < nw; w += RASTER_THREADS) W[w] = 0u;
+            __syncthreads();
+            int2 e = make_int2(0, 0);
+            if (tid < count) {
+                e = bin[tid];
+                atomicOr(&W[e.x >> 5], 1u << (e.x & 31));
+                Stage<T> sf;
+                const int bb = e.y;
+                sf.bb = pack_bb(bb & 15, (bb >> 4) & 15, (bb >> 8) & 15, (bb >> 12) & 15);
+                sf.wmask = warp_mask_of(bb & 15, (bb >> 4) & 15, (bb >> 8) & 15, (bb >> 12) & 15);
+                stage_fill<T>(a, g, e.x, sf, ox, oy);
+                st[tid] = sf;
+            }
+            __syncthreads();
+            // P[w]: the set bits of the words before w within the owning
+            // warp's words (each thread owns a run of wpt words); s_scan:
+            // the warps' totals
+            const int wpt = (nw + RASTER_THREADS - 1) / RASTER_THREADS;
+            const int w0 = min(tid * wpt, nw), w1 = min(w0 + wpt, nw);
+            int run = 0;
+            for (int w = w0; w < w1; w++) run += __popc(W[w]);
+            int inc = run;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += t;
+            }
+            if (lane == 31) s_scan[wid] = inc;
+            int before = inc - run;
+            for (int w = w0; w < w1; w++) {
+                P[w] = before;
+                before += __popc(W[w]);
+            }
+            __syncthreads();
+            if (tid < count) {
+                const int w = e.x >> 5;
+                const int owner = (w / wpt) >> 5;
+                int r = P[w] + __popc(W[w] & ((1u << (e.x & 31)) - 1u));
+                for (int ww = 0; ww < owner; ww++) r += s_scan[ww];
+                ids[r] = e;
+                s_perm[r] = (unsigned char)tid;
+            }
+            __syncthreads();
+            replay(count, s_perm);
+            } else {
             // The bin in facet-index order (posvis walks facets in index
             // order). A bin's facets are distinct, so a facet's rank is the
             // number of set bits below it in a bitmap of the bin's facets:
@@ -1066,7 +1197,6 @@ k_raster(RasterArgs a)
             // counts and the raw bin live in the staging area, idle until
             // staging starts; models too large for a bitmap rank by
             // comparisons.
-            const int nw = (a.nf + 31) >> 5;
             if (nw <= BITMAP_MAX_WORDS) {
                 unsigned *W = reinterpret_cast<unsigned *>(st);
                 int *P = reinterpret_cast<int *>(W + nw);
@@ -1129,8 +1259,9 @@ k_raster(RasterArgs a)
                     st[tid] = sf;
                 }
                 __syncthreads();
-                replay(nst);
+                replay(nst, nullptr);
                 __syncthreads();
+            }
             }
         } else if (count > a.cap) {
             // Bin overflow: stream every facet of the model in index order,
@@ -1150,7 +1281,7 @@ k_raster(RasterArgs a)
                 }
                 if (ok) st[before + __popc(bal & ((1u << lane) - 1u))] = sf;
                 __syncthreads();
-                replay(total);
+                replay(total, nullptr);
                 __syncthreads();
             }
         }
@@ -1168,15 +1299,19 @@ k_raster(RasterArgs a)
                                      &good, gmv, &gfv);
                 zz = (float)zw;
                 zlo = (float)(zw - (double)zz);
-                gm0 = good_tag<T>(lcv, gfv, gmv[0]); gm1 = gmv[1]; gm2 = gmv[2];
+                gfac = gfv; gm0 = gmv[0]; gm1 = gmv[1]; gm2 = gmv[2];
+                gready = true;
             }
+        }
+        if constexpr (sizeof(T) == 4) {
+            if (good && !lcv && !gready) good_normal_f32(a, g, gfac, gsv, gtv, smooth, gm0, gm1, gm2);
         }
 
         // cos(e) / cos(i) of the last winner whose smoothed normal faced the
         // viewer: cotrans + normalize (posvis.c:250-274), once per pixel
         double ce64 = 0.0, ci64 = 0.0;      // lcv: the FP64 cosines
         if (good && lcv) {
-            lc_cos64(a, g, __float_as_int((float)gm0), (double)pi * g.kmpp, (double)pj * g.kmpp, smooth,
+            lc_cos64(a, g, gfac, (double)pi * g.kmpp, (double)pj * g.kmpp, smooth,
                      bistatic_obs, &ce64, &ci64);
             cosa = (T)ce64;
             cosb = (T)ci64;
@@ -1405,6 +1540,9 @@ k_raster_w(RasterArgs a)
         T zze = 0, zlo = 0;
         bool amb = false, good = false;
         T gm0 = 0, gm1 = 0, gm2 = 0;
+        int gfac = -1;
+        float gsv = 0.0f, gtv = 0.0f;
+        bool gready = false;
         const bool smooth = g.smooth != 0;
         const bool bistatic_obs = (g.kind == VIEW_LC_OBS);
         const T oa6 = (T)g.oa[6], oa7 = (T)g.oa[7], oa8 = (T)g.oa[8];
@@ -1454,14 +1592,21 @@ k_raster_w(RasterArgs a)
                 const float bv = z - p2.y;
                 zlo = ((p2.y - (z - bv)) + (zr - bv)) + p2.x;
             }
-            if (smooth) {
+            if constexpr (sizeof(T) == 4) {
+                // FP32: the sign from the staged linear form (as k_raster)
+                if (smooth) {
+                    const T r2 = s.q[0] + sv * s.q[1] + tv * s.q[2];
+                    if constexpr (EXACT) amb = amb || (fabsf(r2) <= 4 * (s.es + s.et) + 3e-6f);
+                    if (r2 > (T)0) { good = true; gfac = s.f; gsv = sv; gtv = tv; }
+                } else {
+                    good = true; gfac = s.f;
+                }
+            } else if (smooth) {
                 const T m0 = s.q[0] + sv * (s.q[3] - s.q[0]) + tv * (s.q[6] - s.q[3]);
                 const T m1 = s.q[1] + sv * (s.q[4] - s.q[1]) + tv * (s.q[7] - s.q[4]);
                 const T m2 = s.q[2] + sv * (s.q[5] - s.q[2]) + tv * (s.q[8] - s.q[5]);
                 T r2 = 0;
                 r2 += oa6 * m0; r2 += oa7 * m1; r2 += oa8 * m2;
-                if constexpr (sizeof(T) == 4 && EXACT)
-                    amb = amb || (fabsf(r2) <= 4 * (s.es + s.et) + 1e-6f * (fabsf(m0) + fabsf(m1) + fabsf(m2)));
                 if (r2 > (T)0) { good = true; gm0 = m0; gm1 = m1; gm2 = m2; }
             } else {
                 good = true; gm0 = p2.z; gm1 = p2.w; gm2 = s.nz;
@@ -1556,8 +1701,12 @@ k_raster_w(RasterArgs a)
                                      gmv, &gfv);
                 zz = (float)zw;
                 zlo = (float)(zw - (double)zz);
-                gm0 = gmv[0]; gm1 = gmv[1]; gm2 = gmv[2];
+                gfac = gfv; gm0 = gmv[0]; gm1 = gmv[1]; gm2 = gmv[2];
+                gready = true;
             }
+        }
+        if constexpr (sizeof(T) == 4) {
+            if (good && !gready) good_normal_f32(a, g, gfac, gsv, gtv, smooth, gm0, gm1, gm2);
         }
 
         if (good) {
@@ -1676,8 +1825,8 @@ template <typename T>
 inline size_t raster_smem_bytes(int cap, int nf)
 {
     const size_t nw = ((size_t)nf + 31) / 32;
-    const size_t scratch = (nw <= (size_t)BITMAP_MAX_WORDS ? 8 * nw : 0) + (size_t)cap * sizeof(int2);
-    return raster_ids_bytes(cap) + std::max((size_t)STAGE_FACETS * sizeof(Stage<T>), scratch);
+    const size_t fused = nw <= (size_t)FUSED_RANK_MAX_WORDS ? 8 * nw : 0;
+    return raster_ids_bytes(cap) + raster_stage_bytes<T>(cap, nf) + fused;
 }
 
 // Called once per device before any launch (not inside stream capture).
