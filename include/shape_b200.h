@@ -259,7 +259,12 @@ int shape_engine_set_point_view(shape_engine *e, int point, const double ae[9], 
  * (chi2/dof + the penalty sum) times the bad-model factors, and bestfit
  * minimises that. The model's moments and its edge and vertex sums are
  * reduced on the device after each evaluation (two more launches and a
- * 128-byte copy), and the penalties follow from them on the host. The
+ * small copy), and the penalties follow from them on the host. A model of
+ * several components first gets check_surface's active flags
+ * (src/shape/realize_mod.c:572-756; one more launch): vertices, facets
+ * (by their centroids) and edges inside another component are left out of
+ * the moments, the edge terms and the vertex deviations, as
+ * compute_moments and penalties() leave them out. The
  * shape penalties need a closed surface. INERTIADEV, NONPA and IMPULSE need
  * the spin model. The photometric penalties, MAXELLIPDEV, NONCOSINE and
  * BIFURCATION return SHAPE_E_UNSUPPORTED. n = 0 removes the penalties.
@@ -268,6 +273,11 @@ int shape_engine_set_penalties(shape_engine *e, int n, const int *type, const do
 /* Each penalty's value after its weight's sign rule (par->pen.base) at the
  * last evaluation, for up to max penalties; returns the penalty count. */
 int shape_engine_get_penalties(shape_engine *e, double *base, int max);
+/* check_surface's flags at the last evaluation with penalties (1: active,
+ * 0: inside another component), nv vertices and nf facets in model order;
+ * all 1 for a model of one component (src/shape/realize_mod.c:582-594).
+ * SHAPE_E_STATE before such an evaluation. */
+int shape_engine_get_active(shape_engine *e, unsigned char *vertex_act, unsigned char *facet_act);
 
 /* The spin model of the engine's views, for spin fits (realize_spin,
  * src/shape/realize_spin.c:41-285): the spin state; each dataset's angle and

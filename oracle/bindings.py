@@ -240,6 +240,7 @@ class Reference:
         L.ref_evaluate_mt.restype = C.c_double
         L.ref_evaluate_mt.argtypes = [P(C.c_void_p), C.c_int]
         L.ref_get_realized.argtypes = [C.c_void_p, cd.dptr, cd.dptr, cd.dptr, cd.dptr]
+        L.ref_get_active.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_get_flags.argtypes = [C.c_void_p, cd.dptr]
         L.ref_penalties.argtypes = [C.c_void_p, C.c_int, cd.iptr, cd.dptr, P(cd.SpinState), cd.dptr, cd.dptr,
                                     cd.dptr]
@@ -407,6 +408,14 @@ class RefSession:
                                    cd.as_dptr(ao) if ao is not None else None,
                                    cd.as_dptr(oo) if oo is not None else None, cd.as_dptr(base))
         return tot, base[:n].copy()
+
+    def active(self):
+        """check_surface's (vertex, facet) act flags after the last realize_mod."""
+        m = self.model
+        v = np.zeros(m.nv, dtype=np.uint8)
+        f = np.zeros(m.nf, dtype=np.uint8)
+        self.L.ref_get_active(self.h, v.ctypes.data_as(C.c_void_p), f.ctypes.data_as(C.c_void_p))
+        return v, f
 
     def realized(self):
         m = self.model

@@ -778,8 +778,10 @@ double ref_penalties(void *h, int n, const int *type, const double *weight, cons
                      const double *angleoff, const double *omegaoff, double *base)
 {
     ref_session *S = h;
-    struct vertices_t *real = &S->mod.shape.comp[0].real;
-    if (!real->s) setupsides(real);
+    for (int c = 0; c < S->mod.shape.ncomp; c++) {
+        struct vertices_t *real = &S->mod.shape.comp[c].real;
+        if (!real->s) setupsides(real);
+    }
     if (sp) {
         S->mod.spin.n_impulse = sp->n_impulse;
         for (int j = 0; j < 3; j++) S->mod.spin.inertia[j].val = sp->inertia[j];
@@ -811,6 +813,22 @@ double ref_penalties(void *h, int n, const int *type, const double *weight, cons
     par->pen.type = NULL;
     par->pen.weight = par->pen.base = NULL;
     return sum;
+}
+
+
+/* The act flags realize_mod's check_surface left (src/shape/realize_mod.c:
+ * 572-756), model-wide: vertices, then facets, components back to back. */
+void ref_get_active(void *h, unsigned char *vact, unsigned char *fact)
+{
+    ref_session *S = h;
+    int v0 = 0, f0 = 0;
+    for (int c = 0; c < S->mod.shape.ncomp; c++) {
+        const struct vertices_t *real = &S->mod.shape.comp[c].real;
+        for (int i = 0; i < real->nv; i++) vact[v0 + i] = (unsigned char)real->v[i].act;
+        for (int f = 0; f < real->nf; f++) fact[f0 + f] = (unsigned char)real->f[f].act;
+        v0 += real->nv;
+        f0 += real->nf;
+    }
 }
 
 

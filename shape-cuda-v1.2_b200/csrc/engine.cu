@@ -90,6 +90,7 @@ int EngineImpl::finalize()
     for (int f = 0; f < 3; f++) tuned[f] = 0;
     d_work_sorted = nullptr;
     d_sides = nullptr; d_msum_part = d_msum = nullptr;
+    d_side_v2 = nullptr; d_comp_facets = nullptr; d_act_v = d_act_f = nullptr; d_surf_err = nullptr;
     cap = fixed_cap > 0 ? fixed_cap : 512;
     geoms.clear(); fh.clear(); work.clear(); view_work0.clear(); view_nwork.clear();
     chi2_items.clear(); frame_view.clear(); dop_extra.clear(); set_delpp.clear(); set_doppp.clear();
@@ -715,8 +716,6 @@ int EngineImpl::set_penalties(int n, const int *type, const double *weight)
 // facets) and the device buffers of the model sums, built on first use.
 int EngineImpl::prepare_penalties()
 {
-    if (ncomp > 1)
-        return set_err(SHAPE_E_UNSUPPORTED, "penalties: models of several components (check_surface's active flags)");
     for (int t : pen_type)
         if (pen_needs_spin(t) && !have_spin)
             return set_err(SHAPE_E_STATE, "penalties: inertiadev, nonpa and impulse need the spin model");
@@ -733,14 +732,34 @@ int EngineImpl::prepare_penalties()
             return x.key != y.key ? x.key < y.key : x.f < y.f;
         });
         std::vector<int4> sides;
+        std::vector<int> side_v2;
         for (size_t k = 0; k < hs.size(); k += 2) {
             if (k + 1 >= hs.size() || hs[k + 1].key != hs[k].key || (k + 2 < hs.size() && hs[k + 2].key == hs[k].key))
                 return set_err(SHAPE_E_ARG, "penalties: the model is not a closed surface (an edge without two facets)");
             const Half &h1 = hs[k];
             sides.push_back(make_int4(fv[3 * h1.f + h1.j], fv[3 * h1.f + (h1.j + 2) % 3], h1.f, hs[k + 1].f));
+            side_v2.push_back(fv[3 * h1.f + (h1.j + 1) % 3]);
         }
         nsides = (int)sides.size();
         int rc;
+        if (ncomp > 1) {
+            // check_surface's inputs and flags: each component's facet range
+            // (components listed back to back), the edges' other ends
+            std::vector<int2> cf((size_t)ncomp, make_int2(0, 0));
+            for (int f = 0; f < nf; f++) {
+                const int c = vcomp[fv[3 * f]];
+                if (cf[c].y == 0) cf[c].x = f;
+                cf[c].y++;
+            }
+            if ((rc = mem.alloc(&d_comp_facets, cf.size())) != SHAPE_OK) return rc;
+            if ((rc = mem.alloc(&d_side_v2, side_v2.size())) != SHAPE_OK) return rc;
+            if ((rc = mem.alloc(&d_act_v, (size_t)nv)) != SHAPE_OK) return rc;
+            if ((rc = mem.alloc(&d_act_f, (size_t)nf)) != SHAPE_OK) return rc;
+            if ((rc = mem.alloc(&d_surf_err, 1)) != SHAPE_OK) return rc;
+            CK(cudaMemcpyAsync(d_comp_facets, cf.data(), sizeof(int2) * cf.size(), cudaMemcpyHostToDevice, stream));
+            CK(cudaMemcpyAsync(d_side_v2, side_v2.data(), sizeof(int) * side_v2.size(), cudaMemcpyHostToDevice,
+                               stream));
+        }
         if ((rc = mem.alloc(&d_sides, sides.size())) != SHAPE_OK) return rc;
         if ((rc = mem.alloc(&d_msum_part, (size_t)model_sums_blocks() * MSUM_N)) != SHAPE_OK) return rc;
         if ((rc = mem.alloc(&d_msum, (size_t)MSUM_N)) != SHAPE_OK) return rc;
@@ -755,11 +774,22 @@ int EngineImpl::prepare_penalties()
 int EngineImpl::enqueue_model_sums()
 {
     ModelSumArgs a;
+    memset(&a, 0, sizeof a);
     a.m = md;
     a.sides = d_sides;
     a.nsides = nsides;
+    a.ncomp = ncomp;
     a.part = d_msum_part;
     a.out = d_msum;
+    if (ncomp > 1) {
+        a.side_v2 = d_side_v2;
+        a.comp_facets = d_comp_facets;
+        a.act_v = d_act_v;
+        a.act_f = d_act_f;
+        a.surf_err = d_surf_err;
+        CK(cudaMemsetAsync(d_surf_err, 0, sizeof(int), stream));
+        launch_check_surface(a, stream);
+    }
     launch_model_sums(a, stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h_msum, d_msum, sizeof(double) * MSUM_N, cudaMemcpyDeviceToHost, stream));
@@ -843,9 +873,9 @@ double EngineImpl::penalty_sum(const double *ms)
     for (size_t i = 0; i < pen_type.size(); i++) {
         double pen = 0.0;
         switch (pen_type[i]) {
-        case SHAPE_PEN_NONSMOOTH: pen = ms[MSUM_NONSMOOTH] / nsides; break;
-        case SHAPE_PEN_CONCAVITY: pen = ms[MSUM_CONCAVITY] / nsides; break;
-        case SHAPE_PEN_RDEV: pen = ms[MSUM_RDEV] / (r_eff * r_eff) / nv; break;
+        case SHAPE_PEN_NONSMOOTH: pen = ms[MSUM_NONSMOOTH] / ms[MSUM_NSIDES]; break;
+        case SHAPE_PEN_CONCAVITY: pen = ms[MSUM_CONCAVITY] / ms[MSUM_NSIDES]; break;
+        case SHAPE_PEN_RDEV: pen = ms[MSUM_RDEV] / (r_eff * r_eff) / ms[MSUM_NVERT]; break;
         case SHAPE_PEN_MAXRDEV: pen = ms[MSUM_RDEV_MAX] / (r_eff * r_eff); break;
         case SHAPE_PEN_VOLUME: pen = V; break;
         case SHAPE_PEN_COMDEV:
@@ -1189,7 +1219,7 @@ int EngineImpl::kernels_per_eval(int form) const
     }
     n += lcdev.empty() ? 0 : 1;          // lightcurve finalize
     n += dop_frames.empty() ? 0 : 1;     // Doppler overflow spectra
-    n += pen_type.empty() ? 0 : 2;       // model sums for the penalties
+    n += pen_type.empty() ? 0 : (ncomp > 1 ? 3 : 2);   // model sums (and check_surface) for the penalties
     return n + 1;                        // finalize + summary (with the chi-square partials when fused)
 }
 
@@ -1372,6 +1402,8 @@ int EngineImpl::finish(shape_eval_summary *out)
     if (!pen_type.empty()) {
         // objective() (src/shape/bestfit.c:789-866): reduced chi-square plus
         // penalties, then the bad-model factors
+        if (h_msum[MSUM_SURF_ERR] != 0.0)
+            return set_err(SHAPE_E_UNSUPPORTED, "check_surface: a ray crossed more than 100 facet edges");
         sm.penalties = penalty_sum(h_msum);
         double err = sm.chi2 / sm.dof + sm.penalties;
         if (pending_baddiam) err *= bad_objfactor * exp(pending_bdl);
@@ -1982,6 +2014,25 @@ int shape_engine_get_penalties(shape_engine *h, double *base, int max)
     const int n = std::min<int>(max, (int)E.pen_base.size());
     for (int i = 0; i < n; i++) base[i] = E.pen_base[i];
     return (int)E.pen_base.size();
+}
+
+int shape_engine_get_active(shape_engine *h, unsigned char *vertex_act, unsigned char *facet_act)
+{
+    if (!h || !vertex_act || !facet_act) return shape::set_err(SHAPE_E_ARG, "get_active: null argument");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0 || E.pen_type.empty() || !E.d_sides)
+        return shape::set_err(SHAPE_E_STATE, "get_active: no evaluation with penalties yet");
+    if (E.ncomp == 1) {
+        memset(vertex_act, 1, (size_t)E.nv);
+        memset(facet_act, 1, (size_t)E.nf);
+        return SHAPE_OK;
+    }
+    cudaSetDevice(E.device);
+    cudaError_t e = cudaStreamSynchronize(E.stream);
+    if (e == cudaSuccess) e = cudaMemcpy(vertex_act, E.d_act_v, (size_t)E.nv, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(facet_act, E.d_act_f, (size_t)E.nf, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, std::string("get_active: ") + cudaGetErrorString(e));
+    return SHAPE_OK;
 }
 
 int shape_engine_set_fp32_exact(shape_engine *h, int exact)

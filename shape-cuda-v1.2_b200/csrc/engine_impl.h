@@ -176,6 +176,10 @@ struct EngineImpl {
     std::vector<double> pen_weight, pen_base;
     int nsides = 0;                         // edges of the closed surface
     int4 *d_sides = nullptr;                // (v1, f1's third vertex, f1, f2); built on first use
+    int *d_side_v2 = nullptr;               // several components: the edges' other ends
+    int2 *d_comp_facets = nullptr;          // several components: (first facet, facets) each
+    unsigned char *d_act_v = nullptr, *d_act_f = nullptr;   // check_surface's active flags
+    int *d_surf_err = nullptr;
     double *d_msum_part = nullptr, *d_msum = nullptr;
     double *h_msum = nullptr;               // pinned [MSUM_N]
     int set_penalties(int n, const int *type, const double *weight);

@@ -101,19 +101,29 @@ void launch_realize_vf(const ModelDev &m, cudaStream_t s);   // vertices, facet 
 void launch_realize_vn(const ModelDev &m, cudaStream_t s);   // vertex normals (after _vf)
 
 // Model sums for the penalty terms (penalty.cu), in this order.
+// The sums run over the model's active facets, edges and vertices: all of
+// them for one component; for several, those check_surface leaves active
+// (not inside another component), with the counts of active edges and
+// vertices and check_surface's error flag (an edge-crossing list overflow).
 enum {
     MSUM_VOLUME, MSUM_COM, MSUM_IXX = MSUM_COM + 3, MSUM_IYY, MSUM_IZZ, MSUM_IXY, MSUM_IXZ, MSUM_IYZ,
-    MSUM_NONSMOOTH, MSUM_CONCAVITY, MSUM_RDEV, MSUM_RDEV_MAX, MSUM_N
+    MSUM_NONSMOOTH, MSUM_CONCAVITY, MSUM_RDEV, MSUM_RDEV_MAX, MSUM_NSIDES, MSUM_NVERT, MSUM_SURF_ERR, MSUM_N
 };
 struct ModelSumArgs {
-    ModelDev m;                 // realized model (vx, fn, fv, u, r, scale)
+    ModelDev m;                 // realized model (vx, fn, fv, u, r, scale, vcomp)
     const int4 *sides;          // edges: (end vertex v1, f1's third vertex, f1, f2)
+    const int *side_v2;         // the edges' other end vertices (several components)
     int nsides;
+    int ncomp;
+    const int2 *comp_facets;    // [ncomp] (first facet, facets) of each component
+    unsigned char *act_v, *act_f;   // check_surface's flags (null: one component, all active)
+    int *surf_err;              // check_surface's error flag (zeroed before it runs)
     double *part;               // [model_sums_blocks() * MSUM_N]
     double *out;                // [MSUM_N]
 };
 int model_sums_blocks();
 void launch_model_sums(const ModelSumArgs &a, cudaStream_t s);   // two launches
+void launch_check_surface(const ModelSumArgs &a, cudaStream_t s);   // several components: the active flags
 void launch_reset_state(FrameState *st, int nviews, int *bin_count, int ntiles, cudaStream_t s);
 // pdl: programmatic dependent launch (launch_k)
 void launch_xform_f64(const FrameGeom *g, int nviews, const double4 *vx, int nv, double4 *vt,

@@ -7,7 +7,10 @@
 //
 // One pass over facets, edges and vertices by a grid of fixed shape writes
 // per-block partials; a one-block kernel reduces them in a fixed order, so
-// the sums are the same on every run.
+// the sums are the same on every run. A model of several components first
+// gets check_surface's active flags (src/shape/realize_mod.c:572-756), which
+// leave the facets, edges and vertices inside another component out of
+// the sums, as compute_moments and the penalties do.
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -22,6 +25,124 @@ constexpr int MS_BLOCKS = 148;
 __device__ __forceinline__ double d3(const double4 &a, const double4 &b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
 __device__ __forceinline__ double comp(const double4 &p, int k) { return k == 0 ? p.x : (k == 1 ? p.y : p.z); }
+
+// check_surface's tolerances (src/shape/realize_mod.c:142-144): the edge
+// tolerance of the ray-facet test, the distance tolerance of an
+// intersection beyond the point and of two edge crossings being one, and
+// the edge crossings one ray may record.
+constexpr double SURF_EDGETOL = 1.0e-14;
+constexpr double SURF_RTOL = 1000 * 1.0e-14;
+constexpr int SURF_MAXEDGE = 100;
+
+// Where the ray r * u from the origin meets the plane of facet (v0, v1, v2)
+// with normal n (Badouel's projection method, as src/shape/rayfacint.c
+// states it, with the same operations): r along the ray, (s, t) in the facet
+// (v0 + s (v1 - v0) + t (v2 - v1)); true when the point lies in the facet
+// to within tol.
+__device__ bool ray_facet(const double u[3], const double4 &v0, const double4 &v1, const double4 &v2,
+                          const double4 &n, double tol, double &r, double &s, double &t)
+{
+    const double a[3] = {0.0, 0.0, 0.0};
+    const double p0[3] = {v0.x, v0.y, v0.z}, p1[3] = {v1.x, v1.y, v1.z}, p2[3] = {v2.x, v2.y, v2.z};
+    const double nn[3] = {n.x, n.y, n.z};
+    double ra0[3], r01[3], r12[3], r0p[3];
+    for (int i = 0; i < 3; i++) {
+        ra0[i] = p0[i] - a[i];
+        r01[i] = p1[i] - p0[i];
+        r12[i] = p2[i] - p1[i];
+    }
+    const double ndu = nn[0] * u[0] + nn[1] * u[1] + nn[2] * u[2];
+    if (ndu == 0.0) {
+        r = s = t = -SHAPE_HUGENUMBER;
+        return false;
+    }
+    r = (nn[0] * ra0[0] + nn[1] * ra0[1] + nn[2] * ra0[2]) / ndu;
+    for (int i = 0; i < 3; i++) r0p[i] = (a[i] + r * u[i]) - p0[i];
+    const double ax = fabs(nn[0]), ay = fabs(nn[1]), az = fabs(nn[2]);
+    int i0 = 0;
+    double mx = ax;
+    if (ay > mx) { i0 = 1; mx = ay; }
+    if (az > mx) i0 = 2;
+    const int i1 = (i0 + 1) % 3, i2 = (i1 + 1) % 3;
+    if (r01[i1] == 0.0) {
+        t = r0p[i1] / r12[i1];
+        s = (r0p[i2] - t * r12[i2]) / r01[i2];
+    } else {
+        t = (r0p[i2] * r01[i1] - r0p[i1] * r01[i2]) / (r12[i2] * r01[i1] - r12[i1] * r01[i2]);
+        s = (r0p[i1] - t * r12[i1]) / r01[i1];
+    }
+    return (s >= -tol) && (s <= 1.0 + tol) && (t >= -tol) && (t <= s + tol);
+}
+
+// check_surface for a model of several components: one thread per vertex
+// (the ray from the origin through it) and per facet (through its
+// centroid). The point is inactive when, for some other component, the ray
+// crosses that component's surface an odd number of times beyond the point;
+// crossings at a facet edge or corner are counted once per distinct
+// distance. Components are tried in the reference's order (0 or 1 first,
+// skipping the point's own), stopping at the first that encloses it.
+__global__ void __launch_bounds__(MS_THREADS) k_check_surface(ModelSumArgs a)
+{
+    const ModelDev &m = a.m;
+    const int idx = blockIdx.x * MS_THREADS + threadIdx.x;
+    if (idx >= m.nv + m.nf) return;
+    const bool isv = idx < m.nv;
+    double u[3];
+    int c;
+    if (isv) {
+        const double4 p = m.vx[idx];
+        u[0] = p.x; u[1] = p.y; u[2] = p.z;
+        c = m.vcomp[idx];
+    } else {
+        const int f = idx - m.nv;
+        const double4 p0 = m.vx[m.fv[3 * f]], p1 = m.vx[m.fv[3 * f + 1]], p2 = m.vx[m.fv[3 * f + 2]];
+        u[0] = (p0.x + p1.x + p2.x) / 3;
+        u[1] = (p0.y + p1.y + p2.y) / 3;
+        u[2] = (p0.z + p1.z + p2.z) / 3;
+        c = m.vcomp[m.fv[3 * f]];
+    }
+    double dist = 0.0;
+    dist += u[0] * u[0];
+    dist += u[1] * u[1];
+    dist += u[2] * u[2];
+    dist = sqrt(dist);
+    if (dist != 0.0)
+        for (int i = 0; i < 3; i++) u[i] /= dist;
+    double r_edge[SURF_MAXEDGE];
+    bool act = true;
+    int c2 = (c == 0) ? 1 : 0;
+    do {
+        const int2 fr = a.comp_facets[c2];
+        int nint = 0, nedge = 0;
+        for (int f2 = fr.x; f2 < fr.x + fr.y; f2++) {
+            double r, s, t;
+            if (!ray_facet(u, m.vx[m.fv[3 * f2]], m.vx[m.fv[3 * f2 + 1]], m.vx[m.fv[3 * f2 + 2]], m.fn[f2],
+                           SURF_EDGETOL, r, s, t))
+                continue;
+            if (!(r > dist + SURF_RTOL)) continue;
+            if (fabs(s) < SURF_EDGETOL || fabs(s - 1.0) < SURF_EDGETOL || fabs(t) < SURF_EDGETOL ||
+                fabs(t - s) < SURF_EDGETOL) {
+                bool fresh = true;
+                for (int k = 0; k < nedge; k++)
+                    if (fabs(r - r_edge[k]) < SURF_RTOL) fresh = false;
+                if (fresh) {
+                    if (nedge == SURF_MAXEDGE) {
+                        atomicExch(a.surf_err, 1);
+                        break;
+                    }
+                    r_edge[nedge++] = r;
+                    nint++;
+                }
+            } else {
+                nint++;
+            }
+        }
+        if (nint % 2 == 1) act = false;
+        c2 = (c2 == c - 1) ? c2 + 2 : c2 + 1;
+    } while (act && c2 < a.ncomp);
+    if (isv) a.act_v[idx] = act ? 1 : 0;
+    else a.act_f[idx - m.nv] = act ? 1 : 0;
+}
 
 // Moments of the prism between facet (p0, p1, p2), normal n, and the
 // coordinate plane normal to axis k, projected along k, for each k in the
@@ -85,10 +206,14 @@ __global__ void __launch_bounds__(MS_THREADS) k_model_sums(ModelSumArgs a)
     const ModelDev &m = a.m;
     const int stride = gridDim.x * MS_THREADS, t0 = blockIdx.x * MS_THREADS + threadIdx.x;
     for (int f = t0; f < m.nf; f += stride)
-        facet_moments(m.vx[m.fv[3 * f]], m.vx[m.fv[3 * f + 1]], m.vx[m.fv[3 * f + 2]], m.fn[f], acc);
-    // edges (v1, v3, f1, f2): v3 is f1's vertex off the edge, v1 an end
+        if (!a.act_f || a.act_f[f])
+            facet_moments(m.vx[m.fv[3 * f]], m.vx[m.fv[3 * f + 1]], m.vx[m.fv[3 * f + 2]], m.fn[f], acc);
+    // edges (v1, v3, f1, f2): v3 is f1's vertex off the edge, v1 an end;
+    // an edge is active when both its ends are
     for (int s = t0; s < a.nsides; s += stride) {
         const int4 e = a.sides[s];
+        if (a.act_v && !(a.act_v[e.x] && a.act_v[a.side_v2[s]])) continue;
+        acc[MSUM_NSIDES] += 1.0;
         const double4 n1 = m.fn[e.z], n2 = m.fn[e.w];
         const double x = 1.0 - d3(n1, n2);
         acc[MSUM_NONSMOOTH] += x * x * x * x;
@@ -96,17 +221,22 @@ __global__ void __launch_bounds__(MS_THREADS) k_model_sums(ModelSumArgs a)
         const double4 disp = make_double4(p3.x - p1.x, p3.y - p1.y, p3.z - p1.z, 0.0);
         if (d3(disp, n2) > 0.0) acc[MSUM_CONCAVITY] += x * x;
     }
-    // vertex deviation lengths |u . scale| * r
+    // vertex deviation lengths |u . scale| * r (the vertex's component's
+    // scale factors)
     for (int v = t0; v < m.nv; v += stride) {
+        if (a.act_v && !a.act_v[v]) continue;
+        acc[MSUM_NVERT] += 1.0;
+        const double *sc = m.scale + (m.vcomp ? 3 * m.vcomp[v] : 0);
         double len = 0.0;
         for (int j = 0; j < 3; j++) {
-            const double y = m.u[3 * v + j] * m.scale[j];
+            const double y = m.u[3 * v + j] * sc[j];
             len += y * y;
         }
         const double d = sqrt(len) * m.r[v];
         acc[MSUM_RDEV] += d * d;
         acc[MSUM_RDEV_MAX] = fmax(acc[MSUM_RDEV_MAX], d * d);
     }
+    if (t0 == 0 && a.surf_err) acc[MSUM_SURF_ERR] = (double)*a.surf_err;
     block_reduce(acc, sh);
     if (threadIdx.x == 0)
         for (int q = 0; q < MSUM_N; q++) a.part[(size_t)blockIdx.x * MSUM_N + q] = acc[q];
@@ -130,6 +260,12 @@ __global__ void __launch_bounds__(MS_THREADS) k_model_sums_final(ModelSumArgs a,
 }  // namespace
 
 int model_sums_blocks() { return MS_BLOCKS; }
+
+void launch_check_surface(const ModelSumArgs &a, cudaStream_t s)
+{
+    const int n = a.m.nv + a.m.nf;
+    k_check_surface<<<(n + MS_THREADS - 1) / MS_THREADS, MS_THREADS, 0, s>>>(a);
+}
 
 void launch_model_sums(const ModelSumArgs &a, cudaStream_t s)
 {

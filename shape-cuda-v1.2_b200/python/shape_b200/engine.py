@@ -109,6 +109,7 @@ def load_library(path=LIB_PATH):
                                                cd.dptr, cd.dptr]
     L.shape_engine_get_radar_overflow.argtypes = [vp, cd.dptr, C.c_int]
     L.shape_engine_finalize.argtypes = [vp]
+    L.shape_engine_get_active.argtypes = [vp, vp, vp]
     L.shape_engine_set_scale.argtypes = [vp, C.c_int, C.c_double]
     L.shape_engine_set_vertex_r.argtypes = [vp, C.c_int, C.c_double]
     L.shape_engine_get_vertex_r.argtypes = [vp, C.c_int, P(C.c_double)]
@@ -410,6 +411,14 @@ class Engine:
         out = np.zeros(64)
         n = _chk(self.L.shape_engine_get_penalties(self.h, cd.as_dptr(out), 64))
         return out[:n].copy()
+
+    def active(self):
+        """check_surface's (vertex, facet) active flags at the last
+        evaluation with penalties."""
+        v = np.zeros(self.model.nv, dtype=np.uint8)
+        f = np.zeros(self.model.nf, dtype=np.uint8)
+        _chk(self.L.shape_engine_get_active(self.h, v.ctypes.data_as(C.c_void_p), f.ctypes.data_as(C.c_void_p)))
+        return v, f
 
     def write_fitdat(self, frame, sdev, path):
         _chk(self.L.shape_engine_write_fitdat(self.h, int(frame), float(sdev), os.fsencode(path)))

@@ -87,3 +87,42 @@ def test_penalty_errors(cuda_device):
     s = e.evaluate(eng.FORM_BATCHED_FP64)              # the engine is still usable
     assert s["penalties"] > 0.0
     e.close()
+
+
+def test_penalties_two_components(cuda_device):
+    """A model of two VERTEX components, the second mostly inside the
+    first: check_surface's active flags equal the reference's realize_mod
+    (vertices, and facets by their centroids), and every shape penalty,
+    which leaves inactive facets, edges and vertices out, matches the
+    reference's penalties() in every form."""
+    from shape_b200 import synth
+    m = synth.two_component_model()
+    m.r = np.random.default_rng(78).normal(0.0, 0.02, m.nv)
+    p = synth.eval_params()
+    ds = synth.config1_frames(2, None, p)
+    ref = Reference().session(m, p, deldops=[ds])
+    rtot, rbase = ref.penalties(SHAPE_PENS)
+    rv, rf = ref.active()
+    assert 0 < rv.sum() < m.nv and 0 < rf.sum() < m.nf, (rv.sum(), rf.sum())
+    e = eng.make_engine(m, p, deldops=[ds])
+    k0 = e.kernels_per_eval(eng.FORM_BATCHED_FP64)
+    e.set_penalties(SHAPE_PENS)
+    assert e.kernels_per_eval(eng.FORM_BATCHED_FP64) == k0 + 3
+    for form in FORMS:
+        s = e.evaluate(form)
+        gv, gf = e.active()
+        assert np.array_equal(gv, rv) and np.array_equal(gf, rf), form
+        np.testing.assert_allclose(e.penalties(), rbase, rtol=1e-9, atol=1e-14, err_msg=str(form))
+        assert abs(s["penalties"] - rtot) <= 1e-9 * rtot, (form, s["penalties"], rtot)
+    # a trial that moves the second component: the flags follow it
+    e.set_scale(3, 1.2)
+    R = Reference()
+    ref2 = R.session(m, p, deldops=[ds])
+    R.lib.ref_set_scale(ref2.h, 3, 1.2)
+    rtot2, rbase2 = ref2.penalties(SHAPE_PENS)
+    rv2, rf2 = ref2.active()
+    s = e.evaluate(eng.FORM_BATCHED_FP64)
+    gv, gf = e.active()
+    assert np.array_equal(gv, rv2) and np.array_equal(gf, rf2)
+    np.testing.assert_allclose(e.penalties(), rbase2, rtol=1e-9, atol=1e-14)
+    e.close()
