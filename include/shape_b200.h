@@ -63,6 +63,9 @@ typedef struct shape_eval_summary {
                                   (src/shape/bestfit.c:789-866) */
     double penalties;          /* the penalty sum (shape_engine_set_penalties;
                                   0 with none) */
+    double chi2_poset;         /* plane-of-sky sets' part of chi2 */
+    int badposet;              /* par->badposet */
+    double badposet_logfactor; /* par->badposet_logfactor after /= dat->dof_poset */
 } shape_eval_summary;
 
 const char *shape_last_error(void);
@@ -70,7 +73,8 @@ const char *shape_version(void);
 /* sizeof() of every struct in shape_types.h, in the order
  * model_desc, radar_law, optical_law, eval_params, deldop_frame,
  * deldop_set, lghtcrv_point, lghtcrv_set, deldop_result, eval_summary,
- * doppler_frame, doppler_set, spin_state, ephem_point;
+ * doppler_frame, doppler_set, spin_state, ephem_point, poset_frame,
+ * poset_set, poset_result;
  * lets bindings verify their layouts. Returns the number written. */
 int shape_abi_sizes(size_t *out, int max);
 
@@ -112,6 +116,25 @@ int shape_engine_add_lghtcrv_set(shape_engine *e, const shape_lghtcrv_set *set,
 int shape_engine_add_doppler_set(shape_engine *e, const shape_doppler_set *set,
                                  int nframes, const shape_doppler_frame *frames,
                                  const double *obs, const double *oneovervar);
+/* A plane-of-sky set (calc_poset, src/shape/calc_fits.c:1156-1330, and
+ * chi2_poset, src/shape/chi2.c): each frame is rendered from the observer
+ * and from the sun (shadows by posmask), its brightness per POS pixel taken
+ * by apply_photo, the brightness image resampled onto the frame's fit grid
+ * by resampim (COM offsets, north angle, interpolation mode, rebinning),
+ * checked by checkposet (badposet) and compared with the observed image
+ * under a floating calibration. obs / oneovervar: the frames' ncol x nrow
+ * images back to back (layout of shape_poset_frame). Bicubic resampling
+ * returns SHAPE_E_UNSUPPORTED. Returns the set index. */
+int shape_engine_add_poset_set(shape_engine *e, const shape_poset_set *set, int nframes,
+                               const shape_poset_frame *frames, const double *obs, const double *oneovervar);
+/* A plane-of-sky frame after the last evaluation: its fit image (ncol x
+ * nrow, the layout of obs), its sky rendering's brightness image
+ * ((2 pos_n + 1)^2, element (i, j) for i, j = -pos_n..pos_n at
+ * (i + pos_n) * (2 pos_n + 1) + (j + pos_n), as pos->b[i][j]) and its
+ * results; a NULL pointer skips that output. */
+int shape_engine_get_poset(shape_engine *e, int set, int frame, double *fit, double *brightness,
+                           shape_poset_result *result);
+
 /* Allocates device state for everything added so far. */
 int shape_engine_finalize(shape_engine *e);
 

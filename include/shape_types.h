@@ -215,6 +215,51 @@ typedef struct shape_lghtcrv_set {
     shape_optical_law law;  /* photo->optical[lghtcrv->ioptlaw] */
 } shape_lghtcrv_set;
 
+/* Plane-of-sky frame (struct posetfrm_t, src/shape/shape2.h:1303-1325) with
+ * one view: the sky rendering's POS window and view geometry, and the fit
+ * grid the rendering is resampled onto (calc_poset,
+ * src/shape/calc_fits.c:1156-1330). The observed image and its 1/variance
+ * are ncol x nrow arrays, element (i, j) (1-based column i, row j) at
+ * (i - 1) * nrow + (j - 1), as frame->obs.b[i][j]. */
+typedef struct shape_poset_frame {
+    int pos_n;              /* sky rendering: (2 pos_n + 1)^2 pixels */
+    double km_per_pixel;    /* frame->pos.km_per_pixel */
+    double ae[9], oe[9], se[9];
+    double solar_phase;     /* view[v0].solar_phase (radians) */
+    int ncol, nrow;         /* fit image (after vignetting) */
+    double fit_km_per_pixel;/* frame->fit.km_per_pixel */
+    double colcom_vig, rowcom_vig;  /* 1-based COM column and row at zero offsets */
+    double xoff, yoff;      /* frame->off[0..1].val (fit-grid pixels) */
+    double northangle;      /* radians, clockwise heading of north */
+    double weight, dof;
+} shape_poset_frame;
+
+/* resampim interpolation modes (par->poset_resample, src/util/resampim.c) */
+#define SHAPE_RESAMPLE_NONE 0
+#define SHAPE_RESAMPLE_NEAREST 1
+#define SHAPE_RESAMPLE_BILINEAR 2
+#define SHAPE_RESAMPLE_BICUBIC 3     /* not supported (SHAPE_E_UNSUPPORTED) */
+#define SHAPE_RESAMPLE_CUBICCONV 4
+
+/* Plane-of-sky set (struct poset_t, src/shape/shape2.h:1328-1341) with one
+ * view per frame; the calibration always floats (chi2_poset). */
+typedef struct shape_poset_set {
+    shape_optical_law law;  /* photo->optical[poset->ioptlaw] */
+    int resample;           /* par->poset_resample: SHAPE_RESAMPLE_* */
+    int rebin;              /* par->image_rebin */
+} shape_poset_set;
+
+/* Per-frame results of a plane-of-sky frame. */
+typedef struct shape_poset_result {
+    int outbnd;             /* 1: the observer view's posvis returned 1; 2: the sun view's; 3: both */
+    double posbnd_logsum;   /* sum over those views of dof/2 * posbnd_logfactor (calc_poset) */
+    int badposet;           /* checkposet returned 1 */
+    double badposet_logfactor;  /* checkposet's log area ratio */
+    double o2, m2, om;      /* chi-square partial sums */
+    double cal;             /* om/m2, or TINYCALFACT when om <= 0 */
+    double chi2;            /* frame chi-square */
+} shape_poset_result;
+
 /* Per-frame results of one radar frame evaluation (delay-Doppler image or
  * Doppler spectrum; a Doppler frame leaves the delay fields at their blank
  * values, and its o2 / m2 include the overflow spectrum's terms). */

@@ -241,6 +241,10 @@ class Reference:
         L.ref_evaluate_mt.argtypes = [P(C.c_void_p), C.c_int]
         L.ref_get_realized.argtypes = [C.c_void_p, cd.dptr, cd.dptr, cd.dptr, cd.dptr]
         L.ref_get_active.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_add_poset_set.argtypes = [C.c_void_p, C.POINTER(cd.PosetSet), C.c_int, C.POINTER(cd.PosetFrame),
+                                        cd.dptr, cd.dptr]
+        L.ref_get_poset_frame.argtypes = [C.c_void_p, C.c_int, C.c_int, cd.dptr, cd.dptr, cd.dptr]
+        L.ref_get_badposet.argtypes = [C.c_void_p, cd.dptr]
         L.ref_get_flags.argtypes = [C.c_void_p, cd.dptr]
         L.ref_penalties.argtypes = [C.c_void_p, C.c_int, cd.iptr, cd.dptr, P(cd.SpinState), cd.dptr, cd.dptr,
                                     cd.dptr]
@@ -286,17 +290,20 @@ class Reference:
                                     C.c_double, C.c_double, cd.dptr]
 
     def session(self, model, params, deldops=(), lghtcrvs=(), radar_law=None, optical_law=None,
-                dopplers=()):
+                dopplers=(), posets=()):
         """A reference session with the sets in the order deldops, dopplers,
-        lightcurves (all radar sets share one radar law)."""
+        lightcurves, plane-of-sky sets (all radar sets share one radar law,
+        all optical sets one optical law)."""
         d = model.desc()
-        h = self.lib.ref_new(C.byref(d), C.byref(params), len(deldops) + len(dopplers) + len(lghtcrvs))
+        h = self.lib.ref_new(C.byref(d), C.byref(params),
+                             len(deldops) + len(dopplers) + len(lghtcrvs) + len(posets))
         keep = [d]
         if deldops or dopplers:
             first = deldops[0] if deldops else dopplers[0]
             self.lib.ref_set_radar_law(h, C.byref(radar_law or first.set.law))
-        if lghtcrvs:
-            self.lib.ref_set_optical_law(h, C.byref(optical_law or lghtcrvs[0].set.law))
+        if lghtcrvs or posets:
+            law = optical_law or (lghtcrvs[0].set.law if lghtcrvs else posets[0].law)
+            self.lib.ref_set_optical_law(h, C.byref(law))
         for ds in deldops:
             if getattr(ds, "views", None):
                 arr = ds.view_array()
@@ -317,6 +324,10 @@ class Reference:
             arr = ls.point_array()
             keep.append(arr)
             self.lib.ref_add_lghtcrv_set(h, C.byref(ls.bind()), arr)
+        for ds in posets:
+            st, frames, obs, oov = ds.bind()
+            keep.extend([st, frames, obs, oov])
+            self.lib.ref_add_poset_set(h, C.byref(st), ds.nframes, frames, cd.as_dptr(obs), cd.as_dptr(oov))
         return RefSession(self, h, model, keep)
 
     def read_mod(self, path):
@@ -408,6 +419,21 @@ class RefSession:
                                    cd.as_dptr(ao) if ao is not None else None,
                                    cd.as_dptr(oo) if oo is not None else None, cd.as_dptr(base))
         return tot, base[:n].copy()
+
+    def poset_frame(self, s, f, frame):
+        """(fit [ncol, nrow], sky brightness [2n+1, 2n+1], cal, chi2) of a
+        plane-of-sky frame after evaluate(); frame: its description dict."""
+        fit = np.zeros((frame["ncol"], frame["nrow"]))
+        side = 2 * frame["pos_n"] + 1
+        b = np.zeros((side, side))
+        out = np.zeros(2)
+        self.L.ref_get_poset_frame(self.h, s, f, cd.as_dptr(fit), cd.as_dptr(b), cd.as_dptr(out))
+        return fit, b, out[0], out[1]
+
+    def badposet(self):
+        out = np.zeros(2)
+        self.L.ref_get_badposet(self.h, cd.as_dptr(out))
+        return int(out[0]), out[1]
 
     def active(self):
         """check_surface's (vertex, facet) act flags after the last realize_mod."""

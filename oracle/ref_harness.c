@@ -353,6 +353,96 @@ int ref_add_lghtcrv_set(void *h, const shape_lghtcrv_set *ls, const shape_lghtcr
     return S->dat.nsets - 1;
 }
 
+/* A plane-of-sky set (struct poset_t, src/shape/shape2.h:1290-1341) with one
+ * view per frame, as read_poset and set_up_pos leave it: the sky rendering
+ * (bistatic POS window), the observed and fit images [1..ncol][1..nrow],
+ * 1/variance, COM offsets, north angle and the floating calibration; the
+ * set's resampling mode and rebinning go to par (poset_resample,
+ * image_rebin), its law is optical law 0. Returns the set index. */
+int ref_add_poset_set(void *h, const shape_poset_set *ps, int nframes, const shape_poset_frame *frames,
+                      const double *obs, const double *oov)
+{
+    ref_session *S = h;
+    if (S->dat.nsets >= S->nsets_cap) return -1;
+    struct set_t *set = &S->dat.set[S->dat.nsets++];
+    set->type = POS;
+    struct poset_t *po = &set->desc.poset;
+    po->ioptlaw = 0;
+    po->nviews = 1;
+    po->v0 = 0;
+    po->nframes = nframes;
+    po->frame = calloc((size_t)nframes, sizeof(struct posetfrm_t));
+    S->par.poset_resample = (unsigned char)ps->resample;
+    S->par.image_rebin = (unsigned char)ps->rebin;
+    size_t off = 0;
+    double dof = 0.0;
+    for (int f = 0; f < nframes; f++) {
+        const shape_poset_frame *F = &frames[f];
+        struct posetfrm_t *fr = &po->frame[f];
+        fr->view = calloc(1, sizeof(struct posetview_t));
+        ref_copy_rm(fr->view[0].ae, F->ae);
+        ref_copy_rm(fr->view[0].oe, F->oe);
+        ref_copy_rm(fr->view[0].se, F->se);
+        fr->view[0].solar_phase = F->solar_phase;
+        fr->ncol = F->ncol;
+        fr->nrow = F->nrow;
+        fr->colcom_vig = F->colcom_vig;
+        fr->rowcom_vig = F->rowcom_vig;
+        fr->off[0].state = fr->off[1].state = 'c';
+        fr->off[0].val = F->xoff;
+        fr->off[1].val = F->yoff;
+        fr->northangle = F->northangle;
+        fr->weight = F->weight;
+        fr->dof = F->dof;
+        fr->cal.state = 'f';
+        fr->cal.val = 1.0;
+        ref_alloc_pos(&fr->pos, F->pos_n, F->km_per_pixel, 1);
+        fr->obs.b = matrix(1, F->ncol, 1, F->nrow);
+        fr->fit.b = matrix(1, F->ncol, 1, F->nrow);
+        fr->oneovervar = matrix(1, F->ncol, 1, F->nrow);
+        fr->fit.km_per_pixel = F->fit_km_per_pixel;
+        fr->obs.km_per_pixel = F->fit_km_per_pixel;
+        for (int i = 1; i <= F->ncol; i++)
+            for (int j = 1; j <= F->nrow; j++, off++) {
+                fr->obs.b[i][j] = obs[off];
+                fr->oneovervar[i][j] = oov[off];
+                fr->fit.b[i][j] = 0.0;
+            }
+        dof += F->dof;
+    }
+    po->dof = dof;
+    set->dof = dof;
+    S->dat.dof_poset += dof;
+    S->dat.dof += dof;
+    return S->dat.nsets - 1;
+}
+
+/* A plane-of-sky frame after calc_fits + chi2: the fit image (layout of
+ * the observed one), the sky rendering's brightness pos->b ((2n+1)^2, j
+ * contiguous), cal and chi2 (out[0..1]); NULL skips. */
+void ref_get_poset_frame(void *h, int s, int f, double *fit, double *b, double *out)
+{
+    ref_session *S = h;
+    struct posetfrm_t *fr = &S->dat.set[s].desc.poset.frame[f];
+    if (fit)
+        for (int i = 1; i <= fr->ncol; i++)
+            for (int j = 1; j <= fr->nrow; j++) fit[(size_t)(i - 1) * fr->nrow + (j - 1)] = fr->fit.b[i][j];
+    if (b) {
+        const int n = fr->pos.n, side = 2 * n + 1;
+        for (int i = -n; i <= n; i++)
+            for (int j = -n; j <= n; j++) b[(size_t)(i + n) * side + (j + n)] = fr->pos.b[i][j];
+    }
+    if (out) { out[0] = fr->cal.val; out[1] = fr->chi2; }
+}
+
+/* par's badposet flag and log factor after calc_fits (src/shape/calc_fits.c:408). */
+void ref_get_badposet(void *h, double out[2])
+{
+    ref_session *S = h;
+    out[0] = S->par.badposet;
+    out[1] = S->par.badposet_logfactor;
+}
+
 /* Scale factor j of the component (a SIZEPAR free parameter, src/shape/mkparlist.c:219-226). */
 void ref_set_scale(void *h, int j, double val)
 {
@@ -646,6 +736,17 @@ void ref_free(void *h)
             struct lghtcrv_t *lc = &set->desc.lghtcrv;
             for (int i = 1; i <= lc->ncalc; i++) ref_free_pos(&lc->rend[i].pos);
             free(lc->rend);
+        } else if (set->type == POS) {
+            struct poset_t *po = &set->desc.poset;
+            for (int f = 0; f < po->nframes; f++) {
+                struct posetfrm_t *fr = &po->frame[f];
+                ref_free_pos(&fr->pos);
+                free_matrix(fr->obs.b, 1, fr->ncol, 1, fr->nrow);
+                free_matrix(fr->fit.b, 1, fr->ncol, 1, fr->nrow);
+                free_matrix(fr->oneovervar, 1, fr->ncol, 1, fr->nrow);
+                free(fr->view);
+            }
+            free(po->frame);
         }
     }
     free(S->dat.set);

@@ -592,12 +592,18 @@ __global__ void k_lc_photo(LcArgs a)
         const int *F = a.f + go.pos_base;
         const int *FI = a.fill + gs.pos_base;
         const double bignum = 0.99 * HUGENUMBER;
+        // a plane-of-sky frame keeps its brightness image (pos->b of
+        // apply_photo, zero where nothing is lit)
+        double *Bimg = (a.bimg && P.b_base >= 0) ? a.bimg + P.b_base : nullptr;
         double bsum = 0.0;
         long long pend = (long long)item.y + a.chunk;
         if (pend > npix) pend = npix;
         for (long long p = item.y + threadIdx.x; p < pend; p += blockDim.x) {
             double cose = (double)CE[p];
-            if (cose == 0.0) continue;
+            if (cose == 0.0) {
+                if (Bimg) Bimg[p] = 0.0;
+                continue;
+            }
             int i = (int)(p / side) - n, j = (int)(p % side) - n;
             double xin[3] = {i * go.kmpp, j * go.kmpp, (double)Z[p]};
             double x[3];
@@ -623,6 +629,7 @@ __global__ void k_lc_photo(LcArgs a)
             int f = F[p];
             if (a.mark_seen && cose > a.mincosine_seen && cosi > a.mincosine_seen && f >= 0)
                 a.seen[f] = 1;
+            double bv = 0.0;
             if (cose > 0.0 && cosi > 0.0 && f >= 0) {
                 double b;
                 if (P.law_type == SHAPE_OPTLAW_LAMBERT)
@@ -632,7 +639,9 @@ __global__ void k_lc_photo(LcArgs a)
                 else
                     b = P.intensityfactor * cosi * (P.s_ls / (cosi + cose) + P.s_l);
                 bsum += b;
+                bv = b;
             }
+            if (Bimg) Bimg[p] = bv;
         }
         for (int off = 16; off > 0; off >>= 1)
             bsum += __shfl_down_sync(0xffffffffu, bsum, off);
@@ -675,6 +684,177 @@ __device__ double view_logfactor(const FrameGeom &g, const FrameState &st)
     double xfactor = (dmax_(oimax, n) - dmin_(oimin, -n) + 1) / (2 * n + 1);
     double yfactor = (dmax_(ojmax, n) - dmin_(ojmin, -n) + 1) / (2 * n + 1);
     return log(xfactor * yfactor);
+}
+
+
+// ---- plane-of-sky frames (calc_poset, src/shape/calc_fits.c:1156-1330)
+
+// The interpolation polynomial of cubic convolution with parameter -1 (the
+// original kernel; resampim's CUBICPAR), in resampim's operations.
+__device__ double cubicconv_w(double x)
+{
+    const double c = -1.0;
+    const double ax = fabs(x);
+    if (ax < 1) return (c + 2) * ax * ax * ax - (c + 3) * ax * ax + 1;
+    if (ax < 2) return c * (ax * ax * ax - 5 * ax * ax + 8 * ax - 4);
+    return 0.0;
+}
+
+// One sample of the resampling grid (src/util/resampim.c): the grid point
+// of temporary column it and row jt, reached by resampim's running sums
+// (x1start and y1start advance once per column, x1 and y1 once per row),
+// read from the brightness image B ([-n..n]^2, j contiguous) by the
+// frame's interpolation; 0 where the input pixels it needs leave the image.
+__device__ double poset_sample(const double *B, int n, int side, int mode, double x1start, double y1start,
+                               double dxx, double dyx, double dxy, double dyy, int it, int jt)
+{
+    double x1 = x1start, y1 = y1start;
+    for (int k = 1; k < it; k++) { x1 += dxx; y1 += dyx; }
+    for (int k = 1; k < jt; k++) { x1 += dxy; y1 += dyy; }
+#define IM(i_, j_) B[(long long)((i_) + n) * side + ((j_) + n)]
+    if (mode == SHAPE_RESAMPLE_NONE || mode == SHAPE_RESAMPLE_NEAREST) {
+        const int ix = iround_(x1), iy = iround_(y1);
+        return (ix >= -n && ix <= n && iy >= -n && iy <= n) ? IM(ix, iy) : 0.0;
+    }
+    const int ix = (int)floor(x1), iy = (int)floor(y1);
+    if (mode == SHAPE_RESAMPLE_BILINEAR) {
+        if (!(ix >= -n && ix < n && iy >= -n && iy < n)) return 0.0;
+        const double t = x1 - ix, u = y1 - iy;
+        return (1 - t) * (1 - u) * IM(ix, iy) + t * (1 - u) * IM(ix + 1, iy) + t * u * IM(ix + 1, iy + 1) +
+               (1 - t) * u * IM(ix, iy + 1);
+    }
+    // cubic convolution: four interpolations along rows, then one along the column
+    double v = 0.0;
+    if (ix > -n && ix < n - 1 && iy > -n && iy < n - 1) {
+        const double t = x1 - ix, u = y1 - iy;
+        double xp[4];
+        for (int k = -1; k <= 2; k++) xp[k + 1] = cubicconv_w(k - t);
+        for (int l = -1; l <= 2; l++) {
+            double xi = 0.0;
+            for (int k = -1; k <= 2; k++) xi += xp[k + 1] * IM(ix + k, iy + l);
+            v += cubicconv_w(l - u) * xi;
+        }
+    }
+    return v;
+#undef IM
+}
+
+// One block per plane-of-sky frame: the fit image by resampim (with
+// rebinning when the grid undersamples the rendering by an integer factor
+// and image_rebin is set; cubic convolution clipped at 0), checkposet's
+// test of the lit pixels' corners against the rotated fit grid
+// (src/util/checkposet.c), chi2_poset's sums with the floating
+// calibration (src/shape/chi2.c) and the views' posbnd terms.
+__global__ void k_poset_frames(PosetArgs a)
+{
+    __shared__ double red[5][32];
+    __shared__ int redi[32];
+    const PosetFrameDev F = a.frames[blockIdx.x];
+    const LcPointDev &P = a.pts[F.point];
+    const FrameGeom &go = a.geoms[P.obs_view], &gs = a.geoms[P.sun_view];
+    const int n = go.n, side = go.side;
+    const double *B = a.bimg + P.b_base;
+    const int ncol = F.ncol, nrow = F.nrow;
+    double *FIT = a.fit + F.img_base;
+    const double *OBS = a.obs + F.img_base, *OOV = a.oov + F.img_base;
+    // resampim's grid over the temporary image (1..xt2) x (1..yt2)
+    int xb = 1, yb = 1;
+    if (F.rebin) {
+        xb = max(iround_(F.xwidth / (ncol - 1)), 1);
+        yb = max(iround_(F.ywidth / (nrow - 1)), 1);
+    }
+    const int npix = xb * yb;
+    const bool rebin = F.rebin && npix > 1;
+    const int xt2 = rebin ? xb * ncol : ncol, yt2 = rebin ? yb * nrow : nrow;
+    const double xstep = (F.mode == SHAPE_RESAMPLE_NONE) ? 1.0 : F.xwidth / (xt2 - 1);
+    const double ystep = (F.mode == SHAPE_RESAMPLE_NONE) ? 1.0 : F.ywidth / (yt2 - 1);
+    const double dxx = xstep * F.cosang, dxy = ystep * F.sinang;
+    const double dyx = -xstep * F.sinang, dyy = ystep * F.cosang;
+    const double x1s = F.x0 - ((xt2 - 1) / 2.0) * dxx - ((yt2 - 1) / 2.0) * dxy;
+    const double y1s = F.y0 - ((xt2 - 1) / 2.0) * dyx - ((yt2 - 1) / 2.0) * dyy;
+    double o2 = 0.0, m2 = 0.0, om = 0.0;
+    for (int p = threadIdx.x; p < ncol * nrow; p += blockDim.x) {
+        const int i = p / nrow + 1, j = p % nrow + 1;
+        double v;
+        if (rebin) {
+            v = 0.0;
+            for (int k = 1 + (i - 1) * xb; k < 1 + i * xb; k++)
+                for (int l = 1 + (j - 1) * yb; l < 1 + j * yb; l++)
+                    v += poset_sample(B, n, side, F.mode, x1s, y1s, dxx, dyx, dxy, dyy, k, l);
+            v /= npix;
+        } else {
+            v = poset_sample(B, n, side, F.mode, x1s, y1s, dxx, dyx, dxy, dyy, i, j);
+        }
+        if (F.mode == SHAPE_RESAMPLE_CUBICCONV) v = fmax(0.0, v);
+        FIT[p] = v;
+        const double ob = OBS[p], w = OOV[p];
+        o2 += ob * ob * w;
+        m2 += v * v * w;
+        om += v * ob * w;
+    }
+    // checkposet: every corner of a lit POS pixel against the fit grid
+    const double xl1 = -F.xwidth / 2 - 0.5, xl2 = F.xwidth / 2 + 0.5;
+    const double yl1 = -F.ywidth / 2 - 0.5, yl2 = F.ywidth / 2 + 0.5;
+    double xmin = xl1, xmax = xl2, ymin = yl1, ymax = yl2;
+    int bad = 0;
+    const int cside = side + 1;
+    for (int c = threadIdx.x; c < cside * cside; c += blockDim.x) {
+        const int ci = c / cside - n, cj = c % cside - n;      // corner (ci, cj): ci, cj = -n..n+1
+        bool lit = false;
+        for (int di = -1; di <= 0 && !lit; di++)
+            for (int dj = -1; dj <= 0 && !lit; dj++) {
+                const int pi = ci + di, pj = cj + dj;
+                if (pi >= -n && pi <= n && pj >= -n && pj <= n && B[(long long)(pi + n) * side + (pj + n)] > 0.0)
+                    lit = true;
+            }
+        if (!lit) continue;
+        const double xs = (ci - 0.5) - F.x0, ys = (cj - 0.5) - F.y0;
+        const double xf = xs * F.cosang + ys * F.sinang;
+        const double yf = -xs * F.sinang + ys * F.cosang;
+        if (xf < xl1) { bad = 1; xmin = fmin(xmin, xf); }
+        else if (xf > xl2) { bad = 1; xmax = fmax(xmax, xf); }
+        if (yf < yl1) { bad = 1; ymin = fmin(ymin, yf); }
+        else if (yf > yl2) { bad = 1; ymax = fmax(ymax, yf); }
+    }
+    // block reductions: sums, extremes, the flag
+    for (int off = 16; off > 0; off >>= 1) {
+        o2 += __shfl_down_sync(0xffffffffu, o2, off);
+        m2 += __shfl_down_sync(0xffffffffu, m2, off);
+        om += __shfl_down_sync(0xffffffffu, om, off);
+        xmin = fmin(xmin, __shfl_down_sync(0xffffffffu, xmin, off));
+        xmax = fmax(xmax, __shfl_down_sync(0xffffffffu, xmax, off));
+        ymin = fmin(ymin, __shfl_down_sync(0xffffffffu, ymin, off));
+        ymax = fmax(ymax, __shfl_down_sync(0xffffffffu, ymax, off));
+        bad |= __shfl_down_sync(0xffffffffu, bad, off);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ double ext[4][32];
+    if (lane == 0) {
+        red[0][wid] = o2; red[1][wid] = m2; red[2][wid] = om;
+        ext[0][wid] = xmin; ext[1][wid] = xmax; ext[2][wid] = ymin; ext[3][wid] = ymax;
+        redi[wid] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    o2 = m2 = om = 0.0;
+    for (int w = 0; w < nw; w++) {
+        o2 += red[0][w]; m2 += red[1][w]; om += red[2][w];
+        xmin = fmin(xmin, ext[0][w]); xmax = fmax(xmax, ext[1][w]);
+        ymin = fmin(ymin, ext[2][w]); ymax = fmax(ymax, ext[3][w]);
+        bad |= redi[w];
+    }
+    shape_poset_result r;
+    r.o2 = o2; r.m2 = m2; r.om = om;
+    r.cal = (om > 0.0) ? om / m2 : SHAPE_TINYCALFACT;
+    r.chi2 = F.weight * (o2 - 2 * r.cal * om + r.cal * r.cal * m2);
+    r.badposet = bad;
+    r.badposet_logfactor = bad ? log((xmax - xmin) * (ymax - ymin) / ((F.xwidth + 1) * (F.ywidth + 1))) : 0.0;
+    const FrameState &so = a.states[P.obs_view], &ss = a.states[P.sun_view];
+    r.outbnd = (so.outbnd ? 1 : 0) | (ss.outbnd ? 2 : 0);
+    r.posbnd_logsum = 0.0;
+    if (so.outbnd) r.posbnd_logsum += 0.5 * F.dof * view_logfactor(go, so);
+    if (ss.outbnd) r.posbnd_logsum += 0.5 * F.dof * view_logfactor(gs, ss);
+    a.res[blockIdx.x] = r;
 }
 
 // Natural cubic spline second derivatives and evaluation (the role of
@@ -873,12 +1053,23 @@ __global__ void k_summary(FinalizeArgs fa, SummaryArgs a)
 template <typename Term>
 __device__ void summary_totals(const SummaryArgs &a, Term term)
 {
-    double chi2 = 0.0, chi2_dd = 0.0, chi2_lc = 0.0, plog = 0.0, blog = 0.0;
-    int posbnd = 0, badradar = 0;
+    double chi2 = 0.0, chi2_dd = 0.0, chi2_lc = 0.0, chi2_ps = 0.0, plog = 0.0, blog = 0.0, pslog = 0.0;
+    int posbnd = 0, badradar = 0, badposet = 0;
     for (int s = 0; s < a.nsets; s++) {
         const SetRec &R = a.sets[s];
         double cs = 0.0;
-        if (R.type == 0) {
+        if (R.type == 2) {
+            // plane-of-sky frames: chi2_poset's frame sum; calc_poset's
+            // posbnd terms (dof/2 per view) and badposet terms (dof times
+            // checkposet's log factor)
+            for (int f = R.first; f < R.first + R.count; f++) {
+                const shape_poset_result &r = a.ps_res[f];
+                cs += r.chi2;
+                if (r.outbnd) { posbnd = 1; plog += r.posbnd_logsum; }
+                if (r.badposet) { badposet = 1; pslog += a.ps_frames[f].dof * r.badposet_logfactor; }
+            }
+            chi2_ps += cs;
+        } else if (R.type == 0) {
             for (int f = R.first; f < R.first + R.count; f++) {
                 double c, pl, bl;
                 int fl;
@@ -906,9 +1097,13 @@ __device__ void summary_totals(const SummaryArgs &a, Term term)
     out.posbnd_logfactor = plog / a.dof;
     out.badradar = badradar;
     out.badradar_logfactor = blog / a.dof_radar;
+    out.chi2_poset = chi2_ps;
+    out.badposet = badposet;
+    out.badposet_logfactor = badposet ? pslog / a.dof_poset : 0.0;
     double err = chi2 / a.dof;
     if (a.baddiam) err *= a.bad_objfactor * exp(a.baddiam_logfactor);
     if (posbnd) err *= a.bad_objfactor * exp(out.posbnd_logfactor);
+    if (badposet) err *= a.bad_objfactor * exp(out.badposet_logfactor);
     if (badradar) err *= a.bad_objfactor * exp(out.badradar_logfactor);
     out.objective = err;
     out.penalties = 0.0;
@@ -1111,6 +1306,12 @@ void launch_doppler_overflow(const DopOvfArgs &a, cudaStream_t s)
     k_doppler_overflow<<<a.n, 256, 0, s>>>(a);
 }
 
+
+void launch_poset_frames(const PosetArgs &a, cudaStream_t s)
+{
+    if (a.nframes <= 0) return;
+    k_poset_frames<<<a.nframes, 256, 0, s>>>(a);
+}
 
 void launch_lc_photo(const LcArgs &a, int fp32, cudaStream_t s)
 {

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <set>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -84,7 +85,7 @@ void radar_set_consts(FrameGeom &g, const shape_deldop_set &S, const shape_eval_
 int EngineImpl::finalize()
 {
     if (!have_model) return set_err(SHAPE_E_STATE, "finalize: no model set");
-    if (dd.empty() && lc.empty()) return set_err(SHAPE_E_STATE, "finalize: no datasets");
+    if (dd.empty() && lc.empty() && ps.empty()) return set_err(SHAPE_E_STATE, "finalize: no datasets");
     mem.release();
     invalidate_graphs();
     for (int f = 0; f < 3; f++) tuned[f] = 0;
@@ -98,7 +99,7 @@ int EngineImpl::finalize()
 
     const int nframes = (int)frames.size();
     const int npts = (int)points.size();
-    nviews = 2 * npts;
+    nviews = 2 * npts + 2 * nps_frames;      // lightcurve points and plane-of-sky frames: two views each
     for (int fi = 0; fi < nframes; fi++) nviews += fviews[fi].empty() ? 1 : (int)fviews[fi].size();
     int tile_base = 0;
     long long pos_base = 0;
@@ -202,8 +203,52 @@ int EngineImpl::finalize()
         fused_chi2 = every && !chi2_items.empty() && chi2_summary_fits((int)fh.size(), max_items);
         fused_smem = fused_chi2 ? chi2_summary_smem((int)fh.size(), max_items) : 0;
     }
-    // lightcurve points: two views each (src/shape/calc_fits.c:1634-1716)
+    // lightcurve points: two views each (src/shape/calc_fits.c:1634-1716);
+    // a plane-of-sky frame is rendered the same way (calc_poset,
+    // src/shape/calc_fits.c:1205-1266) and keeps its brightness image
     const int LC_CHUNK = 4096;
+    auto add_point = [&](const shape_lghtcrv_point &P, const shape_optical_law &law, int set, long long b_base) {
+        LcPointDev pd;
+        memset(&pd, 0, sizeof pd);
+        FrameGeom go, gs;
+        memset(&go, 0, sizeof go);
+        memset(&gs, 0, sizeof gs);
+        go.wscale = gs.wscale = 1.0;
+        lc_view_geom(go, gs, pd, P);
+        go.kind = VIEW_LC_OBS;
+        go.smooth = params.pos_smooth;
+        go.frame_index = (int)lcpts.size();
+        pd.obs_view = (int)geoms.size();
+        add_view(go, P.pos_n, P.km_per_pixel);
+        gs.kind = VIEW_LC_SUN;
+        gs.smooth = 0;
+        gs.frame_index = (int)lcpts.size();
+        pd.sun_view = (int)geoms.size();
+        add_view(gs, P.pos_n, P.km_per_pixel);
+        pd.set = set;
+        pd.law_type = law.type;
+        pd.intensityfactor = pow(P.km_per_pixel / SHAPE_AU, 2.0);
+        if (law.type == SHAPE_OPTLAW_LAMBERT) {
+            pd.scale = law.R / SHAPE_PIE;
+        } else if (law.type == SHAPE_OPTLAW_LOMMEL) {
+            pd.scale = law.R / (4 * SHAPE_PIE);
+        } else {
+            double phasefunc = law.A0 * exp(-P.solar_phase / law.D) + law.k * P.solar_phase + 1;
+            pd.s_ls = (1 - law.wt) * phasefunc * law.R / (4 * SHAPE_PIE);
+            pd.s_l = law.wt * phasefunc * law.R / SHAPE_PIE;
+        }
+        pd.mask_tol = params.mask_tol;
+        pd.pixels_per_km = 1 / P.km_per_pixel;
+        pd.b_base = b_base;
+        int side = 2 * P.pos_n + 1;
+        long long np = (long long)side * side;
+        pt_items.push_back((int)lc_items.size());
+        int cnt = 0;
+        for (long long p0 = 0; p0 < np; p0 += LC_CHUNK, cnt++)
+            lc_items.push_back(make_int2((int)lcpts.size(), (int)p0));
+        pt_items.push_back(cnt);
+        lcpts.push_back(pd);
+    };
     for (size_t s = 0; s < lc.size(); s++) {
         const shape_lghtcrv_set &S = lc[s].set;
         if (S.law.type != SHAPE_OPTLAW_LAMBERT && S.law.type != SHAPE_OPTLAW_LOMMEL &&
@@ -219,50 +264,55 @@ int EngineImpl::finalize()
         L.dof = S.dof;
         L.cal_in = S.cal;
         L.cal_floating = S.cal_floating;
-        for (int k = 0; k < lc[s].npts; k++) {
-            const shape_lghtcrv_point &P = points[lc[s].pt0 + k];
-            LcPointDev pd;
-            memset(&pd, 0, sizeof pd);
-            FrameGeom go, gs;
-            memset(&go, 0, sizeof go);
-            memset(&gs, 0, sizeof gs);
-            go.wscale = gs.wscale = 1.0;
-            lc_view_geom(go, gs, pd, P);
-            go.kind = VIEW_LC_OBS;
-            go.smooth = params.pos_smooth;
-            go.frame_index = lc[s].pt0 + k;
-            pd.obs_view = (int)geoms.size();
-            add_view(go, P.pos_n, P.km_per_pixel);
-            gs.kind = VIEW_LC_SUN;
-            gs.smooth = 0;
-            gs.frame_index = lc[s].pt0 + k;
-            pd.sun_view = (int)geoms.size();
-            add_view(gs, P.pos_n, P.km_per_pixel);
-            pd.set = (int)s;
-            pd.law_type = S.law.type;
-            pd.intensityfactor = pow(P.km_per_pixel / SHAPE_AU, 2.0);
-            if (S.law.type == SHAPE_OPTLAW_LAMBERT) {
-                pd.scale = S.law.R / SHAPE_PIE;
-            } else if (S.law.type == SHAPE_OPTLAW_LOMMEL) {
-                pd.scale = S.law.R / (4 * SHAPE_PIE);
-            } else {
-                double phasefunc = S.law.A0 * exp(-P.solar_phase / S.law.D) + S.law.k * P.solar_phase + 1;
-                pd.s_ls = (1 - S.law.wt) * phasefunc * S.law.R / (4 * SHAPE_PIE);
-                pd.s_l = S.law.wt * phasefunc * S.law.R / SHAPE_PIE;
-            }
-            pd.mask_tol = params.mask_tol;
-            pd.pixels_per_km = 1 / P.km_per_pixel;
-            int side = 2 * P.pos_n + 1;
-            long long np = (long long)side * side;
-            pt_items.push_back((int)lc_items.size());
-            int cnt = 0;
-            for (long long p0 = 0; p0 < np; p0 += LC_CHUNK, cnt++)
-                lc_items.push_back(make_int2((int)lcpts.size(), (int)p0));
-            pt_items.push_back(cnt);
-            lcpts.push_back(pd);
-        }
+        for (int k = 0; k < lc[s].npts; k++) add_point(points[lc[s].pt0 + k], S.law, (int)s, -1);
         L.nitems = (int)lc_items.size() - L.item0;
         lcdev.push_back(L);
+    }
+    // plane-of-sky frames after every lightcurve point: their views'
+    // points (ps_points), brightness images and resampling descriptors
+    ps_points.clear();
+    psf.clear();
+    ps_img_elems = ps_b_elems = 0;
+    for (size_t s = 0; s < ps.size(); s++) {
+        const PosetHost &H = ps[s];
+        for (size_t k = 0; k < H.frames.size(); k++) {
+            const shape_poset_frame &Fr = H.frames[k];
+            shape_lghtcrv_point P;
+            memset(&P, 0, sizeof P);
+            P.pos_n = Fr.pos_n;
+            P.km_per_pixel = Fr.km_per_pixel;
+            memcpy(P.ae, Fr.ae, sizeof P.ae);
+            memcpy(P.oe, Fr.oe, sizeof P.oe);
+            memcpy(P.se, Fr.se, sizeof P.se);
+            P.solar_phase = Fr.solar_phase;
+            ps_points.push_back(P);
+            PosetFrameDev d;
+            memset(&d, 0, sizeof d);
+            d.point = (int)lcpts.size();
+            d.ncol = Fr.ncol;
+            d.nrow = Fr.nrow;
+            d.img_base = ps_img_elems;
+            // the resampling grid of calc_poset (src/shape/calc_fits.c:1278-1291)
+            const double xcom_fit = (Fr.colcom_vig - (Fr.ncol + 1) / 2.0) + Fr.xoff;
+            const double ycom_fit = (Fr.rowcom_vig - (Fr.nrow + 1) / 2.0) + Fr.yoff;
+            const double fact = Fr.fit_km_per_pixel / Fr.km_per_pixel;
+            d.x0 = -xcom_fit * fact;
+            d.y0 = -ycom_fit * fact;
+            d.xwidth = fact * (Fr.ncol - 1);
+            d.ywidth = fact * (Fr.nrow - 1);
+            const double angle = -Fr.northangle;
+            d.cosang = cos(angle);
+            d.sinang = sin(angle);
+            d.mode = H.set.resample;
+            d.rebin = H.set.rebin ? 1 : 0;
+            d.weight = Fr.weight;
+            d.dof = Fr.dof;
+            psf.push_back(d);
+            add_point(P, H.set.law, -1, ps_b_elems);
+            const long long side = 2 * (long long)Fr.pos_n + 1;
+            ps_b_elems += side * side;
+            ps_img_elems += (long long)Fr.ncol * Fr.nrow;
+        }
     }
     if (laws.empty()) laws.push_back(RadarLawDev{SHAPE_RADLAW_COSINE_DIFF, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0});
     ntiles = tile_base;
@@ -304,6 +354,9 @@ int EngineImpl::finalize()
     AL(d_lcsets, lcdev.size()); AL(d_lc_out, 4 * lcdev.size());
     AL(d_lc_dof, lcdev.size()); AL(d_lc_npts, lcdev.size());
     AL(d_setrecs, setrecs.size());
+    AL(d_psf, psf.size()); AL(d_ps_res, psf.size());
+    AL(d_ps_obs, (size_t)ps_img_elems); AL(d_ps_oov, (size_t)ps_img_elems); AL(d_ps_fit, (size_t)ps_img_elems);
+    AL(d_ps_b, (size_t)ps_b_elems);
     if (!dop_frames.empty()) {
         AL(d_ovf, dop_frames.size() * DOP_MAXOVERFLOW);
         AL(d_ovf_out, dop_frames.size() * DOP_OVF_TERMS);
@@ -393,6 +446,14 @@ int EngineImpl::finalize()
         CK(cudaMemcpyAsync(d_lc_npts, lcnp.data(), sizeof(double) * lcnp.size(), cudaMemcpyHostToDevice, s));
     }
     CK(cudaMemcpyAsync(d_setrecs, setrecs.data(), sizeof(SetRec) * setrecs.size(), cudaMemcpyHostToDevice, s));
+    if (!psf.empty()) {
+        CK(cudaMemcpyAsync(d_psf, psf.data(), sizeof(PosetFrameDev) * psf.size(), cudaMemcpyHostToDevice, s));
+        for (const PosetHost &H : ps) {
+            const long long b = psf[H.frame0].img_base;
+            CK(cudaMemcpyAsync(d_ps_obs + b, H.obs.data(), sizeof(double) * H.obs.size(), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(d_ps_oov + b, H.oov.data(), sizeof(double) * H.oov.size(), cudaMemcpyHostToDevice, s));
+        }
+    }
     if (!dop_frames.empty())
         CK(cudaMemcpyAsync(d_dop_frames, dop_frames.data(), sizeof(int) * dop_frames.size(),
                            cudaMemcpyHostToDevice, s));
@@ -527,6 +588,7 @@ double *EngineImpl::spin_param(int kind, int index)
 // model, dataset by dataset, then refreshes the view constants.
 int EngineImpl::realize_views()
 {
+    if (!ps.empty()) return set_err(SHAPE_E_UNSUPPORTED, "spin model: plane-of-sky sets take their views as given");
     if (spin_angleoff.size() != 3 * setrecs.size() || frame_t.size() != frames.size())
         return set_err(SHAPE_E_STATE, "spin model: datasets were added after set_spin_model");
     for (const auto &V : fviews)
@@ -567,6 +629,8 @@ int EngineImpl::setup_spin_device()
     n_spin_src = 0;
     if (!spin_device) return SHAPE_OK;
     if (!have_spin) return set_err(SHAPE_E_STATE, "device spin realization: no spin model");
+    if (!ps.empty())
+        return set_err(SHAPE_E_UNSUPPORTED, "device spin realization: plane-of-sky sets take their views as given");
     if (!spin_st.pa)
         return set_err(SHAPE_E_UNSUPPORTED, "device spin realization: principal-axis rotators only");
     for (const auto &V : fviews)
@@ -668,7 +732,8 @@ int EngineImpl::refresh_views()
         }
     for (size_t pt = 0; pt < lcpts.size(); pt++) {
         LcPointDev &pd = lcpts[pt];
-        lc_view_geom(geoms[pd.obs_view], geoms[pd.sun_view], pd, points[pt]);
+        const shape_lghtcrv_point &P = pt < points.size() ? points[pt] : ps_points[pt - points.size()];
+        lc_view_geom(geoms[pd.obs_view], geoms[pd.sun_view], pd, P);
         view_float_consts(geoms[pd.obs_view]);
         view_float_consts(geoms[pd.sun_view]);
     }
@@ -993,6 +1058,13 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     cudaStream_t s = stream;
     const bool f32 = (form == SHAPE_FORM_BATCHED_FP32);
     auto mark = [&](int k) { if (marks) cudaEventRecord(marks[k], s); };
+    // a launch rejected by the runtime (configuration, resources) is
+    // reported with the stage it belongs to
+    auto launched = [&](const char *stage) -> int {
+        const cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) return SHAPE_OK;
+        return set_err(SHAPE_E_CUDA, std::string(stage) + ": " + cudaGetErrorString(e));
+    };
     // The batched forms run two side branches beside the view transform
     // (which realizes its vertices on the fly): the state reset and image
     // clears (stream2), and realize with the facet and vertex normals
@@ -1014,6 +1086,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         launch_realize(md, s);
     }
     mark(0);
+    if (int rc_ = launched("realize")) return rc_;
     launch_reset_state(d_states, nviews, d_bin_count, ntiles, sr);
     if (fit_elems) {
         if (f32) CK(cudaMemsetAsync(d_fit32, 0, sizeof(float) * fit_elems, sr));
@@ -1026,6 +1099,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     if (fused) CK(cudaMemsetAsync(d_chi2_counters, 0, sizeof(int) * (fh.size() + 1), sr));
     if (fork) CK(cudaEventRecord(evf[2], stream2));   // reset and clears done
     mark(1);
+    if (int rc_ = launched("state reset")) return rc_;
 
     RasterArgs ra;
     memset(&ra, 0, sizeof ra);
@@ -1064,6 +1138,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     la.zill = static_cast<const double *>(d_pos_z);
     la.f = d_pos_f; la.fill = d_pos_f;
     la.partials = d_lc_partials;
+    la.bimg = d_ps_b;
     la.seen = d_seen;
     la.mincosine_seen = params.mincosine_seen;
     la.mark_seen = params.mark_seen;
@@ -1094,6 +1169,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
                 lv.partials = d_lc_partials + pt_items[2 * pt];
                 launch_lc_photo(lv, 0, s);
             }
+            if (int rc_ = launched(g.kind == VIEW_RADAR ? "radar view chain" : "lightcurve view chain")) return rc_;
         }
     } else {
         // graph-captured chain: each kernel after the first is a programmatic
@@ -1103,6 +1179,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         if (fork) launch_xform_realize_f64(d_geoms, nviews, md, d_vt64, s);
         else launch_xform_f64(d_geoms, nviews, md.vx, nv, d_vt64, s);
         mark(2);
+        if (int rc_ = launched("view transform")) return rc_;
         if (fork) {
             CK(cudaStreamWaitEvent(s, evf[1], 0));
             CK(cudaStreamWaitEvent(s, evf[2], 0));
@@ -1110,6 +1187,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         launch_bin_f64(d_geoms, 0, nviews, md, d_vt64, d_states, d_bin_count, d_bin_ids, cap, s, pdl);
         if (fork) CK(cudaStreamWaitEvent(s, evf[3], 0));
         mark(3);
+        if (int rc_ = launched("binning")) return rc_;
         // one CTA per tile, heaviest tiles first (empty tiles sort last and
         // exit at once); the block scheduler balances the rest
         // one CTA per tile that was non-empty when the bins were tuned (they
@@ -1139,11 +1217,13 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
             launch_raster_f64(ra, s);
         }
         mark(4);
+        if (int rc_ = launched("raster")) return rc_;
         ca.items = d_chi2_items;
         ca.nitems = (int)chi2_items.size();
         // fused: the chi-square partials run with the summary, last
         if (!chi2_items.empty() && !fused) launch_chi2_partials(ca, f32 ? 1 : 0, s);
         mark(5);
+        if (int rc_ = launched("chi-square partials")) return rc_;
         if (!lc_items.empty()) {
             la.items = d_lc_items;
             la.nitems = (int)lc_items.size();
@@ -1151,6 +1231,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
             launch_lc_photo(la, 0, s);
         }
         mark(6);
+        if (int rc_ = launched("lightcurve photometry")) return rc_;
     }
     FinalizeArgs fa;
     memset(&fa, 0, sizeof fa);
@@ -1165,6 +1246,15 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         oa.frames = d_dop_frames; oa.fh = d_fh; oa.geoms = d_geoms; oa.states = d_states;
         oa.ovf = d_ovf; oa.out = d_ovf_out;
         launch_doppler_overflow(oa, s);
+        if (int rc_ = launched("Doppler overflow")) return rc_;
+    }
+    if (!psf.empty()) {
+        PosetArgs pa;
+        pa.nframes = (int)psf.size();
+        pa.frames = d_psf; pa.pts = d_lcpts; pa.geoms = d_geoms; pa.states = d_states;
+        pa.bimg = d_ps_b; pa.obs = d_ps_obs; pa.oov = d_ps_oov; pa.fit = d_ps_fit; pa.res = d_ps_res;
+        launch_poset_frames(pa, s);
+        if (int rc_ = launched("plane-of-sky frames")) return rc_;
     }
     if (!lcdev.empty()) {
         LcFinalizeArgs lf;
@@ -1178,12 +1268,14 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
         }
         lf.smem_per_set = sm;
         launch_lc_finalize(lf, s);
+        if (int rc_ = launched("lightcurve finalize")) return rc_;
     }
     SummaryArgs sa;
     memset(&sa, 0, sizeof sa);
     sa.nsets = (int)setrecs.size();
     sa.sets = d_setrecs; sa.fh = d_fh; sa.results = d_results;
     sa.lc_out = d_lc_out; sa.lc_dof = d_lc_dof; sa.lc_npts = d_lc_npts;
+    sa.ps_res = d_ps_res; sa.ps_frames = d_psf; sa.dof_poset = dof_poset;
     sa.dof = dof; sa.dof_radar = dof_deldop + dof_doppler; sa.bad_objfactor = bad_objfactor;
     sa.nitems = (int)chi2_items.size();
     // the bad-diameter factor depends only on host-side scale factors and is
@@ -1218,6 +1310,7 @@ int EngineImpl::kernels_per_eval(int form) const
         n += lc_items.empty() ? 0 : 1;
     }
     n += lcdev.empty() ? 0 : 1;          // lightcurve finalize
+    n += psf.empty() ? 0 : 1;            // plane-of-sky frames
     n += dop_frames.empty() ? 0 : 1;     // Doppler overflow spectra
     n += pen_type.empty() ? 0 : (ncomp > 1 ? 3 : 2);   // model sums (and check_surface) for the penalties
     return n + 1;                        // finalize + summary (with the chi-square partials when fused)
@@ -1325,6 +1418,71 @@ struct TuneChoice {
 };
 std::mutex tune_mu;
 std::map<TuneKey, TuneChoice> tune_cache;
+
+// The tuning file (SHAPE_B200_TUNING_CACHE names it; none by default): one
+// JSON object per line and size class, keyed by the GPU's name and SM count
+// so that a file carried to another machine of the same kind is reused and
+// one of another kind is ignored. Read once per device, rewritten whenever
+// a new size class is tuned.
+std::string gpu_tag(int device)
+{
+    cudaDeviceProp pr;
+    if (cudaGetDeviceProperties(&pr, device) != cudaSuccess) return std::string();
+    std::string name(pr.name);
+    for (char &c : name)
+        if (c == '"' || c == '\\') c = '_';
+    return name + "/" + std::to_string(pr.multiProcessorCount);
+}
+std::set<int> tune_file_read;
+
+void tune_file_load(int device)
+{
+    const char *path = getenv("SHAPE_B200_TUNING_CACHE");
+    if (!path || !*path || tune_file_read.count(device)) return;
+    tune_file_read.insert(device);
+    FILE *fp = fopen(path, "r");
+    if (!fp) return;
+    const std::string tag = gpu_tag(device);
+    char line[1024], gpu[256];
+    while (fgets(line, sizeof line, fp)) {
+        TuneKey k{};
+        TuneChoice c{};
+        if (sscanf(line,
+                   "{\"gpu\": \"%255[^\"]\", \"form\": %d, \"exact\": %d, \"views\": %d, \"facets\": %d, "
+                   "\"nonempty\": %d, \"maxcount16\": %d, \"variant\": %d, \"persistent\": %d, "
+                   "\"ms\": [%lf, %lf, %lf, %lf]}",
+                   gpu, &k.form, &k.exact, &k.nviews, &k.nf, &k.nonempty, &k.maxcount, &c.variant, &c.persistent,
+                   &c.ms[0], &c.ms[1], &c.ms[2], &c.ms[3]) != 13)
+            continue;
+        if (tag != gpu || c.variant < 0 || c.variant > 1 || c.persistent < 0 || c.persistent > 1) continue;
+        k.device = device;
+        tune_cache.emplace(k, c);
+    }
+    fclose(fp);
+}
+
+void tune_file_save()
+{
+    const char *path = getenv("SHAPE_B200_TUNING_CACHE");
+    if (!path || !*path) return;
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE *fp = fopen(tmp.c_str(), "w");
+    if (!fp) return;
+    std::map<int, std::string> tags;
+    for (const auto &kv : tune_cache) {
+        const TuneKey &k = kv.first;
+        const TuneChoice &c = kv.second;
+        if (!tags.count(k.device)) tags[k.device] = gpu_tag(k.device);
+        fprintf(fp,
+                "{\"gpu\": \"%s\", \"form\": %d, \"exact\": %d, \"views\": %d, \"facets\": %d, "
+                "\"nonempty\": %d, \"maxcount16\": %d, \"variant\": %d, \"persistent\": %d, "
+                "\"ms\": [%.6g, %.6g, %.6g, %.6g]}\n",
+                tags[k.device].c_str(), k.form, k.exact, k.nviews, k.nf, k.nonempty, k.maxcount, c.variant,
+                c.persistent, c.ms[0], c.ms[1], c.ms[2], c.ms[3]);
+    }
+    fclose(fp);
+    rename(tmp.c_str(), path);
+}
 }  // namespace
 
 // Measures the raster stage of this form with each kernel and grid (one
@@ -1336,6 +1494,7 @@ int EngineImpl::autotune(int form)
                       tuned_nonempty, tuned_max_count / 16};
     {
         std::lock_guard<std::mutex> lk(tune_mu);
+        tune_file_load(device);
         auto it = tune_cache.find(key);
         if (it != tune_cache.end()) {
             raster_variant[form] = it->second.variant;
@@ -1380,6 +1539,7 @@ int EngineImpl::autotune(int form)
     TuneChoice ch{raster_variant[form], raster_persistent[form], {}};
     memcpy(ch.ms, tune_ms[form], sizeof ch.ms);
     tune_cache[key] = ch;
+    tune_file_save();
     return SHAPE_OK;
 }
 
@@ -1408,6 +1568,7 @@ int EngineImpl::finish(shape_eval_summary *out)
         double err = sm.chi2 / sm.dof + sm.penalties;
         if (pending_baddiam) err *= bad_objfactor * exp(pending_bdl);
         if (sm.posbnd) err *= bad_objfactor * exp(sm.posbnd_logfactor);
+        if (sm.badposet) err *= bad_objfactor * exp(sm.badposet_logfactor);
         if (sm.badradar) err *= bad_objfactor * exp(sm.badradar_logfactor);
         sm.objective = err;
     } else if (pending_baddiam) {
@@ -1415,6 +1576,7 @@ int EngineImpl::finish(shape_eval_summary *out)
         const double bdl = pending_bdl;
         sm.objective = sm.chi2 / sm.dof * (bad_objfactor * exp(bdl));
         if (sm.posbnd) sm.objective *= bad_objfactor * exp(sm.posbnd_logfactor);
+        if (sm.badposet) sm.objective *= bad_objfactor * exp(sm.badposet_logfactor);
         if (sm.badradar) sm.objective *= bad_objfactor * exp(sm.badradar_logfactor);
     }
     if (out) *out = sm;
@@ -1438,7 +1600,8 @@ int shape_abi_sizes(size_t *out, int max)
                   sizeof(shape_eval_params), sizeof(shape_deldop_frame), sizeof(shape_deldop_set),
                   sizeof(shape_lghtcrv_point), sizeof(shape_lghtcrv_set), sizeof(shape_deldop_result),
                   sizeof(shape_eval_summary), sizeof(shape_doppler_frame), sizeof(shape_doppler_set),
-                  sizeof(shape_spin_state), sizeof(shape_ephem_point)};
+                  sizeof(shape_spin_state), sizeof(shape_ephem_point), sizeof(shape_poset_frame),
+                  sizeof(shape_poset_set), sizeof(shape_poset_result)};
     int n = (int)(sizeof v / sizeof v[0]);
     for (int i = 0; i < n && i < max; i++) out[i] = v[i];
     return n;
@@ -1709,6 +1872,75 @@ int shape_engine_add_lghtcrv_set(shape_engine *h, const shape_lghtcrv_set *set,
     E.lc.push_back(std::move(L));
     E.finalized = false;
     return (int)E.setrecs.size() - 1;
+}
+
+int shape_engine_add_poset_set(shape_engine *h, const shape_poset_set *set, int nframes,
+                               const shape_poset_frame *frames, const double *obs, const double *oneovervar)
+{
+    if (!h || !set || nframes < 1 || !frames || !obs || !oneovervar)
+        return shape::set_err(SHAPE_E_ARG, "add_poset_set: invalid argument");
+    const int law = set->law.type;
+    if (law != SHAPE_OPTLAW_LAMBERT && law != SHAPE_OPTLAW_LOMMEL && law != SHAPE_OPTLAW_KAASALAINEN)
+        return shape::set_err(SHAPE_E_UNSUPPORTED, "add_poset_set: optical scattering law not supported");
+    if (set->resample == SHAPE_RESAMPLE_BICUBIC)
+        return shape::set_err(SHAPE_E_UNSUPPORTED, "add_poset_set: bicubic resampling is not supported");
+    if (set->resample < SHAPE_RESAMPLE_NONE || set->resample > SHAPE_RESAMPLE_CUBICCONV)
+        return shape::set_err(SHAPE_E_ARG, "add_poset_set: unknown resampling mode");
+    EngineImpl &E = h->impl;
+    shape::PosetHost H;
+    H.set = *set;
+    H.frame0 = E.nps_frames;
+    size_t total = 0;
+    for (int k = 0; k < nframes; k++) {
+        const shape_poset_frame &F = frames[k];
+        if (F.pos_n < 1 || !(F.km_per_pixel > 0) || F.ncol < 2 || F.nrow < 2 || !(F.fit_km_per_pixel > 0))
+            return shape::set_err(SHAPE_E_ARG, "add_poset_set: bad frame size");
+        if (set->resample == SHAPE_RESAMPLE_NONE && fabs(cos(F.northangle)) > 1.0e-10 &&
+            fabs(sin(F.northangle)) > 1.0e-10)
+            return shape::set_err(SHAPE_E_ARG, "add_poset_set: no interpolation with an oblique north angle");
+        total += (size_t)F.ncol * F.nrow;
+        H.frames.push_back(F);
+    }
+    H.obs.assign(obs, obs + total);
+    H.oov.assign(oneovervar, oneovervar + total);
+    for (const shape_poset_frame &F : H.frames) {
+        E.dof += F.dof;
+        E.dof_poset += F.dof;
+    }
+    E.setrecs.push_back(shape::SetRec{2, E.nps_frames, nframes});
+    E.nps_frames += nframes;
+    E.ps.push_back(std::move(H));
+    E.finalized = false;
+    return (int)E.setrecs.size() - 1;
+}
+
+int shape_engine_get_poset(shape_engine *h, int set, int frame, double *fit, double *brightness,
+                           shape_poset_result *result)
+{
+    if (!h) return shape::set_err(SHAPE_E_ARG, "null engine");
+    EngineImpl &E = h->impl;
+    if (E.last_form < 0) return shape::set_err(SHAPE_E_STATE, "no evaluation yet");
+    if (set < 0 || set >= (int)E.setrecs.size() || E.setrecs[set].type != 2)
+        return shape::set_err(SHAPE_E_ARG, "get_poset: not a plane-of-sky set");
+    const shape::SetRec &R = E.setrecs[set];
+    if (frame < 0 || frame >= R.count) return shape::set_err(SHAPE_E_ARG, "get_poset: bad frame");
+    const int g = R.first + frame;
+    const shape::PosetFrameDev &D = E.psf[g];
+    cudaSetDevice(E.device);
+    cudaError_t e = cudaStreamSynchronize(E.stream);
+    if (e == cudaSuccess && fit)
+        e = cudaMemcpy(fit, E.d_ps_fit + D.img_base, sizeof(double) * (size_t)D.ncol * D.nrow,
+                       cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && brightness) {
+        const shape::LcPointDev &P = E.lcpts[D.point];
+        const long long side = 2 * (long long)E.geoms[P.obs_view].n + 1;
+        e = cudaMemcpy(brightness, E.d_ps_b + P.b_base, sizeof(double) * (size_t)(side * side),
+                       cudaMemcpyDeviceToHost);
+    }
+    if (e == cudaSuccess && result)
+        e = cudaMemcpy(result, E.d_ps_res + g, sizeof(shape_poset_result), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return shape::set_err(SHAPE_E_CUDA, std::string("get_poset: ") + cudaGetErrorString(e));
+    return SHAPE_OK;
 }
 
 int shape_engine_finalize(shape_engine *h)
@@ -2102,6 +2334,7 @@ int shape_engine_vary_params(shape_engine *h, const shape_vary_options *opt, dou
     if (!h || !opt || !out) return shape::set_err(SHAPE_E_ARG, "vary_params: null argument");
     EngineImpl &E = h->impl;
     if (!E.finalized) return shape::set_err(SHAPE_E_STATE, "vary_params before finalize");
+    if (!E.ps.empty()) return shape::set_err(SHAPE_E_UNSUPPORTED, "vary_params: plane-of-sky sets");
     const int nsets = (int)E.setrecs.size();
     auto dfree = [&](const int *a, int s) { return a ? a[s] != 0 : false; };
     // the weight sums over every dataset

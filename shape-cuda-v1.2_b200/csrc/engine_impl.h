@@ -69,6 +69,15 @@ struct LcSetHost {
     std::vector<double> x, t, obs, oov;
 };
 
+// A plane-of-sky set as added: its frames (global POS frame numbers from
+// frame0) and their observed images back to back.
+struct PosetHost {
+    shape_poset_set set;
+    std::vector<shape_poset_frame> frames;
+    std::vector<double> obs, oov;
+    int frame0;
+};
+
 struct EngineImpl {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -107,9 +116,11 @@ struct EngineImpl {
     std::vector<double> obs, oov;
     std::vector<LcSetHost> lc;
     std::vector<shape_lghtcrv_point> points;
+    std::vector<PosetHost> ps;          // plane-of-sky sets
+    int nps_frames = 0;
     std::vector<SetRec> setrecs;
     std::vector<RadarLawDev> laws;
-    double dof = 0, dof_deldop = 0, dof_doppler = 0, dof_lghtcrv = 0;
+    double dof = 0, dof_deldop = 0, dof_doppler = 0, dof_lghtcrv = 0, dof_poset = 0;
     std::vector<double> frame_sdev;     // per radar frame: Doppler noise sdev (0 for delay-Doppler)
 
     // derived (host)
@@ -164,6 +175,14 @@ struct EngineImpl {
     double *d_lc_x = nullptr, *d_lc_t = nullptr, *d_lc_obs = nullptr, *d_lc_oov = nullptr;
     double *d_lc_y = nullptr, *d_lc_y2 = nullptr, *d_lc_fit = nullptr, *d_lc_out = nullptr;
     double *d_lc_dof = nullptr, *d_lc_npts = nullptr;
+    // plane-of-sky frames: descriptors, images (obs, 1/var, fit), the sky
+    // renderings' brightness and the per-frame results
+    std::vector<PosetFrameDev> psf;
+    std::vector<shape_lghtcrv_point> ps_points;   // the frames' view geometry, after the lightcurve points
+    long long ps_img_elems = 0, ps_b_elems = 0;
+    PosetFrameDev *d_psf = nullptr;
+    double *d_ps_obs = nullptr, *d_ps_oov = nullptr, *d_ps_fit = nullptr, *d_ps_b = nullptr;
+    shape_poset_result *d_ps_res = nullptr;
     SetRec *d_setrecs = nullptr;
     shape_eval_summary *d_summary_map = nullptr;   // device address of the mapped pinned h_summary
     std::vector<LcSetDev> lcdev;
@@ -271,6 +290,7 @@ struct EngineImpl {
         dd = o.dd; frames = o.frames; frame_off = o.frame_off; obs = o.obs; oov = o.oov;
         fviews = o.fviews;
         lc = o.lc; points = o.points; setrecs = o.setrecs;
+        ps = o.ps; nps_frames = o.nps_frames; dof_poset = o.dof_poset;
         dof = o.dof; dof_deldop = o.dof_deldop; dof_doppler = o.dof_doppler; dof_lghtcrv = o.dof_lghtcrv;
         frame_sdev = o.frame_sdev;
         fixed_cap = o.fixed_cap;

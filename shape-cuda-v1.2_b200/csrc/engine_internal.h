@@ -107,6 +107,18 @@ struct LcPointDev {
     double s_ls, s_l, scale;  // law constants (apply_photo.c:85-133, 226-248)
     double mask_tol;
     double pixels_per_km;     // 1/kmpp
+    long long b_base;         // plane-of-sky frame: offset of its brightness image (-1: a lightcurve point)
+};
+
+// Plane-of-sky frame descriptor (calc_poset's resampling and chi2_poset).
+struct PosetFrameDev {
+    int point;                // its LcPointDev (observer and sun views, brightness image)
+    int ncol, nrow;
+    long long img_base;       // offset of its fit / observed / 1/variance images
+    double x0, xwidth, y0, ywidth;    // resampim's grid (src/shape/calc_fits.c:1278-1287)
+    double cosang, sinang;    // cos and sin of the grid rotation (-northangle), from the C library
+    int mode, rebin;          // SHAPE_RESAMPLE_*, image_rebin
+    double weight, dof;
 };
 
 // Order-preserving 64-bit key of a double (for atomicMin/atomicMax).

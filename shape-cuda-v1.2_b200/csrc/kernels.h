@@ -205,6 +205,7 @@ struct LcArgs {
     void *cose;                 // masked in place, as posmask does
     const int *f, *fill;
     double *partials;           // brightness partial per item
+    double *bimg;               // brightness images of plane-of-sky frames (LcPointDev::b_base)
     unsigned char *seen;
     double mincosine_seen;
     int mark_seen;
@@ -263,7 +264,23 @@ struct SpinRealizeArgs {
 };
 void launch_realize_views(const SpinRealizeArgs &a, cudaStream_t s);
 
-struct SetRec { int type; int first; int count; };   // type 0 deldop (frames), 1 lightcurve (set index)
+struct SetRec { int type; int first; int count; };   // type 0 deldop (frames), 1 lightcurve (set index), 2 plane-of-sky (frames)
+
+// Plane-of-sky frames (calc_poset after apply_photo, and chi2_poset): one
+// block per frame resamples the brightness image onto the fit grid,
+// checks that the grid holds every lit pixel and forms the chi-square.
+struct PosetArgs {
+    int nframes;
+    const PosetFrameDev *frames;
+    const LcPointDev *pts;
+    const FrameGeom *geoms;
+    const FrameState *states;
+    const double *bimg;         // brightness images
+    const double *obs, *oov;    // observed images and 1/variance
+    double *fit;                // fit images
+    shape_poset_result *res;    // per-frame results
+};
+void launch_poset_frames(const PosetArgs &a, cudaStream_t s);
 struct SummaryArgs {
     int nsets;
     const SetRec *sets;
@@ -272,6 +289,9 @@ struct SummaryArgs {
     const double *lc_out;       // per lightcurve set: cal, chi2, posbnd, logfactor sum
     const double *lc_dof;
     const double *lc_npts;
+    const shape_poset_result *ps_res;   // plane-of-sky frames' results
+    const PosetFrameDev *ps_frames;
+    double dof_poset;           // plane-of-sky dof (calc_fits.c:408)
     double dof, dof_radar;      // all data / delay-Doppler + Doppler (calc_fits.c:409)
     double bad_objfactor;
     int baddiam;

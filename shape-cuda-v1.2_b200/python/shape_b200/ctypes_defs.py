@@ -121,6 +121,31 @@ class LghtcrvSet(C.Structure):
     ]
 
 
+class PosetFrame(C.Structure):
+    _fields_ = [
+        ("pos_n", C.c_int), ("km_per_pixel", C.c_double),
+        ("ae", C.c_double * 9), ("oe", C.c_double * 9), ("se", C.c_double * 9),
+        ("solar_phase", C.c_double),
+        ("ncol", C.c_int), ("nrow", C.c_int), ("fit_km_per_pixel", C.c_double),
+        ("colcom_vig", C.c_double), ("rowcom_vig", C.c_double),
+        ("xoff", C.c_double), ("yoff", C.c_double), ("northangle", C.c_double),
+        ("weight", C.c_double), ("dof", C.c_double),
+    ]
+
+
+class PosetSet(C.Structure):
+    _fields_ = [("law", OpticalLaw), ("resample", C.c_int), ("rebin", C.c_int)]
+
+
+class PosetResult(C.Structure):
+    _fields_ = [
+        ("outbnd", C.c_int), ("posbnd_logsum", C.c_double),
+        ("badposet", C.c_int), ("badposet_logfactor", C.c_double),
+        ("o2", C.c_double), ("m2", C.c_double), ("om", C.c_double),
+        ("cal", C.c_double), ("chi2", C.c_double),
+    ]
+
+
 class DeldopResult(C.Structure):
     _fields_ = [
         ("outbnd", C.c_int), ("posbnd_logfactor", C.c_double),

@@ -73,7 +73,8 @@ class EvalSummary(C.Structure):
     _fields_ = [("chi2", C.c_double), ("dof", C.c_double), ("chi2_deldop", C.c_double),
                 ("chi2_lghtcrv", C.c_double), ("posbnd", C.c_int), ("posbnd_logfactor", C.c_double),
                 ("badradar", C.c_int), ("badradar_logfactor", C.c_double), ("objective", C.c_double),
-                ("penalties", C.c_double)]
+                ("penalties", C.c_double), ("chi2_poset", C.c_double), ("badposet", C.c_int),
+                ("badposet_logfactor", C.c_double)]
 
 
 ABI_ORDER = ["shape_model_desc", "shape_radar_law", "shape_optical_law", "shape_eval_params",
@@ -110,6 +111,8 @@ def load_library(path=LIB_PATH):
     L.shape_engine_get_radar_overflow.argtypes = [vp, cd.dptr, C.c_int]
     L.shape_engine_finalize.argtypes = [vp]
     L.shape_engine_get_active.argtypes = [vp, vp, vp]
+    L.shape_engine_add_poset_set.argtypes = [vp, P(cd.PosetSet), C.c_int, P(cd.PosetFrame), cd.dptr, cd.dptr]
+    L.shape_engine_get_poset.argtypes = [vp, C.c_int, C.c_int, cd.dptr, cd.dptr, P(cd.PosetResult)]
     L.shape_engine_set_scale.argtypes = [vp, C.c_int, C.c_double]
     L.shape_engine_set_vertex_r.argtypes = [vp, C.c_int, C.c_double]
     L.shape_engine_get_vertex_r.argtypes = [vp, C.c_int, P(C.c_double)]
@@ -203,9 +206,9 @@ def load_library(path=LIB_PATH):
 
 def abi_sizes():
     L = load_library()
-    out = (C.c_size_t * 16)()
-    n = L.shape_abi_sizes(out, 16)
-    return [out[i] for i in range(n)]
+    out = (C.c_size_t * 32)()
+    n = L.shape_abi_sizes(out, 32)
+    return [out[i] for i in range(min(n, 32))]
 
 
 class EngineError(RuntimeError):
@@ -231,6 +234,7 @@ class Engine:
         _chk(self.L.shape_engine_create(device, C.byref(h)))
         self.h = h
         self.deldops, self.lghtcrvs, self.set_index = [], [], []
+        self.posets = []
         self.model = None
         self._keep = []
 
@@ -294,6 +298,31 @@ class Engine:
         self.lghtcrvs.append(ds)
         self.set_index.append(("lghtcrv", len(self.lghtcrvs) - 1))
         return idx
+
+    def add_poset(self, ds):
+        """A plane-of-sky set (synth.PosetDataset)."""
+        st, frames, obs, oov = ds.bind()
+        self._keep.extend([frames, obs, oov])
+        idx = _chk(self.L.shape_engine_add_poset_set(self.h, C.byref(st), len(ds.frames), frames,
+                                                     cd.as_dptr(obs), cd.as_dptr(oov)))
+        self.posets.append(ds)
+        self.set_index.append(("poset", len(self.posets) - 1))
+        return idx
+
+    def poset(self, set_idx, frame):
+        """(fit image [ncol, nrow], brightness image [2n+1, 2n+1], results dict)
+        of a plane-of-sky frame after the last evaluation."""
+        kind, k = self.set_index[set_idx]
+        assert kind == "poset", kind
+        ds = self.posets[k]
+        fr = ds.frames[frame]
+        fit = np.zeros((fr["ncol"], fr["nrow"]))
+        side = 2 * fr["pos_n"] + 1
+        b = np.zeros((side, side))
+        r = cd.PosetResult()
+        _chk(self.L.shape_engine_get_poset(self.h, int(set_idx), int(frame), cd.as_dptr(fit), cd.as_dptr(b),
+                                           C.byref(r)))
+        return fit, b, {k: getattr(r, k) for k, _ in cd.PosetResult._fields_}
 
     def finalize(self):
         _chk(self.L.shape_engine_finalize(self.h))
@@ -823,8 +852,8 @@ def realize_spin(spin, t, orbspin=None, angleoff=(0.0, 0.0, 0.0), omegaoff=(0.0,
     return ae, sp
 
 
-def make_engine(model, params, deldops=(), lghtcrvs=(), device=0, dopplers=()):
-    """An engine with the sets added in the order deldops, dopplers, lightcurves."""
+def make_engine(model, params, deldops=(), lghtcrvs=(), device=0, dopplers=(), posets=()):
+    """An engine with the sets added in the order deldops, dopplers, lightcurves, plane-of-sky sets."""
     e = Engine(device)
     e.set_model(model)
     e.set_params(params)
@@ -834,6 +863,8 @@ def make_engine(model, params, deldops=(), lghtcrvs=(), device=0, dopplers=()):
         e.add_doppler(ds)
     for ds in lghtcrvs:
         e.add_lghtcrv(ds)
+    for ds in posets:
+        e.add_poset(ds)
     e.finalize()
     return e
 

@@ -647,6 +647,78 @@ def lightcurve_dataset(npoints=200, pos_range=(129, 257), synthesize=None, param
     return ds
 
 
+class PosetDataset:
+    """A plane-of-sky set: frames (dicts of shape_poset_frame's fields; ae,
+    oe, se as 3x3), the optical law, the resampling mode and rebinning, and
+    the frames' observed images and 1/variance back to back (ncol x nrow,
+    row index contiguous)."""
+
+    def __init__(self, frames, law, resample, rebin, obs, oneovervar):
+        self.frames, self.law, self.resample, self.rebin = frames, law, resample, rebin
+        self.obs, self.oneovervar = obs, oneovervar
+        sizes = [f["ncol"] * f["nrow"] for f in frames]
+        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+
+    @property
+    def nframes(self):
+        return len(self.frames)
+
+    def bind(self):
+        st = cd.PosetSet()
+        st.law, st.resample, st.rebin = self.law, int(self.resample), int(self.rebin)
+        arr = (cd.PosetFrame * len(self.frames))()
+        for k, f in enumerate(self.frames):
+            c = arr[k]
+            for key, val in f.items():
+                if key in ("ae", "oe", "se"):
+                    cd.fill9(getattr(c, key), val)
+                else:
+                    setattr(c, key, val)
+        return st, arr, np.ascontiguousarray(self.obs, dtype=np.float64), \
+            np.ascontiguousarray(self.oneovervar, dtype=np.float64)
+
+
+def poset_dataset(nframes=2, synthesize=None, params=None, pos_n=60, ncol=44, nrow=38, fit_scale=1.9,
+                  resample=2, rebin=False, northangle=0.35, offsets=(1.3, -0.7), radius=1.0, seed=5,
+                  law_type=3, northangle_step=0.2):
+    """A plane-of-sky set of the config-1 body: sky renderings of (2 pos_n + 1)^2
+    pixels spanning the body, resampled onto ncol x nrow fit images whose
+    pixels are fit_scale rendering pixels wide, turned by the north angle
+    and shifted by the COM offsets (fit-grid pixels); frame k's north angle
+    is northangle + k northangle_step. Observed images: A *
+    fit / max(fit) + N(0, 1) from synthesize(ds, params) (a list of fit
+    images), or zeros."""
+    rng = np.random.default_rng(seed)
+    pole = ecl_dir(30.0, 60.0)
+    frames = []
+    for k in range(nframes):
+        to_earth = ecl_dir(15.0 + 40.0 * k, 10.0 - 5.0 * k)
+        alpha = float(rng.uniform(10.0, 50.0)) * DEG
+        axis = np.cross(to_earth, [0.0, 0.0, 1.0])
+        to_sun = rotate_about(to_earth, axis, alpha)
+        kmpp = 2.2 * radius / (2 * pos_n + 1)
+        frames.append({
+            "pos_n": pos_n, "km_per_pixel": kmpp,
+            "ae": body_matrix(pole, 0.9 * k), "oe": observer_matrix(to_earth), "se": observer_matrix(to_sun),
+            "solar_phase": alpha, "ncol": ncol, "nrow": nrow, "fit_km_per_pixel": fit_scale * kmpp,
+            "colcom_vig": (ncol + 1) / 2.0 + 0.25 * k, "rowcom_vig": (nrow + 1) / 2.0 - 0.4 * k,
+            "xoff": float(offsets[0]), "yoff": float(offsets[1]), "northangle": northangle + northangle_step * k,
+            "weight": 1.0, "dof": float(ncol * nrow),
+        })
+    law = cd.OpticalLaw()
+    law.type, law.R, law.wt, law.A0, law.D, law.k = law_type, 1.0, 0.3, 0.0, 0.1, 0.0
+    total = sum(f["ncol"] * f["nrow"] for f in frames)
+    ds = PosetDataset(frames, law, resample, rebin, np.zeros(total), np.ones(total))
+    if synthesize is not None:
+        fits = synthesize(ds, params or eval_params())
+        nrng = np.random.default_rng(1234 + seed)
+        for k, fit in enumerate(fits):
+            a, b = ds.offsets[k], ds.offsets[k + 1]
+            f = np.asarray(fit, dtype=np.float64).ravel()
+            ds.obs[a:b] = 20.0 * f / max(f.max(), 1e-300) + nrng.standard_normal(b - a)
+    return ds
+
+
 def config3_datasets(synthesize=None, params=None, npoints=200):
     return [lightcurve_dataset(npoints, (129, 257), synthesize, params, set_index=k) for k in range(4)]
 

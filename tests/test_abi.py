@@ -43,6 +43,9 @@ def test_struct_layouts_match_compiler():
         assert C.sizeof(cd.STRUCTS[name]) == sizes[len(eng.ABI_ORDER) + 1 + k], name
     assert C.sizeof(cd.SpinState) == sizes[len(eng.ABI_ORDER) + 3], "shape_spin_state"
     assert C.sizeof(cd.EphemPoint) == sizes[len(eng.ABI_ORDER) + 4], "shape_ephem_point"
+    assert C.sizeof(cd.PosetFrame) == sizes[len(eng.ABI_ORDER) + 5], "shape_poset_frame"
+    assert C.sizeof(cd.PosetSet) == sizes[len(eng.ABI_ORDER) + 6], "shape_poset_set"
+    assert C.sizeof(cd.PosetResult) == sizes[len(eng.ABI_ORDER) + 7], "shape_poset_result"
 
 
 def test_errors_without_device_are_reported():

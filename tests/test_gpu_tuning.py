@@ -70,3 +70,48 @@ def test_choice_is_shared_by_size_class(cuda_device):
         e2.evaluate(eng.FORM_BATCHED_FP32)["chi2"], rel=1e-6)
     e1.close()
     e2.close()
+
+
+_TUNE_SNIPPET = r"""
+import json, os, sys
+sys.path.insert(0, os.environ["REPO"]); sys.path.insert(0, os.path.join(os.environ["REPO"], "tests"))
+sys.path.insert(0, os.path.join(os.environ["REPO"], "shape-cuda-v1.2_b200", "python"))
+import cases
+from shape_b200 import engine as eng
+m, p, ds = cases.c2(12)
+e = eng.make_engine(m, p, deldops=[ds])
+e.evaluate(eng.FORM_BATCHED_FP32)
+print(json.dumps(e.raster_tuning(eng.FORM_BATCHED_FP32)))
+e.close()
+"""
+
+
+def test_tuning_file_carries_choices(cuda_device, tmp_path):
+    """SHAPE_B200_TUNING_CACHE: the first process times the candidates and
+    writes its choice for the size class; a second process reads the file
+    and takes the same choice and times without timing again."""
+    import json
+    import os
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    path = tmp_path / "tuning.jsonl"
+    env = dict(os.environ, REPO=repo, SHAPE_B200_TUNING_CACHE=str(path))
+    runs = []
+    for _ in range(2):
+        out = subprocess.run([sys.executable, "-c", _TUNE_SNIPPET], env=env, capture_output=True, text=True,
+                             timeout=600)
+        assert out.returncode == 0, out.stderr[-2000:]
+        runs.append(json.loads(out.stdout.strip().splitlines()[-1]))
+    lines = path.read_text().splitlines()
+    assert len(lines) == 1, lines
+    rec = json.loads(lines[0])
+    assert rec["form"] == eng.FORM_BATCHED_FP32 and rec["views"] == ds_views(), rec
+    a, b = runs
+    assert a["tuned"] and b["tuned"]
+    assert (a["variant"], a["persistent"]) == (b["variant"], b["persistent"]) == (rec["variant"], rec["persistent"])
+    np.testing.assert_allclose(b["ms"], rec["ms"], rtol=1e-5)
+
+
+def ds_views():
+    return cases.c2(12)[2].nframes
