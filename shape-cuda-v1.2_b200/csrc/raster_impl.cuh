@@ -413,6 +413,7 @@ template <typename T>
 struct PixDD {
     T delPOS, dopPOS, codefactor;
     T ddel0, ddop0, dfrac;     // FP32 form: delPOS - idel_min, dopPOS - idop_min, frac(dopPOS) from FP64
+    int ifl;                   // FP32 form: floor(dopPOS) from FP64; column idop's offset is dfrac + (ifl - idop)
     int idel_min, idel_max, idop_min, idop_max;
     bool ok;   // in_bounds: the whole footprint lies inside the frame
 };
@@ -460,6 +461,7 @@ __device__ inline PixDD<float> pixel_dd_setup_x(const FrameGeom &g, int x, int y
     d.ddel0 = (float)(del - (double)d.idel_min);
     d.ddop0 = (float)(dop - (double)d.idop_min);
     d.dfrac = (float)(dop - floor(dop));
+    d.ifl = (int)floor(dop);
     d.codefactor = ((g.codemethod == SHAPE_CODE_SHORT) ? sinc2<float>((float)((dop - g.dopDC_vig) / g.dopfftlen))
                                                         : 1.0f) * (float)g.wscale;
     pp.del = del;
@@ -572,17 +574,21 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
     const T delPOS = d.delPOS, dopPOS = d.dopPOS;
     const int idel_min = d.idel_min, idel_max = d.idel_max, idop_min = d.idop_min, idop_max = d.idop_max;
     const int nr = idel_max - idel_min + 1, nc = idop_max - idop_min + 1;
+    // FP32 form: the offsets from the FP64 positions (frac + integer)
+    constexpr bool f32 = sizeof(T) == 4;
     T s2u = 0;
     if (g.nsinc2 == 1) {
-        const T su = tsin<T>((T)3.141592653589793 * (dopPOS - floor(dopPOS)));
+        const T su = tsin<T>((T)3.141592653589793 * (f32 ? d.dfrac : (dopPOS - floor(dopPOS))));
         s2u = su * su;
     }
+    auto ddop_of = [&](int idop) -> T { return f32 ? d.dfrac + (T)(d.ifl - idop) : dopPOS - (T)idop; };
+    auto ddel_of = [&](int idel) -> T { return f32 ? d.ddel0 - (T)(idel - idel_min) : delPOS - (T)idel; };
     const T kmpp = k.kmpp;
     const T rl = radlaw_dev<T>(a.laws[g.law], cose) * kmpp * kmpp * d.codefactor;
     if (nr <= FAST_ROWS && nc <= FAST_COLS) {
         T dc[FAST_ROWS], pc[FAST_COLS];
         T sdel = 0, sdop = 0;
-        const T ddel0 = delPOS - (T)idel_min, ddop0 = dopPOS - (T)idop_min;
+        const T ddel0 = ddel_of(idel_min), ddop0 = dopPOS - (T)idop_min;
         // the common responses (LONG_ORIG or spb = 1, nsinc2 = 1) written
         // out with del_resp / dop_resp's own operations, so the same values
         if (g.nsinc2 == 1 && (g.codemethod == SHAPE_CODE_LONG_ORIG || g.spb == 1)) {
@@ -594,7 +600,7 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
             }
 #pragma unroll
             for (int c = 0; c < FAST_COLS; c++) {
-                const T t = fabs((T)3.141592653589793 * (ddop0 - (T)c));
+                const T t = fabs((T)3.141592653589793 * (f32 ? ddop_of(idop_min + c) : ddop0 - (T)c));
                 pc[c] = (c < nc) ? ((t > (T)1.0e-4) ? s2u / (t * t) : (T)1.0) : (T)0;
                 if (c < nc) sdop += pc[c];
             }
@@ -606,7 +612,8 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
             }
 #pragma unroll
             for (int c = 0; c < FAST_COLS; c++) {
-                pc[c] = (c < nc) ? dop_resp<T>(g, k, dopPOS, ddop0 - (T)c, s2u, idop_min + c) : (T)0;
+                pc[c] = (c < nc) ? dop_resp<T>(g, k, dopPOS, f32 ? ddop_of(idop_min + c) : ddop0 - (T)c, s2u,
+                                               idop_min + c) : (T)0;
                 if (c < nc) sdop += pc[c];
             }
         }
@@ -626,9 +633,9 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
     T del_c[SHAPE_MAXBINS];
     T dop_c[SHAPE_MAXBINS + 1];
     for (int idel = idel_min; idel <= idel_max; idel++)
-        del_c[idel - idel_min] = del_resp<T>(g, k, delPOS, delPOS - (T)idel, idel);
+        del_c[idel - idel_min] = del_resp<T>(g, k, delPOS, ddel_of(idel), idel);
     for (int idop = idop_min; idop <= idop_max; idop++)
-        dop_c[min(idop - idop_min, SHAPE_MAXBINS)] = dop_resp<T>(g, k, dopPOS, dopPOS - (T)idop, s2u, idop);
+        dop_c[min(idop - idop_min, SHAPE_MAXBINS)] = dop_resp<T>(g, k, dopPOS, ddop_of(idop), s2u, idop);
     T sdel = 0, sdop = 0;
     for (int idel = idel_min; idel <= idel_max; idel++) sdel += del_c[idel - idel_min];
     for (int idop = idop_min; idop <= idop_max; idop++) sdop += dop_c[min(idop - idop_min, SHAPE_MAXBINS)];
@@ -705,12 +712,16 @@ __device__ inline void pixel_dd_scatter_f32_direct(const RasterArgs &a, const Fr
         dc[r] = (r < nr) ? tri2<float>(__fdividef(ddel0 - (float)r, sos)) : 0.0f;
         if (r < nr) sdel += dc[r];
     }
+    // the Doppler offset of column c as frac + integer: exact to a float's
+    // rounding of its own size, also for the columns next to the pixel
+    const int i0 = d.ifl - d.idop_min;
 #pragma unroll
     for (int c = 0; c < FAST_COLS; c++) {
-        const float t = fabsf(3.141592653589793f * (ddop0 - (float)c));
+        const float t = fabsf(3.141592653589793f * (d.dfrac + (float)(i0 - c)));
         pc[c] = (c < nc) ? ((t > 1.0e-4f) ? __fdividef(s2u, t * t) : 1.0f) : 0.0f;
         if (c < nc) sdop += pc[c];
     }
+    (void)ddop0;
     const float amp = __fdividef(rl, sdel * sdop);
 #pragma unroll
     for (int r = 0; r < FAST_ROWS; r++) {
@@ -742,7 +753,7 @@ __device__ RARE_FN void pixel_dop_overflow(const RasterArgs &a, const FrameGeom 
     T dop_c[SHAPE_MAXBINS + 1];
     for (int idop = idop_min; idop <= idop_max; idop++) {
         T ddop;
-        if constexpr (sizeof(T) == 4) ddop = d.ddop0 - (T)(idop - idop_min); else ddop = d.dopPOS - (T)idop;
+        if constexpr (sizeof(T) == 4) ddop = d.dfrac + (T)(d.ifl - idop); else ddop = d.dopPOS - (T)idop;
         dop_c[min(idop - idop_min, SHAPE_MAXBINS)] = dop_resp<T>(g, k, d.dopPOS, ddop, s2u, idop);
     }
     T sdop = 0;
