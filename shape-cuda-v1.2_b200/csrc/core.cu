@@ -1300,6 +1300,23 @@ void launch_chi2_partials(const Chi2Args &a, int fp32, cudaStream_t s)
     else k_chi2_partials<double><<<blocks, CHI2_THREADS, 0, s>>>(a);
 }
 
+// FP32 form: each Doppler frame's FP64 sums rounded once into its float
+// fit bins.
+__global__ void k_dop_fit_f32(const int *dop_frames, const FrameHost *fh, const FrameGeom *geoms,
+                              const double *fit64, float *fit32)
+{
+    const FrameGeom &g = geoms[fh[dop_frames[blockIdx.x]].view];
+    const long long n = (long long)g.ndel * g.ndop;
+    for (long long j = threadIdx.x; j < n; j += blockDim.x) fit32[g.fit_base + j] = (float)fit64[g.fit_base + j];
+}
+
+void launch_dop_fit_f32(const int *dop_frames, int n, const FrameHost *fh, const FrameGeom *geoms,
+                        const double *fit64, float *fit32, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_dop_fit_f32<<<n, 256, 0, s>>>(dop_frames, fh, geoms, fit64, fit32);
+}
+
 void launch_doppler_overflow(const DopOvfArgs &a, cudaStream_t s)
 {
     if (a.n <= 0) return;

@@ -1090,7 +1090,8 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     launch_reset_state(d_states, nviews, d_bin_count, ntiles, sr);
     if (fit_elems) {
         if (f32) CK(cudaMemsetAsync(d_fit32, 0, sizeof(float) * fit_elems, sr));
-        else CK(cudaMemsetAsync(d_fit64, 0, sizeof(double) * fit_elems, sr));
+        // the FP32 form sums Doppler spectra in FP64 (then rounds them once)
+        if (!f32 || !dop_frames.empty()) CK(cudaMemsetAsync(d_fit64, 0, sizeof(double) * fit_elems, sr));
     }
     CK(cudaMemsetAsync(d_seen, 0, nf, sr));
     if (!dop_frames.empty())
@@ -1115,6 +1116,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
     ra.states = d_states;
     ra.laws = d_laws;
     ra.fit = f32 ? (void *)d_fit32 : (void *)d_fit64;
+    ra.fit64 = d_fit64;
     ra.pos_z = d_pos_z; ra.pos_cose = d_pos_cose; ra.pos_cosi = d_pos_cosi; ra.pos_f = d_pos_f;
     ra.seen = d_seen;
     ra.mincosine_seen = params.mincosine_seen;
@@ -1211,6 +1213,7 @@ int EngineImpl::enqueue(int form, cudaEvent_t *marks)
             rl.grid = raster_grid(form, nonempty_lc, rl, true);
             launch_raster_f32(rr, s);
             launch_raster_f32(rl, s);
+            launch_dop_fit_f32(d_dop_frames, (int)dop_frames.size(), d_fh, d_geoms, d_fit64, d_fit32, s);
         } else {
             ra.nwork = (int)work.size();
             ra.grid = raster_grid(form, tuned_nonempty, ra, false);
@@ -1306,6 +1309,8 @@ int EngineImpl::kernels_per_eval(int form) const
         n += 3;                          // transform, bin, raster
         if (form == SHAPE_FORM_BATCHED_FP32 && work_radar > 0 && work_radar < (int)work.size())
             n += 1;                      // FP32: radar and lightcurve views in two launches
+        if (form == SHAPE_FORM_BATCHED_FP32 && !dop_frames.empty())
+            n += 1;                      // FP32: Doppler spectra rounded from their FP64 sums
         n += (chi2_items.empty() || fused_chi2) ? 0 : 1;   // fused: counted with the summary
         n += lc_items.empty() ? 0 : 1;
     }

@@ -71,6 +71,7 @@ struct RasterArgs {
     FrameState *states;
     const RadarLawDev *laws;
     void *fit;                 // T image arena (radar views)
+    double *fit64;             // FP32 form: FP64 sums of the one-row (Doppler) frames, at their fit offsets
     void *pos_z, *pos_cose, *pos_cosi;  // POS maps: z double, cos(e) / cos(i) T (keep_pos or lightcurves)
     int *pos_f;
     unsigned char *seen;
@@ -190,6 +191,10 @@ struct DopOvfArgs {
     const double *ovf;          // overflow spectra
     double *out;                // [n * DOP_OVF_TERMS]
 };
+// FP32 form: the Doppler frames' FP64 sums rounded into the float fit
+// images the chi-square reads (one block per Doppler frame).
+void launch_dop_fit_f32(const int *dop_frames, int n, const FrameHost *fh, const FrameGeom *geoms,
+                        const double *fit64, float *fit32, cudaStream_t s);
 void launch_doppler_overflow(const DopOvfArgs &a, cudaStream_t s);
 
 struct LcArgs {

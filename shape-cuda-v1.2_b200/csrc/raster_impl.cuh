@@ -567,9 +567,9 @@ constexpr int FAST_COLS = 8;
 // most FAST_ROWS x FAST_COLS bins (the common LONG_ORIG spb=1 / nsinc2=1 /
 // sinc2width<=7 case) keep their weights in registers and scatter through
 // fully unrolled, predicated loops, so the lanes of a warp stay converged.
-template <typename T>
+template <typename T, typename A = T>
 __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const DDC<T> &k, T cose,
-                                 const PixDD<T> &d, T *dst, int row0, int col0, int stride)
+                                 const PixDD<T> &d, A *dst, int row0, int col0, int stride)
 {
     const T delPOS = d.delPOS, dopPOS = d.dopPOS;
     const int idel_min = d.idel_min, idel_max = d.idel_max, idop_min = d.idop_min, idop_max = d.idop_max;
@@ -623,10 +623,10 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
 #pragma unroll
         for (int r = 0; r < FAST_ROWS; r++) {
             const T ad = amp * dc[r];
-            T *row = dst + (long long)(idel_min + r - row0) * stride + (idop_min - col0);
+            A *row = dst + (long long)(idel_min + r - row0) * stride + (idop_min - col0);
 #pragma unroll
             for (int c = 0; c < FAST_COLS; c++)
-                if (r < nr && c < nc) atomic_add_any<T>(row + c, ad * pc[c]);
+                if (r < nr && c < nc) atomic_add_any<A>(row + c, (A)(ad * pc[c]));
         }
         return;
     }
@@ -642,15 +642,25 @@ __device__ void pixel_dd_scatter(const RasterArgs &a, const FrameGeom &g, const 
     const T amp = rl / (sdel * sdop);
     for (int idel = idel_min; idel <= idel_max; idel++) {
         T ad = amp * del_c[idel - idel_min];
-        T *row = dst + (long long)(idel - row0) * stride - col0;
+        A *row = dst + (long long)(idel - row0) * stride - col0;
         for (int idop = idop_min; idop <= idop_max; idop++)
-            atomic_add_any<T>(row + idop, ad * dop_c[min(idop - idop_min, SHAPE_MAXBINS)]);
+            atomic_add_any<A>(row + idop, (A)(ad * dop_c[min(idop - idop_min, SHAPE_MAXBINS)]));
     }
 }
 
 // The FP32 raster's general scatter (footprints beyond the fast path's, or
 // responses other than its two), kept out of line so its arrays and
 // constants do not raise the fast path's register use.
+// FP32 form, one-row (Doppler) frames: the FP32 weights added in FP64
+// (fit64 at the frame's offset): every lit pixel of a spectrum lands in
+// the same few hundred bins, so float sums would round thousands of times
+// per bin.
+static __device__ RARE_FN void pixel_dop_scatter_f32_64(const RasterArgs &a, const FrameGeom &g,
+                                                       const DDC<float> &k, float cose, const PixDD<float> &d)
+{
+    pixel_dd_scatter<float, double>(a, g, k, cose, d, a.fit64 + g.fit_base, 1, 1, g.ndop);
+}
+
 static __device__ RARE_FN void pixel_dd_scatter_f32_generic(const RasterArgs &a, const FrameGeom &g,
                                                            const DDC<float> &k, float cose, const PixDD<float> &d,
                                                            float *fit)
@@ -1445,9 +1455,10 @@ k_raster(RasterArgs a)
         // 16-byte vector reductions, FP64 as scalar atomics (both measured
         // faster than a shared-memory accumulator flushed per tile).
         if (g.kind == VIEW_RADAR && dd.ok) {
-            if constexpr (sizeof(T) == 4)
-                pixel_dd_scatter_f32_direct(a, g, kc, scose, dd, static_cast<float *>(a.fit) + g.fit_base);
-            else
+            if constexpr (sizeof(T) == 4) {
+                if (g.dop1d) pixel_dop_scatter_f32_64(a, g, kc, scose, dd);
+                else pixel_dd_scatter_f32_direct(a, g, kc, scose, dd, static_cast<float *>(a.fit) + g.fit_base);
+            } else
                 pixel_dd_scatter<T>(a, g, kc, scose, dd, static_cast<T *>(a.fit) + g.fit_base, 1, 1, g.ndop);
         } else if (g.kind == VIEW_RADAR && g.dop1d && lit) {
             a.states[item.x].any_overflow = 1;
@@ -1816,9 +1827,10 @@ k_raster_w(RasterArgs a)
                 if (!*(volatile int *)&S.any_lit) S.any_lit = 1;
             }
             if (dd.ok) {
-                if constexpr (sizeof(T) == 4)
-                    pixel_dd_scatter_f32_direct(a, g, kc, cosa, dd, static_cast<float *>(a.fit) + g.fit_base);
-                else
+                if constexpr (sizeof(T) == 4) {
+                    if (g.dop1d) pixel_dop_scatter_f32_64(a, g, kc, cosa, dd);
+                    else pixel_dd_scatter_f32_direct(a, g, kc, cosa, dd, static_cast<float *>(a.fit) + g.fit_base);
+                } else
                     pixel_dd_scatter<T>(a, g, kc, cosa, dd, static_cast<T *>(a.fit) + g.fit_base, 1, 1, g.ndop);
             } else if (g.dop1d && lit) {
                 S.any_overflow = 1;
