@@ -457,14 +457,19 @@ def per_config(lrank, flush, budget_cpu_s=3.0):
         nu = units(dds, lcs)
         E = eng.make_engine(model, params, deldops=dds, lghtcrvs=lcs, device=lrank)
         rng = np.random.default_rng(17)
-        worst = 0.0
+        worst = worst_frame = 0.0
         for k in range(4):
             sc = [1.0, 1.0, 1.0] if k == 0 else list(1.0 + 0.02 * rng.uniform(-1, 1, 3))
             for j in range(3):
                 E.set_scale(j, sc[j])
             c64 = E.evaluate(eng.FORM_BATCHED_FP64)["chi2"]
+            r64 = E.results() if dds else []
             c32 = E.evaluate(eng.FORM_BATCHED_FP32)["chi2"]
+            r32 = E.results() if dds else []
             worst = max(worst, abs(c32 - c64) / abs(c64))
+            for a, b in zip(r64, r32):
+                if a["chi2"] != 0.0:
+                    worst_frame = max(worst_frame, abs(b["chi2"] - a["chi2"]) / abs(a["chi2"]))
         for j in range(3):
             E.set_scale(j, 1.0)
         for k in range(3):
@@ -486,6 +491,7 @@ def per_config(lrank, flush, budget_cpu_s=3.0):
                      "p50_ms": statistics.median(dev), "p99_ms": float(np.percentile(dev, 99)),
                      "raster_ms": rs_ms, "roofline_frac": rs_bytes / (rs_ms / 1e3) / 1e9 / peak,
                      "max_dchi2_rel_fp32_vs_fp64": worst,
+                     "max_dchi2_rel_per_frame_fp32_vs_fp64": worst_frame if dds else None,
                      "cpu_reference_frame_evals_per_s": cpu["value"], "cpu_cores": cpu["cores"]}
     # config 4: the vertex-deviation sweep over its first parameters
     params = synth.eval_params()
@@ -559,8 +565,14 @@ def main():
     # accuracy of the batched FP32 form against FP64 on the same trial model
     E.set_scale(0, trial(0))
     chi64 = E.evaluate(eng.FORM_BATCHED_FP64)["chi2"]
+    r64 = E.results() if dds else []
     chi32 = E.evaluate(eng.FORM_BATCHED_FP32)["chi2"]
+    r32 = E.results() if dds else []
     dchi = abs(chi32 - chi64) / abs(chi64)
+    # the same error frame by frame (each frame's chi-square, FP32 against FP64)
+    per_frame = [abs(b["chi2"] - a["chi2"]) / abs(a["chi2"]) for a, b in zip(r64, r32) if a["chi2"] != 0.0]
+    dchi_frames = ({"frames": len(per_frame), "max": max(per_frame), "median": statistics.median(per_frame)}
+                   if per_frame else None)
 
     ev_a = torch.cuda.Event(enable_timing=True)
     ev_b = torch.cuda.Event(enable_timing=True)
@@ -661,6 +673,7 @@ def main():
                    "model_facets": model.nf, "l2": "flushed (2x L2 buffer written) before every step",
                    "parallelism": "frame shards, one per GPU" if ws > 1 else "single GPU",
                    "dchi2_rel_fp32_vs_fp64": dchi,
+                   "dchi2_rel_per_frame_fp32_vs_fp64": dchi_frames,
                    "plain_fp64_frame_evals_per_s": plain_rate,
                    "batched_over_plain_fp64": value / ws / plain_rate,
                    "fp32_fast_option": fast,
