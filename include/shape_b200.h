@@ -720,8 +720,26 @@ void shape_obs_free(shape_obs_file *o);
 int shape_obs_nsets(const shape_obs_file *o);
 /* 0: set s is a delay-Doppler set (shape_obs_set / shape_obs_frames);
  * 1: a Doppler set (shape_obs_doppler); 2: a lightcurve or heliocurve set
- * (shape_obs_lghtcrv_info / shape_obs_lghtcrv). */
+ * (shape_obs_lghtcrv_info / shape_obs_lghtcrv); 3: a plane-of-sky set
+ * (shape_obs_poset_info / shape_obs_poset). */
 int shape_obs_set_type(const shape_obs_file *o, int s);
+/* A plane-of-sky set (read_poset, src/shape/read_dat.c:1392-1560): its
+ * optical law index and frame count; each frame's image file (the data
+ * directory joined with its name) and pixel-weighting flag. The images are
+ * FITS files, which this library does not read (cfitsio is not part of
+ * it); the caller reads them. */
+int shape_obs_poset_info(const shape_obs_file *o, int s, int *ioptlaw, int *nframes);
+int shape_obs_poset_file(const shape_obs_file *o, int s, int frame, char *path, int size, int *pixels_weighted);
+/* The geometry of the set's frames (one view per frame): oe, se and the
+ * solar phase by ephem2mat at the frame epoch (light-time corrected when
+ * opt->perform_ltc is set), ae from the spin model at that epoch, the fit
+ * grid's km per pixel (angular pixel size times the distance before the
+ * light-time correction, as read_poset computes it), the north angle, the
+ * COM offsets and the weight. pos_n, km_per_pixel, ncol, nrow, colcom_vig,
+ * rowcom_vig and dof are left as the caller set them (set_up_pos and the
+ * image). Smeared plane-of-sky frames return SHAPE_E_UNSUPPORTED. */
+int shape_obs_poset(const shape_obs_file *o, int s, const shape_spin_state *spin, const shape_obs_options *opt,
+                    shape_poset_frame *frames);
 /* Set s's radar setup (set->law is kept: take it from the model's radar
  * law iradlaw), its frame count, angle and spin offsets (rad, rad/day) and
  * the number of data elements of its frames. iradlaw is >= 0 (a negative

@@ -787,6 +787,15 @@ struct shape_obs_file {
         char lc_cal_state = 'c';
         double lc_cal = 0.0, lc_weight = 0.0;
         std::vector<double> lc_t0, lc_mag, lc_magerr;   // the data file's points
+        // plane-of-sky sets (read_poset, src/shape/read_dat.c:1392-1560)
+        int poset = 0;
+        double angle_per_pixel = 0.0;    // radians
+        struct PosFrame {
+            std::string name;            // image file (FITS) in dir
+            double t0, northangle, off[2], weight;
+            int pixels_weighted;
+        };
+        std::vector<PosFrame> pframes;
     };
     std::vector<Set> sets;
     std::string maskdir;                 // "" : the sets' data directories
@@ -806,6 +815,49 @@ static std::vector<shape_ephem_point> read_ephem(Tokens &tk, const char *what)
         v[i].dist = tk.real("distance");
     }
     return v;
+}
+
+// The body of a plane-of-sky set (read_poset,
+// src/shape/read_dat.c:1392-1460): optical law, the asteroid's and the
+// Sun's ephemerides, the angular pixel size (arcsec), the smearing line,
+// the data directory and per frame its image file, epoch, north angle
+// (degrees), COM offsets (fit-grid pixels, free parameters), weight and
+// pixel-weighting flag. The images are FITS files, which this reader does
+// not open.
+static void read_poset_set(Tokens &tk, shape_obs_file::Set &S)
+{
+    S.poset = 1;
+    S.delcor_state = 'c';
+    memset(&S.dd, 0, sizeof S.dd);
+    S.ndel = S.ndop = 0;
+    S.iradlaw = 0;
+    S.ioptlaw = tk.integer("optical law");
+    if (S.ioptlaw < 0) tk.fail("negative optical law index");
+    S.ephem = read_ephem(tk, "asteroid ephemeris points");
+    S.solephem = read_ephem(tk, "solar ephemeris points");
+    S.angle_per_pixel = (tk.real("angular pixel size") / 3600) * D2R;
+    S.nviews = tk.integer("views per frame");
+    if (S.nviews < 1) tk.fail("views per frame must be at least 1");
+    S.view_interval = tk.real("view interval") / 86400;
+    const std::string mode = tk.word("smearing mode");
+    if (mode == "center") S.v0 = S.nviews / 2;
+    else if (mode == "first") S.v0 = 0;
+    else tk.fail("smearing mode " + mode + " is not supported", SHAPE_E_UNSUPPORTED);
+    S.dir = tk.word("data directory");
+    const int nfr = tk.integer("frames");
+    if (nfr < 1) tk.fail("a set needs at least one frame");
+    for (int i = 0; i < nfr; i++) {
+        shape_obs_file::Set::PosFrame F;
+        F.name = tk.word("image file");
+        F.t0 = read_epoch(tk, "frame epoch");
+        F.northangle = tk.real("north angle") * D2R;
+        char st;
+        F.off[0] = tk.param("x offset", &st);
+        F.off[1] = tk.param("y offset", &st);
+        F.weight = tk.real("frame weight");
+        F.pixels_weighted = tk.integer("pixel-weighting flag");
+        S.pframes.push_back(F);
+    }
 }
 
 // The body of a lightcurve or heliocurve set (read_lghtcrv,
@@ -901,7 +953,7 @@ static void tie_obs_sets(std::vector<shape_obs_file::Set> &sets, const Tokens &t
     int sd = -1;
     for (size_t s = 0; s < sets.size(); s++) {
         shape_obs_file::Set &S = sets[s];
-        if (S.lightcurve) continue;              // no delay polynomial
+        if (S.lightcurve || S.poset) continue;   // no delay polynomial
         if (S.delcor_state != '=') { sd = (int)s; continue; }
         if (sd < 0) tk.fail("the first delay-correction polynomial cannot take the = state");
         const shape_obs_file::Set &T = sets[sd];
@@ -928,7 +980,7 @@ extern "C" {
 static int load_masks(shape_obs_file &o, int s, bool required)
 {
     shape_obs_file::Set &S = o.sets[s];
-    if (S.lightcurve) return SHAPE_OK;
+    if (S.lightcurve || S.poset) return SHAPE_OK;
     const int nf = (int)S.frames.size();
     const int nd = S.doppler ? 1 : S.ndel, np = S.ndop;
     const std::string dir = o.maskdir.empty() ? S.dir : o.maskdir;
@@ -1030,6 +1082,11 @@ int shape_obs_read(const char *path, shape_obs_file **out)
             const std::string type = tk.word("dataset type");
             if (type == "lightcurve" || type == "heliocurve") {
                 read_lghtcrv_set(tk, S);
+                o->sets.push_back(std::move(S));
+                continue;
+            }
+            if (type == "plane-of-sky") {
+                read_poset_set(tk, S);
                 o->sets.push_back(std::move(S));
                 continue;
             }
@@ -1141,7 +1198,7 @@ int shape_obs_nsets(const shape_obs_file *o) { return o ? (int)o->sets.size() : 
 int shape_obs_set_type(const shape_obs_file *o, int s)
 {
     if (!o || s < 0 || s >= (int)o->sets.size()) return shape::report_error(SHAPE_E_ARG, "obs_set_type: no such set");
-    return o->sets[s].lightcurve ? 2 : o->sets[s].doppler;
+    return o->sets[s].poset ? 3 : (o->sets[s].lightcurve ? 2 : o->sets[s].doppler);
 }
 
 int shape_obs_set(const shape_obs_file *o, int s, shape_deldop_set *set, int *iradlaw, int *nframes,
@@ -1254,7 +1311,7 @@ int shape_obs_frames_views(const shape_obs_file *o, int s, const shape_spin_stat
     if (!o || s < 0 || s >= (int)o->sets.size() || !spin || !opt || !views || !obs || !oneovervar)
         return shape::report_error(SHAPE_E_ARG, "obs_frames_views: invalid argument");
     const shape_obs_file::Set &S = o->sets[s];
-    if (S.lightcurve || S.doppler)
+    if (S.lightcurve || S.doppler || S.poset)
         return shape::report_error(SHAPE_E_ARG, "obs_frames_views: not a delay-Doppler set");
     return obs_deldop_views(S, spin, pos_n, km_per_pixel, opt, views, obs, oneovervar, sdev);
 }
@@ -1266,7 +1323,8 @@ int shape_obs_frames(const shape_obs_file *o, int s, const shape_spin_state *spi
     if (!o || s < 0 || s >= (int)o->sets.size() || !spin || !opt || !frames || !obs || !oneovervar)
         return shape::report_error(SHAPE_E_ARG, "obs_frames: invalid argument");
     const shape_obs_file::Set &S = o->sets[s];
-    if (S.lightcurve) return shape::report_error(SHAPE_E_ARG, "obs_frames: a lightcurve set (use shape_obs_lghtcrv)");
+    if (S.lightcurve || S.poset)
+        return shape::report_error(SHAPE_E_ARG, "obs_frames: a lightcurve or plane-of-sky set");
     if (S.doppler) return shape::report_error(SHAPE_E_ARG, "obs_frames: a Doppler set (use shape_obs_doppler)");
     if (S.nviews != 1)
         return shape::report_error(SHAPE_E_UNSUPPORTED, "obs_frames: smeared frames (use shape_obs_frames_views)");
@@ -1353,6 +1411,71 @@ int shape_obs_lghtcrv_info(const shape_obs_file *o, int s, int *ioptlaw, int *nc
 // offsets; each observation's magnitude turned into an intensity relative
 // to the Sun's (sun_appmag, the .par file's value for this set's optical
 // law) and its epoch light-time corrected the same way.
+int shape_obs_poset_info(const shape_obs_file *o, int s, int *ioptlaw, int *nframes)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size() || !o->sets[s].poset || !ioptlaw || !nframes)
+        return shape::report_error(SHAPE_E_ARG, "obs_poset_info: not a plane-of-sky set");
+    *ioptlaw = o->sets[s].ioptlaw;
+    *nframes = (int)o->sets[s].pframes.size();
+    return SHAPE_OK;
+}
+
+int shape_obs_poset_file(const shape_obs_file *o, int s, int frame, char *path, int size, int *pixels_weighted)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size() || !o->sets[s].poset || !path || size < 1 ||
+        frame < 0 || frame >= (int)o->sets[s].pframes.size())
+        return shape::report_error(SHAPE_E_ARG, "obs_poset_file: invalid argument");
+    const shape_obs_file::Set &S = o->sets[s];
+    const std::string full = S.dir + "/" + S.pframes[frame].name;
+    if ((int)full.size() >= size) return shape::report_error(SHAPE_E_ARG, "obs_poset_file: buffer too small");
+    memcpy(path, full.c_str(), full.size() + 1);
+    if (pixels_weighted) *pixels_weighted = S.pframes[frame].pixels_weighted;
+    return SHAPE_OK;
+}
+
+// read_poset's views (src/shape/read_dat.c:1520-1560) for one view per frame:
+// ephem2mat at the frame epoch, with light-time correction when asked (the
+// fit grid's km per pixel takes the distance before the correction, as
+// read_poset's does), then the spin realized at the corrected epochs.
+int shape_obs_poset(const shape_obs_file *o, int s, const shape_spin_state *spin, const shape_obs_options *opt,
+                    shape_poset_frame *frames)
+{
+    if (!o || s < 0 || s >= (int)o->sets.size() || !o->sets[s].poset || !spin || !opt || !frames)
+        return shape::report_error(SHAPE_E_ARG, "obs_poset: invalid argument");
+    const shape_obs_file::Set &S = o->sets[s];
+    if (S.nviews != 1)
+        return shape::report_error(SHAPE_E_UNSUPPORTED, "obs_poset: smeared plane-of-sky frames");
+    const double DAYSPERAU = 5.775518328e-3;   // src/shape/const.h:144
+    const double AU = 1.4959787061e8;         // km (src/shape/const.h:135)
+    const int nf = (int)S.pframes.size();
+    const shape_ephem_point *A = S.ephem.data(), *U = S.solephem.data();
+    const int na = (int)S.ephem.size(), nu = (int)S.solephem.size();
+    std::vector<double> t(nf), orb(3 * (size_t)nf), ae(9 * (size_t)nf), sp(3 * (size_t)nf);
+    for (int i = 0; i < nf; i++) {
+        shape_poset_frame &F = frames[i];
+        const shape_obs_file::Set::PosFrame &R = S.pframes[i];
+        double az, dist, dist1;
+        t[i] = R.t0;
+        if (int rc = shape_ephem_view(A, na, U, nu, t[i], F.oe, F.se, &orb[3 * (size_t)i], &F.solar_phase, &az, &dist))
+            return rc;
+        if (opt->perform_ltc) {
+            t[i] -= DAYSPERAU * dist;
+            if (int rc = shape_ephem_view(A, na, U, nu, t[i], F.oe, F.se, &orb[3 * (size_t)i], &F.solar_phase, &az,
+                                          &dist1))
+                return rc;
+        }
+        F.fit_km_per_pixel = S.angle_per_pixel * (dist * AU);
+        F.northangle = R.northangle;
+        F.xoff = R.off[0];
+        F.yoff = R.off[1];
+        F.weight = R.weight;
+    }
+    if (int rc = shape_realize_spin(spin, S.angleoff, S.omegaoff, nf, t.data(), orb.data(), ae.data(), sp.data()))
+        return rc;
+    for (int i = 0; i < nf; i++) memcpy(frames[i].ae, &ae[9 * (size_t)i], sizeof frames[i].ae);
+    return SHAPE_OK;
+}
+
 int shape_obs_lghtcrv(const shape_obs_file *o, int s, const shape_spin_state *spin, int pos_n, double km_per_pixel,
                       const shape_obs_options *opt, double sun_appmag, shape_lghtcrv_set *set,
                       shape_lghtcrv_point *points, double *x, double *t, double *obs, double *oneovervar)

@@ -111,6 +111,9 @@ def load_library(path=LIB_PATH):
     L.shape_engine_get_radar_overflow.argtypes = [vp, cd.dptr, C.c_int]
     L.shape_engine_finalize.argtypes = [vp]
     L.shape_engine_get_active.argtypes = [vp, vp, vp]
+    L.shape_obs_poset_info.argtypes = [vp, C.c_int, P(C.c_int), P(C.c_int)]
+    L.shape_obs_poset_file.argtypes = [vp, C.c_int, C.c_int, C.c_char_p, C.c_int, P(C.c_int)]
+    L.shape_obs_poset.argtypes = [vp, C.c_int, P(cd.SpinState), P(ObsOptions), P(cd.PosetFrame)]
     L.shape_engine_add_poset_set.argtypes = [vp, P(cd.PosetSet), C.c_int, P(cd.PosetFrame), cd.dptr, cd.dptr]
     L.shape_engine_get_poset.argtypes = [vp, C.c_int, C.c_int, cd.dptr, cd.dptr, P(cd.PosetResult)]
     L.shape_engine_set_scale.argtypes = [vp, C.c_int, C.c_double]
@@ -695,6 +698,22 @@ class ObsFile:
         ds = synth.LightcurveDataset(st, list(pts), x, t, obs, oov)
         ds.bind()
         return ds
+
+    def poset(self, s, spin, perform_ltc=1):
+        """A plane-of-sky set's frames (list of cd.PosetFrame with the
+        geometry filled), their image files and pixel-weighting flags."""
+        law, nf = C.c_int(), C.c_int()
+        _chk(self.L.shape_obs_poset_info(self.h, s, C.byref(law), C.byref(nf)))
+        frames = (cd.PosetFrame * nf.value)()
+        opt = ObsOptions(perform_ltc, 1.0, 0, 1)
+        _chk(self.L.shape_obs_poset(self.h, s, C.byref(spin), C.byref(opt), frames))
+        files = []
+        for k in range(nf.value):
+            buf = C.create_string_buffer(4096)
+            w = C.c_int()
+            _chk(self.L.shape_obs_poset_file(self.h, s, k, buf, 4096, C.byref(w)))
+            files.append((buf.value.decode(), w.value))
+        return list(frames), files, law.value
 
     def set_maskdir(self, path):
         """The .par file's mask directory: weighted frames' masks read from it."""

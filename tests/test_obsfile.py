@@ -5,6 +5,8 @@ delay-correction polynomial, dataset angle and spin offsets and ASCII and
 big-endian binary data files: every frame's observer and body matrices,
 spin vector, delay and Doppler offsets, COM bins, weight, dof,
 calibration, sdev, and its obs and 1/variance images, bit for bit."""
+import math
+
 import numpy as np
 import pytest
 
@@ -438,3 +440,63 @@ def test_obs_masks_match_reference(tmp_path, monkeypatch):
             assert np.array_equal(dob[off:off + n], ro[:n]) and np.array_equal(dov[off:off + n], rv[:n]), f
             off += n
         assert dfr[1].ndop == 45
+
+
+POS_SET = """0
+c 0 c 0 c 10.0
+c 0 c 0 c 0.05
+plane-of-sky
+0
+3
+2018 3 14 0 0 0  359.5 10.2 0.031
+2018 3 15 0 0 0  0.4 10.0 0.030
+2018 3 16 0 0 0  1.1 9.8 0.029
+3
+2018 3 14 0 0 0  170.0 -5.0 0.99
+2018 3 15 0 0 0  171.0 -5.4 0.99
+2018 3 16 0 0 0  172.0 -5.8 0.99
+0.25
+1 0.0 center
+imgs
+2
+f0.fits 2018 3 14 12 0 0  30.0  c 1.5 c -0.5  1.0 0
+f1.fits 2018 3 15 6 0 0  -12.5 f 0.25 c 0  2.0 1
+"""
+
+
+@pytest.mark.parametrize("ltc", [0, 1])
+def test_obs_poset_geometry(tmp_path, monkeypatch, ltc):
+    """A plane-of-sky set in the .obs grammar (read_poset): its frames'
+    observer, Sun and body matrices and solar phases equal those of a
+    lightcurve set with the same ephemerides and offsets whose calculated
+    epochs are the frames' epochs (a reader pinned to the reference's
+    read_lghtcrv); north angles to radians, COM offsets, weights, image
+    files and mask flags as written; the fit grid's km per pixel is the
+    angular pixel size times the distance before the light-time
+    correction."""
+    monkeypatch.chdir(tmp_path)
+    write_mod(tmp_path / "m.mod", cases.c1()[0], seed=3)
+    (tmp_path / "lc0.dat").write_text("".join("%.3f 14.0 0.02\n" % (2458192.0 + 0.2 * k) for k in range(5)))
+    lc = LC_SETS.replace("{CALC}", "2\n2458192.0 2458192.75").replace("{K}", "0")
+    (tmp_path / "t.obs").write_text("2\n" + POS_SET + lc)
+    o = eng.ObsFile("t.obs")
+    spin = eng.ModFile("m.mod").spin()
+    assert o.set_type(0) == 3 and o.set_type(1) == 2
+    frames, files, law = o.poset(0, spin, perform_ltc=ltc)
+    ds = o.lghtcrv(1, spin, 60, 0.03, perform_ltc=ltc)
+    assert law == 0 and len(frames) == 2
+    assert files == [("imgs/f0.fits", 0), ("imgs/f1.fits", 1)]
+    D2R = math.pi / 180.0
+    for f, (fr, p) in enumerate(zip(frames, ds.points)):
+        assert list(fr.oe) == list(p.oe) and list(fr.se) == list(p.se) and list(fr.ae) == list(p.ae), f
+        assert fr.solar_phase == p.solar_phase, f
+    np.testing.assert_allclose([frames[0].northangle, frames[1].northangle], [30.0 * D2R, -12.5 * D2R],
+                               rtol=1e-15)
+    assert (frames[0].xoff, frames[0].yoff, frames[1].xoff, frames[1].yoff) == (1.5, -0.5, 0.25, 0.0)
+    assert (frames[0].weight, frames[1].weight) == (1.0, 2.0)
+    rows = [(2458191.5 + k, r * D2R, d * D2R, a) for k, (r, d, a) in
+            enumerate([(359.5, 10.2, 0.031), (0.4, 10.0, 0.030), (1.1, 9.8, 0.029)])]
+    for fr, t0 in zip(frames, (2458192.0, 2458192.75)):
+        dist = eng.ephem_view(rows, t0)["dist"]
+        want = (0.25 / 3600) * D2R * (dist * 1.4959787061e8)
+        assert abs(fr.fit_km_per_pixel - want) <= 1e-15 * want
