@@ -135,7 +135,7 @@ def test_obs_doppler_set_matches_reference(tmp_path, monkeypatch, speckle):
 def test_obs_refusals(tmp_path, monkeypatch):
     monkeypatch.chdir(tmp_path)
     p = tmp_path / "u.obs"
-    p.write_text(OBS.replace("delay-doppler", "plane-of-sky"))
+    p.write_text(OBS.replace("delay-doppler", "radar-image"))
     with pytest.raises(eng.EngineError, match="error -4"):
         eng.ObsFile(p)
     p.write_text(OBS.replace("1 0.0 center", "0 60.0 center"))
