@@ -35,8 +35,9 @@
  * (src/shape/mkparlist.c:218-235), are pushed on every call.
  *
  * Supported inputs (anything else stops with bailout(), the reference's
- * error convention): one VERTEX component; delay-Doppler, Doppler and
- * lightcurve sets with one view per frame/point (speckle off); radar laws COSINELAW_DIFF,
+ * error convention): one VERTEX component; delay-Doppler, Doppler,
+ * lightcurve and plane-of-sky sets with one view per frame/point (speckle
+ * off; no bicubic plane-of-sky resampling); radar laws COSINELAW_DIFF,
  * GAUSSIANLAW, HAGFORSLAW, COSINELAW_QS and the three hybrids; optical laws
  * LAMBERTLAW, LOMMEL and KAASALAINEN; dd_gamma = 1; exclude_seen not naming
  * a set of the dataset.
@@ -134,6 +135,21 @@ static uint64_t b200_fingerprint(const struct par_t *par, const struct mod_t *mo
                 FNV(h, po); FNV(h, pv);
                 const struct dopview_t *v = &fr->view[dp->v0];
                 FNV(h, v->ae); FNV(h, v->oe); FNV(h, v->spin); FNV(h, v->dopoff);
+            }
+        } else if (set->type == POS) {
+            const struct poset_t *po = &set->desc.poset;
+            FNV(h, po->nframes); FNV(h, po->nviews); FNV(h, po->ioptlaw);
+            FNV(h, par->poset_resample); FNV(h, par->image_rebin);
+            for (int f = 0; f < po->nframes; f++) {
+                const struct posetfrm_t *fr = &po->frame[f];
+                const struct posetview_t *v = &fr->view[po->v0];
+                FNV(h, fr->ncol); FNV(h, fr->nrow); FNV(h, fr->pos.n); FNV(h, fr->pos.km_per_pixel);
+                FNV(h, fr->fit.km_per_pixel); FNV(h, fr->colcom_vig); FNV(h, fr->rowcom_vig);
+                FNV(h, fr->off[0].val); FNV(h, fr->off[1].val); FNV(h, fr->northangle);
+                FNV(h, fr->weight); FNV(h, fr->dof);
+                const void *po_ = fr->obs.b, *pv = fr->oneovervar;
+                FNV(h, po_); FNV(h, pv);
+                FNV(h, v->ae); FNV(h, v->oe); FNV(h, v->se); FNV(h, v->solar_phase);
             }
         } else if (set->type == LGHTCRV) {
             const struct lghtcrv_t *lc = &set->desc.lghtcrv;
@@ -309,8 +325,41 @@ static void b200_build(struct par_t *par, struct mod_t *mod, struct dat_t *dat)
             int rc = shape_engine_add_lghtcrv_set(g_eng, &L, P);
             free(x); free(t); free(obs); free(oov); free(P);
             b200_check(rc, "add_lghtcrv_set");
+        } else if (set->type == POS) {
+            struct poset_t *po = &set->desc.poset;
+            if (po->nviews != 1) b200_unsupported("plane-of-sky smearing (nviews > 1)");
+            shape_poset_set PS;
+            memset(&PS, 0, sizeof PS);
+            PS.law = optical_law_of(&mod->photo, po->ioptlaw);
+            PS.resample = par->poset_resample;
+            PS.rebin = par->image_rebin;
+            shape_poset_frame *F = calloc((size_t)po->nframes, sizeof *F);
+            size_t total = 0;
+            for (int f = 0; f < po->nframes; f++) total += (size_t)po->frame[f].ncol * po->frame[f].nrow;
+            double *obs = malloc(sizeof(double) * total), *oov = malloc(sizeof(double) * total);
+            size_t off = 0;
+            for (int f = 0; f < po->nframes; f++) {
+                struct posetfrm_t *fr = &po->frame[f];
+                struct posetview_t *v = &fr->view[po->v0];
+                shape_poset_frame *G = &F[f];
+                G->pos_n = fr->pos.n; G->km_per_pixel = fr->pos.km_per_pixel;
+                rm9(G->ae, v->ae); rm9(G->oe, v->oe); rm9(G->se, v->se);
+                G->solar_phase = v->solar_phase;
+                G->ncol = fr->ncol; G->nrow = fr->nrow; G->fit_km_per_pixel = fr->fit.km_per_pixel;
+                G->colcom_vig = fr->colcom_vig; G->rowcom_vig = fr->rowcom_vig;
+                G->xoff = fr->off[0].val; G->yoff = fr->off[1].val; G->northangle = fr->northangle;
+                G->weight = fr->weight; G->dof = fr->dof;
+                for (int i = 1; i <= fr->ncol; i++)
+                    for (int j = 1; j <= fr->nrow; j++, off++) {
+                        obs[off] = fr->obs.b[i][j];
+                        oov[off] = fr->oneovervar[i][j];
+                    }
+            }
+            int rc = shape_engine_add_poset_set(g_eng, &PS, po->nframes, F, obs, oov);
+            free(F); free(obs); free(oov);
+            b200_check(rc, "add_poset_set");
         } else {
-            b200_unsupported("plane-of-sky datasets");
+            b200_unsupported("dataset type");
         }
     }
     g_keep_pos = (par->action == WRITE);
@@ -337,10 +386,10 @@ static void b200_evaluate(struct par_t *par, struct mod_t *mod, struct dat_t *da
     /* flags of calc_fits (src/shape/calc_fits.c:349-354, 407-409) */
     par->posbnd = sm->posbnd;
     par->posbnd_logfactor = sm->posbnd_logfactor;
+    par->badposet = sm->badposet;
+    par->badposet_logfactor = sm->badposet_logfactor;
     par->badradar = sm->badradar;
     par->badradar_logfactor = sm->badradar_logfactor;
-    par->badposet = 0;
-    par->badposet_logfactor = 0.0;
 
     /* facet "seen" flags */
     int nf = c->real.nf;
@@ -363,6 +412,37 @@ static int total_frames(const struct dat_t *dat)
 }
 
 /* Per-frame limits, log-factor, cal and chi2 from the engine's results. */
+/* Plane-of-sky frames: fit images and sky brightness written back, and
+ * with_chi2: cal, frame and set chi-square (chi2_poset's side effects). */
+static void copy_poset_results(struct dat_t *dat, int with_chi2)
+{
+    for (int s = 0; s < dat->nsets; s++) {
+        if (dat->set[s].type != POS) continue;
+        struct poset_t *po = &dat->set[s].desc.poset;
+        double set_chi2 = 0.0;
+        for (int f = 0; f < po->nframes; f++) {
+            struct posetfrm_t *fr = &po->frame[f];
+            const int n = fr->pos.n, side = 2 * n + 1;
+            double *fit = malloc(sizeof(double) * (size_t)fr->ncol * fr->nrow);
+            double *b = malloc(sizeof(double) * (size_t)side * side);
+            shape_poset_result r;
+            b200_check(shape_engine_get_poset(g_eng, s, f, fit, b, &r), "get_poset");
+            size_t k = 0;
+            for (int i = 1; i <= fr->ncol; i++)
+                for (int j = 1; j <= fr->nrow; j++) fr->fit.b[i][j] = fit[k++];
+            for (int i = -n; i <= n; i++)
+                for (int j = -n; j <= n; j++) fr->pos.b[i][j] = b[(size_t)(i + n) * side + (size_t)(j + n)];
+            free(fit); free(b);
+            if (with_chi2) {
+                fr->cal.val = r.cal;
+                fr->chi2 = r.chi2;
+                set_chi2 += r.chi2;
+            }
+        }
+        if (with_chi2) dat->set[s].chi2 = set_chi2;
+    }
+}
+
 static void copy_frame_results(struct dat_t *dat, int with_chi2)
 {
     int nfr = total_frames(dat);
@@ -429,6 +509,7 @@ void SHAPE_B200_CALC_FITS(struct par_t *par, struct mod_t *mod, struct dat_t *da
     memset(&sm, 0, sizeof sm);
     b200_evaluate(par, mod, dat, &sm);
     copy_frame_results(dat, 0);
+    copy_poset_results(dat, 0);
     size_t maxd = 1;
     for (int s = 0; s < dat->nsets; s++) {
         if (dat->set[s].type == DELAY)
@@ -505,6 +586,7 @@ double SHAPE_B200_CALC_FITS_CHI2(struct par_t *par, struct mod_t *mod, struct da
     memset(&sm, 0, sizeof sm);
     b200_evaluate(par, mod, dat, &sm);
     copy_frame_results(dat, 1);
+    copy_poset_results(dat, 1);
     for (int s = 0; s < dat->nsets; s++) {
         struct set_t *set = &dat->set[s];
         if (set->type != LGHTCRV) continue;

@@ -44,7 +44,24 @@ def _dop_synth(m):
 
 
 def _inputs(name):
-    """(model, params, deldops, lightcurves, dopplers)."""
+    """(model, params, deldops, lightcurves, dopplers, plane-of-sky sets)."""
+    if name == "poset":
+        from oracle.bindings import Reference
+        from shape_b200 import synth
+        R = Reference()
+        m = synth.ellipsoid_model()
+        p = synth.eval_params()
+
+        def syn(ds, params):
+            s = R.session(m, params, posets=[ds])
+            s.evaluate()
+            return [s.poset_frame(0, k, fr)[0] for k, fr in enumerate(ds.frames)]
+        ps = synth.poset_dataset(synthesize=syn, params=p, resample=4, rebin=True, fit_scale=2.6)
+        return m, p, [], [], [], [ps]
+    return _inputs_radar(name) + ([],)
+
+
+def _inputs_radar(name):
     if name == "mixed":
         m = gc.octa3_model()
         p = gc.P_DEFAULT
@@ -72,7 +89,7 @@ def _chi2s(L, sess, s, nfr):
     return d.value, st.value, fc, fk
 
 
-def _compare_outputs(a, b, dds, lcs, dps):
+def _compare_outputs(a, b, dds, lcs, dps, pss=()):
     fa, fb = a.flags(), b.flags()
     assert fa["posbnd"] == fb["posbnd"] and fa["badradar"] == fb["badradar"]
     for k in ("posbnd_logfactor", "badradar_logfactor"):
@@ -103,6 +120,13 @@ def _compare_outputs(a, b, dds, lcs, dps):
             # overflow spectrum terms written back for chi2_doppler (o2: bin count, m2)
             assert ra["res"]["o2"] == rb["res"]["o2"], (s, f)
             assert abs(ra["res"]["m2"] - rb["res"]["m2"]) <= 1e-12 * max(1e-300, abs(ra["res"]["m2"]))
+    for k, ds in enumerate(pss):
+        s = len(dds) + len(dps) + len(lcs) + k
+        for f, fr in enumerate(ds.frames):
+            fa_, ba_, _, _ = a.poset_frame(s, f, fr)
+            fb_, bb_, _, _ = b.poset_frame(s, f, fr)
+            assert np.abs(fa_ - fb_).max() <= 1e-12 * max(fa_.max(), 1e-300), (s, f)
+            assert np.abs(ba_ - bb_).max() <= 1e-12 * ba_.max(), (s, f)
     for k, ds in enumerate(lcs):
         s = len(dds) + len(dps) + k
         ya, yb = a.lghtcrv(s, ds), b.lghtcrv(s, ds)
@@ -111,7 +135,7 @@ def _compare_outputs(a, b, dds, lcs, dps):
 
 
 CASES = ["c1", "c1_outbnd", "small_short", "small_long_mod_spb3_nsinc3", "law_hagfors_cosine",
-         "kaasalainen", "lommel", "c3_short", "dop_small", "dop_overflow", "dop_overflow_far", "mixed"]
+         "kaasalainen", "lommel", "c3_short", "dop_small", "dop_overflow", "dop_overflow_far", "mixed", "poset"]
 
 
 @pytest.mark.parametrize("form", ["plain_fp64", "batched_fp64"])
@@ -119,10 +143,10 @@ CASES = ["c1", "c1_outbnd", "small_short", "small_long_mod_spb3_nsinc3", "law_ha
 def test_dropin_calc_fits_matches_reference(dropin, name, form, monkeypatch, cuda_device):
     ref, L = dropin
     monkeypatch.setenv("SHAPE_B200_FORM", form)
-    m, p, dds, lcs, dps = _inputs(name)
-    sa = ref.session(m, p, deldops=dds, lghtcrvs=lcs, dopplers=dps)
-    sb = ref.session(m, p, deldops=dds, lghtcrvs=lcs, dopplers=dps)
-    sc = ref.session(m, p, deldops=dds, lghtcrvs=lcs, dopplers=dps)
+    m, p, dds, lcs, dps, pss = _inputs(name)
+    sa = ref.session(m, p, deldops=dds, lghtcrvs=lcs, dopplers=dps, posets=pss)
+    sb = ref.session(m, p, deldops=dds, lghtcrvs=lcs, dopplers=dps, posets=pss)
+    sc = ref.session(m, p, deldops=dds, lghtcrvs=lcs, dopplers=dps, posets=pss)
     for trial, scale0 in enumerate((None, 1.03)):
         if scale0 is not None:       # a bestfit trial: engine reused, parameters pushed
             for s in (sa, sb, sc):
@@ -132,9 +156,11 @@ def test_dropin_calc_fits_matches_reference(dropin, name, form, monkeypatch, cud
         cc = L.ref_dropin_objective(sc.h)
         assert abs(cb - ca) <= 1e-10 * abs(ca), (trial, ca, cb)
         assert abs(cc - ca) <= 1e-10 * abs(ca), (trial, ca, cc)
-        _compare_outputs(sa, sb, dds, lcs, dps)
+        _compare_outputs(sa, sb, dds, lcs, dps, pss)
         fa, fc = sa.flags(), sc.flags()
         assert (fa["posbnd"], fa["badradar"]) == (fc["posbnd"], fc["badradar"])
+        if pss:
+            assert sa.badposet()[0] == sb.badposet()[0] == sc.badposet()[0]
         radar = list(dds) + list(dps)
         for s in range(len(radar) + len(lcs)):
             nfr = radar[s].nframes if s < len(radar) else 1
